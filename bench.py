@@ -1,0 +1,325 @@
+#!/usr/bin/env python
+"""Benchmark: f128 GEMM GFLOP/s on one B200 (chosen Ozaki-II int8 path vs the
+plain CUDA-core dd path), plus the CPU baseline and an end-to-end number.
+
+Workload: C = A * B, m = n = k = 2048, full double-double entries (SplitMix64
+seed 0, hi ~ U[-1,1), lo = hi * 2^-53 * U[-1,1)). One step = one GEMM.
+  value  = chosen-path GFLOP/s (2mnk per step) with inputs resident in HBM,
+           device-timed with CUDA events; L2 flushed between timed steps.
+  e2e    = the same GEMM through the host-pointer C ABI (hp_f128_gemm) from
+           pinned host buffers, copies inside the timed region.
+Multi-GPU (torchrun): every rank runs its own independent GEMM (weak scaling,
+no collective in the data path); value = all ranks' flops / max rank time.
+
+--impl reference times the reference algorithm on the host cores (the C++
+restatement in oracle/, since the Rust reference cannot be built here) on a
+bounded sample of C rows per step.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+M = N = K = 2048
+METRIC = "f128 GEMM GFLOP/s; SPD solves/s at ≤1e-25 rel err: chosen vs plain, 1 B200"
+WORKLOAD = "f128 GEMM C=A*B, m=n=k=2048, full double-double entries (SplitMix64 seed 0)"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------- clocks
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+        self.th = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self.th:
+            self.th.join(timeout=2)
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if r[4 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ---------------------------------------------------------------- helpers
+def peaks():
+    p = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return d.get("hbm_gbs", 6650.0), d.get("bf16_tflops", 1590.0), "measured"
+    return 6650.0, 1590.0, "fallback"
+
+
+def cpu_sample_gflops(target_s: float = 12.0) -> dict:
+    """Oracle (C++ restatement of linalg.rs:150 gemm) on a bounded row sample."""
+    import numpy as np
+
+    import oracle
+    from quadprec_b200.workloads import gemm_operands
+
+    a, b = gemm_operands(M, N, K, seed=0)
+    threads = oracle.num_threads()
+    rows = max(1, threads)
+    t0 = time.perf_counter()
+    oracle.gemm(a, b, M, N, K, rows=(0, rows))
+    dt = time.perf_counter() - t0
+    reps = max(1, min(64, int(target_s / max(dt, 1e-3))))
+    total_rows = 0
+    t0 = time.perf_counter()
+    for r in range(reps):
+        r0 = (r * rows) % M
+        oracle.gemm(a, b, M, N, K, rows=(r0, min(M, r0 + rows)))
+        total_rows += min(M, r0 + rows) - r0
+    dt = time.perf_counter() - t0
+    return {"value": 2.0 * total_rows * N * K / dt / 1e9, "unit": "GFLOP/s", "cores": threads, "kind": "port",
+            "sample": f"{total_rows} of {M} rows of C (each a full 2048x2048 dd dot-product sweep), "
+                      f"{dt:.1f} s; oracle/hp_oracle.cpp restates crates/quad/src/linalg.rs:150-165"}
+
+
+def run_reference(args):
+    """--impl reference: the reference algorithm on host cores (rank 0 only)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    import oracle
+    from quadprec_b200.workloads import gemm_operands
+
+    a, b = gemm_operands(M, N, K, seed=0)
+    threads = oracle.num_threads()
+    rows = threads
+    for w in range(args.warmup):
+        oracle.gemm(a, b, M, N, K, rows=(0, rows))
+    t0 = time.perf_counter()
+    done = 0
+    for s in range(args.steps):
+        r0 = (s * rows) % M
+        oracle.gemm(a, b, M, N, K, rows=(r0, r0 + rows))
+        done += rows
+    dt = time.perf_counter() - t0
+    v = 2.0 * done * N * K / dt / 1e9
+    line = {"metric": METRIC, "value": v, "unit": "GFLOP/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dt * 1e3 / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64 (double-double EFT arithmetic)",
+            "data": "synthetic", "impl": "reference",
+            "config": {"workload": WORKLOAD, "m": M, "n": N, "k": K,
+                       "step": f"{rows} rows of C per step (bounded sample of the 2048^3 GEMM)"},
+            "cpu_baseline": {"value": v, "unit": "GFLOP/s", "cores": threads, "kind": "port",
+                             "sample": f"{done} rows of C over {args.steps} steps; C++ restatement of "
+                                       "crates/quad/src/linalg.rs:150-165 (no Rust toolchain on this image)"},
+            "e2e": {"value": v, "unit": "GFLOP/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ---------------------------------------------------------------- main arm
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--plain-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+
+    import numpy as np
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+    import quadprec_b200 as hp
+    from quadprec_b200.workloads import gemm_operands
+
+    assert hp.device_ok(), "no sm_100 device"
+    a_np, b_np = gemm_operands(M, N, K, seed=rank)
+    dev = torch.device("cuda", local)
+    A = torch.from_numpy(a_np).to(dev)
+    B = torch.from_numpy(b_np).to(dev)
+    C = torch.empty((M, N, 2), dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def timed(mode, steps, warmup):
+        for _ in range(warmup):
+            hp.f128_gemm_dev(A, B, C, M, N, K, mode, stream=sptr)
+        torch.cuda.synchronize()
+        barrier()
+        torch.cuda.synchronize()
+        evs = []
+        for _ in range(steps):
+            flush.fill_(1.0)  # L2 flush, outside the timed interval
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            hp.f128_gemm_dev(A, B, C, M, N, K, mode, stream=sptr)
+            e.record(stream)
+            evs.append((s, e))
+        torch.cuda.synchronize()
+        barrier()
+        ms = sum(s.elapsed_time(e) for s, e in evs) / steps
+        if dist is not None:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms
+
+    flops = 2.0 * M * N * K
+    clk = ClockSampler(local)
+    clk.start()
+    ms_chosen = timed(hp.OZAKI, args.steps, args.warmup)
+    clocks = clk.stop()
+    ms_plain = timed(hp.PLAIN, args.plain_steps, 1)
+
+    # correctness spot check of the timed output against the plain result
+    hp.f128_gemm_dev(A, B, C, M, N, K, hp.OZAKI, stream=sptr)
+    torch.cuda.synchronize()
+    c_oz = C.cpu().numpy()
+    hp.f128_gemm_dev(A, B, C, M, N, K, hp.PLAIN, stream=sptr)
+    torch.cuda.synchronize()
+    c_pl = C.cpu().numpy()
+    diff = (c_oz[..., 0] - c_pl[..., 0]) + (c_oz[..., 1] - c_pl[..., 1])
+    absab = np.abs(a_np[..., 0]) @ np.abs(b_np[..., 0])
+    rel_err = float(np.linalg.norm(diff) / np.linalg.norm(absab))
+
+    # phase timing of one chosen-path step (dominant kernel roofline)
+    flush.fill_(1.0)
+    torch.cuda.synchronize()
+    hp.profile_enable(True)
+    hp.f128_gemm_dev(A, B, C, M, N, K, hp.OZAKI, stream=sptr)
+    phases = hp.profile_read()
+    hp.profile_enable(False)
+
+    L = 30
+    hbm_gbs, bf16_tf, peak_kind = peaks()
+    i8_peak = 2.0 * bf16_tf  # dense int8 issue rate is twice dense bf16 on B200
+    mm = phases.get("i8_gemm", float("nan"))
+    i8_tops = L * 2.0 * M * N * K / (mm * 1e-3) / 1e12
+    res_ms = phases.get("residues", float("nan"))
+    res_bytes = 2 * (M * K * 16) + L * (M * K + N * K)
+    crt_ms = phases.get("crt", float("nan"))
+    crt_bytes = L * M * N + M * N * 16
+    roofline = {"bound": "tensor", "kernel": "i8_gemm_mod_kernel (tcgen05.mma kind::i8, one launch for all "
+                "30 moduli)", "achieved": i8_tops, "peak": i8_peak, "unit": "TOPS (int8)",
+                "frac": i8_tops / i8_peak, "traffic": None,
+                "peak_source": f"2 x {peak_kind} dense bf16 ({bf16_tf} TFLOP/s) in MEASURED_PEAKS.json",
+                "algorithmic": f"{L} moduli x 2mnk int8 ops = {L * 2.0 * M * N * K:.3e} per launch"}
+    phase_report = {k: round(v, 4) for k, v in phases.items()}
+    phase_roofline = {
+        "residues_hbm_frac": (res_bytes / (res_ms * 1e-3) / 1e9) / hbm_gbs if res_ms == res_ms else None,
+        "crt_hbm_frac": (crt_bytes / (crt_ms * 1e-3) / 1e9) / hbm_gbs if crt_ms == crt_ms else None,
+    }
+
+    # end to end through the host-pointer C ABI (pinned host buffers)
+    ha = torch.from_numpy(a_np).pin_memory()
+    hb = torch.from_numpy(b_np).pin_memory()
+    hc = torch.empty((M, N, 2), dtype=torch.float64).pin_memory()
+    lib = hp.lib()
+    for _ in range(2):
+        hp.check(lib.hp_f128_gemm(ha.data_ptr(), hb.data_ptr(), hc.data_ptr(), M, N, K, hp.OZAKI))
+    barrier()
+    e2e_steps = max(3, args.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        hp.check(lib.hp_f128_gemm(ha.data_ptr(), hb.data_ptr(), hc.data_ptr(), M, N, K, hp.OZAKI))
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if dist is not None:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_sample_gflops()
+
+    value = world * flops / (ms_chosen * 1e-3) / 1e9
+    plain_value = world * flops / (ms_plain * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": "GFLOP/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_chosen, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "int8 residues -> int32 (exact) + f64 EFT (double-double result)",
+        "data": "synthetic",
+        "config": {"workload": WORKLOAD, "m": M, "n": N, "k": K, "mode": "ozaki (Ozaki-II, 30 int8 moduli)",
+                   "l2": "flushed between timed steps (256 MiB write, untimed)",
+                   "parallelism": f"{world} independent GEMMs (one per GPU)"},
+        "plain": {"value": plain_value, "unit": "GFLOP/s", "ms_per_step": ms_plain, "steps": args.plain_steps,
+                  "mode": "plain CUDA-core dd FMA, bit-identical to the reference"},
+        "chosen_over_plain": value / plain_value,
+        "normwise_rel_err_vs_plain": rel_err,
+        "e2e": {"value": world * flops / e2e_s / 1e9, "unit": "GFLOP/s",
+                "h2d_bytes_per_step": int(2 * M * K * 16), "d2h_bytes_per_step": int(M * N * 16),
+                "path": "hp_f128_gemm (host pointers, pinned), copies inside the timed region"},
+        "roofline": roofline, "phases_ms": phase_report, "phase_roofline": phase_roofline,
+        "gpu_launches": 6 * args.steps,
+        "clocks": clocks,
+    }
+    if cpu is not None:
+        line["cpu_baseline"] = cpu
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,111 @@
+/*
+ * hyperprec_gpu.h -- C ABI of the B200 (sm_100a) extended-precision
+ * linear-algebra library (quadprec_b200/libhyperprec_gpu.so).
+ *
+ * Each entry point replaces one public function of hyperprec (m0at/quadprec)
+ * and keeps its argument meaning; the Rust signature it replaces is cited at
+ * each declaration (paths relative to the hyperprec repository).
+ *
+ * Data layout is the reference's in-memory layout, so a Rust caller passes
+ * `slice.as_ptr() as *const f64` without conversion:
+ *   f128            = { double hi; double lo; }            (16 bytes)
+ *   MultiFloat<N>   = { double limbs[N]; } most significant first
+ *   matrices        = row-major, dense, no leading dimension.
+ *
+ * Conventions
+ *   - Return value: HP_OK (0) or a negative HP_ERR_* code; nothing aborts.
+ *     hp_last_error() returns a thread-local message for the last failure.
+ *   - Plain entry points take HOST pointers: they copy inputs to the GPU,
+ *     compute on the library's stream, copy results back and return when the
+ *     results are in host memory (synchronous, like the Rust functions).
+ *   - *_dev entry points take DEVICE pointers and a cudaStream_t (passed as
+ *     void*; NULL = legacy default stream). They are stream-ordered and
+ *     return after enqueueing; status codes that depend on data (e.g. a
+ *     failed Cholesky pivot) are only available from the host-pointer form.
+ *   - Sizes of zero are valid and do nothing. NULL pointers with non-zero
+ *     sizes return HP_ERR_INVALID_ARG. The Rust wrapper keeps the
+ *     reference's assert_eq! length checks before calling (slices carry
+ *     lengths; raw pointers do not).
+ *   - No CPU fallback exists: without a usable CUDA device every compute
+ *     entry point returns HP_ERR_CUDA.
+ */
+#ifndef HYPERPREC_GPU_H
+#define HYPERPREC_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define HP_OK 0
+#define HP_ERR_INVALID_ARG (-1)  /* null pointer, overflow, bad mode, size limit */
+#define HP_ERR_NOT_SPD (-2)      /* Cholesky pivot <= 0 (linalg.rs:54-57)          */
+#define HP_ERR_NO_CONVERGE (-3)  /* iteration limit reached (linalg.rs:361)         */
+#define HP_ERR_CUDA (-4)         /* CUDA runtime / launch failure, or no device    */
+#define HP_ERR_TIMEOUT (-5)      /* a bounded device-side wait gave up              */
+#define HP_ERR_UNSUPPORTED (-6)  /* valid request this build does not support      */
+
+/* ---- GEMM modes ---- */
+#define HP_MODE_PLAIN 0 /* CUDA-core dd/qd FMA; bit-identical to the reference */
+#define HP_MODE_OZAKI 1 /* exact int8 residue split on tcgen05 tensor cores     */
+
+/* Library / device information. */
+const char* hp_last_error(void);
+const char* hp_version(void);
+/* 1 if a CUDA device of compute capability 10.0 is visible, else 0. */
+int hp_device_ok(void);
+
+/* Phase timing for benchmarks (no counterpart in the reference). While
+ * enabled, the multi-kernel drivers record a CUDA event at each phase
+ * boundary on their stream; hp_profile_read() waits for the last one and
+ * returns up to max_phases durations in ms (phase i ends at mark i+1) and a
+ * comma-separated list of phase names. Not thread-safe; off by default. */
+void hp_profile_enable(int on);
+int hp_profile_read(double* ms, int max_phases, char* names, size_t names_len);
+
+/* ------------------------------------------------------------------------
+ * f128 GEMM
+ * replaces: pub fn gemm(a: &[f128], b: &[f128], c: &mut [f128],
+ *                       m: usize, n: usize, k: usize)
+ *           crates/quad/src/linalg.rs:150-165
+ * C (m x n) = A (m x k) * B (k x n).
+ * HP_MODE_PLAIN: each C entry is accumulated s += a*b in k order with the
+ * reference's f128 Mul and Add, so C is bit-identical to the reference.
+ * HP_MODE_OZAKI: normwise relative error <= 4*k*2^-104 against the same.
+ * ---------------------------------------------------------------------- */
+int hp_f128_gemm(const double* a, const double* b, double* c, size_t m, size_t n, size_t k,
+                 int mode);
+/* replaces: pub fn gemm_atb(...)  crates/quad/src/linalg.rs:168-182
+ * C (m x n) = A^T * B with A stored k x m. */
+int hp_f128_gemm_atb(const double* a, const double* b, double* c, size_t m, size_t n, size_t k,
+                     int mode);
+/* Device-pointer forms of the two calls above. */
+int hp_f128_gemm_dev(const double* a, const double* b, double* c, size_t m, size_t n, size_t k,
+                     int mode, void* stream);
+int hp_f128_gemm_atb_dev(const double* a, const double* b, double* c, size_t m, size_t n,
+                         size_t k, int mode, void* stream);
+
+/* ------------------------------------------------------------------------
+ * f256 (MultiFloat<4>) GEMM
+ * replaces: pub fn mf_gemm<const N: usize>(a, b, c, m, n, k)   (N = 4)
+ *           crates/quad/src/multifloat/linalg.rs:39-61
+ *           pub fn mf_gemm_atb<const N: usize>(...)            (N = 4)
+ *           crates/quad/src/multifloat/linalg.rs:64-85
+ * HP_MODE_PLAIN is bit-identical to the reference.
+ * ---------------------------------------------------------------------- */
+int hp_f256_gemm(const double* a, const double* b, double* c, size_t m, size_t n, size_t k,
+                 int mode);
+int hp_f256_gemm_atb(const double* a, const double* b, double* c, size_t m, size_t n, size_t k,
+                     int mode);
+int hp_f256_gemm_dev(const double* a, const double* b, double* c, size_t m, size_t n, size_t k,
+                     int mode, void* stream);
+int hp_f256_gemm_atb_dev(const double* a, const double* b, double* c, size_t m, size_t n,
+                         size_t k, int mode, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HYPERPREC_GPU_H */

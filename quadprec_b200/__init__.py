@@ -1,0 +1,139 @@
+"""quadprec_b200: ctypes binding of the B200 extended-precision library.
+
+The product is the C ABI in ``include/hyperprec_gpu.h`` implemented by
+``libhyperprec_gpu.so`` (hand-written sm_100a CUDA). This module only loads
+that library and converts numpy/torch buffers to pointers for the test suite
+and ``bench.py``. There is no CPU fallback: if the library or a CUDA device is
+missing, calls raise.
+
+Arrays use the reference's layout: an f128 matrix is float64 of shape
+(rows, cols, 2) (hi, lo); an f256 matrix is (rows, cols, 4).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libhyperprec_gpu.so")
+
+HP_OK = 0
+HP_ERR_INVALID_ARG = -1
+HP_ERR_NOT_SPD = -2
+HP_ERR_NO_CONVERGE = -3
+HP_ERR_CUDA = -4
+HP_ERR_TIMEOUT = -5
+HP_ERR_UNSUPPORTED = -6
+
+PLAIN = 0
+OZAKI = 1
+
+_lib = None
+_d = ctypes.POINTER(ctypes.c_double)
+_sz = ctypes.c_size_t
+_vp = ctypes.c_void_p
+_i64p = ctypes.POINTER(ctypes.c_int64)
+
+
+class HPError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"hyperprec error {code}: {msg}")
+        self.code = code
+
+
+# name -> (argtypes, restype); kept in step with include/hyperprec_gpu.h
+SIGNATURES = {
+    "hp_last_error": ([], ctypes.c_char_p),
+    "hp_version": ([], ctypes.c_char_p),
+    "hp_device_ok": ([], ctypes.c_int),
+    "hp_profile_enable": ([ctypes.c_int], None),
+    "hp_profile_read": ([_d, ctypes.c_int, ctypes.c_char_p, _sz], ctypes.c_int),
+    "hp_f128_gemm": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int], ctypes.c_int),
+    "hp_f128_gemm_atb": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int], ctypes.c_int),
+    "hp_f128_gemm_dev": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int, _vp], ctypes.c_int),
+    "hp_f128_gemm_atb_dev": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int, _vp], ctypes.c_int),
+    "hp_f256_gemm": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int], ctypes.c_int),
+    "hp_f256_gemm_atb": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int], ctypes.c_int),
+    "hp_f256_gemm_dev": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int, _vp], ctypes.c_int),
+    "hp_f256_gemm_atb_dev": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int, _vp], ctypes.c_int),
+}
+
+
+def lib():
+    """Load libhyperprec_gpu.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise OSError(f"{LIB_PATH} is missing: run quadprec_b200.build.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, (args, res) in SIGNATURES.items():
+            f = getattr(L, name)
+            f.argtypes = args
+            f.restype = res
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> None:
+    if rc != HP_OK:
+        raise HPError(rc, (lib().hp_last_error() or b"").decode())
+
+
+def _ptr(a) -> int:
+    if isinstance(a, np.ndarray):
+        assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+        return a.ctypes.data
+    return int(a.data_ptr())  # torch tensor (host pinned or device)
+
+
+def _c(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def device_ok() -> bool:
+    return bool(lib().hp_device_ok())
+
+
+def profile_enable(on: bool = True) -> None:
+    lib().hp_profile_enable(1 if on else 0)
+
+
+def profile_read() -> dict:
+    """Phase durations (ms) recorded since profile_enable(); waits for them."""
+    ms = (ctypes.c_double * 32)()
+    names = ctypes.create_string_buffer(1024)
+    n = lib().hp_profile_read(ms, 32, names, 1024)
+    keys = names.value.decode().split(",") if n else []
+    return {k: ms[i] for i, k in enumerate(keys)}
+
+
+# ---------------- GEMM ----------------
+def f128_gemm(a, b, m, n, k, mode=PLAIN, atb=False) -> np.ndarray:
+    """linalg.rs:150 gemm / :168 gemm_atb through the host-pointer C ABI."""
+    a, b = _c(a), _c(b)
+    c = np.empty((m, n, 2))
+    fn = lib().hp_f128_gemm_atb if atb else lib().hp_f128_gemm
+    check(fn(_ptr(a), _ptr(b), _ptr(c), m, n, k, mode))
+    return c
+
+
+def f256_gemm(a, b, m, n, k, mode=PLAIN, atb=False) -> np.ndarray:
+    """multifloat/linalg.rs:39 mf_gemm / :64 mf_gemm_atb with N = 4."""
+    a, b = _c(a), _c(b)
+    c = np.empty((m, n, 4))
+    fn = lib().hp_f256_gemm_atb if atb else lib().hp_f256_gemm
+    check(fn(_ptr(a), _ptr(b), _ptr(c), m, n, k, mode))
+    return c
+
+
+def f128_gemm_dev(a, b, c, m, n, k, mode=PLAIN, atb=False, stream=0) -> None:
+    """Device-pointer form; a, b, c are CUDA tensors (float64, AoS)."""
+    fn = lib().hp_f128_gemm_atb_dev if atb else lib().hp_f128_gemm_dev
+    check(fn(_ptr(a), _ptr(b), _ptr(c), m, n, k, mode, stream))
+
+
+def f256_gemm_dev(a, b, c, m, n, k, mode=PLAIN, atb=False, stream=0) -> None:
+    fn = lib().hp_f256_gemm_atb_dev if atb else lib().hp_f256_gemm_dev
+    check(fn(_ptr(a), _ptr(b), _ptr(c), m, n, k, mode, stream))

@@ -1,0 +1,800 @@
+// Exact extended-precision GEMM on the int8 tensor cores (Ozaki scheme II:
+// residue number system + Chinese remainder reconstruction).
+//
+// For C = op(A) * B with f128 entries:
+//  1. Row i of op(A) and column j of B are scaled by powers of two so that
+//     every entry becomes an integer of at most BETA bits:
+//        X_ip = rint(A_ip * 2^sa_i),  Y_pj = rint(B_pj * 2^sb_j).
+//     This rounding is the only approximation (|error| <= 2^-BETA of the
+//     row/column maximum, per limb).
+//  2. For each of L pairwise-coprime moduli m_l <= 256, X and Y are reduced
+//     to balanced int8 residues (exact integer arithmetic).
+//  3. One int8 GEMM per modulus on tcgen05 (int32 accumulation in TMEM,
+//     exact while k * 2^14 < 2^31); the epilogue reduces each int32 to its
+//     residue mod m_l and stores one byte.
+//  4. The CRT combines the L residues into the exact integer
+//     Z_ij = sum_p X_ip Y_pj (|Z| < M/4, M = prod m_l), which is rounded
+//     once to f128 and scaled by 2^-(sa_i + sb_j).
+// L is the smallest count with log2 M >= 2*BETA + ceil(log2 k) + 2.
+//
+// The reference computes the same product with f128 multiply-adds
+// (crates/quad/src/linalg.rs:150-182); this path returns that product to
+// within 2^-(BETA-3) normwise, i.e. inside the 4*k*2^-104 tolerance.
+#include <cudaTypedefs.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "hp_arith.cuh"
+#include "hp_runtime.cuh"
+#include "kernels.cuh"
+#include "sm100_ptx.cuh"
+
+namespace hp {
+namespace ozaki {
+
+constexpr int MAXL = 49;        // number of pairwise-coprime moduli <= 256 in the table
+constexpr int NDIG = 5;         // base-2^22 digits of a scaled integer (110 bits)
+constexpr int CRT_BITS = 39;    // chunk width of the CRT accumulators
+constexpr int NCMAX = 10;       // chunks needed for M < 2^342
+constexpr int BETA_DD = 106;    // bits kept per f128 operand entry
+constexpr int EXP_NONFINITE = 0x7FF;
+
+struct ModTable {
+  int mod[MAXL];
+  uint32_t magic[MAXL];   // floor(2^32 / m)
+  uint32_t offset[MAXL];  // m * ceil(2^31 / m): makes |x| <= 2^30 + 2^27 non-negative
+  int pw[MAXL][NDIG];     // 2^(22 c) mod m, balanced into [-m/2, m/2]
+};
+__constant__ ModTable c_tab;
+
+struct CrtTable {
+  int L, nc;
+  double w[MAXL][NCMAX];  // W_l = (M/m_l) * ((M/m_l)^-1 mod m_l) in 39-bit chunks
+  double mchunk[NCMAX];   // M in 39-bit chunks
+  double inv_m;           // 1 / M (rounded)
+};
+
+// ---------------------------------------------------------------------------
+// Host tables
+// ---------------------------------------------------------------------------
+struct HostTables {
+  ModTable mt;
+  std::vector<CrtTable> crt;  // index L (1..MAXL)
+  double cum_log2[MAXL + 1];
+};
+
+// Little-endian base-2^32 unsigned big integer (host only, table set-up).
+struct Big {
+  std::vector<uint32_t> d;
+};
+static void big_mul_small(Big& a, uint32_t m) {
+  uint64_t carry = 0;
+  for (auto& x : a.d) {
+    uint64_t t = (uint64_t)x * m + carry;
+    x = (uint32_t)t;
+    carry = t >> 32;
+  }
+  if (carry) a.d.push_back((uint32_t)carry);
+}
+static uint32_t big_mod_small(const Big& a, uint32_t m) {
+  uint64_t r = 0;
+  for (size_t i = a.d.size(); i-- > 0;) r = ((r << 32) | a.d[i]) % m;
+  return (uint32_t)r;
+}
+static Big big_div_small(const Big& a, uint32_t m) {
+  Big q;
+  q.d.assign(a.d.size(), 0);
+  uint64_t r = 0;
+  for (size_t i = a.d.size(); i-- > 0;) {
+    uint64_t cur = (r << 32) | a.d[i];
+    q.d[i] = (uint32_t)(cur / m);
+    r = cur % m;
+  }
+  while (!q.d.empty() && q.d.back() == 0) q.d.pop_back();
+  return q;
+}
+static double big_chunk(const Big& a, int c) {  // bits [39c, 39c+39) as a double
+  uint64_t v = 0;
+  for (int b = 0; b < CRT_BITS; b++) {
+    int bit = c * CRT_BITS + b;
+    size_t w = bit / 32;
+    if (w < a.d.size() && ((a.d[w] >> (bit % 32)) & 1u)) v |= (1ull << b);
+  }
+  return (double)v;
+}
+static int64_t modinv(int64_t a, int64_t m) {
+  int64_t g = m, x = 0, x1 = 1, a1 = a % m;
+  while (a1) {
+    int64_t q = g / a1;
+    int64_t t = g - q * a1;
+    g = a1;
+    a1 = t;
+    t = x - q * x1;
+    x = x1;
+    x1 = t;
+  }
+  return ((x % m) + m) % m;
+}
+
+static const HostTables& host_tables() {
+  static HostTables T;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    // Greedy pairwise-coprime moduli from 256 down.
+    std::vector<int> mods;
+    for (int m = 256; m > 1 && (int)mods.size() < MAXL; m--) {
+      bool ok = true;
+      for (int x : mods)
+        if (std::__gcd(x, m) != 1) ok = false;
+      if (ok) mods.push_back(m);
+    }
+    T.cum_log2[0] = 0;
+    for (int l = 0; l < MAXL; l++) {
+      int m = mods[l];
+      T.mt.mod[l] = m;
+      T.mt.magic[l] = (uint32_t)((1ull << 32) / (uint64_t)m);
+      T.mt.offset[l] = (uint32_t)((((1ull << 31) + m - 1) / m) * m);
+      for (int c = 0; c < NDIG; c++) {
+        // 2^(22c) mod m, balanced
+        uint64_t r = 1;
+        for (int t = 0; t < 22 * c; t++) r = (r * 2) % m;
+        int b = (int)r;
+        if (b > m / 2) b -= m;
+        T.mt.pw[l][c] = b;
+      }
+      T.cum_log2[l + 1] = T.cum_log2[l] + std::log2((double)m);
+    }
+    T.crt.resize(MAXL + 1);
+    for (int L = 1; L <= MAXL; L++) {
+      CrtTable& ct = T.crt[L];
+      std::memset(&ct, 0, sizeof(ct));
+      ct.L = L;
+      Big M;
+      M.d = {1};
+      for (int l = 0; l < L; l++) big_mul_small(M, (uint32_t)mods[l]);
+      int bits = (int)M.d.size() * 32;
+      while (bits > 0 && !((M.d[(bits - 1) / 32] >> ((bits - 1) % 32)) & 1u)) bits--;
+      ct.nc = (bits + CRT_BITS - 1) / CRT_BITS;
+      for (int c = 0; c < ct.nc; c++) ct.mchunk[c] = big_chunk(M, c);
+      {  // 1/M, rounded
+        long double mv = 0;
+        for (size_t i = M.d.size(); i-- > 0;) mv = mv * 4294967296.0L + (long double)M.d[i];
+        ct.inv_m = (double)(1.0L / mv);
+      }
+      for (int l = 0; l < L; l++) {
+        Big P = big_div_small(M, (uint32_t)mods[l]);
+        int64_t pm = big_mod_small(P, (uint32_t)mods[l]);
+        int64_t inv = modinv(pm, mods[l]);
+        Big W = P;
+        big_mul_small(W, (uint32_t)inv);  // < M since inv < m_l
+        for (int c = 0; c < ct.nc; c++) ct.w[l][c] = big_chunk(W, c);
+      }
+    }
+  });
+  return T;
+}
+
+// Per-device upload of the tables (once per device).
+struct DevTables {
+  bool ready = false;
+  CrtTable* crt = nullptr;
+  int num_sms = 0;
+};
+static DevTables g_dev[64];
+static std::mutex g_dev_mu;
+
+static int device_tables(DevTables** out) {
+  int d = 0;
+  HP_CUDA_TRY(cudaGetDevice(&d));
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  DevTables& D = g_dev[d];
+  if (!D.ready) {
+    const HostTables& T = host_tables();
+    HP_CUDA_TRY(cudaMemcpyToSymbol(c_tab, &T.mt, sizeof(ModTable)));
+    HP_CUDA_TRY(cudaMalloc(&D.crt, sizeof(CrtTable) * (MAXL + 1)));
+    HP_CUDA_TRY(cudaMemcpy(D.crt, T.crt.data(), sizeof(CrtTable) * (MAXL + 1), cudaMemcpyHostToDevice));
+    HP_CUDA_TRY(cudaDeviceGetAttribute(&D.num_sms, cudaDevAttrMultiProcessorCount, d));
+    D.ready = true;
+  }
+  *out = &D;
+  return HP_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Device helpers
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int exp_field(double x) {
+  return (int)((__double_as_longlong(x) >> 52) & 0x7FF);
+}
+// x * 2^s for any s in [-2100, 2100], exact when the result is a normal
+// number (the scaled integers of this file always are, or are discarded).
+__device__ __forceinline__ double scale_pow2(double x, int s) {
+  while (s > 1000) {
+    x = __dmul_rn(x, 0x1p1000);
+    s -= 1000;
+  }
+  while (s < -1000) {
+    x = __dmul_rn(x, 0x1p-1000);
+    s += 1000;
+  }
+  return __dmul_rn(x, __longlong_as_double((long long)(s + 1023) << 52));
+}
+__device__ __forceinline__ uint32_t mod_reduce(int32_t x, int l) {
+  uint32_t u = (uint32_t)(x + (int32_t)0) + c_tab.offset[l];  // x + offset, as unsigned
+  uint32_t m = (uint32_t)c_tab.mod[l];
+  uint32_t q = __umulhi(u, c_tab.magic[l]);
+  uint32_t r = u - q * m;
+  return r >= m ? r - m : r;
+}
+
+// Max exponent field over each row of a row-major R x C f128 matrix (one
+// warp per row). out[r] = max over the row of max(e(hi), e(lo) + 1).
+__global__ void maxexp_rows_kernel(const double2* __restrict__ src, int64_t R, int64_t C, int* __restrict__ out) {
+  int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  int lane = threadIdx.x % 32;
+  if (row >= R) return;
+  int e = 0;
+  for (int64_t p = lane; p < C; p += 32) {
+    double2 v = src[row * C + p];
+    e = max(e, max(exp_field(v.x), min(exp_field(v.y) + 1, EXP_NONFINITE)));
+    if (exp_field(v.y) == EXP_NONFINITE) e = EXP_NONFINITE;
+  }
+  for (int o = 16; o; o >>= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, o));
+  if (lane == 0) out[row] = e;
+}
+// Max exponent field over each column of a row-major R x C f128 matrix.
+// Block: 32 columns x 8 row-lanes, each block covers a slab of rows.
+__global__ void maxexp_cols_kernel(const double2* __restrict__ src, int64_t R, int64_t C, int64_t slab,
+                                   int* __restrict__ out) {
+  __shared__ int red[8][33];
+  int64_t c = (int64_t)blockIdx.x * 32 + threadIdx.x;
+  int64_t r0 = (int64_t)blockIdx.y * slab, r1 = min(R, r0 + slab);
+  int e = 0;
+  if (c < C) {
+    for (int64_t r = r0 + threadIdx.y; r < r1; r += 8) {
+      double2 v = src[r * C + c];
+      e = max(e, max(exp_field(v.x), min(exp_field(v.y) + 1, EXP_NONFINITE)));
+      if (exp_field(v.y) == EXP_NONFINITE) e = EXP_NONFINITE;
+    }
+  }
+  red[threadIdx.y][threadIdx.x] = e;
+  __syncthreads();
+  if (threadIdx.y == 0 && c < C) {
+    for (int y = 1; y < 8; y++) e = max(e, red[y][threadIdx.x]);
+    atomicMax(out + c, e);
+  }
+}
+
+// Balanced base-2^22 digits of rint(v) for |v| < 2^108 (exact).
+__device__ __forceinline__ void int_digits(double v, int32_t* d) {
+  double a = fabs(rint(v));
+  double t4 = floor(__dmul_rn(a, 0x1p-88));
+  double r = __dsub_rn(a, __dmul_rn(t4, 0x1p88));
+  double t3 = floor(__dmul_rn(r, 0x1p-66));
+  r = __dsub_rn(r, __dmul_rn(t3, 0x1p66));
+  double t2 = floor(__dmul_rn(r, 0x1p-44));
+  r = __dsub_rn(r, __dmul_rn(t2, 0x1p44));
+  double t1 = floor(__dmul_rn(r, 0x1p-22));
+  r = __dsub_rn(r, __dmul_rn(t1, 0x1p22));
+  int32_t s = signbit(v) ? -1 : 1;
+  d[0] = s * (int32_t)r;
+  d[1] = s * (int32_t)t1;
+  d[2] = s * (int32_t)t2;
+  d[3] = s * (int32_t)t3;
+  d[4] = s * (int32_t)t4;
+}
+
+// Residues of the scaled operand. Logical operand is R x K (row r, reduction
+// index p); element (r, p) is src[r*K + p] (P_CONTIG) or src[p*R + r].
+// Writes out[l][r][p] (int8), row stride Kp, plane stride Rp*Kp, for all
+// r < Rp, p < Kp (zero outside R x K). Tile: 64 rows x 32 p per block.
+constexpr int RT_R = 64, RT_P = 32, RT_STRIDE = 40;
+template <bool P_CONTIG>
+__global__ void __launch_bounds__(256) residue_kernel(const double2* __restrict__ src, int64_t R, int64_t K,
+                                                      const int* __restrict__ expf, int beta, int L, int64_t Rp,
+                                                      int64_t Kp, int8_t* __restrict__ out) {
+  __shared__ __align__(16) uint8_t T[2][RT_R * RT_STRIDE];
+  const int t = threadIdx.x;
+  const int64_t r0 = (int64_t)blockIdx.y * RT_R, p0 = (int64_t)blockIdx.x * RT_P;
+  int32_t dig[8][NDIG];
+  int rl[8], pl[8];
+#pragma unroll
+  for (int q = 0; q < 8; q++) {
+    if (P_CONTIG) {
+      rl[q] = t / 32 + 8 * q;
+      pl[q] = t % 32;
+    } else {
+      rl[q] = t % 64;
+      pl[q] = t / 64 + 4 * q;
+    }
+    int64_t r = r0 + rl[q], p = p0 + pl[q];
+#pragma unroll
+    for (int c = 0; c < NDIG; c++) dig[q][c] = 0;
+    if (r < R && p < K) {
+      int e = expf[r];
+      if (e != EXP_NONFINITE) {
+        double2 v = P_CONTIG ? src[r * K + p] : src[p * R + r];
+        int s = beta + 1022 - e;
+        int32_t dh[NDIG], dl[NDIG];
+        int_digits(scale_pow2(v.x, s), dh);
+        int_digits(scale_pow2(v.y, s), dl);
+        int32_t D[NDIG];
+#pragma unroll
+        for (int c = 0; c < NDIG; c++) D[c] = dh[c] + dl[c];
+#pragma unroll
+        for (int c = 0; c < NDIG - 1; c++) {
+          int32_t carry = (D[c] + (1 << 21)) >> 22;
+          D[c] -= carry << 22;
+          D[c + 1] += carry;
+        }
+#pragma unroll
+        for (int c = 0; c < NDIG; c++) dig[q][c] = D[c];
+      }
+    }
+  }
+  for (int l = 0; l < L; l++) {
+    uint8_t* Tb = T[l & 1];
+    const int m = c_tab.mod[l];
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      int32_t x = 0;
+#pragma unroll
+      for (int c = 0; c < NDIG; c++) x += dig[q][c] * c_tab.pw[l][c];
+      int r = (int)mod_reduce(x, l);
+      if (r > 127) r -= m;
+      Tb[rl[q] * RT_STRIDE + pl[q]] = (uint8_t)(int8_t)r;
+    }
+    __syncthreads();
+    {
+      int row = t / 4, part = t % 4;
+      uint2 v = *reinterpret_cast<const uint2*>(Tb + row * RT_STRIDE + part * 8);
+      *reinterpret_cast<uint2*>(out + (size_t)l * Rp * Kp + (size_t)(r0 + row) * Kp + p0 + part * 8) = v;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// tcgen05 int8 GEMM, one modulus per output tile:
+//   cres[l][i][j] = (sum_p Ares[l][i][p] * Bres[l][j][p]) mod m_l   (uint8)
+// Persistent, warp-specialised: warp 0 = TMA producer, warp 1 = MMA issuer,
+// warp 2 = TMEM owner, warps 4-7 = epilogue (TMEM -> residue bytes).
+// Tile 128 x 256, K-block 128 bytes, 4-stage smem ring, 2 TMEM accumulators.
+// ---------------------------------------------------------------------------
+constexpr int GB_M = 128, GB_N = 256, GB_K = 128, GSTAGES = 4;
+constexpr int A_STAGE = GB_M * GB_K, B_STAGE = GB_N * GB_K, STAGE_BYTES = A_STAGE + B_STAGE;
+constexpr int GEMM_SMEM = GSTAGES * STAGE_BYTES + 1024 + 256;
+constexpr int MAX_K_CHUNK = 65536;  // |int32 accumulator| <= 2^16 * 2^14 = 2^30
+
+__global__ void __launch_bounds__(256, 1)
+    i8_gemm_mod_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int L,
+                       int tiles_m, int tiles_n, int kb0, int kb1, int accumulate, uint8_t* __restrict__ cres,
+                       int64_t Np, int64_t plane, uint32_t* status) {
+  using namespace sm100;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
+  uint8_t* smem = smem_raw + pad;
+  uint8_t* sA = smem;
+  uint8_t* sB = smem + GSTAGES * A_STAGE;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + GSTAGES * STAGE_BYTES);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + GSTAGES;
+  uint64_t* tfull = bars + 2 * GSTAGES;
+  uint64_t* tempty = tfull + 2;
+  uint64_t* drain = tempty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < GSTAGES; s++) {
+      mbar_init(&full[s], 1);
+      mbar_init(&empty[s], 1);
+    }
+    for (int a = 0; a < 2; a++) {
+      mbar_init(&tfull[a], 1);
+      mbar_init(&tempty[a], 128);
+    }
+    mbar_init(drain, 1);
+    fence_mbarrier_init();
+  }
+  if (warp == 0 && lane == 0) {
+    prefetch_tmap(&mapA);
+    prefetch_tmap(&mapB);
+  }
+  if (warp == 2) {
+    tmem_alloc(tmem_slot, 512);
+    tmem_relinquish();
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+
+  const int nkb = kb1 - kb0;
+  const int per_l = tiles_m * tiles_n;
+  const int num_tiles = L * per_l;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      uint32_t stage = 0, phase = 0;
+      bool ok = true;
+      int filled_phase[GSTAGES];
+      for (int s = 0; s < GSTAGES; s++) filled_phase[s] = -1;
+      for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
+        const int l = t / per_l, rem = t % per_l, tm = rem / tiles_n, tn = rem % tiles_n;
+        for (int kb = 0; kb < nkb; kb++) {
+          if (!mbar_wait(&empty[stage], phase ^ 1, status, DEV_STATUS_TIMEOUT)) {
+            ok = false;
+            break;
+          }
+          mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
+          tma_load_3d(sA + stage * A_STAGE, &mapA, &full[stage], (kb0 + kb) * GB_K, tm * GB_M, l);
+          tma_load_3d(sB + stage * B_STAGE, &mapB, &full[stage], (kb0 + kb) * GB_K, tn * GB_N, l);
+          filled_phase[stage] = (int)phase;
+          if (++stage == GSTAGES) {
+            stage = 0;
+            phase ^= 1;
+          }
+        }
+      }
+      if (!ok) {  // let loads still in flight land before the CTA exits
+        for (int s = 0; s < GSTAGES; s++)
+          if (filled_phase[s] >= 0) mbar_wait(&full[s], (uint32_t)filled_phase[s], status, DEV_STATUS_TIMEOUT, 100000000ull);
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      uint32_t stage = 0, phase = 0, it = 0;
+      bool ok = true;
+      bool issued = false;
+      const uint32_t idesc = idesc_i8(GB_M, GB_N);
+      for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x, it++) {
+        const uint32_t acc = it & 1, aph = (it >> 1) & 1;
+        if (!mbar_wait(&tempty[acc], aph ^ 1, status, DEV_STATUS_TIMEOUT)) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem_base + acc * GB_N;
+        for (int kb = 0; kb < nkb; kb++) {
+          if (!mbar_wait(&full[stage], phase, status, DEV_STATUS_TIMEOUT)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(sA + stage * A_STAGE), b0 = smem_u32(sB + stage * B_STAGE);
+#pragma unroll
+          for (int kk = 0; kk < GB_K / 32; kk++)
+            mma_i8(d, desc_k_sw128(a0 + kk * 32), desc_k_sw128(b0 + kk * 32), idesc, (kb | kk) ? 1u : 0u);
+          issued = true;
+          mma_commit(&empty[stage]);
+          if (++stage == GSTAGES) {
+            stage = 0;
+            phase ^= 1;
+          }
+        }
+        if (!ok) break;
+        mma_commit(&tfull[acc]);
+      }
+      if (!ok && issued) {  // wait for issued MMAs before TMEM is released
+        mma_commit(drain);
+        mbar_wait(drain, 0, status, DEV_STATUS_TIMEOUT, 100000000ull);
+      }
+    }
+  } else if (warp >= 4) {
+    const int ew = warp - 4;
+    uint32_t it = 0;
+    for (int t = blockIdx.x; t < num_tiles; t += gridDim.x, it++) {
+      const int l = t / per_l, rem = t % per_l, tm = rem / tiles_n, tn = rem % tiles_n;
+      const uint32_t acc = it & 1, aph = (it >> 1) & 1;
+      bool ok = mbar_wait(&tfull[acc], aph, status, DEV_STATUS_TIMEOUT);
+      if (!__all_sync(0xffffffffu, ok)) break;
+      tc_fence_after();
+      const uint32_t m = (uint32_t)c_tab.mod[l];
+      const int64_t row = (int64_t)tm * GB_M + ew * 32 + lane;
+      uint8_t* dst = cres + (size_t)l * plane + (size_t)row * Np + (size_t)tn * GB_N;
+#pragma unroll 1
+      for (int ch = 0; ch < GB_N / 32; ch++) {
+        uint32_t v[32];
+        tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(ew * 32) << 16) + acc * GB_N + ch * 32, v);
+        tmem_wait_ld();
+        uint32_t packed[8];
+        uint4 prev0 = make_uint4(0, 0, 0, 0), prev1 = make_uint4(0, 0, 0, 0);
+        if (accumulate) {
+          prev0 = *reinterpret_cast<const uint4*>(dst + ch * 32);
+          prev1 = *reinterpret_cast<const uint4*>(dst + ch * 32 + 16);
+        }
+        const uint32_t pv[8] = {prev0.x, prev0.y, prev0.z, prev0.w, prev1.x, prev1.y, prev1.z, prev1.w};
+#pragma unroll
+        for (int w = 0; w < 8; w++) {
+          uint32_t word = 0;
+#pragma unroll
+          for (int b = 0; b < 4; b++) {
+            uint32_t r = mod_reduce((int32_t)v[4 * w + b], l);
+            if (accumulate) {
+              r += (pv[w] >> (8 * b)) & 0xFFu;
+              if (r >= m) r -= m;
+            }
+            word |= r << (8 * b);
+          }
+          packed[w] = word;
+        }
+        *reinterpret_cast<uint4*>(dst + ch * 32) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+        *reinterpret_cast<uint4*>(dst + ch * 32 + 16) = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+      }
+      tc_fence_before();
+      mbar_arrive(&tempty[acc]);
+    }
+  }
+  __syncthreads();
+  if (warp == 2) {
+    tc_fence_after();
+    tmem_dealloc(tmem_base, 512);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// CRT reconstruction: residues -> exact integer -> f128, scaled back.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) crt_dd_kernel(const uint8_t* __restrict__ cres, int64_t plane, int64_t Np,
+                                                     int64_t m, int64_t n, const int* __restrict__ expA,
+                                                     const int* __restrict__ expB, int beta,
+                                                     const CrtTable* __restrict__ tab, double2* __restrict__ C) {
+  __shared__ double w_s[MAXL][NCMAX];
+  __shared__ double mch_s[NCMAX];
+  const int L = tab->L, nc = tab->nc;
+  for (int i = threadIdx.x; i < L * NCMAX; i += blockDim.x) w_s[i / NCMAX][i % NCMAX] = tab->w[i / NCMAX][i % NCMAX];
+  if (threadIdx.x < NCMAX) mch_s[threadIdx.x] = tab->mchunk[threadIdx.x];
+  __syncthreads();
+  const double inv_m = tab->inv_m;
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= m * n) return;
+  const int64_t i = idx / n, j = idx % n;
+  const int ea = expA[i], eb = expB[j];
+  if (ea == EXP_NONFINITE || eb == EXP_NONFINITE) {
+    C[idx] = make_double2(__longlong_as_double(0x7ff8000000000000ll), 0.0);
+    return;
+  }
+  double acc[NCMAX + 1];
+#pragma unroll
+  for (int c = 0; c <= NCMAX; c++) acc[c] = 0.0;
+  const uint8_t* rp = cres + (size_t)i * Np + j;
+  for (int l = 0; l < L; l++) {
+    const double r = (double)rp[(size_t)l * plane];
+#pragma unroll
+    for (int c = 0; c < NCMAX; c++)
+      if (c < nc) acc[c] = __fma_rn(r, w_s[l][c], acc[c]);
+  }
+  // carry-normalise into [0, 2^39) chunks; acc[nc] takes the carry out
+#pragma unroll
+  for (int c = 0; c < NCMAX; c++)
+    if (c < nc) {
+      double carry = floor(__dmul_rn(acc[c], 0x1p-39));
+      acc[c] = __dsub_rn(acc[c], __dmul_rn(carry, 0x1p39));
+      acc[c + 1] = __dadd_rn(acc[c + 1], carry);
+    }
+  // q = round(X / M): the true value is X - qM with |X - qM| <= M/4
+  double xa = 0.0;
+#pragma unroll
+  for (int c = NCMAX; c >= 0; c--)
+    if (c <= nc && c >= nc - 2) xa = __fma_rn(acc[c], scale_pow2(1.0, CRT_BITS * c), xa);
+  const double q = rint(__dmul_rn(xa, inv_m));
+#pragma unroll
+  for (int c = 0; c < NCMAX; c++)
+    if (c < nc) acc[c] = __fma_rn(-q, mch_s[c], acc[c]);
+#pragma unroll
+  for (int c = 0; c < NCMAX; c++)
+    if (c < nc) {
+      double carry = floor(__dmul_rn(acc[c], 0x1p-39));
+      acc[c] = __dsub_rn(acc[c], __dmul_rn(carry, 0x1p39));
+      acc[c + 1] = __dadd_rn(acc[c + 1], carry);
+    }
+  bool neg = false;
+  double top = 0.0;
+#pragma unroll
+  for (int c = 0; c <= NCMAX; c++)
+    if (c == nc) top = acc[c];
+  if (top < 0.0) {  // negate: chunks become -acc, renormalise (top -> 0)
+    neg = true;
+#pragma unroll
+    for (int c = 0; c <= NCMAX; c++) acc[c] = -acc[c];
+#pragma unroll
+    for (int c = 0; c < NCMAX; c++)
+      if (c < nc) {
+        double carry = floor(__dmul_rn(acc[c], 0x1p-39));
+        acc[c] = __dsub_rn(acc[c], __dmul_rn(carry, 0x1p39));
+        acc[c + 1] = __dadd_rn(acc[c + 1], carry);
+      }
+  }
+  // sum the non-negative, non-overlapping chunks from the top into f128
+  dd s = dd{0.0, 0.0};
+#pragma unroll
+  for (int c = NCMAX - 1; c >= 0; c--)
+    if (c < nc) {
+      double v = scale_pow2(acc[c], CRT_BITS * c);
+      double hs, he;
+      two_sum(s.hi, v, hs, he);
+      s = dd_renorm(hs, __dadd_rn(he, s.lo));
+    }
+  const int shift = -((beta + 1022 - ea) + (beta + 1022 - eb));
+  double hi = scale_pow2(s.hi, shift), lo = scale_pow2(s.lo, shift);
+  dd o = dd_renorm(hi, lo);
+  if (neg) o = dd_neg(o);
+  C[idx] = make_double2(o.hi, o.lo);
+}
+
+// ---------------------------------------------------------------------------
+// Host driver
+// ---------------------------------------------------------------------------
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    cudaDriverEntryPointQueryResult q;
+    void* p = nullptr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (PFN_cuTensorMapEncodeTiled_v12000)p;
+  });
+  return fn;
+}
+
+static int make_map(CUtensorMap* map, const void* base, uint64_t K, uint64_t R, uint64_t L, uint32_t box_r) {
+  auto fn = encode_fn();
+  if (!fn) {
+    set_error("cuTensorMapEncodeTiled unavailable");
+    return HP_ERR_CUDA;
+  }
+  cuuint64_t dims[3] = {K, R, L};
+  cuuint64_t strides[2] = {K, K * R};
+  cuuint32_t box[3] = {(cuuint32_t)GB_K, box_r, 1};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult rc = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (rc != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (%d)", (int)rc);
+    return HP_ERR_CUDA;
+  }
+  return HP_OK;
+}
+
+static inline size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+static inline int ceil_log2(size_t x) {
+  int b = 0;
+  while (((size_t)1 << b) < x) b++;
+  return b;
+}
+
+}  // namespace ozaki
+
+int ozaki_moduli_for(size_t k, int beta) {
+  const ozaki::HostTables& T = ozaki::host_tables();
+  double need = 2.0 * beta + ozaki::ceil_log2(k) + 2.0;
+  for (int L = 1; L <= ozaki::MAXL; L++)
+    if (T.cum_log2[L] >= need) return L;
+  return -1;
+}
+
+// Residue GEMM core shared by the f128 and f256 drivers: given int8 residue
+// planes of op(A) (L x Mp x Kp) and B (L x Np x Kp), writes cres (L x Mp x Np).
+int ozaki_residue_gemm(const int8_t* ares, const int8_t* bres, uint8_t* cres, int L, size_t Mp, size_t Np,
+                       size_t Kp, cudaStream_t s) {
+  using namespace ozaki;
+  DevTables* D;
+  HP_TRY(device_tables(&D));
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev]) {
+    HP_CUDA_TRY(cudaFuncSetAttribute(i8_gemm_mod_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM));
+    attr_set[dev] = true;
+  }
+  CUtensorMap mapA, mapB;
+  HP_TRY(make_map(&mapA, ares, Kp, Mp, L, GB_M));
+  HP_TRY(make_map(&mapB, bres, Kp, Np, L, GB_N));
+  uint32_t* status = device_status(s);
+  if (!status) {
+    set_error("status word allocation failed");
+    return HP_ERR_CUDA;
+  }
+  const int tiles_m = (int)(Mp / GB_M), tiles_n = (int)(Np / GB_N);
+  const int num_tiles = L * tiles_m * tiles_n;
+  const int grid = std::min(num_tiles, D->num_sms);
+  const int nkb_total = (int)(Kp / GB_K);
+  const int kb_chunk = MAX_K_CHUNK / GB_K;
+  for (int kb0 = 0; kb0 < nkb_total; kb0 += kb_chunk) {
+    int kb1 = std::min(nkb_total, kb0 + kb_chunk);
+    i8_gemm_mod_kernel<<<grid, 256, GEMM_SMEM, s>>>(mapA, mapB, L, tiles_m, tiles_n, kb0, kb1, kb0 > 0 ? 1 : 0,
+                                                     cres, (int64_t)Np, (int64_t)(Mp * Np), status);
+    HP_LAUNCH_CHECK();
+  }
+  return HP_OK;
+}
+
+int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t n, size_t k, bool atb,
+                  cudaStream_t s) {
+  using namespace ozaki;
+  if (m == 0 || n == 0) return HP_OK;
+  if (k == 0) {
+    HP_CUDA_TRY(cudaMemsetAsync(c, 0, m * n * 16, s));
+    return HP_OK;
+  }
+  DevTables* D;
+  HP_TRY(device_tables(&D));
+  const int beta = BETA_DD;
+  const int L = ozaki_moduli_for(k, beta);
+  if (L < 0) {
+    set_error("ozaki: k = %zu needs more moduli than the table holds", k);
+    return HP_ERR_UNSUPPORTED;
+  }
+  const size_t Mp = round_up(m, GB_M), Np = round_up(n, GB_N), Kp = round_up(k, GB_K);
+  if (Mp / GB_M * (Np / GB_N) * (size_t)L > (size_t)INT32_MAX || Kp > (size_t)INT32_MAX) {
+    set_error("ozaki: problem too large");
+    return HP_ERR_INVALID_ARG;
+  }
+  DevBuf expA(Mp * sizeof(int), s), expB(Np * sizeof(int), s);
+  DevBuf ares((size_t)L * Mp * Kp, s), bres((size_t)L * Np * Kp, s), cres((size_t)L * Mp * Np, s);
+  if (!expA.p || !expB.p || !ares.p || !bres.p || !cres.p) {
+    set_error("ozaki: workspace allocation failed");
+    return HP_ERR_CUDA;
+  }
+  HP_CUDA_TRY(cudaMemsetAsync(expA.p, 0, Mp * sizeof(int), s));
+  HP_CUDA_TRY(cudaMemsetAsync(expB.p, 0, Np * sizeof(int), s));
+  profile_mark(s, "start");
+  const double2* A2 = reinterpret_cast<const double2*>(a);
+  const double2* B2 = reinterpret_cast<const double2*>(b);
+  // 1. exponents
+  if (!atb) {
+    maxexp_rows_kernel<<<(unsigned)((m + 7) / 8), 256, 0, s>>>(A2, m, k, expA.as<int>());
+  } else {
+    int64_t slab = 256;
+    dim3 g((unsigned)((m + 31) / 32), (unsigned)((k + slab - 1) / slab));
+    maxexp_cols_kernel<<<g, dim3(32, 8), 0, s>>>(A2, k, m, slab, expA.as<int>());
+  }
+  HP_LAUNCH_CHECK();
+  {
+    int64_t slab = 256;
+    dim3 g((unsigned)((n + 31) / 32), (unsigned)((k + slab - 1) / slab));
+    maxexp_cols_kernel<<<g, dim3(32, 8), 0, s>>>(B2, k, n, slab, expB.as<int>());
+    HP_LAUNCH_CHECK();
+  }
+  profile_mark(s, "exponents");
+  // 2. residues
+  {
+    dim3 ga((unsigned)(Kp / RT_P), (unsigned)(Mp / RT_R));
+    if (!atb)
+      residue_kernel<true><<<ga, 256, 0, s>>>(A2, m, k, expA.as<int>(), beta, L, Mp, Kp, ares.as<int8_t>());
+    else
+      residue_kernel<false><<<ga, 256, 0, s>>>(A2, m, k, expA.as<int>(), beta, L, Mp, Kp, ares.as<int8_t>());
+    HP_LAUNCH_CHECK();
+    dim3 gb((unsigned)(Kp / RT_P), (unsigned)(Np / RT_R));
+    residue_kernel<false><<<gb, 256, 0, s>>>(B2, n, k, expB.as<int>(), beta, L, Np, Kp, bres.as<int8_t>());
+    HP_LAUNCH_CHECK();
+  }
+  profile_mark(s, "residues");
+  // 3. one int8 GEMM per modulus
+  HP_TRY(ozaki_residue_gemm(ares.as<int8_t>(), bres.as<int8_t>(), cres.as<uint8_t>(), L, Mp, Np, Kp, s));
+  profile_mark(s, "i8_gemm");
+  // 4. CRT
+  {
+    int64_t total = (int64_t)(m * n);
+    crt_dd_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(cres.as<uint8_t>(), (int64_t)(Mp * Np),
+                                                                  (int64_t)Np, m, n, expA.as<int>(),
+                                                                  expB.as<int>(), beta, D->crt + L,
+                                                                  reinterpret_cast<double2*>(c));
+    HP_LAUNCH_CHECK();
+  }
+  profile_mark(s, "crt");
+  return HP_OK;
+}
+
+int ozaki_qd_gemm(const double*, const double*, double*, size_t, size_t, size_t, bool, cudaStream_t) {
+  set_error("f256 Ozaki GEMM is not built yet");
+  return HP_ERR_UNSUPPORTED;
+}
+
+}  // namespace hp

@@ -1,0 +1,81 @@
+"""Deterministic synthetic inputs for the benchmark configurations.
+
+RNG: SplitMix64 (seed 0 unless stated); U[0,1) = (x >> 11) * 2^-53.
+All generators are vectorised numpy and reproduce bit-for-bit on any host.
+
+Configurations (sizes as benchmarked):
+  * dense_dd(m, k, seed, offset): full double-double entries,
+    hi ~ U[-1,1), lo = hi * 2^-53 * U[-1,1), renormalised with
+    quick_two_sum (crates/quad/src/dd.rs:86-89). Used for the f128 GEMM at
+    m = n = k = 2048 and, limb-extended, for f256 GEMM at 1024.
+  * shifted_hilbert(n): A_ij = 1/(i+j+1) (f64), A_ii += 1, b = ones
+    (the README / linalg.rs:548-557 construction), n = 512.
+  * overlap_lattice(...): s-Gaussian basis on a jittered cubic lattice.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+_GOLDEN = np.uint64(0x9E3779B97F4A7C15)
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+
+
+def splitmix64(count: int, seed: int = 0, offset: int = 0) -> np.ndarray:
+    """The outputs number offset+1 .. offset+count of SplitMix64(seed)."""
+    with np.errstate(over="ignore"):
+        idx = np.arange(offset + 1, offset + count + 1, dtype=np.uint64)
+        z = np.uint64(seed) + idx * _GOLDEN
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+        return z ^ (z >> np.uint64(31))
+
+
+def uniform(count: int, seed: int = 0, offset: int = 0) -> np.ndarray:
+    return (splitmix64(count, seed, offset) >> np.uint64(11)).astype(np.float64) * 2.0 ** -53
+
+
+def quick_two_sum(a: np.ndarray, b: np.ndarray):
+    s = a + b
+    return s, b - (s - a)
+
+
+def dense_dd(rows: int, cols: int, seed: int = 0, offset: int = 0) -> np.ndarray:
+    """rows x cols f128 matrix (shape (rows, cols, 2)); consumes 2 draws/entry."""
+    u = uniform(2 * rows * cols, seed, offset).reshape(rows * cols, 2)
+    hi = 2.0 * u[:, 0] - 1.0
+    lo = hi * 2.0 ** -53 * (2.0 * u[:, 1] - 1.0)
+    s, e = quick_two_sum(hi, lo)
+    return np.stack([s, e], axis=-1).reshape(rows, cols, 2)
+
+
+def gemm_operands(m: int, n: int, k: int, seed: int = 0, atb: bool = False):
+    """A (m x k, or k x m if atb) then B (k x n), one SplitMix64 stream."""
+    a = dense_dd(k, m, seed, 0) if atb else dense_dd(m, k, seed, 0)
+    b = dense_dd(k, n, seed, 2 * m * k)
+    return a, b
+
+
+def dd_to_qd(x: np.ndarray) -> np.ndarray:
+    """Limb-extend f128 entries to f256 (MultiFloat<4>::from_f128, conv.rs:121-126)."""
+    out = np.zeros(x.shape[:-1] + (4,))
+    out[..., :2] = x
+    return out
+
+
+def shifted_hilbert(n: int):
+    """f128 matrix 1/(i+j+1) (from f64) + I, and b = ones (README construction)."""
+    i = np.arange(n, dtype=np.float64)
+    h = 1.0 / (i[:, None] + i[None, :] + 1.0)
+    a = np.zeros((n, n, 2))
+    a[..., 0] = h
+    # f128::from_f64(h_ii) + f128::from_f64(1.0): exact two_sum of two doubles
+    d = np.diag(h).copy()
+    s = d + 1.0
+    v = s - d
+    e = (d - (s - v)) + (1.0 - v)
+    a[np.arange(n), np.arange(n), 0] = s
+    a[np.arange(n), np.arange(n), 1] = e
+    b = np.zeros((n, 2))
+    b[:, 0] = 1.0
+    return a, b

@@ -1,0 +1,81 @@
+// Host build of quadprec_b200/csrc/hp_arith.cuh for the CPU test suite.
+// The device intrinsics are replaced by their IEEE host equivalents (each is
+// one correctly rounded operation), so the header's operation sequences can
+// be compared bit-for-bit against the oracle without a GPU.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <math.h>
+
+#define __device__
+#define __forceinline__ inline
+static inline double __dadd_rn(double a, double b) { return a + b; }
+static inline double __dsub_rn(double a, double b) { return a - b; }
+static inline double __dmul_rn(double a, double b) { return a * b; }
+static inline double __ddiv_rn(double a, double b) { return a / b; }
+static inline double __fma_rn(double a, double b, double c) { return std::fma(a, b, c); }
+static inline double __dsqrt_rn(double a) { return std::sqrt(a); }
+static inline double __longlong_as_double(long long v) {
+  double d;
+  std::memcpy(&d, &v, 8);
+  return d;
+}
+using std::fabs;
+using std::isfinite;
+using std::round;
+using std::signbit;
+
+#include "../quadprec_b200/csrc/hp_arith.cuh"
+
+using namespace hp;
+extern "C" {
+void sh_dd_add(const double* a, const double* b, double* o) {
+  dd r = dd_add(dd{a[0], a[1]}, dd{b[0], b[1]});
+  o[0] = r.hi, o[1] = r.lo;
+}
+void sh_dd_mul(const double* a, const double* b, double* o) {
+  dd r = dd_mul(dd{a[0], a[1]}, dd{b[0], b[1]});
+  o[0] = r.hi, o[1] = r.lo;
+}
+void sh_dd_div(const double* a, const double* b, double* o) {
+  dd r = dd_div(dd{a[0], a[1]}, dd{b[0], b[1]});
+  o[0] = r.hi, o[1] = r.lo;
+}
+void sh_dd_sqrt(const double* a, double* o) {
+  dd r = dd_sqrt(dd{a[0], a[1]});
+  o[0] = r.hi, o[1] = r.lo;
+}
+void sh_dd_recip(const double* a, double* o) {
+  dd r = dd_recip(dd{a[0], a[1]});
+  o[0] = r.hi, o[1] = r.lo;
+}
+void sh_dd_exp(const double* a, double* o) {
+  dd r = dd_exp(dd{a[0], a[1]});
+  o[0] = r.hi, o[1] = r.lo;
+}
+static qd ldq(const double* p) { return qd{{p[0], p[1], p[2], p[3]}}; }
+static void stq(double* p, const qd& v) {
+  for (int i = 0; i < 4; i++) p[i] = v.l[i];
+}
+void sh_qd_add(const double* a, const double* b, double* o) { stq(o, qd_add(ldq(a), ldq(b))); }
+void sh_qd_mul(const double* a, const double* b, double* o) { stq(o, qd_mul(ldq(a), ldq(b))); }
+void sh_qd_div(const double* a, const double* b, double* o) { stq(o, qd_div(ldq(a), ldq(b))); }
+void sh_qd_sqrt(const double* a, double* o) { stq(o, qd_sqrt(ldq(a))); }
+// Many ops at once (count entries of 2 or 4 limbs each).
+void sh_batch(int op, const double* a, const double* b, double* o, long count) {
+  for (long i = 0; i < count; i++) {
+    switch (op) {
+      case 0: sh_dd_add(a + 2 * i, b + 2 * i, o + 2 * i); break;
+      case 1: sh_dd_mul(a + 2 * i, b + 2 * i, o + 2 * i); break;
+      case 2: sh_dd_div(a + 2 * i, b + 2 * i, o + 2 * i); break;
+      case 3: sh_dd_sqrt(a + 2 * i, o + 2 * i); break;
+      case 4: sh_dd_recip(a + 2 * i, o + 2 * i); break;
+      case 5: sh_dd_exp(a + 2 * i, o + 2 * i); break;
+      case 10: sh_qd_add(a + 4 * i, b + 4 * i, o + 4 * i); break;
+      case 11: sh_qd_mul(a + 4 * i, b + 4 * i, o + 4 * i); break;
+      case 12: sh_qd_div(a + 4 * i, b + 4 * i, o + 4 * i); break;
+      case 13: sh_qd_sqrt(a + 4 * i, o + 4 * i); break;
+    }
+  }
+}
+}

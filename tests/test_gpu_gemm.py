@@ -1,0 +1,125 @@
+"""GPU parity for the GEMM entry points (through the C ABI).
+
+HP_MODE_PLAIN must be bit-identical to the oracle (the reference's gemm /
+mf_gemm). HP_MODE_OZAKI must satisfy the normwise tolerance
+||C - C_ref||_F / || |A| |B| ||_F <= 4 k 2^-104 (f128) stated for this path.
+Sizes cover ragged edges of every tile shape (1, 2, 3, 17, 63, 65, 127, 129,
+255, 257) plus zeros, cancellation and wide exponent ranges.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from quadprec_b200.workloads import dense_dd, dd_to_qd, gemm_operands
+
+pytestmark = pytest.mark.gpu
+
+
+def normwise_err(c, cref, a_abs_b_abs):
+    d = (c[..., 0] - cref[..., 0]) + (c[..., 1] - cref[..., 1])
+    return np.linalg.norm(d) / max(np.linalg.norm(a_abs_b_abs), 1e-300)
+
+
+def abs_prod(a, b, atb):
+    A = np.abs(a[..., 0] + a[..., 1])
+    B = np.abs(b[..., 0] + b[..., 1])
+    return (A.T if atb else A) @ B
+
+
+SHAPES = [(1, 1, 1), (2, 2, 2), (3, 5, 7), (17, 63, 65), (65, 17, 129), (127, 129, 63), (130, 257, 255),
+          (64, 64, 16), (257, 65, 300)]
+
+
+@pytest.mark.parametrize("atb", [False, True])
+@pytest.mark.parametrize("m,n,k", SHAPES)
+def test_f128_plain_bitexact(gpu, m, n, k, atb):
+    a, b = gemm_operands(m, n, k, seed=m * 1000 + n * 10 + k, atb=atb)
+    c = gpu.f128_gemm(a, b, m, n, k, gpu.PLAIN, atb)
+    ref = O.gemm(a, b, m, n, k, atb=atb)
+    assert np.array_equal(c, ref)
+
+
+def test_f128_plain_reference_kats(gpu):
+    f = lambda v: np.stack([np.asarray(v, float), np.zeros(len(v))], -1)
+    c = gpu.f128_gemm(f([1, 2, 3, 4]).reshape(2, 2, 2), f([5, 6, 7, 8]).reshape(2, 2, 2), 2, 2, 2)
+    assert np.array_equal(c[..., 0].ravel(), [19, 22, 43, 50])  # linalg.rs:437-447
+    a = f([1, 2, 3, 4, 5, 6]).reshape(3, 2, 2)
+    b = f(range(1, 13)).reshape(3, 4, 2)
+    at = f([1, 3, 5, 2, 4, 6]).reshape(2, 3, 2)
+    assert np.array_equal(gpu.f128_gemm(at, b, 2, 4, 3), gpu.f128_gemm(a, b, 2, 4, 3, atb=True))
+
+
+@pytest.mark.parametrize("atb", [False, True])
+@pytest.mark.parametrize("m,n,k", SHAPES + [(300, 520, 1030)])
+def test_f128_ozaki_tolerance(gpu, m, n, k, atb):
+    a, b = gemm_operands(m, n, k, seed=7 + m + n + k, atb=atb)
+    c = gpu.f128_gemm(a, b, m, n, k, gpu.OZAKI, atb)
+    ref = O.gemm(a, b, m, n, k, atb=atb)
+    err = normwise_err(c, ref, abs_prod(a, b, atb))
+    assert err <= 4 * k * 2.0 ** -104, err
+
+
+def test_f128_ozaki_wide_exponents_and_zeros(gpu):
+    rng = np.random.default_rng(3)
+    m, n, k = 70, 90, 150
+    a = dense_dd(m, k, seed=11)
+    b = dense_dd(k, n, seed=12)
+    a *= (2.0 ** rng.integers(-300, 300, size=(m, 1)))[..., None]  # per-row scales
+    b *= (2.0 ** rng.integers(-300, 300, size=(1, n)))[..., None]  # per-column scales
+    a[5] = 0.0          # an all-zero row
+    b[:, 7] = 0.0       # an all-zero column
+    a[9, :] = a[10, :]  # two equal rows
+    c = gpu.f128_gemm(a, b, m, n, k, gpu.OZAKI)
+    ref = O.gemm(a, b, m, n, k)
+    assert np.all(c[5] == 0.0) and np.all(c[:, 7] == 0.0)
+    # row/column scaling makes the error bound entrywise in |A||B|
+    ab = abs_prod(a, b, False)
+    d = np.abs((c[..., 0] - ref[..., 0]) + (c[..., 1] - ref[..., 1]))
+    assert np.all(d <= 4 * k * 2.0 ** -104 * ab + 1e-300)
+
+
+def test_f128_ozaki_cancellation(gpu):
+    """C = A B with B = [x, -x]: the two halves must cancel to (near) zero."""
+    m, k = 40, 200
+    a = dense_dd(m, k, seed=21)
+    x = dense_dd(k, 8, seed=22)
+    b = np.concatenate([x, -x], axis=1)
+    c = gpu.f128_gemm(a, b, m, 16, k, gpu.OZAKI)
+    s = (c[:, :8, 0] + c[:, 8:, 0]) + (c[:, :8, 1] + c[:, 8:, 1])
+    assert np.all(s == 0.0)
+
+
+@pytest.mark.parametrize("atb", [False, True])
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (3, 5, 7), (17, 33, 20), (40, 31, 37)])
+def test_f256_plain_bitexact(gpu, m, n, k, atb):
+    a, b = gemm_operands(m, n, k, seed=5 + m, atb=atb)
+    a4, b4 = dd_to_qd(a), dd_to_qd(b)
+    a4[..., 2] = a4[..., 1] * 2.0 ** -60  # fill the low limbs too
+    c = gpu.f256_gemm(a4, b4, m, n, k, gpu.PLAIN, atb)
+    ref = O.mf_gemm(4, a4, b4, m, n, k, atb=atb)
+    assert np.array_equal(c, ref)
+
+
+def test_zero_sizes_and_nulls(gpu):
+    e = np.zeros((0, 0, 2))
+    assert gpu.f128_gemm(e, e, 0, 0, 0).shape == (0, 0, 2)
+    c = gpu.f128_gemm(np.zeros((3, 0, 2)), np.zeros((0, 4, 2)), 3, 4, 0)
+    assert np.all(c == 0.0)
+    with pytest.raises(gpu.HPError) as ei:
+        gpu.check(gpu.lib().hp_f128_gemm(None, None, None, 2, 2, 2, 0))
+    assert ei.value.code == gpu.HP_ERR_INVALID_ARG
+    with pytest.raises(gpu.HPError):
+        gpu.f128_gemm(np.zeros((2, 2, 2)), np.zeros((2, 2, 2)), 2, 2, 2, mode=7)
+
+
+def test_device_pointer_form(gpu):
+    import torch
+
+    m, n, k = 96, 80, 70
+    a, b = gemm_operands(m, n, k, seed=99)
+    da, db = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+    dc = torch.empty((m, n, 2), dtype=torch.float64, device="cuda")
+    s = torch.cuda.current_stream()
+    gpu.f128_gemm_dev(da, db, dc, m, n, k, gpu.PLAIN, stream=s.cuda_stream)
+    s.synchronize()
+    assert np.array_equal(dc.cpu().numpy(), O.gemm(a, b, m, n, k))
