@@ -155,6 +155,25 @@ def run_reference(args):
     return 0
 
 
+def profile_case(args):
+    """Chosen-path GEMM steps only: the command that ncu captures."""
+    import torch
+
+    import quadprec_b200 as hp
+    from quadprec_b200.workloads import gemm_operands
+
+    a_np, b_np = gemm_operands(M, N, K, seed=0)
+    A = torch.from_numpy(a_np).cuda()
+    B = torch.from_numpy(b_np).cuda()
+    C = torch.empty((M, N, 2), dtype=torch.float64, device="cuda")
+    sptr = torch.cuda.current_stream().cuda_stream
+    for _ in range(args.warmup + args.steps):
+        hp.f128_gemm_dev(A, B, C, M, N, K, hp.OZAKI, stream=sptr)
+    torch.cuda.synchronize()
+    print("profile case done", file=sys.stderr)
+    return 0
+
+
 # ---------------------------------------------------------------- main arm
 def main():
     ap = argparse.ArgumentParser()
@@ -164,9 +183,13 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--profile-case", action="store_true",
+                    help="only run warmup + steps of the chosen path (for ncu captures)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile_case:
+        return profile_case(args)
 
     import numpy as np
     import torch

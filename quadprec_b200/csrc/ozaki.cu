@@ -291,68 +291,83 @@ __device__ __forceinline__ void int_digits(double v, int32_t* d) {
 // Residues of the scaled operand. Logical operand is R x K (row r, reduction
 // index p); element (r, p) is src[r*K + p] (P_CONTIG) or src[p*R + r].
 // Writes out[l][r][p] (int8), row stride Kp, plane stride Rp*Kp, for all
-// r < Rp, p < Kp (zero outside R x K). Tile: 64 rows x 32 p per block.
-constexpr int RT_R = 64, RT_P = 32, RT_STRIDE = 40;
+// r < Rp, p < Kp (zero outside R x K).
+// Block tile: 64 rows x 32 p; each thread owns one row and 8 consecutive p,
+// so its 8 residues of one modulus pack into two 32-bit words.
+//   P_CONTIG: thread reads 8 consecutive f128 (128 B) and stores its 8 bytes
+//             straight to global (a warp writes 8 full 32-byte sectors).
+//   else:     loads are coalesced along r; the bytes are transposed through
+//             shared memory so the global stores run along p.
+constexpr int RT_R = 64, RT_P = 32;
+__device__ __forceinline__ void element_digits(double2 v, int s, int32_t* D) {
+  int32_t dh[NDIG], dl[NDIG];
+  int_digits(scale_pow2(v.x, s), dh);
+  int_digits(scale_pow2(v.y, s), dl);
+#pragma unroll
+  for (int c = 0; c < NDIG; c++) D[c] = dh[c] + dl[c];
+#pragma unroll
+  for (int c = 0; c < NDIG - 1; c++) {
+    int32_t carry = (D[c] + (1 << 21)) >> 22;
+    D[c] -= carry << 22;
+    D[c + 1] += carry;
+  }
+}
+__device__ __forceinline__ uint32_t balanced_byte(const int32_t* D, int l, int m) {
+  int32_t x = 0;
+#pragma unroll
+  for (int c = 0; c < NDIG; c++) x += D[c] * c_tab.pw[l][c];
+  int r = (int)mod_reduce(x, l);
+  if (r > 127) r -= m;
+  return (uint32_t)(r & 0xFF);
+}
 template <bool P_CONTIG>
 __global__ void __launch_bounds__(256) residue_kernel(const double2* __restrict__ src, int64_t R, int64_t K,
                                                       const int* __restrict__ expf, int beta, int L, int64_t Rp,
                                                       int64_t Kp, int8_t* __restrict__ out) {
-  __shared__ __align__(16) uint8_t T[2][RT_R * RT_STRIDE];
+  __shared__ __align__(16) uint32_t T[2][RT_R][RT_P / 4 + 1];
   const int t = threadIdx.x;
-  const int64_t r0 = (int64_t)blockIdx.y * RT_R, p0 = (int64_t)blockIdx.x * RT_P;
+  const int rl = P_CONTIG ? t / 4 : t % 64;
+  const int oct = P_CONTIG ? t % 4 : t / 64;
+  const int64_t r = (int64_t)blockIdx.y * RT_R + rl;
+  const int64_t p0 = (int64_t)blockIdx.x * RT_P + 8 * oct;
   int32_t dig[8][NDIG];
-  int rl[8], pl[8];
 #pragma unroll
-  for (int q = 0; q < 8; q++) {
-    if (P_CONTIG) {
-      rl[q] = t / 32 + 8 * q;
-      pl[q] = t % 32;
-    } else {
-      rl[q] = t % 64;
-      pl[q] = t / 64 + 4 * q;
-    }
-    int64_t r = r0 + rl[q], p = p0 + pl[q];
+  for (int e = 0; e < 8; e++)
 #pragma unroll
-    for (int c = 0; c < NDIG; c++) dig[q][c] = 0;
-    if (r < R && p < K) {
-      int e = expf[r];
-      if (e != EXP_NONFINITE) {
-        double2 v = P_CONTIG ? src[r * K + p] : src[p * R + r];
-        int s = beta + 1022 - e;
-        int32_t dh[NDIG], dl[NDIG];
-        int_digits(scale_pow2(v.x, s), dh);
-        int_digits(scale_pow2(v.y, s), dl);
-        int32_t D[NDIG];
+    for (int c = 0; c < NDIG; c++) dig[e][c] = 0;
+  if (r < R) {
+    const int ex = expf[r];
+    if (ex != EXP_NONFINITE) {
+      const int s = beta + 1022 - ex;
 #pragma unroll
-        for (int c = 0; c < NDIG; c++) D[c] = dh[c] + dl[c];
-#pragma unroll
-        for (int c = 0; c < NDIG - 1; c++) {
-          int32_t carry = (D[c] + (1 << 21)) >> 22;
-          D[c] -= carry << 22;
-          D[c + 1] += carry;
-        }
-#pragma unroll
-        for (int c = 0; c < NDIG; c++) dig[q][c] = D[c];
+      for (int e = 0; e < 8; e++) {
+        const int64_t p = p0 + e;
+        if (p < K) element_digits(P_CONTIG ? src[r * K + p] : src[p * R + r], s, dig[e]);
       }
     }
   }
+  int8_t* const base = out + (size_t)(blockIdx.y * RT_R) * Kp + blockIdx.x * RT_P;
   for (int l = 0; l < L; l++) {
-    uint8_t* Tb = T[l & 1];
     const int m = c_tab.mod[l];
+    uint32_t w0 = 0, w1 = 0;
 #pragma unroll
-    for (int q = 0; q < 8; q++) {
-      int32_t x = 0;
-#pragma unroll
-      for (int c = 0; c < NDIG; c++) x += dig[q][c] * c_tab.pw[l][c];
-      int r = (int)mod_reduce(x, l);
-      if (r > 127) r -= m;
-      Tb[rl[q] * RT_STRIDE + pl[q]] = (uint8_t)(int8_t)r;
+    for (int e = 0; e < 4; e++) {
+      w0 |= balanced_byte(dig[e], l, m) << (8 * e);
+      w1 |= balanced_byte(dig[e + 4], l, m) << (8 * e);
     }
-    __syncthreads();
-    {
-      int row = t / 4, part = t % 4;
-      uint2 v = *reinterpret_cast<const uint2*>(Tb + row * RT_STRIDE + part * 8);
-      *reinterpret_cast<uint2*>(out + (size_t)l * Rp * Kp + (size_t)(r0 + row) * Kp + p0 + part * 8) = v;
+    int8_t* plane = base + (size_t)l * Rp * Kp;
+    if (P_CONTIG) {
+      *reinterpret_cast<uint2*>(plane + (size_t)rl * Kp + 8 * oct) = make_uint2(w0, w1);
+    } else {
+      T[l & 1][rl][2 * oct] = w0;
+      T[l & 1][rl][2 * oct + 1] = w1;
+      __syncthreads();
+      if (t < 2 * RT_R) {
+        const int row = t / 2, half = t % 2;
+        const uint32_t* src_w = &T[l & 1][row][4 * half];
+        *reinterpret_cast<uint4*>(plane + (size_t)row * Kp + 16 * half) =
+            make_uint4(src_w[0], src_w[1], src_w[2], src_w[3]);
+      }
     }
   }
 }
@@ -538,92 +553,99 @@ __global__ void __launch_bounds__(256, 1)
 
 // ---------------------------------------------------------------------------
 // CRT reconstruction: residues -> exact integer -> f128, scaled back.
+// Each thread reconstructs 4 consecutive entries of a row (one 4-byte load
+// per modulus). With NC chunks of 39 bits, every accumulator stays an exact
+// integer below 2^53: 255 * (2^39 - 1) * L < 2^53 for L <= 64.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) crt_dd_kernel(const uint8_t* __restrict__ cres, int64_t plane, int64_t Np,
-                                                     int64_t m, int64_t n, const int* __restrict__ expA,
-                                                     const int* __restrict__ expB, int beta,
-                                                     const CrtTable* __restrict__ tab, double2* __restrict__ C) {
-  __shared__ double w_s[MAXL][NCMAX];
-  __shared__ double mch_s[NCMAX];
-  const int L = tab->L, nc = tab->nc;
-  for (int i = threadIdx.x; i < L * NCMAX; i += blockDim.x) w_s[i / NCMAX][i % NCMAX] = tab->w[i / NCMAX][i % NCMAX];
-  if (threadIdx.x < NCMAX) mch_s[threadIdx.x] = tab->mchunk[threadIdx.x];
-  __syncthreads();
-  const double inv_m = tab->inv_m;
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= m * n) return;
-  const int64_t i = idx / n, j = idx % n;
-  const int ea = expA[i], eb = expB[j];
-  if (ea == EXP_NONFINITE || eb == EXP_NONFINITE) {
-    C[idx] = make_double2(__longlong_as_double(0x7ff8000000000000ll), 0.0);
-    return;
+__device__ __forceinline__ double byte_to_double(uint32_t b) {
+  // exact: 2^52 + b has b in its low mantissa bits
+  return __dsub_rn(__hiloint2double(0x43300000, (int)b), 4503599627370496.0);
+}
+template <int NC>
+__device__ __forceinline__ void carry_normalise(double* acc) {
+#pragma unroll
+  for (int c = 0; c < NC; c++) {
+    double carry = floor(__dmul_rn(acc[c], 0x1p-39));
+    acc[c] = __fma_rn(-carry, 0x1p39, acc[c]);
+    acc[c + 1] = __dadd_rn(acc[c + 1], carry);
   }
-  double acc[NCMAX + 1];
-#pragma unroll
-  for (int c = 0; c <= NCMAX; c++) acc[c] = 0.0;
-  const uint8_t* rp = cres + (size_t)i * Np + j;
-  for (int l = 0; l < L; l++) {
-    const double r = (double)rp[(size_t)l * plane];
-#pragma unroll
-    for (int c = 0; c < NCMAX; c++)
-      if (c < nc) acc[c] = __fma_rn(r, w_s[l][c], acc[c]);
-  }
-  // carry-normalise into [0, 2^39) chunks; acc[nc] takes the carry out
-#pragma unroll
-  for (int c = 0; c < NCMAX; c++)
-    if (c < nc) {
-      double carry = floor(__dmul_rn(acc[c], 0x1p-39));
-      acc[c] = __dsub_rn(acc[c], __dmul_rn(carry, 0x1p39));
-      acc[c + 1] = __dadd_rn(acc[c + 1], carry);
-    }
+}
+template <int NC>
+__device__ __forceinline__ dd crt_finish(double* acc, const double* mch, double inv_m, bool* neg_out) {
+  carry_normalise<NC>(acc);
   // q = round(X / M): the true value is X - qM with |X - qM| <= M/4
-  double xa = 0.0;
+  double xa = __fma_rn(acc[NC], 0x1p39, acc[NC - 1]);
+  xa = __fma_rn(xa, 0x1p39, acc[NC - 2]);
+  const double q = rint(__dmul_rn(__dmul_rn(xa, scale_pow2(1.0, CRT_BITS * (NC - 2))), inv_m));
 #pragma unroll
-  for (int c = NCMAX; c >= 0; c--)
-    if (c <= nc && c >= nc - 2) xa = __fma_rn(acc[c], scale_pow2(1.0, CRT_BITS * c), xa);
-  const double q = rint(__dmul_rn(xa, inv_m));
+  for (int c = 0; c < NC; c++) acc[c] = __fma_rn(-q, mch[c], acc[c]);
+  carry_normalise<NC>(acc);
+  bool neg = acc[NC] < 0.0;
+  if (neg) {
 #pragma unroll
-  for (int c = 0; c < NCMAX; c++)
-    if (c < nc) acc[c] = __fma_rn(-q, mch_s[c], acc[c]);
-#pragma unroll
-  for (int c = 0; c < NCMAX; c++)
-    if (c < nc) {
-      double carry = floor(__dmul_rn(acc[c], 0x1p-39));
-      acc[c] = __dsub_rn(acc[c], __dmul_rn(carry, 0x1p39));
-      acc[c + 1] = __dadd_rn(acc[c + 1], carry);
-    }
-  bool neg = false;
-  double top = 0.0;
-#pragma unroll
-  for (int c = 0; c <= NCMAX; c++)
-    if (c == nc) top = acc[c];
-  if (top < 0.0) {  // negate: chunks become -acc, renormalise (top -> 0)
-    neg = true;
-#pragma unroll
-    for (int c = 0; c <= NCMAX; c++) acc[c] = -acc[c];
-#pragma unroll
-    for (int c = 0; c < NCMAX; c++)
-      if (c < nc) {
-        double carry = floor(__dmul_rn(acc[c], 0x1p-39));
-        acc[c] = __dsub_rn(acc[c], __dmul_rn(carry, 0x1p39));
-        acc[c + 1] = __dadd_rn(acc[c + 1], carry);
-      }
+    for (int c = 0; c <= NC; c++) acc[c] = -acc[c];
+    carry_normalise<NC>(acc);
   }
   // sum the non-negative, non-overlapping chunks from the top into f128
   dd s = dd{0.0, 0.0};
 #pragma unroll
-  for (int c = NCMAX - 1; c >= 0; c--)
-    if (c < nc) {
-      double v = scale_pow2(acc[c], CRT_BITS * c);
-      double hs, he;
-      two_sum(s.hi, v, hs, he);
-      s = dd_renorm(hs, __dadd_rn(he, s.lo));
+  for (int c = NC - 1; c >= 0; c--) {
+    double v = scale_pow2(acc[c], CRT_BITS * c);
+    double hs, he;
+    two_sum(s.hi, v, hs, he);
+    s = dd_renorm(hs, __dadd_rn(he, s.lo));
+  }
+  *neg_out = neg;
+  return s;
+}
+template <int NC>
+__global__ void __launch_bounds__(256) crt_dd_kernel(const uint8_t* __restrict__ cres, int64_t plane, int64_t Np,
+                                                     int64_t m, int64_t n, const int* __restrict__ expA,
+                                                     const int* __restrict__ expB, int beta,
+                                                     const CrtTable* __restrict__ tab, double2* __restrict__ C) {
+  __shared__ double w_s[MAXL][NC];
+  __shared__ double mch_s[NC];
+  const int L = tab->L;
+  for (int i = threadIdx.x; i < L * NC; i += blockDim.x) w_s[i / NC][i % NC] = tab->w[i / NC][i % NC];
+  if (threadIdx.x < NC) mch_s[threadIdx.x] = tab->mchunk[threadIdx.x];
+  __syncthreads();
+  const double inv_m = tab->inv_m;
+  const int64_t qpr = (n + 3) / 4;  // 4-entry groups per row
+  const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= m * qpr) return;
+  const int64_t i = g / qpr, j0 = 4 * (g % qpr);
+  const int ea = expA[i];
+  double acc[4][NC + 1];
+#pragma unroll
+  for (int e = 0; e < 4; e++)
+#pragma unroll
+    for (int c = 0; c <= NC; c++) acc[e][c] = 0.0;
+  const uint8_t* rp = cres + (size_t)i * Np + j0;
+  for (int l = 0; l < L; l++) {
+    const uint32_t v = *reinterpret_cast<const uint32_t*>(rp + (size_t)l * plane);
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const double r = byte_to_double((v >> (8 * e)) & 0xFFu);
+#pragma unroll
+      for (int c = 0; c < NC; c++) acc[e][c] = __fma_rn(r, w_s[l][c], acc[e][c]);
     }
-  const int shift = -((beta + 1022 - ea) + (beta + 1022 - eb));
-  double hi = scale_pow2(s.hi, shift), lo = scale_pow2(s.lo, shift);
-  dd o = dd_renorm(hi, lo);
-  if (neg) o = dd_neg(o);
-  C[idx] = make_double2(o.hi, o.lo);
+  }
+#pragma unroll
+  for (int e = 0; e < 4; e++) {
+    const int64_t j = j0 + e;
+    if (j >= n) break;
+    const int eb = expB[j];
+    if (ea == EXP_NONFINITE || eb == EXP_NONFINITE) {
+      C[i * n + j] = make_double2(__longlong_as_double(0x7ff8000000000000ll), 0.0);
+      continue;
+    }
+    bool neg;
+    dd s = crt_finish<NC>(acc[e], mch_s, inv_m, &neg);
+    const int shift = -((beta + 1022 - ea) + (beta + 1022 - eb));
+    dd o = dd_renorm(scale_pow2(s.hi, shift), scale_pow2(s.lo, shift));
+    if (neg) o = dd_neg(o);
+    C[i * n + j] = make_double2(o.hi, o.lo);
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -659,6 +681,25 @@ static int make_map(CUtensorMap* map, const void* base, uint64_t K, uint64_t R, 
     set_error("cuTensorMapEncodeTiled failed (%d)", (int)rc);
     return HP_ERR_CUDA;
   }
+  return HP_OK;
+}
+
+static int launch_crt_dd(const uint8_t* cres, size_t Mp, size_t Np, size_t m, size_t n, const int* expA,
+                         const int* expB, int beta, const CrtTable* tab, int nc, double2* C, cudaStream_t s) {
+  const int64_t groups = (int64_t)m * (int64_t)((n + 3) / 4);
+  const unsigned grid = (unsigned)((groups + 255) / 256);
+#define HP_CRT_CASE(NC)                                                                                       \
+  case NC:                                                                                                    \
+    crt_dd_kernel<NC><<<grid, 256, 0, s>>>(cres, (int64_t)(Mp * Np), (int64_t)Np, m, n, expA, expB, beta, tab, C); \
+    break;
+  switch (nc) {
+    HP_CRT_CASE(3) HP_CRT_CASE(4) HP_CRT_CASE(5) HP_CRT_CASE(6) HP_CRT_CASE(7) HP_CRT_CASE(8) HP_CRT_CASE(9)
+    default:
+      set_error("ozaki: unsupported CRT chunk count %d", nc);
+      return HP_ERR_UNSUPPORTED;
+  }
+#undef HP_CRT_CASE
+  HP_LAUNCH_CHECK();
   return HP_OK;
 }
 
@@ -780,14 +821,8 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
   HP_TRY(ozaki_residue_gemm(ares.as<int8_t>(), bres.as<int8_t>(), cres.as<uint8_t>(), L, Mp, Np, Kp, s));
   profile_mark(s, "i8_gemm");
   // 4. CRT
-  {
-    int64_t total = (int64_t)(m * n);
-    crt_dd_kernel<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(cres.as<uint8_t>(), (int64_t)(Mp * Np),
-                                                                  (int64_t)Np, m, n, expA.as<int>(),
-                                                                  expB.as<int>(), beta, D->crt + L,
-                                                                  reinterpret_cast<double2*>(c));
-    HP_LAUNCH_CHECK();
-  }
+  HP_TRY(launch_crt_dd(cres.as<uint8_t>(), Mp, Np, m, n, expA.as<int>(), expB.as<int>(), beta, D->crt + L,
+                       host_tables().crt[L].nc, reinterpret_cast<double2*>(c), s));
   profile_mark(s, "crt");
   return HP_OK;
 }
