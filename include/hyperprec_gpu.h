@@ -105,6 +105,58 @@ int hp_f256_gemm_dev(const double* a, const double* b, double* c, size_t m, size
 int hp_f256_gemm_atb_dev(const double* a, const double* b, double* c, size_t m, size_t n,
                          size_t k, int mode, void* stream);
 
+/* ------------------------------------------------------------------------
+ * f128 Cholesky and triangular solves
+ * ---------------------------------------------------------------------- */
+/* replaces: pub fn cholesky(a: &mut [f128], n: usize) -> Result<(), CholeskyError>
+ *           crates/quad/src/linalg.rs:42-96
+ * In place: the lower triangle of a becomes L (bit-identical to the
+ * reference); the strict upper triangle is left untouched. On a pivot <= 0
+ * returns HP_ERR_NOT_SPD with *pivot and *value (CholeskyError{pivot,value},
+ * linalg.rs:197-200; either pointer may be NULL) and a is unspecified. */
+int hp_f128_cholesky(double* a, size_t n, int64_t* pivot, double* value);
+/* replaces: pub fn cholesky_blocked(a: &mut [f128], n: usize, nb: usize)
+ *           crates/quad/src/linalg.rs:238-293  (nb = 0 means 64; nb <= 64)
+ * Bit-identical to the reference's blocked arithmetic for the same nb. */
+int hp_f128_cholesky_blocked(double* a, size_t n, size_t nb, int64_t* pivot, double* value);
+/* Device-pointer form of hp_f128_cholesky; synchronises `stream` to report
+ * HP_ERR_NOT_SPD. */
+int hp_f128_cholesky_dev(double* a, size_t n, int64_t* pivot, double* value, void* stream);
+/* replaces: pub fn forward_solve(l, b, n) -> Vec<f128>   linalg.rs:99-108
+ * L y = b; bit-identical. */
+int hp_f128_forward_solve(const double* l, const double* b, double* y, size_t n);
+/* replaces: pub fn backward_solve(l, y, n) -> Vec<f128>  linalg.rs:111-120
+ * L^T x = y; normwise error within the reference's bound (summation order
+ * differs, see quadprec_b200/csrc/solve.cu). */
+int hp_f128_backward_solve(const double* l, const double* y, double* x, size_t n);
+/* replaces: pub fn solve_cholesky(l, b, n) -> Vec<f128>  linalg.rs:123-126 */
+int hp_f128_solve_cholesky(const double* l, const double* b, double* x, size_t n);
+/* replaces: pub fn matvec(a, x, n) -> Vec<f128>          linalg.rs:129-147
+ * bit-identical. */
+int hp_f128_matvec(const double* a, const double* x, double* y, size_t n);
+/* replaces: pub fn cond_estimate(l, n) -> f64            linalg.rs:185-194 */
+int hp_f128_cond_estimate(const double* l, size_t n, double* kappa);
+
+/* ------------------------------------------------------------------------
+ * SPD solver (crates/solver/src/lib.rs)
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  double kappa;          /* Solution.kappa            (lib.rs:16) */
+  double residual_norm;  /* Solution.residual_norm    (lib.rs:18) */
+  int32_t strategy;      /* 0 Float64, 1 MixedPrecision, 2 Float128 (lib.rs:26-30) */
+  int32_t refinement_iters;
+} hp_solution_t;
+/* replaces: pub fn solve_spd(a_f64: &[f64], b_f64: &[f64], n) -> Result<Solution, SolveError>
+ *           crates/solver/src/lib.rs:38-68
+ * Same strategy selection (f64 Cholesky, kappa < 1e10, f128 refinement up
+ * to 30 steps, f128 fallback). x: n f128 (Solution.x), x_f64: n doubles
+ * (may be NULL). HP_ERR_NOT_SPD sets *pivot (SolveError::NotPositiveDefinite). */
+int hp_solve_spd(const double* a_f64, const double* b_f64, size_t n, double* x, double* x_f64,
+                 hp_solution_t* sol, int64_t* pivot);
+/* replaces: pub fn solve_spd_f128(a: &[f128], b: &[f128], n)  lib.rs:71-73 */
+int hp_solve_spd_f128(const double* a, const double* b, size_t n, double* x, double* x_f64,
+                      hp_solution_t* sol, int64_t* pivot);
+
 #ifdef __cplusplus
 }
 #endif

@@ -58,7 +58,26 @@ SIGNATURES = {
     "hp_f256_gemm_atb": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int], ctypes.c_int),
     "hp_f256_gemm_dev": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int, _vp], ctypes.c_int),
     "hp_f256_gemm_atb_dev": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int, _vp], ctypes.c_int),
+    "hp_f128_cholesky": ([_vp, _sz, _i64p, _d], ctypes.c_int),
+    "hp_f128_cholesky_blocked": ([_vp, _sz, _sz, _i64p, _d], ctypes.c_int),
+    "hp_f128_cholesky_dev": ([_vp, _sz, _i64p, _d, _vp], ctypes.c_int),
+    "hp_f128_forward_solve": ([_vp, _vp, _vp, _sz], ctypes.c_int),
+    "hp_f128_backward_solve": ([_vp, _vp, _vp, _sz], ctypes.c_int),
+    "hp_f128_solve_cholesky": ([_vp, _vp, _vp, _sz], ctypes.c_int),
+    "hp_f128_matvec": ([_vp, _vp, _vp, _sz], ctypes.c_int),
+    "hp_f128_cond_estimate": ([_vp, _sz, _d], ctypes.c_int),
+    "hp_solve_spd": ([_vp, _vp, _sz, _vp, _vp, _vp, _i64p], ctypes.c_int),
+    "hp_solve_spd_f128": ([_vp, _vp, _sz, _vp, _vp, _vp, _i64p], ctypes.c_int),
 }
+
+
+class Solution(ctypes.Structure):
+    """hp_solution_t (crates/solver/src/lib.rs:10-23 Solution, without vectors)."""
+    _fields_ = [("kappa", ctypes.c_double), ("residual_norm", ctypes.c_double),
+                ("strategy", ctypes.c_int32), ("refinement_iters", ctypes.c_int32)]
+
+
+STRATEGIES = ("Float64", "MixedPrecision", "Float128")
 
 
 def lib():
@@ -137,3 +156,74 @@ def f128_gemm_dev(a, b, c, m, n, k, mode=PLAIN, atb=False, stream=0) -> None:
 def f256_gemm_dev(a, b, c, m, n, k, mode=PLAIN, atb=False, stream=0) -> None:
     fn = lib().hp_f256_gemm_atb_dev if atb else lib().hp_f256_gemm_dev
     check(fn(_ptr(a), _ptr(b), _ptr(c), m, n, k, mode, stream))
+
+
+# ---------------- Cholesky / solves / SPD ----------------
+class CholeskyError(HPError):
+    """linalg.rs:197-200 CholeskyError { pivot, value }."""
+
+    def __init__(self, pivot: int, value: float):
+        RuntimeError.__init__(self, f"Cholesky failed at pivot {pivot} (value={value:.4e})")
+        self.code, self.pivot, self.value = HP_ERR_NOT_SPD, pivot, value
+
+
+def _chol_call(fn, a, *args):
+    a = _c(a).copy()
+    pv, val = ctypes.c_int64(-1), ctypes.c_double(0.0)
+    rc = fn(_ptr(a), *args, ctypes.byref(pv), ctypes.byref(val))
+    if rc == HP_ERR_NOT_SPD:
+        raise CholeskyError(pv.value, val.value)
+    check(rc)
+    return a
+
+
+def f128_cholesky(a, n):
+    """linalg.rs:42 cholesky; returns a copy with L in the lower triangle."""
+    return _chol_call(lib().hp_f128_cholesky, a, n)
+
+
+def f128_cholesky_blocked(a, n, nb):
+    """linalg.rs:238 cholesky_blocked."""
+    return _chol_call(lib().hp_f128_cholesky_blocked, a, n, nb)
+
+
+def _solve(name, l, b, n):
+    l, b = _c(l), _c(b)
+    out = np.empty((n, 2))
+    check(getattr(lib(), name)(_ptr(l), _ptr(b), _ptr(out), n))
+    return out
+
+
+def f128_forward_solve(l, b, n): return _solve("hp_f128_forward_solve", l, b, n)
+def f128_backward_solve(l, y, n): return _solve("hp_f128_backward_solve", l, y, n)
+def f128_solve_cholesky(l, b, n): return _solve("hp_f128_solve_cholesky", l, b, n)
+def f128_matvec(a, x, n): return _solve("hp_f128_matvec", a, x, n)
+
+
+def f128_cond_estimate(l, n) -> float:
+    out = ctypes.c_double(0)
+    check(lib().hp_f128_cond_estimate(_ptr(_c(l)), n, ctypes.byref(out)))
+    return out.value
+
+
+def _spd(fn, a, b, n):
+    a, b = _c(a), _c(b)
+    x, xf = np.empty((n, 2)), np.empty(n)
+    sol = Solution()
+    pv = ctypes.c_int64(-1)
+    rc = fn(_ptr(a), _ptr(b), n, _ptr(x), _ptr(xf), ctypes.byref(sol), ctypes.byref(pv))
+    if rc == HP_ERR_NOT_SPD:
+        raise HPError(rc, f"Matrix is not positive definite (failed at pivot {pv.value})")
+    check(rc)
+    return {"x": x, "x_f64": xf, "kappa": sol.kappa, "residual_norm": sol.residual_norm,
+            "strategy": STRATEGIES[sol.strategy], "refinement_iters": sol.refinement_iters}
+
+
+def solve_spd(a_f64, b_f64, n):
+    """crates/solver/src/lib.rs:38 solve_spd."""
+    return _spd(lib().hp_solve_spd, a_f64, b_f64, n)
+
+
+def solve_spd_f128(a, b, n):
+    """crates/solver/src/lib.rs:71 solve_spd_f128."""
+    return _spd(lib().hp_solve_spd_f128, a, b, n)

@@ -1,0 +1,303 @@
+// Blocked right-looking Cholesky on the GPU that reproduces the reference's
+// factorisations bit-for-bit.
+//
+// reference `cholesky` (crates/quad/src/linalg.rs:42-96) and `cholesky_f64`
+// (crates/solver/src/lib.rs:169-195): for each column j,
+//     s_ij = sum_{k<j} L_ik L_jk  (accumulated in k order from zero),
+//     L_jj = sqrt(A_jj - s_jj),  L_ij = (A_ij - s_ij) * recip(L_jj).
+// Here the sums s_ij live in a separate accumulator S. Processing columns in
+// blocks of nb, the trailing update adds the block's products to S in k
+// order, so every s_ij sees exactly the reference's sequence of additions:
+// the result does not depend on nb and equals the reference bit-for-bit.
+//
+// reference `cholesky_blocked` (linalg.rs:238-293, with trsm_right_lt
+// :224-235): the diagonal block is factored from zero sums, the panel is
+// solved by subtracting products one at a time, and the trailing block
+// subtracts each block-sum from A. The BLOCKED template flag reproduces that
+// arithmetic (nb is then part of the definition, as in the reference).
+//
+// Three kernels per block column: diag (one CTA), panel (one thread per row),
+// syrk (64 x 64 lower-triangular tiles of the trailing matrix, CUDA cores).
+#include "hp_arith.cuh"
+#include "hp_runtime.cuh"
+#include "kernels.cuh"
+
+namespace hp {
+
+// Scalar traits: the same kernels run in f64 (cholesky_f64) and f128.
+struct OpsF64 {
+  using T = double;
+  __device__ static T zero() { return 0.0; }
+  __device__ static T add(T a, T b) { return __dadd_rn(a, b); }
+  __device__ static T sub(T a, T b) { return __dsub_rn(a, b); }
+  __device__ static T mul(T a, T b) { return __dmul_rn(a, b); }
+  __device__ static T sqrt_(T a) { return __dsqrt_rn(a); }
+  __device__ static T inv(T a) { return __ddiv_rn(1.0, a); }  // lib.rs:182: 1.0 / ljj
+  __device__ static double hi(T a) { return a; }
+  __device__ static double to_f64(T a) { return a; }
+};
+struct OpsDD {
+  using T = dd;
+  __device__ static T zero() { return dd{0.0, 0.0}; }
+  __device__ static T add(T a, T b) { return dd_add(a, b); }
+  __device__ static T sub(T a, T b) { return dd_sub(a, b); }
+  __device__ static T mul(T a, T b) { return dd_mul(a, b); }
+  __device__ static T sqrt_(T a) { return dd_sqrt(a); }
+  __device__ static T inv(T a) { return dd_recip(a); }  // linalg.rs:60: ljj.recip()
+  __device__ static double hi(T a) { return a.hi; }
+  __device__ static double to_f64(T a) { return __dadd_rn(a.hi, a.lo); }
+};
+
+struct CholErr {
+  int flag;
+  int pad;
+  int64_t pivot;
+  double value;
+};
+
+namespace {
+
+constexpr int CH_MAXNB = 64;
+
+// Diagonal block [kb, kb+jb): one CTA of 64 threads, thread t owns row kb+t.
+template <class O, bool BLOCKED>
+__global__ void __launch_bounds__(CH_MAXNB) chol_diag_kernel(typename O::T* A, const typename O::T* S, int64_t n,
+                                                             int64_t kb, int jb, typename O::T* invd, CholErr* err) {
+  using T = typename O::T;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  T* Ls = reinterpret_cast<T*>(sm_raw);  // [64][65]
+  __shared__ T inv_s[CH_MAXNB];
+  __shared__ int fail;
+  const int t = threadIdx.x;
+  if (err->flag) return;
+  if (t == 0) fail = 0;
+  if (t < jb)
+    for (int c = 0; c <= t; c++) Ls[t * 65 + c] = A[(kb + t) * n + kb + c];
+  __syncthreads();
+  for (int j = 0; j < jb; j++) {
+    if (t == j) {
+      T s = BLOCKED ? O::zero() : S[(kb + j) * n + kb + j];
+      for (int k = 0; k < j; k++) {
+        T l = Ls[j * 65 + k];
+        s = O::add(s, O::mul(l, l));
+      }
+      T d = O::sub(Ls[j * 65 + j], s);
+      if (!(O::hi(d) > 0.0) && !(O::hi(d) != O::hi(d))) {  // diag <= 0 (NaN passes, as in Rust)
+        fail = 1;
+        err->flag = 1;
+        err->pivot = kb + j;
+        err->value = O::to_f64(d);
+      } else {
+        T l = O::sqrt_(d);
+        Ls[j * 65 + j] = l;
+        inv_s[j] = O::inv(l);
+      }
+    }
+    __syncthreads();
+    if (fail) return;
+    if (t > j && t < jb) {
+      T s = BLOCKED ? O::zero() : S[(kb + t) * n + kb + j];
+      for (int k = 0; k < j; k++) s = O::add(s, O::mul(Ls[t * 65 + k], Ls[j * 65 + k]));
+      Ls[t * 65 + j] = O::mul(O::sub(Ls[t * 65 + j], s), inv_s[j]);
+    }
+    __syncthreads();
+  }
+  if (t < jb) {
+    for (int c = 0; c <= t; c++) A[(kb + t) * n + kb + c] = Ls[t * 65 + c];
+    invd[kb + t] = inv_s[t];
+  }
+}
+
+// Panel rows i >= kb+jb, columns [kb, kb+jb): one thread per row.
+template <class O, bool BLOCKED>
+__global__ void __launch_bounds__(64) chol_panel_kernel(typename O::T* A, const typename O::T* S, int64_t n,
+                                                        int64_t kb, int jb, const typename O::T* invd,
+                                                        const CholErr* err) {
+  using T = typename O::T;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  T* Ld = reinterpret_cast<T*>(sm_raw);  // [jb][jb]
+  T* Lr = Ld + jb * jb;                   // [jb][64]: this block's rows, column-major
+  if (err->flag) return;
+  const int t = threadIdx.x;
+  for (int e = t; e < jb * jb; e += 64) {
+    int r = e / jb, c = e % jb;
+    Ld[e] = (c <= r) ? A[(kb + r) * n + kb + c] : O::zero();
+  }
+  __syncthreads();
+  const int64_t i = kb + jb + (int64_t)blockIdx.x * 64 + t;
+  if (i >= n) return;
+  T* arow = A + i * n + kb;
+  for (int j = 0; j < jb; j++) {
+    T v;
+    if (BLOCKED) {  // trsm_right_lt: s = b_ij; s -= b_ik l_jk; b_ij = s * recip(l_jj)
+      T s = arow[j];
+      for (int k = 0; k < j; k++) s = O::sub(s, O::mul(Lr[k * 64 + t], Ld[j * jb + k]));
+      v = O::mul(s, invd[kb + j]);
+    } else {
+      T s = S[i * n + kb + j];
+      for (int k = 0; k < j; k++) s = O::add(s, O::mul(Lr[k * 64 + t], Ld[j * jb + k]));
+      v = O::mul(O::sub(arow[j], s), invd[kb + j]);
+    }
+    Lr[j * 64 + t] = v;
+  }
+  for (int j = 0; j < jb; j++) arow[j] = Lr[j * 64 + t];
+}
+
+// Trailing update on the lower triangle of rows/cols >= t0 = kb + jb:
+//   unblocked semantics: S_ij = S_ij + sum_{k in block} L_ik L_jk  (k order)
+//   BLOCKED:             A_ij = A_ij - (sum_{k in block} L_ik L_jk)
+// 64 x 64 tiles, 256 threads, 4 x 4 entries per thread; the block's jb
+// columns are staged through shared memory in k-slices of 16.
+template <class O, bool BLOCKED>
+__global__ void __launch_bounds__(256) chol_syrk_kernel(typename O::T* A, typename O::T* S, int64_t n, int64_t kb,
+                                                        int jb, const CholErr* err) {
+  using T = typename O::T;
+  __shared__ T Ps[16][64 + 1], Qs[16][64 + 1];
+  if (err->flag) return;
+  const int64_t t0 = kb + jb;
+  // lower-triangular tile index -> (bi, bj), bi >= bj
+  int64_t idx = blockIdx.x;
+  int64_t bi = (int64_t)((sqrt(8.0 * (double)idx + 1.0) - 1.0) * 0.5);
+  while (bi * (bi + 1) / 2 > idx) bi--;
+  while ((bi + 1) * (bi + 2) / 2 <= idx) bi++;
+  const int64_t bj = idx - bi * (bi + 1) / 2;
+  const int64_t i0 = t0 + bi * 64, j0 = t0 + bj * 64;
+  const int tx = threadIdx.x % 16, ty = threadIdx.x / 16, tid = threadIdx.x;
+  T acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      int64_t i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
+      acc[a][b] = (!BLOCKED && i < n && j < n && j <= i) ? S[i * n + j] : O::zero();
+    }
+  for (int k0 = 0; k0 < jb; k0 += 16) {
+    __syncthreads();
+    for (int e = tid; e < 16 * 64; e += 256) {
+      int r = e / 16, c = e % 16;  // row r of the tile, k offset c
+      int64_t gi = i0 + r, gj = j0 + r;
+      bool kin = k0 + c < jb;
+      Ps[c][r] = (gi < n && kin) ? A[gi * n + kb + k0 + c] : O::zero();
+      Qs[c][r] = (gj < n && kin) ? A[gj * n + kb + k0 + c] : O::zero();
+    }
+    __syncthreads();
+    const int kmax = min(16, jb - k0);
+    for (int kk = 0; kk < kmax; kk++) {
+      T p[4], q[4];
+#pragma unroll
+      for (int a = 0; a < 4; a++) p[a] = Ps[kk][ty + 16 * a];
+#pragma unroll
+      for (int b = 0; b < 4; b++) q[b] = Qs[kk][tx + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; a++)
+#pragma unroll
+        for (int b = 0; b < 4; b++) acc[a][b] = O::add(acc[a][b], O::mul(p[a], q[b]));
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 4; a++)
+#pragma unroll
+    for (int b = 0; b < 4; b++) {
+      int64_t i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
+      if (i < n && j < n && j <= i) {
+        if (BLOCKED)
+          A[i * n + j] = O::sub(A[i * n + j], acc[a][b]);
+        else
+          S[i * n + j] = acc[a][b];
+      }
+    }
+}
+
+// cholesky_f64 zeroes the strict upper triangle (lib.rs:190-192).
+__global__ void zero_upper_kernel(double* L, int64_t n) {
+  int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= n * n) return;
+  int64_t i = idx / n, j = idx % n;
+  if (j > i) L[idx] = 0.0;
+}
+
+template <class O, bool BLOCKED>
+int cholesky_run(typename O::T* A, size_t n, size_t nb, CholErr* derr, cudaStream_t s) {
+  using T = typename O::T;
+  DevBuf Sbuf(BLOCKED ? 0 : n * n * sizeof(T), s), invd(n * sizeof(T), s);
+  if ((!BLOCKED && !Sbuf.p) || !invd.p) {
+    set_error("cholesky: workspace allocation failed");
+    return HP_ERR_CUDA;
+  }
+  T* S = Sbuf.as<T>();
+  if (!BLOCKED) HP_CUDA_TRY(cudaMemsetAsync(S, 0, n * n * sizeof(T), s));
+  const size_t diag_smem = 64 * 65 * sizeof(T);
+  static bool attr[2] = {false, false};
+  if (!attr[0]) {
+    cudaFuncSetAttribute(chol_diag_kernel<O, BLOCKED>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 65 * 16);
+    cudaFuncSetAttribute(chol_panel_kernel<O, BLOCKED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         (64 * 64 + 64 * 64) * 16);
+    attr[0] = true;
+  }
+  for (size_t kb = 0; kb < n; kb += nb) {
+    const int jb = (int)std::min(nb, n - kb);
+    chol_diag_kernel<O, BLOCKED><<<1, CH_MAXNB, diag_smem, s>>>(A, S, n, kb, jb, invd.as<T>(), derr);
+    HP_LAUNCH_CHECK();
+    const size_t rest = n - kb - jb;
+    if (rest == 0) break;
+    const size_t panel_smem = (size_t)(jb * jb + jb * 64) * sizeof(T);
+    chol_panel_kernel<O, BLOCKED><<<(unsigned)((rest + 63) / 64), 64, panel_smem, s>>>(A, S, n, kb, jb,
+                                                                                      invd.as<T>(), derr);
+    HP_LAUNCH_CHECK();
+    const size_t tiles = (rest + 63) / 64;
+    chol_syrk_kernel<O, BLOCKED><<<(unsigned)(tiles * (tiles + 1) / 2), 256, 0, s>>>(A, S, n, kb, jb, derr);
+    HP_LAUNCH_CHECK();
+  }
+  return HP_OK;
+}
+
+}  // namespace
+
+int dd_cholesky(double* a, size_t n, size_t nb, bool blocked, int64_t* pivot, double* value, cudaStream_t s,
+                bool sync_status) {
+  if (n == 0) return HP_OK;
+  if (nb == 0) nb = blocked ? 64 : 32;
+  if (nb > (size_t)CH_MAXNB) {
+    set_error("cholesky: block size %zu exceeds %d", nb, CH_MAXNB);
+    return HP_ERR_UNSUPPORTED;
+  }
+  DevBuf err(sizeof(CholErr), s);
+  if (!err.p) return HP_ERR_CUDA;
+  HP_CUDA_TRY(cudaMemsetAsync(err.p, 0, sizeof(CholErr), s));
+  int rc = blocked ? cholesky_run<OpsDD, true>(reinterpret_cast<dd*>(a), n, nb, err.as<CholErr>(), s)
+                   : cholesky_run<OpsDD, false>(reinterpret_cast<dd*>(a), n, nb, err.as<CholErr>(), s);
+  if (rc != HP_OK) return rc;
+  if (sync_status) {
+    CholErr h;
+    HP_CUDA_TRY(cudaMemcpyAsync(&h, err.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));
+    if (h.flag) {
+      if (pivot) *pivot = h.pivot;
+      if (value) *value = h.value;
+      set_error("Cholesky failed at pivot %lld (value=%.4e)", (long long)h.pivot, h.value);
+      return HP_ERR_NOT_SPD;
+    }
+  }
+  return HP_OK;
+}
+
+int f64_cholesky(double* a, size_t n, int64_t* pivot, cudaStream_t s) {
+  if (n == 0) return HP_OK;
+  DevBuf err(sizeof(CholErr), s);
+  if (!err.p) return HP_ERR_CUDA;
+  HP_CUDA_TRY(cudaMemsetAsync(err.p, 0, sizeof(CholErr), s));
+  HP_TRY((cholesky_run<OpsF64, false>(a, n, 32, err.as<CholErr>(), s)));
+  CholErr h;
+  HP_CUDA_TRY(cudaMemcpyAsync(&h, err.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  if (h.flag) {
+    if (pivot) *pivot = h.pivot;
+    set_error("f64 Cholesky failed at pivot %lld", (long long)h.pivot);
+    return HP_ERR_NOT_SPD;
+  }
+  zero_upper_kernel<<<(unsigned)((n * n + 255) / 256), 256, 0, s>>>(a, n);
+  HP_LAUNCH_CHECK();
+  return HP_OK;
+}
+
+}  // namespace hp

@@ -621,13 +621,22 @@ __global__ void __launch_bounds__(256) crt_dd_kernel(const uint8_t* __restrict__
 #pragma unroll
     for (int c = 0; c <= NC; c++) acc[e][c] = 0.0;
   const uint8_t* rp = cres + (size_t)i * Np + j0;
-  for (int l = 0; l < L; l++) {
-    const uint32_t v = *reinterpret_cast<const uint32_t*>(rp + (size_t)l * plane);
+  // Issue the residue loads of 8 moduli back to back, then consume them, so
+  // each thread waits for memory once per 8 moduli rather than once each.
+  for (int l0 = 0; l0 < L; l0 += 8) {
+    uint32_t v[8];
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const double r = byte_to_double((v >> (8 * e)) & 0xFFu);
+    for (int u = 0; u < 8; u++)
+      v[u] = (l0 + u < L) ? __ldg(reinterpret_cast<const uint32_t*>(rp + (size_t)(l0 + u) * plane)) : 0u;
 #pragma unroll
-      for (int c = 0; c < NC; c++) acc[e][c] = __fma_rn(r, w_s[l][c], acc[e][c]);
+    for (int u = 0; u < 8; u++) {
+      if (l0 + u >= L) break;
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const double r = byte_to_double((v[u] >> (8 * e)) & 0xFFu);
+#pragma unroll
+        for (int c = 0; c < NC; c++) acc[e][c] = __fma_rn(r, w_s[l0 + u][c], acc[e][c]);
+      }
     }
   }
 #pragma unroll

@@ -1,0 +1,158 @@
+"""GPU parity for Cholesky, triangular solves, matvec and the SPD solver.
+
+Bit-identical to the oracle: cholesky (any internal block size),
+cholesky_blocked (same nb), forward_solve, matvec, cond_estimate.
+Within the normwise bound: backward_solve / solve_cholesky (summation order
+differs) and hence solve_spd's refined x; its strategy and kappa must match.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from quadprec_b200.workloads import shifted_hilbert, dense_dd
+
+pytestmark = pytest.mark.gpu
+
+
+def spd_dd(n, seed, shift=None):
+    """Symmetric positive definite f128 matrix: B B^T / n + shift I."""
+    b = dense_dd(n, n, seed=seed)
+    bh = b[..., 0] + b[..., 1]
+    a = bh @ bh.T / n + (shift if shift is not None else 1.0) * np.eye(n)
+    out = np.zeros((n, n, 2))
+    out[..., 0] = a
+    out[..., 1] = dense_dd(n, n, seed=seed + 1)[..., 1] * 1e-3
+    out[..., 1] = (out[..., 1] + out[..., 1].transpose()) * 0.5 * np.abs(a) * 2.0 ** -50
+    return out
+
+
+def lower(x):
+    n = x.shape[0]
+    return x * np.tril(np.ones((n, n)))[..., None]
+
+
+def nwerr(x, ref):
+    d = (x[..., 0] - ref[..., 0]) + (x[..., 1] - ref[..., 1])
+    return np.linalg.norm(d) / max(np.linalg.norm(ref[..., 0]), 1e-300)
+
+
+@pytest.mark.parametrize("n", [1, 2, 3, 17, 64, 65, 130, 257])
+def test_cholesky_bitexact(gpu, n):
+    a = spd_dd(n, seed=n)
+    L = gpu.f128_cholesky(a, n)
+    ref = O.cholesky(a, n)
+    assert np.array_equal(lower(L), lower(ref))
+    # strict upper triangle untouched
+    iu = np.triu_indices(n, 1)
+    assert np.array_equal(L[iu], a[iu])
+
+
+def test_cholesky_reference_kats(gpu):
+    f = lambda v: np.stack([np.asarray(v, float), np.zeros(len(v))], -1)
+    L = gpu.f128_cholesky(f([4, 2, 0, 2, 5, 1, 0, 1, 6]).reshape(3, 3, 2), 3)  # linalg.rs:377
+    assert np.array_equal(lower(L), lower(O.cholesky(f([4, 2, 0, 2, 5, 1, 0, 1, 6]).reshape(3, 3, 2), 3)))
+    n = 200  # linalg.rs:406-418
+    i = np.arange(n, dtype=np.float64)
+    a = f((1.0 / (np.abs(i[:, None] - i[None, :]) + 1.0)).ravel()).reshape(n, n, 2)
+    for d in range(n):
+        a[d, d] = O.dd_add(a[d, d], O.dd(2.0))
+    assert np.array_equal(lower(gpu.f128_cholesky(a, n)), lower(O.cholesky(a, n)))
+
+
+@pytest.mark.parametrize("n,nb", [(20, 8), (130, 64), (100, 7), (257, 32), (64, 64)])
+def test_cholesky_blocked_bitexact(gpu, n, nb):
+    a = spd_dd(n, seed=3 * n + nb)
+    L = gpu.f128_cholesky_blocked(a, n, nb)
+    ref = O.cholesky_blocked(a, n, nb)
+    assert np.array_equal(lower(L), lower(ref))
+
+
+def test_cholesky_not_spd(gpu):
+    n = 70
+    a = spd_dd(n, seed=5)
+    a[40, 40] = [-1.0, 0.0]
+    with pytest.raises(gpu.CholeskyError) as ei:
+        gpu.f128_cholesky(a, n)
+    with pytest.raises(O.CholeskyError) as eo:
+        O.cholesky(a, n)
+    assert ei.value.pivot == eo.value.pivot == 40
+    assert ei.value.value == eo.value.value
+    with pytest.raises(gpu.CholeskyError) as eb:
+        gpu.f128_cholesky_blocked(a, n, 16)
+    assert eb.value.pivot == 40
+
+
+@pytest.mark.parametrize("n", [1, 5, 64, 300, 1100])
+def test_solves_and_matvec(gpu, n):
+    a = spd_dd(n, seed=11 + n)
+    L = O.cholesky(a, n)
+    b = dense_dd(n, 1, seed=7)[:, 0]
+    assert np.array_equal(gpu.f128_forward_solve(L, b, n), O.forward_solve(L, b, n))
+    assert np.array_equal(gpu.f128_matvec(a, b, n), O.matvec(a, b, n))
+    tol = 4 * n * 2.0 ** -104 * 1e3
+    assert nwerr(gpu.f128_backward_solve(L, b, n), O.backward_solve(L, b, n)) <= tol
+    assert nwerr(gpu.f128_solve_cholesky(L, b, n), O.solve_cholesky(L, b, n)) <= tol
+    assert gpu.f128_cond_estimate(L, n) == O.cond_estimate(L, n)
+
+
+def test_solve_roundtrip_readme_matrix(gpu):  # linalg.rs:544-563 at n=4 and the n=512 workload
+    for n in (4, 512):
+        a, b = shifted_hilbert(n)
+        L = gpu.f128_cholesky(a, n)
+        assert np.array_equal(lower(L), lower(O.cholesky(a, n)))
+        x = gpu.f128_solve_cholesky(L, b, n)
+        ax = O.matvec(a, x, n)
+        r = (ax[:, 0] - b[:, 0]) + (ax[:, 1] - b[:, 1])
+        assert np.max(np.abs(r)) < 1e-28
+
+
+def hilbert(n):
+    i = np.arange(n, dtype=np.float64)
+    return 1.0 / (i[:, None] + i[None, :] + 1.0)
+
+
+@pytest.mark.parametrize("case", ["well", "hilbert12", "hilbert13", "shifted200"])
+def test_solve_spd_matches_reference(gpu, case):  # solver/src/lib.rs:271-340
+    if case == "well":
+        n = 10
+        a = hilbert(n) + np.eye(n)
+        b = np.ones(n)
+    elif case == "hilbert12":
+        n = 12
+        a = hilbert(n)
+        b = a.sum(axis=1)
+    elif case == "hilbert13":
+        n = 13
+        a = hilbert(n)
+        b = np.ones(n)
+    else:
+        n = 200
+        a = hilbert(n) + 5.0 * np.eye(n)
+        b = a.sum(axis=1)
+    g = gpu.solve_spd(a, b, n)
+    r = O.solve_spd(a, b, n)
+    assert g["strategy"] == r["strategy"]
+    assert g["kappa"] == r["kappa"]
+    if case == "well":
+        assert g["residual_norm"] < 1e-12
+    if case == "hilbert12":
+        assert g["residual_norm"] < 1e-25
+    # x differs from the oracle's only through summation order in the
+    # backward solves (f64 and f128); both are within kappa * n * u of x*.
+    xe = nwerr(g["x"], r["x"])
+    assert xe <= max(np.linalg.cond(a), 1.0) * n * 2.0 ** -100
+
+
+def test_solve_spd_f128_hilbert12(gpu):  # solver/src/lib.rs:319-340
+    n = 12
+    a = np.zeros((n, n, 2))
+    a[..., 0] = hilbert(n)
+    b = np.zeros((n, 2))
+    for i in range(n):
+        for j in range(n):
+            b[i] = O.dd_add(b[i], O.dd_mul(a[i, j], O.dd(1.0)))
+    g = gpu.solve_spd_f128(a, b, n)
+    r = O.solve_spd_f128(a, b, n)
+    err = np.sqrt(np.sum(((g["x"][:, 0] - 1.0) + g["x"][:, 1]) ** 2))
+    assert err < 1e-15 and g["strategy"] == "Float128" and g["kappa"] == r["kappa"]
+    assert abs(g["residual_norm"]) < 1e-30
