@@ -157,6 +157,58 @@ int hp_solve_spd(const double* a_f64, const double* b_f64, size_t n, double* x, 
 int hp_solve_spd_f128(const double* a, const double* b, size_t n, double* x, double* x_f64,
                       hp_solution_t* sol, int64_t* pivot);
 
+/* ------------------------------------------------------------------------
+ * SPD solve to 1e-25 for ill-conditioned f128 matrices (kappa up to ~1e28)
+ * extends: crates/solver/src/lib.rs:75-125 iterative_refinement. Same
+ * scheme (f128 Cholesky factor, refine x += L^-T L^-1 (b - S x)), with the
+ * residual evaluated to ~2^-159 instead of f128, so the attainable error is
+ * kappa * 2^-159 rather than kappa * 2^-104 (the reference solver stalls at
+ * ~1e-14 for kappa ~ 1e18).
+ *   HP_MODE_PLAIN: the reference's f128 cholesky (bit-identical) + residual
+ *                  in MultiFloat<4> arithmetic (mf_gemv semantics).
+ *   HP_MODE_OZAKI: Cholesky whose trailing matrix lives in the int8 residue
+ *                  domain (exact Schur updates on tcgen05), residual by
+ *                  error-free products with a 3-level TwoSum cascade.
+ * S: n x n f128 (symmetric, SPD; lower triangle and diagonal are read);
+ * b, x: n f128. Stops when max|dx| <= tol * max|x| or after max_iter steps.
+ * ---------------------------------------------------------------------- */
+typedef struct {
+  int32_t iterations;      /* refinement steps taken */
+  int32_t converged;       /* 1 if the tol criterion was met */
+  double last_correction;  /* max|dx| / max|x| of the last step */
+  double factor_ms;        /* device time of the factorisation */
+  double total_ms;         /* device time of factor + solves + refinement */
+} hp_refine_info_t;
+int hp_spd_solve_refined(const double* S, const double* b, size_t n, int mode, double tol,
+                         int max_iter, double* x, hp_refine_info_t* info, int64_t* pivot);
+int hp_spd_solve_refined_dev(const double* S, const double* b, size_t n, int mode, double tol,
+                             int max_iter, double* x, hp_refine_info_t* info, int64_t* pivot,
+                             void* stream);
+
+/* ------------------------------------------------------------------------
+ * Gaussian overlap assembly (crates/overlap)
+ * ---------------------------------------------------------------------- */
+/* replaces: pub fn assemble_overlap_mixed(basis: &BasisSet, params: &ScreenParams)
+ *           -> OverlapResult      crates/overlap/src/assemble.rs:35-85
+ * for bases of s shells (ShellKind::S, basis.rs:10-12). Shell s has centre
+ * centers[3s..3s+2] and primitives prim_off[s] .. prim_off[s+1]-1 of
+ * (alpha, coeff) (Primitive, basis.rs:2-6). params = {diffuse_threshold,
+ * ratio_threshold, eps_skip, safe_distance} (ScreenParams, screen.rs:16-45).
+ * matrix: n_shells x n_shells f64 (OverlapResult.matrix); tier_counts =
+ * {f64_pairs, f128_pairs, skipped_pairs} (TierCounts, assemble.rs:16-21). */
+int hp_assemble_overlap_s(size_t n_shells, const double* centers, const int64_t* prim_off,
+                          const double* alpha, const double* coeff, const double* params,
+                          double* matrix, int64_t* tier_counts);
+/* f128 overlap matrix of normalised s Gaussians (one primitive per basis
+ * function): S_ij = (4 a b/(a+b)^2)^{3/4} exp(-a b/(a+b) |R_i - R_j|^2),
+ * evaluated with the reference's f128 operations (dd.rs:61-121) so it is
+ * bit-identical to the CPU evaluation; exponents below -700 give 0. This is
+ * the problem matrix of the overlap SPD workloads (the reference's own
+ * assembly stores f64, assemble.rs:57-58). s_out: n x n f128. */
+int hp_overlap_norm_dd(size_t n, const double* centers, const double* alpha, double* s_out);
+int hp_overlap_norm_dd_dev(size_t n, const double* centers, const double* alpha, double* s_out,
+                           void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -68,6 +68,13 @@ SIGNATURES = {
     "hp_f128_cond_estimate": ([_vp, _sz, _d], ctypes.c_int),
     "hp_solve_spd": ([_vp, _vp, _sz, _vp, _vp, _vp, _i64p], ctypes.c_int),
     "hp_solve_spd_f128": ([_vp, _vp, _sz, _vp, _vp, _vp, _i64p], ctypes.c_int),
+    "hp_spd_solve_refined": ([_vp, _vp, _sz, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp, _vp, _i64p],
+                             ctypes.c_int),
+    "hp_spd_solve_refined_dev": ([_vp, _vp, _sz, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp, _vp, _i64p,
+                                  _vp], ctypes.c_int),
+    "hp_assemble_overlap_s": ([_sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp], ctypes.c_int),
+    "hp_overlap_norm_dd": ([_sz, _vp, _vp, _vp], ctypes.c_int),
+    "hp_overlap_norm_dd_dev": ([_sz, _vp, _vp, _vp, _vp], ctypes.c_int),
 }
 
 
@@ -78,6 +85,12 @@ class Solution(ctypes.Structure):
 
 
 STRATEGIES = ("Float64", "MixedPrecision", "Float128")
+
+
+class RefineInfo(ctypes.Structure):
+    _fields_ = [("iterations", ctypes.c_int32), ("converged", ctypes.c_int32),
+                ("last_correction", ctypes.c_double), ("factor_ms", ctypes.c_double),
+                ("total_ms", ctypes.c_double)]
 
 
 def lib():
@@ -227,3 +240,49 @@ def solve_spd(a_f64, b_f64, n):
 def solve_spd_f128(a, b, n):
     """crates/solver/src/lib.rs:71 solve_spd_f128."""
     return _spd(lib().hp_solve_spd_f128, a, b, n)
+
+
+# ---------------- overlap ----------------
+DEFAULT_SCREEN = (0.1, 500.0, 1e-14, 12.0)  # crates/overlap/src/screen.rs:36-45
+
+
+def assemble_overlap_s(centers, prim_alpha, prim_coeff, params=DEFAULT_SCREEN):
+    """assemble.rs:35 assemble_overlap_mixed for a basis of s shells."""
+    n = len(centers)
+    off = np.zeros(n + 1, dtype=np.int64)
+    for i, al in enumerate(prim_alpha):
+        off[i + 1] = off[i] + len(al)
+    al = _c(np.concatenate([np.asarray(x, dtype=np.float64) for x in prim_alpha]))
+    co = _c(np.concatenate([np.asarray(x, dtype=np.float64) for x in prim_coeff]))
+    mat = np.zeros((n, n))
+    tc = np.zeros(3, dtype=np.int64)
+    pr = _c(params)
+    check(lib().hp_assemble_overlap_s(n, _ptr(_c(centers)), off.ctypes.data, _ptr(al), _ptr(co), _ptr(pr),
+                                      _ptr(mat), tc.ctypes.data))
+    return mat, {"f64_pairs": int(tc[0]), "f128_pairs": int(tc[1]), "skipped_pairs": int(tc[2])}
+
+
+def overlap_norm_dd(centers, alpha) -> np.ndarray:
+    """f128 overlap matrix of normalised s Gaussians (n x n x 2)."""
+    centers, alpha = _c(centers), _c(alpha)
+    n = len(alpha)
+    s = np.empty((n, n, 2))
+    check(lib().hp_overlap_norm_dd(n, _ptr(centers), _ptr(alpha), _ptr(s)))
+    return s
+
+
+def spd_solve_refined(S, b, n, mode=OZAKI, tol=1e-28, max_iter=10):
+    """Refined SPD solve to 1e-25 (see hp_spd_solve_refined). b may be f64 (n,) or f128 (n,2)."""
+    S = _c(S)
+    b = _c(b)
+    if b.ndim == 1:
+        b = np.stack([b, np.zeros_like(b)], -1)
+    x = np.empty((n, 2))
+    info = RefineInfo()
+    pv = ctypes.c_int64(-1)
+    rc = lib().hp_spd_solve_refined(_ptr(S), _ptr(b), n, mode, tol, max_iter, _ptr(x), ctypes.byref(info),
+                                    ctypes.byref(pv))
+    if rc == HP_ERR_NOT_SPD:
+        raise HPError(rc, f"Matrix is not positive definite (failed at pivot {pv.value})")
+    check(rc)
+    return x, {f: getattr(info, f) for f, _ in RefineInfo._fields_}

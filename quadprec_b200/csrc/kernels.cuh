@@ -38,3 +38,27 @@ int cond_estimate(const double* L, size_t n, bool is_dd, double* out_dev, cudaSt
 // op: 0 out=a-b, 1 out=a+b, 2 out=promote(f), 3 out(f64)=to_f64(a)
 int dd_vec(int op, const double* a, const double* b, double* out, const double* f, size_t n, cudaStream_t s);
 }  // namespace hp
+
+namespace hp {
+// overlap.cu
+int overlap_norm_dd(size_t n, const double* centers, const double* alpha, double* S, cudaStream_t s);
+}  // namespace hp
+
+namespace hp {
+// ozaki.cu: int8 residue GEMM core. cres[l][c_row0 + i][c_col0 + j] is set /
+// incremented / decremented (acc_mode 0 / 1 / 2) by (A_l B_l^T)_ij mod m_l
+// for i < Mp, j < Np (tile extents, multiples of 128 / 256). ares / bres hold
+// ra_rows / rb_rows rows of Kp bytes per modulus.
+int ozaki_residue_gemm(const int8_t* ares, const int8_t* bres, uint8_t* cres, int L, size_t Mp, size_t Np,
+                       size_t Kp, cudaStream_t s);
+int ozaki_residue_gemm_ex(const int8_t* ares, const int8_t* bres, uint8_t* cres, int L, size_t Mp, size_t Np,
+                          size_t Kp, size_t ldc, size_t plane, size_t c_row0, size_t c_col0, int acc_mode,
+                          cudaStream_t s, size_t ra_rows, size_t rb_rows);
+int ozaki_moduli_for(size_t k, int beta);
+// refine.cu
+int dd_residual(const double* S, const double* x, const double* b, double* r, size_t n, bool accurate_qd,
+                cudaStream_t s);
+int dd_maxabs(const double* v, size_t n, double* out_dev, cudaStream_t s);
+// ozaki.cu: Cholesky with the trailing matrix kept in the residue domain.
+int rns_cholesky(const double* S, double* L, size_t n, int64_t* pivot, cudaStream_t s);
+}  // namespace hp

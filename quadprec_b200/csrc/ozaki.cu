@@ -38,6 +38,7 @@ namespace ozaki {
 
 constexpr int MAXL = 49;        // number of pairwise-coprime moduli <= 256 in the table
 constexpr int NDIG = 5;         // base-2^22 digits of a scaled integer (110 bits)
+constexpr int NDIG2 = 10;       // digits of the 220-bit integers of the residue-domain Cholesky
 constexpr int CRT_BITS = 39;    // chunk width of the CRT accumulators
 constexpr int NCMAX = 10;       // chunks needed for M < 2^342
 constexpr int BETA_DD = 106;    // bits kept per f128 operand entry
@@ -47,7 +48,7 @@ struct ModTable {
   int mod[MAXL];
   uint32_t magic[MAXL];   // floor(2^32 / m)
   uint32_t offset[MAXL];  // m * ceil(2^31 / m): makes |x| <= 2^30 + 2^27 non-negative
-  int pw[MAXL][NDIG];     // 2^(22 c) mod m, balanced into [-m/2, m/2]
+  int pw[MAXL][NDIG2];    // 2^(22 c) mod m, balanced into [-m/2, m/2]
 };
 __constant__ ModTable c_tab;
 
@@ -138,7 +139,7 @@ static const HostTables& host_tables() {
       T.mt.mod[l] = m;
       T.mt.magic[l] = (uint32_t)((1ull << 32) / (uint64_t)m);
       T.mt.offset[l] = (uint32_t)((((1ull << 31) + m - 1) / m) * m);
-      for (int c = 0; c < NDIG; c++) {
+      for (int c = 0; c < NDIG2; c++) {
         // 2^(22c) mod m, balanced
         uint64_t r = 1;
         for (int t = 0; t < 22 * c; t++) r = (r * 2) % m;
@@ -386,8 +387,8 @@ constexpr int MAX_K_CHUNK = 65536;  // |int32 accumulator| <= 2^16 * 2^14 = 2^30
 
 __global__ void __launch_bounds__(256, 1)
     i8_gemm_mod_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int L,
-                       int tiles_m, int tiles_n, int kb0, int kb1, int accumulate, uint8_t* __restrict__ cres,
-                       int64_t Np, int64_t plane, uint32_t* status) {
+                       int tiles_m, int tiles_n, int kb0, int kb1, int acc_mode, uint8_t* __restrict__ cres,
+                       int64_t ldc, int64_t plane, int64_t c_row0, int64_t c_col0, uint32_t* status) {
   using namespace sm100;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
@@ -509,8 +510,8 @@ __global__ void __launch_bounds__(256, 1)
       if (!__all_sync(0xffffffffu, ok)) break;
       tc_fence_after();
       const uint32_t m = (uint32_t)c_tab.mod[l];
-      const int64_t row = (int64_t)tm * GB_M + ew * 32 + lane;
-      uint8_t* dst = cres + (size_t)l * plane + (size_t)row * Np + (size_t)tn * GB_N;
+      const int64_t row = c_row0 + (int64_t)tm * GB_M + ew * 32 + lane;
+      uint8_t* dst = cres + (size_t)l * plane + (size_t)row * ldc + (size_t)(c_col0 + (int64_t)tn * GB_N);
 #pragma unroll 1
       for (int ch = 0; ch < GB_N / 32; ch++) {
         uint32_t v[32];
@@ -518,7 +519,7 @@ __global__ void __launch_bounds__(256, 1)
         tmem_wait_ld();
         uint32_t packed[8];
         uint4 prev0 = make_uint4(0, 0, 0, 0), prev1 = make_uint4(0, 0, 0, 0);
-        if (accumulate) {
+        if (acc_mode) {
           prev0 = *reinterpret_cast<const uint4*>(dst + ch * 32);
           prev1 = *reinterpret_cast<const uint4*>(dst + ch * 32 + 16);
         }
@@ -529,9 +530,12 @@ __global__ void __launch_bounds__(256, 1)
 #pragma unroll
           for (int b = 0; b < 4; b++) {
             uint32_t r = mod_reduce((int32_t)v[4 * w + b], l);
-            if (accumulate) {
+            if (acc_mode == 1) {  // C = (C + AB) mod m
               r += (pv[w] >> (8 * b)) & 0xFFu;
               if (r >= m) r -= m;
+            } else if (acc_mode == 2) {  // C = (C - AB) mod m
+              const uint32_t old = (pv[w] >> (8 * b)) & 0xFFu;
+              r = old >= r ? old - r : old + m - r;
             }
             word |= r << (8 * b);
           }
@@ -733,6 +737,12 @@ int ozaki_moduli_for(size_t k, int beta) {
 // planes of op(A) (L x Mp x Kp) and B (L x Np x Kp), writes cres (L x Mp x Np).
 int ozaki_residue_gemm(const int8_t* ares, const int8_t* bres, uint8_t* cres, int L, size_t Mp, size_t Np,
                        size_t Kp, cudaStream_t s) {
+  return ozaki_residue_gemm_ex(ares, bres, cres, L, Mp, Np, Kp, Np, Mp * Np, 0, 0, 0, s, Mp, Np);
+}
+
+int ozaki_residue_gemm_ex(const int8_t* ares, const int8_t* bres, uint8_t* cres, int L, size_t Mp, size_t Np,
+                          size_t Kp, size_t ldc, size_t plane, size_t c_row0, size_t c_col0, int acc_mode,
+                          cudaStream_t s, size_t ra_rows, size_t rb_rows) {
   using namespace ozaki;
   DevTables* D;
   HP_TRY(device_tables(&D));
@@ -744,8 +754,8 @@ int ozaki_residue_gemm(const int8_t* ares, const int8_t* bres, uint8_t* cres, in
     attr_set[dev] = true;
   }
   CUtensorMap mapA, mapB;
-  HP_TRY(make_map(&mapA, ares, Kp, Mp, L, GB_M));
-  HP_TRY(make_map(&mapB, bres, Kp, Np, L, GB_N));
+  HP_TRY(make_map(&mapA, ares, Kp, ra_rows ? ra_rows : Mp, L, GB_M));
+  HP_TRY(make_map(&mapB, bres, Kp, rb_rows ? rb_rows : Np, L, GB_N));
   uint32_t* status = device_status(s);
   if (!status) {
     set_error("status word allocation failed");
@@ -758,8 +768,10 @@ int ozaki_residue_gemm(const int8_t* ares, const int8_t* bres, uint8_t* cres, in
   const int kb_chunk = MAX_K_CHUNK / GB_K;
   for (int kb0 = 0; kb0 < nkb_total; kb0 += kb_chunk) {
     int kb1 = std::min(nkb_total, kb0 + kb_chunk);
-    i8_gemm_mod_kernel<<<grid, 256, GEMM_SMEM, s>>>(mapA, mapB, L, tiles_m, tiles_n, kb0, kb1, kb0 > 0 ? 1 : 0,
-                                                     cres, (int64_t)Np, (int64_t)(Mp * Np), status);
+    const int mode = kb0 > 0 ? (acc_mode == 2 ? 2 : 1) : acc_mode;
+    i8_gemm_mod_kernel<<<grid, 256, GEMM_SMEM, s>>>(mapA, mapB, L, tiles_m, tiles_n, kb0, kb1, mode, cres,
+                                                     (int64_t)ldc, (int64_t)plane, (int64_t)c_row0,
+                                                     (int64_t)c_col0, status);
     HP_LAUNCH_CHECK();
   }
   return HP_OK;
@@ -839,6 +851,333 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
 int ozaki_qd_gemm(const double*, const double*, double*, size_t, size_t, size_t, bool, cudaStream_t) {
   set_error("f256 Ozaki GEMM is not built yet");
   return HP_ERR_UNSUPPORTED;
+}
+
+
+// ===========================================================================
+// Cholesky with the trailing matrix kept in the residue domain.
+//
+// With D = diag(2^e_i) chosen so that (D S D)_ii lies in [2^(2B-2), 2^(2B)),
+// B = 106, the scaled matrix A~ = round(D S D) is an integer matrix whose
+// Schur complements stay below 2^(2B) in magnitude (for an SPD matrix
+// |a_ij| <= sqrt(a_ii a_jj) and the diagonal only decreases). A~ is held as
+// residues modulo L = 29 moduli (M > 2^(2B+3)). Per block column of width
+// nb = 64:
+//   1. CRT the panel (rows kb.., columns kb..kb+nb) back to f128 integers;
+//   2. factor the nb x nb diagonal block in f128 (one CTA) and invert it;
+//   3. L21 = A21 L11^-T in f128 and round L21 to integers (|L21| < 2^B);
+//   4. subtract L21 L21^T from the trailing residues with the int8 tcgen05
+//      GEMM (exact modular arithmetic: no rounding at all in the update).
+// The factor returned is L = D^-1 L~, in f128. Errors: the f128 rounding of
+// the panel values (2^-104 relative) and the rounding of L21 to B-bit
+// integers, i.e. an f128-quality factor whose O(n^3) work ran on the tensor
+// cores.
+// ===========================================================================
+namespace ozaki {
+
+constexpr int BETA_CH = 106;
+constexpr int CH_NB = 64;
+
+struct RnsErr {
+  int flag;
+  int pad;
+  long long pivot;
+};
+
+__global__ void rns_scale_kernel(const dd* __restrict__ S, int64_t n, int beta, int* __restrict__ e,
+                                 RnsErr* err) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double d = S[i * n + i].hi;
+  if (!(d > 0.0) || !isfinite(d)) {
+    err->flag = 1;
+    atomicMin(&err->pivot, (long long)i);
+    e[i] = 0;
+    return;
+  }
+  const int E = exp_field(d) - 1022;  // d = m 2^E, m in [0.5, 1)
+  e[i] = (2 * beta - E) >> 1;         // floor((2B - E) / 2)
+}
+
+// Balanced base-2^22 digits of rint(v), |v| < 2^214 (exact).
+__device__ __forceinline__ void int_digits10(double v, int32_t* d) {
+  double a = fabs(rint(v));
+  int32_t s = signbit(v) ? -1 : 1;
+#pragma unroll
+  for (int c = NDIG2 - 1; c >= 1; c--) {
+    const double sc = scale_pow2(1.0, -22 * c), up = scale_pow2(1.0, 22 * c);
+    double t = floor(__dmul_rn(a, sc));
+    a = __dsub_rn(a, __dmul_rn(t, up));
+    d[c] = s * (int32_t)t;
+  }
+  d[0] = s * (int32_t)a;
+}
+
+// Res[l][i][j] = round((D S D)_ij) mod m_l (unbalanced bytes) for i, j < Rp;
+// zero outside n x n. Block tile 64 rows x 32 columns, 8 columns per thread.
+__global__ void __launch_bounds__(256) rns_init_kernel(const dd* __restrict__ S, int64_t n, const int* __restrict__ e,
+                                                       int L, int64_t Rp, uint8_t* __restrict__ res) {
+  const int t = threadIdx.x;
+  const int64_t i = (int64_t)blockIdx.y * 64 + t / 4;
+  const int64_t j0 = (int64_t)blockIdx.x * 32 + 8 * (t % 4);
+  int32_t dig[8][NDIG2];
+#pragma unroll
+  for (int q = 0; q < 8; q++)
+#pragma unroll
+    for (int c = 0; c < NDIG2; c++) dig[q][c] = 0;
+  if (i < n) {
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      const int64_t j = j0 + q;
+      if (j < n) {
+        const dd v = S[i * n + j];
+        const int sft = e[i] + e[j];
+        int32_t dh[NDIG2], dl[NDIG2];
+        int_digits10(scale_pow2(v.hi, sft), dh);
+        int_digits10(scale_pow2(v.lo, sft), dl);
+#pragma unroll
+        for (int c = 0; c < NDIG2; c++) dig[q][c] = dh[c] + dl[c];
+#pragma unroll
+        for (int c = 0; c < NDIG2 - 1; c++) {
+          int32_t carry = (dig[q][c] + (1 << 21)) >> 22;
+          dig[q][c] -= carry << 22;
+          dig[q][c + 1] += carry;
+        }
+      }
+    }
+  }
+  for (int l = 0; l < L; l++) {
+    const uint32_t m = (uint32_t)c_tab.mod[l];
+    uint32_t w0 = 0, w1 = 0;
+#pragma unroll
+    for (int q = 0; q < 8; q++) {
+      int32_t x1 = 0, x2 = 0;
+#pragma unroll
+      for (int c = 0; c < 5; c++) x1 += dig[q][c] * c_tab.pw[l][c];
+#pragma unroll
+      for (int c = 5; c < NDIG2; c++) x2 += dig[q][c] * c_tab.pw[l][c];
+      uint32_t r = mod_reduce(x1, l) + mod_reduce(x2, l);
+      if (r >= m) r -= m;
+      if (q < 4)
+        w0 |= r << (8 * q);
+      else
+        w1 |= r << (8 * (q - 4));
+    }
+    *reinterpret_cast<uint2*>(res + (size_t)l * Rp * Rp + (size_t)i * Rp + j0) = make_uint2(w0, w1);
+  }
+}
+
+// P[r][c] = CRT(Res[.][r0 + r][c0 + c]) as an f128 integer, r < R, c < C.
+template <int NC>
+__global__ void __launch_bounds__(256) crt_block_kernel(const uint8_t* __restrict__ res, int64_t ld, int64_t plane,
+                                                        int64_t r0, int64_t c0, int64_t R, int64_t C,
+                                                        const CrtTable* __restrict__ tab, dd* __restrict__ P) {
+  __shared__ double w_s[MAXL][NC];
+  __shared__ double mch_s[NC];
+  const int L = tab->L;
+  for (int i = threadIdx.x; i < L * NC; i += blockDim.x) w_s[i / NC][i % NC] = tab->w[i / NC][i % NC];
+  if (threadIdx.x < NC) mch_s[threadIdx.x] = tab->mchunk[threadIdx.x];
+  __syncthreads();
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= R * C) return;
+  const int64_t r = idx / C, c = idx % C;
+  const uint8_t* rp = res + (size_t)(r0 + r) * ld + c0 + c;
+  double acc[NC + 1];
+#pragma unroll
+  for (int q = 0; q <= NC; q++) acc[q] = 0.0;
+  for (int l0 = 0; l0 < L; l0 += 8) {
+    uint32_t v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) v[u] = (l0 + u < L) ? (uint32_t)__ldg(rp + (size_t)(l0 + u) * plane) : 0u;
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      if (l0 + u >= L) break;
+      const double x = byte_to_double(v[u]);
+#pragma unroll
+      for (int q = 0; q < NC; q++) acc[q] = __fma_rn(x, w_s[l0 + u][q], acc[q]);
+    }
+  }
+  bool neg;
+  dd s = crt_finish<NC>(acc, mch_s, tab->inv_m, &neg);
+  P[idx] = neg ? dd_neg(s) : s;
+}
+
+// 1/sqrt(d) to ~2^-104: one Newton step in f128 from the f64 seed.
+__device__ __forceinline__ dd dd_rsqrt(dd d) {
+  const double x0 = __ddiv_rn(1.0, __dsqrt_rn(d.hi));
+  const dd x = dd_from(x0);
+  const dd e = dd_sub(dd_from(1.0), dd_mul(d, dd_mul(x, x)));
+  return dd_add(x, dd_mul(x, dd_mul(e, dd_from(0.5))));
+}
+
+// Factor the jb x jb block P[0..jb)[0..jb) (row stride jb, symmetric values)
+// in f128, write L~11 scaled back to Lout, and X^T = (L~11^-1)^T to XT.
+__global__ void __launch_bounds__(256) chol_inv_block_kernel(const dd* __restrict__ P, int jb, int64_t kb, int64_t n,
+                                                             const int* __restrict__ e, dd* __restrict__ Lout,
+                                                             dd* __restrict__ XT, RnsErr* err) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  dd* A = reinterpret_cast<dd*>(sm_raw);  // [64][65]
+  dd* X = A + 64 * 65;                    // [64][65]
+  __shared__ dd rinv[64];
+  __shared__ int fail;
+  const int t = threadIdx.x;
+  if (err->flag) return;
+  if (t == 0) fail = 0;
+  for (int q = t; q < jb * jb; q += 256) {
+    const int r = q / jb, c = q % jb;
+    A[r * 65 + c] = P[q];
+    X[r * 65 + c] = dd_from(r == c ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  for (int j = 0; j < jb; j++) {
+    if (t == 0) {
+      const dd d = A[j * 65 + j];
+      if (!(d.hi > 0.0)) {
+        fail = 1;
+        err->flag = 1;
+        err->pivot = kb + j;
+      } else {
+        const dd r = dd_rsqrt(d);
+        A[j * 65 + j] = dd_mul(d, r);
+        rinv[j] = r;
+      }
+    }
+    __syncthreads();
+    if (fail) return;
+    for (int i = j + 1 + t; i < jb; i += 256) A[i * 65 + j] = dd_mul(A[i * 65 + j], rinv[j]);
+    __syncthreads();
+    const int m = jb - j - 1;  // trailing (i, k), j < k <= i < jb
+    for (int q = t; q < m * m; q += 256) {
+      const int i = j + 1 + q / m, k = j + 1 + q % m;
+      if (k <= i) A[i * 65 + k] = dd_sub(A[i * 65 + k], dd_mul(A[i * 65 + j], A[k * 65 + j]));
+    }
+    __syncthreads();
+  }
+  // X = L~^-1 by row-oriented forward substitution on all columns at once
+  for (int k = 0; k < jb; k++) {
+    for (int c = t; c <= k; c += 256) X[k * 65 + c] = dd_mul(X[k * 65 + c], rinv[k]);
+    __syncthreads();
+    const int rows = jb - k - 1;
+    for (int q = t; q < rows * (k + 1); q += 256) {
+      const int i = k + 1 + q / (k + 1), c = q % (k + 1);
+      X[i * 65 + c] = dd_sub(X[i * 65 + c], dd_mul(A[i * 65 + k], X[k * 65 + c]));
+    }
+    __syncthreads();
+  }
+  for (int q = t; q < jb * jb; q += 256) {
+    const int r = q / jb, c = q % jb;
+    if (c <= r) {
+      const dd v = A[r * 65 + c];
+      const int sh = -e[kb + r];
+      Lout[(kb + r) * n + kb + c] = dd_renorm(scale_pow2(v.hi, sh), scale_pow2(v.lo, sh));
+    }
+    XT[c * jb + r] = (c <= r) ? X[r * 65 + c] : dd{0.0, 0.0};  // XT[k][j] = X[j][k]
+  }
+}
+
+// Round L21 to integers (rint of each limb, as the residue kernel does) and
+// store D^-1 L21 into Lout[t0 + r][kb + c].
+__global__ void round_store_kernel(const dd* __restrict__ Q, int64_t m, int jb, int64_t t0, int64_t kb, int64_t n,
+                                   const int* __restrict__ e, dd* __restrict__ Lout) {
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= m * jb) return;
+  const int64_t r = idx / jb, c = idx % jb;
+  const dd v = Q[idx];
+  const dd x = dd_renorm(rint(v.hi), rint(v.lo));
+  const int sh = -e[t0 + r];
+  Lout[(t0 + r) * n + kb + c] = dd_renorm(scale_pow2(x.hi, sh), scale_pow2(x.lo, sh));
+}
+
+__global__ void fill_int_kernel(int* p, int64_t n, int v) {
+  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) p[i] = v;
+}
+
+}  // namespace ozaki
+
+int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStream_t s) {
+  using namespace ozaki;
+  if (n == 0) return HP_OK;
+  DevTables* D;
+  HP_TRY(device_tables(&D));
+  const HostTables& T = host_tables();
+  int L = -1;
+  for (int q = 1; q <= MAXL; q++)
+    if (T.cum_log2[q] >= 2.0 * BETA_CH + 3.0) {
+      L = q;
+      break;
+    }
+  const int nc = T.crt[L].nc;
+  const dd* S = reinterpret_cast<const dd*>(S_);
+  dd* Lout = reinterpret_cast<dd*>(L_);
+  const size_t Rp = round_up(n, GB_N);   // rows of the L21 residue planes
+  const size_t Np = Rp + GB_N;           // trailing-matrix residue planes (room for tile overhang)
+  const size_t nb = CH_NB, Kp = GB_K;
+  DevBuf ebuf(n * sizeof(int), s), e1022(Rp * sizeof(int), s), res((size_t)L * Np * Np, s),
+      rl((size_t)L * Rp * Kp, s), P(n * nb * 16, s), Q(n * nb * 16, s), XT(nb * nb * 16, s), err(sizeof(RnsErr), s);
+  if (!ebuf.p || !e1022.p || !res.p || !rl.p || !P.p || !Q.p || !XT.p || !err.p) {
+    set_error("rns_cholesky: workspace allocation failed");
+    return HP_ERR_CUDA;
+  }
+  RnsErr h0{0, 0, (long long)0x7fffffffffffffffll};
+  HP_CUDA_TRY(cudaMemcpyAsync(err.p, &h0, sizeof(h0), cudaMemcpyHostToDevice, s));
+  HP_CUDA_TRY(cudaMemsetAsync(res.p, 0, (size_t)L * Np * Np, s));
+  HP_CUDA_TRY(cudaMemsetAsync(rl.p, 0, (size_t)L * Rp * Kp, s));
+  if ((const void*)S_ != (const void*)L_) HP_CUDA_TRY(cudaMemcpyAsync(L_, S_, n * n * 16, cudaMemcpyDeviceToDevice, s));
+  rns_scale_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(S, n, BETA_CH, ebuf.as<int>(), err.as<RnsErr>());
+  fill_int_kernel<<<(unsigned)((Rp + 255) / 256), 256, 0, s>>>(e1022.as<int>(), Rp, 1022);
+  HP_LAUNCH_CHECK();
+  {
+    dim3 g((unsigned)(Np / 32), (unsigned)(Np / 64));
+    rns_init_kernel<<<g, 256, 0, s>>>(S, n, ebuf.as<int>(), L, Np, res.as<uint8_t>());
+    HP_LAUNCH_CHECK();
+  }
+  const size_t inv_smem = 2 * 64 * 65 * 16;
+  HP_CUDA_TRY(cudaFuncSetAttribute(chol_inv_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
+  for (size_t kb = 0; kb < n; kb += nb) {
+    const int jb = (int)std::min(nb, n - kb);
+    const size_t R = n - kb;
+#define HP_CRTB(NC)                                                                                          \
+  case NC:                                                                                                   \
+    crt_block_kernel<NC><<<(unsigned)((R * jb + 255) / 256), 256, 0, s>>>(                                    \
+        res.as<uint8_t>(), (int64_t)Np, (int64_t)(Np * Np), (int64_t)kb, (int64_t)kb, (int64_t)R, (int64_t)jb, \
+        D->crt + L, P.as<dd>());                                                                             \
+    break;
+    switch (nc) {
+      HP_CRTB(5) HP_CRTB(6) HP_CRTB(7)
+      default:
+        set_error("rns_cholesky: unsupported chunk count %d", nc);
+        return HP_ERR_UNSUPPORTED;
+    }
+#undef HP_CRTB
+    HP_LAUNCH_CHECK();
+    chol_inv_block_kernel<<<1, 256, inv_smem, s>>>(P.as<dd>(), jb, (int64_t)kb, (int64_t)n, ebuf.as<int>(), Lout,
+                                                   XT.as<dd>(), err.as<RnsErr>());
+    HP_LAUNCH_CHECK();
+    if (R <= (size_t)jb) break;
+    const size_t m = R - jb, t0 = kb + jb;
+    HP_TRY(dd_gemm_plain(P.as<double>() + 2 * (size_t)jb * jb, XT.as<double>(), Q.as<double>(), m, jb, jb, false, s));
+    round_store_kernel<<<(unsigned)((m * jb + 255) / 256), 256, 0, s>>>(Q.as<dd>(), (int64_t)m, jb, (int64_t)t0,
+                                                                        (int64_t)kb, (int64_t)n, ebuf.as<int>(), Lout);
+    HP_LAUNCH_CHECK();
+    {
+      dim3 g((unsigned)(Kp / RT_P), (unsigned)(Rp / RT_R));
+      residue_kernel<true><<<g, 256, 0, s>>>(Q.as<double2>(), (int64_t)m, (int64_t)jb, e1022.as<int>(), 0, L,
+                                             (int64_t)Rp, (int64_t)Kp, rl.as<int8_t>());
+      HP_LAUNCH_CHECK();
+    }
+    HP_TRY(ozaki_residue_gemm_ex(rl.as<int8_t>(), rl.as<int8_t>(), res.as<uint8_t>(), L, round_up(m, GB_M),
+                                 round_up(m, GB_N), Kp, Np, Np * Np, t0, t0, 2, s, Rp, Rp));
+  }
+  RnsErr h;
+  HP_CUDA_TRY(cudaMemcpyAsync(&h, err.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  if (h.flag) {
+    if (pivot) *pivot = h.pivot;
+    set_error("Cholesky failed at pivot %lld", (long long)h.pivot);
+    return HP_ERR_NOT_SPD;
+  }
+  return HP_OK;
 }
 
 }  // namespace hp

@@ -79,3 +79,43 @@ def shifted_hilbert(n: int):
     b = np.zeros((n, 2))
     b[:, 0] = 1.0
     return a, b
+
+
+def normal(count: int, seed: int = 0, offset: int = 0) -> np.ndarray:
+    """Approximately N(0,1): Irwin-Hall sum of 12 SplitMix64 uniforms minus 6.
+
+    Only additions, so b is bit-reproducible on any host (a Box-Muller b would
+    inherit the host libm's last-ulp differences, which an extended-precision
+    solve amplifies far above the 1e-25 accuracy target).
+    """
+    u = uniform(12 * count, seed, offset).reshape(count, 12)
+    acc = np.zeros(count)
+    for t in range(12):
+        acc = acc + u[:, t]
+    return acc - 6.0
+
+
+def overlap_lattice(nx: int, ny: int, nz: int, spacing: float = 1.4, jitter: float = 0.05, n_exp: int = 4,
+                    lo: float = 0.01, hi: float = 10.0, seed: int = 0):
+    """s-Gaussian basis on a jittered cubic lattice (center-major order).
+
+    Centres are visited in row-major (ix, iy, iz) order; each takes 3 jitter
+    draws (coordinate + jitter*(2U-1)) then n_exp exponent draws,
+    log-uniform in [lo, hi]. Returns (centers (N,3), alpha (N,)) with one
+    entry per basis function, N = nx*ny*nz*n_exp.
+    """
+    nc = nx * ny * nz
+    per = 3 + n_exp
+    u = uniform(nc * per, seed, 0).reshape(nc, per)
+    grid = np.array([(ix, iy, iz) for ix in range(nx) for iy in range(ny) for iz in range(nz)], dtype=np.float64)
+    cen = grid * spacing + jitter * (2.0 * u[:, :3] - 1.0)
+    alpha = lo * (hi / lo) ** u[:, 3:]
+    return np.repeat(cen, n_exp, axis=0), alpha.reshape(-1)
+
+
+def overlap_spd_problem(nx: int, ny: int, nz: int, seed: int = 0):
+    """Overlap SPD workload: lattice basis and b ~ N(0,1) (n = nx*ny*nz*4)."""
+    cen, alpha = overlap_lattice(nx, ny, nz, seed=seed)
+    n = len(alpha)
+    b = normal(n, seed, offset=10 ** 9)
+    return cen, alpha, b
