@@ -174,6 +174,102 @@ def profile_case(args):
     return 0
 
 
+SPD_LATTICE = (5, 10, 10)  # 500 centres x 4 exponents = 2000 basis functions
+
+
+def spd_section(hp, torch, dev, stream, sptr, args, rank, world, dist):
+    """Overlap SPD solve to <= 1e-25: assemble S (f128, GPU) + factor + refine.
+
+    One step = one complete solve of the n = 2000 overlap system (assembly of
+    S from the basis on the device, Cholesky, refinement to max|dx| <= 1e-28
+    max|x|). Reported as solves/s for the chosen (residue-domain tcgen05
+    Cholesky) and plain (reference f128 Cholesky + f256 residuals) modes.
+    """
+    import ctypes
+
+    import numpy as np
+
+    from quadprec_b200.workloads import overlap_spd_problem
+
+    cen, alpha, b = overlap_spd_problem(*SPD_LATTICE, seed=0)
+    n = len(alpha)
+    dcen = torch.from_numpy(np.ascontiguousarray(cen)).to(dev)
+    dal = torch.from_numpy(alpha).to(dev)
+    b2 = np.stack([b, np.zeros_like(b)], -1)
+    db = torch.from_numpy(b2).to(dev)
+    dS = torch.empty((n, n, 2), dtype=torch.float64, device=dev)
+    dx = torch.empty((n, 2), dtype=torch.float64, device=dev)
+    lib = hp.lib()
+    fix = os.path.join(REPO, "tests", "golden", "overlap_5x10x10.npz")
+    xs = np.load(fix)["x_star"] if os.path.exists(fix) else None
+
+    def one(mode):
+        info = hp.RefineInfo()
+        pv = ctypes.c_int64(-1)
+        hp.check(lib.hp_overlap_norm_dd_dev(n, dcen.data_ptr(), dal.data_ptr(), dS.data_ptr(), sptr))
+        hp.check(lib.hp_spd_solve_refined_dev(dS.data_ptr(), db.data_ptr(), n, mode, 1e-28, 10, dx.data_ptr(),
+                                              ctypes.byref(info), ctypes.byref(pv), sptr))
+        return info
+
+    out = {"workload": f"overlap SPD, {n} s-Gaussians on a jittered 5x10x10 lattice (spacing 1.4 bohr, 4 exponents "
+                       "log-uniform in [0.01, 10]), b ~ N(0,1) (Irwin-Hall); S assembled in f128 on the GPU",
+           "n": n, "unit": "solves/s", "target": "max rel err <= 1e-25 vs the f512 oracle solution"}
+    for name, mode in (("chosen", hp.OZAKI), ("plain", hp.PLAIN)):
+        one(mode)  # warm-up
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        evs, infos = [], []
+        for _ in range(args.spd_steps):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record(stream)
+            infos.append(one(mode))
+            e.record(stream)
+            evs.append((s, e))
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(z) for a, z in evs) / args.spd_steps
+        if dist is not None:
+            t = torch.tensor([ms], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ms = float(t.item())
+        x = dx.cpu().numpy()
+        err = None
+        if xs is not None:
+            d = (xs[:, 0] - x[:, 0]) + (xs[:, 1] - x[:, 1]) + xs[:, 2] + xs[:, 3]
+            err = float(np.linalg.norm(d) / np.linalg.norm(xs[:, 0]))
+        out[name] = {"solves_per_s": world * 1e3 / ms, "ms_per_solve": ms,
+                     "factor_ms": infos[-1].factor_ms, "refine_iterations": infos[-1].iterations,
+                     "converged": bool(infos[-1].converged), "rel_err_vs_f512": err}
+    out["chosen_over_plain"] = out["chosen"]["solves_per_s"] / out["plain"]["solves_per_s"]
+    return out
+
+
+def cpu_spd_sample() -> dict:
+    """The reference's solve_spd_f128 (solver/src/lib.rs:71) on the same S, host cores."""
+    import numpy as np
+
+    import oracle
+    from quadprec_b200.workloads import overlap_spd_problem
+
+    cen, alpha, b = overlap_spd_problem(*SPD_LATTICE, seed=0)
+    n = len(alpha)
+    S = oracle.overlap_norm_dd(cen, alpha)
+    b2 = np.stack([b, np.zeros_like(b)], -1)
+    t0 = time.perf_counter()
+    sol = oracle.solve_spd_f128(S, b2, n)
+    dt = time.perf_counter() - t0
+    fix = os.path.join(REPO, "tests", "golden", "overlap_5x10x10.npz")
+    err = None
+    if os.path.exists(fix):
+        xs = np.load(fix)["x_star"]
+        x = sol["x"]
+        d = (xs[:, 0] - x[:, 0]) + (xs[:, 1] - x[:, 1]) + xs[:, 2] + xs[:, 3]
+        err = float(np.linalg.norm(d) / np.linalg.norm(xs[:, 0]))
+    return {"value": 1.0 / dt, "unit": "solves/s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"one solve_spd_f128 (f128 cholesky + solve_cholesky, crates/solver/src/lib.rs:127-144) "
+                      f"of the same n={n} S, {dt:.2f} s; reaches rel err {err} (f128 alone cannot reach 1e-25)"}
+
+
 # ---------------------------------------------------------------- main arm
 def main():
     ap = argparse.ArgumentParser()
@@ -183,6 +279,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--plain-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-spd", action="store_true", help="skip the overlap SPD solve section")
+    ap.add_argument("--spd-steps", type=int, default=3)
     ap.add_argument("--profile-case", action="store_true",
                     help="only run warmup + steps of the chosen path (for ncu captures)")
     args = ap.parse_args()
@@ -310,9 +408,13 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
 
+    spd = None if args.no_spd else spd_section(hp, torch, dev, stream, sptr, args, rank, world, dist)
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_sample_gflops()
+        if spd is not None:
+            spd["cpu_baseline"] = cpu_spd_sample()
 
     value = world * flops / (ms_chosen * 1e-3) / 1e9
     plain_value = world * flops / (ms_plain * 1e-3) / 1e9
@@ -337,6 +439,8 @@ def main():
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    if spd is not None:
+        line["spd"] = spd
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
