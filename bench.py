@@ -270,6 +270,20 @@ def cpu_spd_sample() -> dict:
                       f"of the same n={n} S, {dt:.2f} s; reaches rel err {err} (f128 alone cannot reach 1e-25)"}
 
 
+def profile_case_spd(args):
+    """One overlap SPD solve per mode (chosen, then plain): the command ncu captures."""
+    import torch
+
+    import quadprec_b200 as hp
+
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    args.spd_steps = max(1, args.steps)
+    out = spd_section(hp, torch, dev, stream, stream.cuda_stream, args, 0, 1, None)
+    print(json.dumps(out), file=sys.stderr)
+    return 0
+
+
 # ---------------------------------------------------------------- main arm
 def main():
     ap = argparse.ArgumentParser()
@@ -281,13 +295,15 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-spd", action="store_true", help="skip the overlap SPD solve section")
     ap.add_argument("--spd-steps", type=int, default=3)
-    ap.add_argument("--profile-case", action="store_true",
-                    help="only run warmup + steps of the chosen path (for ncu captures)")
+    ap.add_argument("--profile-case", nargs="?", const="gemm", default=None, choices=["gemm", "spd"],
+                    help="only run warmup + steps of one chosen-path workload (for ncu captures)")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
-    if args.profile_case:
+    if args.profile_case == "gemm":
         return profile_case(args)
+    if args.profile_case == "spd":
+        return profile_case_spd(args)
 
     import numpy as np
     import torch

@@ -62,3 +62,10 @@ int dd_maxabs(const double* v, size_t n, double* out_dev, cudaStream_t s);
 // ozaki.cu: Cholesky with the trailing matrix kept in the residue domain.
 int rns_cholesky(const double* S, double* L, size_t n, int64_t* pivot, cudaStream_t s);
 }  // namespace hp
+
+namespace hp {
+// trsv_blocked.cu: solves with precomputed inverses of the 64 x 64 diagonal blocks.
+int dd_block_inverses(const double* L, size_t n, double* Xall, cudaStream_t s);
+size_t dd_block_inverses_bytes(size_t n);
+int dd_trsv_blocked(const double* L, const double* Xall, double* v, size_t n, bool upper_t, cudaStream_t s);
+}  // namespace hp

@@ -506,13 +506,20 @@ __global__ void __launch_bounds__(256, 1)
     for (int t = blockIdx.x; t < num_tiles; t += gridDim.x, it++) {
       const int l = t / per_l, rem = t % per_l, tm = rem / tiles_n, tn = rem % tiles_n;
       const uint32_t acc = it & 1, aph = (it >> 1) & 1;
-      bool ok = mbar_wait(&tfull[acc], aph, status, DEV_STATUS_TIMEOUT);
-      if (!__all_sync(0xffffffffu, ok)) break;
-      tc_fence_after();
       const uint32_t m = (uint32_t)c_tab.mod[l];
       const int64_t row = c_row0 + (int64_t)tm * GB_M + ew * 32 + lane;
       uint8_t* dst = cres + (size_t)l * plane + (size_t)row * ldc + (size_t)(c_col0 + (int64_t)tn * GB_N);
-#pragma unroll 1
+      // read-modify-write tiles: fetch this row's 256 old bytes before waiting
+      // for the accumulator, so the loads overlap the MMAs
+      uint4 prev[GB_N / 16];
+      if (acc_mode) {
+#pragma unroll
+        for (int q = 0; q < GB_N / 16; q++) prev[q] = *reinterpret_cast<const uint4*>(dst + 16 * q);
+      }
+      bool ok = mbar_wait(&tfull[acc], aph, status, DEV_STATUS_TIMEOUT);
+      if (!__all_sync(0xffffffffu, ok)) break;
+      tc_fence_after();
+#pragma unroll
       for (int ch = 0; ch < GB_N / 32; ch++) {
         uint32_t v[32];
         tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(ew * 32) << 16) + acc * GB_N + ch * 32, v);
@@ -520,8 +527,12 @@ __global__ void __launch_bounds__(256, 1)
         uint32_t packed[8];
         uint4 prev0 = make_uint4(0, 0, 0, 0), prev1 = make_uint4(0, 0, 0, 0);
         if (acc_mode) {
-          prev0 = *reinterpret_cast<const uint4*>(dst + ch * 32);
-          prev1 = *reinterpret_cast<const uint4*>(dst + ch * 32 + 16);
+#pragma unroll
+          for (int q = 0; q < GB_N / 32; q++)
+            if (q == ch) {
+              prev0 = prev[2 * q];
+              prev1 = prev[2 * q + 1];
+            }
         }
         const uint32_t pv[8] = {prev0.x, prev0.y, prev0.z, prev0.w, prev1.x, prev1.y, prev1.z, prev1.w};
 #pragma unroll
@@ -1046,10 +1057,13 @@ __global__ void __launch_bounds__(256) chol_inv_block_kernel(const dd* __restric
     if (fail) return;
     for (int i = j + 1 + t; i < jb; i += 256) A[i * 65 + j] = dd_mul(A[i * 65 + j], rinv[j]);
     __syncthreads();
-    const int m = jb - j - 1;  // trailing (i, k), j < k <= i < jb
-    for (int q = t; q < m * m; q += 256) {
-      const int i = j + 1 + q / m, k = j + 1 + q % m;
-      if (k <= i) A[i * 65 + k] = dd_sub(A[i * 65 + k], dd_mul(A[i * 65 + j], A[k * 65 + j]));
+    const int m = jb - j - 1;  // trailing (i, k), j < k <= i < jb: m(m+1)/2 entries
+    for (int q = t; q < m * (m + 1) / 2; q += 256) {
+      int ii = (int)((sqrtf(8.0f * (float)q + 1.0f) - 1.0f) * 0.5f);
+      while (ii * (ii + 1) / 2 > q) ii--;
+      while ((ii + 1) * (ii + 2) / 2 <= q) ii++;
+      const int i = j + 1 + ii, k = j + 1 + (q - ii * (ii + 1) / 2);
+      A[i * 65 + k] = dd_sub(A[i * 65 + k], dd_mul(A[i * 65 + j], A[k * 65 + j]));
     }
     __syncthreads();
   }
@@ -1072,6 +1086,34 @@ __global__ void __launch_bounds__(256) chol_inv_block_kernel(const dd* __restric
       Lout[(kb + r) * n + kb + c] = dd_renorm(scale_pow2(v.hi, sh), scale_pow2(v.lo, sh));
     }
     XT[c * jb + r] = (c <= r) ? X[r * 65 + c] : dd{0.0, 0.0};  // XT[k][j] = X[j][k]
+  }
+}
+
+// Q = P21 X^T for the panel: Q[r][c] = sum_k P21[r][k] X[c][k] (k < jb),
+// XT[k][c] = X[c][k] in shared memory; one warp per row, lane c owns output
+// columns c and c + 32, P21[r][k] is broadcast by shuffle.
+__global__ void __launch_bounds__(256) panel_apply_kernel(const dd* __restrict__ P21, const dd* __restrict__ XT,
+                                                          dd* __restrict__ Q, int64_t m, int jb) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  dd(*xs)[CH_NB] = reinterpret_cast<dd(*)[CH_NB]>(sm_raw);  // [CH_NB][CH_NB]
+  for (int q = threadIdx.x; q < jb * jb; q += blockDim.x) xs[q / jb][q % jb] = XT[q];
+  __syncthreads();
+  const int lane = threadIdx.x % 32;
+  const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+  const int64_t nw = (int64_t)gridDim.x * blockDim.x / 32;
+  for (int64_t r = w0; r < m; r += nw) {
+    const dd a0 = lane < jb ? P21[r * jb + lane] : dd{0.0, 0.0};
+    const dd a1 = lane + 32 < jb ? P21[r * jb + lane + 32] : dd{0.0, 0.0};
+    dd acc0 = dd{0.0, 0.0}, acc1 = dd{0.0, 0.0};
+    for (int k = 0; k < jb; k++) {
+      dd ak;
+      ak.hi = __shfl_sync(0xffffffffu, k < 32 ? a0.hi : a1.hi, k % 32);
+      ak.lo = __shfl_sync(0xffffffffu, k < 32 ? a0.lo : a1.lo, k % 32);
+      if (lane < jb) acc0 = dd_add(acc0, dd_mul(ak, xs[k][lane]));
+      if (lane + 32 < jb) acc1 = dd_add(acc1, dd_mul(ak, xs[k][lane + 32]));
+    }
+    if (lane < jb) Q[r * jb + lane] = acc0;
+    if (lane + 32 < jb) Q[r * jb + lane + 32] = acc1;
   }
 }
 
@@ -1134,6 +1176,7 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
   }
   const size_t inv_smem = 2 * 64 * 65 * 16;
   HP_CUDA_TRY(cudaFuncSetAttribute(chol_inv_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
+  HP_CUDA_TRY(cudaFuncSetAttribute(panel_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, CH_NB * CH_NB * 16));
   for (size_t kb = 0; kb < n; kb += nb) {
     const int jb = (int)std::min(nb, n - kb);
     const size_t R = n - kb;
@@ -1156,7 +1199,12 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
     HP_LAUNCH_CHECK();
     if (R <= (size_t)jb) break;
     const size_t m = R - jb, t0 = kb + jb;
-    HP_TRY(dd_gemm_plain(P.as<double>() + 2 * (size_t)jb * jb, XT.as<double>(), Q.as<double>(), m, jb, jb, false, s));
+    {
+      const unsigned blocks = (unsigned)std::min<size_t>((m + 7) / 8, (size_t)D->num_sms * 4);
+      panel_apply_kernel<<<blocks, 256, CH_NB * CH_NB * 16, s>>>(P.as<dd>() + (size_t)jb * jb, XT.as<dd>(), Q.as<dd>(),
+                                                                 (int64_t)m, jb);
+      HP_LAUNCH_CHECK();
+    }
     round_store_kernel<<<(unsigned)((m * jb + 255) / 256), 256, 0, s>>>(Q.as<dd>(), (int64_t)m, jb, (int64_t)t0,
                                                                         (int64_t)kb, (int64_t)n, ebuf.as<int>(), Lout);
     HP_LAUNCH_CHECK();

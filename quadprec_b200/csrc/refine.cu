@@ -165,15 +165,18 @@ int spd_refined(const double* S, const double* b, size_t n, int mode, double tol
   }
   if (rc != HP_OK) return rc;
   cudaEventRecord(e1, s);
+  DevBuf Xinv(dd_block_inverses_bytes(n), s);
+  if (!Xinv.p) return HP_ERR_CUDA;
+  HP_TRY(dd_block_inverses(L.as<double>(), n, Xinv.as<double>(), s));
   HP_CUDA_TRY(cudaMemcpyAsync(x, b, n * 16, cudaMemcpyDeviceToDevice, s));
-  HP_TRY(dd_trsv(L.as<double>(), x, n, false, s));
-  HP_TRY(dd_trsv(L.as<double>(), x, n, true, s));
+  HP_TRY(dd_trsv_blocked(L.as<double>(), Xinv.as<double>(), x, n, false, s));
+  HP_TRY(dd_trsv_blocked(L.as<double>(), Xinv.as<double>(), x, n, true, s));
   int it = 0, converged = 0;
   double ratio = 0.0;
   for (it = 1; it <= max_iter; it++) {
     HP_TRY(dd_residual(S, x, b, r.as<double>(), n, mode == HP_MODE_PLAIN, s));
-    HP_TRY(dd_trsv(L.as<double>(), r.as<double>(), n, false, s));
-    HP_TRY(dd_trsv(L.as<double>(), r.as<double>(), n, true, s));
+    HP_TRY(dd_trsv_blocked(L.as<double>(), Xinv.as<double>(), r.as<double>(), n, false, s));
+    HP_TRY(dd_trsv_blocked(L.as<double>(), Xinv.as<double>(), r.as<double>(), n, true, s));
     HP_TRY(dd_vec(1, x, r.as<double>(), x, nullptr, n, s));
     HP_TRY(dd_maxabs(r.as<double>(), n, scal.as<double>(), s));
     HP_TRY(dd_maxabs(x, n, scal.as<double>() + 1, s));
