@@ -209,6 +209,50 @@ int hp_overlap_norm_dd(size_t n, const double* centers, const double* alpha, dou
 int hp_overlap_norm_dd_dev(size_t n, const double* centers, const double* alpha, double* s_out,
                            void* stream);
 
+/* ------------------------------------------------------------------------
+ * Batched uneven overlap SPD solves (no single reference counterpart: a
+ * batch of the reference's assemble -> solve_spd chains, each solved to
+ * 1e-25 as hp_spd_solve_refined does).
+ * System s owns basis functions offsets[s] .. offsets[s+1]-1 (centres
+ * 3 doubles each, exponents alpha, one normalised s Gaussian per function)
+ * and b[offsets[s] ..] (f128). All systems run in ONE persistent launch: CTAs
+ * pull systems from a queue ordered largest first; per system, in one CTA:
+ * f128 assembly, Cholesky, solve, refinement with ~2^-159 residuals until
+ * max|dx| <= tol max|x| (at most max_iter steps).
+ * status[s] = HP_OK, HP_ERR_NOT_SPD or HP_ERR_NO_CONVERGE; iters[s] = steps.
+ * _dev: offsets is a HOST array (count+1), everything else device memory;
+ * the launch is captured in a CUDA graph on first use and replayed for
+ * identical arguments. The plain form takes host arrays (b as f128). */
+int hp_spd_solve_batched(int count, const int64_t* offsets, const double* centers,
+                         const double* alpha, const double* b, double* x, int32_t* status,
+                         int32_t* iters, double tol, int max_iter);
+int hp_spd_solve_batched_dev(int count, const int64_t* offsets, const double* centers,
+                             const double* alpha, const double* b, double* x, int32_t* status,
+                             int32_t* iters, double tol, int max_iter, void* stream);
+/* Packed f128 overlap matrices of a batch (S_s at the running sum of n_t^2
+ * entries, t < s); same evaluation as hp_overlap_norm_dd. offsets: host. */
+int hp_overlap_norm_dd_batched_dev(int count, const int64_t* offsets, const double* centers,
+                                   const double* alpha, double* S, void* stream);
+
+/* ------------------------------------------------------------------------
+ * Jacobi eigensolver
+ * replaces: pub fn jacobi_eigen(a: &[f128], n: usize, max_iter: usize)
+ *           -> Result<(Vec<f128>, Vec<f128>), &'static str>
+ *           crates/quad/src/linalg.rs:299-362
+ * Same rotation formulas, skip and stopping rules; rotations are applied in
+ * the parallel round-robin order (n/2 disjoint rotations per round) instead
+ * of the sequential cyclic order, so results agree to rounding, not bits.
+ * evals: n f128; evecs: n x n f128, eigenvectors as ROWS (as the reference
+ * returns them). n <= 128. HP_ERR_NO_CONVERGE after max_iter sweeps. */
+int hp_f128_jacobi_eigen(const double* a, size_t n, size_t max_iter, double* evals,
+                         double* evecs, size_t* sweeps);
+/* Batch of matrices packed back to back (matrix s is n_s x n_s with
+ * n_s = n_off[s+1] - n_off[s]; n_off is a HOST array); evals packed by
+ * n_off, evecs packed like A. One CTA per matrix. */
+int hp_f128_jacobi_eigen_batched_dev(int count, const int64_t* n_off, const double* A,
+                                     size_t max_iter, double* evals, double* evecs,
+                                     int32_t* sweeps, int32_t* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -72,6 +72,13 @@ SIGNATURES = {
                              ctypes.c_int),
     "hp_spd_solve_refined_dev": ([_vp, _vp, _sz, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp, _vp, _i64p,
                                   _vp], ctypes.c_int),
+    "hp_spd_solve_batched": ([ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int],
+                             ctypes.c_int),
+    "hp_spd_solve_batched_dev": ([ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int,
+                                  _vp], ctypes.c_int),
+    "hp_overlap_norm_dd_batched_dev": ([ctypes.c_int, _vp, _vp, _vp, _vp, _vp], ctypes.c_int),
+    "hp_f128_jacobi_eigen": ([_vp, _sz, _sz, _vp, _vp, ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
+    "hp_f128_jacobi_eigen_batched_dev": ([ctypes.c_int, _vp, _vp, _sz, _vp, _vp, _vp, _vp, _vp], ctypes.c_int),
     "hp_assemble_overlap_s": ([_sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp], ctypes.c_int),
     "hp_overlap_norm_dd": ([_sz, _vp, _vp, _vp], ctypes.c_int),
     "hp_overlap_norm_dd_dev": ([_sz, _vp, _vp, _vp, _vp], ctypes.c_int),
@@ -286,3 +293,31 @@ def spd_solve_refined(S, b, n, mode=OZAKI, tol=1e-28, max_iter=10):
         raise HPError(rc, f"Matrix is not positive definite (failed at pivot {pv.value})")
     check(rc)
     return x, {f: getattr(info, f) for f, _ in RefineInfo._fields_}
+
+
+# ---------------- batched solves / Jacobi ----------------
+def spd_solve_batched(batch, tol=1e-28, max_iter=10):
+    """Solve every system of workloads.batched_overlap_systems() (host arrays)."""
+    off = np.ascontiguousarray(batch["offsets"], dtype=np.int64)
+    count = len(off) - 1
+    b = _c(batch["b"])
+    if b.ndim == 1:
+        b = np.stack([b, np.zeros_like(b)], -1)
+    x = np.empty((int(off[-1]), 2))
+    st = np.zeros(count, dtype=np.int32)
+    it = np.zeros(count, dtype=np.int32)
+    check(lib().hp_spd_solve_batched(count, off.ctypes.data, _ptr(_c(batch["centers"])), _ptr(_c(batch["alpha"])),
+                                      _ptr(b), _ptr(x), st.ctypes.data, it.ctypes.data, tol, max_iter))
+    return x, st, it
+
+
+def f128_jacobi_eigen(a, n, max_iter):
+    """linalg.rs:299 jacobi_eigen: (evals (n,2), eigenvectors as rows (n,n,2), sweeps)."""
+    ev = np.empty((n, 2))
+    vec = np.empty((n, n, 2))
+    sw = ctypes.c_size_t(0)
+    rc = lib().hp_f128_jacobi_eigen(_ptr(_c(a)), n, max_iter, _ptr(ev), _ptr(vec), ctypes.byref(sw))
+    if rc == HP_ERR_NO_CONVERGE:
+        raise HPError(rc, "Jacobi eigenvalue solver did not converge within max iterations")
+    check(rc)
+    return ev, vec, sw.value

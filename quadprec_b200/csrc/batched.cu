@@ -1,0 +1,429 @@
+// Batched uneven overlap SPD solves and batched Jacobi eigensolves.
+//
+// batched_spd_kernel: one persistent launch for a whole batch. CTAs (512
+// threads) pull system indices from a global counter; the host orders the
+// queue largest-n first so the long systems start early. Per system, inside
+// one CTA, with its working matrices in a per-CTA global slot (L2-resident):
+//   1. assemble S (f128) from the basis with overlap_norm_pair (the same
+//      f128 evaluation as hp_overlap_norm_dd, bit-identical);
+//   2. right-looking f128 Cholesky (crates/quad/src/linalg.rs:42-96 algebra,
+//      pivots by 1/sqrt in f128), pivot <= 0 -> status NOT_SPD;
+//   3. x = L^-T L^-1 b, then refinement x += L^-T L^-1 (b - S x) with the
+//      residual from error-free products and a 3-level TwoSum cascade
+//      (~2^-159), until max|dx| <= tol max|x| (crates/solver/src/lib.rs
+//      :75-125 with an f256-grade residual).
+// Only __syncthreads inside a CTA and one atomicAdd for the queue: no wait
+// can spin.
+//
+// batched_jacobi_kernel: one CTA per matrix (n <= 128), cyclic Jacobi in
+// the parallel (round-robin tournament) ordering: each round applies n/2
+// disjoint rotations at once, n-1 rounds per sweep. Rotation formulas, skip
+// rule (|a_pq| < 1e-60), stopping rule (off-norm < 1e-30 at the start of a
+// sweep) and the row-eigenvector output follow linalg.rs:299-362; the
+// rotation order differs (parallel instead of sequential), so results agree
+// with the reference to rounding, not bit-for-bit.
+#include "hp_arith.cuh"
+#include "hp_overlap.cuh"
+#include "hp_runtime.cuh"
+#include "kernels.cuh"
+
+namespace hp {
+
+namespace {
+
+constexpr int BT = 512;  // threads per CTA
+
+__device__ __forceinline__ dd rsqrt_dd(dd d) {
+  const double x0 = __ddiv_rn(1.0, __dsqrt_rn(d.hi));
+  const dd x = dd_from(x0);
+  const dd e = dd_sub(dd_from(1.0), dd_mul(d, dd_mul(x, x)));
+  return dd_add(x, dd_mul(x, dd_mul(e, dd_from(0.5))));
+}
+
+__device__ double block_max(double v, double* red) {
+  v = fmax(v, __shfl_xor_sync(0xffffffffu, v, 16));
+  v = fmax(v, __shfl_xor_sync(0xffffffffu, v, 8));
+  v = fmax(v, __shfl_xor_sync(0xffffffffu, v, 4));
+  v = fmax(v, __shfl_xor_sync(0xffffffffu, v, 2));
+  v = fmax(v, __shfl_xor_sync(0xffffffffu, v, 1));
+  __syncthreads();
+  if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = v;
+  __syncthreads();
+  double m = 0.0;
+  for (int w = 0; w < BT / 32; w++) m = fmax(m, red[w]);
+  __syncthreads();
+  return m;
+}
+
+// In-CTA triangular solves with L (row-major n x n, lower), v in place.
+__device__ void cta_trsv(const dd* L, dd* v, int n, bool upper_t, dd* bc) {
+  for (int s = 0; s < n; s++) {
+    const int j = upper_t ? n - 1 - s : s;
+    if (threadIdx.x == 0) {
+      v[j] = dd_div(v[j], L[(size_t)j * n + j]);
+      *bc = v[j];
+    }
+    __syncthreads();
+    const dd vj = *bc;
+    if (!upper_t) {
+      for (int i = j + 1 + threadIdx.x; i < n; i += BT) v[i] = dd_sub(v[i], dd_mul(L[(size_t)i * n + j], vj));
+    } else {
+      for (int i = threadIdx.x; i < j; i += BT) v[i] = dd_sub(v[i], dd_mul(L[(size_t)j * n + i], vj));
+    }
+    __syncthreads();
+  }
+}
+
+struct Casc3 {
+  double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+  __device__ __forceinline__ void add(double t) {
+    double a, e1, e2;
+    two_sum(s1, t, a, e1);
+    s1 = a;
+    two_sum(s2, e1, a, e2);
+    s2 = a;
+    s3 = __dadd_rn(s3, e2);
+  }
+};
+
+__global__ void __launch_bounds__(BT) batched_spd_kernel(int count, const int* __restrict__ order,
+                                                         const int64_t* __restrict__ off,
+                                                         const double* __restrict__ centers,
+                                                         const double* __restrict__ alpha, const dd* __restrict__ b,
+                                                         dd* __restrict__ x_out, int* __restrict__ status,
+                                                         int* __restrict__ iters, int* queue, dd* __restrict__ work,
+                                                         int64_t slot_elems, double tol, int max_iter) {
+  __shared__ int sys_sh;
+  __shared__ dd bc;
+  __shared__ double red[BT / 32];
+  __shared__ int fail;
+  dd* S = work + (size_t)blockIdx.x * 2 * slot_elems;
+  dd* L = S + slot_elems;
+  dd* r = x_out;  // placeholder, set per system
+  while (true) {
+    if (threadIdx.x == 0) {
+      int q = atomicAdd(queue, 1);
+      sys_sh = q < count ? order[q] : -1;
+      fail = 0;
+    }
+    __syncthreads();
+    const int sys = sys_sh;
+    if (sys < 0) break;
+    const int64_t o = off[sys];
+    const int n = (int)(off[sys + 1] - o);
+    const double* cen = centers + 3 * o;
+    const double* al = alpha + o;
+    dd* x = x_out + o;
+    r = L + (size_t)n * n;  // residual vector after L inside the slot
+    // 1. assemble S (lower triangle evaluated, mirrored), copy to L
+    for (int p = threadIdx.x; p < n * (n + 1) / 2; p += BT) {
+      int i = (int)((sqrtf(8.0f * (float)p + 1.0f) - 1.0f) * 0.5f);
+      while (i * (i + 1) / 2 > p) i--;
+      while ((i + 1) * (i + 2) / 2 <= p) i++;
+      const int j = p - i * (i + 1) / 2;
+      const dd v = overlap_norm_pair(al[i], cen + 3 * i, al[j], cen + 3 * j);
+      S[(size_t)i * n + j] = v;
+      S[(size_t)j * n + i] = v;
+      L[(size_t)i * n + j] = v;
+    }
+    __syncthreads();
+    // 2. right-looking Cholesky
+    for (int j = 0; j < n; j++) {
+      if (threadIdx.x == 0) {
+        const dd d = L[(size_t)j * n + j];
+        if (!(d.hi > 0.0)) {
+          fail = 1;
+        } else {
+          const dd rs = rsqrt_dd(d);
+          L[(size_t)j * n + j] = dd_mul(d, rs);
+          bc = rs;
+        }
+      }
+      __syncthreads();
+      if (fail) break;
+      const dd rs = bc;
+      for (int i = j + 1 + threadIdx.x; i < n; i += BT) L[(size_t)i * n + j] = dd_mul(L[(size_t)i * n + j], rs);
+      __syncthreads();
+      const int m = n - j - 1;
+      for (int p = threadIdx.x; p < m * (m + 1) / 2; p += BT) {
+        int ii = (int)((sqrtf(8.0f * (float)p + 1.0f) - 1.0f) * 0.5f);
+        while (ii * (ii + 1) / 2 > p) ii--;
+        while ((ii + 1) * (ii + 2) / 2 <= p) ii++;
+        const int i = j + 1 + ii, k = j + 1 + (p - ii * (ii + 1) / 2);
+        L[(size_t)i * n + k] = dd_sub(L[(size_t)i * n + k], dd_mul(L[(size_t)i * n + j], L[(size_t)k * n + j]));
+      }
+      __syncthreads();
+    }
+    if (fail) {
+      if (threadIdx.x == 0) {
+        status[sys] = HP_ERR_NOT_SPD;
+        iters[sys] = 0;
+      }
+      __syncthreads();
+      continue;
+    }
+    // 3. solve and refine
+    for (int i = threadIdx.x; i < n; i += BT) x[i] = b[o + i];
+    __syncthreads();
+    cta_trsv(L, x, n, false, &bc);
+    cta_trsv(L, x, n, true, &bc);
+    int it = 0, conv = 0;
+    for (it = 1; it <= max_iter; it++) {
+      const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+      for (int row = warp; row < n; row += BT / 32) {
+        Casc3 c;
+        if (lane == 0) {
+          c.add(-b[o + row].hi);
+          c.add(-b[o + row].lo);
+        }
+        for (int j = lane; j < n; j += 32) {
+          const dd sv = S[(size_t)row * n + j], xv = x[j];
+          double pp, e;
+          two_prod(sv.hi, xv.hi, pp, e);
+          c.add(pp);
+          c.add(e);
+          two_prod(sv.hi, xv.lo, pp, e);
+          c.add(pp);
+          c.add(e);
+          two_prod(sv.lo, xv.hi, pp, e);
+          c.add(pp);
+          c.add(e);
+          c.add(__dmul_rn(sv.lo, xv.lo));
+        }
+        for (int w = 16; w; w >>= 1) {
+          const double t1 = __shfl_down_sync(0xffffffffu, c.s1, w);
+          const double t2 = __shfl_down_sync(0xffffffffu, c.s2, w);
+          const double t3 = __shfl_down_sync(0xffffffffu, c.s3, w);
+          if (lane < w) {
+            c.add(t1);
+            c.add(t2);
+            c.add(t3);
+          }
+        }
+        if (lane == 0) {
+          double h, l;
+          two_sum(c.s1, c.s2, h, l);
+          r[row] = dd_neg(dd_renorm(h, __dadd_rn(l, c.s3)));
+        }
+      }
+      __syncthreads();
+      cta_trsv(L, r, n, false, &bc);
+      cta_trsv(L, r, n, true, &bc);
+      double md = 0.0, mx = 0.0;
+      for (int i = threadIdx.x; i < n; i += BT) {
+        x[i] = dd_add(x[i], r[i]);
+        md = fmax(md, fabs(r[i].hi));
+        mx = fmax(mx, fabs(x[i].hi));
+      }
+      md = block_max(md, red);
+      mx = block_max(mx, red);
+      if (md <= tol * mx) {
+        conv = 1;
+        break;
+      }
+    }
+    if (threadIdx.x == 0) {
+      status[sys] = conv ? HP_OK : HP_ERR_NO_CONVERGE;
+      iters[sys] = conv ? it : max_iter;
+    }
+    __syncthreads();
+  }
+}
+
+// Round-robin tournament over nn (even) players: in round r, slot k pairs
+// with slot nn-1-k; slot 0 is fixed and the others rotate.
+__device__ __forceinline__ int rr_player(int slot, int round, int nn) {
+  if (slot == 0) return 0;
+  return 1 + (slot - 1 + round) % (nn - 1);
+}
+
+// Jacobi on a copy of A (row-major n x n f128) in the per-CTA slot.
+__global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __restrict__ n_off,
+                                                            const int64_t* __restrict__ mat_off,
+                                                            const dd* __restrict__ Ain, dd* __restrict__ evals,
+                                                            dd* __restrict__ evecs, int* __restrict__ sweeps_out,
+                                                            int* __restrict__ status, dd* __restrict__ work,
+                                                            int64_t slot_elems, int max_sweeps) {
+  __shared__ dd cs[64][2];
+  __shared__ dd old[64][3];  // a_pp, a_qq, a_pq before the round
+  __shared__ dd tt[64];
+  __shared__ int prs[64][3];  // p, q, rotated?
+  __shared__ dd red[BT / 32];
+  __shared__ int stop;
+  const int sys = blockIdx.x;
+  const int n = (int)(n_off[sys + 1] - n_off[sys]);
+  const dd* Asrc = Ain + mat_off[sys];
+  dd* A = work + (size_t)blockIdx.x * 2 * slot_elems;
+  dd* V = A + slot_elems;
+  for (int p = threadIdx.x; p < n * n; p += BT) {
+    A[p] = Asrc[p];
+    V[p] = dd_from(p / n == p % n ? 1.0 : 0.0);
+  }
+  __syncthreads();
+  const int nn = n + (n & 1), half = nn / 2;
+  int sweep = 0, converged = 0;
+  for (sweep = 0; sweep < max_sweeps; sweep++) {
+    // off-diagonal norm (linalg.rs:307-315)
+    dd acc = dd{0.0, 0.0};
+    for (int p = threadIdx.x; p < n * n; p += BT)
+      if (p % n > p / n) acc = dd_add(acc, dd_mul(A[p], A[p]));
+    for (int w = 16; w; w >>= 1) {
+      dd t;
+      t.hi = __shfl_xor_sync(0xffffffffu, acc.hi, w);
+      t.lo = __shfl_xor_sync(0xffffffffu, acc.lo, w);
+      acc = dd_add(acc, t);
+    }
+    if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      dd tot = dd{0.0, 0.0};
+      for (int w = 0; w < BT / 32; w++) tot = dd_add(tot, red[w]);
+      stop = dd_lt(dd_sqrt(tot), dd_from(1e-30)) ? 1 : 0;
+    }
+    __syncthreads();
+    if (stop) {
+      converged = 1;
+      break;
+    }
+    for (int round = 0; round < nn - 1; round++) {
+      if (threadIdx.x < half) {
+        const int k = threadIdx.x;
+        int p = rr_player(k, round, nn), q = rr_player(nn - 1 - k, round, nn);
+        if (p > q) {
+          const int t = p;
+          p = q;
+          q = t;
+        }
+        dd c = dd_from(1.0), sr = dd_from(0.0), t = dd_from(0.0);
+        int rot = 0;
+        if (q < n) {
+          const dd apq = A[(size_t)p * n + q];
+          if (!dd_lt(dd_abs(apq), dd_from(1e-60))) {  // linalg.rs:326-335
+            const dd app = A[(size_t)p * n + p], aqq = A[(size_t)q * n + q];
+            const dd tau = dd_div(dd_sub(aqq, app), dd_mul(dd_from(2.0), apq));
+            const dd tden = dd_add(dd_abs(tau), dd_sqrt(dd_add(dd_from(1.0), dd_mul(tau, tau))));
+            t = tau.hi >= 0.0 ? dd_div(dd_from(1.0), tden) : dd_div(dd_neg(dd_from(1.0)), tden);
+            c = dd_div(dd_from(1.0), dd_sqrt(dd_add(dd_from(1.0), dd_mul(t, t))));
+            sr = dd_mul(t, c);
+            old[k][0] = app;
+            old[k][1] = aqq;
+            old[k][2] = apq;
+            rot = 1;
+          }
+        }
+        prs[k][0] = p;
+        prs[k][1] = q;
+        prs[k][2] = rot;
+        cs[k][0] = c;
+        cs[k][1] = sr;
+        tt[k] = t;
+      }
+      __syncthreads();
+      // columns p, q of A and V (linalg.rs:342-357)
+      for (int e = threadIdx.x; e < half * n; e += BT) {
+        const int k = e / n, row = e % n;
+        if (!prs[k][2]) continue;
+        const int p = prs[k][0], q = prs[k][1];
+        const dd c = cs[k][0], sr = cs[k][1];
+        const dd arp = A[(size_t)row * n + p], arq = A[(size_t)row * n + q];
+        A[(size_t)row * n + p] = dd_sub(dd_mul(c, arp), dd_mul(sr, arq));
+        A[(size_t)row * n + q] = dd_add(dd_mul(sr, arp), dd_mul(c, arq));
+        const dd vrp = V[(size_t)row * n + p], vrq = V[(size_t)row * n + q];
+        V[(size_t)row * n + p] = dd_sub(dd_mul(c, vrp), dd_mul(sr, vrq));
+        V[(size_t)row * n + q] = dd_add(dd_mul(sr, vrp), dd_mul(c, vrq));
+      }
+      __syncthreads();
+      // rows p, q of A
+      for (int e = threadIdx.x; e < half * n; e += BT) {
+        const int k = e / n, col = e % n;
+        if (!prs[k][2]) continue;
+        const int p = prs[k][0], q = prs[k][1];
+        const dd c = cs[k][0], sr = cs[k][1];
+        const dd apr = A[(size_t)p * n + col], aqr = A[(size_t)q * n + col];
+        A[(size_t)p * n + col] = dd_sub(dd_mul(c, apr), dd_mul(sr, aqr));
+        A[(size_t)q * n + col] = dd_add(dd_mul(sr, apr), dd_mul(c, aqr));
+      }
+      __syncthreads();
+      if (threadIdx.x < half && prs[threadIdx.x][2]) {  // linalg.rs:337-340
+        const int k = threadIdx.x, p = prs[k][0], q = prs[k][1];
+        A[(size_t)p * n + p] = dd_sub(old[k][0], dd_mul(tt[k], old[k][2]));
+        A[(size_t)q * n + q] = dd_add(old[k][1], dd_mul(tt[k], old[k][2]));
+        A[(size_t)p * n + q] = dd{0.0, 0.0};
+        A[(size_t)q * n + p] = dd{0.0, 0.0};
+      }
+      __syncthreads();
+    }
+  }
+  dd* ev = evals + n_off[sys];
+  dd* vo = evecs + mat_off[sys];
+  for (int i = threadIdx.x; i < n; i += BT) ev[i] = A[(size_t)i * n + i];
+  for (int p = threadIdx.x; p < n * n; p += BT) vo[p] = V[(size_t)(p % n) * n + p / n];  // rows = eigenvectors
+  if (threadIdx.x == 0) {
+    sweeps_out[sys] = sweep;
+    status[sys] = converged ? HP_OK : HP_ERR_NO_CONVERGE;
+  }
+}
+
+// Packed overlap matrices for a batch: S_s at S + mat_off[s] (n_s x n_s).
+__global__ void batched_assemble_kernel(const int64_t* __restrict__ off, const double* __restrict__ centers,
+                                        const double* __restrict__ alpha, const int64_t* __restrict__ mat_off,
+                                        dd* __restrict__ S) {
+  const int sys = blockIdx.x;
+  const int64_t o = off[sys];
+  const int n = (int)(off[sys + 1] - o);
+  dd* out = S + mat_off[sys];
+  for (int p = threadIdx.x; p < n * n; p += blockDim.x) {
+    const int i = p / n, j = p % n;
+    out[p] = overlap_norm_pair(alpha[o + i], centers + 3 * (o + i), alpha[o + j], centers + 3 * (o + j));
+  }
+}
+
+}  // namespace
+
+int batched_spd(int count, const int* order, const int64_t* off, const double* centers, const double* alpha,
+                const double* b, double* x, int* status, int* iters, int nmax, double tol, int max_iter,
+                cudaStream_t s, int grid_override) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = grid_override > 0 ? grid_override : sms;
+  const int64_t slot = (int64_t)nmax * nmax + 2 * (int64_t)nmax;  // S, then L + r
+  DevBuf work((size_t)grid * 2 * slot * 16, s), queue(sizeof(int), s);
+  if (!work.p || !queue.p) {
+    set_error("batched: workspace allocation failed");
+    return HP_ERR_CUDA;
+  }
+  HP_CUDA_TRY(cudaMemsetAsync(queue.p, 0, sizeof(int), s));
+  batched_spd_kernel<<<grid, BT, 0, s>>>(count, order, off, centers, alpha, reinterpret_cast<const dd*>(b),
+                                         reinterpret_cast<dd*>(x), status, iters, queue.as<int>(), work.as<dd>(),
+                                         slot, tol, max_iter);
+  HP_LAUNCH_CHECK();
+  return HP_OK;
+}
+
+int batched_jacobi(int count, const int64_t* n_off, const int64_t* mat_off, const double* A, double* evals,
+                   double* evecs, int* sweeps, int* status, int nmax, int max_sweeps, cudaStream_t s) {
+  if (count == 0) return HP_OK;
+  if (nmax > 128) {
+    set_error("batched jacobi: n <= 128 supported (got %d)", nmax);
+    return HP_ERR_UNSUPPORTED;
+  }
+  const int64_t slot = (int64_t)nmax * nmax;
+  DevBuf work((size_t)count * 2 * slot * 16, s);
+  if (!work.p) return HP_ERR_CUDA;
+  batched_jacobi_kernel<<<count, BT, 0, s>>>(n_off, mat_off, reinterpret_cast<const dd*>(A), reinterpret_cast<dd*>(evals),
+                                             reinterpret_cast<dd*>(evecs), sweeps, status, work.as<dd>(), slot,
+                                             max_sweeps);
+  HP_LAUNCH_CHECK();
+  return HP_OK;
+}
+
+int batched_assemble(int count, const int64_t* off, const double* centers, const double* alpha,
+                     const int64_t* mat_off, double* S, cudaStream_t s) {
+  if (count == 0) return HP_OK;
+  batched_assemble_kernel<<<count, 256, 0, s>>>(off, centers, alpha, mat_off, reinterpret_cast<dd*>(S));
+  HP_LAUNCH_CHECK();
+  return HP_OK;
+}
+
+}  // namespace hp

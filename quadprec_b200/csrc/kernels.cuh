@@ -69,3 +69,14 @@ int dd_block_inverses(const double* L, size_t n, double* Xall, cudaStream_t s);
 size_t dd_block_inverses_bytes(size_t n);
 int dd_trsv_blocked(const double* L, const double* Xall, double* v, size_t n, bool upper_t, cudaStream_t s);
 }  // namespace hp
+
+namespace hp {
+// batched.cu
+int batched_spd(int count, const int* order, const int64_t* off, const double* centers, const double* alpha,
+                const double* b, double* x, int* status, int* iters, int nmax, double tol, int max_iter,
+                cudaStream_t s, int grid_override);
+int batched_jacobi(int count, const int64_t* n_off, const int64_t* mat_off, const double* A, double* evals,
+                   double* evecs, int* sweeps, int* status, int nmax, int max_sweeps, cudaStream_t s);
+int batched_assemble(int count, const int64_t* off, const double* centers, const double* alpha,
+                     const int64_t* mat_off, double* S, cudaStream_t s);
+}  // namespace hp

@@ -119,3 +119,53 @@ def overlap_spd_problem(nx: int, ny: int, nz: int, seed: int = 0):
     n = len(alpha)
     b = normal(n, seed, offset=10 ** 9)
     return cen, alpha, b
+
+
+def batched_overlap_systems(count: int = 4096, seed: int = 0, n_min: int = 16, n_max: int = 384):
+    """Uneven batch of overlap SPD systems (random 3-D clusters).
+
+    System s uses its own SplitMix64 stream (seed, offset s * 2^24):
+      n = 4 * clamp(round(n_min * (n_max/n_min)^U / 4), n_min/4, n_max/4);
+      n/4 centres: the first at the origin, each next one at distance
+      U[1.2, 2.0] bohr from a uniformly chosen existing centre along a
+      direction drawn by rejection from the unit ball (no libm calls),
+      rejected (up to 64 tries) if closer than 1.2 to any existing centre;
+      4 exponents per centre, log-uniform in [0.01, 10]; b ~ N(0,1)
+      (Irwin-Hall, see normal()).
+    Returns dict with offsets (count+1), n (count), centers (N,3), alpha (N,), b (N,).
+    """
+    ns, cens, alphas, bs = [], [], [], []
+    for s in range(count):
+        u = uniform(1 << 15, seed, s << 24)
+        pos = 0
+
+        def draw():
+            nonlocal pos
+            v = u[pos]
+            pos += 1
+            return v
+
+        n = 4 * int(min(max(round(n_min * (n_max / n_min) ** draw() / 4.0), n_min // 4), n_max // 4))
+        pts = [np.zeros(3)]
+        while len(pts) < n // 4:
+            for _try in range(64):
+                base = pts[int(draw() * len(pts)) % len(pts)]
+                while True:
+                    d = np.array([2 * draw() - 1, 2 * draw() - 1, 2 * draw() - 1])
+                    r2 = float(d @ d)
+                    if 0.01 < r2 <= 1.0:
+                        break
+                cand = base + (1.2 + 0.8 * draw()) * d / np.sqrt(r2)
+                if min(float(np.sqrt(((p - cand) ** 2).sum())) for p in pts) >= 1.2:
+                    break
+            pts.append(cand)
+        ex = np.array([0.01 * 1000.0 ** draw() for _ in range(n)])
+        cen = np.repeat(np.array(pts), 4, axis=0)
+        ns.append(n)
+        cens.append(cen)
+        alphas.append(ex)
+        bs.append(normal(n, seed, (s << 24) + (1 << 20)))
+    off = np.zeros(count + 1, dtype=np.int64)
+    off[1:] = np.cumsum(ns)
+    return {"offsets": off, "n": np.array(ns, dtype=np.int64), "centers": np.concatenate(cens),
+            "alpha": np.concatenate(alphas), "b": np.concatenate(bs)}

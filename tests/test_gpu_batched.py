@@ -1,0 +1,115 @@
+"""GPU batched overlap SPD solves and Jacobi eigensolves."""
+import numpy as np
+import pytest
+
+import oracle as O
+from quadprec_b200.workloads import batched_overlap_systems
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small_batch():
+    return batched_overlap_systems(count=24, seed=3, n_min=16, n_max=64)
+
+
+def test_batched_solves_match_f256_oracle(gpu, small_batch):
+    B = small_batch
+    x, st, it = gpu.spd_solve_batched(B)
+    assert np.all(st == 0), st
+    off = B["offsets"]
+    for s in range(len(off) - 1):
+        o, e = off[s], off[s + 1]
+        n = e - o
+        S = O.overlap_norm_dd(B["centers"][o:e], B["alpha"][o:e])
+        S4 = np.zeros((n, n, 4))
+        S4[..., :2] = S
+        L4 = O.mf_cholesky(4, S4, n)
+        b4 = np.zeros((n, 4))
+        b4[:, 0] = B["b"][o:e]
+        xs = O.mf_cholesky_solve(4, L4, b4, n)
+        d = (xs[:, 0] - x[o:e, 0]) + (xs[:, 1] - x[o:e, 1]) + xs[:, 2]
+        assert np.linalg.norm(d) / np.linalg.norm(xs[:, 0]) <= 1e-25, s
+
+
+def test_batched_flags_only_bad_systems(gpu, small_batch):
+    """A non-SPD system (exponent made negative -> S_ii = nan/neg) fails alone."""
+    B = {k: np.array(v, copy=True) for k, v in small_batch.items()}
+    o = B["offsets"][5]
+    B["centers"][o + 1] = B["centers"][o]      # duplicate basis function ->
+    B["alpha"][o + 1] = B["alpha"][o]          # S exactly singular
+    x, st, it = gpu.spd_solve_batched(B)
+    assert st[5] != 0
+    assert np.all(np.delete(st, 5) == 0)
+
+
+def f128m(a):
+    out = np.zeros(a.shape + (2,))
+    out[..., 0] = a
+    return out
+
+
+def to_f64(x):
+    return x[..., 0] + x[..., 1]
+
+
+@pytest.mark.parametrize("n", [2, 3, 4, 7, 16, 33, 64])
+def test_jacobi_matches_reference(gpu, n):
+    rng = np.random.default_rng(n)
+    m = rng.standard_normal((n, n))
+    a = f128m((m + m.T) / 2.0)
+    ev, vec, sw = gpu.f128_jacobi_eigen(a, n, 200)
+    er, vr, swr = O.jacobi_eigen(a, n, 200)
+    # eigenvalues agree to f128 rounding (order may differ)
+    assert np.allclose(np.sort(to_f64(ev)), np.sort(to_f64(er)), rtol=0, atol=1e-26 * max(1.0, np.abs(m).max()))
+    # rows are orthonormal eigenvectors: A v = lambda v
+    A = to_f64(a)
+    V = to_f64(vec)
+    assert np.allclose(V @ V.T, np.eye(n), atol=1e-14)
+    assert np.allclose(A @ V.T, V.T * to_f64(ev)[None, :], atol=1e-13)
+
+
+def test_jacobi_reference_kats(gpu):  # linalg.rs:496-541
+    ev, vec, _ = gpu.f128_jacobi_eigen(f128m(np.array([[2.0, 1], [1, 2]])), 2, 100)
+    e = np.sort(to_f64(ev))
+    assert abs(e[0] - 1) < 1e-28 and abs(e[1] - 3) < 1e-28
+    ev, _, _ = gpu.f128_jacobi_eigen(f128m(np.eye(4)), 4, 10)
+    assert np.all(np.abs(to_f64(ev) - 1.0) < 1e-30)
+    ev, vec, _ = gpu.f128_jacobi_eigen(f128m(np.array([[4.0, 1, 0], [1, 3, 1], [0, 1, 2]])), 3, 200)
+    assert abs(to_f64(ev).sum() - 9.0) < 1e-25
+    with pytest.raises(gpu.HPError):
+        gpu.f128_jacobi_eigen(f128m(np.array([[2.0, 1], [1, 2]])), 2, 0)
+
+
+def test_batched_jacobi_on_overlap_matrices(gpu, small_batch):
+    import torch
+
+    B = small_batch
+    off = B["offsets"]
+    count = len(off) - 1
+    dc = torch.from_numpy(np.ascontiguousarray(B["centers"])).cuda()
+    da = torch.from_numpy(B["alpha"]).cuda()
+    ns = np.diff(off)
+    S = torch.empty(int((ns ** 2).sum()) * 2, dtype=torch.float64, device="cuda")
+    gpu.check(gpu.lib().hp_overlap_norm_dd_batched_dev(count, off.ctypes.data, dc.data_ptr(), da.data_ptr(),
+                                                       S.data_ptr(), 0))
+    ev = torch.empty(int(off[-1]) * 2, dtype=torch.float64, device="cuda")
+    vec = torch.empty_like(S)
+    sw = torch.zeros(count, dtype=torch.int32, device="cuda")
+    st = torch.zeros(count, dtype=torch.int32, device="cuda")
+    gpu.check(gpu.lib().hp_f128_jacobi_eigen_batched_dev(count, off.ctypes.data, S.data_ptr(), 200, ev.data_ptr(),
+                                                         vec.data_ptr(), sw.data_ptr(), st.data_ptr(), 0))
+    torch.cuda.synchronize()
+    assert int(st.abs().sum()) == 0
+    Sh = S.cpu().numpy().reshape(-1, 2)
+    evh = ev.cpu().numpy().reshape(-1, 2)
+    m0 = 0
+    for s in range(count):
+        n = int(ns[s])
+        Sm = Sh[m0:m0 + n * n].reshape(n, n, 2)
+        ref = O.overlap_norm_dd(B["centers"][off[s]:off[s + 1]], B["alpha"][off[s]:off[s + 1]])
+        assert np.array_equal(Sm, ref)
+        w = np.sort(to_f64(evh[off[s]:off[s + 1]]))
+        wr = np.sort(np.linalg.eigvalsh(to_f64(ref)))
+        assert np.allclose(w, wr, atol=1e-12)
+        m0 += n * n
