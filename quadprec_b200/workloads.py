@@ -134,32 +134,33 @@ def batched_overlap_systems(count: int = 4096, seed: int = 0, n_min: int = 16, n
       (Irwin-Hall, see normal()).
     Returns dict with offsets (count+1), n (count), centers (N,3), alpha (N,), b (N,).
     """
+    import math
+
     ns, cens, alphas, bs = [], [], [], []
     for s in range(count):
-        u = uniform(1 << 15, seed, s << 24)
+        u = uniform(1 << 15, seed, s << 24).tolist()
         pos = 0
-
-        def draw():
-            nonlocal pos
-            v = u[pos]
-            pos += 1
-            return v
-
-        n = 4 * int(min(max(round(n_min * (n_max / n_min) ** draw() / 4.0), n_min // 4), n_max // 4))
-        pts = [np.zeros(3)]
+        n = 4 * int(min(max(round(n_min * (n_max / n_min) ** u[pos] / 4.0), n_min // 4), n_max // 4))
+        pos += 1
+        pts = [(0.0, 0.0, 0.0)]
         while len(pts) < n // 4:
             for _try in range(64):
-                base = pts[int(draw() * len(pts)) % len(pts)]
+                bx, by, bz = pts[int(u[pos] * len(pts)) % len(pts)]
+                pos += 1
                 while True:
-                    d = np.array([2 * draw() - 1, 2 * draw() - 1, 2 * draw() - 1])
-                    r2 = float(d @ d)
+                    dx, dy, dz = 2 * u[pos] - 1, 2 * u[pos + 1] - 1, 2 * u[pos + 2] - 1
+                    pos += 3
+                    r2 = dx * dx + dy * dy + dz * dz
                     if 0.01 < r2 <= 1.0:
                         break
-                cand = base + (1.2 + 0.8 * draw()) * d / np.sqrt(r2)
-                if min(float(np.sqrt(((p - cand) ** 2).sum())) for p in pts) >= 1.2:
+                sc = (1.2 + 0.8 * u[pos]) / math.sqrt(r2)
+                pos += 1
+                cand = (bx + sc * dx, by + sc * dy, bz + sc * dz)
+                if min(math.sqrt((p[0] - cand[0]) ** 2 + (p[1] - cand[1]) ** 2 + (p[2] - cand[2]) ** 2)
+                       for p in pts) >= 1.2:
                     break
             pts.append(cand)
-        ex = np.array([0.01 * 1000.0 ** draw() for _ in range(n)])
+        ex = np.array([0.01 * 1000.0 ** u[pos + t] for t in range(n)])
         cen = np.repeat(np.array(pts), 4, axis=0)
         ns.append(n)
         cens.append(cen)
