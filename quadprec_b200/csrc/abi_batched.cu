@@ -29,6 +29,8 @@ struct GraphCache {
   std::vector<const void*> key;
   void* order_dev = nullptr;
   void* off_dev = nullptr;
+  void* work = nullptr;
+  void* queue = nullptr;
 };
 GraphCache g_cache;
 
@@ -60,6 +62,8 @@ int hp_spd_solve_batched_dev(int count, const int64_t* offsets, const double* ce
     cudaGraphDestroy(g_cache.graph);
     cudaFree(g_cache.order_dev);
     cudaFree(g_cache.off_dev);
+    cudaFree(g_cache.work);
+    cudaFree(g_cache.queue);
     g_cache.exec = nullptr;
   }
   std::vector<int> order;
@@ -69,14 +73,16 @@ int hp_spd_solve_batched_dev(int count, const int64_t* offsets, const double* ce
   HP_CUDA_TRY(cudaMalloc(&g_cache.off_dev, (count + 1) * sizeof(int64_t)));
   HP_CUDA_TRY(cudaMemcpy(g_cache.order_dev, order.data(), count * sizeof(int), cudaMemcpyHostToDevice));
   HP_CUDA_TRY(cudaMemcpy(g_cache.off_dev, offsets, (count + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
-  // capture the launch (queue reset + persistent kernel) on a private stream
+  // The workspace belongs to the cached graph (allocated here, outside the
+  // capture); the graph holds only the queue reset and the persistent kernel.
+  const int grid = batched_spd_grid(0);
+  HP_CUDA_TRY(cudaMalloc(&g_cache.work, batched_spd_work_bytes(grid, nmax)));
+  HP_CUDA_TRY(cudaMalloc(&g_cache.queue, sizeof(int)));
   cudaStream_t cap;
   HP_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
-  // workspace is allocated outside the graph (stream-ordered allocations in a
-  // captured graph would be freed at the end of every replay)
   HP_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
-  int rc = batched_spd(count, (const int*)g_cache.order_dev, (const int64_t*)g_cache.off_dev, centers, alpha, b, x,
-                       status, iters, nmax, tol, max_iter, cap, 0);
+  int rc = batched_spd_launch(count, (const int*)g_cache.order_dev, (const int64_t*)g_cache.off_dev, centers, alpha,
+                              b, x, status, iters, nmax, tol, max_iter, g_cache.work, (int*)g_cache.queue, grid, cap);
   cudaGraph_t graph = nullptr;
   cudaError_t ce = cudaStreamEndCapture(cap, &graph);
   cudaStreamDestroy(cap);

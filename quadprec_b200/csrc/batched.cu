@@ -380,25 +380,42 @@ __global__ void batched_assemble_kernel(const int64_t* __restrict__ off, const d
 
 }  // namespace
 
-int batched_spd(int count, const int* order, const int64_t* off, const double* centers, const double* alpha,
-                const double* b, double* x, int* status, int* iters, int nmax, double tol, int max_iter,
-                cudaStream_t s, int grid_override) {
+int batched_spd_grid(int grid_override) {
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int grid = grid_override > 0 ? grid_override : sms;
+  return grid_override > 0 ? grid_override : sms;
+}
+size_t batched_spd_work_bytes(int grid, int nmax) {
   const int64_t slot = (int64_t)nmax * nmax + 2 * (int64_t)nmax;  // S, then L + r
-  DevBuf work((size_t)grid * 2 * slot * 16, s), queue(sizeof(int), s);
+  return (size_t)grid * 2 * slot * 16;
+}
+
+// Queue reset + persistent launch on caller-provided workspace (no
+// allocation: safe inside stream capture).
+int batched_spd_launch(int count, const int* order, const int64_t* off, const double* centers, const double* alpha,
+                       const double* b, double* x, int* status, int* iters, int nmax, double tol, int max_iter,
+                       void* work, int* queue, int grid, cudaStream_t s) {
+  const int64_t slot = (int64_t)nmax * nmax + 2 * (int64_t)nmax;
+  HP_CUDA_TRY(cudaMemsetAsync(queue, 0, sizeof(int), s));
+  batched_spd_kernel<<<grid, BT, 0, s>>>(count, order, off, centers, alpha, reinterpret_cast<const dd*>(b),
+                                         reinterpret_cast<dd*>(x), status, iters, queue, reinterpret_cast<dd*>(work),
+                                         slot, tol, max_iter);
+  HP_LAUNCH_CHECK();
+  return HP_OK;
+}
+
+int batched_spd(int count, const int* order, const int64_t* off, const double* centers, const double* alpha,
+                const double* b, double* x, int* status, int* iters, int nmax, double tol, int max_iter,
+                cudaStream_t s, int grid_override) {
+  const int grid = batched_spd_grid(grid_override);
+  DevBuf work(batched_spd_work_bytes(grid, nmax), s), queue(sizeof(int), s);
   if (!work.p || !queue.p) {
     set_error("batched: workspace allocation failed");
     return HP_ERR_CUDA;
   }
-  HP_CUDA_TRY(cudaMemsetAsync(queue.p, 0, sizeof(int), s));
-  batched_spd_kernel<<<grid, BT, 0, s>>>(count, order, off, centers, alpha, reinterpret_cast<const dd*>(b),
-                                         reinterpret_cast<dd*>(x), status, iters, queue.as<int>(), work.as<dd>(),
-                                         slot, tol, max_iter);
-  HP_LAUNCH_CHECK();
-  return HP_OK;
+  return batched_spd_launch(count, order, off, centers, alpha, b, x, status, iters, nmax, tol, max_iter, work.p,
+                            queue.as<int>(), grid, s);
 }
 
 int batched_jacobi(int count, const int64_t* n_off, const int64_t* mat_off, const double* A, double* evals,

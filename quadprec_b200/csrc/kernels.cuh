@@ -75,6 +75,11 @@ namespace hp {
 int batched_spd(int count, const int* order, const int64_t* off, const double* centers, const double* alpha,
                 const double* b, double* x, int* status, int* iters, int nmax, double tol, int max_iter,
                 cudaStream_t s, int grid_override);
+int batched_spd_grid(int grid_override);
+size_t batched_spd_work_bytes(int grid, int nmax);
+int batched_spd_launch(int count, const int* order, const int64_t* off, const double* centers, const double* alpha,
+                       const double* b, double* x, int* status, int* iters, int nmax, double tol, int max_iter,
+                       void* work, int* queue, int grid, cudaStream_t s);
 int batched_jacobi(int count, const int64_t* n_off, const int64_t* mat_off, const double* A, double* evals,
                    double* evecs, int* sweeps, int* status, int nmax, int max_sweeps, cudaStream_t s);
 int batched_assemble(int count, const int64_t* off, const double* centers, const double* alpha,
