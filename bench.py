@@ -327,6 +327,57 @@ def batched_section(hp, torch, dev, stream, sptr, args, world, dist):
     return out
 
 
+ADJ_LATTICE = (5, 5, 10)  # 250 centres x 4 exponents = 1000 basis functions
+
+
+def adjoint_section(hp, torch, dev, stream, sptr, args, world, dist):
+    """Gradient of L = b^T S^-1 b wrt 750 centre coordinates and 1000
+    log-exponents (n = 1000): assembly + refined solve + adjoint sweep."""
+    import ctypes
+
+    import numpy as np
+
+    from quadprec_b200.workloads import overlap_spd_problem
+
+    cen, alpha, b = overlap_spd_problem(*ADJ_LATTICE, seed=0)
+    n = len(alpha)
+    nc = n // 4
+    co = np.arange(n, dtype=np.int32) // 4
+    dcen = torch.from_numpy(np.ascontiguousarray(cen)).to(dev)
+    dal = torch.from_numpy(alpha).to(dev)
+    db = torch.from_numpy(np.stack([b, np.zeros(n)], -1)).to(dev)
+    dco = torch.from_numpy(co).to(dev)
+    loss = torch.empty(2, dtype=torch.float64, device=dev)
+    gR = torch.empty((nc, 3, 2), dtype=torch.float64, device=dev)
+    ga = torch.empty((n, 2), dtype=torch.float64, device=dev)
+    lib = hp.lib()
+    out = {"workload": f"dL/dtheta for L = b^T S^-1 b, n = {n} s-Gaussians (250 jittered 5x5x10 lattice centres x 4 "
+                       "exponents), theta = 750 centre coordinates + 1000 log-exponents", "unit": "gradients/s"}
+    for name, mode in (("chosen", hp.OZAKI), ("plain", hp.PLAIN)):
+        info = hp.RefineInfo()
+
+        def one():
+            hp.check(lib.hp_overlap_adjoint_dev(n, dcen.data_ptr(), dal.data_ptr(), db.data_ptr(), dco.data_ptr(), nc,
+                                                mode, loss.data_ptr(), gR.data_ptr(), ga.data_ptr(),
+                                                ctypes.byref(info), sptr))
+
+        one()
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        steps = max(2, args.spd_steps)
+        s0, e0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(steps):
+            one()
+        e0.record(stream)
+        torch.cuda.synchronize()
+        ms = s0.elapsed_time(e0) / steps
+        out[name] = {"gradients_per_s": world * 1e3 / ms, "ms_per_gradient": ms, "converged": bool(info.converged)}
+    out["chosen_over_plain"] = out["chosen"]["gradients_per_s"] / out["plain"]["gradients_per_s"]
+    return out
+
+
 def cpu_spd_sample() -> dict:
     """The reference's solve_spd_f128 (solver/src/lib.rs:71) on the same S, host cores."""
     import numpy as np
@@ -379,6 +430,7 @@ def main():
     ap.add_argument("--no-spd", action="store_true", help="skip the overlap SPD solve section")
     ap.add_argument("--spd-steps", type=int, default=3)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched SPD / Jacobi section")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint section")
     ap.add_argument("--profile-case", nargs="?", const="gemm", default=None, choices=["gemm", "spd", "batched"],
                     help="only run warmup + steps of one chosen-path workload (for ncu captures)")
     args = ap.parse_args()
@@ -520,6 +572,7 @@ def main():
 
     spd = None if args.no_spd else spd_section(hp, torch, dev, stream, sptr, args, rank, world, dist)
     batched = None if args.no_batched else batched_section(hp, torch, dev, stream, sptr, args, world, dist)
+    adjoint = None if args.no_adjoint else adjoint_section(hp, torch, dev, stream, sptr, args, world, dist)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -554,6 +607,8 @@ def main():
         line["spd"] = spd
     if batched is not None:
         line["batched"] = batched
+    if adjoint is not None:
+        line["adjoint"] = adjoint
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -235,6 +235,25 @@ int hp_overlap_norm_dd_batched_dev(int count, const int64_t* offsets, const doub
                                    const double* alpha, double* S, void* stream);
 
 /* ------------------------------------------------------------------------
+ * Adjoint of overlap assembly + SPD solve (no reference counterpart: the
+ * reference has no derivatives; this differentiates its assemble -> solve
+ * chain). L = b^T S^-1 b with S the normalised s-Gaussian overlap matrix
+ * (hp_overlap_norm_dd) of n basis functions; basis function u sits on
+ * centre center_of[u] < n_centers. Returns loss (f128), grad_R
+ * (n_centers x 3 f128: dL/d coordinates of each centre) and grad_lnalpha
+ * (n f128: dL/d ln alpha_u). lambda = S^-1 b comes from the refined solve
+ * (mode as hp_spd_solve_refined, tol 1e-28); dS is never stored: the
+ * contraction sweeps the stored S and forms dS/dtheta = S dlnS/dtheta on
+ * the fly. b is f64 (host form) / f128 (_dev form). */
+int hp_overlap_adjoint(size_t n, const double* centers, const double* alpha, const double* b,
+                       const int32_t* center_of, size_t n_centers, int mode, double* loss,
+                       double* grad_R, double* grad_lnalpha, hp_refine_info_t* info);
+int hp_overlap_adjoint_dev(size_t n, const double* centers, const double* alpha, const double* b,
+                           const int32_t* center_of, size_t n_centers, int mode, double* loss,
+                           double* grad_R, double* grad_lnalpha, hp_refine_info_t* info,
+                           void* stream);
+
+/* ------------------------------------------------------------------------
  * Jacobi eigensolver
  * replaces: pub fn jacobi_eigen(a: &[f128], n: usize, max_iter: usize)
  *           -> Result<(Vec<f128>, Vec<f128>), &'static str>

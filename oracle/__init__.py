@@ -86,6 +86,8 @@ def lib():
             "or_overlap_primitive_f128": ([ctypes.c_double, _d, ctypes.c_double, _d, _d], None),
             "or_assemble_overlap_s": ([_sz, _d, _i64, _d, _d, _d, _d, _i64], None),
             "or_overlap_norm_dd": ([_sz, _d, _d, _d], None),
+            "or_adjoint_f128": ([_sz, _d, _d, _d, ctypes.POINTER(ctypes.c_int32), _sz, _d, _d, _d], ctypes.c_int),
+            "or_loss_f256": ([_sz, _d, _d, _d, _d], ctypes.c_int),
         }
         for name, (args, res) in sigs.items():
             f = getattr(L, name)
@@ -353,3 +355,31 @@ def overlap_norm_dd(centers, alpha) -> np.ndarray:
     s = np.zeros((n, n, 2))
     lib().or_overlap_norm_dd(n, _p(_f(centers)), _p(_f(alpha)), _p(s))
     return s
+
+
+# ---------------- adjoint ----------------
+def adjoint_f128(centers, alpha, b, center_of, n_centers):
+    """Gradient of L = b^T S^-1 b from the reference's f128 primitives.
+
+    Returns (loss (2,), grad wrt centre coordinates (n_centers,3,2),
+    grad wrt log-exponents (n,2))."""
+    n = len(alpha)
+    co = np.ascontiguousarray(center_of, dtype=np.int32)
+    loss = np.zeros(2)
+    gR = np.zeros((max(n, n_centers), 3, 2))
+    ga = np.zeros((n, 2))
+    rc = lib().or_adjoint_f128(n, _p(_f(centers)), _p(_f(alpha)), _p(_f(b)),
+                               co.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), n_centers, _p(loss), _p(gR), _p(ga))
+    if rc != 0:
+        raise RuntimeError("not positive definite")
+    return loss, gR[:n_centers].copy(), ga
+
+
+def loss_f256(centers4, alpha4, b):
+    """L = b^T S^-1 b in MultiFloat<4> from f256 centres (n,3,4) and exponents (n,4)."""
+    n = len(alpha4)
+    out = np.zeros(4)
+    rc = lib().or_loss_f256(n, _p(_f(centers4)), _p(_f(alpha4)), _p(_f(b)), _p(out))
+    if rc != 0:
+        raise RuntimeError("not positive definite")
+    return out

@@ -867,3 +867,106 @@ void or_overlap_norm_dd(size_t n, const double* centers, const double* alpha, do
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Adjoint of L = b^T S^-1 b for the normalised s-Gaussian overlap matrix
+// (test infrastructure for the GPU adjoint).
+//   dS_uv/dR_u = -2 p (R_u - R_v) S_uv,  p = a b / (a + b)
+//   a dS_uv/da = S_uv [ (3/4)(b - a)/(a + b) - r^2 a b^2 / (a + b)^2 ]
+//   dL/dtheta = -lambda^T (dS/dtheta) lambda,  lambda = S^-1 b
+// ---------------------------------------------------------------------------
+extern "C" {
+
+// "Reference-primitive" gradient: lambda from the reference's f128
+// cholesky + solve_cholesky (linalg.rs:42-126) and the contraction in f128
+// operations, row by row in index order.
+int or_adjoint_f128(size_t n, const double* centers, const double* alpha, const double* b,
+                    const int32_t* center_of, size_t n_centers, double* loss, double* grad_R,
+                    double* grad_lnalpha) {
+  std::vector<dd> S(n * n);
+  for (size_t i = 0; i < n; i++)
+    for (size_t j = 0; j <= i; j++) {
+      dd v = overlap_norm_dd(alpha[i], centers + 3 * i, alpha[j], centers + 3 * j);
+      S[i * n + j] = v;
+      S[j * n + i] = v;
+    }
+  std::vector<dd> L = S;
+  int64_t pv;
+  double val;
+  if (cholesky_vec(L, n, &pv, &val) != 0) return -2;
+  std::vector<dd> bv(n);
+  for (size_t i = 0; i < n; i++) bv[i] = dd_from(b[i]);
+  std::vector<dd> lam = backward_solve_v(L, forward_solve_v(L, bv, n), n);
+  dd Lsum{0, 0};
+  for (size_t i = 0; i < n; i++) Lsum = dd_add(Lsum, dd_mul(bv[i], lam[i]));
+  st(loss, 0, Lsum);
+  std::vector<dd> gR(3 * n_centers, dd{0, 0});
+#pragma omp parallel for schedule(dynamic, 8)
+  for (size_t u = 0; u < n; u++) {
+    dd accR[3] = {{0, 0}, {0, 0}, {0, 0}}, acca{0, 0};
+    const dd a = dd_from(alpha[u]);
+    for (size_t v = 0; v < n; v++) {
+      if (v == u) continue;
+      const dd bb = dd_from(alpha[v]);
+      const dd sum = dd_add(a, bb);
+      const dd p = dd_div(dd_mul(a, bb), sum);
+      dd d[3], r2{0, 0};
+      for (int c = 0; c < 3; c++) {
+        d[c] = dd_sub(dd_from(centers[3 * u + c]), dd_from(centers[3 * v + c]));
+        r2 = dd_add(r2, dd_mul(d[c], d[c]));
+      }
+      const dd w = dd_mul(lam[v], S[u * n + v]);
+      for (int c = 0; c < 3; c++) accR[c] = dd_add(accR[c], dd_mul(w, dd_mul(p, d[c])));
+      const dd f = dd_sub(dd_div(dd_mul(dd_from(0.75), dd_sub(bb, a)), sum),
+                          dd_div(dd_mul(r2, dd_mul(a, dd_mul(bb, bb))), dd_mul(sum, sum)));
+      acca = dd_add(acca, dd_mul(w, f));
+    }
+    const dd l4 = dd_mul(dd_from(4.0), lam[u]);
+    for (int c = 0; c < 3; c++) st(grad_R, 3 * u + c, dd_mul(l4, accR[c]));  // per basis function first
+    st(grad_lnalpha, u, dd_mul(dd_from(-2.0), dd_mul(lam[u], acca)));
+  }
+  // sum basis-function contributions per centre (index order)
+  std::vector<dd> per(3 * n);
+  for (size_t u = 0; u < 3 * n; u++) per[u] = ld(grad_R, u);
+  for (size_t c = 0; c < 3 * n_centers; c++) gR[c] = dd{0, 0};
+  for (size_t u = 0; u < n; u++)
+    for (int c = 0; c < 3; c++) gR[3 * center_of[u] + c] = dd_add(gR[3 * center_of[u] + c], per[3 * u + c]);
+  for (size_t c = 0; c < 3 * n_centers; c++) st(grad_R, c, gR[c]);
+  return 0;
+}
+
+// L = b^T S^-1 b in MultiFloat<4> with S from f256 centres / exponents
+// (for central finite differences): centers4 n x 3 x 4, alpha4 n x 4.
+int or_loss_f256(size_t n, const double* centers4, const double* alpha4, const double* b, double* loss4) {
+  std::vector<mf<4>> S(n * n);
+  auto ldq = [&](const double* p) { return ldm<4>(p, 0); };
+#pragma omp parallel for schedule(dynamic, 4)
+  for (size_t i = 0; i < n; i++)
+    for (size_t j = 0; j <= i; j++) {
+      mf<4> a = ldq(alpha4 + 4 * i), bb = ldq(alpha4 + 4 * j);
+      mf<4> sum = mf_add<4>(a, bb), prod = mf_mul<4>(a, bb);
+      mf<4> ratio = mf_div<4>(mf_mul<4>(mf_from<4>(4.0), prod), mf_mul<4>(sum, sum));
+      mf<4> sq = mf_sqrt<4>(ratio);
+      mf<4> pref = mf_mul<4>(sq, mf_sqrt<4>(sq));
+      mf<4> mu = mf_div<4>(prod, sum);
+      mf<4> r2 = mf_zero<4>();
+      for (int c = 0; c < 3; c++) {
+        mf<4> d = mf_sub<4>(ldq(centers4 + 12 * i + 4 * c), ldq(centers4 + 12 * j + 4 * c));
+        r2 = mf_add<4>(r2, mf_mul<4>(d, d));
+      }
+      mf<4> v = mf_mul<4>(pref, mf_exp<4>(mf_neg<4>(mf_mul<4>(mu, r2))));
+      S[i * n + j] = v;
+      S[j * n + i] = v;
+    }
+  std::vector<double> Sp(n * n * 4), bq(n * 4, 0.0), x(n * 4);
+  for (size_t i = 0; i < n * n; i++) stm<4>(Sp.data(), i, S[i]);
+  for (size_t i = 0; i < n; i++) bq[4 * i] = b[i];
+  if (mf_cholesky_t<4>(Sp.data(), n) != 0) return -2;
+  mf_cholesky_solve_t<4>(Sp.data(), bq.data(), x.data(), n);
+  mf<4> Ls = mf_zero<4>();
+  for (size_t i = 0; i < n; i++) Ls = mf_add<4>(Ls, mf_mul<4>(mf_from<4>(b[i]), ldm<4>(x.data(), i)));
+  stm<4>(loss4, 0, Ls);
+  return 0;
+}
+
+}  // extern "C"

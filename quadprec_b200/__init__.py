@@ -79,6 +79,8 @@ SIGNATURES = {
     "hp_overlap_norm_dd_batched_dev": ([ctypes.c_int, _vp, _vp, _vp, _vp, _vp], ctypes.c_int),
     "hp_f128_jacobi_eigen": ([_vp, _sz, _sz, _vp, _vp, ctypes.POINTER(ctypes.c_size_t)], ctypes.c_int),
     "hp_f128_jacobi_eigen_batched_dev": ([ctypes.c_int, _vp, _vp, _sz, _vp, _vp, _vp, _vp, _vp], ctypes.c_int),
+    "hp_overlap_adjoint": ([_sz, _vp, _vp, _vp, _vp, _sz, ctypes.c_int, _vp, _vp, _vp, _vp], ctypes.c_int),
+    "hp_overlap_adjoint_dev": ([_sz, _vp, _vp, _vp, _vp, _sz, ctypes.c_int, _vp, _vp, _vp, _vp, _vp], ctypes.c_int),
     "hp_assemble_overlap_s": ([_sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp], ctypes.c_int),
     "hp_overlap_norm_dd": ([_sz, _vp, _vp, _vp], ctypes.c_int),
     "hp_overlap_norm_dd_dev": ([_sz, _vp, _vp, _vp, _vp], ctypes.c_int),
@@ -321,3 +323,17 @@ def f128_jacobi_eigen(a, n, max_iter):
         raise HPError(rc, "Jacobi eigenvalue solver did not converge within max iterations")
     check(rc)
     return ev, vec, sw.value
+
+
+# ---------------- adjoint ----------------
+def overlap_adjoint(centers, alpha, b, center_of, n_centers, mode=OZAKI):
+    """Gradient of L = b^T S^-1 b: (loss (2,), grad_R (n_centers,3,2), grad_lnalpha (n,2), info)."""
+    n = len(alpha)
+    co = np.ascontiguousarray(center_of, dtype=np.int32)
+    loss = np.empty(2)
+    gR = np.empty((n_centers, 3, 2))
+    ga = np.empty((n, 2))
+    info = RefineInfo()
+    check(lib().hp_overlap_adjoint(n, _ptr(_c(centers)), _ptr(_c(alpha)), _ptr(_c(b)), co.ctypes.data, n_centers,
+                                   mode, _ptr(loss), _ptr(gR), _ptr(ga), ctypes.byref(info)))
+    return loss, gR, ga, {f: getattr(info, f) for f, _ in RefineInfo._fields_}
