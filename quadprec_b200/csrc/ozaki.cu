@@ -387,7 +387,8 @@ constexpr int MAX_K_CHUNK = 65536;  // |int32 accumulator| <= 2^16 * 2^14 = 2^30
 
 __global__ void __launch_bounds__(256, 1)
     i8_gemm_mod_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int L,
-                       int tiles_m, int tiles_n, int kb0, int kb1, int acc_mode, uint8_t* __restrict__ cres,
+                       int tiles_m, int tiles_n, int kb0, int kb1, int kb_off_b, int acc_mode,
+                       uint8_t* __restrict__ cres,
                        int64_t ldc, int64_t plane, int64_t c_row0, int64_t c_col0, uint32_t* status) {
   using namespace sm100;
   extern __shared__ uint8_t smem_raw[];
@@ -448,7 +449,7 @@ __global__ void __launch_bounds__(256, 1)
           }
           mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
           tma_load_3d(sA + stage * A_STAGE, &mapA, &full[stage], (kb0 + kb) * GB_K, tm * GB_M, l);
-          tma_load_3d(sB + stage * B_STAGE, &mapB, &full[stage], (kb0 + kb) * GB_K, tn * GB_N, l);
+          tma_load_3d(sB + stage * B_STAGE, &mapB, &full[stage], (kb0 + kb + kb_off_b) * GB_K, tn * GB_N, l);
           filled_phase[stage] = (int)phase;
           if (++stage == GSTAGES) {
             stage = 0;
@@ -754,6 +755,17 @@ int ozaki_residue_gemm(const int8_t* ares, const int8_t* bres, uint8_t* cres, in
 int ozaki_residue_gemm_ex(const int8_t* ares, const int8_t* bres, uint8_t* cres, int L, size_t Mp, size_t Np,
                           size_t Kp, size_t ldc, size_t plane, size_t c_row0, size_t c_col0, int acc_mode,
                           cudaStream_t s, size_t ra_rows, size_t rb_rows) {
+  return ozaki_residue_gemm_k(ares, bres, cres, L, Mp, Np, Kp, Kp, 0, Kp, 0, ldc, plane, c_row0, c_col0, acc_mode, s,
+                              ra_rows, rb_rows);
+}
+
+// General form: the residue planes have row length ka (A) / kb (B) bytes;
+// the product runs over k_len bytes starting at byte a_k0 of A's rows and
+// b_k0 of B's rows (multiples of 128).
+int ozaki_residue_gemm_k(const int8_t* ares, const int8_t* bres, uint8_t* cres, int L, size_t Mp, size_t Np,
+                         size_t ka, size_t kb_len_b, size_t a_k0, size_t k_len, size_t b_k0, size_t ldc,
+                         size_t plane, size_t c_row0, size_t c_col0, int acc_mode, cudaStream_t s, size_t ra_rows,
+                         size_t rb_rows) {
   using namespace ozaki;
   DevTables* D;
   HP_TRY(device_tables(&D));
@@ -765,8 +777,8 @@ int ozaki_residue_gemm_ex(const int8_t* ares, const int8_t* bres, uint8_t* cres,
     attr_set[dev] = true;
   }
   CUtensorMap mapA, mapB;
-  HP_TRY(make_map(&mapA, ares, Kp, ra_rows ? ra_rows : Mp, L, GB_M));
-  HP_TRY(make_map(&mapB, bres, Kp, rb_rows ? rb_rows : Np, L, GB_N));
+  HP_TRY(make_map(&mapA, ares, ka, ra_rows ? ra_rows : Mp, L, GB_M));
+  HP_TRY(make_map(&mapB, bres, kb_len_b, rb_rows ? rb_rows : Np, L, GB_N));
   uint32_t* status = device_status(s);
   if (!status) {
     set_error("status word allocation failed");
@@ -775,12 +787,13 @@ int ozaki_residue_gemm_ex(const int8_t* ares, const int8_t* bres, uint8_t* cres,
   const int tiles_m = (int)(Mp / GB_M), tiles_n = (int)(Np / GB_N);
   const int num_tiles = L * tiles_m * tiles_n;
   const int grid = std::min(num_tiles, D->num_sms);
-  const int nkb_total = (int)(Kp / GB_K);
+  const int kb_first = (int)(a_k0 / GB_K), nkb_total = (int)(k_len / GB_K);
+  const int boff = (int)(b_k0 / GB_K) - kb_first;
   const int kb_chunk = MAX_K_CHUNK / GB_K;
-  for (int kb0 = 0; kb0 < nkb_total; kb0 += kb_chunk) {
-    int kb1 = std::min(nkb_total, kb0 + kb_chunk);
-    const int mode = kb0 > 0 ? (acc_mode == 2 ? 2 : 1) : acc_mode;
-    i8_gemm_mod_kernel<<<grid, 256, GEMM_SMEM, s>>>(mapA, mapB, L, tiles_m, tiles_n, kb0, kb1, mode, cres,
+  for (int c0 = 0; c0 < nkb_total; c0 += kb_chunk) {
+    const int kb0 = kb_first + c0, kb1 = kb_first + std::min(nkb_total, c0 + kb_chunk);
+    const int mode = c0 > 0 ? (acc_mode == 2 ? 2 : 1) : acc_mode;
+    i8_gemm_mod_kernel<<<grid, 256, GEMM_SMEM, s>>>(mapA, mapB, L, tiles_m, tiles_n, kb0, kb1, boff, mode, cres,
                                                      (int64_t)ldc, (int64_t)plane, (int64_t)c_row0,
                                                      (int64_t)c_col0, status);
     HP_LAUNCH_CHECK();
@@ -859,9 +872,311 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
   return HP_OK;
 }
 
-int ozaki_qd_gemm(const double*, const double*, double*, size_t, size_t, size_t, bool, cudaStream_t) {
-  set_error("f256 Ozaki GEMM is not built yet");
-  return HP_ERR_UNSUPPORTED;
+// ===========================================================================
+// f256 (MultiFloat<4>) Ozaki-II GEMM.
+// Entries are scaled to integers X of <= 210 bits and split X = Xh 2^105 + Xl
+// (balanced base-2^21 digits, |Xh|, |Xl| <= 2^105). Two exact residue GEMM
+// groups are formed,
+//     G1 = Xh Yh  (k terms),   G2 = [Xh | Xl] [Yl ; Yh] = Xh Yl + Xl Yh (2k),
+// each rebuilt by the CRT and rounded to f256, and C = (G1 2^105 + G2) 2^-s.
+// The omitted Xl Yl term is below 2^-209 of |A||B| (the f256 tolerance is
+// 4k 2^-208 normwise). Residue rows are 2 Kp bytes: A = [Xh | Xl], B = [Yl | Yh].
+// ===========================================================================
+namespace ozaki {
+constexpr int BETA_QD = 210;
+
+// Balanced base-2^21 digits of rint(v) for |v| < 2^212 (exact).
+__device__ __forceinline__ void int_digits21x10(double v, int32_t* d) {
+  double a = fabs(rint(v));
+  const int32_t sg = signbit(v) ? -1 : 1;
+#pragma unroll
+  for (int c = 9; c >= 1; c--) {
+    const double sc = scale_pow2(1.0, -21 * c), up = scale_pow2(1.0, 21 * c);
+    const double t = floor(__dmul_rn(a, sc));
+    a = __dsub_rn(a, __dmul_rn(t, up));
+    d[c] = sg * (int32_t)t;
+  }
+  d[0] = sg * (int32_t)a;
+}
+
+// residues of a 5-digit (base 2^21) number
+__device__ __forceinline__ uint32_t balanced_byte21(const int32_t* D, const int* w, int l, int m) {
+  int32_t x = 0;
+#pragma unroll
+  for (int c = 0; c < 5; c++) x += D[c] * w[c];
+  int r = (int)mod_reduce(x, l);
+  if (r > 127) r -= m;
+  return (uint32_t)(r & 0xFF);
+}
+
+// Operand residues for the f256 GEMM. Element (r, p) is src[r*K + p]
+// (P_CONTIG) or src[p*R + r], 4 limbs. Writes hi digits at byte offset
+// hi_off and lo digits at lo_off of each 2*Kp-byte row, planes of Rp rows.
+template <bool P_CONTIG>
+__global__ void __launch_bounds__(256) residue_qd_kernel(const double4* __restrict__ src, int64_t R, int64_t K,
+                                                         const int* __restrict__ expf, int L, int64_t Rp, int64_t Kp,
+                                                         int64_t hi_off, int64_t lo_off, int8_t* __restrict__ out) {
+  __shared__ int w21[MAXL][5];
+  for (int q = threadIdx.x; q < L * 5; q += blockDim.x) {
+    const int l = q / 5, c = q % 5;
+    const int m = c_tab.mod[l];
+    int64_t r = 1;
+    for (int t = 0; t < 21 * c; t++) r = (r * 2) % m;
+    int b = (int)r;
+    if (b > m / 2) b -= m;
+    w21[l][c] = b;
+  }
+  __shared__ __align__(16) uint32_t T[2][2][RT_R][RT_P / 4 + 1];
+  __syncthreads();
+  const int t = threadIdx.x;
+  const int rl = P_CONTIG ? t / 4 : t % 64;
+  const int oct = P_CONTIG ? t % 4 : t / 64;
+  const int64_t r = (int64_t)blockIdx.y * RT_R + rl;
+  const int64_t p0 = (int64_t)blockIdx.x * RT_P + 8 * oct;
+  int32_t dig[8][10];
+#pragma unroll
+  for (int e = 0; e < 8; e++)
+#pragma unroll
+    for (int c = 0; c < 10; c++) dig[e][c] = 0;
+  if (r < R) {
+    const int ex = expf[r];
+    if (ex != EXP_NONFINITE) {
+      const int sh = BETA_QD + 1022 - ex;
+#pragma unroll
+      for (int e = 0; e < 8; e++) {
+        const int64_t p = p0 + e;
+        if (p < K) {
+          const double4 v = P_CONTIG ? src[r * K + p] : src[p * R + r];
+          const double lim[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+          for (int q = 0; q < 4; q++) {
+            int32_t d[10];
+            int_digits21x10(scale_pow2(lim[q], sh), d);
+#pragma unroll
+            for (int c = 0; c < 10; c++) dig[e][c] += d[c];
+          }
+#pragma unroll
+          for (int c = 0; c < 9; c++) {
+            const int32_t carry = (dig[e][c] + (1 << 20)) >> 21;
+            dig[e][c] -= carry << 21;
+            dig[e][c + 1] += carry;
+          }
+        }
+      }
+    }
+  }
+  int8_t* const base = out + (size_t)(blockIdx.y * RT_R) * (2 * Kp) + blockIdx.x * RT_P;
+  for (int l = 0; l < L; l++) {
+    const int m = c_tab.mod[l];
+    uint32_t wh0 = 0, wh1 = 0, wl0 = 0, wl1 = 0;
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      wl0 |= balanced_byte21(dig[e], w21[l], l, m) << (8 * e);
+      wl1 |= balanced_byte21(dig[e + 4], w21[l], l, m) << (8 * e);
+      wh0 |= balanced_byte21(dig[e] + 5, w21[l], l, m) << (8 * e);
+      wh1 |= balanced_byte21(dig[e + 4] + 5, w21[l], l, m) << (8 * e);
+    }
+    int8_t* plane = base + (size_t)l * Rp * (2 * Kp);
+    if (P_CONTIG) {
+      *reinterpret_cast<uint2*>(plane + (size_t)rl * (2 * Kp) + hi_off + 8 * oct) = make_uint2(wh0, wh1);
+      *reinterpret_cast<uint2*>(plane + (size_t)rl * (2 * Kp) + lo_off + 8 * oct) = make_uint2(wl0, wl1);
+    } else {
+      T[l & 1][0][rl][2 * oct] = wh0;
+      T[l & 1][0][rl][2 * oct + 1] = wh1;
+      T[l & 1][1][rl][2 * oct] = wl0;
+      T[l & 1][1][rl][2 * oct + 1] = wl1;
+      __syncthreads();
+      {
+        const int row = t / 4, part = (t % 4) / 2, half = t % 2;
+        const uint32_t* sw = &T[l & 1][part][row][4 * half];
+        *reinterpret_cast<uint4*>(plane + (size_t)row * (2 * Kp) + (part ? lo_off : hi_off) + 16 * half) =
+            make_uint4(sw[0], sw[1], sw[2], sw[3]);
+      }
+    }
+  }
+}
+
+// f256 CRT: rebuild G1 and G2, C = (G1 2^105 + G2) 2^-(sa + sb).
+__device__ __forceinline__ qd chunks_to_qd(const double* acc, int nc) {
+  double v[8];
+#pragma unroll
+  for (int i = 0; i < 8; i++) v[i] = 0.0;
+  // most significant chunk first
+#pragma unroll
+  for (int i = 0; i < 8; i++) {
+    const int c = nc - 1 - i;
+    if (c >= 0) v[i] = scale_pow2(acc[c], CRT_BITS * c);
+  }
+  qd r;
+  qd_renormalize_from8(v, r.l);
+  return r;
+}
+template <int NC>
+__device__ __forceinline__ qd crt_group_qd(const uint8_t* rp, int64_t plane, int L, const double (*w_s)[NC],
+                                           const double* mch, double inv_m) {
+  double acc[NC + 1];
+#pragma unroll
+  for (int q = 0; q <= NC; q++) acc[q] = 0.0;
+  for (int l0 = 0; l0 < L; l0 += 8) {
+    uint32_t v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) v[u] = (l0 + u < L) ? (uint32_t)__ldg(rp + (size_t)(l0 + u) * plane) : 0u;
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      if (l0 + u >= L) break;
+      const double x = byte_to_double(v[u]);
+#pragma unroll
+      for (int q = 0; q < NC; q++) acc[q] = __fma_rn(x, w_s[l0 + u][q], acc[q]);
+    }
+  }
+  bool neg;
+  (void)crt_finish<NC>(acc, mch, inv_m, &neg);  // leaves |value| in normalised chunks
+  qd r = chunks_to_qd(acc, NC);
+  return neg ? qd_neg(r) : r;
+}
+template <int NC>
+__global__ void __launch_bounds__(256) crt_qd_kernel(const uint8_t* __restrict__ g1, const uint8_t* __restrict__ g2,
+                                                     int64_t plane, int64_t Np, int64_t m, int64_t n,
+                                                     const int* __restrict__ expA, const int* __restrict__ expB,
+                                                     const CrtTable* __restrict__ tab, double4* __restrict__ C) {
+  __shared__ double w_s[MAXL][NC];
+  __shared__ double mch_s[NC];
+  const int L = tab->L;
+  for (int i = threadIdx.x; i < L * NC; i += blockDim.x) w_s[i / NC][i % NC] = tab->w[i / NC][i % NC];
+  if (threadIdx.x < NC) mch_s[threadIdx.x] = tab->mchunk[threadIdx.x];
+  __syncthreads();
+  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= m * n) return;
+  const int64_t i = idx / n, j = idx % n;
+  const int ea = expA[i], eb = expB[j];
+  if (ea == EXP_NONFINITE || eb == EXP_NONFINITE) {
+    const double nan = __longlong_as_double(0x7ff8000000000000ll);
+    C[idx] = make_double4(nan, 0.0, 0.0, 0.0);
+    return;
+  }
+  const size_t o = (size_t)i * Np + j;
+  const qd a = crt_group_qd<NC>(g1 + o, plane, L, w_s, mch_s, tab->inv_m);
+  const qd b = crt_group_qd<NC>(g2 + o, plane, L, w_s, mch_s, tab->inv_m);
+  qd a_sh;
+#pragma unroll
+  for (int q = 0; q < 4; q++) a_sh.l[q] = scale_pow2(a.l[q], 105);
+  qd c = qd_add(a_sh, b);
+  const int shift = -((BETA_QD + 1022 - ea) + (BETA_QD + 1022 - eb));
+  C[idx] = make_double4(scale_pow2(c.l[0], shift), scale_pow2(c.l[1], shift), scale_pow2(c.l[2], shift),
+                        scale_pow2(c.l[3], shift));
+}
+
+// exponent scans over f256 rows / columns (limb 0 and 1 as in the f128 scan)
+__global__ void maxexp_rows_qd_kernel(const double4* __restrict__ src, int64_t R, int64_t C, int* __restrict__ out) {
+  int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
+  int lane = threadIdx.x % 32;
+  if (row >= R) return;
+  int e = 0;
+  for (int64_t p = lane; p < C; p += 32) {
+    double4 v = src[row * C + p];
+    e = max(e, max(exp_field(v.x), min(exp_field(v.y) + 1, EXP_NONFINITE)));
+    if (exp_field(v.y) == EXP_NONFINITE || exp_field(v.z) == EXP_NONFINITE || exp_field(v.w) == EXP_NONFINITE)
+      e = EXP_NONFINITE;
+  }
+  for (int o = 16; o; o >>= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, o));
+  if (lane == 0) out[row] = e;
+}
+__global__ void maxexp_cols_qd_kernel(const double4* __restrict__ src, int64_t R, int64_t C, int64_t slab,
+                                      int* __restrict__ out) {
+  __shared__ int red[8][33];
+  int64_t c = (int64_t)blockIdx.x * 32 + threadIdx.x;
+  int64_t r0 = (int64_t)blockIdx.y * slab, r1 = min(R, r0 + slab);
+  int e = 0;
+  if (c < C) {
+    for (int64_t r = r0 + threadIdx.y; r < r1; r += 8) {
+      double4 v = src[r * C + c];
+      e = max(e, max(exp_field(v.x), min(exp_field(v.y) + 1, EXP_NONFINITE)));
+      if (exp_field(v.y) == EXP_NONFINITE || exp_field(v.z) == EXP_NONFINITE || exp_field(v.w) == EXP_NONFINITE)
+        e = EXP_NONFINITE;
+    }
+  }
+  red[threadIdx.y][threadIdx.x] = e;
+  __syncthreads();
+  if (threadIdx.y == 0 && c < C) {
+    for (int y = 1; y < 8; y++) e = max(e, red[y][threadIdx.x]);
+    atomicMax(out + c, e);
+  }
+}
+}  // namespace ozaki
+
+int ozaki_qd_gemm(const double* a, const double* b, double* c, size_t m, size_t n, size_t k, bool atb,
+                  cudaStream_t s) {
+  using namespace ozaki;
+  if (m == 0 || n == 0) return HP_OK;
+  if (k == 0) {
+    HP_CUDA_TRY(cudaMemsetAsync(c, 0, m * n * 32, s));
+    return HP_OK;
+  }
+  DevTables* D;
+  HP_TRY(device_tables(&D));
+  // |G| < 2k 2^210: need log2 M >= 210 + ceil(log2 2k) + 2
+  const int L = ozaki_moduli_for(2 * k, BETA_QD / 2);
+  if (L < 0) {
+    set_error("ozaki f256: k = %zu needs more moduli than the table holds", k);
+    return HP_ERR_UNSUPPORTED;
+  }
+  const size_t Mp = round_up(m, GB_M), Np = round_up(n, GB_N), Kp = round_up(k, GB_K);
+  DevBuf expA(Mp * sizeof(int), s), expB(Np * sizeof(int), s);
+  DevBuf ares((size_t)L * Mp * 2 * Kp, s), bres((size_t)L * Np * 2 * Kp, s);
+  DevBuf g1((size_t)L * Mp * Np, s), g2((size_t)L * Mp * Np, s);
+  if (!expA.p || !expB.p || !ares.p || !bres.p || !g1.p || !g2.p) {
+    set_error("ozaki f256: workspace allocation failed");
+    return HP_ERR_CUDA;
+  }
+  HP_CUDA_TRY(cudaMemsetAsync(expA.p, 0, Mp * sizeof(int), s));
+  HP_CUDA_TRY(cudaMemsetAsync(expB.p, 0, Np * sizeof(int), s));
+  const double4* A4 = reinterpret_cast<const double4*>(a);
+  const double4* B4 = reinterpret_cast<const double4*>(b);
+  if (!atb) {
+    maxexp_rows_qd_kernel<<<(unsigned)((m + 7) / 8), 256, 0, s>>>(A4, m, k, expA.as<int>());
+  } else {
+    dim3 g((unsigned)((m + 31) / 32), (unsigned)((k + 255) / 256));
+    maxexp_cols_qd_kernel<<<g, dim3(32, 8), 0, s>>>(A4, k, m, 256, expA.as<int>());
+  }
+  HP_LAUNCH_CHECK();
+  {
+    dim3 g((unsigned)((n + 31) / 32), (unsigned)((k + 255) / 256));
+    maxexp_cols_qd_kernel<<<g, dim3(32, 8), 0, s>>>(B4, k, n, 256, expB.as<int>());
+    HP_LAUNCH_CHECK();
+  }
+  {
+    dim3 ga((unsigned)(Kp / RT_P), (unsigned)(Mp / RT_R));
+    if (!atb)
+      residue_qd_kernel<true><<<ga, 256, 0, s>>>(A4, m, k, expA.as<int>(), L, Mp, Kp, 0, Kp, ares.as<int8_t>());
+    else
+      residue_qd_kernel<false><<<ga, 256, 0, s>>>(A4, m, k, expA.as<int>(), L, Mp, Kp, 0, Kp, ares.as<int8_t>());
+    HP_LAUNCH_CHECK();
+    dim3 gb((unsigned)(Kp / RT_P), (unsigned)(Np / RT_R));
+    residue_qd_kernel<false><<<gb, 256, 0, s>>>(B4, n, k, expB.as<int>(), L, Np, Kp, Kp, 0, bres.as<int8_t>());
+    HP_LAUNCH_CHECK();
+  }
+  // G1 = Xh Yh: A bytes [0, Kp), B bytes [Kp, 2Kp)
+  HP_TRY(ozaki_residue_gemm_k(ares.as<int8_t>(), bres.as<int8_t>(), g1.as<uint8_t>(), L, Mp, Np, 2 * Kp, 2 * Kp, 0, Kp,
+                              Kp, Np, Mp * Np, 0, 0, 0, s, Mp, Np));
+  // G2 = [Xh | Xl] [Yl ; Yh]: both over [0, 2Kp)
+  HP_TRY(ozaki_residue_gemm_k(ares.as<int8_t>(), bres.as<int8_t>(), g2.as<uint8_t>(), L, Mp, Np, 2 * Kp, 2 * Kp, 0,
+                              2 * Kp, 0, Np, Mp * Np, 0, 0, 0, s, Mp, Np));
+  const int nc = host_tables().crt[L].nc;
+  const unsigned grid = (unsigned)((m * n + 255) / 256);
+#define HP_CRTQ(NC)                                                                                                  \
+  case NC:                                                                                                           \
+    crt_qd_kernel<NC><<<grid, 256, 0, s>>>(g1.as<uint8_t>(), g2.as<uint8_t>(), (int64_t)(Mp * Np), (int64_t)Np, m, n, \
+                                           expA.as<int>(), expB.as<int>(), D->crt + L, reinterpret_cast<double4*>(c)); \
+    break;
+  switch (nc) {
+    HP_CRTQ(5) HP_CRTQ(6) HP_CRTQ(7) HP_CRTQ(8)
+    default:
+      set_error("ozaki f256: unsupported chunk count %d", nc);
+      return HP_ERR_UNSUPPORTED;
+  }
+#undef HP_CRTQ
+  HP_LAUNCH_CHECK();
+  return HP_OK;
 }
 
 

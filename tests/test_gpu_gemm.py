@@ -123,3 +123,44 @@ def test_device_pointer_form(gpu):
     gpu.f128_gemm_dev(da, db, dc, m, n, k, gpu.PLAIN, stream=s.cuda_stream)
     s.synchronize()
     assert np.array_equal(dc.cpu().numpy(), O.gemm(a, b, m, n, k))
+
+
+def qd_operand(rows, cols, seed):
+    """Full 4-limb f256 entries: a dd entry plus two lower limbs."""
+    x = dense_dd(rows, cols, seed=seed)
+    y = dense_dd(rows, cols, seed=seed + 1000)
+    q = np.zeros((rows, cols, 4))
+    q[..., :2] = x
+    q[..., 2] = y[..., 0] * np.abs(x[..., 1]) * 2.0 ** -53
+    q[..., 3] = y[..., 1] * np.abs(x[..., 1]) * 2.0 ** -53
+    return q
+
+
+def qd_normwise_err(c, ref, a, b, atb):
+    d = ((c[..., 0] - ref[..., 0]) + (c[..., 1] - ref[..., 1])) + ((c[..., 2] - ref[..., 2]) + (c[..., 3] - ref[..., 3]))
+    A = np.abs(a[..., 0])
+    B = np.abs(b[..., 0])
+    return np.linalg.norm(d) / np.linalg.norm((A.T if atb else A) @ B)
+
+
+@pytest.mark.parametrize("atb", [False, True])
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (3, 5, 7), (17, 33, 20), (70, 40, 130)])
+def test_f256_ozaki_tolerance(gpu, m, n, k, atb):
+    a = qd_operand(k, m, 31) if atb else qd_operand(m, k, 31)
+    b = qd_operand(k, n, 37)
+    c = gpu.f256_gemm(a, b, m, n, k, gpu.OZAKI, atb)
+    ref = O.mf_gemm(4, a, b, m, n, k, atb=atb)
+    err = qd_normwise_err(c, ref, a, b, atb)
+    assert err <= 4 * k * 2.0 ** -208, err
+
+
+def test_f256_ozaki_exact_small_integers(gpu):
+    """Integer matrices: the f256 Ozaki product is exact."""
+    rng = np.random.default_rng(9)
+    m, n, k = 20, 30, 40
+    A = np.zeros((m, k, 4))
+    B = np.zeros((k, n, 4))
+    A[..., 0] = rng.integers(-1000, 1000, (m, k))
+    B[..., 0] = rng.integers(-1000, 1000, (k, n))
+    c = gpu.f256_gemm(A, B, m, n, k, gpu.OZAKI)
+    assert np.array_equal(c[..., 0], A[..., 0] @ B[..., 0]) and np.all(c[..., 1:] == 0)
