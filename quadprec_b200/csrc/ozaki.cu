@@ -878,7 +878,8 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
 // (balanced base-2^21 digits, |Xh|, |Xl| <= 2^105). Two exact residue GEMM
 // groups are formed,
 //     G1 = Xh Yh  (k terms),   G2 = [Xh | Xl] [Yl ; Yh] = Xh Yl + Xl Yh (2k),
-// each rebuilt by the CRT and rounded to f256, and C = (G1 2^105 + G2) 2^-s.
+// each rebuilt by the CRT and rounded to f256, and since
+// X Y = G1 2^210 + G2 2^105 + Xl Yl, C = (G1 2^105 + G2) 2^(105 - sa - sb).
 // The omitted Xl Yl term is below 2^-209 of |A||B| (the f256 tolerance is
 // 4k 2^-208 normwise). Residue rows are 2 Kp bytes: A = [Xh | Xl], B = [Yl | Yh].
 // ===========================================================================
@@ -996,7 +997,7 @@ __global__ void __launch_bounds__(256) residue_qd_kernel(const double4* __restri
   }
 }
 
-// f256 CRT: rebuild G1 and G2, C = (G1 2^105 + G2) 2^-(sa + sb).
+// f256 CRT: rebuild G1 and G2, C = (G1 2^105 + G2) 2^(105 - sa - sb).
 __device__ __forceinline__ qd chunks_to_qd(const double* acc, int nc) {
   double v[8];
 #pragma unroll
@@ -1060,8 +1061,8 @@ __global__ void __launch_bounds__(256) crt_qd_kernel(const uint8_t* __restrict__
   qd a_sh;
 #pragma unroll
   for (int q = 0; q < 4; q++) a_sh.l[q] = scale_pow2(a.l[q], 105);
-  qd c = qd_add(a_sh, b);
-  const int shift = -((BETA_QD + 1022 - ea) + (BETA_QD + 1022 - eb));
+  qd c = qd_add(a_sh, b);  // X Y / 2^105 = G1 2^105 + G2 (+ Xl Yl / 2^105, omitted)
+  const int shift = 105 - ((BETA_QD + 1022 - ea) + (BETA_QD + 1022 - eb));
   C[idx] = make_double4(scale_pow2(c.l[0], shift), scale_pow2(c.l[1], shift), scale_pow2(c.l[2], shift),
                         scale_pow2(c.l[3], shift));
 }
