@@ -174,6 +174,57 @@ def profile_case(args):
     return 0
 
 
+def gemm_more_section(hp, torch, dev, stream, sptr, world, dist):
+    """gemm_atb at 2048^3 (f128) and mf_gemm at 1024^3 (f256), chosen and plain."""
+    import numpy as np
+
+    from quadprec_b200.workloads import dd_to_qd, gemm_operands
+
+    def timed(fn, steps):
+        fn()
+        torch.cuda.synchronize()
+        s0, e0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record(stream)
+        for _ in range(steps):
+            fn()
+        e0.record(stream)
+        torch.cuda.synchronize()
+        return s0.elapsed_time(e0) / steps
+
+    out = {}
+    a, b = gemm_operands(M, N, K, seed=1, atb=True)
+    A, B = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
+    C = torch.empty((M, N, 2), dtype=torch.float64, device=dev)
+    for name, mode, steps in (("chosen", hp.OZAKI, 5), ("plain", hp.PLAIN, 1)):
+        ms = timed(lambda: hp.f128_gemm_dev(A, B, C, M, N, K, mode, atb=True, stream=sptr), steps)
+        out.setdefault("f128_gemm_atb_2048", {})[name] = {"gflops": world * 2.0 * M * N * K / (ms * 1e-3) / 1e9,
+                                                          "ms": ms}
+    del A, B, C
+    n4 = 1024
+    a, b = gemm_operands(n4, n4, n4, seed=2)
+    a4, b4 = dd_to_qd(a), dd_to_qd(b)
+    a4[..., 2] = a4[..., 1] * 2.0 ** -60  # full 4-limb entries
+    b4[..., 2] = b4[..., 1] * 2.0 ** -60
+    A, B = torch.from_numpy(a4).to(dev), torch.from_numpy(b4).to(dev)
+    C = torch.empty((n4, n4, 4), dtype=torch.float64, device=dev)
+    res = {}
+    for name, mode, steps in (("chosen", hp.OZAKI, 5), ("plain", hp.PLAIN, 1)):
+        ms = timed(lambda: hp.f256_gemm_dev(A, B, C, n4, n4, n4, mode, stream=sptr), steps)
+        res[name] = {"gflops": world * 2.0 * n4 ** 3 / (ms * 1e-3) / 1e9, "ms": ms}
+        torch.cuda.synchronize()
+        res[name + "_c"] = C.cpu().numpy()
+    d = ((res["chosen_c"][..., 0] - res["plain_c"][..., 0]) + (res["chosen_c"][..., 1] - res["plain_c"][..., 1])
+         + (res["chosen_c"][..., 2] - res["plain_c"][..., 2]))
+    absab = np.abs(a4[..., 0]) @ np.abs(b4[..., 0])
+    out["f256_mf_gemm_1024"] = {"chosen": res["chosen"], "plain": res["plain"],
+                                "chosen_over_plain": res["chosen"]["ms"] and res["plain"]["ms"] / res["chosen"]["ms"],
+                                "normwise_rel_err_vs_plain": float(np.linalg.norm(d) / np.linalg.norm(absab)),
+                                "unit": "GFLOP/s (2mnk f256 ops)"}
+    out["f128_gemm_atb_2048"]["chosen_over_plain"] = (out["f128_gemm_atb_2048"]["plain"]["ms"]
+                                                       / out["f128_gemm_atb_2048"]["chosen"]["ms"])
+    return out
+
+
 SPD_LATTICE = (5, 10, 10)  # 500 centres x 4 exponents = 2000 basis functions
 
 
@@ -570,6 +621,7 @@ def main():
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         e2e_s = float(t.item())
 
+    more = gemm_more_section(hp, torch, dev, stream, sptr, world, dist)
     spd = None if args.no_spd else spd_section(hp, torch, dev, stream, sptr, args, rank, world, dist)
     batched = None if args.no_batched else batched_section(hp, torch, dev, stream, sptr, args, world, dist)
     adjoint = None if args.no_adjoint else adjoint_section(hp, torch, dev, stream, sptr, args, world, dist)
@@ -603,6 +655,7 @@ def main():
     }
     if cpu is not None:
         line["cpu_baseline"] = cpu
+    line["gemm_more"] = more
     if spd is not None:
         line["spd"] = spd
     if batched is not None:
