@@ -214,7 +214,7 @@ def gemm_more_section(hp, torch, dev, stream, sptr, world, dist):
         torch.cuda.synchronize()
         res[name + "_c"] = C.cpu().numpy()
     d = ((res["chosen_c"][..., 0] - res["plain_c"][..., 0]) + (res["chosen_c"][..., 1] - res["plain_c"][..., 1])
-         + (res["chosen_c"][..., 2] - res["plain_c"][..., 2]))
+         + (res["chosen_c"][..., 2] - res["plain_c"][..., 2]) + (res["chosen_c"][..., 3] - res["plain_c"][..., 3]))
     absab = np.abs(a4[..., 0]) @ np.abs(b4[..., 0])
     out["f256_mf_gemm_1024"] = {"chosen": res["chosen"], "plain": res["plain"],
                                 "chosen_over_plain": res["chosen"]["ms"] and res["plain"]["ms"] / res["chosen"]["ms"],

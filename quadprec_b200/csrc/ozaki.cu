@@ -1339,6 +1339,21 @@ __device__ __forceinline__ dd dd_rsqrt(dd d) {
 
 // Factor the jb x jb block P[0..jb)[0..jb) (row stride jb, symmetric values)
 // in f128, write L~11 scaled back to Lout, and X^T = (L~11^-1)^T to XT.
+// Thread (ti, tk) = (t / 16, t % 16) owns the entries (i, k) with
+// i = ti (mod 16), k = tk (mod 16) (at most 4 x 4), so every column step
+// spreads its rank-1 update evenly and each thread reuses 4 row and 4 column
+// multipliers from registers. Iteration j runs factor step j and inverse
+// step j - 1 between one pair of barriers:
+//   factor:  l_i = a_ij / sqrt(d_j) for the thread's rows and columns,
+//            a_ik -= l_i l_k (k <= i); the scaled column goes to the unused
+//            upper triangle (A[j][i] = l_ij), so raw and scaled values never
+//            share an address; the owner of (j+1, j+1) updates it first and
+//            forms 1/sqrt of the next pivot while the others finish.
+//   inverse: row-oriented forward substitution for X = L~^-1:
+//            x_kc = X[k][c] / l_kk, X[i][c] -= l_ik x_kc (i > k); the final
+//            row k goes straight to XT.
+// Every entry sees the same f128 operations in the same order as a plain
+// right-looking column Cholesky followed by the forward substitution.
 __global__ void __launch_bounds__(256) chol_inv_block_kernel(const dd* __restrict__ P, int jb, int64_t kb, int64_t n,
                                                              const int* __restrict__ e, dd* __restrict__ Lout,
                                                              dd* __restrict__ XT, RnsErr* err) {
@@ -1347,61 +1362,106 @@ __global__ void __launch_bounds__(256) chol_inv_block_kernel(const dd* __restric
   dd* X = A + 64 * 65;                    // [64][65]
   __shared__ dd rinv[64];
   __shared__ int fail;
-  const int t = threadIdx.x;
+  const int t = threadIdx.x, ti = t / 16, tk = t % 16;
   if (err->flag) return;
-  if (t == 0) fail = 0;
   for (int q = t; q < jb * jb; q += 256) {
     const int r = q / jb, c = q % jb;
     A[r * 65 + c] = P[q];
     X[r * 65 + c] = dd_from(r == c ? 1.0 : 0.0);
   }
+  if (t == 0) fail = 0;
   __syncthreads();
-  for (int j = 0; j < jb; j++) {
-    if (t == 0) {
-      const dd d = A[j * 65 + j];
-      if (!(d.hi > 0.0)) {
-        fail = 1;
-        err->flag = 1;
-        err->pivot = kb + j;
-      } else {
-        const dd r = dd_rsqrt(d);
-        A[j * 65 + j] = dd_mul(d, r);
-        rinv[j] = r;
+  auto pivot = [&](int j) {  // A[j][j] <- sqrt(d), rinv[j] <- 1/sqrt(d)
+    const dd d = A[j * 65 + j];
+    if (!(d.hi > 0.0)) {
+      fail = 1;
+      err->flag = 1;
+      err->pivot = kb + j;
+    } else {
+      const dd r = dd_rsqrt(d);
+      A[j * 65 + j] = dd_mul(d, r);
+      rinv[j] = r;
+    }
+  };
+  if (t == 0) pivot(0);
+  __syncthreads();
+  for (int j = 0; j <= jb; j++) {
+    if (fail) return;
+    if (j < jb) {  // factor step j
+      const dd r = rinv[j];
+      dd li[4], lk[4];
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const int i = ti + 16 * a, k = tk + 16 * a;
+        li[a] = (i > j && i < jb) ? dd_mul(A[i * 65 + j], r) : dd{0.0, 0.0};
+        lk[a] = (k > j && k < jb) ? dd_mul(A[k * 65 + j], r) : dd{0.0, 0.0};
+      }
+      if (tk == j % 16) {
+#pragma unroll
+        for (int a = 0; a < 4; a++) {
+          const int i = ti + 16 * a;
+          if (i > j && i < jb) A[j * 65 + i] = li[a];
+        }
+      }
+      const int p = j + 1;
+      const bool owner = p < jb && ti == p % 16 && tk == p % 16;
+      if (owner) {
+        const dd lp = dd_mul(A[p * 65 + j], r);  // = li, lk of slot p / 16 (same operation)
+        A[p * 65 + p] = dd_sub(A[p * 65 + p], dd_mul(lp, lp));
+        pivot(p);
+      }
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const int i = ti + 16 * a;
+        if (i <= j || i >= jb) continue;
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+          const int k = tk + 16 * b;
+          if (k <= j || k > i || (owner && i == p && k == p)) continue;
+          A[i * 65 + k] = dd_sub(A[i * 65 + k], dd_mul(li[a], lk[b]));
+        }
+      }
+    }
+    if (j >= 1) {  // inverse step k = j - 1 (column k of L~ and rinv[k] are final)
+      const int k = j - 1;
+      const dd rk = rinv[k];
+      dd xk[4];
+#pragma unroll
+      for (int b = 0; b < 4; b++) {
+        const int c = tk + 16 * b;
+        xk[b] = c <= k ? dd_mul(X[k * 65 + c], rk) : dd{0.0, 0.0};
+      }
+      if (ti == k % 16) {
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+          const int c = tk + 16 * b;
+          if (c <= k) XT[c * jb + k] = xk[b];
+        }
+      }
+#pragma unroll
+      for (int a = 0; a < 4; a++) {
+        const int i = ti + 16 * a;
+        if (i <= k || i >= jb) continue;
+        const dd lik = A[k * 65 + i];
+#pragma unroll
+        for (int b = 0; b < 4; b++) {
+          const int c = tk + 16 * b;
+          if (c <= k) X[i * 65 + c] = dd_sub(X[i * 65 + c], dd_mul(lik, xk[b]));
+        }
       }
     }
     __syncthreads();
-    if (fail) return;
-    for (int i = j + 1 + t; i < jb; i += 256) A[i * 65 + j] = dd_mul(A[i * 65 + j], rinv[j]);
-    __syncthreads();
-    const int m = jb - j - 1;  // trailing (i, k), j < k <= i < jb: m(m+1)/2 entries
-    for (int q = t; q < m * (m + 1) / 2; q += 256) {
-      int ii = (int)((sqrtf(8.0f * (float)q + 1.0f) - 1.0f) * 0.5f);
-      while (ii * (ii + 1) / 2 > q) ii--;
-      while ((ii + 1) * (ii + 2) / 2 <= q) ii++;
-      const int i = j + 1 + ii, k = j + 1 + (q - ii * (ii + 1) / 2);
-      A[i * 65 + k] = dd_sub(A[i * 65 + k], dd_mul(A[i * 65 + j], A[k * 65 + j]));
-    }
-    __syncthreads();
   }
-  // X = L~^-1 by row-oriented forward substitution on all columns at once
-  for (int k = 0; k < jb; k++) {
-    for (int c = t; c <= k; c += 256) X[k * 65 + c] = dd_mul(X[k * 65 + c], rinv[k]);
-    __syncthreads();
-    const int rows = jb - k - 1;
-    for (int q = t; q < rows * (k + 1); q += 256) {
-      const int i = k + 1 + q / (k + 1), c = q % (k + 1);
-      X[i * 65 + c] = dd_sub(X[i * 65 + c], dd_mul(A[i * 65 + k], X[k * 65 + c]));
-    }
-    __syncthreads();
-  }
+  if (fail) return;
   for (int q = t; q < jb * jb; q += 256) {
     const int r = q / jb, c = q % jb;
     if (c <= r) {
-      const dd v = A[r * 65 + c];
+      const dd v = c == r ? A[r * 65 + r] : A[c * 65 + r];
       const int sh = -e[kb + r];
       Lout[(kb + r) * n + kb + c] = dd_renorm(scale_pow2(v.hi, sh), scale_pow2(v.lo, sh));
+    } else {
+      XT[c * jb + r] = dd{0.0, 0.0};  // X[r][c] = 0 above the diagonal
     }
-    XT[c * jb + r] = (c <= r) ? X[r * 65 + c] : dd{0.0, 0.0};  // XT[k][j] = X[j][k]
   }
 }
 
