@@ -87,6 +87,15 @@ int hp_f128_gemm_dev(const double* a, const double* b, double* c, size_t m, size
                      int mode, void* stream);
 int hp_f128_gemm_atb_dev(const double* a, const double* b, double* c, size_t m, size_t n,
                          size_t k, int mode, void* stream);
+/* Allocation-free form of hp_f128_gemm_dev in HP_MODE_OZAKI (no counterpart
+ * in the reference): C = A * B on device pointers, with the whole workspace in
+ * a static 64 MiB device array (about m = n = k = 768 at most; larger sizes
+ * return HP_ERR_INVALID_ARG naming the bytes needed). It calls no device
+ * allocator. The first call on each device does a blocking set-up, so make
+ * it before any stream capture; calls that overlap in time share the scratch
+ * and race, so the caller must order them. */
+int hp_f128_gemm_noalloc_dev(const double* a, const double* b, double* c, size_t m, size_t n,
+                             size_t k, void* stream);
 
 /* ------------------------------------------------------------------------
  * f256 (MultiFloat<4>) GEMM

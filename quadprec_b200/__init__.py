@@ -54,6 +54,7 @@ SIGNATURES = {
     "hp_f128_gemm_atb": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int], ctypes.c_int),
     "hp_f128_gemm_dev": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int, _vp], ctypes.c_int),
     "hp_f128_gemm_atb_dev": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int, _vp], ctypes.c_int),
+    "hp_f128_gemm_noalloc_dev": ([_vp, _vp, _vp, _sz, _sz, _sz, _vp], ctypes.c_int),
     "hp_f256_gemm": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int], ctypes.c_int),
     "hp_f256_gemm_atb": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int], ctypes.c_int),
     "hp_f256_gemm_dev": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int, _vp], ctypes.c_int),

@@ -1605,3 +1605,175 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
 }
 
 }  // namespace hp
+
+// ===========================================================================
+// Allocation-free f128 Ozaki GEMM (hp_f128_gemm_noalloc_dev).
+// Some callers cannot let a library allocate device memory in the middle of
+// a call: a host that hands all device memory to its own pool at start-up,
+// a latency-bound loop where cudaMalloc / cudaFree (which may synchronise
+// the whole device) would stall its other streams, or an embedding whose
+// device memory belongs to a foreign allocator. For them this entry point
+// keeps its entire workspace in one file-scope device array of
+// NOALLOC_SCRATCH_BYTES bytes and calls no allocating routine. Every call on
+// a device shares that one array, so calls that overlap in time (two host
+// threads, or two streams) race on it: the caller must order them. The
+// first call on each device does the set-up (symbol addresses, table
+// upload, kernel attribute) and blocks the host while it does, so that
+// first call should come before any stream capture.
+// ===========================================================================
+namespace hp {
+namespace ozaki {
+constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)64 << 20;  // 64 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[NOALLOC_SCRATCH_BYTES];
+static __device__ __align__(16) CrtTable g_noalloc_crt[MAXL + 1];
+static __device__ __align__(16) uint32_t g_noalloc_status[4];
+
+struct NoAllocDev {
+  bool ready = false;
+  unsigned char* scratch = nullptr;
+  CrtTable* crt = nullptr;
+  uint32_t* status = nullptr;
+  int num_sms = 0;
+};
+static NoAllocDev g_noalloc[64];
+
+// Once per device, with that device current.
+static int noalloc_setup(NoAllocDev** out) {
+  int d = 0;
+  HP_CUDA_TRY(cudaGetDevice(&d));
+  if (d < 0 || d >= 64) {
+    set_error("device ordinal %d out of range", d);
+    return HP_ERR_UNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lk(g_dev_mu);
+  NoAllocDev& N = g_noalloc[d];
+  if (!N.ready) {
+    const HostTables& T = host_tables();
+    // the modulus table is uploaded by whichever Ozaki path runs first
+    if (!g_dev[d].ready) HP_CUDA_TRY(cudaMemcpyToSymbol(c_tab, &T.mt, sizeof(ModTable)));
+    HP_CUDA_TRY(cudaMemcpyToSymbol(g_noalloc_crt, T.crt.data(), sizeof(CrtTable) * (MAXL + 1)));
+    HP_CUDA_TRY(cudaGetSymbolAddress((void**)&N.scratch, g_noalloc_scratch));
+    HP_CUDA_TRY(cudaGetSymbolAddress((void**)&N.crt, g_noalloc_crt));
+    HP_CUDA_TRY(cudaGetSymbolAddress((void**)&N.status, g_noalloc_status));
+    HP_CUDA_TRY(cudaDeviceGetAttribute(&N.num_sms, cudaDevAttrMultiProcessorCount, d));
+    HP_CUDA_TRY(cudaFuncSetAttribute(i8_gemm_mod_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM));
+    N.ready = true;
+  }
+  *out = &N;
+  return HP_OK;
+}
+
+// Byte offset of the next 256-byte aligned region of `bytes` bytes.
+static size_t carve(size_t* off, size_t bytes) {
+  const size_t o = *off;
+  *off = round_up(o + bytes, 256);
+  return o;
+}
+
+}  // namespace ozaki
+
+// Same four phases as ozaki_dd_gemm (C = A B, row-major f128), with the
+// exponent vectors, residue planes and product residues carved from the
+// static scratch instead of allocated.
+static int ozaki_dd_gemm_noalloc(const double* a, const double* b, double* c, size_t m, size_t n, size_t k,
+                                 cudaStream_t s) {
+  using namespace ozaki;
+  NoAllocDev* N;
+  HP_TRY(noalloc_setup(&N));
+  if (m == 0 || n == 0) return HP_OK;
+  if (k == 0) {
+    HP_CUDA_TRY(cudaMemsetAsync(c, 0, m * n * 16, s));
+    return HP_OK;
+  }
+  const int beta = BETA_DD;
+  const int L = ozaki_moduli_for(k, beta);
+  if (L < 0) {
+    set_error("ozaki: k = %zu needs more moduli than the table holds", k);
+    return HP_ERR_UNSUPPORTED;
+  }
+  size_t need = SIZE_MAX, Mp = 0, Np = 0, Kp = 0, o_ea = 0, o_eb = 0, o_a = 0, o_b = 0, o_c = 0;
+  if (m <= NOALLOC_SCRATCH_BYTES && n <= NOALLOC_SCRATCH_BYTES && k <= NOALLOC_SCRATCH_BYTES) {
+    Mp = round_up(m, GB_M);
+    Np = round_up(n, GB_N);
+    Kp = round_up(k, GB_K);
+    size_t off = 0;
+    o_ea = carve(&off, Mp * sizeof(int));
+    o_eb = carve(&off, Np * sizeof(int));
+    o_a = carve(&off, (size_t)L * Mp * Kp);
+    o_b = carve(&off, (size_t)L * Np * Kp);
+    o_c = carve(&off, (size_t)L * Mp * Np);
+    need = off;
+  }
+  if (need > NOALLOC_SCRATCH_BYTES) {
+    set_error("hp_f128_gemm_noalloc_dev: %zu x %zu x %zu needs %s%zu bytes of scratch, the static scratch holds %zu",
+              m, n, k, need == SIZE_MAX ? "more than " : "", need == SIZE_MAX ? NOALLOC_SCRATCH_BYTES : need,
+              NOALLOC_SCRATCH_BYTES);
+    return HP_ERR_INVALID_ARG;
+  }
+  int* expA = reinterpret_cast<int*>(N->scratch + o_ea);
+  int* expB = reinterpret_cast<int*>(N->scratch + o_eb);
+  int8_t* ares = reinterpret_cast<int8_t*>(N->scratch + o_a);
+  int8_t* bres = reinterpret_cast<int8_t*>(N->scratch + o_b);
+  uint8_t* cres = N->scratch + o_c;
+  // what must start at zero: the exponent maxima (atomicMax) and the status
+  // word; residue and product planes are fully overwritten
+  HP_CUDA_TRY(cudaMemsetAsync(expA, 0, Mp * sizeof(int), s));
+  HP_CUDA_TRY(cudaMemsetAsync(expB, 0, Np * sizeof(int), s));
+  HP_CUDA_TRY(cudaMemsetAsync(N->status, 0, sizeof(uint32_t), s));
+  const double2* A2 = reinterpret_cast<const double2*>(a);
+  const double2* B2 = reinterpret_cast<const double2*>(b);
+  maxexp_rows_kernel<<<(unsigned)((m + 7) / 8), 256, 0, s>>>(A2, m, k, expA);
+  HP_LAUNCH_CHECK();
+  {
+    const int64_t slab = 256;
+    dim3 g((unsigned)((n + 31) / 32), (unsigned)((k + slab - 1) / slab));
+    maxexp_cols_kernel<<<g, dim3(32, 8), 0, s>>>(B2, k, n, slab, expB);
+    HP_LAUNCH_CHECK();
+  }
+  {
+    dim3 ga((unsigned)(Kp / RT_P), (unsigned)(Mp / RT_R));
+    residue_kernel<true><<<ga, 256, 0, s>>>(A2, m, k, expA, beta, L, Mp, Kp, ares);
+    HP_LAUNCH_CHECK();
+    dim3 gb((unsigned)(Kp / RT_P), (unsigned)(Np / RT_R));
+    residue_kernel<false><<<gb, 256, 0, s>>>(B2, n, k, expB, beta, L, Np, Kp, bres);
+    HP_LAUNCH_CHECK();
+  }
+  {
+    CUtensorMap mapA, mapB;
+    HP_TRY(make_map(&mapA, ares, Kp, Mp, L, GB_M));
+    HP_TRY(make_map(&mapB, bres, Kp, Np, L, GB_N));
+    const int tiles_m = (int)(Mp / GB_M), tiles_n = (int)(Np / GB_N);
+    const int grid = std::min(L * tiles_m * tiles_n, N->num_sms);
+    const int nkb = (int)(Kp / GB_K), kb_chunk = MAX_K_CHUNK / GB_K;
+    for (int c0 = 0; c0 < nkb; c0 += kb_chunk) {
+      i8_gemm_mod_kernel<<<grid, 256, GEMM_SMEM, s>>>(mapA, mapB, L, tiles_m, tiles_n, c0, std::min(nkb, c0 + kb_chunk),
+                                                       0, c0 > 0 ? 1 : 0, cres, (int64_t)Np, (int64_t)(Mp * Np), 0, 0,
+                                                       N->status);
+      HP_LAUNCH_CHECK();
+    }
+  }
+  return launch_crt_dd(cres, Mp, Np, m, n, expA, expB, beta, N->crt + L, host_tables().crt[L].nc,
+                       reinterpret_cast<double2*>(c), s);
+}
+
+}  // namespace hp
+
+extern "C" int hp_f128_gemm_noalloc_dev(const double* a, const double* b, double* c, size_t m, size_t n, size_t k,
+                                        void* stream) {
+  using namespace hp;
+  size_t t, ba, bb, bc;
+  if (mul_overflows(m, k, &t) || mul_overflows(t, 16, &ba) || mul_overflows(k, n, &t) || mul_overflows(t, 16, &bb) ||
+      mul_overflows(m, n, &t) || mul_overflows(t, 16, &bc)) {
+    set_error("matrix size overflows size_t");
+    return HP_ERR_INVALID_ARG;
+  }
+  if ((ba && !a) || (bb && !b) || (bc && !c)) {
+    set_error("null pointer with non-zero size");
+    return HP_ERR_INVALID_ARG;
+  }
+  if (((uintptr_t)a | (uintptr_t)b | (uintptr_t)c) % 16) {
+    set_error("device pointers must be 16-byte aligned");
+    return HP_ERR_INVALID_ARG;
+  }
+  return ozaki_dd_gemm_noalloc(a, b, c, m, n, k, (cudaStream_t)stream);
+}
