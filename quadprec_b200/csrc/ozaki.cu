@@ -1329,140 +1329,156 @@ __global__ void __launch_bounds__(256) crt_block_kernel(const uint8_t* __restric
   P[idx] = neg ? dd_neg(s) : s;
 }
 
-// 1/sqrt(d) to ~2^-104: one Newton step in f128 from the f64 seed.
+// 1/sqrt(d) to ~2^-103 from the f64 seed x = rsqrt(d.hi) (relative error
+// delta of a few 2^-53) by one Newton step x1 = x + x e / 2, e = 1 - d x^2.
+// e is ~delta, so it is needed only to ~2^-104 absolute: with x^2 = s + s'
+// exact (FMA), e = fma(-d.hi, s, 1) - (d.hi s' + d.lo s), each rounding
+// below 2^-104; x1 = x + c, c = x e / 2, is kept unevaluated as (x, c)
+// renormalised. The result's error is 1.5 delta^2 + O(2^-104).
 __device__ __forceinline__ dd dd_rsqrt(dd d) {
-  const double x0 = __ddiv_rn(1.0, __dsqrt_rn(d.hi));
-  const dd x = dd_from(x0);
-  const dd e = dd_sub(dd_from(1.0), dd_mul(d, dd_mul(x, x)));
-  return dd_add(x, dd_mul(x, dd_mul(e, dd_from(0.5))));
+  const double x = rsqrt(d.hi);
+  const double s = __dmul_rn(x, x), s2 = __fma_rn(x, x, -s);
+  const double t = __fma_rn(-d.hi, s, 1.0);
+  const double u = __fma_rn(d.hi, s2, __dmul_rn(d.lo, s));
+  const double c = __dmul_rn(__dmul_rn(x, __dsub_rn(t, u)), 0.5);
+  return dd_renorm(x, c);
 }
 
 // Factor the jb x jb block P[0..jb)[0..jb) (row stride jb, symmetric values)
 // in f128, write L~11 scaled back to Lout, and X^T = (L~11^-1)^T to XT.
-// Thread (ti, tk) = (t / 16, t % 16) owns the entries (i, k) with
-// i = ti (mod 16), k = tk (mod 16) (at most 4 x 4), so every column step
-// spreads its rank-1 update evenly and each thread reuses 4 row and 4 column
-// multipliers from registers. Iteration j runs factor step j and inverse
-// step j - 1 between one pair of barriers:
-//   factor:  l_i = a_ij / sqrt(d_j) for the thread's rows and columns,
-//            a_ik -= l_i l_k (k <= i); the scaled column goes to the unused
-//            upper triangle (A[j][i] = l_ij), so raw and scaled values never
-//            share an address; the owner of (j+1, j+1) updates it first and
-//            forms 1/sqrt of the next pivot while the others finish.
-//   inverse: row-oriented forward substitution for X = L~^-1:
-//            x_kc = X[k][c] / l_kk, X[i][c] -= l_ik x_kc (i > k); the final
-//            row k goes straight to XT.
+// The block is padded to 64 x 64 with the identity, so every step has the
+// same shape. X = L~^-1 is formed by row-oriented forward substitution
+// alongside the factorisation. Iteration j (one barrier):
+//   warp 31 (the critical path): column p = j + 1 gets its last update
+//     a_ip -= l_ij l_pj (i >= p); lane 0 forms 1/sqrt(a_pp) and broadcasts
+//     it; the column is scaled, l_ip = a_ip / sqrt(a_pp), into the next
+//     column buffer. Row p of X gets its last update X[p][c] -= l_pj x_jc
+//     (c <= j) and is scaled, x_pc = X[p][c] / l_pp, into the next row
+//     buffer.
+//   the bulk warps (those on the three other schedulers, warp % 4 != 3):
+//     every other live update of step j, as one index space: the trailing
+//     triangle a_ik -= l_ij l_kj (j + 2 <= k <= i; a table ordered by
+//     column makes these the first T_{j+1} slots), then the inverse
+//     rectangle X[i][c] -= l_ij x_jc (i >= j + 2, c <= j).
+//   the other warps of warp 31's scheduler: write column j and row j (the
+//     buffers warp 31 filled one iteration earlier) to Lout and XT, so the
+//     critical warp keeps its scheduler to itself.
 // Every entry sees the same f128 operations in the same order as a plain
-// right-looking column Cholesky followed by the forward substitution.
-__global__ void __launch_bounds__(256) chol_inv_block_kernel(const dd* __restrict__ P, int jb, int64_t kb, int64_t n,
-                                                             const int* __restrict__ e, dd* __restrict__ Lout,
-                                                             dd* __restrict__ XT, RnsErr* err) {
+// right-looking column Cholesky and row-oriented substitution.
+constexpr int CI_THREADS = 1024;
+constexpr int CI_BULK = CI_THREADS / 4 * 3;     // warps with warp % 4 != 3
+constexpr int CI_OUT = CI_THREADS / 4 - 32;     // the other warps with warp % 4 == 3
+__global__ void __launch_bounds__(CI_THREADS) chol_inv_block_kernel(const dd* __restrict__ P, int jb, int64_t kb,
+                                                                    int64_t n, const int* __restrict__ e,
+                                                                    dd* __restrict__ Lout, dd* __restrict__ XT,
+                                                                    RnsErr* err) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   dd* A = reinterpret_cast<dd*>(sm_raw);  // [64][65]
   dd* X = A + 64 * 65;                    // [64][65]
-  __shared__ dd rinv[64];
+  __shared__ dd Lc[2][64], xs[2][64];     // scaled column j of L~ / row j of X, double-buffered
+  __shared__ dd ldiag[64];                // l_jj = sqrt(a_jj)
+  __shared__ uint16_t tab[2016];          // (i << 6) | k, column k = 63..1, rows i = k..63
+  __shared__ uint64_t kmagic[64];         // ceil(2^32 / (j + 1)): q / (j + 1) = (q kmagic[j]) >> 32, q < 2^12
+  __shared__ int esh[64];
   __shared__ int fail;
-  const int t = threadIdx.x, ti = t / 16, tk = t % 16;
+  const int t = threadIdx.x, lane = t % 32, warp = t / 32;
+  const bool critical = warp == CI_THREADS / 32 - 1;
+  const bool bulk = warp % 4 != 3;
+  const int bt = (warp / 4 * 3 + warp % 4) * 32 + lane;  // bulk thread index
+  const int ot = (warp / 4) * 32 + lane;                 // index among the output warps (warp % 4 == 3)
   if (err->flag) return;
-  for (int q = t; q < jb * jb; q += 256) {
-    const int r = q / jb, c = q % jb;
-    A[r * 65 + c] = P[q];
-    X[r * 65 + c] = dd_from(r == c ? 1.0 : 0.0);
+  if (t < 64) {
+    kmagic[t] = ((1ull << 32) + (uint64_t)t) / (uint64_t)(t + 1);
+    esh[t] = t < jb ? e[kb + t] : 0;
   }
   if (t == 0) fail = 0;
+#pragma unroll 4
+  for (int q = t; q < 64 * 64; q += CI_THREADS) {
+    const int r = q / 64, c = q % 64;
+    A[r * 65 + c] = (r < jb && c < jb) ? P[r * jb + c] : dd_from(r == c ? 1.0 : 0.0);
+    X[r * 65 + c] = dd_from(r == c ? 1.0 : 0.0);
+    if (c >= 1 && r >= c) tab[(63 - c) * (64 - c) / 2 + (r - c)] = (uint16_t)((r << 6) | c);
+    if (c > r && c < jb) XT[c * jb + r] = dd{0.0, 0.0};  // X[r][c] = 0 above the diagonal
+  }
   __syncthreads();
-  auto pivot = [&](int j) {  // A[j][j] <- sqrt(d), rinv[j] <- 1/sqrt(d)
-    const dd d = A[j * 65 + j];
+  // Pivot p on warp 31, branch-free: every lane forms r = 1/sqrt(d) from
+  // the same d (so no broadcast is needed); a failure is flagged once.
+  auto pivot = [&](int p, dd d, dd& r) -> bool {
     if (!(d.hi > 0.0)) {
-      fail = 1;
-      err->flag = 1;
-      err->pivot = kb + j;
-    } else {
-      const dd r = dd_rsqrt(d);
-      A[j * 65 + j] = dd_mul(d, r);
-      rinv[j] = r;
+      if (lane == 0) {
+        fail = 1;
+        err->flag = 1;
+        err->pivot = kb + p;
+      }
+      return false;
     }
+    r = dd_rsqrt(d);
+    if (lane == 0) ldiag[p] = dd_mul(d, r);
+    return true;
   };
-  if (t == 0) pivot(0);
-  __syncthreads();
-  for (int j = 0; j <= jb; j++) {
-    if (fail) return;
-    if (j < jb) {  // factor step j
-      const dd r = rinv[j];
-      dd li[4], lk[4];
-#pragma unroll
-      for (int a = 0; a < 4; a++) {
-        const int i = ti + 16 * a, k = tk + 16 * a;
-        li[a] = (i > j && i < jb) ? dd_mul(A[i * 65 + j], r) : dd{0.0, 0.0};
-        lk[a] = (k > j && k < jb) ? dd_mul(A[k * 65 + j], r) : dd{0.0, 0.0};
-      }
-      if (tk == j % 16) {
-#pragma unroll
-        for (int a = 0; a < 4; a++) {
-          const int i = ti + 16 * a;
-          if (i > j && i < jb) A[j * 65 + i] = li[a];
-        }
-      }
-      const int p = j + 1;
-      const bool owner = p < jb && ti == p % 16 && tk == p % 16;
-      if (owner) {
-        const dd lp = dd_mul(A[p * 65 + j], r);  // = li, lk of slot p / 16 (same operation)
-        A[p * 65 + p] = dd_sub(A[p * 65 + p], dd_mul(lp, lp));
-        pivot(p);
-      }
-#pragma unroll
-      for (int a = 0; a < 4; a++) {
-        const int i = ti + 16 * a;
-        if (i <= j || i >= jb) continue;
-#pragma unroll
-        for (int b = 0; b < 4; b++) {
-          const int k = tk + 16 * b;
-          if (k <= j || k > i || (owner && i == p && k == p)) continue;
-          A[i * 65 + k] = dd_sub(A[i * 65 + k], dd_mul(li[a], lk[b]));
-        }
-      }
+  // column j of L~ and row j of X, from the buffers, to Lout and XT
+  auto write_out = [&](int j, int buf) {
+    if (j >= jb) return;
+    for (int i = j + ot; i < jb; i += CI_OUT) {
+      const dd v = i == j ? ldiag[j] : Lc[buf][i];
+      const int sh = -esh[i];
+      Lout[(kb + i) * n + kb + j] = dd_renorm(scale_pow2(v.hi, sh), scale_pow2(v.lo, sh));
     }
-    if (j >= 1) {  // inverse step k = j - 1 (column k of L~ and rinv[k] are final)
-      const int k = j - 1;
-      const dd rk = rinv[k];
-      dd xk[4];
-#pragma unroll
-      for (int b = 0; b < 4; b++) {
-        const int c = tk + 16 * b;
-        xk[b] = c <= k ? dd_mul(X[k * 65 + c], rk) : dd{0.0, 0.0};
+    for (int c = ot; c <= j; c += CI_OUT) XT[c * jb + j] = xs[buf][c];
+  };
+  if (critical) {  // step 0: pivot 0, column 0, row 0
+    dd r = {0.0, 0.0};
+    if (pivot(0, A[0], r)) {
+      for (int i = 1 + lane; i < 64; i += 32) Lc[0][i] = dd_mul(A[i * 65], r);
+      if (lane == 0) xs[0][0] = r;
+    }
+  }
+  __syncthreads();
+  for (int j = 0; j < 63; j++) {
+    if (fail) return;
+    const int cur = j & 1, nxt = cur ^ 1, p = j + 1;
+    if (critical) {
+      // column p: last update, pivot, scale; row p of X: last update, scale.
+      // Indices are clamped so that all four chains run unconditionally
+      // (interleaved); only the stores are predicated.
+      const dd lpj = Lc[cur][p];
+      const int i0 = p + lane, i1 = p + 32 + lane, c0 = lane, c1 = 32 + lane;
+      const int i0c = min(i0, 63), i1c = min(i1, 63), c0c = c0 <= j ? c0 : 0, c1c = c1 <= j ? c1 : 0;
+      const dd a0 = dd_sub(A[i0c * 65 + p], dd_mul(Lc[cur][i0c], lpj));
+      const dd a1 = dd_sub(A[i1c * 65 + p], dd_mul(Lc[cur][i1c], lpj));
+      const dd x0 = dd_sub(X[p * 65 + c0c], dd_mul(lpj, xs[cur][c0c]));
+      const dd x1 = dd_sub(X[p * 65 + c1c], dd_mul(lpj, xs[cur][c1c]));
+      const dd d = {__shfl_sync(0xffffffffu, a0.hi, 0), __shfl_sync(0xffffffffu, a0.lo, 0)};  // a_pp (lane 0)
+      dd r;
+      if (pivot(p, d, r)) {
+        const dd s0 = dd_mul(a0, r), s1 = dd_mul(a1, r), y0 = dd_mul(x0, r), y1 = dd_mul(x1, r);
+        if (i0 < 64 && i0 > p) Lc[nxt][i0] = s0;
+        if (i1 < 64) Lc[nxt][i1] = s1;
+        if (c0 <= p) xs[nxt][c0] = c0 == p ? r : y0;
+        if (c1 <= p) xs[nxt][c1] = c1 == p ? r : y1;
       }
-      if (ti == k % 16) {
-#pragma unroll
-        for (int b = 0; b < 4; b++) {
-          const int c = tk + 16 * b;
-          if (c <= k) XT[c * jb + k] = xk[b];
-        }
+    } else if (bulk) {
+      const int Tn = (62 - j) * (63 - j) / 2;  // trailing slots with column >= j + 2
+      const int total = Tn + (62 - j) * (j + 1);
+      const uint64_t magic = kmagic[j];
+      int u = bt;
+      for (; u < Tn; u += CI_BULK) {
+        const int ent = tab[u], i = ent >> 6, kk = ent & 63;
+        A[i * 65 + kk] = dd_sub(A[i * 65 + kk], dd_mul(Lc[cur][i], Lc[cur][kk]));
       }
-#pragma unroll
-      for (int a = 0; a < 4; a++) {
-        const int i = ti + 16 * a;
-        if (i <= k || i >= jb) continue;
-        const dd lik = A[k * 65 + i];
-#pragma unroll
-        for (int b = 0; b < 4; b++) {
-          const int c = tk + 16 * b;
-          if (c <= k) X[i * 65 + c] = dd_sub(X[i * 65 + c], dd_mul(lik, xk[b]));
-        }
+      for (; u < total; u += CI_BULK) {
+        const int q = u - Tn;
+        const int ii = (int)(((uint64_t)q * magic) >> 32), c = q - ii * (j + 1);
+        const int i = j + 2 + ii;
+        X[i * 65 + c] = dd_sub(X[i * 65 + c], dd_mul(Lc[cur][i], xs[cur][c]));
       }
+    } else {
+      write_out(j, cur);
     }
     __syncthreads();
   }
   if (fail) return;
-  for (int q = t; q < jb * jb; q += 256) {
-    const int r = q / jb, c = q % jb;
-    if (c <= r) {
-      const dd v = c == r ? A[r * 65 + r] : A[c * 65 + r];
-      const int sh = -e[kb + r];
-      Lout[(kb + r) * n + kb + c] = dd_renorm(scale_pow2(v.hi, sh), scale_pow2(v.lo, sh));
-    } else {
-      XT[c * jb + r] = dd{0.0, 0.0};  // X[r][c] = 0 above the diagonal
-    }
-  }
+  if (!bulk && !critical) write_out(63, 63 & 1);
 }
 
 // Q = P21 X^T for the panel: Q[r][c] = sum_k P21[r][k] X[c][k] (k < jb),
@@ -1570,7 +1586,7 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
     }
 #undef HP_CRTB
     HP_LAUNCH_CHECK();
-    chol_inv_block_kernel<<<1, 256, inv_smem, s>>>(P.as<dd>(), jb, (int64_t)kb, (int64_t)n, ebuf.as<int>(), Lout,
+    chol_inv_block_kernel<<<1, CI_THREADS, inv_smem, s>>>(P.as<dd>(), jb, (int64_t)kb, (int64_t)n, ebuf.as<int>(), Lout,
                                                    XT.as<dd>(), err.as<RnsErr>());
     HP_LAUNCH_CHECK();
     if (R <= (size_t)jb) break;
