@@ -72,6 +72,8 @@ namespace hp {
 int dd_block_inverses(const double* L, size_t n, double* Xall, cudaStream_t s);
 size_t dd_block_inverses_bytes(size_t n);
 int dd_trsv_blocked(const double* L, const double* Xall, double* v, size_t n, bool upper_t, cudaStream_t s);
+// HP_ERR_TIMEOUT if a wavefront wait of dd_trsv_blocked gave up (synchronises s).
+int dd_trsv_status(const double* Xall, size_t n, cudaStream_t s);
 }  // namespace hp
 
 namespace hp {

@@ -191,6 +191,7 @@ int spd_refined(const double* S, const double* b, size_t n, int mode, double tol
   }
   cudaEventRecord(e2, s);
   cudaEventSynchronize(e2);
+  HP_TRY(dd_trsv_status(Xinv.as<double>(), n, s));
   float fm = 0, tm = 0;
   cudaEventElapsedTime(&fm, e0, e1);
   cudaEventElapsedTime(&tm, e0, e2);

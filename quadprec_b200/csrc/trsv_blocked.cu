@@ -1,22 +1,26 @@
 // Blocked f128 triangular solves for refinement loops: L y = b and L^T x = y
-// with the inverses of the 64 x 64 diagonal blocks of L precomputed once per
-// factorisation. One cooperative launch sweeps the block columns:
-//   forward:  y_k = X_k (b_k - sum_{j<k} L_kj y_j)     (X_k = L_kk^-1)
+// with the inverses X_k = L_kk^-1 of the 64 x 64 diagonal blocks of L
+// precomputed once per factorisation:
+//   forward:  y_k = X_k (b_k - sum_{j<k} L_kj y_j)
 //   backward: x_k = X_k^T (y_k - sum_{j>k} L_jk^T x_j)
-// Step k: CTA 0 applies X_k to block k (4 threads per output, partial dd
-// sums combined in order); grid sync; every warp updates its rows of the
-// remaining right-hand side with block column k; grid sync.
+// One launch, one CTA per block row, no grid-wide barrier: CTAs take block
+// rows in dependency order from a ticket counter; each accumulates the
+// products with the solved blocks as their ready flags appear (its L tile is
+// loaded before the wait), then applies X_k, stores its block and raises its
+// own flag. A CTA only ever waits for CTAs that took earlier tickets, so the
+// wavefront makes progress whatever the residency. Every wait is bounded
+// (2 s of global time, or an abort raised by another CTA) and a CTA that
+// gives up records DEV_STATUS_TIMEOUT in the status word the host reads.
 // Same operations as the reference's substitutions (crates/quad/src/
 // linalg.rs:99-120) grouped by blocks, in another order: f128-level accuracy,
 // not bit-identical. Used where a solve is repeated (refinement), with the
 // reference-order kernels in solve.cu kept for the single-solve entry points.
-#include <cooperative_groups.h>
+#include <atomic>
 
 #include "hp_arith.cuh"
 #include "hp_runtime.cuh"
 #include "kernels.cuh"
-
-namespace cg = cooperative_groups;
+#include "sm100_ptx.cuh"
 
 namespace hp {
 namespace {
@@ -57,64 +61,116 @@ __global__ void __launch_bounds__(256) block_inverse_kernel(const dd* __restrict
   for (int q = t; q < TB * TB; q += 256) out[q] = X[q / TB][q % TB];
 }
 
-template <bool UPPER_T>
-__global__ void __launch_bounds__(256) trsv_blocked_kernel(const dd* __restrict__ L, const dd* __restrict__ Xall,
-                                                           dd* __restrict__ v, int64_t n) {
-  cg::grid_group grid = cg::this_grid();
-  __shared__ dd part[TB][4];
-  __shared__ dd vk[TB];
-  const int t = threadIdx.x, lane = t % 32;
-  const int nblk = (int)((n + TB - 1) / TB);
-  const int64_t gwarp = ((int64_t)blockIdx.x * blockDim.x + t) / 32;
-  const int64_t nwarps = (int64_t)gridDim.x * blockDim.x / 32;
-  for (int s = 0; s < nblk; s++) {
-    const int k = UPPER_T ? nblk - 1 - s : s;
-    const int64_t k0 = (int64_t)k * TB;
-    const int jb = (int)min((int64_t)TB, n - k0);
-    if (blockIdx.x == 0) {
-      // block k of v <- X_k v_k (forward) or X_k^T v_k (backward)
-      const dd* X = Xall + (size_t)k * TB * TB;
-      const int r = t / 4, q = t % 4;
-      dd acc = dd{0.0, 0.0};
-      if (r < jb)
-        for (int c = q; c < jb; c += 4) {
-          const dd xv = UPPER_T ? X[c * TB + r] : X[r * TB + c];
-          acc = dd_add(acc, dd_mul(xv, v[k0 + c]));
-        }
-      part[r][q] = acc;
-      __syncthreads();
-      if (q == 0 && r < jb) vk[r] = dd_add(dd_add(part[r][0], part[r][1]), dd_add(part[r][2], part[r][3]));
-      __syncthreads();
-      if (t < jb) v[k0 + t] = vk[t];
-    }
-    grid.sync();
-    // update the remaining rows with block column k
-    const int64_t lo = UPPER_T ? 0 : k0 + jb, hi = UPPER_T ? k0 : n;
-    for (int64_t i = lo + gwarp; i < hi; i += nwarps) {
-      dd acc = dd{0.0, 0.0};
-      for (int c = lane; c < jb; c += 32) {
-        const dd lv = UPPER_T ? L[(k0 + c) * n + i] : L[i * n + k0 + c];
-        acc = dd_add(acc, dd_mul(lv, v[k0 + c]));
-      }
-#pragma unroll
-      for (int o = 16; o; o >>= 1) {
-        dd other;
-        other.hi = __shfl_down_sync(0xffffffffu, acc.hi, o);
-        other.lo = __shfl_down_sync(0xffffffffu, acc.lo, o);
-        if (lane < o) acc = dd_add(acc, other);
-      }
-      if (lane == 0) v[i] = dd_sub(v[i], acc);
-    }
-    grid.sync();
-  }
+// Wavefront bookkeeping behind the inverses in the same workspace.
+struct TrsvSync {
+  unsigned ticket;  // next block row to hand out (reset before each launch)
+  unsigned abort;   // a CTA gave up: the others stop waiting
+  unsigned status;  // DEV_STATUS_* bits, read by the host
+  unsigned pad;
+};
+inline size_t nblocks(size_t n) { return (n + TB - 1) / TB; }
+inline size_t inverses_bytes(size_t n) { return nblocks(n) * TB * TB * 16; }
+
+__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_gpu(unsigned* p, unsigned v) {
+  asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ dd ld_dd_cg(const dd* p) {
+  const double2 v = __ldcg(reinterpret_cast<const double2*>(p));
+  return dd{v.x, v.y};
 }
 
-int coop_grid(const void* fn, int threads) {
-  int dev = 0, sms = 0, per_sm = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, 0);
-  return sms * (per_sm > 0 ? (per_sm > 2 ? 2 : per_sm) : 1);
+// Block row k: thread (r, q) = (t / 4, t % 4) owns row r of the block and
+// the columns c = q (mod 4) of each 64 x 64 tile it multiplies.
+constexpr uint64_t TRSV_WAIT_NS = 2000000000ull;
+template <bool UPPER_T>
+__global__ void __launch_bounds__(256) trsv_wave_kernel(const dd* __restrict__ L, const dd* __restrict__ Xall,
+                                                        dd* v, int64_t n, int nblk, TrsvSync* sync,
+                                                        unsigned* flags, unsigned epoch) {
+  __shared__ unsigned my;
+  __shared__ int bad;
+  __shared__ dd vj[TB], sv[TB];
+  __shared__ dd part[TB][4];
+  const int t = threadIdx.x, r = t / 4, q = t % 4;
+  if (t == 0) {
+    my = atomicAdd(&sync->ticket, 1u);
+    bad = 0;
+  }
+  __syncthreads();
+  const int s = (int)my;
+  if (s >= nblk) return;
+  const int k = UPPER_T ? nblk - 1 - s : s;
+  const int64_t k0 = (int64_t)k * TB;
+  const int jb = (int)min((int64_t)TB, n - k0);
+  // X_k row r (forward) or column r (backward), loaded before any wait
+  const dd* X = Xall + (size_t)k * TB * TB;
+  dd xr[TB / 4];
+#pragma unroll
+  for (int m = 0; m < TB / 4; m++) {
+    const int c = q + 4 * m;
+    xr[m] = UPPER_T ? X[c * TB + r] : X[r * TB + c];
+  }
+  dd acc0 = {0.0, 0.0}, acc1 = {0.0, 0.0};
+  for (int d = 0; d < s; d++) {
+    const int j = UPPER_T ? nblk - 1 - d : d;
+    const int64_t j0 = (int64_t)j * TB;
+    const int jbj = (int)min((int64_t)TB, n - j0);
+    dd lv[TB / 4];
+#pragma unroll
+    for (int m = 0; m < TB / 4; m++) {
+      const int c = q + 4 * m;
+      const bool in = r < jb && c < jbj;
+      lv[m] = in ? (UPPER_T ? L[(j0 + c) * n + k0 + r] : L[(k0 + r) * n + j0 + c]) : dd{0.0, 0.0};
+    }
+    if (t == 0) {
+      const uint64_t t0 = sm100::globaltimer_ns();
+      while (ld_acquire_gpu(flags + j) != epoch) {
+        if (ld_acquire_gpu(&sync->abort) || sm100::globaltimer_ns() - t0 > TRSV_WAIT_NS) {
+          atomicOr(&sync->status, (unsigned)DEV_STATUS_TIMEOUT);
+          atomicExch(&sync->abort, 1u);
+          bad = 1;
+          break;
+        }
+      }
+    }
+    __syncthreads();
+    if (bad) return;
+    if (t < TB) vj[t] = t < jbj ? ld_dd_cg(v + j0 + t) : dd{0.0, 0.0};
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < TB / 4; m += 2) {
+      acc0 = dd_add(acc0, dd_mul(lv[m], vj[q + 4 * m]));
+      acc1 = dd_add(acc1, dd_mul(lv[m + 1], vj[q + 4 * m + 4]));
+    }
+    __syncthreads();  // vj is rewritten by the next dependency
+  }
+  part[r][q] = dd_add(acc0, acc1);
+  __syncthreads();
+  if (q == 0)
+    sv[r] = r < jb ? dd_sub(ld_dd_cg(v + k0 + r), dd_add(dd_add(part[r][0], part[r][1]), dd_add(part[r][2], part[r][3])))
+                   : dd{0.0, 0.0};
+  __syncthreads();
+  acc0 = acc1 = dd{0.0, 0.0};
+#pragma unroll
+  for (int m = 0; m < TB / 4; m += 2) {
+    acc0 = dd_add(acc0, dd_mul(xr[m], sv[q + 4 * m]));
+    acc1 = dd_add(acc1, dd_mul(xr[m + 1], sv[q + 4 * m + 4]));
+  }
+  part[r][q] = dd_add(acc0, acc1);
+  __syncthreads();
+  if (q == 0 && r < jb) {
+    v[k0 + r] = dd_add(dd_add(part[r][0], part[r][1]), dd_add(part[r][2], part[r][3]));
+    __threadfence();
+  }
+  __syncthreads();
+  if (t == 0) {
+    __threadfence();
+    st_release_gpu(flags + k, epoch);
+  }
 }
 
 }  // namespace
@@ -123,24 +179,50 @@ int dd_block_inverses(const double* L, size_t n, double* Xall, cudaStream_t s) {
   if (n == 0) return HP_OK;
   const int smem = 2 * TB * (TB + 1) * 16;
   HP_CUDA_TRY(cudaFuncSetAttribute(block_inverse_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  block_inverse_kernel<<<(unsigned)((n + TB - 1) / TB), 256, smem, s>>>(reinterpret_cast<const dd*>(L), n,
-                                                                        reinterpret_cast<dd*>(Xall));
+  block_inverse_kernel<<<(unsigned)nblocks(n), 256, smem, s>>>(reinterpret_cast<const dd*>(L), n,
+                                                              reinterpret_cast<dd*>(Xall));
+  HP_LAUNCH_CHECK();
+  // wavefront bookkeeping: ticket, abort, status and the ready flags start at 0
+  HP_CUDA_TRY(cudaMemsetAsync(reinterpret_cast<char*>(Xall) + inverses_bytes(n), 0,
+                              sizeof(TrsvSync) + nblocks(n) * sizeof(unsigned), s));
+  return HP_OK;
+}
+
+size_t dd_block_inverses_bytes(size_t n) {
+  return inverses_bytes(n) + sizeof(TrsvSync) + (nblocks(n) * sizeof(unsigned) + 15) / 16 * 16;
+}
+
+int dd_trsv_blocked(const double* L, const double* Xall, double* v, size_t n, bool upper_t, cudaStream_t s) {
+  if (n == 0) return HP_OK;
+  static std::atomic<unsigned> epochs{0};
+  unsigned epoch = ++epochs;
+  if (epoch == 0) epoch = ++epochs;  // 0 is the flags' initial value
+  char* tail = const_cast<char*>(reinterpret_cast<const char*>(Xall)) + inverses_bytes(n);
+  TrsvSync* sync = reinterpret_cast<TrsvSync*>(tail);
+  unsigned* flags = reinterpret_cast<unsigned*>(tail + sizeof(TrsvSync));
+  HP_CUDA_TRY(cudaMemsetAsync(&sync->ticket, 0, sizeof(unsigned), s));
+  const int nblk = (int)nblocks(n);
+  const dd* Lp = reinterpret_cast<const dd*>(L);
+  const dd* Xp = reinterpret_cast<const dd*>(Xall);
+  dd* vp = reinterpret_cast<dd*>(v);
+  if (upper_t)
+    trsv_wave_kernel<true><<<nblk, 256, 0, s>>>(Lp, Xp, vp, (int64_t)n, nblk, sync, flags, epoch);
+  else
+    trsv_wave_kernel<false><<<nblk, 256, 0, s>>>(Lp, Xp, vp, (int64_t)n, nblk, sync, flags, epoch);
   HP_LAUNCH_CHECK();
   return HP_OK;
 }
 
-size_t dd_block_inverses_bytes(size_t n) { return ((n + TB - 1) / TB) * TB * TB * 16; }
-
-int dd_trsv_blocked(const double* L, const double* Xall, double* v, size_t n, bool upper_t, cudaStream_t s) {
+int dd_trsv_status(const double* Xall, size_t n, cudaStream_t s) {
   if (n == 0) return HP_OK;
-  const dd* Lp = reinterpret_cast<const dd*>(L);
-  const dd* Xp = reinterpret_cast<const dd*>(Xall);
-  dd* vp = reinterpret_cast<dd*>(v);
-  int64_t nn = (int64_t)n;
-  void* args[] = {(void*)&Lp, (void*)&Xp, (void*)&vp, (void*)&nn};
-  const void* fn = upper_t ? (const void*)trsv_blocked_kernel<true> : (const void*)trsv_blocked_kernel<false>;
-  const int grid = coop_grid(fn, 256);
-  HP_CUDA_TRY(cudaLaunchCooperativeKernel(fn, grid, 256, args, 0, s));
+  const TrsvSync* sync = reinterpret_cast<const TrsvSync*>(reinterpret_cast<const char*>(Xall) + inverses_bytes(n));
+  unsigned h = 0;
+  HP_CUDA_TRY(cudaMemcpyAsync(&h, &sync->status, sizeof(h), cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  if (h & DEV_STATUS_TIMEOUT) {
+    set_error("triangular solve: a block wait timed out");
+    return HP_ERR_TIMEOUT;
+  }
   return HP_OK;
 }
 
