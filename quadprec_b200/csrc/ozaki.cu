@@ -291,8 +291,9 @@ __device__ __forceinline__ void int_digits(double v, int32_t* d) {
 
 // Residues of the scaled operand. Logical operand is R x K (row r, reduction
 // index p); element (r, p) is src[r*K + p] (P_CONTIG) or src[p*R + r].
-// Writes out[l][r][p] (int8), row stride Kp, plane stride Rp*Kp, for all
-// r < Rp, p < Kp (zero outside R x K).
+// Writes out[l][r][p] (int8), row stride ld, plane stride plane_stride, for
+// every (r, p) the grid covers (64 gridDim.y rows, 32 gridDim.x columns;
+// zero outside R x K).
 // Block tile: 64 rows x 32 p; each thread owns one row and 8 consecutive p,
 // so its 8 residues of one modulus pack into two 32-bit words.
 //   P_CONTIG: thread reads 8 consecutive f128 (128 B) and stores its 8 bytes
@@ -323,8 +324,8 @@ __device__ __forceinline__ uint32_t balanced_byte(const int32_t* D, int l, int m
 }
 template <bool P_CONTIG>
 __global__ void __launch_bounds__(256) residue_kernel(const double2* __restrict__ src, int64_t R, int64_t K,
-                                                      const int* __restrict__ expf, int beta, int L, int64_t Rp,
-                                                      int64_t Kp, int8_t* __restrict__ out) {
+                                                      const int* __restrict__ expf, int beta, int L, int64_t ld,
+                                                      int64_t plane_stride, int8_t* __restrict__ out) {
   __shared__ __align__(16) uint32_t T[2][RT_R][RT_P / 4 + 1];
   const int t = threadIdx.x;
   const int rl = P_CONTIG ? t / 4 : t % 64;
@@ -347,7 +348,7 @@ __global__ void __launch_bounds__(256) residue_kernel(const double2* __restrict_
       }
     }
   }
-  int8_t* const base = out + (size_t)(blockIdx.y * RT_R) * Kp + blockIdx.x * RT_P;
+  int8_t* const base = out + (size_t)(blockIdx.y * RT_R) * ld + blockIdx.x * RT_P;
   for (int l = 0; l < L; l++) {
     const int m = c_tab.mod[l];
     uint32_t w0 = 0, w1 = 0;
@@ -356,9 +357,9 @@ __global__ void __launch_bounds__(256) residue_kernel(const double2* __restrict_
       w0 |= balanced_byte(dig[e], l, m) << (8 * e);
       w1 |= balanced_byte(dig[e + 4], l, m) << (8 * e);
     }
-    int8_t* plane = base + (size_t)l * Rp * Kp;
+    int8_t* plane = base + (size_t)l * plane_stride;
     if (P_CONTIG) {
-      *reinterpret_cast<uint2*>(plane + (size_t)rl * Kp + 8 * oct) = make_uint2(w0, w1);
+      *reinterpret_cast<uint2*>(plane + (size_t)rl * ld + 8 * oct) = make_uint2(w0, w1);
     } else {
       T[l & 1][rl][2 * oct] = w0;
       T[l & 1][rl][2 * oct + 1] = w1;
@@ -366,7 +367,7 @@ __global__ void __launch_bounds__(256) residue_kernel(const double2* __restrict_
       if (t < 2 * RT_R) {
         const int row = t / 2, half = t % 2;
         const uint32_t* src_w = &T[l & 1][row][4 * half];
-        *reinterpret_cast<uint4*>(plane + (size_t)row * Kp + 16 * half) =
+        *reinterpret_cast<uint4*>(plane + (size_t)row * ld + 16 * half) =
             make_uint4(src_w[0], src_w[1], src_w[2], src_w[3]);
       }
     }
@@ -378,35 +379,50 @@ __global__ void __launch_bounds__(256) residue_kernel(const double2* __restrict_
 //   cres[l][i][j] = (sum_p Ares[l][i][p] * Bres[l][j][p]) mod m_l   (uint8)
 // Persistent, warp-specialised: warp 0 = TMA producer, warp 1 = MMA issuer,
 // warp 2 = TMEM owner, warps 4-7 = epilogue (TMEM -> residue bytes).
-// Tile 128 x 256, K-block 128 bytes, 4-stage smem ring, 2 TMEM accumulators.
+// Tile 128 x BN (GemmCfg), K-block 128 bytes, smem ring, 2 TMEM accumulators.
 // ---------------------------------------------------------------------------
 constexpr int GB_M = 128, GB_N = 256, GB_K = 128, GSTAGES = 4;
 constexpr int A_STAGE = GB_M * GB_K, B_STAGE = GB_N * GB_K, STAGE_BYTES = A_STAGE + B_STAGE;
 constexpr int GEMM_SMEM = GSTAGES * STAGE_BYTES + 1024 + 256;
 constexpr int MAX_K_CHUNK = 65536;  // |int32 accumulator| <= 2^16 * 2^14 = 2^30
 
+// Tile shapes: BN = 256 (4-stage ring, the general GEMM) or BN = 64 (8-stage
+// ring, for the 64-column panels of the residue-domain Cholesky). The
+// accumulators take 2 * BN TMEM columns (two tiles in flight).
+template <int BN>
+struct GemmCfg {
+  static constexpr int STAGES = BN >= 256 ? 4 : 8;
+  static constexpr int B_STAGE = BN * GB_K;
+  static constexpr int STAGE_BYTES = A_STAGE + B_STAGE;
+  static constexpr int SMEM = STAGES * STAGE_BYTES + 1024 + 256;
+  static constexpr int TMEM_COLS = 2 * BN;
+};
+static_assert(GemmCfg<256>::SMEM == GEMM_SMEM, "BN = 256 keeps the general GEMM's layout");
+
+template <int BN>
 __global__ void __launch_bounds__(256, 1)
     i8_gemm_mod_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int L,
                        int tiles_m, int tiles_n, int kb0, int kb1, int kb_off_b, int acc_mode,
                        uint8_t* __restrict__ cres,
                        int64_t ldc, int64_t plane, int64_t c_row0, int64_t c_col0, uint32_t* status) {
   using namespace sm100;
+  using Cfg = GemmCfg<BN>;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
   uint8_t* smem = smem_raw + pad;
   uint8_t* sA = smem;
-  uint8_t* sB = smem + GSTAGES * A_STAGE;
-  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + GSTAGES * STAGE_BYTES);
+  uint8_t* sB = smem + Cfg::STAGES * A_STAGE;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + Cfg::STAGES * Cfg::STAGE_BYTES);
   uint64_t* full = bars;
-  uint64_t* empty = bars + GSTAGES;
-  uint64_t* tfull = bars + 2 * GSTAGES;
+  uint64_t* empty = bars + Cfg::STAGES;
+  uint64_t* tfull = bars + 2 * Cfg::STAGES;
   uint64_t* tempty = tfull + 2;
   uint64_t* drain = tempty + 2;
   uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
 
   const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
   if (threadIdx.x == 0) {
-    for (int s = 0; s < GSTAGES; s++) {
+    for (int s = 0; s < Cfg::STAGES; s++) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
@@ -422,7 +438,7 @@ __global__ void __launch_bounds__(256, 1)
     prefetch_tmap(&mapB);
   }
   if (warp == 2) {
-    tmem_alloc(tmem_slot, 512);
+    tmem_alloc(tmem_slot, Cfg::TMEM_COLS);
     tmem_relinquish();
   }
   tc_fence_before();
@@ -438,8 +454,8 @@ __global__ void __launch_bounds__(256, 1)
     if (lane == 0) {
       uint32_t stage = 0, phase = 0;
       bool ok = true;
-      int filled_phase[GSTAGES];
-      for (int s = 0; s < GSTAGES; s++) filled_phase[s] = -1;
+      int filled_phase[Cfg::STAGES];
+      for (int s = 0; s < Cfg::STAGES; s++) filled_phase[s] = -1;
       for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x) {
         const int l = t / per_l, rem = t % per_l, tm = rem / tiles_n, tn = rem % tiles_n;
         for (int kb = 0; kb < nkb; kb++) {
@@ -447,18 +463,18 @@ __global__ void __launch_bounds__(256, 1)
             ok = false;
             break;
           }
-          mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
+          mbar_arrive_expect_tx(&full[stage], Cfg::STAGE_BYTES);
           tma_load_3d(sA + stage * A_STAGE, &mapA, &full[stage], (kb0 + kb) * GB_K, tm * GB_M, l);
-          tma_load_3d(sB + stage * B_STAGE, &mapB, &full[stage], (kb0 + kb + kb_off_b) * GB_K, tn * GB_N, l);
+          tma_load_3d(sB + stage * Cfg::B_STAGE, &mapB, &full[stage], (kb0 + kb + kb_off_b) * GB_K, tn * BN, l);
           filled_phase[stage] = (int)phase;
-          if (++stage == GSTAGES) {
+          if (++stage == Cfg::STAGES) {
             stage = 0;
             phase ^= 1;
           }
         }
       }
       if (!ok) {  // let loads still in flight land before the CTA exits
-        for (int s = 0; s < GSTAGES; s++)
+        for (int s = 0; s < Cfg::STAGES; s++)
           if (filled_phase[s] >= 0) mbar_wait(&full[s], (uint32_t)filled_phase[s], status, DEV_STATUS_TIMEOUT, 100000000ull);
       }
     }
@@ -467,7 +483,7 @@ __global__ void __launch_bounds__(256, 1)
       uint32_t stage = 0, phase = 0, it = 0;
       bool ok = true;
       bool issued = false;
-      const uint32_t idesc = idesc_i8(GB_M, GB_N);
+      const uint32_t idesc = idesc_i8(GB_M, BN);
       for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x, it++) {
         const uint32_t acc = it & 1, aph = (it >> 1) & 1;
         if (!mbar_wait(&tempty[acc], aph ^ 1, status, DEV_STATUS_TIMEOUT)) {
@@ -475,20 +491,20 @@ __global__ void __launch_bounds__(256, 1)
           break;
         }
         tc_fence_after();
-        const uint32_t d = tmem_base + acc * GB_N;
+        const uint32_t d = tmem_base + acc * BN;
         for (int kb = 0; kb < nkb; kb++) {
           if (!mbar_wait(&full[stage], phase, status, DEV_STATUS_TIMEOUT)) {
             ok = false;
             break;
           }
           tc_fence_after();
-          const uint32_t a0 = smem_u32(sA + stage * A_STAGE), b0 = smem_u32(sB + stage * B_STAGE);
+          const uint32_t a0 = smem_u32(sA + stage * A_STAGE), b0 = smem_u32(sB + stage * Cfg::B_STAGE);
 #pragma unroll
           for (int kk = 0; kk < GB_K / 32; kk++)
             mma_i8(d, desc_k_sw128(a0 + kk * 32), desc_k_sw128(b0 + kk * 32), idesc, (kb | kk) ? 1u : 0u);
           issued = true;
           mma_commit(&empty[stage]);
-          if (++stage == GSTAGES) {
+          if (++stage == Cfg::STAGES) {
             stage = 0;
             phase ^= 1;
           }
@@ -509,27 +525,27 @@ __global__ void __launch_bounds__(256, 1)
       const uint32_t acc = it & 1, aph = (it >> 1) & 1;
       const uint32_t m = (uint32_t)c_tab.mod[l];
       const int64_t row = c_row0 + (int64_t)tm * GB_M + ew * 32 + lane;
-      uint8_t* dst = cres + (size_t)l * plane + (size_t)row * ldc + (size_t)(c_col0 + (int64_t)tn * GB_N);
+      uint8_t* dst = cres + (size_t)l * plane + (size_t)row * ldc + (size_t)(c_col0 + (int64_t)tn * BN);
       // read-modify-write tiles: fetch this row's 256 old bytes before waiting
       // for the accumulator, so the loads overlap the MMAs
-      uint4 prev[GB_N / 16];
+      uint4 prev[BN / 16];
       if (acc_mode) {
 #pragma unroll
-        for (int q = 0; q < GB_N / 16; q++) prev[q] = *reinterpret_cast<const uint4*>(dst + 16 * q);
+        for (int q = 0; q < BN / 16; q++) prev[q] = *reinterpret_cast<const uint4*>(dst + 16 * q);
       }
       bool ok = mbar_wait(&tfull[acc], aph, status, DEV_STATUS_TIMEOUT);
       if (!__all_sync(0xffffffffu, ok)) break;
       tc_fence_after();
 #pragma unroll
-      for (int ch = 0; ch < GB_N / 32; ch++) {
+      for (int ch = 0; ch < BN / 32; ch++) {
         uint32_t v[32];
-        tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(ew * 32) << 16) + acc * GB_N + ch * 32, v);
+        tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(ew * 32) << 16) + acc * BN + ch * 32, v);
         tmem_wait_ld();
         uint32_t packed[8];
         uint4 prev0 = make_uint4(0, 0, 0, 0), prev1 = make_uint4(0, 0, 0, 0);
         if (acc_mode) {
 #pragma unroll
-          for (int q = 0; q < GB_N / 32; q++)
+          for (int q = 0; q < BN / 32; q++)
             if (q == ch) {
               prev0 = prev[2 * q];
               prev1 = prev[2 * q + 1];
@@ -563,7 +579,7 @@ __global__ void __launch_bounds__(256, 1)
   __syncthreads();
   if (warp == 2) {
     tc_fence_after();
-    tmem_dealloc(tmem_base, 512);
+    tmem_dealloc(tmem_base, Cfg::TMEM_COLS);
   }
 }
 
@@ -689,14 +705,17 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-static int make_map(CUtensorMap* map, const void* base, uint64_t K, uint64_t R, uint64_t L, uint32_t box_r) {
+// Planes of R rows x K bytes; consecutive planes are plane_stride bytes apart
+// (K * R when 0).
+static int make_map(CUtensorMap* map, const void* base, uint64_t K, uint64_t R, uint64_t L, uint32_t box_r,
+                    uint64_t plane_stride = 0) {
   auto fn = encode_fn();
   if (!fn) {
     set_error("cuTensorMapEncodeTiled unavailable");
     return HP_ERR_CUDA;
   }
   cuuint64_t dims[3] = {K, R, L};
-  cuuint64_t strides[2] = {K, K * R};
+  cuuint64_t strides[2] = {K, plane_stride ? plane_stride : K * R};
   cuuint32_t box[3] = {(cuuint32_t)GB_K, box_r, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult rc = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, estr,
@@ -773,7 +792,7 @@ int ozaki_residue_gemm_k(const int8_t* ares, const int8_t* bres, uint8_t* cres, 
   int dev = 0;
   cudaGetDevice(&dev);
   if (!attr_set[dev]) {
-    HP_CUDA_TRY(cudaFuncSetAttribute(i8_gemm_mod_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM));
+    HP_CUDA_TRY(cudaFuncSetAttribute(i8_gemm_mod_kernel<GB_N>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM));
     attr_set[dev] = true;
   }
   CUtensorMap mapA, mapB;
@@ -793,7 +812,7 @@ int ozaki_residue_gemm_k(const int8_t* ares, const int8_t* bres, uint8_t* cres, 
   for (int c0 = 0; c0 < nkb_total; c0 += kb_chunk) {
     const int kb0 = kb_first + c0, kb1 = kb_first + std::min(nkb_total, c0 + kb_chunk);
     const int mode = c0 > 0 ? (acc_mode == 2 ? 2 : 1) : acc_mode;
-    i8_gemm_mod_kernel<<<grid, 256, GEMM_SMEM, s>>>(mapA, mapB, L, tiles_m, tiles_n, kb0, kb1, boff, mode, cres,
+    i8_gemm_mod_kernel<GB_N><<<grid, 256, GEMM_SMEM, s>>>(mapA, mapB, L, tiles_m, tiles_n, kb0, kb1, boff, mode, cres,
                                                      (int64_t)ldc, (int64_t)plane, (int64_t)c_row0,
                                                      (int64_t)c_col0, status);
     HP_LAUNCH_CHECK();
@@ -853,12 +872,12 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
   {
     dim3 ga((unsigned)(Kp / RT_P), (unsigned)(Mp / RT_R));
     if (!atb)
-      residue_kernel<true><<<ga, 256, 0, s>>>(A2, m, k, expA.as<int>(), beta, L, Mp, Kp, ares.as<int8_t>());
+      residue_kernel<true><<<ga, 256, 0, s>>>(A2, m, k, expA.as<int>(), beta, L, (int64_t)Kp, (int64_t)(Mp * Kp), ares.as<int8_t>());
     else
-      residue_kernel<false><<<ga, 256, 0, s>>>(A2, m, k, expA.as<int>(), beta, L, Mp, Kp, ares.as<int8_t>());
+      residue_kernel<false><<<ga, 256, 0, s>>>(A2, m, k, expA.as<int>(), beta, L, (int64_t)Kp, (int64_t)(Mp * Kp), ares.as<int8_t>());
     HP_LAUNCH_CHECK();
     dim3 gb((unsigned)(Kp / RT_P), (unsigned)(Np / RT_R));
-    residue_kernel<false><<<gb, 256, 0, s>>>(B2, n, k, expB.as<int>(), beta, L, Np, Kp, bres.as<int8_t>());
+    residue_kernel<false><<<gb, 256, 0, s>>>(B2, n, k, expB.as<int>(), beta, L, (int64_t)Kp, (int64_t)(Np * Kp), bres.as<int8_t>());
     HP_LAUNCH_CHECK();
   }
   profile_mark(s, "residues");
@@ -1529,6 +1548,42 @@ __global__ void fill_int_kernel(int* p, int64_t n, int v) {
 
 }  // namespace ozaki
 
+// res[l][c_row0 + i][c_row0 + j] -= sum_p A[l][i][p] B[l][j][p] (mod m_l) for
+// i < R, j < CH_NB, p < K: A = the R rows of L~ residues starting at lrow,
+// B = its first CH_NB rows (row length KL bytes, rows_avail rows, planes
+// plane_stride bytes apart). One launch of the 128 x 64 tile GEMM.
+static int rns_panel_update(const uint8_t* lrow, size_t KL, size_t rows_avail, size_t plane_stride, int L, size_t R,
+                            size_t K, uint8_t* res, size_t Np, size_t c0, int num_sms, cudaStream_t s) {
+  using namespace ozaki;
+  constexpr int BN = CH_NB;
+  static bool attr_set[64] = {};
+  int dev = 0;
+  HP_CUDA_TRY(cudaGetDevice(&dev));
+  if (!attr_set[dev]) {
+    HP_CUDA_TRY(cudaFuncSetAttribute(i8_gemm_mod_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     GemmCfg<BN>::SMEM));
+    attr_set[dev] = true;
+  }
+  CUtensorMap mapA, mapB;
+  HP_TRY(make_map(&mapA, lrow, KL, rows_avail, L, GB_M, plane_stride));
+  HP_TRY(make_map(&mapB, lrow, KL, rows_avail, L, BN, plane_stride));
+  uint32_t* status = device_status(s);
+  if (!status) {
+    set_error("status word allocation failed");
+    return HP_ERR_CUDA;
+  }
+  const int tiles_m = (int)((R + GB_M - 1) / GB_M);
+  const int grid = std::min(L * tiles_m, num_sms);
+  const int nkb = (int)(K / GB_K), kb_chunk = MAX_K_CHUNK / GB_K;
+  for (int k0 = 0; k0 < nkb; k0 += kb_chunk) {
+    i8_gemm_mod_kernel<BN><<<grid, 256, GemmCfg<BN>::SMEM, s>>>(mapA, mapB, L, tiles_m, 1, k0, std::min(nkb, k0 + kb_chunk),
+                                                                 0, 2, res, (int64_t)Np, (int64_t)(Np * Np),
+                                                                 (int64_t)c0, (int64_t)c0, status);
+    HP_LAUNCH_CHECK();
+  }
+  return HP_OK;
+}
+
 int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStream_t s) {
   using namespace ozaki;
   if (n == 0) return HP_OK;
@@ -1544,19 +1599,21 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
   const int nc = T.crt[L].nc;
   const dd* S = reinterpret_cast<const dd*>(S_);
   dd* Lout = reinterpret_cast<dd*>(L_);
-  const size_t Rp = round_up(n, GB_N);   // rows of the L21 residue planes
-  const size_t Np = Rp + GB_N;           // trailing-matrix residue planes (room for tile overhang)
-  const size_t nb = CH_NB, Kp = GB_K;
+  const size_t Rp = round_up(n, GB_N);   // rows of the scale vector e1022
+  const size_t Np = Rp + GB_N;           // residue planes of A~ (room for tile overhang)
+  const size_t KL = round_up(n, GB_K);   // L~ residue planes: row length (bytes)
+  const size_t RL = round_up(n, GB_M) + GB_M;  // and rows
+  const size_t nb = CH_NB;
   DevBuf ebuf(n * sizeof(int), s), e1022(Rp * sizeof(int), s), res((size_t)L * Np * Np, s),
-      rl((size_t)L * Rp * Kp, s), P(n * nb * 16, s), Q(n * nb * 16, s), XT(nb * nb * 16, s), err(sizeof(RnsErr), s);
-  if (!ebuf.p || !e1022.p || !res.p || !rl.p || !P.p || !Q.p || !XT.p || !err.p) {
+      lres((size_t)L * RL * KL, s), P(n * nb * 16, s), Q(n * nb * 16, s), XT(nb * nb * 16, s), err(sizeof(RnsErr), s);
+  if (!ebuf.p || !e1022.p || !res.p || !lres.p || !P.p || !Q.p || !XT.p || !err.p) {
     set_error("rns_cholesky: workspace allocation failed");
     return HP_ERR_CUDA;
   }
   RnsErr h0{0, 0, (long long)0x7fffffffffffffffll};
   HP_CUDA_TRY(cudaMemcpyAsync(err.p, &h0, sizeof(h0), cudaMemcpyHostToDevice, s));
   HP_CUDA_TRY(cudaMemsetAsync(res.p, 0, (size_t)L * Np * Np, s));
-  HP_CUDA_TRY(cudaMemsetAsync(rl.p, 0, (size_t)L * Rp * Kp, s));
+  HP_CUDA_TRY(cudaMemsetAsync(lres.p, 0, (size_t)L * RL * KL, s));
   if ((const void*)S_ != (const void*)L_) HP_CUDA_TRY(cudaMemcpyAsync(L_, S_, n * n * 16, cudaMemcpyDeviceToDevice, s));
   rns_scale_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(S, n, BETA_CH, ebuf.as<int>(), err.as<RnsErr>());
   fill_int_kernel<<<(unsigned)((Rp + 255) / 256), 256, 0, s>>>(e1022.as<int>(), Rp, 1022);
@@ -1569,9 +1626,20 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
   const size_t inv_smem = 2 * 64 * 65 * 16;
   HP_CUDA_TRY(cudaFuncSetAttribute(chol_inv_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
   HP_CUDA_TRY(cudaFuncSetAttribute(panel_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, CH_NB * CH_NB * 16));
+  // Left-looking: the panel of block column kb receives all earlier updates
+  // at once, A~[kb.., kb..kb+nb) -= L~[kb.., 0..kb) L~[kb..kb+nb, 0..kb)^T,
+  // as one residue GEMM with N = nb and K = kb over the stored residue
+  // planes of L~ (columns from kb on are still zero there, so K may be
+  // rounded up to the 128-byte k-block). The integers are those of the
+  // right-looking order; only the schedule differs.
   for (size_t kb = 0; kb < n; kb += nb) {
     const int jb = (int)std::min(nb, n - kb);
     const size_t R = n - kb;
+    if (kb > 0) {
+      const uint8_t* lrow = lres.as<uint8_t>() + kb * KL;
+      HP_TRY(rns_panel_update(lrow, KL, RL - kb, RL * KL, L, R, round_up(kb, GB_K), res.as<uint8_t>(),
+                              Np, kb, D->num_sms, s));
+    }
 #define HP_CRTB(NC)                                                                                          \
   case NC:                                                                                                   \
     crt_block_kernel<NC><<<(unsigned)((R * jb + 255) / 256), 256, 0, s>>>(                                    \
@@ -1587,7 +1655,7 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
 #undef HP_CRTB
     HP_LAUNCH_CHECK();
     chol_inv_block_kernel<<<1, CI_THREADS, inv_smem, s>>>(P.as<dd>(), jb, (int64_t)kb, (int64_t)n, ebuf.as<int>(), Lout,
-                                                   XT.as<dd>(), err.as<RnsErr>());
+                                                          XT.as<dd>(), err.as<RnsErr>());
     HP_LAUNCH_CHECK();
     if (R <= (size_t)jb) break;
     const size_t m = R - jb, t0 = kb + jb;
@@ -1600,14 +1668,13 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
     round_store_kernel<<<(unsigned)((m * jb + 255) / 256), 256, 0, s>>>(Q.as<dd>(), (int64_t)m, jb, (int64_t)t0,
                                                                         (int64_t)kb, (int64_t)n, ebuf.as<int>(), Lout);
     HP_LAUNCH_CHECK();
-    {
-      dim3 g((unsigned)(Kp / RT_P), (unsigned)(Rp / RT_R));
+    {  // residues of the rounded L~21 into rows t0.., columns kb..kb+nb of the L~ planes
+      dim3 g((unsigned)(CH_NB / RT_P), (unsigned)((m + RT_R - 1) / RT_R));
       residue_kernel<true><<<g, 256, 0, s>>>(Q.as<double2>(), (int64_t)m, (int64_t)jb, e1022.as<int>(), 0, L,
-                                             (int64_t)Rp, (int64_t)Kp, rl.as<int8_t>());
+                                             (int64_t)KL, (int64_t)(RL * KL),
+                                             reinterpret_cast<int8_t*>(lres.as<uint8_t>() + t0 * KL + kb));
       HP_LAUNCH_CHECK();
     }
-    HP_TRY(ozaki_residue_gemm_ex(rl.as<int8_t>(), rl.as<int8_t>(), res.as<uint8_t>(), L, round_up(m, GB_M),
-                                 round_up(m, GB_N), Kp, Np, Np * Np, t0, t0, 2, s, Rp, Rp));
   }
   RnsErr h;
   HP_CUDA_TRY(cudaMemcpyAsync(&h, err.p, sizeof(h), cudaMemcpyDeviceToHost, s));
@@ -1672,7 +1739,7 @@ static int noalloc_setup(NoAllocDev** out) {
     HP_CUDA_TRY(cudaGetSymbolAddress((void**)&N.crt, g_noalloc_crt));
     HP_CUDA_TRY(cudaGetSymbolAddress((void**)&N.status, g_noalloc_status));
     HP_CUDA_TRY(cudaDeviceGetAttribute(&N.num_sms, cudaDevAttrMultiProcessorCount, d));
-    HP_CUDA_TRY(cudaFuncSetAttribute(i8_gemm_mod_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM));
+    HP_CUDA_TRY(cudaFuncSetAttribute(i8_gemm_mod_kernel<GB_N>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM));
     N.ready = true;
   }
   *out = &N;
@@ -1748,10 +1815,10 @@ static int ozaki_dd_gemm_noalloc(const double* a, const double* b, double* c, si
   }
   {
     dim3 ga((unsigned)(Kp / RT_P), (unsigned)(Mp / RT_R));
-    residue_kernel<true><<<ga, 256, 0, s>>>(A2, m, k, expA, beta, L, Mp, Kp, ares);
+    residue_kernel<true><<<ga, 256, 0, s>>>(A2, m, k, expA, beta, L, (int64_t)Kp, (int64_t)(Mp * Kp), ares);
     HP_LAUNCH_CHECK();
     dim3 gb((unsigned)(Kp / RT_P), (unsigned)(Np / RT_R));
-    residue_kernel<false><<<gb, 256, 0, s>>>(B2, n, k, expB, beta, L, Np, Kp, bres);
+    residue_kernel<false><<<gb, 256, 0, s>>>(B2, n, k, expB, beta, L, (int64_t)Kp, (int64_t)(Np * Kp), bres);
     HP_LAUNCH_CHECK();
   }
   {
@@ -1762,7 +1829,7 @@ static int ozaki_dd_gemm_noalloc(const double* a, const double* b, double* c, si
     const int grid = std::min(L * tiles_m * tiles_n, N->num_sms);
     const int nkb = (int)(Kp / GB_K), kb_chunk = MAX_K_CHUNK / GB_K;
     for (int c0 = 0; c0 < nkb; c0 += kb_chunk) {
-      i8_gemm_mod_kernel<<<grid, 256, GEMM_SMEM, s>>>(mapA, mapB, L, tiles_m, tiles_n, c0, std::min(nkb, c0 + kb_chunk),
+      i8_gemm_mod_kernel<GB_N><<<grid, 256, GEMM_SMEM, s>>>(mapA, mapB, L, tiles_m, tiles_n, c0, std::min(nkb, c0 + kb_chunk),
                                                        0, c0 > 0 ? 1 : 0, cres, (int64_t)Np, (int64_t)(Mp * Np), 0, 0,
                                                        N->status);
       HP_LAUNCH_CHECK();
