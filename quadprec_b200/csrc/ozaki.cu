@@ -1259,10 +1259,14 @@ __device__ __forceinline__ void int_digits10(double v, int32_t* d) {
   d[0] = s * (int32_t)a;
 }
 
-// Res[l][i][j] = round((D S D)_ij) mod m_l (unbalanced bytes) for i, j < Rp;
-// zero outside n x n. Block tile 64 rows x 32 columns, 8 columns per thread.
+// Res[l][i][j] = round((D S D)_ij) mod m_l (unbalanced bytes) for the tiles
+// that meet the lower triangle of n x n (the factorisation reads no other
+// entry; the rest stays as the caller zeroed it). Block tile 64 rows x 32
+// columns, 8 columns per thread.
 __global__ void __launch_bounds__(256) rns_init_kernel(const dd* __restrict__ S, int64_t n, const int* __restrict__ e,
                                                        int L, int64_t Rp, uint8_t* __restrict__ res) {
+  const int64_t row0 = (int64_t)blockIdx.y * 64, col0 = (int64_t)blockIdx.x * 32;
+  if (row0 >= n || col0 >= n || col0 > row0 + 63) return;
   const int t = threadIdx.x;
   const int64_t i = (int64_t)blockIdx.y * 64 + t / 4;
   const int64_t j0 = (int64_t)blockIdx.x * 32 + 8 * (t % 4);
@@ -1348,6 +1352,23 @@ __global__ void __launch_bounds__(256) crt_block_kernel(const uint8_t* __restric
   P[idx] = neg ? dd_neg(s) : s;
 }
 
+// a - b c in f128 with 16 operations instead of the 29 of a reference-order
+// multiply and add: the exact product p + pe of the high parts, the cross
+// terms b.hi c.lo + b.lo c.hi, one two_sum of the high parts and a final
+// renormalisation (the cheaper "sloppy" addition). Error below
+// ~3 2^-104 (|a| + |b c|), the bound that the backward-error analysis of
+// Cholesky and substitution assumes of each update. For the chosen path's
+// f128 kernels only, never where results must match the reference's bits.
+__device__ __forceinline__ dd dd_fms_fast(dd a, dd b, dd c) {
+  const double p = __dmul_rn(b.hi, c.hi);
+  const double pe = __fma_rn(b.hi, c.hi, -p);
+  const double t = __fma_rn(b.hi, c.lo, __dmul_rn(b.lo, c.hi));
+  double s, se;
+  two_sum(a.hi, -p, s, se);
+  const double e = __dadd_rn(se, __dsub_rn(a.lo, __dadd_rn(pe, t)));
+  return dd_renorm(s, e);
+}
+
 // 1/sqrt(d) to ~2^-103 from the f64 seed x = rsqrt(d.hi) (relative error
 // delta of a few 2^-53) by one Newton step x1 = x + x e / 2, e = 1 - d x^2.
 // e is ~delta, so it is needed only to ~2^-104 absolute: with x^2 = s + s'
@@ -1366,24 +1387,23 @@ __device__ __forceinline__ dd dd_rsqrt(dd d) {
 // Factor the jb x jb block P[0..jb)[0..jb) (row stride jb, symmetric values)
 // in f128, write L~11 scaled back to Lout, and X^T = (L~11^-1)^T to XT.
 // The block is padded to 64 x 64 with the identity, so every step has the
-// same shape. X = L~^-1 is formed by row-oriented forward substitution
-// alongside the factorisation. Iteration j (one barrier):
+// same shape. The inverse is formed as X = diag(1 / l_rr) Y with
+// Y = L1^-1, L1 = L~ diag(1 / l_rr) unit lower triangular, so its rows need
+// no scaling step: Y[i][.] -= L1[i][r] Y[r][.] for i > r, in row order r.
+// Iteration j (one barrier):
 //   warp 31 (the critical path): column p = j + 1 gets its last update
-//     a_ip -= l_ij l_pj (i >= p); lane 0 forms 1/sqrt(a_pp) and broadcasts
-//     it; the column is scaled, l_ip = a_ip / sqrt(a_pp), into the next
-//     column buffer. Row p of X gets its last update X[p][c] -= l_pj x_jc
-//     (c <= j) and is scaled, x_pc = X[p][c] / l_pp, into the next row
+//     a_ip -= l_ij l_pj (i >= p); every lane forms 1/sqrt(a_pp) and the
+//     column is scaled, l_ip = a_ip / sqrt(a_pp), into the next column
 //     buffer.
 //   the bulk warps (those on the three other schedulers, warp % 4 != 3):
 //     every other live update of step j, as one index space: the trailing
 //     triangle a_ik -= l_ij l_kj (j + 2 <= k <= i; a table ordered by
 //     column makes these the first T_{j+1} slots), then the inverse
-//     rectangle X[i][c] -= l_ij x_jc (i >= j + 2, c <= j).
-//   the other warps of warp 31's scheduler: write column j and row j (the
-//     buffers warp 31 filled one iteration earlier) to Lout and XT, so the
-//     critical warp keeps its scheduler to itself.
-// Every entry sees the same f128 operations in the same order as a plain
-// right-looking column Cholesky and row-oriented substitution.
+//     rectangle Y[i][c] -= L1[i][r] Y[r][c] for r = j - 1 (i >= j, c <= r).
+//   the other warps of warp 31's scheduler: L1 column j (for the bulk's
+//     next iteration), L~ column j to Lout and row j - 1 of X (final since
+//     the last iteration) to XT.
+// Updates use dd_fms_fast (f128-level accuracy, not the reference's bits).
 constexpr int CI_THREADS = 1024;
 constexpr int CI_BULK = CI_THREADS / 4 * 3;     // warps with warp % 4 != 3
 constexpr int CI_OUT = CI_THREADS / 4 - 32;     // the other warps with warp % 4 == 3
@@ -1393,9 +1413,10 @@ __global__ void __launch_bounds__(CI_THREADS) chol_inv_block_kernel(const dd* __
                                                                     RnsErr* err) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   dd* A = reinterpret_cast<dd*>(sm_raw);  // [64][65]
-  dd* X = A + 64 * 65;                    // [64][65]
-  __shared__ dd Lc[2][64], xs[2][64];     // scaled column j of L~ / row j of X, double-buffered
-  __shared__ dd ldiag[64];                // l_jj = sqrt(a_jj)
+  dd* Y = A + 64 * 65;                    // [64][65]
+  __shared__ dd Lc[2][64];                // scaled column j of L~, double-buffered
+  __shared__ dd L1c[2][64];               // column j of L1, double-buffered
+  __shared__ dd rinv[64], ldiag[64];      // 1 / l_jj and l_jj = sqrt(a_jj)
   __shared__ uint16_t tab[2016];          // (i << 6) | k, column k = 63..1, rows i = k..63
   __shared__ uint64_t kmagic[64];         // ceil(2^32 / (j + 1)): q / (j + 1) = (q kmagic[j]) >> 32, q < 2^12
   __shared__ int esh[64];
@@ -1415,7 +1436,7 @@ __global__ void __launch_bounds__(CI_THREADS) chol_inv_block_kernel(const dd* __
   for (int q = t; q < 64 * 64; q += CI_THREADS) {
     const int r = q / 64, c = q % 64;
     A[r * 65 + c] = (r < jb && c < jb) ? P[r * jb + c] : dd_from(r == c ? 1.0 : 0.0);
-    X[r * 65 + c] = dd_from(r == c ? 1.0 : 0.0);
+    Y[r * 65 + c] = dd_from(r == c ? 1.0 : 0.0);
     if (c >= 1 && r >= c) tab[(63 - c) * (64 - c) / 2 + (r - c)] = (uint16_t)((r << 6) | c);
     if (c > r && c < jb) XT[c * jb + r] = dd{0.0, 0.0};  // X[r][c] = 0 above the diagonal
   }
@@ -1432,77 +1453,86 @@ __global__ void __launch_bounds__(CI_THREADS) chol_inv_block_kernel(const dd* __
       return false;
     }
     r = dd_rsqrt(d);
-    if (lane == 0) ldiag[p] = dd_mul(d, r);
+    if (lane == 0) {
+      rinv[p] = r;
+      ldiag[p] = dd_mul(d, r);
+    }
     return true;
   };
-  // column j of L~ and row j of X, from the buffers, to Lout and XT
-  auto write_out = [&](int j, int buf) {
-    if (j >= jb) return;
-    for (int i = j + ot; i < jb; i += CI_OUT) {
-      const dd v = i == j ? ldiag[j] : Lc[buf][i];
-      const int sh = -esh[i];
-      Lout[(kb + i) * n + kb + j] = dd_renorm(scale_pow2(v.hi, sh), scale_pow2(v.lo, sh));
+  // Output-warp work of iteration j: L1 column j, L~ column j to Lout,
+  // X row j - 1 to XT.
+  auto outputs = [&](int j) {
+    if (j < 64) {
+      const dd rj = rinv[j];
+      for (int i = j + 1 + ot; i < 64; i += CI_OUT) L1c[j & 1][i] = dd_mul(Lc[j & 1][i], rj);
+      if (j < jb)
+        for (int i = j + ot; i < jb; i += CI_OUT) {
+          const dd v = i == j ? ldiag[j] : Lc[j & 1][i];
+          const int sh = -esh[i];
+          Lout[(kb + i) * n + kb + j] = dd_renorm(scale_pow2(v.hi, sh), scale_pow2(v.lo, sh));
+        }
     }
-    for (int c = ot; c <= j; c += CI_OUT) XT[c * jb + j] = xs[buf][c];
+    const int r = j - 1;
+    if (r >= 0 && r < jb) {
+      const dd rr = rinv[r];
+      for (int c = ot; c <= r; c += CI_OUT) XT[c * jb + r] = c == r ? rr : dd_mul(rr, Y[r * 65 + c]);
+    }
   };
-  if (critical) {  // step 0: pivot 0, column 0, row 0
+  if (critical) {  // pivot 0 and column 0
     dd r = {0.0, 0.0};
-    if (pivot(0, A[0], r)) {
+    if (pivot(0, A[0], r))
       for (int i = 1 + lane; i < 64; i += 32) Lc[0][i] = dd_mul(A[i * 65], r);
-      if (lane == 0) xs[0][0] = r;
-    }
   }
   __syncthreads();
-  for (int j = 0; j < 63; j++) {
+  for (int j = 0; j < 64; j++) {
     if (fail) return;
     const int cur = j & 1, nxt = cur ^ 1, p = j + 1;
     if (critical) {
-      // column p: last update, pivot, scale; row p of X: last update, scale.
-      // Indices are clamped so that all four chains run unconditionally
-      // (interleaved); only the stores are predicated.
-      const dd lpj = Lc[cur][p];
-      const int i0 = p + lane, i1 = p + 32 + lane, c0 = lane, c1 = 32 + lane;
-      const int i0c = min(i0, 63), i1c = min(i1, 63), c0c = c0 <= j ? c0 : 0, c1c = c1 <= j ? c1 : 0;
-      const dd a0 = dd_sub(A[i0c * 65 + p], dd_mul(Lc[cur][i0c], lpj));
-      const dd a1 = dd_sub(A[i1c * 65 + p], dd_mul(Lc[cur][i1c], lpj));
-      const dd x0 = dd_sub(X[p * 65 + c0c], dd_mul(lpj, xs[cur][c0c]));
-      const dd x1 = dd_sub(X[p * 65 + c1c], dd_mul(lpj, xs[cur][c1c]));
-      const dd d = {__shfl_sync(0xffffffffu, a0.hi, 0), __shfl_sync(0xffffffffu, a0.lo, 0)};  // a_pp (lane 0)
-      dd r;
-      if (pivot(p, d, r)) {
-        const dd s0 = dd_mul(a0, r), s1 = dd_mul(a1, r), y0 = dd_mul(x0, r), y1 = dd_mul(x1, r);
-        if (i0 < 64 && i0 > p) Lc[nxt][i0] = s0;
-        if (i1 < 64) Lc[nxt][i1] = s1;
-        if (c0 <= p) xs[nxt][c0] = c0 == p ? r : y0;
-        if (c1 <= p) xs[nxt][c1] = c1 == p ? r : y1;
+      if (p < 64) {
+        // column p: last update, pivot, scale. Indices are clamped so the
+        // two chains run unconditionally (interleaved); stores are predicated.
+        const dd lpj = Lc[cur][p];
+        const int i0 = p + lane, i1 = p + 32 + lane;
+        const int i0c = min(i0, 63), i1c = min(i1, 63);
+        const dd a0 = dd_fms_fast(A[i0c * 65 + p], Lc[cur][i0c], lpj);
+        const dd a1 = dd_fms_fast(A[i1c * 65 + p], Lc[cur][i1c], lpj);
+        const dd d = {__shfl_sync(0xffffffffu, a0.hi, 0), __shfl_sync(0xffffffffu, a0.lo, 0)};  // a_pp (lane 0)
+        dd r;
+        if (pivot(p, d, r)) {
+          const dd s0 = dd_mul(a0, r), s1 = dd_mul(a1, r);
+          if (i0 < 64 && i0 > p) Lc[nxt][i0] = s0;
+          if (i1 < 64) Lc[nxt][i1] = s1;
+        }
       }
     } else if (bulk) {
-      const int Tn = (62 - j) * (63 - j) / 2;  // trailing slots with column >= j + 2
-      const int total = Tn + (62 - j) * (j + 1);
-      const uint64_t magic = kmagic[j];
+      const int Tn = j < 63 ? (62 - j) * (63 - j) / 2 : 0;  // trailing slots with column >= j + 2
+      const int total = Tn + (64 - j) * j;
+      const uint64_t magic = j > 0 ? kmagic[j - 1] : 0;     // q / j
+      const int r = j - 1;
       int u = bt;
       for (; u < Tn; u += CI_BULK) {
         const int ent = tab[u], i = ent >> 6, kk = ent & 63;
-        A[i * 65 + kk] = dd_sub(A[i * 65 + kk], dd_mul(Lc[cur][i], Lc[cur][kk]));
+        A[i * 65 + kk] = dd_fms_fast(A[i * 65 + kk], Lc[cur][i], Lc[cur][kk]);
       }
       for (; u < total; u += CI_BULK) {
         const int q = u - Tn;
-        const int ii = (int)(((uint64_t)q * magic) >> 32), c = q - ii * (j + 1);
-        const int i = j + 2 + ii;
-        X[i * 65 + c] = dd_sub(X[i * 65 + c], dd_mul(Lc[cur][i], xs[cur][c]));
+        const int ii = (int)(((uint64_t)q * magic) >> 32), c = q - ii * j;
+        const int i = j + ii;
+        Y[i * 65 + c] = dd_fms_fast(Y[i * 65 + c], L1c[r & 1][i], Y[r * 65 + c]);
       }
     } else {
-      write_out(j, cur);
+      outputs(j);
     }
     __syncthreads();
   }
   if (fail) return;
-  if (!bulk && !critical) write_out(63, 63 & 1);
+  if (!bulk && !critical) outputs(64);  // X row 63
 }
 
 // Q = P21 X^T for the panel: Q[r][c] = sum_k P21[r][k] X[c][k] (k < jb),
 // XT[k][c] = X[c][k] in shared memory; one warp per row, lane c owns output
-// columns c and c + 32, P21[r][k] is broadcast by shuffle.
+// columns c and c + 32, P21[r][k] is broadcast by shuffle. Accumulation with
+// dd_fms_fast (f128 accuracy; the products are rounded to integers next).
 __global__ void __launch_bounds__(256) panel_apply_kernel(const dd* __restrict__ P21, const dd* __restrict__ XT,
                                                           dd* __restrict__ Q, int64_t m, int jb) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
@@ -1520,8 +1550,9 @@ __global__ void __launch_bounds__(256) panel_apply_kernel(const dd* __restrict__
       dd ak;
       ak.hi = __shfl_sync(0xffffffffu, k < 32 ? a0.hi : a1.hi, k % 32);
       ak.lo = __shfl_sync(0xffffffffu, k < 32 ? a0.lo : a1.lo, k % 32);
-      if (lane < jb) acc0 = dd_add(acc0, dd_mul(ak, xs[k][lane]));
-      if (lane + 32 < jb) acc1 = dd_add(acc1, dd_mul(ak, xs[k][lane + 32]));
+      const dd nk = {-ak.hi, -ak.lo};
+      if (lane < jb) acc0 = dd_fms_fast(acc0, nk, xs[k][lane]);
+      if (lane + 32 < jb) acc1 = dd_fms_fast(acc1, nk, xs[k][lane + 32]);
     }
     if (lane < jb) Q[r * jb + lane] = acc0;
     if (lane + 32 < jb) Q[r * jb + lane + 32] = acc1;
