@@ -84,6 +84,18 @@ __device__ __forceinline__ dd ld_dd_cg(const dd* p) {
   return dd{v.x, v.y};
 }
 
+// a - b c in f128 with 16 operations (exact high product, cross terms, one
+// two_sum, renormalisation); error below ~3 2^-104 (|a| + |b c|), the bound
+// the backward-error analysis of substitution assumes of each update.
+__device__ __forceinline__ dd fms_fast(dd a, dd b, dd c) {
+  const double p = __dmul_rn(b.hi, c.hi);
+  const double pe = __fma_rn(b.hi, c.hi, -p);
+  const double t = __fma_rn(b.hi, c.lo, __dmul_rn(b.lo, c.hi));
+  double s, se;
+  two_sum(a.hi, -p, s, se);
+  return dd_renorm(s, __dadd_rn(se, __dsub_rn(a.lo, __dadd_rn(pe, t))));
+}
+
 // Block row k: thread (r, q) = (t / 4, t % 4) owns row r of the block and
 // the columns c = q (mod 4) of each 64 x 64 tile it multiplies.
 constexpr uint64_t TRSV_WAIT_NS = 2000000000ull;
@@ -143,8 +155,8 @@ __global__ void __launch_bounds__(256) trsv_wave_kernel(const dd* __restrict__ L
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < TB / 4; m += 2) {
-      acc0 = dd_add(acc0, dd_mul(lv[m], vj[q + 4 * m]));
-      acc1 = dd_add(acc1, dd_mul(lv[m + 1], vj[q + 4 * m + 4]));
+      acc0 = fms_fast(acc0, dd{-lv[m].hi, -lv[m].lo}, vj[q + 4 * m]);
+      acc1 = fms_fast(acc1, dd{-lv[m + 1].hi, -lv[m + 1].lo}, vj[q + 4 * m + 4]);
     }
     __syncthreads();  // vj is rewritten by the next dependency
   }
@@ -157,20 +169,15 @@ __global__ void __launch_bounds__(256) trsv_wave_kernel(const dd* __restrict__ L
   acc0 = acc1 = dd{0.0, 0.0};
 #pragma unroll
   for (int m = 0; m < TB / 4; m += 2) {
-    acc0 = dd_add(acc0, dd_mul(xr[m], sv[q + 4 * m]));
-    acc1 = dd_add(acc1, dd_mul(xr[m + 1], sv[q + 4 * m + 4]));
+    acc0 = fms_fast(acc0, dd{-xr[m].hi, -xr[m].lo}, sv[q + 4 * m]);
+    acc1 = fms_fast(acc1, dd{-xr[m + 1].hi, -xr[m + 1].lo}, sv[q + 4 * m + 4]);
   }
   part[r][q] = dd_add(acc0, acc1);
   __syncthreads();
-  if (q == 0 && r < jb) {
-    v[k0 + r] = dd_add(dd_add(part[r][0], part[r][1]), dd_add(part[r][2], part[r][3]));
-    __threadfence();
-  }
+  if (q == 0 && r < jb) v[k0 + r] = dd_add(dd_add(part[r][0], part[r][1]), dd_add(part[r][2], part[r][3]));
+  // the barrier orders the block's stores before thread 0's release store
   __syncthreads();
-  if (t == 0) {
-    __threadfence();
-    st_release_gpu(flags + k, epoch);
-  }
+  if (t == 0) st_release_gpu(flags + k, epoch);
 }
 
 }  // namespace
