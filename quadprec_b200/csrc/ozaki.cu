@@ -293,7 +293,7 @@ __device__ __forceinline__ void int_digits(double v, int32_t* d) {
 // index p); element (r, p) is src[r*K + p] (P_CONTIG) or src[p*R + r].
 // Writes out[l][r][p] (int8), row stride ld, plane stride plane_stride, for
 // every (r, p) the grid covers (64 gridDim.y rows, 32 gridDim.x columns;
-// zero outside R x K).
+// zero outside R x K); blockIdx.z takes the moduli l = z (mod gridDim.z).
 // Block tile: 64 rows x 32 p; each thread owns one row and 8 consecutive p,
 // so its 8 residues of one modulus pack into two 32-bit words.
 //   P_CONTIG: thread reads 8 consecutive f128 (128 B) and stores its 8 bytes
@@ -349,7 +349,8 @@ __global__ void __launch_bounds__(256) residue_kernel(const double2* __restrict_
     }
   }
   int8_t* const base = out + (size_t)(blockIdx.y * RT_R) * ld + blockIdx.x * RT_P;
-  for (int l = 0; l < L; l++) {
+  int it = 0;
+  for (int l = blockIdx.z; l < L; l += gridDim.z, it++) {
     const int m = c_tab.mod[l];
     uint32_t w0 = 0, w1 = 0;
 #pragma unroll
@@ -361,12 +362,12 @@ __global__ void __launch_bounds__(256) residue_kernel(const double2* __restrict_
     if (P_CONTIG) {
       *reinterpret_cast<uint2*>(plane + (size_t)rl * ld + 8 * oct) = make_uint2(w0, w1);
     } else {
-      T[l & 1][rl][2 * oct] = w0;
-      T[l & 1][rl][2 * oct + 1] = w1;
+      T[it & 1][rl][2 * oct] = w0;
+      T[it & 1][rl][2 * oct + 1] = w1;
       __syncthreads();
       if (t < 2 * RT_R) {
         const int row = t / 2, half = t % 2;
-        const uint32_t* src_w = &T[l & 1][row][4 * half];
+        const uint32_t* src_w = &T[it & 1][row][4 * half];
         *reinterpret_cast<uint4*>(plane + (size_t)row * ld + 16 * half) =
             make_uint4(src_w[0], src_w[1], src_w[2], src_w[3]);
       }
@@ -1531,13 +1532,18 @@ __global__ void __launch_bounds__(CI_THREADS) chol_inv_block_kernel(const dd* __
 
 // Q = P21 X^T for the panel: Q[r][c] = sum_k P21[r][k] X[c][k] (k < jb),
 // XT[k][c] = X[c][k] in shared memory; one warp per row, lane c owns output
-// columns c and c + 32, P21[r][k] is broadcast by shuffle. Accumulation with
-// dd_fms_fast (f128 accuracy; the products are rounded to integers next).
-__global__ void __launch_bounds__(256) panel_apply_kernel(const dd* __restrict__ P21, const dd* __restrict__ XT,
+// columns c and c + 32, P21[r][k] is broadcast by shuffle. Each output keeps
+// two independent partial sums (k < 32, k >= 32), so a lane has four f128
+// chains in flight. Accumulation with dd_fms_fast (f128 accuracy; the
+// products are rounded to integers next).
+__global__ void __launch_bounds__(128) panel_apply_kernel(const dd* __restrict__ P21, const dd* __restrict__ XT,
                                                           dd* __restrict__ Q, int64_t m, int jb) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   dd(*xs)[CH_NB] = reinterpret_cast<dd(*)[CH_NB]>(sm_raw);  // [CH_NB][CH_NB]
-  for (int q = threadIdx.x; q < jb * jb; q += blockDim.x) xs[q / jb][q % jb] = XT[q];
+  for (int q = threadIdx.x; q < CH_NB * CH_NB; q += blockDim.x) {
+    const int k = q / CH_NB, c = q % CH_NB;
+    xs[k][c] = (k < jb && c < jb) ? XT[k * jb + c] : dd{0.0, 0.0};
+  }
   __syncthreads();
   const int lane = threadIdx.x % 32;
   const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
@@ -1545,22 +1551,21 @@ __global__ void __launch_bounds__(256) panel_apply_kernel(const dd* __restrict__
   for (int64_t r = w0; r < m; r += nw) {
     const dd a0 = lane < jb ? P21[r * jb + lane] : dd{0.0, 0.0};
     const dd a1 = lane + 32 < jb ? P21[r * jb + lane + 32] : dd{0.0, 0.0};
-    dd acc0 = dd{0.0, 0.0}, acc1 = dd{0.0, 0.0};
-    for (int k = 0; k < jb; k++) {
-      dd ak;
-      ak.hi = __shfl_sync(0xffffffffu, k < 32 ? a0.hi : a1.hi, k % 32);
-      ak.lo = __shfl_sync(0xffffffffu, k < 32 ? a0.lo : a1.lo, k % 32);
-      const dd nk = {-ak.hi, -ak.lo};
-      if (lane < jb) acc0 = dd_fms_fast(acc0, nk, xs[k][lane]);
-      if (lane + 32 < jb) acc1 = dd_fms_fast(acc1, nk, xs[k][lane + 32]);
+    dd s00 = {0.0, 0.0}, s01 = {0.0, 0.0}, s10 = {0.0, 0.0}, s11 = {0.0, 0.0};
+#pragma unroll 4
+    for (int k = 0; k < 32; k++) {
+      // -P21[r][k] and -P21[r][k + 32] (zero beyond jb, with xs zero there)
+      const dd u = {-__shfl_sync(0xffffffffu, a0.hi, k), -__shfl_sync(0xffffffffu, a0.lo, k)};
+      const dd w = {-__shfl_sync(0xffffffffu, a1.hi, k), -__shfl_sync(0xffffffffu, a1.lo, k)};
+      s00 = dd_fms_fast(s00, u, xs[k][lane]);
+      s01 = dd_fms_fast(s01, u, xs[k][lane + 32]);
+      s10 = dd_fms_fast(s10, w, xs[k + 32][lane]);
+      s11 = dd_fms_fast(s11, w, xs[k + 32][lane + 32]);
     }
-    if (lane < jb) Q[r * jb + lane] = acc0;
-    if (lane + 32 < jb) Q[r * jb + lane + 32] = acc1;
+    if (lane < jb) Q[r * jb + lane] = dd_add(s00, s10);
+    if (lane + 32 < jb) Q[r * jb + lane + 32] = dd_add(s01, s11);
   }
 }
-
-// Round L21 to integers (rint of each limb, as the residue kernel does) and
-// store D^-1 L21 into Lout[t0 + r][kb + c].
 __global__ void round_store_kernel(const dd* __restrict__ Q, int64_t m, int jb, int64_t t0, int64_t kb, int64_t n,
                                    const int* __restrict__ e, dd* __restrict__ Lout) {
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -1691,8 +1696,8 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
     if (R <= (size_t)jb) break;
     const size_t m = R - jb, t0 = kb + jb;
     {
-      const unsigned blocks = (unsigned)std::min<size_t>((m + 7) / 8, (size_t)D->num_sms * 4);
-      panel_apply_kernel<<<blocks, 256, CH_NB * CH_NB * 16, s>>>(P.as<dd>() + (size_t)jb * jb, XT.as<dd>(), Q.as<dd>(),
+      const unsigned blocks = (unsigned)std::min<size_t>((m + 3) / 4, (size_t)D->num_sms * 8);
+      panel_apply_kernel<<<blocks, 128, CH_NB * CH_NB * 16, s>>>(P.as<dd>() + (size_t)jb * jb, XT.as<dd>(), Q.as<dd>(),
                                                                  (int64_t)m, jb);
       HP_LAUNCH_CHECK();
     }
@@ -1700,7 +1705,7 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
                                                                         (int64_t)kb, (int64_t)n, ebuf.as<int>(), Lout);
     HP_LAUNCH_CHECK();
     {  // residues of the rounded L~21 into rows t0.., columns kb..kb+nb of the L~ planes
-      dim3 g((unsigned)(CH_NB / RT_P), (unsigned)((m + RT_R - 1) / RT_R));
+      dim3 g((unsigned)(CH_NB / RT_P), (unsigned)((m + RT_R - 1) / RT_R), 4);
       residue_kernel<true><<<g, 256, 0, s>>>(Q.as<double2>(), (int64_t)m, (int64_t)jb, e1022.as<int>(), 0, L,
                                              (int64_t)KL, (int64_t)(RL * KL),
                                              reinterpret_cast<int8_t*>(lres.as<uint8_t>() + t0 * KL + kb));
