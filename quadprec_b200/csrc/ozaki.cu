@@ -1386,40 +1386,32 @@ __device__ __forceinline__ dd dd_rsqrt(dd d) {
 }
 
 // Factor the jb x jb block P[0..jb)[0..jb) (row stride jb, symmetric values)
-// in f128, write L~11 scaled back to Lout, and X^T = (L~11^-1)^T to XT.
-// The block is padded to 64 x 64 with the identity, so every step has the
-// same shape. The inverse is formed as X = diag(1 / l_rr) Y with
-// Y = L1^-1, L1 = L~ diag(1 / l_rr) unit lower triangular, so its rows need
-// no scaling step: Y[i][.] -= L1[i][r] Y[r][.] for i > r, in row order r.
-// Iteration j (one barrier):
+// in f128: L~11 scaled back to Lout, and for the panel solve the unit lower
+// factor L1 = L~11 diag(1 / l_jj) (row-major 64 x 64, zero on and above the
+// diagonal) with rinv[j] = 1 / l_jj. The block is padded to 64 x 64 with the
+// identity, so every step has the same shape. Iteration j (one barrier):
 //   warp 31 (the critical path): column p = j + 1 gets its last update
 //     a_ip -= l_ij l_pj (i >= p); every lane forms 1/sqrt(a_pp) and the
 //     column is scaled, l_ip = a_ip / sqrt(a_pp), into the next column
 //     buffer.
 //   the bulk warps (those on the three other schedulers, warp % 4 != 3):
-//     every other live update of step j, as one index space: the trailing
-//     triangle a_ik -= l_ij l_kj (j + 2 <= k <= i; a table ordered by
-//     column makes these the first T_{j+1} slots), then the inverse
-//     rectangle Y[i][c] -= L1[i][r] Y[r][c] for r = j - 1 (i >= j, c <= r).
-//   the other warps of warp 31's scheduler: L1 column j (for the bulk's
-//     next iteration), L~ column j to Lout and row j - 1 of X (final since
-//     the last iteration) to XT.
+//     every other live update of step j, a_ik -= l_ij l_kj for
+//     j + 2 <= k <= i (a table ordered by column makes these the first
+//     T_{j+1} slots).
+//   the other warps of warp 31's scheduler: column j to Lout, L1 and rinv.
 // Updates use dd_fms_fast (f128-level accuracy, not the reference's bits).
 constexpr int CI_THREADS = 1024;
-constexpr int CI_BULK = CI_THREADS / 4 * 3;     // warps with warp % 4 != 3
-constexpr int CI_OUT = CI_THREADS / 4 - 32;     // the other warps with warp % 4 == 3
-__global__ void __launch_bounds__(CI_THREADS) chol_inv_block_kernel(const dd* __restrict__ P, int jb, int64_t kb,
-                                                                    int64_t n, const int* __restrict__ e,
-                                                                    dd* __restrict__ Lout, dd* __restrict__ XT,
-                                                                    RnsErr* err) {
+constexpr int CI_BULK = CI_THREADS / 4 * 3;  // warps with warp % 4 != 3
+constexpr int CI_OUT = CI_THREADS / 4 - 32;  // the other warps with warp % 4 == 3
+__global__ void __launch_bounds__(CI_THREADS) chol_block_kernel(const dd* __restrict__ P, int jb, int64_t kb,
+                                                                int64_t n, const int* __restrict__ e,
+                                                                dd* __restrict__ Lout, dd* __restrict__ L1g,
+                                                                dd* __restrict__ rinvg, RnsErr* err) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   dd* A = reinterpret_cast<dd*>(sm_raw);  // [64][65]
-  dd* Y = A + 64 * 65;                    // [64][65]
   __shared__ dd Lc[2][64];                // scaled column j of L~, double-buffered
-  __shared__ dd L1c[2][64];               // column j of L1, double-buffered
   __shared__ dd rinv[64], ldiag[64];      // 1 / l_jj and l_jj = sqrt(a_jj)
   __shared__ uint16_t tab[2016];          // (i << 6) | k, column k = 63..1, rows i = k..63
-  __shared__ uint64_t kmagic[64];         // ceil(2^32 / (j + 1)): q / (j + 1) = (q kmagic[j]) >> 32, q < 2^12
   __shared__ int esh[64];
   __shared__ int fail;
   const int t = threadIdx.x, lane = t % 32, warp = t / 32;
@@ -1428,18 +1420,14 @@ __global__ void __launch_bounds__(CI_THREADS) chol_inv_block_kernel(const dd* __
   const int bt = (warp / 4 * 3 + warp % 4) * 32 + lane;  // bulk thread index
   const int ot = (warp / 4) * 32 + lane;                 // index among the output warps (warp % 4 == 3)
   if (err->flag) return;
-  if (t < 64) {
-    kmagic[t] = ((1ull << 32) + (uint64_t)t) / (uint64_t)(t + 1);
-    esh[t] = t < jb ? e[kb + t] : 0;
-  }
+  if (t < 64) esh[t] = t < jb ? e[kb + t] : 0;
   if (t == 0) fail = 0;
 #pragma unroll 4
   for (int q = t; q < 64 * 64; q += CI_THREADS) {
     const int r = q / 64, c = q % 64;
     A[r * 65 + c] = (r < jb && c < jb) ? P[r * jb + c] : dd_from(r == c ? 1.0 : 0.0);
-    Y[r * 65 + c] = dd_from(r == c ? 1.0 : 0.0);
     if (c >= 1 && r >= c) tab[(63 - c) * (64 - c) / 2 + (r - c)] = (uint16_t)((r << 6) | c);
-    if (c > r && c < jb) XT[c * jb + r] = dd{0.0, 0.0};  // X[r][c] = 0 above the diagonal
+    if (c >= r) L1g[r * 64 + c] = dd{0.0, 0.0};  // L1 is stored strictly lower
   }
   __syncthreads();
   // Pivot p on warp 31, branch-free: every lane forms r = 1/sqrt(d) from
@@ -1460,24 +1448,19 @@ __global__ void __launch_bounds__(CI_THREADS) chol_inv_block_kernel(const dd* __
     }
     return true;
   };
-  // Output-warp work of iteration j: L1 column j, L~ column j to Lout,
-  // X row j - 1 to XT.
+  // column j of L~ (from the buffer warp 31 filled one iteration earlier)
+  // to Lout, L1 and rinv
   auto outputs = [&](int j) {
-    if (j < 64) {
-      const dd rj = rinv[j];
-      for (int i = j + 1 + ot; i < 64; i += CI_OUT) L1c[j & 1][i] = dd_mul(Lc[j & 1][i], rj);
-      if (j < jb)
-        for (int i = j + ot; i < jb; i += CI_OUT) {
-          const dd v = i == j ? ldiag[j] : Lc[j & 1][i];
-          const int sh = -esh[i];
-          Lout[(kb + i) * n + kb + j] = dd_renorm(scale_pow2(v.hi, sh), scale_pow2(v.lo, sh));
-        }
+    const dd rj = rinv[j];
+    for (int i = j + ot; i < 64; i += CI_OUT) {
+      const dd v = i == j ? ldiag[j] : Lc[j & 1][i];
+      if (i > j) L1g[i * 64 + j] = dd_mul(v, rj);
+      if (i < jb && j < jb) {
+        const int sh = -esh[i];
+        Lout[(kb + i) * n + kb + j] = dd_renorm(scale_pow2(v.hi, sh), scale_pow2(v.lo, sh));
+      }
     }
-    const int r = j - 1;
-    if (r >= 0 && r < jb) {
-      const dd rr = rinv[r];
-      for (int c = ot; c <= r; c += CI_OUT) XT[c * jb + r] = c == r ? rr : dd_mul(rr, Y[r * 65 + c]);
-    }
+    if (ot == 0) rinvg[j] = rj;
   };
   if (critical) {  // pivot 0 and column 0
     dd r = {0.0, 0.0};
@@ -1485,41 +1468,29 @@ __global__ void __launch_bounds__(CI_THREADS) chol_inv_block_kernel(const dd* __
       for (int i = 1 + lane; i < 64; i += 32) Lc[0][i] = dd_mul(A[i * 65], r);
   }
   __syncthreads();
-  for (int j = 0; j < 64; j++) {
+  for (int j = 0; j < 63; j++) {
     if (fail) return;
     const int cur = j & 1, nxt = cur ^ 1, p = j + 1;
     if (critical) {
-      if (p < 64) {
-        // column p: last update, pivot, scale. Indices are clamped so the
-        // two chains run unconditionally (interleaved); stores are predicated.
-        const dd lpj = Lc[cur][p];
-        const int i0 = p + lane, i1 = p + 32 + lane;
-        const int i0c = min(i0, 63), i1c = min(i1, 63);
-        const dd a0 = dd_fms_fast(A[i0c * 65 + p], Lc[cur][i0c], lpj);
-        const dd a1 = dd_fms_fast(A[i1c * 65 + p], Lc[cur][i1c], lpj);
-        const dd d = {__shfl_sync(0xffffffffu, a0.hi, 0), __shfl_sync(0xffffffffu, a0.lo, 0)};  // a_pp (lane 0)
-        dd r;
-        if (pivot(p, d, r)) {
-          const dd s0 = dd_mul(a0, r), s1 = dd_mul(a1, r);
-          if (i0 < 64 && i0 > p) Lc[nxt][i0] = s0;
-          if (i1 < 64) Lc[nxt][i1] = s1;
-        }
+      // column p: last update, pivot, scale. Indices are clamped so the
+      // two chains run unconditionally (interleaved); stores are predicated.
+      const dd lpj = Lc[cur][p];
+      const int i0 = p + lane, i1 = p + 32 + lane;
+      const int i0c = min(i0, 63), i1c = min(i1, 63);
+      const dd a0 = dd_fms_fast(A[i0c * 65 + p], Lc[cur][i0c], lpj);
+      const dd a1 = dd_fms_fast(A[i1c * 65 + p], Lc[cur][i1c], lpj);
+      const dd d = {__shfl_sync(0xffffffffu, a0.hi, 0), __shfl_sync(0xffffffffu, a0.lo, 0)};  // a_pp (lane 0)
+      dd r;
+      if (pivot(p, d, r)) {
+        const dd s0 = dd_mul(a0, r), s1 = dd_mul(a1, r);
+        if (i0 < 64 && i0 > p) Lc[nxt][i0] = s0;
+        if (i1 < 64) Lc[nxt][i1] = s1;
       }
     } else if (bulk) {
-      const int Tn = j < 63 ? (62 - j) * (63 - j) / 2 : 0;  // trailing slots with column >= j + 2
-      const int total = Tn + (64 - j) * j;
-      const uint64_t magic = j > 0 ? kmagic[j - 1] : 0;     // q / j
-      const int r = j - 1;
-      int u = bt;
-      for (; u < Tn; u += CI_BULK) {
+      const int Tn = (62 - j) * (63 - j) / 2;  // trailing slots with column >= j + 2
+      for (int u = bt; u < Tn; u += CI_BULK) {
         const int ent = tab[u], i = ent >> 6, kk = ent & 63;
         A[i * 65 + kk] = dd_fms_fast(A[i * 65 + kk], Lc[cur][i], Lc[cur][kk]);
-      }
-      for (; u < total; u += CI_BULK) {
-        const int q = u - Tn;
-        const int ii = (int)(((uint64_t)q * magic) >> 32), c = q - ii * j;
-        const int i = j + ii;
-        Y[i * 65 + c] = dd_fms_fast(Y[i * 65 + c], L1c[r & 1][i], Y[r * 65 + c]);
       }
     } else {
       outputs(j);
@@ -1527,43 +1498,44 @@ __global__ void __launch_bounds__(CI_THREADS) chol_inv_block_kernel(const dd* __
     __syncthreads();
   }
   if (fail) return;
-  if (!bulk && !critical) outputs(64);  // X row 63
+  if (!bulk && !critical) outputs(63);
 }
 
-// Q = P21 X^T for the panel: Q[r][c] = sum_k P21[r][k] X[c][k] (k < jb),
-// XT[k][c] = X[c][k] in shared memory; one warp per row, lane c owns output
-// columns c and c + 32, P21[r][k] is broadcast by shuffle. Each output keeps
-// two independent partial sums (k < 32, k >= 32), so a lane has four f128
-// chains in flight. Accumulation with dd_fms_fast (f128 accuracy; the
-// products are rounded to integers next).
-__global__ void __launch_bounds__(128) panel_apply_kernel(const dd* __restrict__ P21, const dd* __restrict__ XT,
-                                                          dd* __restrict__ Q, int64_t m, int jb) {
+// L21 = P21 L~11^-T for the rows below the diagonal block. With
+// L~11 = L1 D (L1 unit lower, D = diag(l_jj)), each row z of z L1^T = P21 is a
+// forward substitution without divisions, z_c = p_c - sum_{k<c} z_k L1[c][k],
+// and L21 = z D^-1. One warp per row; lane c owns columns c and c + 32, z_k
+// is broadcast by shuffle as it becomes final; L1 sits in shared memory with
+// zeros on and above the diagonal, so every update is unconditional.
+// dd_fms_fast accumulation (f128 accuracy; the result is rounded to
+// integers next).
+__global__ void __launch_bounds__(256) panel_trsm_kernel(const dd* __restrict__ P21, const dd* __restrict__ L1g,
+                                                         const dd* __restrict__ rinvg, dd* __restrict__ Q,
+                                                         int64_t m, int jb) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
-  dd(*xs)[CH_NB] = reinterpret_cast<dd(*)[CH_NB]>(sm_raw);  // [CH_NB][CH_NB]
-  for (int q = threadIdx.x; q < CH_NB * CH_NB; q += blockDim.x) {
-    const int k = q / CH_NB, c = q % CH_NB;
-    xs[k][c] = (k < jb && c < jb) ? XT[k * jb + c] : dd{0.0, 0.0};
-  }
+  dd(*L1s)[CH_NB + 1] = reinterpret_cast<dd(*)[CH_NB + 1]>(sm_raw);  // [CH_NB][CH_NB + 1]
+  __shared__ dd rs[CH_NB];
+  for (int q = threadIdx.x; q < CH_NB * CH_NB; q += blockDim.x) L1s[q / CH_NB][q % CH_NB] = L1g[q];
+  if (threadIdx.x < CH_NB) rs[threadIdx.x] = rinvg[threadIdx.x];
   __syncthreads();
   const int lane = threadIdx.x % 32;
   const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
   const int64_t nw = (int64_t)gridDim.x * blockDim.x / 32;
   for (int64_t r = w0; r < m; r += nw) {
-    const dd a0 = lane < jb ? P21[r * jb + lane] : dd{0.0, 0.0};
-    const dd a1 = lane + 32 < jb ? P21[r * jb + lane + 32] : dd{0.0, 0.0};
-    dd s00 = {0.0, 0.0}, s01 = {0.0, 0.0}, s10 = {0.0, 0.0}, s11 = {0.0, 0.0};
-#pragma unroll 4
-    for (int k = 0; k < 32; k++) {
-      // -P21[r][k] and -P21[r][k + 32] (zero beyond jb, with xs zero there)
-      const dd u = {-__shfl_sync(0xffffffffu, a0.hi, k), -__shfl_sync(0xffffffffu, a0.lo, k)};
-      const dd w = {-__shfl_sync(0xffffffffu, a1.hi, k), -__shfl_sync(0xffffffffu, a1.lo, k)};
-      s00 = dd_fms_fast(s00, u, xs[k][lane]);
-      s01 = dd_fms_fast(s01, u, xs[k][lane + 32]);
-      s10 = dd_fms_fast(s10, w, xs[k + 32][lane]);
-      s11 = dd_fms_fast(s11, w, xs[k + 32][lane + 32]);
+    dd z0 = lane < jb ? P21[r * jb + lane] : dd{0.0, 0.0};
+    dd z1 = lane + 32 < jb ? P21[r * jb + lane + 32] : dd{0.0, 0.0};
+    const int kend = min(jb, 32);
+    for (int k = 0; k < kend; k++) {  // columns k < 32: both halves still move
+      const dd zk = {__shfl_sync(0xffffffffu, z0.hi, k), __shfl_sync(0xffffffffu, z0.lo, k)};
+      z0 = dd_fms_fast(z0, zk, L1s[lane][k]);
+      z1 = dd_fms_fast(z1, zk, L1s[lane + 32][k]);
     }
-    if (lane < jb) Q[r * jb + lane] = dd_add(s00, s10);
-    if (lane + 32 < jb) Q[r * jb + lane + 32] = dd_add(s01, s11);
+    for (int k = 32; k < jb; k++) {  // columns k >= 32: only the upper half moves
+      const dd zk = {__shfl_sync(0xffffffffu, z1.hi, k - 32), __shfl_sync(0xffffffffu, z1.lo, k - 32)};
+      z1 = dd_fms_fast(z1, zk, L1s[lane + 32][k]);
+    }
+    if (lane < jb) Q[r * jb + lane] = dd_mul(z0, rs[lane]);
+    if (lane + 32 < jb) Q[r * jb + lane + 32] = dd_mul(z1, rs[lane + 32]);
   }
 }
 __global__ void round_store_kernel(const dd* __restrict__ Q, int64_t m, int jb, int64_t t0, int64_t kb, int64_t n,
@@ -1641,8 +1613,8 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
   const size_t RL = round_up(n, GB_M) + GB_M;  // and rows
   const size_t nb = CH_NB;
   DevBuf ebuf(n * sizeof(int), s), e1022(Rp * sizeof(int), s), res((size_t)L * Np * Np, s),
-      lres((size_t)L * RL * KL, s), P(n * nb * 16, s), Q(n * nb * 16, s), XT(nb * nb * 16, s), err(sizeof(RnsErr), s);
-  if (!ebuf.p || !e1022.p || !res.p || !lres.p || !P.p || !Q.p || !XT.p || !err.p) {
+      lres((size_t)L * RL * KL, s), P(n * nb * 16, s), Q(n * nb * 16, s), L1(nb * nb * 16, s), RI(nb * 16, s), err(sizeof(RnsErr), s);
+  if (!ebuf.p || !e1022.p || !res.p || !lres.p || !P.p || !Q.p || !L1.p || !RI.p || !err.p) {
     set_error("rns_cholesky: workspace allocation failed");
     return HP_ERR_CUDA;
   }
@@ -1659,9 +1631,9 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
     rns_init_kernel<<<g, 256, 0, s>>>(S, n, ebuf.as<int>(), L, Np, res.as<uint8_t>());
     HP_LAUNCH_CHECK();
   }
-  const size_t inv_smem = 2 * 64 * 65 * 16;
-  HP_CUDA_TRY(cudaFuncSetAttribute(chol_inv_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)inv_smem));
-  HP_CUDA_TRY(cudaFuncSetAttribute(panel_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, CH_NB * CH_NB * 16));
+  const size_t blk_smem = 64 * 65 * 16, trsm_smem = CH_NB * (CH_NB + 1) * 16;
+  HP_CUDA_TRY(cudaFuncSetAttribute(chol_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem));
+  HP_CUDA_TRY(cudaFuncSetAttribute(panel_trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
   // Left-looking: the panel of block column kb receives all earlier updates
   // at once, A~[kb.., kb..kb+nb) -= L~[kb.., 0..kb) L~[kb..kb+nb, 0..kb)^T,
   // as one residue GEMM with N = nb and K = kb over the stored residue
@@ -1690,15 +1662,15 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
     }
 #undef HP_CRTB
     HP_LAUNCH_CHECK();
-    chol_inv_block_kernel<<<1, CI_THREADS, inv_smem, s>>>(P.as<dd>(), jb, (int64_t)kb, (int64_t)n, ebuf.as<int>(), Lout,
-                                                          XT.as<dd>(), err.as<RnsErr>());
+    chol_block_kernel<<<1, CI_THREADS, blk_smem, s>>>(P.as<dd>(), jb, (int64_t)kb, (int64_t)n, ebuf.as<int>(), Lout,
+                                                      L1.as<dd>(), RI.as<dd>(), err.as<RnsErr>());
     HP_LAUNCH_CHECK();
     if (R <= (size_t)jb) break;
     const size_t m = R - jb, t0 = kb + jb;
     {
-      const unsigned blocks = (unsigned)std::min<size_t>((m + 3) / 4, (size_t)D->num_sms * 8);
-      panel_apply_kernel<<<blocks, 128, CH_NB * CH_NB * 16, s>>>(P.as<dd>() + (size_t)jb * jb, XT.as<dd>(), Q.as<dd>(),
-                                                                 (int64_t)m, jb);
+      const unsigned blocks = (unsigned)std::min<size_t>((m + 7) / 8, (size_t)D->num_sms * 3);
+      panel_trsm_kernel<<<blocks, 256, trsm_smem, s>>>(P.as<dd>() + (size_t)jb * jb, L1.as<dd>(), RI.as<dd>(), Q.as<dd>(),
+                                                        (int64_t)m, jb);
       HP_LAUNCH_CHECK();
     }
     round_store_kernel<<<(unsigned)((m * jb + 255) / 256), 256, 0, s>>>(Q.as<dd>(), (int64_t)m, jb, (int64_t)t0,
