@@ -1389,17 +1389,20 @@ __device__ __forceinline__ dd dd_rsqrt(dd d) {
 // in f128: L~11 scaled back to Lout, and for the panel solve the unit lower
 // factor L1 = L~11 diag(1 / l_jj) (row-major 64 x 64, zero on and above the
 // diagonal) with rinv[j] = 1 / l_jj. The block is padded to 64 x 64 with the
-// identity, so every step has the same shape. Iteration j (one barrier):
-//   warp 31 (the critical path): column p = j + 1 gets its last update
-//     a_ip -= l_ij l_pj (i >= p); every lane forms 1/sqrt(a_pp) and the
-//     column is scaled, l_ip = a_ip / sqrt(a_pp), into the next column
-//     buffer.
+// identity, so every step has the same shape. Columns go in pairs
+// (2q, 2q + 1); iteration q (one barrier):
+//   warp 31 (the critical path): pair q + 1 gets its last updates from
+//     pair q (four independent chains per lane), then column 2q + 2 is
+//     pivoted and scaled, applied to column 2q + 3 inside the warp, and
+//     column 2q + 3 is pivoted and scaled; every lane forms each 1/sqrt from
+//     the same value, so nothing needs broadcasting but the two l values.
 //   the bulk warps (those on the three other schedulers, warp % 4 != 3):
-//     every other live update of step j, a_ik -= l_ij l_kj for
-//     j + 2 <= k <= i (a table ordered by column makes these the first
-//     T_{j+1} slots).
-//   the other warps of warp 31's scheduler: column j to Lout, L1 and rinv.
-// Updates use dd_fms_fast (f128-level accuracy, not the reference's bits).
+//     pair q applied to every column k >= 2q + 4 (rows i >= k; a table
+//     ordered by column makes these the first T slots).
+//   the other warps of warp 31's scheduler: pair q to Lout, L1 and rinv.
+// Each entry receives its column updates in column order, as in a plain
+// right-looking Cholesky; dd_fms_fast (f128-level accuracy, not the
+// reference's bits).
 constexpr int CI_THREADS = 1024;
 constexpr int CI_BULK = CI_THREADS / 4 * 3;  // warps with warp % 4 != 3
 constexpr int CI_OUT = CI_THREADS / 4 - 32;  // the other warps with warp % 4 == 3
@@ -1409,7 +1412,7 @@ __global__ void __launch_bounds__(CI_THREADS) chol_block_kernel(const dd* __rest
                                                                 dd* __restrict__ rinvg, RnsErr* err) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   dd* A = reinterpret_cast<dd*>(sm_raw);  // [64][65]
-  __shared__ dd Lc[2][64];                // scaled column j of L~, double-buffered
+  __shared__ dd Lc[2][2][64];             // scaled columns 2q, 2q + 1 of L~, double-buffered
   __shared__ dd rinv[64], ldiag[64];      // 1 / l_jj and l_jj = sqrt(a_jj)
   __shared__ uint16_t tab[2016];          // (i << 6) | k, column k = 63..1, rows i = k..63
   __shared__ int esh[64];
@@ -1431,7 +1434,7 @@ __global__ void __launch_bounds__(CI_THREADS) chol_block_kernel(const dd* __rest
   }
   __syncthreads();
   // Pivot p on warp 31, branch-free: every lane forms r = 1/sqrt(d) from
-  // the same d (so no broadcast is needed); a failure is flagged once.
+  // the same d; a failure is flagged once.
   auto pivot = [&](int p, dd d, dd& r) -> bool {
     if (!(d.hi > 0.0)) {
       if (lane == 0) {
@@ -1448,57 +1451,79 @@ __global__ void __launch_bounds__(CI_THREADS) chol_block_kernel(const dd* __rest
     }
     return true;
   };
-  // column j of L~ (from the buffer warp 31 filled one iteration earlier)
-  // to Lout, L1 and rinv
-  auto outputs = [&](int j) {
-    const dd rj = rinv[j];
-    for (int i = j + ot; i < 64; i += CI_OUT) {
-      const dd v = i == j ? ldiag[j] : Lc[j & 1][i];
-      if (i > j) L1g[i * 64 + j] = dd_mul(v, rj);
-      if (i < jb && j < jb) {
-        const int sh = -esh[i];
-        Lout[(kb + i) * n + kb + j] = dd_renorm(scale_pow2(v.hi, sh), scale_pow2(v.lo, sh));
-      }
-    }
-    if (ot == 0) rinvg[j] = rj;
+  // Factor the pair (c0, c0 + 1) on warp 31 from its updated entries a?0
+  // (column c0) and a?1 (column c0 + 1) at rows c0 + lane and c0 + 32 + lane;
+  // scaled columns to buffer b.
+  auto factor_pair = [&](int c0, dd a00, dd a10, dd a01, dd a11, int b) -> bool {
+    const int c1 = c0 + 1, i0 = c0 + lane, i1 = c0 + 32 + lane;
+    dd r0, r1;
+    const dd d0 = {__shfl_sync(0xffffffffu, a00.hi, 0), __shfl_sync(0xffffffffu, a00.lo, 0)};
+    if (!pivot(c0, d0, r0)) return false;
+    const dd s00 = dd_mul(a00, r0), s10 = dd_mul(a10, r0);
+    const dd l10 = {__shfl_sync(0xffffffffu, s00.hi, 1), __shfl_sync(0xffffffffu, s00.lo, 1)};  // l_{c1,c0}
+    a01 = dd_fms_fast(a01, s00, l10);
+    a11 = dd_fms_fast(a11, s10, l10);
+    const dd d1 = {__shfl_sync(0xffffffffu, a01.hi, 1), __shfl_sync(0xffffffffu, a01.lo, 1)};
+    if (!pivot(c1, d1, r1)) return false;
+    const dd s01 = dd_mul(a01, r1), s11 = dd_mul(a11, r1);
+    if (i0 < 64 && i0 > c0) Lc[b][0][i0] = s00;
+    if (i1 < 64) Lc[b][0][i1] = s10;
+    if (i0 < 64 && i0 > c1) Lc[b][1][i0] = s01;
+    if (i1 < 64) Lc[b][1][i1] = s11;
+    return true;
   };
-  if (critical) {  // pivot 0 and column 0
-    dd r = {0.0, 0.0};
-    if (pivot(0, A[0], r))
-      for (int i = 1 + lane; i < 64; i += 32) Lc[0][i] = dd_mul(A[i * 65], r);
+  // pair q (columns 2q, 2q + 1, buffer q & 1) to Lout, L1 and rinv
+  auto outputs = [&](int q) {
+    for (int h = 0; h < 2; h++) {
+      const int j = 2 * q + h;
+      const dd rj = rinv[j];
+      for (int i = j + ot; i < 64; i += CI_OUT) {
+        const dd v = i == j ? ldiag[j] : Lc[q & 1][h][i];
+        if (i > j) L1g[i * 64 + j] = dd_mul(v, rj);
+        if (i < jb && j < jb) {
+          const int sh = -esh[i];
+          Lout[(kb + i) * n + kb + j] = dd_renorm(scale_pow2(v.hi, sh), scale_pow2(v.lo, sh));
+        }
+      }
+      if (ot == 0) rinvg[j] = rj;
+    }
+  };
+  if (critical) {  // pair 0
+    const int i0 = lane, i1 = 32 + lane;
+    factor_pair(0, A[i0 * 65], A[i1 * 65], A[i0 * 65 + 1], A[i1 * 65 + 1], 0);
   }
   __syncthreads();
-  for (int j = 0; j < 63; j++) {
+  for (int q = 0; q < 32; q++) {
     if (fail) return;
-    const int cur = j & 1, nxt = cur ^ 1, p = j + 1;
+    const int cur = q & 1, nxt = cur ^ 1;
     if (critical) {
-      // column p: last update, pivot, scale. Indices are clamped so the
-      // two chains run unconditionally (interleaved); stores are predicated.
-      const dd lpj = Lc[cur][p];
-      const int i0 = p + lane, i1 = p + 32 + lane;
-      const int i0c = min(i0, 63), i1c = min(i1, 63);
-      const dd a0 = dd_fms_fast(A[i0c * 65 + p], Lc[cur][i0c], lpj);
-      const dd a1 = dd_fms_fast(A[i1c * 65 + p], Lc[cur][i1c], lpj);
-      const dd d = {__shfl_sync(0xffffffffu, a0.hi, 0), __shfl_sync(0xffffffffu, a0.lo, 0)};  // a_pp (lane 0)
-      dd r;
-      if (pivot(p, d, r)) {
-        const dd s0 = dd_mul(a0, r), s1 = dd_mul(a1, r);
-        if (i0 < 64 && i0 > p) Lc[nxt][i0] = s0;
-        if (i1 < 64) Lc[nxt][i1] = s1;
+      if (q < 31) {
+        // pair q + 1 (columns c0, c0 + 1): last updates from pair q. Indices
+        // are clamped so the chains run unconditionally; stores are predicated.
+        const int c0 = 2 * q + 2, c1 = c0 + 1;
+        const int i0c = min(c0 + lane, 63), i1c = min(c0 + 32 + lane, 63);
+        const dd* la = Lc[cur][0];
+        const dd* lb = Lc[cur][1];
+        const dd a00 = dd_fms_fast(dd_fms_fast(A[i0c * 65 + c0], la[i0c], la[c0]), lb[i0c], lb[c0]);
+        const dd a10 = dd_fms_fast(dd_fms_fast(A[i1c * 65 + c0], la[i1c], la[c0]), lb[i1c], lb[c0]);
+        const dd a01 = dd_fms_fast(dd_fms_fast(A[i0c * 65 + c1], la[i0c], la[c1]), lb[i0c], lb[c1]);
+        const dd a11 = dd_fms_fast(dd_fms_fast(A[i1c * 65 + c1], la[i1c], la[c1]), lb[i1c], lb[c1]);
+        factor_pair(c0, a00, a10, a01, a11, nxt);
       }
     } else if (bulk) {
-      const int Tn = (62 - j) * (63 - j) / 2;  // trailing slots with column >= j + 2
+      const int m = 60 - 2 * q;  // columns >= 2q + 4: T = m (m + 1) / 2 slots
+      const int Tn = m > 0 ? m * (m + 1) / 2 : 0;
+      const dd* la = Lc[cur][0];
+      const dd* lb = Lc[cur][1];
       for (int u = bt; u < Tn; u += CI_BULK) {
         const int ent = tab[u], i = ent >> 6, kk = ent & 63;
-        A[i * 65 + kk] = dd_fms_fast(A[i * 65 + kk], Lc[cur][i], Lc[cur][kk]);
+        A[i * 65 + kk] = dd_fms_fast(dd_fms_fast(A[i * 65 + kk], la[i], la[kk]), lb[i], lb[kk]);
       }
     } else {
-      outputs(j);
+      outputs(q);
     }
     __syncthreads();
   }
-  if (fail) return;
-  if (!bulk && !critical) outputs(63);
 }
 
 // L21 = P21 L~11^-T for the rows below the diagonal block. With
