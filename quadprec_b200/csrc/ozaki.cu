@@ -1532,11 +1532,14 @@ __global__ void __launch_bounds__(CI_THREADS) chol_block_kernel(const dd* __rest
 // and L21 = z D^-1. One warp per row; lane c owns columns c and c + 32, z_k
 // is broadcast by shuffle as it becomes final; L1 sits in shared memory with
 // zeros on and above the diagonal, so every update is unconditional.
-// dd_fms_fast accumulation (f128 accuracy; the result is rounded to
-// integers next).
+// dd_fms_fast accumulation (f128 accuracy). Epilogue: each entry is rounded
+// to an integer, written scaled back to Lout (rows t0.., columns kb..) and,
+// as balanced bytes modulo every modulus, to the L~ residue planes.
 __global__ void __launch_bounds__(256) panel_trsm_kernel(const dd* __restrict__ P21, const dd* __restrict__ L1g,
-                                                         const dd* __restrict__ rinvg, dd* __restrict__ Q,
-                                                         int64_t m, int jb) {
+                                                         const dd* __restrict__ rinvg, int64_t m, int jb, int64_t t0,
+                                                         int64_t kb, int64_t n, const int* __restrict__ e,
+                                                         dd* __restrict__ Lout, int L, int8_t* __restrict__ lres,
+                                                         int64_t ld, int64_t plane) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   dd(*L1s)[CH_NB + 1] = reinterpret_cast<dd(*)[CH_NB + 1]>(sm_raw);  // [CH_NB][CH_NB + 1]
   __shared__ dd rs[CH_NB];
@@ -1559,25 +1562,23 @@ __global__ void __launch_bounds__(256) panel_trsm_kernel(const dd* __restrict__ 
       const dd zk = {__shfl_sync(0xffffffffu, z1.hi, k - 32), __shfl_sync(0xffffffffu, z1.lo, k - 32)};
       z1 = dd_fms_fast(z1, zk, L1s[lane + 32][k]);
     }
-    if (lane < jb) Q[r * jb + lane] = dd_mul(z0, rs[lane]);
-    if (lane + 32 < jb) Q[r * jb + lane + 32] = dd_mul(z1, rs[lane + 32]);
+    const int sh = -e[t0 + r];
+    for (int h = 0; h < 2; h++) {
+      const int c = lane + 32 * h;
+      if (c >= jb) continue;
+      const dd x = dd_mul(h ? z1 : z0, rs[c]);
+      // L~21 rounded to an integer: scaled back into Lout, and its residues
+      // into row t0 + r, column kb + c of the L~ residue planes
+      const dd xr = dd_renorm(rint(x.hi), rint(x.lo));
+      Lout[(t0 + r) * n + kb + c] = dd_renorm(scale_pow2(xr.hi, sh), scale_pow2(xr.lo, sh));
+      int32_t D[NDIG];
+      element_digits(make_double2(x.hi, x.lo), 0, D);
+      int8_t* dst = lres + (t0 + r) * ld + kb + c;
+      for (int l = 0; l < L; l++) dst[(size_t)l * plane] = (int8_t)balanced_byte(D, l, c_tab.mod[l]);
+    }
   }
 }
-__global__ void round_store_kernel(const dd* __restrict__ Q, int64_t m, int jb, int64_t t0, int64_t kb, int64_t n,
-                                   const int* __restrict__ e, dd* __restrict__ Lout) {
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= m * jb) return;
-  const int64_t r = idx / jb, c = idx % jb;
-  const dd v = Q[idx];
-  const dd x = dd_renorm(rint(v.hi), rint(v.lo));
-  const int sh = -e[t0 + r];
-  Lout[(t0 + r) * n + kb + c] = dd_renorm(scale_pow2(x.hi, sh), scale_pow2(x.lo, sh));
-}
 
-__global__ void fill_int_kernel(int* p, int64_t n, int v) {
-  const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i < n) p[i] = v;
-}
 
 }  // namespace ozaki
 
@@ -1632,14 +1633,13 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
   const int nc = T.crt[L].nc;
   const dd* S = reinterpret_cast<const dd*>(S_);
   dd* Lout = reinterpret_cast<dd*>(L_);
-  const size_t Rp = round_up(n, GB_N);   // rows of the scale vector e1022
-  const size_t Np = Rp + GB_N;           // residue planes of A~ (room for tile overhang)
+  const size_t Np = round_up(n, GB_N) + GB_N;  // residue planes of A~ (room for tile overhang)
   const size_t KL = round_up(n, GB_K);   // L~ residue planes: row length (bytes)
   const size_t RL = round_up(n, GB_M) + GB_M;  // and rows
   const size_t nb = CH_NB;
-  DevBuf ebuf(n * sizeof(int), s), e1022(Rp * sizeof(int), s), res((size_t)L * Np * Np, s),
-      lres((size_t)L * RL * KL, s), P(n * nb * 16, s), Q(n * nb * 16, s), L1(nb * nb * 16, s), RI(nb * 16, s), err(sizeof(RnsErr), s);
-  if (!ebuf.p || !e1022.p || !res.p || !lres.p || !P.p || !Q.p || !L1.p || !RI.p || !err.p) {
+  DevBuf ebuf(n * sizeof(int), s), res((size_t)L * Np * Np, s), lres((size_t)L * RL * KL, s), P(n * nb * 16, s),
+      L1(nb * nb * 16, s), RI(nb * 16, s), err(sizeof(RnsErr), s);
+  if (!ebuf.p || !res.p || !lres.p || !P.p || !L1.p || !RI.p || !err.p) {
     set_error("rns_cholesky: workspace allocation failed");
     return HP_ERR_CUDA;
   }
@@ -1649,7 +1649,6 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
   HP_CUDA_TRY(cudaMemsetAsync(lres.p, 0, (size_t)L * RL * KL, s));
   if ((const void*)S_ != (const void*)L_) HP_CUDA_TRY(cudaMemcpyAsync(L_, S_, n * n * 16, cudaMemcpyDeviceToDevice, s));
   rns_scale_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(S, n, BETA_CH, ebuf.as<int>(), err.as<RnsErr>());
-  fill_int_kernel<<<(unsigned)((Rp + 255) / 256), 256, 0, s>>>(e1022.as<int>(), Rp, 1022);
   HP_LAUNCH_CHECK();
   {
     dim3 g((unsigned)(Np / 32), (unsigned)(Np / 64));
@@ -1694,18 +1693,10 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
     const size_t m = R - jb, t0 = kb + jb;
     {
       const unsigned blocks = (unsigned)std::min<size_t>((m + 7) / 8, (size_t)D->num_sms * 3);
-      panel_trsm_kernel<<<blocks, 256, trsm_smem, s>>>(P.as<dd>() + (size_t)jb * jb, L1.as<dd>(), RI.as<dd>(), Q.as<dd>(),
-                                                        (int64_t)m, jb);
-      HP_LAUNCH_CHECK();
-    }
-    round_store_kernel<<<(unsigned)((m * jb + 255) / 256), 256, 0, s>>>(Q.as<dd>(), (int64_t)m, jb, (int64_t)t0,
-                                                                        (int64_t)kb, (int64_t)n, ebuf.as<int>(), Lout);
-    HP_LAUNCH_CHECK();
-    {  // residues of the rounded L~21 into rows t0.., columns kb..kb+nb of the L~ planes
-      dim3 g((unsigned)(CH_NB / RT_P), (unsigned)((m + RT_R - 1) / RT_R), 4);
-      residue_kernel<true><<<g, 256, 0, s>>>(Q.as<double2>(), (int64_t)m, (int64_t)jb, e1022.as<int>(), 0, L,
-                                             (int64_t)KL, (int64_t)(RL * KL),
-                                             reinterpret_cast<int8_t*>(lres.as<uint8_t>() + t0 * KL + kb));
+      panel_trsm_kernel<<<blocks, 256, trsm_smem, s>>>(P.as<dd>() + (size_t)jb * jb, L1.as<dd>(), RI.as<dd>(), (int64_t)m,
+                                                        jb, (int64_t)t0, (int64_t)kb, (int64_t)n, ebuf.as<int>(), Lout, L,
+                                                        reinterpret_cast<int8_t*>(lres.as<uint8_t>()), (int64_t)KL,
+                                                        (int64_t)(RL * KL));
       HP_LAUNCH_CHECK();
     }
   }
