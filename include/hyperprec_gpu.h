@@ -147,6 +147,25 @@ int hp_f128_matvec(const double* a, const double* x, double* y, size_t n);
 int hp_f128_cond_estimate(const double* l, size_t n, double* kappa);
 
 /* ------------------------------------------------------------------------
+ * f256 (MultiFloat<4>) Cholesky and solve
+ * ---------------------------------------------------------------------- */
+/* replaces: pub fn mf_cholesky<const N: usize>(a, n) -> Result<(), &str>  (N = 4)
+ *           crates/quad/src/multifloat/linalg.rs:88-139
+ * In place on AoS f256 (4 limbs per entry): the lower triangle becomes L,
+ * bit-identical to the reference; the strict upper triangle is untouched.
+ * A first limb <= 0 on the diagonal returns HP_ERR_NOT_SPD with *pivot
+ * (may be NULL). */
+int hp_f256_cholesky(double* a, size_t n, int64_t* pivot);
+/* Device-pointer form (32-byte aligned); synchronises `stream`. */
+int hp_f256_cholesky_dev(double* a, size_t n, int64_t* pivot, void* stream);
+/* replaces: pub fn mf_cholesky_solve<const N: usize>(l, b, x, n)  (N = 4)
+ *           crates/quad/src/multifloat/linalg.rs:141-172
+ * L L^T x = b. The forward sweep is bit-identical; the backward sweep
+ * applies each row's subtractions in descending instead of ascending order
+ * (f256-level accuracy). */
+int hp_f256_cholesky_solve(const double* l, const double* b, double* x, size_t n);
+
+/* ------------------------------------------------------------------------
  * SPD solver (crates/solver/src/lib.rs)
  * ---------------------------------------------------------------------- */
 typedef struct {
@@ -280,6 +299,16 @@ int hp_f128_jacobi_eigen(const double* a, size_t n, size_t max_iter, double* eva
 int hp_f128_jacobi_eigen_batched_dev(int count, const int64_t* n_off, const double* A,
                                      size_t max_iter, double* evals, double* evecs,
                                      int32_t* sweeps, int32_t* status, void* stream);
+
+/* replaces: pub fn canonical_orthogonalize(s: &[f128], n: usize, threshold: f64) -> OrthoBasis
+ *           crates/solver/src/ortho.rs:147-183
+ * X = U diag(1 / sqrt(lambda)) over the eigenvalues with (hi + lo) > threshold,
+ * ascending; x receives n x m f128 row-major (capacity n x n), *n_orth = m.
+ * Eigenpairs from the GPU Jacobi solver above (the reference uses a private
+ * max-pivot Jacobi): eigenvalues to f128 rounding, each column of X to
+ * rounding and sign. n <= 128. */
+int hp_canonical_orthogonalize(const double* s, size_t n, double threshold, double* x,
+                               size_t* n_orth);
 
 #ifdef __cplusplus
 }

@@ -67,6 +67,10 @@ SIGNATURES = {
     "hp_f128_solve_cholesky": ([_vp, _vp, _vp, _sz], ctypes.c_int),
     "hp_f128_matvec": ([_vp, _vp, _vp, _sz], ctypes.c_int),
     "hp_f128_cond_estimate": ([_vp, _sz, _d], ctypes.c_int),
+    "hp_f256_cholesky": ([_vp, _sz, _i64p], ctypes.c_int),
+    "hp_f256_cholesky_dev": ([_vp, _sz, _i64p, _vp], ctypes.c_int),
+    "hp_f256_cholesky_solve": ([_vp, _vp, _vp, _sz], ctypes.c_int),
+    "hp_canonical_orthogonalize": ([_vp, _sz, ctypes.c_double, _vp, ctypes.POINTER(_sz)], ctypes.c_int),
     "hp_solve_spd": ([_vp, _vp, _sz, _vp, _vp, _vp, _i64p], ctypes.c_int),
     "hp_solve_spd_f128": ([_vp, _vp, _sz, _vp, _vp, _vp, _i64p], ctypes.c_int),
     "hp_spd_solve_refined": ([_vp, _vp, _sz, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp, _vp, _i64p],
@@ -208,6 +212,36 @@ def f128_cholesky(a, n):
 def f128_cholesky_blocked(a, n, nb):
     """linalg.rs:238 cholesky_blocked."""
     return _chol_call(lib().hp_f128_cholesky_blocked, a, n, nb)
+
+
+def f256_cholesky(a, n):
+    """multifloat/linalg.rs:88 mf_cholesky::<4>; a is (n, n, 4); returns a copy
+    with L in the lower triangle (bit-identical to the reference)."""
+    a = _c(a).copy()
+    pv = ctypes.c_int64(-1)
+    rc = lib().hp_f256_cholesky(_ptr(a), n, ctypes.byref(pv))
+    if rc == HP_ERR_NOT_SPD:
+        raise CholeskyError(pv.value, float("nan"))
+    check(rc)
+    return a
+
+
+def f256_cholesky_solve(l, b, n):
+    """multifloat/linalg.rs:141 mf_cholesky_solve::<4>; l (n, n, 4), b (n, 4)."""
+    l, b = _c(l), _c(b)
+    out = np.empty((n, 4))
+    check(lib().hp_f256_cholesky_solve(_ptr(l), _ptr(b), _ptr(out), n))
+    return out
+
+
+def canonical_orthogonalize(s, n, threshold):
+    """solver/src/ortho.rs:151 canonical_orthogonalize; s is (n, n, 2).
+    Returns X as (n, n_orth, 2)."""
+    s = _c(s)
+    x = np.zeros((n, n, 2))
+    m = _sz(0)
+    check(lib().hp_canonical_orthogonalize(_ptr(s), n, threshold, _ptr(x), ctypes.byref(m)))
+    return np.ascontiguousarray(x.reshape(-1)[: n * m.value * 2].reshape(n, m.value, 2))
 
 
 def _solve(name, l, b, n):

@@ -18,6 +18,8 @@
 //
 // Three kernels per block column: diag (one CTA), panel (one thread per row),
 // syrk (64 x 64 lower-triangular tiles of the trailing matrix, CUDA cores).
+#include <algorithm>
+
 #include "hp_arith.cuh"
 #include "hp_runtime.cuh"
 #include "kernels.cuh"
@@ -46,6 +48,22 @@ struct OpsDD {
   __device__ static T inv(T a) { return dd_recip(a); }  // linalg.rs:60: ljj.recip()
   __device__ static double hi(T a) { return a.hi; }
   __device__ static double to_f64(T a) { return __dadd_rn(a.hi, a.lo); }
+};
+
+// MultiFloat<4> (f256): mf_cholesky (crates/quad/src/multifloat/linalg.rs:88-139)
+// has the same per-column structure, sum = sum + l_jk l_jk,
+// diag = a_jj - sum, l_jj = diag.sqrt(), l_ij = (a_ij - s) * l_jj.recip(),
+// with the MultiFloat Add/Mul/sqrt/recip restated in hp_arith.cuh.
+struct OpsQD {
+  using T = qd;
+  __device__ static T zero() { return qd_zero(); }
+  __device__ static T add(T a, T b) { return qd_add(a, b); }
+  __device__ static T sub(T a, T b) { return qd_sub(a, b); }
+  __device__ static T mul(T a, T b) { return qd_mul(a, b); }
+  __device__ static T sqrt_(T a) { return qd_sqrt(a); }
+  __device__ static T inv(T a) { return qd_recip(a); }
+  __device__ static double hi(T a) { return a.l[0]; }
+  __device__ static double to_f64(T a) { return a.l[0]; }
 };
 
 struct CholErr {
@@ -146,13 +164,15 @@ __global__ void __launch_bounds__(64) chol_panel_kernel(typename O::T* A, const 
 // Trailing update on the lower triangle of rows/cols >= t0 = kb + jb:
 //   unblocked semantics: S_ij = S_ij + sum_{k in block} L_ik L_jk  (k order)
 //   BLOCKED:             A_ij = A_ij - (sum_{k in block} L_ik L_jk)
-// 64 x 64 tiles, 256 threads, 4 x 4 entries per thread; the block's jb
-// columns are staged through shared memory in k-slices of 16.
-template <class O, bool BLOCKED>
+// (16 TT) x (16 TT) tiles, 256 threads, TT x TT entries per thread (TT = 4 for
+// f64/f128, 2 for f256); the block's jb columns are staged through shared
+// memory in k-slices of 16.
+template <class O, bool BLOCKED, int TT>
 __global__ void __launch_bounds__(256) chol_syrk_kernel(typename O::T* A, typename O::T* S, int64_t n, int64_t kb,
                                                         int jb, const CholErr* err) {
   using T = typename O::T;
-  __shared__ T Ps[16][64 + 1], Qs[16][64 + 1];
+  constexpr int TL = 16 * TT;
+  __shared__ T Ps[16][TL + 1], Qs[16][TL + 1];
   if (err->flag) return;
   const int64_t t0 = kb + jb;
   // lower-triangular tile index -> (bi, bj), bi >= bj
@@ -161,19 +181,19 @@ __global__ void __launch_bounds__(256) chol_syrk_kernel(typename O::T* A, typena
   while (bi * (bi + 1) / 2 > idx) bi--;
   while ((bi + 1) * (bi + 2) / 2 <= idx) bi++;
   const int64_t bj = idx - bi * (bi + 1) / 2;
-  const int64_t i0 = t0 + bi * 64, j0 = t0 + bj * 64;
+  const int64_t i0 = t0 + bi * TL, j0 = t0 + bj * TL;
   const int tx = threadIdx.x % 16, ty = threadIdx.x / 16, tid = threadIdx.x;
-  T acc[4][4];
+  T acc[TT][TT];
 #pragma unroll
-  for (int a = 0; a < 4; a++)
+  for (int a = 0; a < TT; a++)
 #pragma unroll
-    for (int b = 0; b < 4; b++) {
+    for (int b = 0; b < TT; b++) {
       int64_t i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
       acc[a][b] = (!BLOCKED && i < n && j < n && j <= i) ? S[i * n + j] : O::zero();
     }
   for (int k0 = 0; k0 < jb; k0 += 16) {
     __syncthreads();
-    for (int e = tid; e < 16 * 64; e += 256) {
+    for (int e = tid; e < 16 * TL; e += 256) {
       int r = e / 16, c = e % 16;  // row r of the tile, k offset c
       int64_t gi = i0 + r, gj = j0 + r;
       bool kin = k0 + c < jb;
@@ -183,21 +203,21 @@ __global__ void __launch_bounds__(256) chol_syrk_kernel(typename O::T* A, typena
     __syncthreads();
     const int kmax = min(16, jb - k0);
     for (int kk = 0; kk < kmax; kk++) {
-      T p[4], q[4];
+      T p[TT], q[TT];
 #pragma unroll
-      for (int a = 0; a < 4; a++) p[a] = Ps[kk][ty + 16 * a];
+      for (int a = 0; a < TT; a++) p[a] = Ps[kk][ty + 16 * a];
 #pragma unroll
-      for (int b = 0; b < 4; b++) q[b] = Qs[kk][tx + 16 * b];
+      for (int b = 0; b < TT; b++) q[b] = Qs[kk][tx + 16 * b];
 #pragma unroll
-      for (int a = 0; a < 4; a++)
+      for (int a = 0; a < TT; a++)
 #pragma unroll
-        for (int b = 0; b < 4; b++) acc[a][b] = O::add(acc[a][b], O::mul(p[a], q[b]));
+        for (int b = 0; b < TT; b++) acc[a][b] = O::add(acc[a][b], O::mul(p[a], q[b]));
     }
   }
 #pragma unroll
-  for (int a = 0; a < 4; a++)
+  for (int a = 0; a < TT; a++)
 #pragma unroll
-    for (int b = 0; b < 4; b++) {
+    for (int b = 0; b < TT; b++) {
       int64_t i = i0 + ty + 16 * a, j = j0 + tx + 16 * b;
       if (i < n && j < n && j <= i) {
         if (BLOCKED)
@@ -226,13 +246,23 @@ int cholesky_run(typename O::T* A, size_t n, size_t nb, CholErr* derr, cudaStrea
   }
   T* S = Sbuf.as<T>();
   if (!BLOCKED) HP_CUDA_TRY(cudaMemsetAsync(S, 0, n * n * sizeof(T), s));
+  constexpr int TT = sizeof(T) > 16 ? 2 : 4;  // per-thread tile of the trailing update
+  constexpr int TL = 16 * TT;
   const size_t diag_smem = 64 * 65 * sizeof(T);
-  static bool attr[2] = {false, false};
-  if (!attr[0]) {
-    cudaFuncSetAttribute(chol_diag_kernel<O, BLOCKED>, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 65 * 16);
-    cudaFuncSetAttribute(chol_panel_kernel<O, BLOCKED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         (64 * 64 + 64 * 64) * 16);
-    attr[0] = true;
+  const size_t panel_max = (size_t)(nb * nb + nb * 64) * sizeof(T);
+  static bool attr[64] = {};
+  int dev = 0;
+  HP_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 64 && !attr[dev]) {
+    HP_CUDA_TRY(cudaFuncSetAttribute(chol_diag_kernel<O, BLOCKED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)diag_smem));
+    HP_CUDA_TRY(cudaFuncSetAttribute(chol_panel_kernel<O, BLOCKED>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)((64 * 64 + 64 * 64) * std::min(sizeof(T), (size_t)16))));
+    attr[dev] = true;
+  }
+  if (panel_max > (64 * 64 + 64 * 64) * std::min(sizeof(T), (size_t)16)) {
+    set_error("cholesky: block size %zu too large for this element type", nb);
+    return HP_ERR_UNSUPPORTED;
   }
   for (size_t kb = 0; kb < n; kb += nb) {
     const int jb = (int)std::min(nb, n - kb);
@@ -244,8 +274,8 @@ int cholesky_run(typename O::T* A, size_t n, size_t nb, CholErr* derr, cudaStrea
     chol_panel_kernel<O, BLOCKED><<<(unsigned)((rest + 63) / 64), 64, panel_smem, s>>>(A, S, n, kb, jb,
                                                                                       invd.as<T>(), derr);
     HP_LAUNCH_CHECK();
-    const size_t tiles = (rest + 63) / 64;
-    chol_syrk_kernel<O, BLOCKED><<<(unsigned)(tiles * (tiles + 1) / 2), 256, 0, s>>>(A, S, n, kb, jb, derr);
+    const size_t tiles = (rest + TL - 1) / TL;
+    chol_syrk_kernel<O, BLOCKED, TT><<<(unsigned)(tiles * (tiles + 1) / 2), 256, 0, s>>>(A, S, n, kb, jb, derr);
     HP_LAUNCH_CHECK();
   }
   return HP_OK;
@@ -277,6 +307,23 @@ int dd_cholesky(double* a, size_t n, size_t nb, bool blocked, int64_t* pivot, do
       set_error("Cholesky failed at pivot %lld (value=%.4e)", (long long)h.pivot, h.value);
       return HP_ERR_NOT_SPD;
     }
+  }
+  return HP_OK;
+}
+
+int qd_cholesky(double* a, size_t n, int64_t* pivot, cudaStream_t s) {
+  if (n == 0) return HP_OK;
+  DevBuf err(sizeof(CholErr), s);
+  if (!err.p) return HP_ERR_CUDA;
+  HP_CUDA_TRY(cudaMemsetAsync(err.p, 0, sizeof(CholErr), s));
+  HP_TRY((cholesky_run<OpsQD, false>(reinterpret_cast<qd*>(a), n, 32, err.as<CholErr>(), s)));
+  CholErr h;
+  HP_CUDA_TRY(cudaMemcpyAsync(&h, err.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  if (h.flag) {
+    if (pivot) *pivot = h.pivot;
+    set_error("Cholesky failed: matrix is not positive definite (pivot %lld)", (long long)h.pivot);
+    return HP_ERR_NOT_SPD;
   }
   return HP_OK;
 }
