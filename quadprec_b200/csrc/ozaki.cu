@@ -1529,14 +1529,16 @@ __global__ void __launch_bounds__(CI_THREADS) chol_block_kernel(const dd* __rest
 // L21 = P21 L~11^-T for the rows below the diagonal block. With
 // L~11 = L1 D (L1 unit lower, D = diag(l_jj)), each row z of z L1^T = P21 is a
 // forward substitution without divisions, z_c = p_c - sum_{k<c} z_k L1[c][k],
-// and L21 = z D^-1. One warp per row; lane c owns columns c and c + 32, z_k
+// and L21 = z D^-1, for panel rows r0 <= r < m. One warp per row; lane c owns
+// columns c and c + 32, z_k
 // is broadcast by shuffle as it becomes final; L1 sits in shared memory with
 // zeros on and above the diagonal, so every update is unconditional.
 // dd_fms_fast accumulation (f128 accuracy). Epilogue: each entry is rounded
 // to an integer, written scaled back to Lout (rows t0.., columns kb..) and,
 // as balanced bytes modulo every modulus, to the L~ residue planes.
 __global__ void __launch_bounds__(256) panel_trsm_kernel(const dd* __restrict__ P21, const dd* __restrict__ L1g,
-                                                         const dd* __restrict__ rinvg, int64_t m, int jb, int64_t t0,
+                                                         const dd* __restrict__ rinvg, int64_t r0, int64_t m, int jb,
+                                                         int64_t t0,
                                                          int64_t kb, int64_t n, const int* __restrict__ e,
                                                          dd* __restrict__ Lout, int L, int8_t* __restrict__ lres,
                                                          int64_t ld, int64_t plane) {
@@ -1549,7 +1551,7 @@ __global__ void __launch_bounds__(256) panel_trsm_kernel(const dd* __restrict__ 
   const int lane = threadIdx.x % 32;
   const int64_t w0 = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) / 32;
   const int64_t nw = (int64_t)gridDim.x * blockDim.x / 32;
-  for (int64_t r = w0; r < m; r += nw) {
+  for (int64_t r = r0 + w0; r < m; r += nw) {
     dd z0 = lane < jb ? P21[r * jb + lane] : dd{0.0, 0.0};
     dd z1 = lane + 32 < jb ? P21[r * jb + lane + 32] : dd{0.0, 0.0};
     const int kend = min(jb, 32);
@@ -1582,41 +1584,93 @@ __global__ void __launch_bounds__(256) panel_trsm_kernel(const dd* __restrict__ 
 
 }  // namespace ozaki
 
-// res[l][c_row0 + i][c_row0 + j] -= sum_p A[l][i][p] B[l][j][p] (mod m_l) for
-// i < R, j < CH_NB, p < K: A = the R rows of L~ residues starting at lrow,
-// B = its first CH_NB rows (row length KL bytes, rows_avail rows, planes
-// plane_stride bytes apart). One launch of the 128 x 64 tile GEMM.
-static int rns_panel_update(const uint8_t* lrow, size_t KL, size_t rows_avail, size_t plane_stride, int L, size_t R,
-                            size_t K, uint8_t* res, size_t Np, size_t c0, int num_sms, cudaStream_t s) {
+// res[l][r0 + i][c0 + j] -= sum_p A[l][i][p] B[l][j][p] (mod m_l) for
+// i < R, j < CH_NB, p < K: A = R rows of L~ residues from arow, B = CH_NB
+// rows from brow (row length KL bytes, planes plane_stride bytes apart; a
+// map spans rows_a / rows_b rows). One launch of the 128 x 64 tile GEMM on at
+// most max_ctas CTAs.
+static int rns_panel_update(const uint8_t* arow, size_t rows_a, const uint8_t* brow, size_t rows_b, size_t KL,
+                            size_t plane_stride, int L, size_t R, size_t K, uint8_t* res, size_t Np, size_t r0,
+                            size_t c0, int max_ctas, cudaStream_t s) {
   using namespace ozaki;
   constexpr int BN = CH_NB;
+  if (R == 0 || K == 0) return HP_OK;
   static bool attr_set[64] = {};
   int dev = 0;
   HP_CUDA_TRY(cudaGetDevice(&dev));
-  if (!attr_set[dev]) {
+  if (dev < 64 && !attr_set[dev]) {
     HP_CUDA_TRY(cudaFuncSetAttribute(i8_gemm_mod_kernel<BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      GemmCfg<BN>::SMEM));
     attr_set[dev] = true;
   }
   CUtensorMap mapA, mapB;
-  HP_TRY(make_map(&mapA, lrow, KL, rows_avail, L, GB_M, plane_stride));
-  HP_TRY(make_map(&mapB, lrow, KL, rows_avail, L, BN, plane_stride));
+  HP_TRY(make_map(&mapA, arow, KL, rows_a, L, GB_M, plane_stride));
+  HP_TRY(make_map(&mapB, brow, KL, rows_b, L, BN, plane_stride));
   uint32_t* status = device_status(s);
   if (!status) {
     set_error("status word allocation failed");
     return HP_ERR_CUDA;
   }
   const int tiles_m = (int)((R + GB_M - 1) / GB_M);
-  const int grid = std::min(L * tiles_m, num_sms);
+  const int grid = std::max(1, std::min(L * tiles_m, max_ctas));
   const int nkb = (int)(K / GB_K), kb_chunk = MAX_K_CHUNK / GB_K;
   for (int k0 = 0; k0 < nkb; k0 += kb_chunk) {
     i8_gemm_mod_kernel<BN><<<grid, 256, GemmCfg<BN>::SMEM, s>>>(mapA, mapB, L, tiles_m, 1, k0, std::min(nkb, k0 + kb_chunk),
                                                                  0, 2, res, (int64_t)Np, (int64_t)(Np * Np),
-                                                                 (int64_t)c0, (int64_t)c0, status);
+                                                                 (int64_t)r0, (int64_t)c0, status);
     HP_LAUNCH_CHECK();
   }
   return HP_OK;
 }
+
+// The two streams of the panel pipeline (one pair per device, created once):
+// the diagonal path at the device's greatest priority, so that its blocks
+// take SMs ahead of the other path's as they free up, and the other path at
+// the least priority.
+static int pipeline_streams(cudaStream_t* hi, cudaStream_t* lo) {
+  static cudaStream_t streams[64][2] = {};
+  static std::mutex mu;
+  int dev = 0;
+  HP_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) {
+    set_error("device ordinal %d out of range", dev);
+    return HP_ERR_UNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lk(mu);
+  if (!streams[dev][0]) {
+    int least = 0, greatest = 0;
+    HP_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    HP_CUDA_TRY(cudaStreamCreateWithPriority(&streams[dev][0], cudaStreamNonBlocking, greatest));
+    HP_CUDA_TRY(cudaStreamCreateWithPriority(&streams[dev][1], cudaStreamNonBlocking, least));
+  }
+  *hi = streams[dev][0];
+  *lo = streams[dev][1];
+  return HP_OK;
+}
+
+// Events of one factorisation. The pipeline streams start after the
+// caller's stream; on destruction both are joined back into it, so that
+// stream-ordered frees of the workspace come after them.
+struct PipelineEvents {
+  cudaStream_t s, s1, s2;
+  cudaEvent_t F, Td, Gd, Cr, Tr[2], start, join1, join2;
+  bool ok = true;
+  PipelineEvents(cudaStream_t caller, cudaStream_t hi, cudaStream_t lo) : s(caller), s1(hi), s2(lo) {
+    for (cudaEvent_t* e : {&F, &Td, &Gd, &Cr, &Tr[0], &Tr[1], &start, &join1, &join2})
+      ok = ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
+    ok = ok && cudaEventRecord(start, s) == cudaSuccess && cudaStreamWaitEvent(s1, start, 0) == cudaSuccess &&
+         cudaStreamWaitEvent(s2, start, 0) == cudaSuccess;
+  }
+  void join() {
+    if (!ok) return;
+    if (cudaEventRecord(join1, s1) == cudaSuccess) cudaStreamWaitEvent(s, join1, 0);
+    if (cudaEventRecord(join2, s2) == cudaSuccess) cudaStreamWaitEvent(s, join2, 0);
+  }
+  ~PipelineEvents() {
+    join();
+    for (cudaEvent_t e : {F, Td, Gd, Cr, Tr[0], Tr[1], start, join1, join2}) cudaEventDestroy(e);
+  }
+};
 
 int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStream_t s) {
   using namespace ozaki;
@@ -1637,9 +1691,9 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
   const size_t KL = round_up(n, GB_K);   // L~ residue planes: row length (bytes)
   const size_t RL = round_up(n, GB_M) + GB_M;  // and rows
   const size_t nb = CH_NB;
-  DevBuf ebuf(n * sizeof(int), s), res((size_t)L * Np * Np, s), lres((size_t)L * RL * KL, s), P(n * nb * 16, s),
-      L1(nb * nb * 16, s), RI(nb * 16, s), err(sizeof(RnsErr), s);
-  if (!ebuf.p || !res.p || !lres.p || !P.p || !L1.p || !RI.p || !err.p) {
+  DevBuf ebuf(n * sizeof(int), s), res((size_t)L * Np * Np, s), lres((size_t)L * RL * KL, s),
+      Pb(2 * n * nb * 16, s), L1b(2 * nb * nb * 16, s), RIb(2 * nb * 16, s), err(sizeof(RnsErr), s);
+  if (!ebuf.p || !res.p || !lres.p || !Pb.p || !L1b.p || !RIb.p || !err.p) {
     set_error("rns_cholesky: workspace allocation failed");
     return HP_ERR_CUDA;
   }
@@ -1648,6 +1702,13 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
   HP_CUDA_TRY(cudaMemsetAsync(res.p, 0, (size_t)L * Np * Np, s));
   HP_CUDA_TRY(cudaMemsetAsync(lres.p, 0, (size_t)L * RL * KL, s));
   if ((const void*)S_ != (const void*)L_) HP_CUDA_TRY(cudaMemcpyAsync(L_, S_, n * n * 16, cudaMemcpyDeviceToDevice, s));
+  cudaStream_t s_caller = s, s2 = nullptr;
+  HP_TRY(pipeline_streams(&s, &s2));
+  PipelineEvents ev(s_caller, s, s2);  // declared after the buffers: joins both streams before they are freed
+  if (!ev.ok) {
+    set_error("rns_cholesky: event creation failed");
+    return HP_ERR_CUDA;
+  }
   rns_scale_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(S, n, BETA_CH, ebuf.as<int>(), err.as<RnsErr>());
   HP_LAUNCH_CHECK();
   {
@@ -1658,25 +1719,16 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
   const size_t blk_smem = 64 * 65 * 16, trsm_smem = CH_NB * (CH_NB + 1) * 16;
   HP_CUDA_TRY(cudaFuncSetAttribute(chol_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem));
   HP_CUDA_TRY(cudaFuncSetAttribute(panel_trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
-  // Left-looking: the panel of block column kb receives all earlier updates
-  // at once, A~[kb.., kb..kb+nb) -= L~[kb.., 0..kb) L~[kb..kb+nb, 0..kb)^T,
-  // as one residue GEMM with N = nb and K = kb over the stored residue
-  // planes of L~ (columns from kb on are still zero there, so K may be
-  // rounded up to the 128-byte k-block). The integers are those of the
-  // right-looking order; only the schedule differs.
-  for (size_t kb = 0; kb < n; kb += nb) {
-    const int jb = (int)std::min(nb, n - kb);
-    const size_t R = n - kb;
-    if (kb > 0) {
-      const uint8_t* lrow = lres.as<uint8_t>() + kb * KL;
-      HP_TRY(rns_panel_update(lrow, KL, RL - kb, RL * KL, L, R, round_up(kb, GB_K), res.as<uint8_t>(),
-                              Np, kb, D->num_sms, s));
-    }
-#define HP_CRTB(NC)                                                                                          \
-  case NC:                                                                                                   \
-    crt_block_kernel<NC><<<(unsigned)((R * jb + 255) / 256), 256, 0, s>>>(                                    \
-        res.as<uint8_t>(), (int64_t)Np, (int64_t)(Np * Np), (int64_t)kb, (int64_t)kb, (int64_t)R, (int64_t)jb, \
-        D->crt + L, P.as<dd>());                                                                             \
+  int8_t* lres8 = reinterpret_cast<int8_t*>(lres.as<uint8_t>());
+  const size_t plane_l = RL * KL;
+  const int gemm_ctas = std::max(1, D->num_sms - 8);  // leave SMs for the diagonal path
+  auto crt = [&](size_t r0, size_t rows, size_t kb, int jb, dd* out, cudaStream_t st) -> int {
+    if (rows == 0) return HP_OK;
+#define HP_CRTB(NC)                                                                                            \
+  case NC:                                                                                                     \
+    crt_block_kernel<NC><<<(unsigned)((rows * jb + 255) / 256), 256, 0, st>>>(                                  \
+        res.as<uint8_t>(), (int64_t)Np, (int64_t)(Np * Np), (int64_t)r0, (int64_t)kb, (int64_t)rows, (int64_t)jb, \
+        D->crt + L, out);                                                                                      \
     break;
     switch (nc) {
       HP_CRTB(5) HP_CRTB(6) HP_CRTB(7)
@@ -1686,20 +1738,72 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
     }
 #undef HP_CRTB
     HP_LAUNCH_CHECK();
-    chol_block_kernel<<<1, CI_THREADS, blk_smem, s>>>(P.as<dd>(), jb, (int64_t)kb, (int64_t)n, ebuf.as<int>(), Lout,
-                                                      L1.as<dd>(), RI.as<dd>(), err.as<RnsErr>());
+    return HP_OK;
+  };
+  auto trsm = [&](int par, size_t kb, int jb, size_t r0, size_t m, cudaStream_t st) -> int {
+    if (r0 >= m) return HP_OK;
+    const unsigned blocks = (unsigned)std::min<size_t>((m - r0 + 7) / 8, (size_t)D->num_sms * 3);
+    panel_trsm_kernel<<<blocks, 256, trsm_smem, st>>>(Pb.as<dd>() + (size_t)par * n * nb + (size_t)jb * jb,
+                                                       L1b.as<dd>() + (size_t)par * nb * nb, RIb.as<dd>() + par * nb,
+                                                       (int64_t)r0, (int64_t)m, jb, (int64_t)(kb + jb), (int64_t)kb,
+                                                       (int64_t)n, ebuf.as<int>(), Lout, L, lres8, (int64_t)KL,
+                                                       (int64_t)plane_l);
     HP_LAUNCH_CHECK();
-    if (R <= (size_t)jb) break;
-    const size_t m = R - jb, t0 = kb + jb;
-    {
-      const unsigned blocks = (unsigned)std::min<size_t>((m + 7) / 8, (size_t)D->num_sms * 3);
-      panel_trsm_kernel<<<blocks, 256, trsm_smem, s>>>(P.as<dd>() + (size_t)jb * jb, L1.as<dd>(), RI.as<dd>(), (int64_t)m,
-                                                        jb, (int64_t)t0, (int64_t)kb, (int64_t)n, ebuf.as<int>(), Lout, L,
-                                                        reinterpret_cast<int8_t*>(lres.as<uint8_t>()), (int64_t)KL,
-                                                        (int64_t)(RL * KL));
-      HP_LAUNCH_CHECK();
+    return HP_OK;
+  };
+  // Left-looking, with a look-ahead pipeline. The panel of block column kb
+  // receives all earlier updates at once, A~[kb.., kb..kb+nb) -=
+  // L~[kb.., 0..kb) L~[kb..kb+nb, 0..kb)^T, as residue GEMMs with N = nb and
+  // K = kb over the stored residue planes of L~ (columns from kb on are still
+  // zero there, so K may be rounded up to the 128-byte k-block). Stream s
+  // carries the diagonal path of each panel (its first 128 rows: GEMM, CRT
+  // of the diagonal block, factor, then the first 128 rows of the panel
+  // solve, which the next diagonal block needs); stream s2 carries the rest
+  // (remaining rows' GEMM, CRT and solve) alongside. Panel buffers (P, L1,
+  // 1/l) alternate by panel parity. The integers are those of the
+  // right-looking order; only the schedule differs.
+  for (size_t kb = 0, p = 0; kb < n; kb += nb, p++) {
+    const int jb = (int)std::min(nb, n - kb);
+    const size_t R = n - kb, m = R - jb;
+    const int par = (int)(p & 1);
+    dd* Pp = Pb.as<dd>() + (size_t)par * n * nb;
+    const size_t Rd = std::min<size_t>(R, GB_M);  // rows of the diagonal path's GEMM
+    if (kb == 0) {
+      HP_TRY(crt(0, R, 0, jb, Pp, s));
+    } else {
+      if (p >= 2) HP_CUDA_TRY(cudaStreamWaitEvent(s, ev.Tr[par], 0));  // solve rows of panel p - 2
+      const uint8_t* lrow = lres.as<uint8_t>() + kb * KL;
+      HP_TRY(rns_panel_update(lrow, RL - kb, lrow, RL - kb, KL, plane_l, L, Rd, round_up(kb, GB_K), res.as<uint8_t>(),
+                              Np, kb, kb, gemm_ctas, s));
+      HP_CUDA_TRY(cudaEventRecord(ev.Gd, s));
+      HP_TRY(crt(kb, (size_t)jb, kb, jb, Pp, s));
+      // s2: the rest of the panel's rows
+      HP_CUDA_TRY(cudaStreamWaitEvent(s2, ev.Td, 0));  // rows kb..kb+nb of the previous panel's solve
+      if (R > Rd) {
+        const uint8_t* arow = lres.as<uint8_t>() + (kb + Rd) * KL;
+        HP_TRY(rns_panel_update(arow, RL - kb - Rd, lrow, RL - kb, KL, plane_l, L, R - Rd, round_up(kb, GB_K),
+                                res.as<uint8_t>(), Np, kb + Rd, kb, gemm_ctas, s2));
+      }
+      HP_CUDA_TRY(cudaStreamWaitEvent(s2, ev.Gd, 0));
+      HP_TRY(crt(kb + jb, m, kb, jb, Pp + (size_t)jb * jb, s2));
+      HP_CUDA_TRY(cudaEventRecord(ev.Cr, s2));
     }
+    chol_block_kernel<<<1, CI_THREADS, blk_smem, s>>>(Pp, jb, (int64_t)kb, (int64_t)n, ebuf.as<int>(), Lout,
+                                                      L1b.as<dd>() + (size_t)par * nb * nb, RIb.as<dd>() + par * nb,
+                                                      err.as<RnsErr>());
+    HP_LAUNCH_CHECK();
+    HP_CUDA_TRY(cudaEventRecord(ev.F, s));
+    if (m == 0) break;
+    const size_t md = std::min<size_t>(m, GB_M);  // panel-solve rows on the diagonal path
+    if (kb > 0) HP_CUDA_TRY(cudaStreamWaitEvent(s, ev.Cr, 0));
+    HP_TRY(trsm(par, kb, jb, 0, md, s));
+    HP_CUDA_TRY(cudaEventRecord(ev.Td, s));
+    HP_CUDA_TRY(cudaStreamWaitEvent(s2, ev.F, 0));
+    HP_TRY(trsm(par, kb, jb, md, m, s2));
+    HP_CUDA_TRY(cudaEventRecord(ev.Tr[par], s2));
   }
+  ev.join();  // both pipeline streams finish before the caller's stream goes on
+  s = s_caller;
   RnsErr h;
   HP_CUDA_TRY(cudaMemcpyAsync(&h, err.p, sizeof(h), cudaMemcpyDeviceToHost, s));
   HP_CUDA_TRY(cudaStreamSynchronize(s));
