@@ -164,6 +164,14 @@ int hp_f256_cholesky_dev(double* a, size_t n, int64_t* pivot, void* stream);
  * applies each row's subtractions in descending instead of ascending order
  * (f256-level accuracy). */
 int hp_f256_cholesky_solve(const double* l, const double* b, double* x, size_t n);
+/* replaces: pub fn mf_gemv<const N: usize>(a, x, y, n, m)  (N = 4)
+ *           crates/quad/src/multifloat/linalg.rs:17-37
+ * y (n) = A (n x m, AoS f256) x (m); bit-identical (each row summed in
+ * column order). */
+int hp_f256_gemv(const double* a, const double* x, double* y, size_t n, size_t m);
+/* replaces: pub fn mf_dot<const N: usize>(a, b) -> MultiFloat<N>  (N = 4)
+ *           crates/quad/src/multifloat/linalg.rs:7-14; bit-identical. */
+int hp_f256_dot(const double* a, const double* b, size_t len, double* out);
 
 /* ------------------------------------------------------------------------
  * SPD solver (crates/solver/src/lib.rs)

@@ -70,6 +70,8 @@ SIGNATURES = {
     "hp_f256_cholesky": ([_vp, _sz, _i64p], ctypes.c_int),
     "hp_f256_cholesky_dev": ([_vp, _sz, _i64p, _vp], ctypes.c_int),
     "hp_f256_cholesky_solve": ([_vp, _vp, _vp, _sz], ctypes.c_int),
+    "hp_f256_gemv": ([_vp, _vp, _vp, _sz, _sz], ctypes.c_int),
+    "hp_f256_dot": ([_vp, _vp, _sz, _vp], ctypes.c_int),
     "hp_canonical_orthogonalize": ([_vp, _sz, ctypes.c_double, _vp, ctypes.POINTER(_sz)], ctypes.c_int),
     "hp_solve_spd": ([_vp, _vp, _sz, _vp, _vp, _vp, _i64p], ctypes.c_int),
     "hp_solve_spd_f128": ([_vp, _vp, _sz, _vp, _vp, _vp, _i64p], ctypes.c_int),
@@ -242,6 +244,22 @@ def canonical_orthogonalize(s, n, threshold):
     m = _sz(0)
     check(lib().hp_canonical_orthogonalize(_ptr(s), n, threshold, _ptr(x), ctypes.byref(m)))
     return np.ascontiguousarray(x.reshape(-1)[: n * m.value * 2].reshape(n, m.value, 2))
+
+
+def f256_gemv(a, x, n, m):
+    """multifloat/linalg.rs:17 mf_gemv::<4>; a (n, m, 4), x (m, 4) -> (n, 4)."""
+    a, x = _c(a), _c(x)
+    y = np.empty((n, 4))
+    check(lib().hp_f256_gemv(_ptr(a), _ptr(x), _ptr(y), n, m))
+    return y
+
+
+def f256_dot(a, b):
+    """multifloat/linalg.rs:7 mf_dot::<4>; a, b (len, 4) -> (4,)."""
+    a, b = _c(a), _c(b)
+    out = np.empty(4)
+    check(lib().hp_f256_dot(_ptr(a), _ptr(b), len(a), _ptr(out)))
+    return out
 
 
 def _solve(name, l, b, n):

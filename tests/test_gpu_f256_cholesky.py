@@ -63,3 +63,18 @@ def test_f256_cholesky_solve(gpu, n):
     xr = O.mf_cholesky_solve(4, l, b, n)
     d = (x[:, 0] - xr[:, 0]) + (x[:, 1] - xr[:, 1]) + (x[:, 2] - xr[:, 2]) + (x[:, 3] - xr[:, 3])
     assert np.linalg.norm(d) <= 1e-55 * np.linalg.norm(xr[:, 0])
+
+
+@pytest.mark.parametrize("n,m", [(1, 1), (3, 7), (33, 130), (200, 65)])
+def test_f256_gemv_bitexact(gpu, n, m):
+    """hp_f256_gemv / hp_f256_dot equal mf_gemv::<4> / mf_dot::<4> bit for bit."""
+    u = uniform(n * m * 4 + m * 4, seed=900 + n + m)
+    a = np.zeros((n, m, 4))
+    a[..., 0] = 2.0 * u[: n * m].reshape(n, m) - 1.0
+    for k in range(1, 4):
+        a[..., k] = a[..., k - 1] * 2.0 ** -54 * (2.0 * u[k * n * m : (k + 1) * n * m].reshape(n, m) - 1.0)
+    x = np.zeros((m, 4))
+    x[:, 0] = 2.0 * u[4 * n * m : 4 * n * m + m] - 1.0
+    x[:, 1] = x[:, 0] * 2.0 ** -54
+    assert np.array_equal(gpu.f256_gemv(a, x, n, m), O.mf_gemv(4, a, x, n, m))
+    assert np.array_equal(gpu.f256_dot(a[0], x), O.mf_gemv(4, a[:1], x, 1, m)[0])
