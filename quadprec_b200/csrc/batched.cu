@@ -7,7 +7,8 @@
 //   1. assemble S (f128) from the basis with overlap_norm_pair (the same
 //      f128 evaluation as hp_overlap_norm_dd, bit-identical);
 //   2. right-looking f128 Cholesky (crates/quad/src/linalg.rs:42-96 algebra,
-//      pivots by 1/sqrt in f128), pivot <= 0 -> status NOT_SPD;
+//      pivots by 1/sqrt in f128, updates with the 16-operation dd_fms_fast),
+//      pivot <= 0 -> status NOT_SPD;
 //   3. x = L^-T L^-1 b, then refinement x += L^-T L^-1 (b - S x) with the
 //      residual from error-free products and a 3-level TwoSum cascade
 //      (~2^-159), until max|dx| <= tol max|x| (crates/solver/src/lib.rs
@@ -33,13 +34,6 @@ namespace {
 
 constexpr int BT = 512;  // threads per CTA
 
-__device__ __forceinline__ dd rsqrt_dd(dd d) {
-  const double x0 = __ddiv_rn(1.0, __dsqrt_rn(d.hi));
-  const dd x = dd_from(x0);
-  const dd e = dd_sub(dd_from(1.0), dd_mul(d, dd_mul(x, x)));
-  return dd_add(x, dd_mul(x, dd_mul(e, dd_from(0.5))));
-}
-
 __device__ double block_max(double v, double* red) {
   v = fmax(v, __shfl_xor_sync(0xffffffffu, v, 16));
   v = fmax(v, __shfl_xor_sync(0xffffffffu, v, 8));
@@ -55,20 +49,21 @@ __device__ double block_max(double v, double* red) {
   return m;
 }
 
-// In-CTA triangular solves with L (row-major n x n, lower), v in place.
-__device__ void cta_trsv(const dd* L, dd* v, int n, bool upper_t, dd* bc) {
+// In-CTA triangular solves with L (row-major n x n, lower) and rinv[j] =
+// 1 / l_jj from the factorisation, v in place.
+__device__ void cta_trsv(const dd* L, const dd* rinv, dd* v, int n, bool upper_t, dd* bc) {
   for (int s = 0; s < n; s++) {
     const int j = upper_t ? n - 1 - s : s;
     if (threadIdx.x == 0) {
-      v[j] = dd_div(v[j], L[(size_t)j * n + j]);
+      v[j] = dd_mul(v[j], rinv[j]);
       *bc = v[j];
     }
     __syncthreads();
     const dd vj = *bc;
     if (!upper_t) {
-      for (int i = j + 1 + threadIdx.x; i < n; i += BT) v[i] = dd_sub(v[i], dd_mul(L[(size_t)i * n + j], vj));
+      for (int i = j + 1 + threadIdx.x; i < n; i += BT) v[i] = dd_fms_fast(v[i], L[(size_t)i * n + j], vj);
     } else {
-      for (int i = threadIdx.x; i < j; i += BT) v[i] = dd_sub(v[i], dd_mul(L[(size_t)j * n + i], vj));
+      for (int i = threadIdx.x; i < j; i += BT) v[i] = dd_fms_fast(v[i], L[(size_t)j * n + i], vj);
     }
     __syncthreads();
   }
@@ -115,6 +110,7 @@ __global__ void __launch_bounds__(BT) batched_spd_kernel(int count, const int* _
     const double* al = alpha + o;
     dd* x = x_out + o;
     r = L + (size_t)n * n;  // residual vector after L inside the slot
+    dd* rd = r + n;           // 1 / l_jj after it
     // 1. assemble S (lower triangle evaluated, mirrored), copy to L
     for (int p = threadIdx.x; p < n * (n + 1) / 2; p += BT) {
       int i = (int)((sqrtf(8.0f * (float)p + 1.0f) - 1.0f) * 0.5f);
@@ -134,8 +130,9 @@ __global__ void __launch_bounds__(BT) batched_spd_kernel(int count, const int* _
         if (!(d.hi > 0.0)) {
           fail = 1;
         } else {
-          const dd rs = rsqrt_dd(d);
+          const dd rs = dd_rsqrt_fast(d);
           L[(size_t)j * n + j] = dd_mul(d, rs);
+          rd[j] = rs;
           bc = rs;
         }
       }
@@ -144,13 +141,13 @@ __global__ void __launch_bounds__(BT) batched_spd_kernel(int count, const int* _
       const dd rs = bc;
       for (int i = j + 1 + threadIdx.x; i < n; i += BT) L[(size_t)i * n + j] = dd_mul(L[(size_t)i * n + j], rs);
       __syncthreads();
-      const int m = n - j - 1;
-      for (int p = threadIdx.x; p < m * (m + 1) / 2; p += BT) {
-        int ii = (int)((sqrtf(8.0f * (float)p + 1.0f) - 1.0f) * 0.5f);
-        while (ii * (ii + 1) / 2 > p) ii--;
-        while ((ii + 1) * (ii + 2) / 2 <= p) ii++;
-        const int i = j + 1 + ii, k = j + 1 + (p - ii * (ii + 1) / 2);
-        L[(size_t)i * n + k] = dd_sub(L[(size_t)i * n + k], dd_mul(L[(size_t)i * n + j], L[(size_t)k * n + j]));
+      {  // trailing update: one warp per row, lanes along k <= i
+        const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+        for (int i = j + 1 + warp; i < n; i += BT / 32) {
+          const dd lij = L[(size_t)i * n + j];
+          for (int k = j + 1 + lane; k <= i; k += 32)
+            L[(size_t)i * n + k] = dd_fms_fast(L[(size_t)i * n + k], lij, L[(size_t)k * n + j]);
+        }
       }
       __syncthreads();
     }
@@ -165,8 +162,8 @@ __global__ void __launch_bounds__(BT) batched_spd_kernel(int count, const int* _
     // 3. solve and refine
     for (int i = threadIdx.x; i < n; i += BT) x[i] = b[o + i];
     __syncthreads();
-    cta_trsv(L, x, n, false, &bc);
-    cta_trsv(L, x, n, true, &bc);
+    cta_trsv(L, rd, x, n, false, &bc);
+    cta_trsv(L, rd, x, n, true, &bc);
     int it = 0, conv = 0;
     for (it = 1; it <= max_iter; it++) {
       const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -207,8 +204,8 @@ __global__ void __launch_bounds__(BT) batched_spd_kernel(int count, const int* _
         }
       }
       __syncthreads();
-      cta_trsv(L, r, n, false, &bc);
-      cta_trsv(L, r, n, true, &bc);
+      cta_trsv(L, rd, r, n, false, &bc);
+      cta_trsv(L, rd, r, n, true, &bc);
       double md = 0.0, mx = 0.0;
       for (int i = threadIdx.x; i < n; i += BT) {
         x[i] = dd_add(x[i], r[i]);

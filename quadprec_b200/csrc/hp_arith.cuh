@@ -101,6 +101,40 @@ __device__ __forceinline__ dd dd_exp(dd a) {
 // stay in registers; each rewrite produces the same values as the loop it
 // replaces (argued at each site).
 // ---------------------------------------------------------------------------
+// ---------------------------------------------------------------------------
+// Fast f128 helpers for the chosen-path kernels only (not the reference's
+// operation order; never used where results must match the reference's bits).
+// ---------------------------------------------------------------------------
+// a - b c with 16 operations instead of the 29 of a reference-order multiply
+// and add: the exact product p + pe of the high parts, the cross terms
+// b.hi c.lo + b.lo c.hi, one two_sum of the high parts and a final
+// renormalisation (the "sloppy" addition). Error below ~3 2^-104
+// (|a| + |b c|), the bound the backward-error analyses of Cholesky and
+// substitution assume of each update.
+__device__ __forceinline__ dd dd_fms_fast(dd a, dd b, dd c) {
+  const double p = __dmul_rn(b.hi, c.hi);
+  const double pe = __fma_rn(b.hi, c.hi, -p);
+  const double t = __fma_rn(b.hi, c.lo, __dmul_rn(b.lo, c.hi));
+  double s, se;
+  two_sum(a.hi, -p, s, se);
+  const double e = __dadd_rn(se, __dsub_rn(a.lo, __dadd_rn(pe, t)));
+  return dd_renorm(s, e);
+}
+// 1/sqrt(d) to ~2^-103 from the f64 seed x = rsqrt(d.hi) (relative error
+// delta of a few 2^-53) by one Newton step x1 = x + x e / 2, e = 1 - d x^2.
+// e is ~delta, so it is needed only to ~2^-104 absolute: with x^2 = s + s'
+// exact (FMA), e = fma(-d.hi, s, 1) - (d.hi s' + d.lo s), each rounding
+// below 2^-104; x1 = x + c, c = x e / 2, is kept unevaluated as (x, c)
+// renormalised. The result's error is 1.5 delta^2 + O(2^-104).
+__device__ __forceinline__ dd dd_rsqrt_fast(dd d) {
+  const double x = rsqrt(d.hi);
+  const double s = __dmul_rn(x, x), s2 = __fma_rn(x, x, -s);
+  const double t = __fma_rn(-d.hi, s, 1.0);
+  const double u = __fma_rn(d.hi, s2, __dmul_rn(d.lo, s));
+  const double c = __dmul_rn(__dmul_rn(x, __dsub_rn(t, u)), 0.5);
+  return dd_renorm(x, c);
+}
+
 struct qd {
   double l[4];
 };

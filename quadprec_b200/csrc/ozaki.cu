@@ -1353,38 +1353,6 @@ __global__ void __launch_bounds__(256) crt_block_kernel(const uint8_t* __restric
   P[idx] = neg ? dd_neg(s) : s;
 }
 
-// a - b c in f128 with 16 operations instead of the 29 of a reference-order
-// multiply and add: the exact product p + pe of the high parts, the cross
-// terms b.hi c.lo + b.lo c.hi, one two_sum of the high parts and a final
-// renormalisation (the cheaper "sloppy" addition). Error below
-// ~3 2^-104 (|a| + |b c|), the bound that the backward-error analysis of
-// Cholesky and substitution assumes of each update. For the chosen path's
-// f128 kernels only, never where results must match the reference's bits.
-__device__ __forceinline__ dd dd_fms_fast(dd a, dd b, dd c) {
-  const double p = __dmul_rn(b.hi, c.hi);
-  const double pe = __fma_rn(b.hi, c.hi, -p);
-  const double t = __fma_rn(b.hi, c.lo, __dmul_rn(b.lo, c.hi));
-  double s, se;
-  two_sum(a.hi, -p, s, se);
-  const double e = __dadd_rn(se, __dsub_rn(a.lo, __dadd_rn(pe, t)));
-  return dd_renorm(s, e);
-}
-
-// 1/sqrt(d) to ~2^-103 from the f64 seed x = rsqrt(d.hi) (relative error
-// delta of a few 2^-53) by one Newton step x1 = x + x e / 2, e = 1 - d x^2.
-// e is ~delta, so it is needed only to ~2^-104 absolute: with x^2 = s + s'
-// exact (FMA), e = fma(-d.hi, s, 1) - (d.hi s' + d.lo s), each rounding
-// below 2^-104; x1 = x + c, c = x e / 2, is kept unevaluated as (x, c)
-// renormalised. The result's error is 1.5 delta^2 + O(2^-104).
-__device__ __forceinline__ dd dd_rsqrt(dd d) {
-  const double x = rsqrt(d.hi);
-  const double s = __dmul_rn(x, x), s2 = __fma_rn(x, x, -s);
-  const double t = __fma_rn(-d.hi, s, 1.0);
-  const double u = __fma_rn(d.hi, s2, __dmul_rn(d.lo, s));
-  const double c = __dmul_rn(__dmul_rn(x, __dsub_rn(t, u)), 0.5);
-  return dd_renorm(x, c);
-}
-
 // Factor the jb x jb block P[0..jb)[0..jb) (row stride jb, symmetric values)
 // in f128: L~11 scaled back to Lout, and for the panel solve the unit lower
 // factor L1 = L~11 diag(1 / l_jj) (row-major 64 x 64, zero on and above the
@@ -1444,7 +1412,7 @@ __global__ void __launch_bounds__(CI_THREADS) chol_block_kernel(const dd* __rest
       }
       return false;
     }
-    r = dd_rsqrt(d);
+    r = dd_rsqrt_fast(d);
     if (lane == 0) {
       rinv[p] = r;
       ldiag[p] = dd_mul(d, r);

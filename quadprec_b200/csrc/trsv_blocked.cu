@@ -84,18 +84,6 @@ __device__ __forceinline__ dd ld_dd_cg(const dd* p) {
   return dd{v.x, v.y};
 }
 
-// a - b c in f128 with 16 operations (exact high product, cross terms, one
-// two_sum, renormalisation); error below ~3 2^-104 (|a| + |b c|), the bound
-// the backward-error analysis of substitution assumes of each update.
-__device__ __forceinline__ dd fms_fast(dd a, dd b, dd c) {
-  const double p = __dmul_rn(b.hi, c.hi);
-  const double pe = __fma_rn(b.hi, c.hi, -p);
-  const double t = __fma_rn(b.hi, c.lo, __dmul_rn(b.lo, c.hi));
-  double s, se;
-  two_sum(a.hi, -p, s, se);
-  return dd_renorm(s, __dadd_rn(se, __dsub_rn(a.lo, __dadd_rn(pe, t))));
-}
-
 // Block row k: thread (r, q) = (t / 4, t % 4) owns row r of the block and
 // the columns c = q (mod 4) of each 64 x 64 tile it multiplies.
 constexpr uint64_t TRSV_WAIT_NS = 2000000000ull;
@@ -155,8 +143,8 @@ __global__ void __launch_bounds__(256) trsv_wave_kernel(const dd* __restrict__ L
     __syncthreads();
 #pragma unroll
     for (int m = 0; m < TB / 4; m += 2) {
-      acc0 = fms_fast(acc0, dd{-lv[m].hi, -lv[m].lo}, vj[q + 4 * m]);
-      acc1 = fms_fast(acc1, dd{-lv[m + 1].hi, -lv[m + 1].lo}, vj[q + 4 * m + 4]);
+      acc0 = dd_fms_fast(acc0, dd{-lv[m].hi, -lv[m].lo}, vj[q + 4 * m]);
+      acc1 = dd_fms_fast(acc1, dd{-lv[m + 1].hi, -lv[m + 1].lo}, vj[q + 4 * m + 4]);
     }
     __syncthreads();  // vj is rewritten by the next dependency
   }
@@ -169,8 +157,8 @@ __global__ void __launch_bounds__(256) trsv_wave_kernel(const dd* __restrict__ L
   acc0 = acc1 = dd{0.0, 0.0};
 #pragma unroll
   for (int m = 0; m < TB / 4; m += 2) {
-    acc0 = fms_fast(acc0, dd{-xr[m].hi, -xr[m].lo}, sv[q + 4 * m]);
-    acc1 = fms_fast(acc1, dd{-xr[m + 1].hi, -xr[m + 1].lo}, sv[q + 4 * m + 4]);
+    acc0 = dd_fms_fast(acc0, dd{-xr[m].hi, -xr[m].lo}, sv[q + 4 * m]);
+    acc1 = dd_fms_fast(acc1, dd{-xr[m + 1].hi, -xr[m + 1].lo}, sv[q + 4 * m + 4]);
   }
   part[r][q] = dd_add(acc0, acc1);
   __syncthreads();

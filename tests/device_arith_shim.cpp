@@ -15,6 +15,8 @@ static inline double __dmul_rn(double a, double b) { return a * b; }
 static inline double __ddiv_rn(double a, double b) { return a / b; }
 static inline double __fma_rn(double a, double b, double c) { return std::fma(a, b, c); }
 static inline double __dsqrt_rn(double a) { return std::sqrt(a); }
+// seed of the chosen-path 1/sqrt helper (not compared bit-for-bit here)
+static inline double rsqrt(double a) { return 1.0 / std::sqrt(a); }
 static inline double __longlong_as_double(long long v) {
   double d;
   std::memcpy(&d, &v, 8);
