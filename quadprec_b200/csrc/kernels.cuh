@@ -63,8 +63,20 @@ int ozaki_moduli_for(size_t k, int beta);
 int dd_residual(const double* S, const double* x, const double* b, double* r, size_t n, bool accurate_qd,
                 cudaStream_t s);
 int dd_maxabs(const double* v, size_t n, double* out_dev, cudaStream_t s);
+// Outcome of a device-side factorisation: flag != 0 when a pivot was not
+// positive, pivot = the first such index.
+struct FactorErr {
+  int flag;
+  int pad;
+  long long pivot;
+};
 // ozaki.cu: Cholesky with the trailing matrix kept in the residue domain.
-int rns_cholesky(const double* S, double* L, size_t n, int64_t* pivot, cudaStream_t s);
+// Writes the lower triangle of L (the strict upper triangle is not touched).
+// With err_out == nullptr it synchronises s and returns HP_ERR_NOT_SPD with
+// *pivot on failure; otherwise it copies the outcome to the device word
+// err_out on s and returns without synchronising.
+int rns_cholesky(const double* S, double* L, size_t n, int64_t* pivot, cudaStream_t s,
+                 FactorErr* err_out = nullptr);
 }  // namespace hp
 
 namespace hp {
@@ -72,8 +84,9 @@ namespace hp {
 int dd_block_inverses(const double* L, size_t n, double* Xall, cudaStream_t s);
 size_t dd_block_inverses_bytes(size_t n);
 int dd_trsv_blocked(const double* L, const double* Xall, double* v, size_t n, bool upper_t, cudaStream_t s);
-// HP_ERR_TIMEOUT if a wavefront wait of dd_trsv_blocked gave up (synchronises s).
-int dd_trsv_status(const double* Xall, size_t n, cudaStream_t s);
+// Device address of the status word of the solves on Xall (DEV_STATUS_TIMEOUT
+// once a wavefront wait gave up).
+const unsigned* dd_trsv_status_word(const double* Xall, size_t n);
 }  // namespace hp
 
 namespace hp {

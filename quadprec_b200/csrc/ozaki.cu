@@ -707,16 +707,18 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 }
 
 // Planes of R rows x K bytes; consecutive planes are plane_stride bytes apart
-// (K * R when 0).
+// (K * R when 0) and rows row_pitch bytes apart (K when 0). Boxes reaching
+// past K bytes or R rows read zeros.
 static int make_map(CUtensorMap* map, const void* base, uint64_t K, uint64_t R, uint64_t L, uint32_t box_r,
-                    uint64_t plane_stride = 0) {
+                    uint64_t plane_stride = 0, uint64_t row_pitch = 0) {
   auto fn = encode_fn();
   if (!fn) {
     set_error("cuTensorMapEncodeTiled unavailable");
     return HP_ERR_CUDA;
   }
+  const uint64_t pitch = row_pitch ? row_pitch : K;
   cuuint64_t dims[3] = {K, R, L};
-  cuuint64_t strides[2] = {K, plane_stride ? plane_stride : K * R};
+  cuuint64_t strides[2] = {pitch, plane_stride ? plane_stride : pitch * R};
   cuuint32_t box[3] = {(cuuint32_t)GB_K, box_r, 1};
   cuuint32_t estr[3] = {1, 1, 1};
   CUresult rc = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void*>(base), dims, strides, box, estr,
@@ -1225,11 +1227,7 @@ namespace ozaki {
 constexpr int BETA_CH = 106;
 constexpr int CH_NB = 64;
 
-struct RnsErr {
-  int flag;
-  int pad;
-  long long pivot;
-};
+using RnsErr = FactorErr;
 
 __global__ void rns_scale_kernel(const dd* __restrict__ S, int64_t n, int beta, int* __restrict__ e,
                                  RnsErr* err) {
@@ -1262,8 +1260,7 @@ __device__ __forceinline__ void int_digits10(double v, int32_t* d) {
 
 // Res[l][i][j] = round((D S D)_ij) mod m_l (unbalanced bytes) for the tiles
 // that meet the lower triangle of n x n (the factorisation reads no other
-// entry; the rest stays as the caller zeroed it). Block tile 64 rows x 32
-// columns, 8 columns per thread.
+// entry below row n). Block tile 64 rows x 32 columns, 8 columns per thread.
 __global__ void __launch_bounds__(256) rns_init_kernel(const dd* __restrict__ S, int64_t n, const int* __restrict__ e,
                                                        int L, int64_t Rp, uint8_t* __restrict__ res) {
   const int64_t row0 = (int64_t)blockIdx.y * 64, col0 = (int64_t)blockIdx.x * 32;
@@ -1554,15 +1551,17 @@ __global__ void __launch_bounds__(256) panel_trsm_kernel(const dd* __restrict__ 
 
 // res[l][r0 + i][c0 + j] -= sum_p A[l][i][p] B[l][j][p] (mod m_l) for
 // i < R, j < CH_NB, p < K: A = R rows of L~ residues from arow, B = CH_NB
-// rows from brow (row length KL bytes, planes plane_stride bytes apart; a
-// map spans rows_a / rows_b rows). One launch of the 128 x 64 tile GEMM on at
-// most max_ctas CTAs.
+// rows from brow (rows KL bytes apart, planes plane_stride bytes apart). The
+// maps cover rows_a / rows_b rows and the first kv bytes of each: the
+// k-blocks past kv (K is kv rounded up to the 128-byte k-block) and the tile
+// rows past the maps read zeros, so the residue planes need no zeroing. One
+// launch of the 128 x 64 tile GEMM on at most max_ctas CTAs.
 static int rns_panel_update(const uint8_t* arow, size_t rows_a, const uint8_t* brow, size_t rows_b, size_t KL,
-                            size_t plane_stride, int L, size_t R, size_t K, uint8_t* res, size_t Np, size_t r0,
-                            size_t c0, int max_ctas, cudaStream_t s) {
+                            size_t kv, size_t plane_stride, int L, size_t R, size_t K, uint8_t* res, size_t Np,
+                            size_t r0, size_t c0, int max_ctas, cudaStream_t s) {
   using namespace ozaki;
   constexpr int BN = CH_NB;
-  if (R == 0 || K == 0) return HP_OK;
+  if (R == 0 || K == 0 || rows_a == 0 || rows_b == 0) return HP_OK;
   static bool attr_set[64] = {};
   int dev = 0;
   HP_CUDA_TRY(cudaGetDevice(&dev));
@@ -1572,8 +1571,8 @@ static int rns_panel_update(const uint8_t* arow, size_t rows_a, const uint8_t* b
     attr_set[dev] = true;
   }
   CUtensorMap mapA, mapB;
-  HP_TRY(make_map(&mapA, arow, KL, rows_a, L, GB_M, plane_stride));
-  HP_TRY(make_map(&mapB, brow, KL, rows_b, L, BN, plane_stride));
+  HP_TRY(make_map(&mapA, arow, kv, rows_a, L, GB_M, plane_stride, KL));
+  HP_TRY(make_map(&mapB, brow, kv, rows_b, L, BN, plane_stride, KL));
   uint32_t* status = device_status(s);
   if (!status) {
     set_error("status word allocation failed");
@@ -1640,7 +1639,7 @@ struct PipelineEvents {
   }
 };
 
-int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStream_t s) {
+int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStream_t s, FactorErr* err_out) {
   using namespace ozaki;
   if (n == 0) return HP_OK;
   DevTables* D;
@@ -1667,9 +1666,9 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
   }
   RnsErr h0{0, 0, (long long)0x7fffffffffffffffll};
   HP_CUDA_TRY(cudaMemcpyAsync(err.p, &h0, sizeof(h0), cudaMemcpyHostToDevice, s));
-  HP_CUDA_TRY(cudaMemsetAsync(res.p, 0, (size_t)L * Np * Np, s));
-  HP_CUDA_TRY(cudaMemsetAsync(lres.p, 0, (size_t)L * RL * KL, s));
-  if ((const void*)S_ != (const void*)L_) HP_CUDA_TRY(cudaMemcpyAsync(L_, S_, n * n * 16, cudaMemcpyDeviceToDevice, s));
+  // No zeroing: rns_init writes every residue tile the panels read (rows
+  // past n feed only output rows past n), and the L~ planes are read
+  // through maps that end at the written columns and rows.
   cudaStream_t s_caller = s, s2 = nullptr;
   HP_TRY(pipeline_streams(&s, &s2));
   PipelineEvents ev(s_caller, s, s2);  // declared after the buffers: joins both streams before they are freed
@@ -1741,15 +1740,15 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
     } else {
       if (p >= 2) HP_CUDA_TRY(cudaStreamWaitEvent(s, ev.Tr[par], 0));  // solve rows of panel p - 2
       const uint8_t* lrow = lres.as<uint8_t>() + kb * KL;
-      HP_TRY(rns_panel_update(lrow, RL - kb, lrow, RL - kb, KL, plane_l, L, Rd, round_up(kb, GB_K), res.as<uint8_t>(),
-                              Np, kb, kb, gemm_ctas, s));
+      HP_TRY(rns_panel_update(lrow, R, lrow, R, KL, kb, plane_l, L, Rd, round_up(kb, GB_K), res.as<uint8_t>(), Np, kb,
+                              kb, gemm_ctas, s));
       HP_CUDA_TRY(cudaEventRecord(ev.Gd, s));
       HP_TRY(crt(kb, (size_t)jb, kb, jb, Pp, s));
       // s2: the rest of the panel's rows
       HP_CUDA_TRY(cudaStreamWaitEvent(s2, ev.Td, 0));  // rows kb..kb+nb of the previous panel's solve
       if (R > Rd) {
         const uint8_t* arow = lres.as<uint8_t>() + (kb + Rd) * KL;
-        HP_TRY(rns_panel_update(arow, RL - kb - Rd, lrow, RL - kb, KL, plane_l, L, R - Rd, round_up(kb, GB_K),
+        HP_TRY(rns_panel_update(arow, R - Rd, lrow, R, KL, kb, plane_l, L, R - Rd, round_up(kb, GB_K),
                                 res.as<uint8_t>(), Np, kb + Rd, kb, gemm_ctas, s2));
       }
       HP_CUDA_TRY(cudaStreamWaitEvent(s2, ev.Gd, 0));
@@ -1772,6 +1771,10 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
   }
   ev.join();  // both pipeline streams finish before the caller's stream goes on
   s = s_caller;
+  if (err_out) {  // the caller reads the outcome later, with its own next readback
+    HP_CUDA_TRY(cudaMemcpyAsync(err_out, err.p, sizeof(RnsErr), cudaMemcpyDeviceToDevice, s));
+    return HP_OK;
+  }
   RnsErr h;
   HP_CUDA_TRY(cudaMemcpyAsync(&h, err.p, sizeof(h), cudaMemcpyDeviceToHost, s));
   HP_CUDA_TRY(cudaStreamSynchronize(s));

@@ -149,7 +149,13 @@ namespace hp {
 int spd_refined(const double* S, const double* b, size_t n, int mode, double tol, int max_iter, double* x,
                 hp_refine_info_t* info, int64_t* pivot, cudaStream_t s) {
   if (n == 0) return HP_OK;
-  DevBuf L(n * n * 16, s), r(n * 16, s), scal(2 * sizeof(double), s);
+  // scal: max|dx|, max|x| (doubles 0, 1) and the factorisation's outcome
+  // (chosen mode), all read back with each iteration's one synchronisation
+  struct Readback {
+    double dx_max, x_max;
+    FactorErr ferr;
+  };
+  DevBuf L(n * n * 16, s), r(n * 16, s), scal(sizeof(Readback), s);
   if (!L.p || !r.p || !scal.p) return HP_ERR_CUDA;
   cudaEvent_t e0, e1, e2;
   cudaEventCreate(&e0);
@@ -161,7 +167,9 @@ int spd_refined(const double* S, const double* b, size_t n, int mode, double tol
     HP_CUDA_TRY(cudaMemcpyAsync(L.p, S, n * n * 16, cudaMemcpyDeviceToDevice, s));
     rc = dd_cholesky(L.as<double>(), n, 0, false, pivot, nullptr, s, true);
   } else {
-    rc = rns_cholesky(S, L.as<double>(), n, pivot, s);
+    // no synchronisation here: a failed pivot is reported with the first
+    // readback below (the solves in between run on a partial factor)
+    rc = rns_cholesky(S, L.as<double>(), n, pivot, s, &scal.as<Readback>()->ferr);
   }
   if (rc != HP_OK) return rc;
   cudaEventRecord(e1, s);
@@ -171,6 +179,7 @@ int spd_refined(const double* S, const double* b, size_t n, int mode, double tol
   HP_CUDA_TRY(cudaMemcpyAsync(x, b, n * 16, cudaMemcpyDeviceToDevice, s));
   HP_TRY(dd_trsv_blocked(L.as<double>(), Xinv.as<double>(), x, n, false, s));
   HP_TRY(dd_trsv_blocked(L.as<double>(), Xinv.as<double>(), x, n, true, s));
+  const unsigned* trsv_status = dd_trsv_status_word(Xinv.as<double>(), n);
   int it = 0, converged = 0;
   double ratio = 0.0;
   for (it = 1; it <= max_iter; it++) {
@@ -178,20 +187,46 @@ int spd_refined(const double* S, const double* b, size_t n, int mode, double tol
     HP_TRY(dd_trsv_blocked(L.as<double>(), Xinv.as<double>(), r.as<double>(), n, false, s));
     HP_TRY(dd_trsv_blocked(L.as<double>(), Xinv.as<double>(), r.as<double>(), n, true, s));
     HP_TRY(dd_vec(1, x, r.as<double>(), x, nullptr, n, s));
-    HP_TRY(dd_maxabs(r.as<double>(), n, scal.as<double>(), s));
-    HP_TRY(dd_maxabs(x, n, scal.as<double>() + 1, s));
-    double h[2];
-    HP_CUDA_TRY(cudaMemcpyAsync(h, scal.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    HP_TRY(dd_maxabs(r.as<double>(), n, &scal.as<Readback>()->dx_max, s));
+    HP_TRY(dd_maxabs(x, n, &scal.as<Readback>()->x_max, s));
+    Readback h;
+    unsigned st = 0;
+    HP_CUDA_TRY(cudaMemcpyAsync(&h, scal.p, sizeof(h), cudaMemcpyDeviceToHost, s));
+    HP_CUDA_TRY(cudaMemcpyAsync(&st, trsv_status, sizeof(st), cudaMemcpyDeviceToHost, s));
     HP_CUDA_TRY(cudaStreamSynchronize(s));
-    ratio = h[1] > 0 ? h[0] / h[1] : 0.0;
+    if (mode != HP_MODE_PLAIN && h.ferr.flag) {
+      if (pivot) *pivot = h.ferr.pivot;
+      set_error("Cholesky failed at pivot %lld", (long long)h.ferr.pivot);
+      return HP_ERR_NOT_SPD;
+    }
+    if (st & DEV_STATUS_TIMEOUT) {
+      set_error("triangular solve: a block wait timed out");
+      return HP_ERR_TIMEOUT;
+    }
+    ratio = h.x_max > 0 ? h.dx_max / h.x_max : 0.0;
     if (ratio <= tol) {
       converged = 1;
       break;
     }
   }
+  if (max_iter < 1) {  // no iteration read the outcomes back
+    FactorErr fe;
+    unsigned st = 0;
+    HP_CUDA_TRY(cudaMemcpyAsync(&fe, &scal.as<Readback>()->ferr, sizeof(fe), cudaMemcpyDeviceToHost, s));
+    HP_CUDA_TRY(cudaMemcpyAsync(&st, trsv_status, sizeof(st), cudaMemcpyDeviceToHost, s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));
+    if (mode != HP_MODE_PLAIN && fe.flag) {
+      if (pivot) *pivot = fe.pivot;
+      set_error("Cholesky failed at pivot %lld", (long long)fe.pivot);
+      return HP_ERR_NOT_SPD;
+    }
+    if (st & DEV_STATUS_TIMEOUT) {
+      set_error("triangular solve: a block wait timed out");
+      return HP_ERR_TIMEOUT;
+    }
+  }
   cudaEventRecord(e2, s);
   cudaEventSynchronize(e2);
-  HP_TRY(dd_trsv_status(Xinv.as<double>(), n, s));
   float fm = 0, tm = 0;
   cudaEventElapsedTime(&fm, e0, e1);
   cudaEventElapsedTime(&tm, e0, e2);

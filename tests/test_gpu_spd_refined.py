@@ -56,6 +56,7 @@ def test_refined_not_spd(gpu):
         with pytest.raises(gpu.HPError) as ei:
             gpu.spd_solve_refined(a, np.ones(n), n, mode=mode)
         assert ei.value.code == gpu.HP_ERR_NOT_SPD
+        assert "pivot 17" in str(ei.value), (mode, str(ei.value))
 
 
 def test_refined_small_hilbert_exact(gpu):
@@ -76,3 +77,30 @@ def test_refined_small_hilbert_exact(gpu):
     for mode in (0, 1):
         x, info = gpu.spd_solve_refined(a, b, n, mode=mode)
         assert rel_err(x, xs) <= 1e-25
+
+
+@pytest.mark.parametrize("n", [1, 2, 63, 64, 65, 130])
+def test_refined_ragged_sizes(gpu, n):
+    """Partial last blocks of the wavefront solves (64-row blocks) and of the
+    residue-domain panels: both modes leave a residual |b - A x| below 1e-30
+    |A| |x| row by row, computed exactly in rationals."""
+    from fractions import Fraction as F
+
+    rng = np.random.default_rng(1000 + n)
+    B = rng.standard_normal((n, n))
+    A = B @ B.T / n + np.eye(n)
+    A = (A + A.T) / 2  # exactly symmetric
+    a = np.zeros((n, n, 2))
+    a[..., 0] = A
+    b = rng.standard_normal(n)
+    for mode in (0, 1):
+        x, info = gpu.spd_solve_refined(a, b, n, mode=mode)
+        assert info["converged"] == 1, (mode, info)
+        xs = [F(float(x[i, 0])) + F(float(x[i, 1])) for i in range(n)]
+        worst = 0
+        for i in range(n):
+            row = [F(float(A[i, j])) for j in range(n)]
+            r = F(float(b[i])) - sum(row[j] * xs[j] for j in range(n))
+            scale = sum(abs(row[j]) * abs(xs[j]) for j in range(n))
+            worst = max(worst, abs(r) / scale)
+        assert worst <= F(1, 10**30), (mode, float(worst))
