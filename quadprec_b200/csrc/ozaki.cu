@@ -26,6 +26,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <utility>
 #include <vector>
 
 #include "hp_arith.cuh"
@@ -446,6 +447,10 @@ __global__ void __launch_bounds__(256, 1)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem_base = *tmem_slot;
+  // set-up done; inputs and the residues it updates may come from the
+  // preceding kernel of a programmatic launch
+  griddep_launch_dependents();
+  griddep_wait();
 
   const int nkb = kb1 - kb0;
   const int per_l = tiles_m * tiles_n;
@@ -1325,6 +1330,8 @@ __global__ void __launch_bounds__(256) crt_block_kernel(const uint8_t* __restric
   const int L = tab->L;
   for (int i = threadIdx.x; i < L * NC; i += blockDim.x) w_s[i / NC][i % NC] = tab->w[i / NC][i % NC];
   if (threadIdx.x < NC) mch_s[threadIdx.x] = tab->mchunk[threadIdx.x];
+  sm100::griddep_launch_dependents();
+  sm100::griddep_wait();  // the residues come from the preceding GEMM
   __syncthreads();
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= R * C) return;
@@ -1387,6 +1394,8 @@ __global__ void __launch_bounds__(CI_THREADS) chol_block_kernel(const dd* __rest
   const bool bulk = warp % 4 != 3;
   const int bt = (warp / 4 * 3 + warp % 4) * 32 + lane;  // bulk thread index
   const int ot = (warp / 4) * 32 + lane;                 // index among the output warps (warp % 4 == 3)
+  sm100::griddep_launch_dependents();
+  sm100::griddep_wait();  // P comes from the preceding CRT
   if (err->flag) return;
   if (t < 64) esh[t] = t < jb ? e[kb + t] : 0;
   if (t == 0) fail = 0;
@@ -1510,6 +1519,8 @@ __global__ void __launch_bounds__(256) panel_trsm_kernel(const dd* __restrict__ 
   extern __shared__ __align__(16) unsigned char sm_raw[];
   dd(*L1s)[CH_NB + 1] = reinterpret_cast<dd(*)[CH_NB + 1]>(sm_raw);  // [CH_NB][CH_NB + 1]
   __shared__ dd rs[CH_NB];
+  sm100::griddep_launch_dependents();
+  sm100::griddep_wait();  // L1 and 1/l come from the preceding block factor
   for (int q = threadIdx.x; q < CH_NB * CH_NB; q += blockDim.x) L1s[q / CH_NB][q % CH_NB] = L1g[q];
   if (threadIdx.x < CH_NB) rs[threadIdx.x] = rinvg[threadIdx.x];
   __syncthreads();
@@ -1549,6 +1560,27 @@ __global__ void __launch_bounds__(256) panel_trsm_kernel(const dd* __restrict__ 
 
 }  // namespace ozaki
 
+// Launch kernel k; with pdl set, as a programmatic dependent launch: the
+// kernel may be scheduled while its predecessor in the stream still runs
+// and waits for it (griddep_wait) before touching the predecessor's
+// output. The residue-domain Cholesky chains its diagonal path this way,
+// so that each launch's set-up overlaps the tail of the previous kernel.
+template <typename... P, typename... A>
+static cudaError_t launch_k(bool pdl, void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                            A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = pdl ? at : nullptr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
+
 // res[l][r0 + i][c0 + j] -= sum_p A[l][i][p] B[l][j][p] (mod m_l) for
 // i < R, j < CH_NB, p < K: A = R rows of L~ residues from arow, B = CH_NB
 // rows from brow (rows KL bytes apart, planes plane_stride bytes apart). The
@@ -1558,7 +1590,7 @@ __global__ void __launch_bounds__(256) panel_trsm_kernel(const dd* __restrict__ 
 // launch of the 128 x 64 tile GEMM on at most max_ctas CTAs.
 static int rns_panel_update(const uint8_t* arow, size_t rows_a, const uint8_t* brow, size_t rows_b, size_t KL,
                             size_t kv, size_t plane_stride, int L, size_t R, size_t K, uint8_t* res, size_t Np,
-                            size_t r0, size_t c0, int max_ctas, cudaStream_t s) {
+                            size_t r0, size_t c0, int max_ctas, cudaStream_t s, bool pdl = false) {
   using namespace ozaki;
   constexpr int BN = CH_NB;
   if (R == 0 || K == 0 || rows_a == 0 || rows_b == 0) return HP_OK;
@@ -1582,10 +1614,9 @@ static int rns_panel_update(const uint8_t* arow, size_t rows_a, const uint8_t* b
   const int grid = std::max(1, std::min(L * tiles_m, max_ctas));
   const int nkb = (int)(K / GB_K), kb_chunk = MAX_K_CHUNK / GB_K;
   for (int k0 = 0; k0 < nkb; k0 += kb_chunk) {
-    i8_gemm_mod_kernel<BN><<<grid, 256, GemmCfg<BN>::SMEM, s>>>(mapA, mapB, L, tiles_m, 1, k0, std::min(nkb, k0 + kb_chunk),
-                                                                 0, 2, res, (int64_t)Np, (int64_t)(Np * Np),
-                                                                 (int64_t)r0, (int64_t)c0, status);
-    HP_LAUNCH_CHECK();
+    HP_CUDA_TRY(launch_k(pdl && k0 == 0, i8_gemm_mod_kernel<BN>, dim3(grid), dim3(256), GemmCfg<BN>::SMEM, s, mapA,
+                         mapB, L, tiles_m, 1, k0, std::min(nkb, k0 + kb_chunk), 0, 2, res, (int64_t)Np,
+                         (int64_t)(Np * Np), (int64_t)r0, (int64_t)c0, status));
   }
   return HP_OK;
 }
@@ -1620,10 +1651,10 @@ static int pipeline_streams(cudaStream_t* hi, cudaStream_t* lo) {
 // stream-ordered frees of the workspace come after them.
 struct PipelineEvents {
   cudaStream_t s, s1, s2;
-  cudaEvent_t F, Td, Gd, Cr, Tr[2], start, join1, join2;
+  cudaEvent_t F, Td, Gd, Cr, E, start, join1, join2;
   bool ok = true;
   PipelineEvents(cudaStream_t caller, cudaStream_t hi, cudaStream_t lo) : s(caller), s1(hi), s2(lo) {
-    for (cudaEvent_t* e : {&F, &Td, &Gd, &Cr, &Tr[0], &Tr[1], &start, &join1, &join2})
+    for (cudaEvent_t* e : {&F, &Td, &Gd, &Cr, &E, &start, &join1, &join2})
       ok = ok && cudaEventCreateWithFlags(e, cudaEventDisableTiming) == cudaSuccess;
     ok = ok && cudaEventRecord(start, s) == cudaSuccess && cudaStreamWaitEvent(s1, start, 0) == cudaSuccess &&
          cudaStreamWaitEvent(s2, start, 0) == cudaSuccess;
@@ -1635,7 +1666,7 @@ struct PipelineEvents {
   }
   ~PipelineEvents() {
     join();
-    for (cudaEvent_t e : {F, Td, Gd, Cr, Tr[0], Tr[1], start, join1, join2}) cudaEventDestroy(e);
+    for (cudaEvent_t e : {F, Td, Gd, Cr, E, start, join1, join2}) cudaEventDestroy(e);
   }
 };
 
@@ -1689,13 +1720,13 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
   int8_t* lres8 = reinterpret_cast<int8_t*>(lres.as<uint8_t>());
   const size_t plane_l = RL * KL;
   const int gemm_ctas = std::max(1, D->num_sms - 8);  // leave SMs for the diagonal path
-  auto crt = [&](size_t r0, size_t rows, size_t kb, int jb, dd* out, cudaStream_t st) -> int {
+  auto crt = [&](size_t r0, size_t rows, size_t kb, int jb, dd* out, cudaStream_t st, bool pdl) -> int {
     if (rows == 0) return HP_OK;
-#define HP_CRTB(NC)                                                                                            \
-  case NC:                                                                                                     \
-    crt_block_kernel<NC><<<(unsigned)((rows * jb + 255) / 256), 256, 0, st>>>(                                  \
-        res.as<uint8_t>(), (int64_t)Np, (int64_t)(Np * Np), (int64_t)r0, (int64_t)kb, (int64_t)rows, (int64_t)jb, \
-        D->crt + L, out);                                                                                      \
+#define HP_CRTB(NC)                                                                                               \
+  case NC:                                                                                                        \
+    HP_CUDA_TRY(launch_k(pdl, crt_block_kernel<NC>, dim3((unsigned)((rows * jb + 255) / 256)), dim3(256), 0, st, \
+                         (const uint8_t*)res.as<uint8_t>(), (int64_t)Np, (int64_t)(Np * Np), (int64_t)r0,        \
+                         (int64_t)kb, (int64_t)rows, (int64_t)jb, (const CrtTable*)(D->crt + L), out));          \
     break;
     switch (nc) {
       HP_CRTB(5) HP_CRTB(6) HP_CRTB(7)
@@ -1704,31 +1735,38 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
         return HP_ERR_UNSUPPORTED;
     }
 #undef HP_CRTB
-    HP_LAUNCH_CHECK();
     return HP_OK;
   };
-  auto trsm = [&](int par, size_t kb, int jb, size_t r0, size_t m, cudaStream_t st) -> int {
+  auto trsm = [&](int par, size_t kb, int jb, size_t r0, size_t m, cudaStream_t st, bool pdl) -> int {
     if (r0 >= m) return HP_OK;
     const unsigned blocks = (unsigned)std::min<size_t>((m - r0 + 7) / 8, (size_t)D->num_sms * 3);
-    panel_trsm_kernel<<<blocks, 256, trsm_smem, st>>>(Pb.as<dd>() + (size_t)par * n * nb + (size_t)jb * jb,
-                                                       L1b.as<dd>() + (size_t)par * nb * nb, RIb.as<dd>() + par * nb,
-                                                       (int64_t)r0, (int64_t)m, jb, (int64_t)(kb + jb), (int64_t)kb,
-                                                       (int64_t)n, ebuf.as<int>(), Lout, L, lres8, (int64_t)KL,
-                                                       (int64_t)plane_l);
-    HP_LAUNCH_CHECK();
+    HP_CUDA_TRY(launch_k(pdl, panel_trsm_kernel, dim3(blocks), dim3(256), trsm_smem, st,
+                         (const dd*)(Pb.as<dd>() + (size_t)par * n * nb + (size_t)jb * jb),
+                         (const dd*)(L1b.as<dd>() + (size_t)par * nb * nb), (const dd*)(RIb.as<dd>() + par * nb),
+                         (int64_t)r0, (int64_t)m, jb, (int64_t)(kb + jb), (int64_t)kb, (int64_t)n,
+                         (const int*)ebuf.as<int>(), Lout, L, lres8, (int64_t)KL, (int64_t)plane_l));
     return HP_OK;
   };
-  // Left-looking, with a look-ahead pipeline. The panel of block column kb
-  // receives all earlier updates at once, A~[kb.., kb..kb+nb) -=
-  // L~[kb.., 0..kb) L~[kb..kb+nb, 0..kb)^T, as residue GEMMs with N = nb and
-  // K = kb over the stored residue planes of L~ (columns from kb on are still
-  // zero there, so K may be rounded up to the 128-byte k-block). Stream s
-  // carries the diagonal path of each panel (its first 128 rows: GEMM, CRT
-  // of the diagonal block, factor, then the first 128 rows of the panel
-  // solve, which the next diagonal block needs); stream s2 carries the rest
-  // (remaining rows' GEMM, CRT and solve) alongside. Panel buffers (P, L1,
-  // 1/l) alternate by panel parity. The integers are those of the
+  // Left-looking, with a look-ahead pipeline. Panel q (block column kb)
+  // receives all earlier updates, A~[kb.., kb..kb+nb) -= L~[kb.., 0..kb)
+  // L~[kb..kb+nb, 0..kb)^T, as residue GEMMs (N = nb) over the stored residue
+  // planes of L~. Residues make the update order free: every GEMM subtracts
+  // its products modulo m, so the panel's update is split by K into
+  //   early: columns [0, kb - nb) (panels q - 2 and before), all rows, on s2,
+  //          enqueued one panel ahead so that it runs while panel q - 1 is
+  //          being factored;
+  //   late:  columns [kb - nb, kb) (panel q - 1, one k-block), on s for the
+  //          first 128 rows (the diagonal path) and on s2 for the others.
+  // Stream s (greatest priority) carries the diagonal path: late GEMM, CRT
+  // of the diagonal block, factor, and the first 128 rows of the panel
+  // solve (which the next late GEMM reads); stream s2 carries the rest of
+  // the rows' late GEMM, CRT and solve, and the next panel's early GEMM.
+  // Two GEMMs touching the same residues are always ordered by a stream or
+  // an event. Panel buffers (P, L1, 1/l) alternate by panel parity; the
+  // maps of every GEMM end at the columns that hold panels, so the partial
+  // 128-byte k-blocks read zeros. The integers are those of the
   // right-looking order; only the schedule differs.
+  const size_t npanel = (n + nb - 1) / nb;
   for (size_t kb = 0, p = 0; kb < n; kb += nb, p++) {
     const int jb = (int)std::min(nb, n - kb);
     const size_t R = n - kb, m = R - jb;
@@ -1736,38 +1774,50 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
     dd* Pp = Pb.as<dd>() + (size_t)par * n * nb;
     const size_t Rd = std::min<size_t>(R, GB_M);  // rows of the diagonal path's GEMM
     if (kb == 0) {
-      HP_TRY(crt(0, R, 0, jb, Pp, s));
+      HP_TRY(crt(0, R, 0, jb, Pp, s, false));
     } else {
-      if (p >= 2) HP_CUDA_TRY(cudaStreamWaitEvent(s, ev.Tr[par], 0));  // solve rows of panel p - 2
+      // late update of the diagonal path: panel q - 1's columns (its solve
+      // rows kb..kb+128 came from this stream); after the early update of
+      // the same rows (event E, recorded on s2 after it)
+      if (p >= 2) HP_CUDA_TRY(cudaStreamWaitEvent(s, ev.E, 0));
       const uint8_t* lrow = lres.as<uint8_t>() + kb * KL;
-      HP_TRY(rns_panel_update(lrow, R, lrow, R, KL, kb, plane_l, L, Rd, round_up(kb, GB_K), res.as<uint8_t>(), Np, kb,
-                              kb, gemm_ctas, s));
+      HP_TRY(rns_panel_update(lrow + (kb - nb), R, lrow + (kb - nb), R, KL, nb, plane_l, L, Rd, GB_K,
+                              res.as<uint8_t>(), Np, kb, kb, gemm_ctas, s, true));
       HP_CUDA_TRY(cudaEventRecord(ev.Gd, s));
-      HP_TRY(crt(kb, (size_t)jb, kb, jb, Pp, s));
-      // s2: the rest of the panel's rows
-      HP_CUDA_TRY(cudaStreamWaitEvent(s2, ev.Td, 0));  // rows kb..kb+nb of the previous panel's solve
+      HP_TRY(crt(kb, (size_t)jb, kb, jb, Pp, s, true));
+      // s2: late update of the other rows (after the previous panel's solve
+      // rows on s), then their CRT
+      HP_CUDA_TRY(cudaStreamWaitEvent(s2, ev.Td, 0));
       if (R > Rd) {
         const uint8_t* arow = lres.as<uint8_t>() + (kb + Rd) * KL;
-        HP_TRY(rns_panel_update(arow, R - Rd, lrow, R, KL, kb, plane_l, L, R - Rd, round_up(kb, GB_K),
+        HP_TRY(rns_panel_update(arow + (kb - nb), R - Rd, lrow + (kb - nb), R, KL, nb, plane_l, L, R - Rd, GB_K,
                                 res.as<uint8_t>(), Np, kb + Rd, kb, gemm_ctas, s2));
       }
       HP_CUDA_TRY(cudaStreamWaitEvent(s2, ev.Gd, 0));
-      HP_TRY(crt(kb + jb, m, kb, jb, Pp + (size_t)jb * jb, s2));
+      HP_TRY(crt(kb + jb, m, kb, jb, Pp + (size_t)jb * jb, s2, false));
       HP_CUDA_TRY(cudaEventRecord(ev.Cr, s2));
     }
-    chol_block_kernel<<<1, CI_THREADS, blk_smem, s>>>(Pp, jb, (int64_t)kb, (int64_t)n, ebuf.as<int>(), Lout,
-                                                      L1b.as<dd>() + (size_t)par * nb * nb, RIb.as<dd>() + par * nb,
-                                                      err.as<RnsErr>());
-    HP_LAUNCH_CHECK();
+    // s2: early update of panel q + 1 (columns [0, kb), every panel up to
+    // q - 1, all of whose rows are solved by now in s2's order or behind
+    // the event Td it waited for), while panel q is factored
+    if (p + 1 < npanel && kb > 0) {
+      const size_t kn = kb + nb, Rn = n - kn;
+      const uint8_t* nrow = lres.as<uint8_t>() + kn * KL;
+      HP_TRY(rns_panel_update(nrow, Rn, nrow, Rn, KL, kb, plane_l, L, Rn, round_up(kb, GB_K), res.as<uint8_t>(),
+                              Np, kn, kn, gemm_ctas, s2));
+      HP_CUDA_TRY(cudaEventRecord(ev.E, s2));
+    }
+    HP_CUDA_TRY(launch_k(true, chol_block_kernel, dim3(1), dim3(CI_THREADS), blk_smem, s, (const dd*)Pp, jb,
+                         (int64_t)kb, (int64_t)n, (const int*)ebuf.as<int>(), Lout,
+                         L1b.as<dd>() + (size_t)par * nb * nb, RIb.as<dd>() + par * nb, err.as<RnsErr>()));
     HP_CUDA_TRY(cudaEventRecord(ev.F, s));
     if (m == 0) break;
     const size_t md = std::min<size_t>(m, GB_M);  // panel-solve rows on the diagonal path
     if (kb > 0) HP_CUDA_TRY(cudaStreamWaitEvent(s, ev.Cr, 0));
-    HP_TRY(trsm(par, kb, jb, 0, md, s));
+    HP_TRY(trsm(par, kb, jb, 0, md, s, true));
     HP_CUDA_TRY(cudaEventRecord(ev.Td, s));
     HP_CUDA_TRY(cudaStreamWaitEvent(s2, ev.F, 0));
-    HP_TRY(trsm(par, kb, jb, md, m, s2));
-    HP_CUDA_TRY(cudaEventRecord(ev.Tr[par], s2));
+    HP_TRY(trsm(par, kb, jb, md, m, s2, false));
   }
   ev.join();  // both pipeline streams finish before the caller's stream goes on
   s = s_caller;
