@@ -57,6 +57,8 @@ int gemm_host(int limbs, const double* a, const double* b, double* c, size_t m, 
   HP_TRY(gemm_dev(limbs, da.as<double>(), db.as<double>(), dc.as<double>(), m, n, k, atb, mode, s));
   HP_CUDA_TRY(cudaMemcpyAsync(c, dc.p, bc, cudaMemcpyDeviceToHost, s));
   HP_CUDA_TRY(cudaStreamSynchronize(s));
+  // the tensor-core path's bounded waits report through the device status word
+  if (mode == HP_MODE_OZAKI) HP_TRY(consume_device_status(s));
   return HP_OK;
 }
 

@@ -26,9 +26,12 @@ cudaStream_t library_stream();
 void* dev_alloc(size_t bytes, cudaStream_t s);
 void dev_free(void* p, cudaStream_t s);
 
-// Device-side status word used by kernels that spin or detect data errors.
-// Kernels only ever OR bits into it.
-uint32_t* device_status(cudaStream_t s);  // zeroed, valid until next call on s
+// Device-side status word (one per device) used by kernels that spin or
+// detect data errors. Kernels only ever OR bits into it; it stays set until
+// consume_device_status() reads and clears it. consume_device_status
+// synchronises s and returns HP_ERR_TIMEOUT when a bounded wait gave up.
+uint32_t* device_status(cudaStream_t s);
+int consume_device_status(cudaStream_t s);
 enum : uint32_t {
   DEV_STATUS_TIMEOUT = 1u,      // a bounded wait gave up
   DEV_STATUS_NOT_SPD = 2u,      // a Cholesky pivot was <= 0
@@ -40,6 +43,7 @@ enum : uint32_t {
 // this is a no-op. Used by bench.py to time the dominant kernel on its own
 // stream with CUDA events.
 void profile_mark(cudaStream_t s, const char* name);
+bool profiling_on();
 
 struct DevBuf {
   void* p = nullptr;

@@ -35,6 +35,28 @@
 #include "sm100_ptx.cuh"
 
 namespace hp {
+// Launch kernel k; with pdl set, as a programmatic dependent launch: the
+// kernel may be scheduled while its predecessor in the stream still runs
+// and waits for it (griddep_wait) before touching the predecessor's
+// output. The Ozaki GEMM's phases and the residue-domain Cholesky's
+// diagonal path are chained this way, so that each launch's set-up
+// overlaps the tail of the previous kernel.
+template <typename... P, typename... A>
+static cudaError_t launch_k(bool pdl, void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
+                            A&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = pdl ? at : nullptr;
+  cfg.numAttrs = pdl ? 1 : 0;
+  return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
+}
+
 namespace ozaki {
 
 constexpr int MAXL = 49;        // number of pairwise-coprime moduli <= 256 in the table
@@ -233,42 +255,82 @@ __device__ __forceinline__ uint32_t mod_reduce(int32_t x, int l) {
   return r >= m ? r - m : r;
 }
 
-// Max exponent field over each row of a row-major R x C f128 matrix (one
-// warp per row). out[r] = max over the row of max(e(hi), e(lo) + 1).
-__global__ void maxexp_rows_kernel(const double2* __restrict__ src, int64_t R, int64_t C, int* __restrict__ out) {
-  int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-  int lane = threadIdx.x % 32;
-  if (row >= R) return;
-  int e = 0;
-  for (int64_t p = lane; p < C; p += 32) {
-    double2 v = src[row * C + p];
-    e = max(e, max(exp_field(v.x), min(exp_field(v.y) + 1, EXP_NONFINITE)));
-    if (exp_field(v.y) == EXP_NONFINITE) e = EXP_NONFINITE;
-  }
-  for (int o = 16; o; o >>= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, o));
-  if (lane == 0) out[row] = e;
+// Exponent pass of the f128 Ozaki GEMM in one launch. A (RA x CA,
+// row-major) contributes one exponent per row (a_rows) or per column, B
+// (RB x CB) one per column; an entry's exponent is max(e(hi), e(lo) + 1),
+// or the non-finite marker. Row blocks: 8 warps, one row each, four loads
+// in flight per lane. Column blocks: 32 columns x 8 row lanes over a slab
+// of `slab` rows, merged with atomicMax into outputs zeroed beforehand.
+// Blocks [0, na) serve A, the rest B.
+__device__ __forceinline__ int entry_exp(double2 v) {
+  const int el = exp_field(v.y);
+  return el == EXP_NONFINITE ? EXP_NONFINITE : max(exp_field(v.x), min(el + 1, EXP_NONFINITE));
 }
-// Max exponent field over each column of a row-major R x C f128 matrix.
-// Block: 32 columns x 8 row-lanes, each block covers a slab of rows.
-__global__ void maxexp_cols_kernel(const double2* __restrict__ src, int64_t R, int64_t C, int64_t slab,
-                                   int* __restrict__ out) {
+__global__ void __launch_bounds__(256) maxexp_kernel(const double2* __restrict__ A, int64_t RA, int64_t CA,
+                                                     bool a_rows, int* __restrict__ outA,
+                                                     const double2* __restrict__ B, int64_t RB, int64_t CB,
+                                                     int* __restrict__ outB, int64_t slab, unsigned na) {
+  sm100::griddep_launch_dependents();
+  const bool isA = blockIdx.x < na;
+  const unsigned bid = isA ? blockIdx.x : blockIdx.x - na;
+  const double2* src = isA ? A : B;
+  const int64_t R = isA ? RA : RB, C = isA ? CA : CB;
+  int* out = isA ? outA : outB;
+  const int lane = threadIdx.x % 32, wy = threadIdx.x / 32;
+  if (isA && a_rows) {
+    const int64_t row = (int64_t)bid * 8 + wy;
+    if (row >= R) return;
+    const double2* rp = src + row * C;
+    int e = 0;
+    for (int64_t p = lane; p < C; p += 128) {
+      double2 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) v[u] = p + 32 * u < C ? rp[p + 32 * u] : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int u = 0; u < 4; u++) e = max(e, entry_exp(v[u]));
+    }
+    for (int o = 16; o; o >>= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, o));
+    if (lane == 0) out[row] = e;
+    return;
+  }
   __shared__ int red[8][33];
-  int64_t c = (int64_t)blockIdx.x * 32 + threadIdx.x;
-  int64_t r0 = (int64_t)blockIdx.y * slab, r1 = min(R, r0 + slab);
+  const int64_t ncb = (C + 31) / 32;
+  const int64_t c = (int64_t)(bid % ncb) * 32 + lane;
+  const int64_t r0 = (int64_t)(bid / ncb) * slab, r1 = min(R, r0 + slab);
   int e = 0;
   if (c < C) {
-    for (int64_t r = r0 + threadIdx.y; r < r1; r += 8) {
-      double2 v = src[r * C + c];
-      e = max(e, max(exp_field(v.x), min(exp_field(v.y) + 1, EXP_NONFINITE)));
-      if (exp_field(v.y) == EXP_NONFINITE) e = EXP_NONFINITE;
+    for (int64_t r = r0 + wy; r < r1; r += 32) {
+      double2 v[4];
+#pragma unroll
+      for (int u = 0; u < 4; u++) v[u] = r + 8 * u < r1 ? src[(r + 8 * u) * C + c] : make_double2(0.0, 0.0);
+#pragma unroll
+      for (int u = 0; u < 4; u++) e = max(e, entry_exp(v[u]));
     }
   }
-  red[threadIdx.y][threadIdx.x] = e;
+  red[wy][lane] = e;
   __syncthreads();
-  if (threadIdx.y == 0 && c < C) {
-    for (int y = 1; y < 8; y++) e = max(e, red[y][threadIdx.x]);
+  if (wy == 0 && c < C) {
+    for (int y = 1; y < 8; y++) e = max(e, red[y][lane]);
     atomicMax(out + c, e);
   }
+}
+// Exponents of the f128 GEMM's operands: expA per row of A (per column when
+// atb, A being k x m) and expB per column of B (k x n), both zeroed by the
+// caller.
+static int launch_maxexp(const double2* A, const double2* B, size_t m, size_t n, size_t k, bool atb, int* expA,
+                         int* expB, cudaStream_t s) {
+  const int64_t slab = 256;
+  const int64_t kslabs = ((int64_t)k + slab - 1) / slab;
+  const int64_t na = atb ? ((int64_t)m + 31) / 32 * kslabs : ((int64_t)m + 7) / 8;
+  const int64_t nb = ((int64_t)n + 31) / 32 * kslabs;
+  if (na + nb > INT32_MAX) {
+    set_error("ozaki: exponent pass grid too large");
+    return HP_ERR_INVALID_ARG;
+  }
+  maxexp_kernel<<<(unsigned)(na + nb), 256, 0, s>>>(A, atb ? (int64_t)k : (int64_t)m, atb ? (int64_t)m : (int64_t)k,
+                                                    !atb, expA, B, (int64_t)k, (int64_t)n, expB, slab, (unsigned)na);
+  HP_LAUNCH_CHECK();
+  return HP_OK;
 }
 
 // Balanced base-2^22 digits of rint(v) for |v| < 2^108 (exact).
@@ -323,35 +385,46 @@ __device__ __forceinline__ uint32_t balanced_byte(const int32_t* D, int l, int m
   if (r > 127) r -= m;
   return (uint32_t)(r & 0xFF);
 }
+// One RT_R x RT_P tile (block coordinates bx, by) of the residue planes of
+// a scaled f128 operand: 8 entries per thread, all L moduli.
 template <bool P_CONTIG>
-__global__ void __launch_bounds__(256) residue_kernel(const double2* __restrict__ src, int64_t R, int64_t K,
-                                                      const int* __restrict__ expf, int beta, int L, int64_t ld,
-                                                      int64_t plane_stride, int8_t* __restrict__ out) {
+__device__ __forceinline__ void residue_tile(const double2* __restrict__ src, int64_t R, int64_t K,
+                                             const int* __restrict__ expf, int beta, int L, int64_t ld,
+                                             int64_t plane_stride, int8_t* __restrict__ out, unsigned bx,
+                                             unsigned by) {
   __shared__ __align__(16) uint32_t T[2][RT_R][RT_P / 4 + 1];
   const int t = threadIdx.x;
   const int rl = P_CONTIG ? t / 4 : t % 64;
   const int oct = P_CONTIG ? t % 4 : t / 64;
-  const int64_t r = (int64_t)blockIdx.y * RT_R + rl;
-  const int64_t p0 = (int64_t)blockIdx.x * RT_P + 8 * oct;
+  const int64_t r = (int64_t)by * RT_R + rl;
+  const int64_t p0 = (int64_t)bx * RT_P + 8 * oct;
   int32_t dig[8][NDIG];
 #pragma unroll
   for (int e = 0; e < 8; e++)
 #pragma unroll
     for (int c = 0; c < NDIG; c++) dig[e][c] = 0;
+  // the entries do not depend on the preceding exponent pass: load them
+  // before waiting for it
+  double2 v[8];
+#pragma unroll
+  for (int e = 0; e < 8; e++) {
+    const int64_t p = p0 + e;
+    v[e] = r < R && p < K ? (P_CONTIG ? src[r * K + p] : src[p * R + r]) : make_double2(0.0, 0.0);
+  }
+  sm100::griddep_launch_dependents();
+  sm100::griddep_wait();
   if (r < R) {
     const int ex = expf[r];
     if (ex != EXP_NONFINITE) {
       const int s = beta + 1022 - ex;
 #pragma unroll
-      for (int e = 0; e < 8; e++) {
-        const int64_t p = p0 + e;
-        if (p < K) element_digits(P_CONTIG ? src[r * K + p] : src[p * R + r], s, dig[e]);
-      }
+      for (int e = 0; e < 8; e++)
+        if (p0 + e < K) element_digits(v[e], s, dig[e]);
     }
   }
-  int8_t* const base = out + (size_t)(blockIdx.y * RT_R) * ld + blockIdx.x * RT_P;
+  int8_t* const base = out + (size_t)by * RT_R * ld + (size_t)bx * RT_P;
   int it = 0;
-  for (int l = blockIdx.z; l < L; l += gridDim.z, it++) {
+  for (int l = 0; l < L; l++, it++) {
     const int m = c_tab.mod[l];
     uint32_t w0 = 0, w1 = 0;
 #pragma unroll
@@ -374,6 +447,21 @@ __global__ void __launch_bounds__(256) residue_kernel(const double2* __restrict_
       }
     }
   }
+}
+
+// Residues of both operands of the f128 Ozaki GEMM in one launch: block
+// rows [0, tiles_ay) cover A (row-contiguous when A_CONTIG), the rest B.
+template <bool A_CONTIG>
+__global__ void __launch_bounds__(256) residue_ab_kernel(const double2* __restrict__ A, int64_t RA,
+                                                         const int* __restrict__ expA, int8_t* __restrict__ outA,
+                                                         int64_t planeA, unsigned tiles_ay,
+                                                         const double2* __restrict__ B, int64_t RB,
+                                                         const int* __restrict__ expB, int8_t* __restrict__ outB,
+                                                         int64_t planeB, int64_t K, int beta, int L, int64_t ld) {
+  if (blockIdx.y < tiles_ay)
+    residue_tile<A_CONTIG>(A, RA, K, expA, beta, L, ld, planeA, outA, blockIdx.x, blockIdx.y);
+  else
+    residue_tile<false>(B, RB, K, expB, beta, L, ld, planeB, outB, blockIdx.x, blockIdx.y - tiles_ay);
 }
 
 // ---------------------------------------------------------------------------
@@ -646,6 +734,8 @@ __global__ void __launch_bounds__(256) crt_dd_kernel(const uint8_t* __restrict__
   const int L = tab->L;
   for (int i = threadIdx.x; i < L * NC; i += blockDim.x) w_s[i / NC][i % NC] = tab->w[i / NC][i % NC];
   if (threadIdx.x < NC) mch_s[threadIdx.x] = tab->mchunk[threadIdx.x];
+  sm100::griddep_launch_dependents();
+  sm100::griddep_wait();  // the product residues come from the preceding GEMM
   __syncthreads();
   const double inv_m = tab->inv_m;
   const int64_t qpr = (n + 3) / 4;  // 4-entry groups per row
@@ -737,12 +827,14 @@ static int make_map(CUtensorMap* map, const void* base, uint64_t K, uint64_t R, 
 }
 
 static int launch_crt_dd(const uint8_t* cres, size_t Mp, size_t Np, size_t m, size_t n, const int* expA,
-                         const int* expB, int beta, const CrtTable* tab, int nc, double2* C, cudaStream_t s) {
+                         const int* expB, int beta, const CrtTable* tab, int nc, double2* C, cudaStream_t s,
+                         bool pdl = false) {
   const int64_t groups = (int64_t)m * (int64_t)((n + 3) / 4);
   const unsigned grid = (unsigned)((groups + 255) / 256);
 #define HP_CRT_CASE(NC)                                                                                       \
   case NC:                                                                                                    \
-    crt_dd_kernel<NC><<<grid, 256, 0, s>>>(cres, (int64_t)(Mp * Np), (int64_t)Np, m, n, expA, expB, beta, tab, C); \
+    HP_CUDA_TRY(launch_k(pdl, crt_dd_kernel<NC>, dim3(grid), dim3(256), 0, s, cres, (int64_t)(Mp * Np),         \
+                         (int64_t)Np, (int64_t)m, (int64_t)n, expA, expB, beta, tab, C));                      \
     break;
   switch (nc) {
     HP_CRT_CASE(3) HP_CRT_CASE(4) HP_CRT_CASE(5) HP_CRT_CASE(6) HP_CRT_CASE(7) HP_CRT_CASE(8) HP_CRT_CASE(9)
@@ -751,7 +843,6 @@ static int launch_crt_dd(const uint8_t* cres, size_t Mp, size_t Np, size_t m, si
       return HP_ERR_UNSUPPORTED;
   }
 #undef HP_CRT_CASE
-  HP_LAUNCH_CHECK();
   return HP_OK;
 }
 
@@ -792,7 +883,7 @@ int ozaki_residue_gemm_ex(const int8_t* ares, const int8_t* bres, uint8_t* cres,
 int ozaki_residue_gemm_k(const int8_t* ares, const int8_t* bres, uint8_t* cres, int L, size_t Mp, size_t Np,
                          size_t ka, size_t kb_len_b, size_t a_k0, size_t k_len, size_t b_k0, size_t ldc,
                          size_t plane, size_t c_row0, size_t c_col0, int acc_mode, cudaStream_t s, size_t ra_rows,
-                         size_t rb_rows) {
+                         size_t rb_rows, bool pdl) {
   using namespace ozaki;
   DevTables* D;
   HP_TRY(device_tables(&D));
@@ -820,10 +911,9 @@ int ozaki_residue_gemm_k(const int8_t* ares, const int8_t* bres, uint8_t* cres, 
   for (int c0 = 0; c0 < nkb_total; c0 += kb_chunk) {
     const int kb0 = kb_first + c0, kb1 = kb_first + std::min(nkb_total, c0 + kb_chunk);
     const int mode = c0 > 0 ? (acc_mode == 2 ? 2 : 1) : acc_mode;
-    i8_gemm_mod_kernel<GB_N><<<grid, 256, GEMM_SMEM, s>>>(mapA, mapB, L, tiles_m, tiles_n, kb0, kb1, boff, mode, cres,
-                                                     (int64_t)ldc, (int64_t)plane, (int64_t)c_row0,
-                                                     (int64_t)c_col0, status);
-    HP_LAUNCH_CHECK();
+    HP_CUDA_TRY(launch_k(pdl && c0 == 0, i8_gemm_mod_kernel<GB_N>, dim3(grid), dim3(256), GEMM_SMEM, s, mapA, mapB, L,
+                         tiles_m, tiles_n, kb0, kb1, boff, mode, cres, (int64_t)ldc, (int64_t)plane,
+                         (int64_t)c_row0, (int64_t)c_col0, status));
   }
   return HP_OK;
 }
@@ -849,52 +939,45 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
     set_error("ozaki: problem too large");
     return HP_ERR_INVALID_ARG;
   }
-  DevBuf expA(Mp * sizeof(int), s), expB(Np * sizeof(int), s);
+  DevBuf exps((Mp + Np) * sizeof(int), s);
   DevBuf ares((size_t)L * Mp * Kp, s), bres((size_t)L * Np * Kp, s), cres((size_t)L * Mp * Np, s);
-  if (!expA.p || !expB.p || !ares.p || !bres.p || !cres.p) {
+  if (!exps.p || !ares.p || !bres.p || !cres.p) {
     set_error("ozaki: workspace allocation failed");
     return HP_ERR_CUDA;
   }
-  HP_CUDA_TRY(cudaMemsetAsync(expA.p, 0, Mp * sizeof(int), s));
-  HP_CUDA_TRY(cudaMemsetAsync(expB.p, 0, Np * sizeof(int), s));
+  int* expA = exps.as<int>();
+  int* expB = expA + Mp;
+  HP_CUDA_TRY(cudaMemsetAsync(exps.p, 0, (Mp + Np) * sizeof(int), s));
+  // With profiling marks (events between the phases) the launches are not
+  // chained programmatically.
+  const bool pdl = !profiling_on();
   profile_mark(s, "start");
   const double2* A2 = reinterpret_cast<const double2*>(a);
   const double2* B2 = reinterpret_cast<const double2*>(b);
   // 1. exponents
-  if (!atb) {
-    maxexp_rows_kernel<<<(unsigned)((m + 7) / 8), 256, 0, s>>>(A2, m, k, expA.as<int>());
-  } else {
-    int64_t slab = 256;
-    dim3 g((unsigned)((m + 31) / 32), (unsigned)((k + slab - 1) / slab));
-    maxexp_cols_kernel<<<g, dim3(32, 8), 0, s>>>(A2, k, m, slab, expA.as<int>());
-  }
-  HP_LAUNCH_CHECK();
-  {
-    int64_t slab = 256;
-    dim3 g((unsigned)((n + 31) / 32), (unsigned)((k + slab - 1) / slab));
-    maxexp_cols_kernel<<<g, dim3(32, 8), 0, s>>>(B2, k, n, slab, expB.as<int>());
-    HP_LAUNCH_CHECK();
-  }
+  HP_TRY(launch_maxexp(A2, B2, m, n, k, atb, expA, expB, s));
   profile_mark(s, "exponents");
-  // 2. residues
+  // 2. residues (their loads of A and B overlap the exponent pass's tail)
   {
-    dim3 ga((unsigned)(Kp / RT_P), (unsigned)(Mp / RT_R));
+    const unsigned tay = (unsigned)(Mp / RT_R);
+    dim3 g((unsigned)(Kp / RT_P), tay + (unsigned)(Np / RT_R));
     if (!atb)
-      residue_kernel<true><<<ga, 256, 0, s>>>(A2, m, k, expA.as<int>(), beta, L, (int64_t)Kp, (int64_t)(Mp * Kp), ares.as<int8_t>());
+      HP_CUDA_TRY(launch_k(pdl, residue_ab_kernel<true>, g, dim3(256), 0, s, A2, (int64_t)m, (const int*)expA,
+                           ares.as<int8_t>(), (int64_t)(Mp * Kp), tay, B2, (int64_t)n, (const int*)expB,
+                           bres.as<int8_t>(), (int64_t)(Np * Kp), (int64_t)k, beta, L, (int64_t)Kp));
     else
-      residue_kernel<false><<<ga, 256, 0, s>>>(A2, m, k, expA.as<int>(), beta, L, (int64_t)Kp, (int64_t)(Mp * Kp), ares.as<int8_t>());
-    HP_LAUNCH_CHECK();
-    dim3 gb((unsigned)(Kp / RT_P), (unsigned)(Np / RT_R));
-    residue_kernel<false><<<gb, 256, 0, s>>>(B2, n, k, expB.as<int>(), beta, L, (int64_t)Kp, (int64_t)(Np * Kp), bres.as<int8_t>());
-    HP_LAUNCH_CHECK();
+      HP_CUDA_TRY(launch_k(pdl, residue_ab_kernel<false>, g, dim3(256), 0, s, A2, (int64_t)m, (const int*)expA,
+                           ares.as<int8_t>(), (int64_t)(Mp * Kp), tay, B2, (int64_t)n, (const int*)expB,
+                           bres.as<int8_t>(), (int64_t)(Np * Kp), (int64_t)k, beta, L, (int64_t)Kp));
   }
   profile_mark(s, "residues");
   // 3. one int8 GEMM per modulus
-  HP_TRY(ozaki_residue_gemm(ares.as<int8_t>(), bres.as<int8_t>(), cres.as<uint8_t>(), L, Mp, Np, Kp, s));
+  HP_TRY(ozaki_residue_gemm_k(ares.as<int8_t>(), bres.as<int8_t>(), cres.as<uint8_t>(), L, Mp, Np, Kp, Kp, 0, Kp, 0, Np,
+                              Mp * Np, 0, 0, 0, s, Mp, Np, pdl));
   profile_mark(s, "i8_gemm");
   // 4. CRT
-  HP_TRY(launch_crt_dd(cres.as<uint8_t>(), Mp, Np, m, n, expA.as<int>(), expB.as<int>(), beta, D->crt + L,
-                       host_tables().crt[L].nc, reinterpret_cast<double2*>(c), s));
+  HP_TRY(launch_crt_dd(cres.as<uint8_t>(), Mp, Np, m, n, expA, expB, beta, D->crt + L, host_tables().crt[L].nc,
+                       reinterpret_cast<double2*>(c), s, pdl));
   profile_mark(s, "crt");
   return HP_OK;
 }
@@ -1560,26 +1643,6 @@ __global__ void __launch_bounds__(256) panel_trsm_kernel(const dd* __restrict__ 
 
 }  // namespace ozaki
 
-// Launch kernel k; with pdl set, as a programmatic dependent launch: the
-// kernel may be scheduled while its predecessor in the stream still runs
-// and waits for it (griddep_wait) before touching the predecessor's
-// output. The residue-domain Cholesky chains its diagonal path this way,
-// so that each launch's set-up overlaps the tail of the previous kernel.
-template <typename... P, typename... A>
-static cudaError_t launch_k(bool pdl, void (*k)(P...), dim3 grid, dim3 block, size_t smem, cudaStream_t s,
-                            A&&... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = grid;
-  cfg.blockDim = block;
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute at[1];
-  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-  at[0].val.programmaticStreamSerializationAllowed = 1;
-  cfg.attrs = pdl ? at : nullptr;
-  cfg.numAttrs = pdl ? 1 : 0;
-  return cudaLaunchKernelEx(&cfg, k, std::forward<A>(args)...);
-}
 
 // res[l][r0 + i][c0 + j] -= sum_p A[l][i][p] B[l][j][p] (mod m_l) for
 // i < R, j < CH_NB, p < K: A = R rows of L~ residues from arow, B = CH_NB
@@ -1954,20 +2017,12 @@ static int ozaki_dd_gemm_noalloc(const double* a, const double* b, double* c, si
   HP_CUDA_TRY(cudaMemsetAsync(N->status, 0, sizeof(uint32_t), s));
   const double2* A2 = reinterpret_cast<const double2*>(a);
   const double2* B2 = reinterpret_cast<const double2*>(b);
-  maxexp_rows_kernel<<<(unsigned)((m + 7) / 8), 256, 0, s>>>(A2, m, k, expA);
-  HP_LAUNCH_CHECK();
+  HP_TRY(launch_maxexp(A2, B2, m, n, k, false, expA, expB, s));
   {
-    const int64_t slab = 256;
-    dim3 g((unsigned)((n + 31) / 32), (unsigned)((k + slab - 1) / slab));
-    maxexp_cols_kernel<<<g, dim3(32, 8), 0, s>>>(B2, k, n, slab, expB);
-    HP_LAUNCH_CHECK();
-  }
-  {
-    dim3 ga((unsigned)(Kp / RT_P), (unsigned)(Mp / RT_R));
-    residue_kernel<true><<<ga, 256, 0, s>>>(A2, m, k, expA, beta, L, (int64_t)Kp, (int64_t)(Mp * Kp), ares);
-    HP_LAUNCH_CHECK();
-    dim3 gb((unsigned)(Kp / RT_P), (unsigned)(Np / RT_R));
-    residue_kernel<false><<<gb, 256, 0, s>>>(B2, n, k, expB, beta, L, (int64_t)Kp, (int64_t)(Np * Kp), bres);
+    const unsigned tay = (unsigned)(Mp / RT_R);
+    dim3 g((unsigned)(Kp / RT_P), tay + (unsigned)(Np / RT_R));
+    residue_ab_kernel<true><<<g, 256, 0, s>>>(A2, m, expA, ares, (int64_t)(Mp * Kp), tay, B2, n, expB, bres,
+                                              (int64_t)(Np * Kp), k, beta, L, (int64_t)Kp);
     HP_LAUNCH_CHECK();
   }
   {

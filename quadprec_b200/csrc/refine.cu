@@ -180,6 +180,21 @@ int spd_refined(const double* S, const double* b, size_t n, int mode, double tol
   HP_TRY(dd_trsv_blocked(L.as<double>(), Xinv.as<double>(), x, n, false, s));
   HP_TRY(dd_trsv_blocked(L.as<double>(), Xinv.as<double>(), x, n, true, s));
   const unsigned* trsv_status = dd_trsv_status_word(Xinv.as<double>(), n);
+  uint32_t* dev_status = device_status(s);  // the residue GEMMs' bounded waits
+  if (!dev_status) {
+    set_error("status word allocation failed");
+    return HP_ERR_CUDA;
+  }
+  // a device-side wait that gave up: clear the word, report HP_ERR_TIMEOUT
+  auto timed_out = [&](unsigned trsv_bits, uint32_t dev_bits) -> bool {
+    if (dev_bits) cudaMemsetAsync(dev_status, 0, sizeof(uint32_t), s);
+    if ((trsv_bits | dev_bits) & DEV_STATUS_TIMEOUT) {
+      set_error(trsv_bits & DEV_STATUS_TIMEOUT ? "triangular solve: a block wait timed out"
+                                               : "residue GEMM: a bounded wait gave up");
+      return true;
+    }
+    return false;
+  };
   int it = 0, converged = 0;
   double ratio = 0.0;
   for (it = 1; it <= max_iter; it++) {
@@ -191,17 +206,16 @@ int spd_refined(const double* S, const double* b, size_t n, int mode, double tol
     HP_TRY(dd_maxabs(x, n, &scal.as<Readback>()->x_max, s));
     Readback h;
     unsigned st = 0;
+    uint32_t ds = 0;
     HP_CUDA_TRY(cudaMemcpyAsync(&h, scal.p, sizeof(h), cudaMemcpyDeviceToHost, s));
     HP_CUDA_TRY(cudaMemcpyAsync(&st, trsv_status, sizeof(st), cudaMemcpyDeviceToHost, s));
+    HP_CUDA_TRY(cudaMemcpyAsync(&ds, dev_status, sizeof(ds), cudaMemcpyDeviceToHost, s));
     HP_CUDA_TRY(cudaStreamSynchronize(s));
+    if (timed_out(st, ds)) return HP_ERR_TIMEOUT;
     if (mode != HP_MODE_PLAIN && h.ferr.flag) {
       if (pivot) *pivot = h.ferr.pivot;
       set_error("Cholesky failed at pivot %lld", (long long)h.ferr.pivot);
       return HP_ERR_NOT_SPD;
-    }
-    if (st & DEV_STATUS_TIMEOUT) {
-      set_error("triangular solve: a block wait timed out");
-      return HP_ERR_TIMEOUT;
     }
     ratio = h.x_max > 0 ? h.dx_max / h.x_max : 0.0;
     if (ratio <= tol) {
@@ -212,17 +226,16 @@ int spd_refined(const double* S, const double* b, size_t n, int mode, double tol
   if (max_iter < 1) {  // no iteration read the outcomes back
     FactorErr fe;
     unsigned st = 0;
+    uint32_t ds = 0;
     HP_CUDA_TRY(cudaMemcpyAsync(&fe, &scal.as<Readback>()->ferr, sizeof(fe), cudaMemcpyDeviceToHost, s));
     HP_CUDA_TRY(cudaMemcpyAsync(&st, trsv_status, sizeof(st), cudaMemcpyDeviceToHost, s));
+    HP_CUDA_TRY(cudaMemcpyAsync(&ds, dev_status, sizeof(ds), cudaMemcpyDeviceToHost, s));
     HP_CUDA_TRY(cudaStreamSynchronize(s));
+    if (timed_out(st, ds)) return HP_ERR_TIMEOUT;
     if (mode != HP_MODE_PLAIN && fe.flag) {
       if (pivot) *pivot = fe.pivot;
       set_error("Cholesky failed at pivot %lld", (long long)fe.pivot);
       return HP_ERR_NOT_SPD;
-    }
-    if (st & DEV_STATUS_TIMEOUT) {
-      set_error("triangular solve: a block wait timed out");
-      return HP_ERR_TIMEOUT;
     }
   }
   cudaEventRecord(e2, s);

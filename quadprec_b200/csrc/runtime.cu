@@ -22,9 +22,9 @@ constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 cudaStream_t g_stream[kMaxDevices] = {};
 bool g_pool_ready[kMaxDevices] = {};
-// One status word per (device, stream) would be ideal; kernels OR bits and
-// the host clears before use, so a small ring per device suffices for the
-// library's serialised host-pointer calls and for *_dev callers on one stream.
+// One sticky status word per device: kernels OR bits into it, and the host
+// entry points read and clear it at their synchronisation points
+// (consume_device_status), so no launch needs a memset in front of it.
 uint32_t* g_status[kMaxDevices] = {};
 
 int cur_dev() {
@@ -67,19 +67,38 @@ void dev_free(void* p, cudaStream_t s) {
   if (p) cudaFreeAsync(p, s);
 }
 
-uint32_t* device_status(cudaStream_t s) {
+uint32_t* device_status(cudaStream_t) {
   int d = cur_dev();
-  {
-    std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_status[d]) {
-      if (cudaMalloc(&g_status[d], 64 * sizeof(uint32_t)) != cudaSuccess) {
-        cudaGetLastError();
-        return nullptr;
-      }
+  std::lock_guard<std::mutex> lk(g_mu);
+  if (!g_status[d]) {
+    if (cudaMalloc(&g_status[d], 64 * sizeof(uint32_t)) != cudaSuccess ||
+        cudaMemset(g_status[d], 0, 64 * sizeof(uint32_t)) != cudaSuccess) {
+      cudaGetLastError();
+      g_status[d] = nullptr;
+      return nullptr;
     }
   }
-  cudaMemsetAsync(g_status[d], 0, sizeof(uint32_t), s);
   return g_status[d];
+}
+
+int consume_device_status(cudaStream_t s) {
+  uint32_t* w = device_status(s);
+  if (!w) {
+    set_error("status word allocation failed");
+    return HP_ERR_CUDA;
+  }
+  uint32_t h = 0;
+  HP_CUDA_TRY(cudaMemcpyAsync(&h, w, sizeof(h), cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  if (h == 0) return HP_OK;
+  HP_CUDA_TRY(cudaMemsetAsync(w, 0, sizeof(uint32_t), s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  if (h & DEV_STATUS_TIMEOUT) {
+    set_error("a bounded device-side wait gave up (status 0x%x)", h);
+    return HP_ERR_TIMEOUT;
+  }
+  set_error("device status 0x%x", h);
+  return HP_ERR_CUDA;
 }
 
 namespace {
@@ -92,6 +111,8 @@ struct ProfState {
 };
 ProfState g_prof;
 }  // namespace
+
+bool profiling_on() { return g_prof.on; }
 
 void profile_mark(cudaStream_t s, const char* name) {
   if (!g_prof.on || g_prof.count >= 32) return;
