@@ -45,17 +45,49 @@ def log(*a):
 
 # ---------------------------------------------------------------- clocks
 class ClockSampler:
+    """SM clock, power and clock-event reasons sampled DURING a timed region.
+
+    NVML is polled every `period_s` seconds from a thread (the timed CUDA
+    work releases the GIL in its driver calls), so that even a region of a
+    few milliseconds gets several samples. The device is the CUDA device
+    `index` of this process, found in NVML by its UUID (NVML numbers every
+    GPU of the machine, CUDA only the visible ones). Falls back to polling
+    nvidia-smi (every 200 ms) when NVML is unavailable.
+    """
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    # NVML clock-event reason bits
+    REASONS = {"hw_slowdown": 0x8, "hw_thermal_slowdown": 0x40, "sw_thermal_slowdown": 0x20, "sw_power_cap": 0x4}
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, period_s: float = 0.002):
         self.index = index
+        self.period = period_s
         self.rows = []
         self.proc = None
         self.th = None
+        self.nvml = None
+        self.stop_evt = threading.Event()
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        uuid = getattr(torch.cuda.get_device_properties(self.index), "uuid", None)
+        if uuid is not None:
+            u = str(uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(u if u.startswith("GPU-") else "GPU-" + u)
+        return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def start(self):
+        try:
+            self.nvml = self._nvml_handle()
+        except Exception:
+            self.nvml = None
+        if self.nvml is not None:
+            self.th = threading.Thread(target=self._poll, daemon=True)
+            self.th.start()
+            return
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
@@ -66,6 +98,18 @@ class ClockSampler:
         self.th = threading.Thread(target=self._read, daemon=True)
         self.th.start()
 
+    def _poll(self):
+        nv, h = self.nvml
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        while not self.stop_evt.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                self.rows.append((float(sm), float(mx), bits))
+            except Exception:
+                pass
+            time.sleep(self.period)
+
     def _read(self):
         for line in self.proc.stdout:
             parts = [p.strip() for p in line.split(",")]
@@ -73,6 +117,14 @@ class ClockSampler:
                 self.rows.append(parts)
 
     def stop(self) -> dict:
+        if self.nvml is not None:
+            self.stop_evt.set()
+            self.th.join(timeout=2)
+            sm = [r[0] for r in self.rows]
+            reasons = sorted({k for r in self.rows for k, bit in self.REASONS.items() if r[2] & bit})
+            return {"sm_mhz": statistics.median(sm) if sm else None,
+                    "sm_max_mhz": max(r[1] for r in self.rows) if self.rows else None,
+                    "reasons": reasons, "samples": len(self.rows), "source": f"NVML every {self.period * 1e3:g} ms"}
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -87,7 +139,7 @@ class ClockSampler:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[i] for r in self.rows for i in range(4) if r[4 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(self.rows), "source": "nvidia-smi every 200 ms"}
 
 
 # ---------------------------------------------------------------- helpers
