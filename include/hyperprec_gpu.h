@@ -317,6 +317,16 @@ int hp_f128_jacobi_eigen_batched_dev(int count, const int64_t* n_off, const doub
  * rounding and sign. n <= 128. */
 int hp_canonical_orthogonalize(const double* s, size_t n, double threshold, double* x,
                                size_t* n_orth);
+/* replaces: pub fn solve_gen_eigen(f: &[f128], s: &[f128], n: usize, threshold: f64)
+ *           -> GenEigenResult          crates/solver/src/ortho.rs:185-239
+ * F C = S C diag(eps) by canonical orthogonalisation: X from S as above,
+ * F' = X^T F X (the reference's f128 gemm_rect / gemm_atb order, bit for bit),
+ * symmetrised, diagonalised on the GPU, eigenpairs ascending. eigenvalues:
+ * capacity n f128 (m used); eigenvectors: capacity n x n f128, receives C as
+ * n x m row-major (column k = eigenvector k); *n_basis = m. n <= 128;
+ * HP_ERR_NO_CONVERGE if a Jacobi sweep limit is reached. */
+int hp_solve_gen_eigen(const double* f, const double* s, size_t n, double threshold,
+                       double* eigenvalues, double* eigenvectors, size_t* n_basis);
 
 #ifdef __cplusplus
 }

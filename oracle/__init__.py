@@ -82,6 +82,7 @@ def lib():
             "or_solve_spd": ([_d, _d, _sz, _d, _d, _d, _i64], ctypes.c_int),
             "or_solve_spd_f128": ([_d, _d, _sz, _d, _d, _d, _i64], ctypes.c_int),
             "or_canonical_orthogonalize": ([_d, _sz, ctypes.c_double, _d], ctypes.c_size_t),
+            "or_solve_gen_eigen": ([_d, _d, _sz, ctypes.c_double, _d, _d], ctypes.c_size_t),
             "or_overlap_primitive_f64": ([ctypes.c_double, _d, ctypes.c_double, _d], ctypes.c_double),
             "or_overlap_primitive_f128": ([ctypes.c_double, _d, ctypes.c_double, _d, _d], None),
             "or_assemble_overlap_s": ([_sz, _d, _i64, _d, _d, _d, _d, _i64], None),
@@ -319,6 +320,14 @@ def canonical_orthogonalize(s, n, threshold):
     x = np.zeros((n, n, 2))
     m = lib().or_canonical_orthogonalize(_p(_f(s)), n, threshold, _p(x))
     return np.ascontiguousarray(x.reshape(-1)[: n * m * 2].reshape(n, m, 2))
+
+
+def solve_gen_eigen(f, s, n, threshold):
+    """solver/src/ortho.rs:191. Returns (eigenvalues (m, 2), C (n, m, 2), m)."""
+    ev = np.zeros((n, 2))
+    c = np.zeros((n, n, 2))
+    m = lib().or_solve_gen_eigen(_p(_f(f)), _p(_f(s)), n, threshold, _p(ev), _p(c))
+    return ev[:m].copy(), np.ascontiguousarray(c.reshape(-1)[: n * m * 2].reshape(n, m, 2)), m
 
 
 # ---------------- overlap ----------------

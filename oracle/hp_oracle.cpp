@@ -773,6 +773,58 @@ size_t or_canonical_orthogonalize(const double* s, size_t n, double threshold, d
   return m;
 }
 
+// solver/src/ortho.rs:41-55: C (m x p) = A (m x n) B (n x p), i-k-j order,
+// zero a_ik skipped.
+static std::vector<dd> gemm_rect_v(const std::vector<dd>& a, const std::vector<dd>& b, size_t m, size_t n,
+                                   size_t p) {
+  std::vector<dd> c(m * p, dd{0, 0});
+  for (size_t i = 0; i < m; i++)
+    for (size_t k = 0; k < n; k++) {
+      const dd aik = a[i * n + k];
+      if (aik.hi == 0.0 && aik.lo == 0.0) continue;
+      for (size_t j = 0; j < p; j++) c[i * p + j] = dd_add(c[i * p + j], dd_mul(aik, b[k * p + j]));
+    }
+  return c;
+}
+
+// solver/src/ortho.rs:191-239. Writes the m eigenvalues (ascending) and C
+// (n x m, row-major, column k = eigenvector k); returns m.
+size_t or_solve_gen_eigen(const double* f, const double* s, size_t n, double threshold, double* evals_out,
+                          double* c_out) {
+  std::vector<double> xb(n * n * 2, 0.0);
+  const size_t m = or_canonical_orthogonalize(s, n, threshold, xb.data());
+  if (m == 0) return 0;
+  std::vector<dd> x = load_vec(xb.data(), n * m), fm = load_vec(f, n * n);
+  std::vector<dd> tmp = gemm_rect_v(fm, x, n, n, m);
+  // F' = X^T tmp: linalg.rs:168-182 gemm_atb with A = X (k x m, k = n)
+  std::vector<dd> fp(m * m);
+  for (size_t i = 0; i < m; i++)
+    for (size_t j = 0; j < m; j++) {
+      dd acc{0, 0};
+      for (size_t q = 0; q < n; q++) acc = dd_add(acc, dd_mul(x[q * m + i], tmp[q * m + j]));
+      fp[i * m + j] = acc;
+    }
+  for (size_t i = 0; i < m; i++)
+    for (size_t j = i + 1; j < m; j++) {
+      const dd avg = dd_mul(dd_add(fp[i * m + j], fp[j * m + i]), dd{0.5, 0.0});
+      fp[i * m + j] = avg;
+      fp[j * m + i] = avg;
+    }
+  std::vector<dd> evals, evecs;
+  ortho_jacobi(fp, m, evals, evecs);
+  std::vector<size_t> order(m);
+  for (size_t i = 0; i < m; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(),
+                   [&](size_t a, size_t b) { return dd_to_f64(evals[a]) < dd_to_f64(evals[b]); });
+  std::vector<dd> sorted(m * m);
+  for (size_t nk = 0; nk < m; nk++)
+    for (size_t i = 0; i < m; i++) sorted[i * m + nk] = evecs[i * m + order[nk]];
+  std::vector<dd> c = gemm_rect_v(x, sorted, n, m, m);
+  for (size_t k = 0; k < m; k++) st(evals_out, k, evals[order[k]]);
+  for (size_t q = 0; q < n * m; q++) st(c_out, q, c[q]);
+  return m;
+}
+
 // ---- overlap (crates/overlap) ----
 double or_overlap_primitive_f64(double ai, const double* ci, double aj, const double* cj) {
   return overlap_primitive_f64(ai, ci, aj, cj);

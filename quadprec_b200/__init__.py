@@ -73,6 +73,7 @@ SIGNATURES = {
     "hp_f256_gemv": ([_vp, _vp, _vp, _sz, _sz], ctypes.c_int),
     "hp_f256_dot": ([_vp, _vp, _sz, _vp], ctypes.c_int),
     "hp_canonical_orthogonalize": ([_vp, _sz, ctypes.c_double, _vp, ctypes.POINTER(_sz)], ctypes.c_int),
+    "hp_solve_gen_eigen": ([_vp, _vp, _sz, ctypes.c_double, _vp, _vp, ctypes.POINTER(_sz)], ctypes.c_int),
     "hp_solve_spd": ([_vp, _vp, _sz, _vp, _vp, _vp, _i64p], ctypes.c_int),
     "hp_solve_spd_f128": ([_vp, _vp, _sz, _vp, _vp, _vp, _i64p], ctypes.c_int),
     "hp_spd_solve_refined": ([_vp, _vp, _sz, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp, _vp, _i64p],
@@ -244,6 +245,18 @@ def canonical_orthogonalize(s, n, threshold):
     m = _sz(0)
     check(lib().hp_canonical_orthogonalize(_ptr(s), n, threshold, _ptr(x), ctypes.byref(m)))
     return np.ascontiguousarray(x.reshape(-1)[: n * m.value * 2].reshape(n, m.value, 2))
+
+
+def solve_gen_eigen(f, s, n, threshold):
+    """solver/src/ortho.rs:191 solve_gen_eigen; f, s are (n, n, 2).
+    Returns (eigenvalues (m, 2) ascending, eigenvectors C (n, m, 2), m)."""
+    f, s = _c(f), _c(s)
+    ev = np.zeros((n, 2))
+    c = np.zeros((n, n, 2))
+    m = _sz(0)
+    check(lib().hp_solve_gen_eigen(_ptr(f), _ptr(s), n, threshold, _ptr(ev), _ptr(c), ctypes.byref(m)))
+    mm = m.value
+    return ev[:mm].copy(), np.ascontiguousarray(c.reshape(-1)[: n * mm * 2].reshape(n, mm, 2)), mm
 
 
 def f256_gemv(a, x, n, m):

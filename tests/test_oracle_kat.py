@@ -381,3 +381,37 @@ def test_overlap_norm_dd_diagonal_and_symmetry():
     s = O.overlap_norm_dd(cen, al)
     assert np.array_equal(s[np.arange(3), np.arange(3)], [[1.0, 0.0]] * 3)
     assert np.array_equal(s, s.transpose(1, 0, 2))
+
+
+def _gen_eigen_residual(f, s, ev, c, n, m):
+    """max_i |(F c_k)_i - eps_k (S c_k)_i| over k, in f128 (the reference
+    tests' dd loops, ortho.rs:316-340)."""
+    worst = 0.0
+    for k in range(m):
+        ck = c[:, k]
+        fc = O.gemm(f, np.ascontiguousarray(ck.reshape(n, 1, 2)), n, 1, n).reshape(n, 2)
+        sc = O.gemm(s, np.ascontiguousarray(ck.reshape(n, 1, 2)), n, 1, n).reshape(n, 2)
+        for i in range(n):
+            esc = O.dd_mul(ev[k], sc[i])
+            d = O.dd_sub(fc[i], esc)
+            worst = max(worst, abs(d[0] + d[1]))
+    return worst
+
+
+def test_solve_gen_eigen_2x2():  # solver/src/ortho.rs:303-343
+    n = 2
+    f = f128v([[2.0, 1.0], [1.0, 3.0]])
+    s = f128v([[1.0, 0.2], [0.2, 1.0]])
+    ev, c, m = O.solve_gen_eigen(f, s, n, 1e-8)
+    assert m == 2
+    assert _gen_eigen_residual(f, s, ev, c, n, m) < 1e-25
+    assert ev[0, 0] + ev[0, 1] < ev[1, 0] + ev[1, 1]
+
+
+def test_solve_gen_eigen_identity_overlap():  # solver/src/ortho.rs:346-377
+    n = 3
+    f = f128v([[3.0, 1.0, 0.0], [1.0, 2.0, 1.0], [0.0, 1.0, 4.0]])
+    s = f128v(np.eye(n))
+    ev, c, m = O.solve_gen_eigen(f, s, n, 1e-8)
+    assert m == 3
+    assert _gen_eigen_residual(f, s, ev, c, n, m) < 1e-25
