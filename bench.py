@@ -401,7 +401,9 @@ def batched_section(hp, torch, dev, stream, sptr, args, world, dist):
            "systems_per_s": world * ok * 1e3 / ms,
            "f128_gflops_factor": world * float((ns.astype(np.float64) ** 3).sum() / 3.0) / (ms * 1e-3) / 1e9,
            "refine_iterations_max": int(it.cpu().numpy().max()),
-           "launch": "one persistent kernel (work queue, largest-first) replayed from a CUDA graph"}
+           "launch": "one persistent kernel (work queue, largest-first) replayed from a CUDA graph",
+           "launch_shape": dict(zip(("threads_per_cta", "ctas_per_sm"), hp.batched_config()),
+                                picked_by="autotuner (every candidate timed on this batch at the first call)")}
     # batched Jacobi on the n <= 128 systems
     sel = np.nonzero(ns <= 128)[0]
     joff = np.zeros(len(sel) + 1, dtype=np.int64)

@@ -258,13 +258,23 @@ int hp_overlap_norm_dd_dev(size_t n, const double* centers, const double* alpha,
  * status[s] = HP_OK, HP_ERR_NOT_SPD or HP_ERR_NO_CONVERGE; iters[s] = steps.
  * _dev: offsets is a HOST array (count+1), everything else device memory;
  * the launch is captured in a CUDA graph on first use and replayed for
- * identical arguments. The plain form takes host arrays (b as f128). */
+ * identical arguments. The plain form takes host arrays (b as f128).
+ * Launch shape: the first call for a batch class (count rounded up to a
+ * power of two, largest n rounded up to 32, per device) times every
+ * candidate CTA size (256 / 512 / 1024 threads) x CTAs per SM (1..4, as
+ * occupancy allows) on the batch itself and keeps the fastest for the
+ * process; that call blocks until the search is done. All candidates
+ * compute the same bits. HP_AUTOTUNE=0 in the environment skips the search
+ * (512 threads, one CTA per SM). */
 int hp_spd_solve_batched(int count, const int64_t* offsets, const double* centers,
                          const double* alpha, const double* b, double* x, int32_t* status,
                          int32_t* iters, double tol, int max_iter);
 int hp_spd_solve_batched_dev(int count, const int64_t* offsets, const double* centers,
                              const double* alpha, const double* b, double* x, int32_t* status,
                              int32_t* iters, double tol, int max_iter, void* stream);
+/* Launch shape (threads per CTA, CTAs per SM) of the latest batched solve in
+ * this process (no reference counterpart: a report of the autotuner). */
+int hp_batched_config(int32_t* threads, int32_t* ctas_per_sm);
 /* Packed f128 overlap matrices of a batch (S_s at the running sum of n_t^2
  * entries, t < s); same evaluation as hp_overlap_norm_dd. offsets: host. */
 int hp_overlap_norm_dd_batched_dev(int count, const int64_t* offsets, const double* centers,

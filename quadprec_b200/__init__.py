@@ -80,6 +80,7 @@ SIGNATURES = {
                              ctypes.c_int),
     "hp_spd_solve_refined_dev": ([_vp, _vp, _sz, ctypes.c_int, ctypes.c_double, ctypes.c_int, _vp, _vp, _i64p,
                                   _vp], ctypes.c_int),
+    "hp_batched_config": ([_vp, _vp], ctypes.c_int),
     "hp_spd_solve_batched": ([ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int],
                              ctypes.c_int),
     "hp_spd_solve_batched_dev": ([ctypes.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.c_double, ctypes.c_int,
@@ -377,6 +378,14 @@ def spd_solve_batched(batch, tol=1e-28, max_iter=10):
     check(lib().hp_spd_solve_batched(count, off.ctypes.data, _ptr(_c(batch["centers"])), _ptr(_c(batch["alpha"])),
                                       _ptr(b), _ptr(x), st.ctypes.data, it.ctypes.data, tol, max_iter))
     return x, st, it
+
+
+def batched_config():
+    """(threads per CTA, CTAs per SM) the autotuner chose for the latest batched solve."""
+    t = np.zeros(1, dtype=np.int32)
+    c = np.zeros(1, dtype=np.int32)
+    check(lib().hp_batched_config(t.ctypes.data, c.ctypes.data))
+    return int(t[0]), int(c[0])
 
 
 def f128_jacobi_eigen(a, n, max_iter):

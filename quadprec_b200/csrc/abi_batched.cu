@@ -1,8 +1,11 @@
 // C ABI: batched overlap SPD solves (one persistent launch replayed from a
 // CUDA graph), batched / single Jacobi eigensolves, batched assembly.
 #include <algorithm>
+#include <cstdlib>
+#include <map>
 #include <mutex>
 #include <numeric>
+#include <string>
 #include <vector>
 
 #include "hp_runtime.cuh"
@@ -19,6 +22,84 @@ void lpt_order(int count, const int64_t* off, std::vector<int>& order, int* nmax
                    [&](int a, int b) { return off[a + 1] - off[a] > off[b + 1] - off[b]; });
   *nmax = 0;
   for (int i = 0; i < count; i++) *nmax = std::max<int>(*nmax, (int)(off[i + 1] - off[i]));
+}
+
+// Autotuner of the persistent launch (threads per CTA x CTAs per SM). The
+// first call for a batch class (device, count rounded up to a power of two,
+// largest n rounded up to 32) runs every candidate once on that batch, timed
+// with CUDA events on the caller's stream, and keeps the fastest for the
+// rest of the process; each candidate rewrites the same outputs with the
+// same bits. HP_AUTOTUNE=0 in the environment skips the search (512 threads,
+// one CTA per SM).
+struct TuneKey {
+  int dev, count_class, nmax_class;
+  bool operator<(const TuneKey& o) const {
+    return dev != o.dev ? dev < o.dev : count_class != o.count_class ? count_class < o.count_class
+                                                                     : nmax_class < o.nmax_class;
+  }
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, BatchedConfig> g_tuned;
+BatchedConfig g_last{512, 1};
+constexpr BatchedConfig kDefaultConfig{512, 1};
+
+bool autotune_enabled() {
+  const char* e = std::getenv("HP_AUTOTUNE");
+  return !(e && std::string(e) == "0");
+}
+
+int tuned_config(int count, const int* order, const int64_t* off, const double* centers, const double* alpha,
+                 const double* b, double* x, int* status, int* iters, int nmax, double tol, int max_iter,
+                 cudaStream_t s, BatchedConfig* out) {
+  int dev = 0;
+  HP_CUDA_TRY(cudaGetDevice(&dev));
+  int cc = 1;
+  while (cc < count) cc *= 2;
+  const TuneKey key{dev, cc, (nmax + 31) / 32};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tuned.find(key);
+    if (it != g_tuned.end()) {
+      *out = g_last = it->second;
+      return HP_OK;
+    }
+  }
+  std::vector<BatchedConfig> cands = autotune_enabled() ? batched_spd_candidates() : std::vector<BatchedConfig>{};
+  BatchedConfig best = kDefaultConfig;
+  if (cands.size() > 1) {
+    int gmax = 0;
+    for (const BatchedConfig& c : cands) gmax = std::max(gmax, batched_spd_grid(c));
+    DevBuf work(batched_spd_work_bytes(gmax, nmax), s), queue(sizeof(int), s);
+    if (!work.p || !queue.p) {
+      set_error("batched autotune: workspace allocation failed");
+      return HP_ERR_CUDA;
+    }
+    // first launch of each kernel variant untimed (an empty queue: every CTA
+    // exits at once), so that loading it does not count
+    for (const BatchedConfig& c : cands)
+      HP_TRY(batched_spd_launch(0, order, off, centers, alpha, b, x, status, iters, nmax, tol, max_iter, work.p,
+                                queue.as<int>(), c, s));
+    std::vector<cudaEvent_t> ev(cands.size() + 1);
+    for (auto& e : ev) HP_CUDA_TRY(cudaEventCreate(&e));
+    HP_CUDA_TRY(cudaEventRecord(ev[0], s));
+    for (size_t i = 0; i < cands.size(); i++) {
+      HP_TRY(batched_spd_launch(count, order, off, centers, alpha, b, x, status, iters, nmax, tol, max_iter, work.p,
+                                queue.as<int>(), cands[i], s));
+      HP_CUDA_TRY(cudaEventRecord(ev[i + 1], s));
+    }
+    HP_CUDA_TRY(cudaEventSynchronize(ev.back()));
+    float best_ms = 0.0f;
+    for (size_t i = 0; i < cands.size(); i++) {
+      float ms = 0.0f;
+      cudaEventElapsedTime(&ms, ev[i], ev[i + 1]);
+      if (i == 0 || ms < best_ms) best_ms = ms, best = cands[i];
+    }
+    for (auto& e : ev) cudaEventDestroy(e);
+  }
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tuned[key] = best;
+  *out = g_last = best;
+  return HP_OK;
 }
 
 // One cached graph: the batched launch for one argument set.
@@ -73,16 +154,19 @@ int hp_spd_solve_batched_dev(int count, const int64_t* offsets, const double* ce
   HP_CUDA_TRY(cudaMalloc(&g_cache.off_dev, (count + 1) * sizeof(int64_t)));
   HP_CUDA_TRY(cudaMemcpy(g_cache.order_dev, order.data(), count * sizeof(int), cudaMemcpyHostToDevice));
   HP_CUDA_TRY(cudaMemcpy(g_cache.off_dev, offsets, (count + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
+  BatchedConfig cfg;
+  HP_TRY(tuned_config(count, (const int*)g_cache.order_dev, (const int64_t*)g_cache.off_dev, centers, alpha, b, x,
+                      status, iters, nmax, tol, max_iter, s, &cfg));
   // The workspace belongs to the cached graph (allocated here, outside the
   // capture); the graph holds only the queue reset and the persistent kernel.
-  const int grid = batched_spd_grid(0);
+  const int grid = batched_spd_grid(cfg);
   HP_CUDA_TRY(cudaMalloc(&g_cache.work, batched_spd_work_bytes(grid, nmax)));
   HP_CUDA_TRY(cudaMalloc(&g_cache.queue, sizeof(int)));
   cudaStream_t cap;
   HP_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
   HP_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));
   int rc = batched_spd_launch(count, (const int*)g_cache.order_dev, (const int64_t*)g_cache.off_dev, centers, alpha,
-                              b, x, status, iters, nmax, tol, max_iter, g_cache.work, (int*)g_cache.queue, grid, cap);
+                              b, x, status, iters, nmax, tol, max_iter, g_cache.work, (int*)g_cache.queue, cfg, cap);
   cudaGraph_t graph = nullptr;
   cudaError_t ce = cudaStreamEndCapture(cap, &graph);
   cudaStreamDestroy(cap);
@@ -117,8 +201,11 @@ int hp_spd_solve_batched(int count, const int64_t* offsets, const double* center
   if (!dord.p || !doff.p) return HP_ERR_CUDA;
   HP_CUDA_TRY(cudaMemcpyAsync(dord.p, order.data(), count * sizeof(int), cudaMemcpyHostToDevice, s));
   HP_CUDA_TRY(cudaMemcpyAsync(doff.p, offsets, (count + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s));
+  BatchedConfig cfg;
+  HP_TRY(tuned_config(count, dord.as<int>(), doff.as<int64_t>(), dc.as<double>(), da.as<double>(), db.as<double>(),
+                      dx.as<double>(), dst.as<int>(), dit.as<int>(), nmax, tol, max_iter, s, &cfg));
   HP_TRY(batched_spd(count, dord.as<int>(), doff.as<int64_t>(), dc.as<double>(), da.as<double>(), db.as<double>(),
-                     dx.as<double>(), dst.as<int>(), dit.as<int>(), nmax, tol, max_iter, s, 0));
+                     dx.as<double>(), dst.as<int>(), dit.as<int>(), nmax, tol, max_iter, s, cfg));
   HP_CUDA_TRY(cudaMemcpyAsync(x, dx.p, N * 16, cudaMemcpyDeviceToHost, s));
   HP_CUDA_TRY(cudaMemcpyAsync(status, dst.p, count * 4, cudaMemcpyDeviceToHost, s));
   HP_CUDA_TRY(cudaMemcpyAsync(iters, dit.p, count * 4, cudaMemcpyDeviceToHost, s));
@@ -195,6 +282,15 @@ int hp_f128_jacobi_eigen(const double* a, size_t n, size_t max_iter, double* eva
     set_error("Jacobi eigenvalue solver did not converge within max iterations");
     return HP_ERR_NO_CONVERGE;
   }
+  return HP_OK;
+}
+
+int hp_batched_config(int32_t* threads, int32_t* ctas_per_sm) {
+  using namespace hp;
+  if (!threads || !ctas_per_sm) return HP_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  *threads = g_last.threads;
+  *ctas_per_sm = g_last.ctas_per_sm;
   return HP_OK;
 }
 

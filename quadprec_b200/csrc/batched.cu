@@ -23,6 +23,9 @@
 // sweep) and the row-eigenvector output follow linalg.rs:299-362; the
 // rotation order differs (parallel instead of sequential), so results agree
 // with the reference to rounding, not bit-for-bit.
+#include <algorithm>
+#include <vector>
+
 #include "hp_arith.cuh"
 #include "hp_overlap.cuh"
 #include "hp_runtime.cuh"
@@ -34,6 +37,7 @@ namespace {
 
 constexpr int BT = 512;  // threads per CTA
 
+template <int NT>
 __device__ double block_max(double v, double* red) {
   v = fmax(v, __shfl_xor_sync(0xffffffffu, v, 16));
   v = fmax(v, __shfl_xor_sync(0xffffffffu, v, 8));
@@ -44,13 +48,14 @@ __device__ double block_max(double v, double* red) {
   if (threadIdx.x % 32 == 0) red[threadIdx.x / 32] = v;
   __syncthreads();
   double m = 0.0;
-  for (int w = 0; w < BT / 32; w++) m = fmax(m, red[w]);
+  for (int w = 0; w < NT / 32; w++) m = fmax(m, red[w]);
   __syncthreads();
   return m;
 }
 
 // In-CTA triangular solves with L (row-major n x n, lower) and rinv[j] =
 // 1 / l_jj from the factorisation, v in place.
+template <int NT>
 __device__ void cta_trsv(const dd* L, const dd* rinv, dd* v, int n, bool upper_t, dd* bc) {
   for (int s = 0; s < n; s++) {
     const int j = upper_t ? n - 1 - s : s;
@@ -61,9 +66,9 @@ __device__ void cta_trsv(const dd* L, const dd* rinv, dd* v, int n, bool upper_t
     __syncthreads();
     const dd vj = *bc;
     if (!upper_t) {
-      for (int i = j + 1 + threadIdx.x; i < n; i += BT) v[i] = dd_fms_fast(v[i], L[(size_t)i * n + j], vj);
+      for (int i = j + 1 + threadIdx.x; i < n; i += NT) v[i] = dd_fms_fast(v[i], L[(size_t)i * n + j], vj);
     } else {
-      for (int i = threadIdx.x; i < j; i += BT) v[i] = dd_fms_fast(v[i], L[(size_t)j * n + i], vj);
+      for (int i = threadIdx.x; i < j; i += NT) v[i] = dd_fms_fast(v[i], L[(size_t)j * n + i], vj);
     }
     __syncthreads();
   }
@@ -81,7 +86,8 @@ struct Casc3 {
   }
 };
 
-__global__ void __launch_bounds__(BT) batched_spd_kernel(int count, const int* __restrict__ order,
+template <int NT>
+__global__ void __launch_bounds__(NT) batched_spd_kernel(int count, const int* __restrict__ order,
                                                          const int64_t* __restrict__ off,
                                                          const double* __restrict__ centers,
                                                          const double* __restrict__ alpha, const dd* __restrict__ b,
@@ -90,7 +96,7 @@ __global__ void __launch_bounds__(BT) batched_spd_kernel(int count, const int* _
                                                          int64_t slot_elems, double tol, int max_iter) {
   __shared__ int sys_sh;
   __shared__ dd bc;
-  __shared__ double red[BT / 32];
+  __shared__ double red[NT / 32];
   __shared__ int fail;
   dd* S = work + (size_t)blockIdx.x * 2 * slot_elems;
   dd* L = S + slot_elems;
@@ -112,7 +118,7 @@ __global__ void __launch_bounds__(BT) batched_spd_kernel(int count, const int* _
     r = L + (size_t)n * n;  // residual vector after L inside the slot
     dd* rd = r + n;           // 1 / l_jj after it
     // 1. assemble S (lower triangle evaluated, mirrored), copy to L
-    for (int p = threadIdx.x; p < n * (n + 1) / 2; p += BT) {
+    for (int p = threadIdx.x; p < n * (n + 1) / 2; p += NT) {
       int i = (int)((sqrtf(8.0f * (float)p + 1.0f) - 1.0f) * 0.5f);
       while (i * (i + 1) / 2 > p) i--;
       while ((i + 1) * (i + 2) / 2 <= p) i++;
@@ -139,11 +145,11 @@ __global__ void __launch_bounds__(BT) batched_spd_kernel(int count, const int* _
       __syncthreads();
       if (fail) break;
       const dd rs = bc;
-      for (int i = j + 1 + threadIdx.x; i < n; i += BT) L[(size_t)i * n + j] = dd_mul(L[(size_t)i * n + j], rs);
+      for (int i = j + 1 + threadIdx.x; i < n; i += NT) L[(size_t)i * n + j] = dd_mul(L[(size_t)i * n + j], rs);
       __syncthreads();
       {  // trailing update: one warp per row, lanes along k <= i
         const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-        for (int i = j + 1 + warp; i < n; i += BT / 32) {
+        for (int i = j + 1 + warp; i < n; i += NT / 32) {
           const dd lij = L[(size_t)i * n + j];
           for (int k = j + 1 + lane; k <= i; k += 32)
             L[(size_t)i * n + k] = dd_fms_fast(L[(size_t)i * n + k], lij, L[(size_t)k * n + j]);
@@ -160,14 +166,14 @@ __global__ void __launch_bounds__(BT) batched_spd_kernel(int count, const int* _
       continue;
     }
     // 3. solve and refine
-    for (int i = threadIdx.x; i < n; i += BT) x[i] = b[o + i];
+    for (int i = threadIdx.x; i < n; i += NT) x[i] = b[o + i];
     __syncthreads();
-    cta_trsv(L, rd, x, n, false, &bc);
-    cta_trsv(L, rd, x, n, true, &bc);
+    cta_trsv<NT>(L, rd, x, n, false, &bc);
+    cta_trsv<NT>(L, rd, x, n, true, &bc);
     int it = 0, conv = 0;
     for (it = 1; it <= max_iter; it++) {
       const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-      for (int row = warp; row < n; row += BT / 32) {
+      for (int row = warp; row < n; row += NT / 32) {
         Casc3 c;
         if (lane == 0) {
           c.add(-b[o + row].hi);
@@ -204,16 +210,16 @@ __global__ void __launch_bounds__(BT) batched_spd_kernel(int count, const int* _
         }
       }
       __syncthreads();
-      cta_trsv(L, rd, r, n, false, &bc);
-      cta_trsv(L, rd, r, n, true, &bc);
+      cta_trsv<NT>(L, rd, r, n, false, &bc);
+      cta_trsv<NT>(L, rd, r, n, true, &bc);
       double md = 0.0, mx = 0.0;
-      for (int i = threadIdx.x; i < n; i += BT) {
+      for (int i = threadIdx.x; i < n; i += NT) {
         x[i] = dd_add(x[i], r[i]);
         md = fmax(md, fabs(r[i].hi));
         mx = fmax(mx, fabs(x[i].hi));
       }
-      md = block_max(md, red);
-      mx = block_max(mx, red);
+      md = block_max<NT>(md, red);
+      mx = block_max<NT>(mx, red);
       if (md <= tol * mx) {
         conv = 1;
         break;
@@ -377,11 +383,33 @@ __global__ void batched_assemble_kernel(const int64_t* __restrict__ off, const d
 
 }  // namespace
 
-int batched_spd_grid(int grid_override) {
+// Launch configurations of the persistent solver: threads per CTA and CTAs
+// per SM (grid = SMs x ctas_per_sm). Every candidate computes the same bits
+// (each entry's operation sequence is independent of the CTA size and
+// count: warp-per-row updates and residual cascades, in-CTA solves with the
+// same j order, order-free max reductions), so the choice is free.
+std::vector<BatchedConfig> batched_spd_candidates() {
+  std::vector<BatchedConfig> out;
+  const int threads[3] = {256, 512, 1024};
+  for (int t : threads) {
+    int nb = 0;
+    cudaError_t e = cudaErrorInvalidValue;
+    if (t == 256) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batched_spd_kernel<256>, 256, 0);
+    if (t == 512) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batched_spd_kernel<512>, 512, 0);
+    if (t == 1024) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batched_spd_kernel<1024>, 1024, 0);
+    if (e != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    for (int c = 1; c <= std::min(nb, 4); c++) out.push_back(BatchedConfig{t, c});
+  }
+  return out;
+}
+int batched_spd_grid(const BatchedConfig& cfg) {
   int dev = 0, sms = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return grid_override > 0 ? grid_override : sms;
+  return sms * std::max(1, cfg.ctas_per_sm);
 }
 size_t batched_spd_work_bytes(int grid, int nmax) {
   const int64_t slot = (int64_t)nmax * nmax + 2 * (int64_t)nmax;  // S, then L + r
@@ -392,27 +420,38 @@ size_t batched_spd_work_bytes(int grid, int nmax) {
 // allocation: safe inside stream capture).
 int batched_spd_launch(int count, const int* order, const int64_t* off, const double* centers, const double* alpha,
                        const double* b, double* x, int* status, int* iters, int nmax, double tol, int max_iter,
-                       void* work, int* queue, int grid, cudaStream_t s) {
+                       void* work, int* queue, const BatchedConfig& cfg, cudaStream_t s) {
   const int64_t slot = (int64_t)nmax * nmax + 2 * (int64_t)nmax;
+  const int grid = batched_spd_grid(cfg);
   HP_CUDA_TRY(cudaMemsetAsync(queue, 0, sizeof(int), s));
-  batched_spd_kernel<<<grid, BT, 0, s>>>(count, order, off, centers, alpha, reinterpret_cast<const dd*>(b),
-                                         reinterpret_cast<dd*>(x), status, iters, queue, reinterpret_cast<dd*>(work),
-                                         slot, tol, max_iter);
+#define HP_BATCHED_LAUNCH(NT)                                                                                      \
+  batched_spd_kernel<NT><<<grid, NT, 0, s>>>(count, order, off, centers, alpha, reinterpret_cast<const dd*>(b),  \
+                                             reinterpret_cast<dd*>(x), status, iters, queue,                       \
+                                             reinterpret_cast<dd*>(work), slot, tol, max_iter)
+  switch (cfg.threads) {
+    case 256: HP_BATCHED_LAUNCH(256); break;
+    case 512: HP_BATCHED_LAUNCH(512); break;
+    case 1024: HP_BATCHED_LAUNCH(1024); break;
+    default:
+      set_error("batched: unsupported CTA size %d", cfg.threads);
+      return HP_ERR_INVALID_ARG;
+  }
+#undef HP_BATCHED_LAUNCH
   HP_LAUNCH_CHECK();
   return HP_OK;
 }
 
 int batched_spd(int count, const int* order, const int64_t* off, const double* centers, const double* alpha,
                 const double* b, double* x, int* status, int* iters, int nmax, double tol, int max_iter,
-                cudaStream_t s, int grid_override) {
-  const int grid = batched_spd_grid(grid_override);
+                cudaStream_t s, const BatchedConfig& cfg) {
+  const int grid = batched_spd_grid(cfg);
   DevBuf work(batched_spd_work_bytes(grid, nmax), s), queue(sizeof(int), s);
   if (!work.p || !queue.p) {
     set_error("batched: workspace allocation failed");
     return HP_ERR_CUDA;
   }
   return batched_spd_launch(count, order, off, centers, alpha, b, x, status, iters, nmax, tol, max_iter, work.p,
-                            queue.as<int>(), grid, s);
+                            queue.as<int>(), cfg, s);
 }
 
 int batched_jacobi(int count, const int64_t* n_off, const int64_t* mat_off, const double* A, double* evals,

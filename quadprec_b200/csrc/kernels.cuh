@@ -5,6 +5,7 @@
 
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 namespace hp {
 
@@ -92,15 +93,21 @@ const unsigned* dd_trsv_status_word(const double* Xall, size_t n);
 }  // namespace hp
 
 namespace hp {
-// batched.cu
+// batched.cu: the persistent batched solver and its launch configurations
+// (threads per CTA, CTAs per SM); all configurations give the same bits.
+struct BatchedConfig {
+  int threads;
+  int ctas_per_sm;
+};
+std::vector<BatchedConfig> batched_spd_candidates();
+int batched_spd_grid(const BatchedConfig& cfg);
+size_t batched_spd_work_bytes(int grid, int nmax);
 int batched_spd(int count, const int* order, const int64_t* off, const double* centers, const double* alpha,
                 const double* b, double* x, int* status, int* iters, int nmax, double tol, int max_iter,
-                cudaStream_t s, int grid_override);
-int batched_spd_grid(int grid_override);
-size_t batched_spd_work_bytes(int grid, int nmax);
+                cudaStream_t s, const BatchedConfig& cfg);
 int batched_spd_launch(int count, const int* order, const int64_t* off, const double* centers, const double* alpha,
                        const double* b, double* x, int* status, int* iters, int nmax, double tol, int max_iter,
-                       void* work, int* queue, int grid, cudaStream_t s);
+                       void* work, int* queue, const BatchedConfig& cfg, cudaStream_t s);
 int batched_jacobi(int count, const int64_t* n_off, const int64_t* mat_off, const double* A, double* evals,
                    double* evecs, int* sweeps, int* status, int nmax, int max_sweeps, cudaStream_t s);
 int batched_assemble(int count, const int64_t* off, const double* centers, const double* alpha,

@@ -1,4 +1,8 @@
 """GPU batched overlap SPD solves and Jacobi eigensolves."""
+import os
+import subprocess
+import sys
+
 import numpy as np
 import pytest
 
@@ -30,6 +34,33 @@ def test_batched_solves_match_f256_oracle(gpu, small_batch):
         xs = O.mf_cholesky_solve(4, L4, b4, n)
         d = (xs[:, 0] - x[o:e, 0]) + (xs[:, 1] - x[o:e, 1]) + xs[:, 2]
         assert np.linalg.norm(d) / np.linalg.norm(xs[:, 0]) <= 1e-25, s
+
+
+def test_autotuned_launch_shape_gives_the_same_bits(gpu, small_batch):
+    """The autotuner picks the CTA size and CTAs per SM of the persistent
+    solver; every candidate must compute the same bits. Compared with the
+    search switched off (HP_AUTOTUNE=0: 512 threads, one CTA per SM) in a
+    fresh process on the same batch."""
+    x, st, it = gpu.spd_solve_batched(small_batch)
+    threads, ctas = gpu.batched_config()
+    assert threads in (256, 512, 1024) and 1 <= ctas <= 4, (threads, ctas)
+    code = (
+        "import sys, numpy as np, quadprec_b200 as hp\n"
+        "from quadprec_b200.workloads import batched_overlap_systems\n"
+        "B = batched_overlap_systems(count=24, seed=3, n_min=16, n_max=64)\n"
+        "x, st, it = hp.spd_solve_batched(B)\n"
+        "assert hp.batched_config() == (512, 1), hp.batched_config()\n"
+        "sys.stdout.buffer.write(np.ascontiguousarray(x).tobytes() + st.tobytes() + it.tobytes())\n"
+    )
+    repo = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = subprocess.run([sys.executable, "-c", code], cwd=repo, env={**os.environ, "HP_AUTOTUNE": "0"},
+                         capture_output=True, timeout=600)
+    assert out.returncode == 0, out.stderr.decode()[-2000:]
+    nx = x.size * 8
+    x0 = np.frombuffer(out.stdout[:nx], dtype=np.float64).reshape(x.shape)
+    st0 = np.frombuffer(out.stdout[nx:nx + st.size * 4], dtype=np.int32)
+    it0 = np.frombuffer(out.stdout[nx + st.size * 4:], dtype=np.int32)
+    assert np.array_equal(x, x0) and np.array_equal(st, st0) and np.array_equal(it, it0)
 
 
 def test_batched_flags_only_bad_systems(gpu, small_batch):
