@@ -724,7 +724,10 @@ __device__ __forceinline__ dd crt_finish(double* acc, const double* mch, double 
   *neg_out = neg;
   return s;
 }
-template <int NC>
+// EPT consecutive entries of a row per thread (one 2- or 4-byte load per
+// modulus); fewer entries per thread hold fewer accumulators, so more warps
+// fit on an SM. The per-entry arithmetic does not depend on EPT.
+template <int NC, int EPT>
 __global__ void __launch_bounds__(256) crt_dd_kernel(const uint8_t* __restrict__ cres, int64_t plane, int64_t Np,
                                                      int64_t m, int64_t n, const int* __restrict__ expA,
                                                      const int* __restrict__ expB, int beta,
@@ -738,14 +741,14 @@ __global__ void __launch_bounds__(256) crt_dd_kernel(const uint8_t* __restrict__
   sm100::griddep_wait();  // the product residues come from the preceding GEMM
   __syncthreads();
   const double inv_m = tab->inv_m;
-  const int64_t qpr = (n + 3) / 4;  // 4-entry groups per row
+  const int64_t qpr = (n + EPT - 1) / EPT;  // EPT-entry groups per row
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= m * qpr) return;
-  const int64_t i = g / qpr, j0 = 4 * (g % qpr);
+  const int64_t i = g / qpr, j0 = EPT * (g % qpr);
   const int ea = expA[i];
-  double acc[4][NC + 1];
+  double acc[EPT][NC + 1];
 #pragma unroll
-  for (int e = 0; e < 4; e++)
+  for (int e = 0; e < EPT; e++)
 #pragma unroll
     for (int c = 0; c <= NC; c++) acc[e][c] = 0.0;
   const uint8_t* rp = cres + (size_t)i * Np + j0;
@@ -755,12 +758,15 @@ __global__ void __launch_bounds__(256) crt_dd_kernel(const uint8_t* __restrict__
     uint32_t v[8];
 #pragma unroll
     for (int u = 0; u < 8; u++)
-      v[u] = (l0 + u < L) ? __ldg(reinterpret_cast<const uint32_t*>(rp + (size_t)(l0 + u) * plane)) : 0u;
+      v[u] = l0 + u >= L    ? 0u
+             : EPT == 4 ? __ldg(reinterpret_cast<const uint32_t*>(rp + (size_t)(l0 + u) * plane))
+             : EPT == 2 ? (uint32_t)__ldg(reinterpret_cast<const unsigned short*>(rp + (size_t)(l0 + u) * plane))
+                        : (uint32_t)__ldg(rp + (size_t)(l0 + u) * plane);
 #pragma unroll
     for (int u = 0; u < 8; u++) {
       if (l0 + u >= L) break;
 #pragma unroll
-      for (int e = 0; e < 4; e++) {
+      for (int e = 0; e < EPT; e++) {
         const double r = byte_to_double((v[u] >> (8 * e)) & 0xFFu);
 #pragma unroll
         for (int c = 0; c < NC; c++) acc[e][c] = __fma_rn(r, w_s[l0 + u][c], acc[e][c]);
@@ -768,7 +774,7 @@ __global__ void __launch_bounds__(256) crt_dd_kernel(const uint8_t* __restrict__
     }
   }
 #pragma unroll
-  for (int e = 0; e < 4; e++) {
+  for (int e = 0; e < EPT; e++) {
     const int64_t j = j0 + e;
     if (j >= n) break;
     const int eb = expB[j];
@@ -826,14 +832,15 @@ static int make_map(CUtensorMap* map, const void* base, uint64_t K, uint64_t R, 
   return HP_OK;
 }
 
+constexpr int CRT_EPT = 2;  // entries per thread of crt_dd_kernel (measured best of 1, 2, 4)
 static int launch_crt_dd(const uint8_t* cres, size_t Mp, size_t Np, size_t m, size_t n, const int* expA,
                          const int* expB, int beta, const CrtTable* tab, int nc, double2* C, cudaStream_t s,
                          bool pdl = false) {
-  const int64_t groups = (int64_t)m * (int64_t)((n + 3) / 4);
+  const int64_t groups = (int64_t)m * (int64_t)((n + CRT_EPT - 1) / CRT_EPT);
   const unsigned grid = (unsigned)((groups + 255) / 256);
 #define HP_CRT_CASE(NC)                                                                                       \
   case NC:                                                                                                    \
-    HP_CUDA_TRY(launch_k(pdl, crt_dd_kernel<NC>, dim3(grid), dim3(256), 0, s, cres, (int64_t)(Mp * Np),         \
+    HP_CUDA_TRY(launch_k(pdl, crt_dd_kernel<NC, CRT_EPT>, dim3(grid), dim3(256), 0, s, cres, (int64_t)(Mp * Np), \
                          (int64_t)Np, (int64_t)m, (int64_t)n, expA, expB, beta, tab, C));                      \
     break;
   switch (nc) {
