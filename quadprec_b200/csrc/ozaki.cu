@@ -385,29 +385,31 @@ __device__ __forceinline__ uint32_t balanced_byte(const int32_t* D, int l, int m
   if (r > 127) r -= m;
   return (uint32_t)(r & 0xFF);
 }
-// One RT_R x RT_P tile (block coordinates bx, by) of the residue planes of
-// a scaled f128 operand: 8 entries per thread, all L moduli.
-template <bool P_CONTIG>
+// One RT_R x (4 EPR) tile (block coordinates bx, by) of the residue planes
+// of a scaled f128 operand: EPR entries per thread (8 or 4: fewer digits
+// live through the moduli loop, more warps per SM), all L moduli.
+template <bool P_CONTIG, int EPR>
 __device__ __forceinline__ void residue_tile(const double2* __restrict__ src, int64_t R, int64_t K,
                                              const int* __restrict__ expf, int beta, int L, int64_t ld,
                                              int64_t plane_stride, int8_t* __restrict__ out, unsigned bx,
                                              unsigned by) {
-  __shared__ __align__(16) uint32_t T[2][RT_R][RT_P / 4 + 1];
+  constexpr int NW = EPR / 4;  // 32-bit words (and 16-byte row chunks of the transposed store) per thread
+  __shared__ __align__(16) uint32_t T[2][RT_R][EPR + 1];
   const int t = threadIdx.x;
   const int rl = P_CONTIG ? t / 4 : t % 64;
-  const int oct = P_CONTIG ? t % 4 : t / 64;
+  const int quad = P_CONTIG ? t % 4 : t / 64;
   const int64_t r = (int64_t)by * RT_R + rl;
-  const int64_t p0 = (int64_t)bx * RT_P + 8 * oct;
-  int32_t dig[8][NDIG];
+  const int64_t p0 = (int64_t)bx * (4 * EPR) + EPR * quad;
+  int32_t dig[EPR][NDIG];
 #pragma unroll
-  for (int e = 0; e < 8; e++)
+  for (int e = 0; e < EPR; e++)
 #pragma unroll
     for (int c = 0; c < NDIG; c++) dig[e][c] = 0;
   // the entries do not depend on the preceding exponent pass: load them
   // before waiting for it
-  double2 v[8];
+  double2 v[EPR];
 #pragma unroll
-  for (int e = 0; e < 8; e++) {
+  for (int e = 0; e < EPR; e++) {
     const int64_t p = p0 + e;
     v[e] = r < R && p < K ? (P_CONTIG ? src[r * K + p] : src[p * R + r]) : make_double2(0.0, 0.0);
   }
@@ -418,29 +420,33 @@ __device__ __forceinline__ void residue_tile(const double2* __restrict__ src, in
     if (ex != EXP_NONFINITE) {
       const int s = beta + 1022 - ex;
 #pragma unroll
-      for (int e = 0; e < 8; e++)
+      for (int e = 0; e < EPR; e++)
         if (p0 + e < K) element_digits(v[e], s, dig[e]);
     }
   }
-  int8_t* const base = out + (size_t)by * RT_R * ld + (size_t)bx * RT_P;
+  int8_t* const base = out + (size_t)by * RT_R * ld + (size_t)bx * (4 * EPR);
   int it = 0;
   for (int l = 0; l < L; l++, it++) {
     const int m = c_tab.mod[l];
-    uint32_t w0 = 0, w1 = 0;
+    uint32_t w[NW];
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-      w0 |= balanced_byte(dig[e], l, m) << (8 * e);
-      w1 |= balanced_byte(dig[e + 4], l, m) << (8 * e);
+    for (int q = 0; q < NW; q++) {
+      w[q] = 0;
+#pragma unroll
+      for (int e = 0; e < 4; e++) w[q] |= balanced_byte(dig[4 * q + e], l, m) << (8 * e);
     }
     int8_t* plane = base + (size_t)l * plane_stride;
     if (P_CONTIG) {
-      *reinterpret_cast<uint2*>(plane + (size_t)rl * ld + 8 * oct) = make_uint2(w0, w1);
+      if (NW == 2)
+        *reinterpret_cast<uint2*>(plane + (size_t)rl * ld + EPR * quad) = make_uint2(w[0], w[NW - 1]);
+      else
+        *reinterpret_cast<uint32_t*>(plane + (size_t)rl * ld + EPR * quad) = w[0];
     } else {
-      T[it & 1][rl][2 * oct] = w0;
-      T[it & 1][rl][2 * oct + 1] = w1;
+#pragma unroll
+      for (int q = 0; q < NW; q++) T[it & 1][rl][NW * quad + q] = w[q];
       __syncthreads();
-      if (t < 2 * RT_R) {
-        const int row = t / 2, half = t % 2;
+      if (t < NW * RT_R) {
+        const int row = t / NW, half = t % NW;
         const uint32_t* src_w = &T[it & 1][row][4 * half];
         *reinterpret_cast<uint4*>(plane + (size_t)row * ld + 16 * half) =
             make_uint4(src_w[0], src_w[1], src_w[2], src_w[3]);
@@ -451,7 +457,7 @@ __device__ __forceinline__ void residue_tile(const double2* __restrict__ src, in
 
 // Residues of both operands of the f128 Ozaki GEMM in one launch: block
 // rows [0, tiles_ay) cover A (row-contiguous when A_CONTIG), the rest B.
-template <bool A_CONTIG>
+template <bool A_CONTIG, int EPR>
 __global__ void __launch_bounds__(256) residue_ab_kernel(const double2* __restrict__ A, int64_t RA,
                                                          const int* __restrict__ expA, int8_t* __restrict__ outA,
                                                          int64_t planeA, unsigned tiles_ay,
@@ -459,9 +465,9 @@ __global__ void __launch_bounds__(256) residue_ab_kernel(const double2* __restri
                                                          const int* __restrict__ expB, int8_t* __restrict__ outB,
                                                          int64_t planeB, int64_t K, int beta, int L, int64_t ld) {
   if (blockIdx.y < tiles_ay)
-    residue_tile<A_CONTIG>(A, RA, K, expA, beta, L, ld, planeA, outA, blockIdx.x, blockIdx.y);
+    residue_tile<A_CONTIG, EPR>(A, RA, K, expA, beta, L, ld, planeA, outA, blockIdx.x, blockIdx.y);
   else
-    residue_tile<false>(B, RB, K, expB, beta, L, ld, planeB, outB, blockIdx.x, blockIdx.y - tiles_ay);
+    residue_tile<false, EPR>(B, RB, K, expB, beta, L, ld, planeB, outB, blockIdx.x, blockIdx.y - tiles_ay);
 }
 
 // ---------------------------------------------------------------------------
@@ -832,6 +838,7 @@ static int make_map(CUtensorMap* map, const void* base, uint64_t K, uint64_t R, 
   return HP_OK;
 }
 
+constexpr int RES_EPR = 4;  // entries per thread of the f128 GEMM's residue kernel
 constexpr int CRT_EPT = 2;  // entries per thread of crt_dd_kernel (measured best of 1, 2, 4)
 static int launch_crt_dd(const uint8_t* cres, size_t Mp, size_t Np, size_t m, size_t n, const int* expA,
                          const int* expB, int beta, const CrtTable* tab, int nc, double2* C, cudaStream_t s,
@@ -967,13 +974,13 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
   // 2. residues (their loads of A and B overlap the exponent pass's tail)
   {
     const unsigned tay = (unsigned)(Mp / RT_R);
-    dim3 g((unsigned)(Kp / RT_P), tay + (unsigned)(Np / RT_R));
+    dim3 g((unsigned)(Kp / (4 * RES_EPR)), tay + (unsigned)(Np / RT_R));
     if (!atb)
-      HP_CUDA_TRY(launch_k(pdl, residue_ab_kernel<true>, g, dim3(256), 0, s, A2, (int64_t)m, (const int*)expA,
+      HP_CUDA_TRY(launch_k(pdl, residue_ab_kernel<true, RES_EPR>, g, dim3(256), 0, s, A2, (int64_t)m, (const int*)expA,
                            ares.as<int8_t>(), (int64_t)(Mp * Kp), tay, B2, (int64_t)n, (const int*)expB,
                            bres.as<int8_t>(), (int64_t)(Np * Kp), (int64_t)k, beta, L, (int64_t)Kp));
     else
-      HP_CUDA_TRY(launch_k(pdl, residue_ab_kernel<false>, g, dim3(256), 0, s, A2, (int64_t)m, (const int*)expA,
+      HP_CUDA_TRY(launch_k(pdl, residue_ab_kernel<false, RES_EPR>, g, dim3(256), 0, s, A2, (int64_t)m, (const int*)expA,
                            ares.as<int8_t>(), (int64_t)(Mp * Kp), tay, B2, (int64_t)n, (const int*)expB,
                            bres.as<int8_t>(), (int64_t)(Np * Kp), (int64_t)k, beta, L, (int64_t)Kp));
   }
@@ -2028,7 +2035,7 @@ static int ozaki_dd_gemm_noalloc(const double* a, const double* b, double* c, si
   {
     const unsigned tay = (unsigned)(Mp / RT_R);
     dim3 g((unsigned)(Kp / RT_P), tay + (unsigned)(Np / RT_R));
-    residue_ab_kernel<true><<<g, 256, 0, s>>>(A2, m, expA, ares, (int64_t)(Mp * Kp), tay, B2, n, expB, bres,
+    residue_ab_kernel<true, 8><<<g, 256, 0, s>>>(A2, m, expA, ares, (int64_t)(Mp * Kp), tay, B2, n, expB, bres,
                                               (int64_t)(Np * Kp), k, beta, L, (int64_t)Kp);
     HP_LAUNCH_CHECK();
   }
