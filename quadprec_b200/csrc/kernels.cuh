@@ -66,6 +66,8 @@ int ozaki_moduli_for(size_t k, int beta);
 int dd_residual(const double* S, const double* x, const double* b, double* r, size_t n, bool accurate_qd,
                 cudaStream_t s);
 int dd_maxabs(const double* v, size_t n, double* out_dev, cudaStream_t s);
+// x += dx; out_dev[0] = max |dx.hi|, out_dev[1] = max |x.hi| (updated x).
+int dd_update_norms(double* x, const double* dx, size_t n, double* out_dev, cudaStream_t s);
 // Outcome of a device-side factorisation: flag != 0 when a pivot was not
 // positive, pivot = the first such index.
 struct FactorErr {

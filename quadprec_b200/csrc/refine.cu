@@ -38,44 +38,64 @@ struct Casc3 {
   }
 };
 
-// r = b - S x, warp per row.
+// r = b - S x, four warps per row (each a quarter of the columns, k-ordered
+// within it); the row's four partial cascades are combined in segment order
+// through shared memory. Two rows per CTA.
+constexpr int RS_SEG = 4;
 __global__ void __launch_bounds__(256) resid_sumk_kernel(const dd* __restrict__ S, const dd* __restrict__ x,
                                                          const dd* __restrict__ b, dd* __restrict__ r, int64_t n) {
-  const int64_t row = (int64_t)blockIdx.x * 8 + threadIdx.x / 32;
-  const int lane = threadIdx.x % 32;
-  if (row >= n) return;
+  __shared__ double part[2][RS_SEG][3];
+  const int w = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const int rloc = w / RS_SEG, seg = w % RS_SEG;
+  const int64_t row = (int64_t)blockIdx.x * 2 + rloc;
   Casc3 c;
-  if (lane == 0) {
-    c.add(-b[row].hi);
-    c.add(-b[row].lo);
-  }
-  const dd* srow = S + row * n;
-  for (int64_t j = lane; j < n; j += 32) {
-    const dd s = srow[j], v = x[j];
-    double p, e;
-    two_prod(s.hi, v.hi, p, e);
-    c.add(p);
-    c.add(e);
-    two_prod(s.hi, v.lo, p, e);
-    c.add(p);
-    c.add(e);
-    two_prod(s.lo, v.hi, p, e);
-    c.add(p);
-    c.add(e);
-    c.add(__dmul_rn(s.lo, v.lo));
-  }
+  if (row < n) {
+    if (seg == 0 && lane == 0) {
+      c.add(-b[row].hi);
+      c.add(-b[row].lo);
+    }
+    const dd* srow = S + row * n;
+    const int64_t j1 = n * (seg + 1) / RS_SEG;
+    for (int64_t j = n * seg / RS_SEG + lane; j < j1; j += 32) {
+      const dd sv = srow[j], v = x[j];
+      double p, e;
+      two_prod(sv.hi, v.hi, p, e);
+      c.add(p);
+      c.add(e);
+      two_prod(sv.hi, v.lo, p, e);
+      c.add(p);
+      c.add(e);
+      two_prod(sv.lo, v.hi, p, e);
+      c.add(p);
+      c.add(e);
+      c.add(__dmul_rn(sv.lo, v.lo));
+    }
 #pragma unroll
-  for (int o = 16; o; o >>= 1) {
-    double t1 = __shfl_down_sync(0xffffffffu, c.s1, o);
-    double t2 = __shfl_down_sync(0xffffffffu, c.s2, o);
-    double t3 = __shfl_down_sync(0xffffffffu, c.s3, o);
-    if (lane < o) {
-      c.add(t1);
-      c.add(t2);
-      c.add(t3);
+    for (int o = 16; o; o >>= 1) {
+      double t1 = __shfl_down_sync(0xffffffffu, c.s1, o);
+      double t2 = __shfl_down_sync(0xffffffffu, c.s2, o);
+      double t3 = __shfl_down_sync(0xffffffffu, c.s3, o);
+      if (lane < o) {
+        c.add(t1);
+        c.add(t2);
+        c.add(t3);
+      }
+    }
+    if (lane == 0) {
+      part[rloc][seg][0] = c.s1;
+      part[rloc][seg][1] = c.s2;
+      part[rloc][seg][2] = c.s3;
     }
   }
-  if (lane == 0) r[row] = dd_neg(c.result());
+  __syncthreads();
+  if (row < n && seg == 0 && lane == 0) {
+    for (int q = 1; q < RS_SEG; q++) {
+      c.add(part[rloc][q][0]);
+      c.add(part[rloc][q][1]);
+      c.add(part[rloc][q][2]);
+    }
+    r[row] = dd_neg(c.result());
+  }
 }
 
 // r = b - S x in MultiFloat<4> arithmetic; lane k of the row's warp sums
@@ -117,7 +137,48 @@ __global__ void maxabs_kernel(const dd* __restrict__ v, int64_t n, double* out) 
   if (threadIdx.x == 0) *out = m[0];
 }
 
+// x += dx, then out[0] = max |dx_i.hi| and out[1] = max |x_i.hi| of the
+// updated x (exact, order independent), in one CTA.
+__global__ void __launch_bounds__(1024) update_norms_kernel(dd* __restrict__ x, const dd* __restrict__ dx, int64_t n,
+                                                            double* out) {
+  __shared__ double md_s[32], mx_s[32];
+  double md = 0.0, mx = 0.0;
+  for (int64_t i = threadIdx.x; i < n; i += blockDim.x) {
+    const dd d = dx[i];
+    const dd v = dd_add(x[i], d);
+    x[i] = v;
+    md = fmax(md, fabs(d.hi));
+    mx = fmax(mx, fabs(v.hi));
+  }
+#pragma unroll
+  for (int o = 16; o; o >>= 1) {
+    md = fmax(md, __shfl_xor_sync(0xffffffffu, md, o));
+    mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+  }
+  if (threadIdx.x % 32 == 0) {
+    md_s[threadIdx.x / 32] = md;
+    mx_s[threadIdx.x / 32] = mx;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x / 32); w++) {
+      md = fmax(md, md_s[w]);
+      mx = fmax(mx, mx_s[w]);
+    }
+    out[0] = md;
+    out[1] = mx;
+  }
+}
+
 }  // namespace
+
+int dd_update_norms(double* x, const double* dx, size_t n, double* out_dev, cudaStream_t s) {
+  if (n == 0) return HP_OK;
+  update_norms_kernel<<<1, 1024, 0, s>>>(reinterpret_cast<dd*>(x), reinterpret_cast<const dd*>(dx), (int64_t)n,
+                                         out_dev);
+  HP_LAUNCH_CHECK();
+  return HP_OK;
+}
 
 int dd_residual(const double* S, const double* x, const double* b, double* r, size_t n, bool accurate_qd,
                 cudaStream_t s) {
@@ -126,7 +187,7 @@ int dd_residual(const double* S, const double* x, const double* b, double* r, si
     resid_qd_kernel<<<(unsigned)((n + 1) / 2), 64, 0, s>>>(reinterpret_cast<const dd*>(S), reinterpret_cast<const dd*>(x),
                                                             reinterpret_cast<const dd*>(b), reinterpret_cast<dd*>(r), n);
   else
-    resid_sumk_kernel<<<(unsigned)((n + 7) / 8), 256, 0, s>>>(reinterpret_cast<const dd*>(S),
+    resid_sumk_kernel<<<(unsigned)((n + 1) / 2), 256, 0, s>>>(reinterpret_cast<const dd*>(S),
                                                                reinterpret_cast<const dd*>(x),
                                                                reinterpret_cast<const dd*>(b), reinterpret_cast<dd*>(r), n);
   HP_LAUNCH_CHECK();
@@ -201,9 +262,7 @@ int spd_refined(const double* S, const double* b, size_t n, int mode, double tol
     HP_TRY(dd_residual(S, x, b, r.as<double>(), n, mode == HP_MODE_PLAIN, s));
     HP_TRY(dd_trsv_blocked(L.as<double>(), Xinv.as<double>(), r.as<double>(), n, false, s));
     HP_TRY(dd_trsv_blocked(L.as<double>(), Xinv.as<double>(), r.as<double>(), n, true, s));
-    HP_TRY(dd_vec(1, x, r.as<double>(), x, nullptr, n, s));
-    HP_TRY(dd_maxabs(r.as<double>(), n, &scal.as<Readback>()->dx_max, s));
-    HP_TRY(dd_maxabs(x, n, &scal.as<Readback>()->x_max, s));
+    HP_TRY(dd_update_norms(x, r.as<double>(), n, &scal.as<Readback>()->dx_max, s));  // dx_max, x_max
     Readback h;
     unsigned st = 0;
     uint32_t ds = 0;
