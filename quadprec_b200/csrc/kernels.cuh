@@ -56,11 +56,12 @@ int ozaki_residue_gemm_ex(const int8_t* ares, const int8_t* bres, uint8_t* cres,
                           size_t Kp, size_t ldc, size_t plane, size_t c_row0, size_t c_col0, int acc_mode,
                           cudaStream_t s, size_t ra_rows, size_t rb_rows);
 // pdl: launch the GEMM as a programmatic dependent launch of the preceding
-// kernel in s (which it waits for before reading the residues).
+// kernel in s (which it waits for before reading the residues). u8: the
+// residues are unsigned bytes in [0, m) (else balanced signed bytes).
 int ozaki_residue_gemm_k(const int8_t* ares, const int8_t* bres, uint8_t* cres, int L, size_t Mp, size_t Np,
                          size_t ka, size_t kb_len_b, size_t a_k0, size_t k_len, size_t b_k0, size_t ldc,
                          size_t plane, size_t c_row0, size_t c_col0, int acc_mode, cudaStream_t s, size_t ra_rows,
-                         size_t rb_rows, bool pdl = false);
+                         size_t rb_rows, bool pdl = false, bool u8 = false);
 int ozaki_moduli_for(size_t k, int beta);
 // refine.cu
 int dd_residual(const double* S, const double* x, const double* b, double* r, size_t n, bool accurate_qd,

@@ -388,7 +388,14 @@ __device__ __forceinline__ uint32_t balanced_byte(const int32_t* D, int l, int m
 // One RT_R x (4 EPR) tile (block coordinates bx, by) of the residue planes
 // of a scaled f128 operand: EPR entries per thread (8 or 4: fewer digits
 // live through the moduli loop, more warps per SM), all L moduli.
-template <bool P_CONTIG, int EPR>
+// the residue in [0, m) as an unsigned byte (operands of the unsigned MMA)
+__device__ __forceinline__ uint32_t unsigned_byte(const int32_t* D, int l) {
+  int32_t x = D[0];  // 2^0 mod m = 1
+#pragma unroll
+  for (int c = 1; c < NDIG; c++) x += D[c] * c_tab.pw[l][c];
+  return mod_reduce(x, l);
+}
+template <bool P_CONTIG, int EPR, bool U8>
 __device__ __forceinline__ void residue_tile(const double2* __restrict__ src, int64_t R, int64_t K,
                                              const int* __restrict__ expf, int beta, int L, int64_t ld,
                                              int64_t plane_stride, int8_t* __restrict__ out, unsigned bx,
@@ -433,7 +440,10 @@ __device__ __forceinline__ void residue_tile(const double2* __restrict__ src, in
     for (int q = 0; q < NW; q++) {
       w[q] = 0;
 #pragma unroll
-      for (int e = 0; e < 4; e++) w[q] |= balanced_byte(dig[4 * q + e], l, m) << (8 * e);
+      for (int e = 0; e < 4; e++) {
+        const uint32_t byte = U8 ? unsigned_byte(dig[4 * q + e], l) : balanced_byte(dig[4 * q + e], l, m);
+        w[q] |= byte << (8 * e);
+      }
     }
     int8_t* plane = base + (size_t)l * plane_stride;
     if (P_CONTIG) {
@@ -457,7 +467,7 @@ __device__ __forceinline__ void residue_tile(const double2* __restrict__ src, in
 
 // Residues of both operands of the f128 Ozaki GEMM in one launch: block
 // rows [0, tiles_ay) cover A (row-contiguous when A_CONTIG), the rest B.
-template <bool A_CONTIG, int EPR>
+template <bool A_CONTIG, int EPR, bool U8>
 __global__ void __launch_bounds__(256) residue_ab_kernel(const double2* __restrict__ A, int64_t RA,
                                                          const int* __restrict__ expA, int8_t* __restrict__ outA,
                                                          int64_t planeA, unsigned tiles_ay,
@@ -465,9 +475,9 @@ __global__ void __launch_bounds__(256) residue_ab_kernel(const double2* __restri
                                                          const int* __restrict__ expB, int8_t* __restrict__ outB,
                                                          int64_t planeB, int64_t K, int beta, int L, int64_t ld) {
   if (blockIdx.y < tiles_ay)
-    residue_tile<A_CONTIG, EPR>(A, RA, K, expA, beta, L, ld, planeA, outA, blockIdx.x, blockIdx.y);
+    residue_tile<A_CONTIG, EPR, U8>(A, RA, K, expA, beta, L, ld, planeA, outA, blockIdx.x, blockIdx.y);
   else
-    residue_tile<false, EPR>(B, RB, K, expB, beta, L, ld, planeB, outB, blockIdx.x, blockIdx.y - tiles_ay);
+    residue_tile<false, EPR, U8>(B, RB, K, expB, beta, L, ld, planeB, outB, blockIdx.x, blockIdx.y - tiles_ay);
 }
 
 // ---------------------------------------------------------------------------
@@ -480,7 +490,10 @@ __global__ void __launch_bounds__(256) residue_ab_kernel(const double2* __restri
 constexpr int GB_M = 128, GB_N = 256, GB_K = 128, GSTAGES = 4;
 constexpr int A_STAGE = GB_M * GB_K, B_STAGE = GB_N * GB_K, STAGE_BYTES = A_STAGE + B_STAGE;
 constexpr int GEMM_SMEM = GSTAGES * STAGE_BYTES + 1024 + 256;
-constexpr int MAX_K_CHUNK = 65536;  // |int32 accumulator| <= 2^16 * 2^14 = 2^30
+constexpr int MAX_K_CHUNK = 65536;  // signed operands: |int32 accumulator| <= 2^16 * 2^14 = 2^30
+// unsigned operands (residues in [0, m)): accumulator <= 2^15 * 255^2 < 2^31,
+// and mod_reduce's offset keeps it below 2^32
+constexpr int MAX_K_CHUNK_U8 = 32768;
 
 // Tile shapes: BN = 256 (4-stage ring, the general GEMM) or BN = 64 (8-stage
 // ring, for the 64-column panels of the residue-domain Cholesky). The
@@ -495,7 +508,7 @@ struct GemmCfg {
 };
 static_assert(GemmCfg<256>::SMEM == GEMM_SMEM, "BN = 256 keeps the general GEMM's layout");
 
-template <int BN>
+template <int BN, bool U8 = false>
 __global__ void __launch_bounds__(256, 1)
     i8_gemm_mod_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int L,
                        int tiles_m, int tiles_n, int kb0, int kb1, int kb_off_b, int acc_mode,
@@ -583,7 +596,7 @@ __global__ void __launch_bounds__(256, 1)
       uint32_t stage = 0, phase = 0, it = 0;
       bool ok = true;
       bool issued = false;
-      const uint32_t idesc = idesc_i8(GB_M, BN);
+      const uint32_t idesc = idesc_i8(GB_M, BN, U8);
       for (int t = blockIdx.x; t < num_tiles && ok; t += gridDim.x, it++) {
         const uint32_t acc = it & 1, aph = (it >> 1) & 1;
         if (!mbar_wait(&tempty[acc], aph ^ 1, status, DEV_STATUS_TIMEOUT)) {
@@ -897,7 +910,7 @@ int ozaki_residue_gemm_ex(const int8_t* ares, const int8_t* bres, uint8_t* cres,
 int ozaki_residue_gemm_k(const int8_t* ares, const int8_t* bres, uint8_t* cres, int L, size_t Mp, size_t Np,
                          size_t ka, size_t kb_len_b, size_t a_k0, size_t k_len, size_t b_k0, size_t ldc,
                          size_t plane, size_t c_row0, size_t c_col0, int acc_mode, cudaStream_t s, size_t ra_rows,
-                         size_t rb_rows, bool pdl) {
+                         size_t rb_rows, bool pdl, bool u8) {
   using namespace ozaki;
   DevTables* D;
   HP_TRY(device_tables(&D));
@@ -906,6 +919,8 @@ int ozaki_residue_gemm_k(const int8_t* ares, const int8_t* bres, uint8_t* cres, 
   cudaGetDevice(&dev);
   if (!attr_set[dev]) {
     HP_CUDA_TRY(cudaFuncSetAttribute(i8_gemm_mod_kernel<GB_N>, cudaFuncAttributeMaxDynamicSharedMemorySize, GEMM_SMEM));
+    HP_CUDA_TRY(cudaFuncSetAttribute(i8_gemm_mod_kernel<GB_N, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     GEMM_SMEM));
     attr_set[dev] = true;
   }
   CUtensorMap mapA, mapB;
@@ -921,13 +936,18 @@ int ozaki_residue_gemm_k(const int8_t* ares, const int8_t* bres, uint8_t* cres, 
   const int grid = std::min(num_tiles, D->num_sms);
   const int kb_first = (int)(a_k0 / GB_K), nkb_total = (int)(k_len / GB_K);
   const int boff = (int)(b_k0 / GB_K) - kb_first;
-  const int kb_chunk = MAX_K_CHUNK / GB_K;
+  const int kb_chunk = (u8 ? MAX_K_CHUNK_U8 : MAX_K_CHUNK) / GB_K;
   for (int c0 = 0; c0 < nkb_total; c0 += kb_chunk) {
     const int kb0 = kb_first + c0, kb1 = kb_first + std::min(nkb_total, c0 + kb_chunk);
     const int mode = c0 > 0 ? (acc_mode == 2 ? 2 : 1) : acc_mode;
-    HP_CUDA_TRY(launch_k(pdl && c0 == 0, i8_gemm_mod_kernel<GB_N>, dim3(grid), dim3(256), GEMM_SMEM, s, mapA, mapB, L,
-                         tiles_m, tiles_n, kb0, kb1, boff, mode, cres, (int64_t)ldc, (int64_t)plane,
-                         (int64_t)c_row0, (int64_t)c_col0, status));
+    if (u8)
+      HP_CUDA_TRY(launch_k(pdl && c0 == 0, i8_gemm_mod_kernel<GB_N, true>, dim3(grid), dim3(256), GEMM_SMEM, s, mapA,
+                           mapB, L, tiles_m, tiles_n, kb0, kb1, boff, mode, cres, (int64_t)ldc, (int64_t)plane,
+                           (int64_t)c_row0, (int64_t)c_col0, status));
+    else
+      HP_CUDA_TRY(launch_k(pdl && c0 == 0, i8_gemm_mod_kernel<GB_N>, dim3(grid), dim3(256), GEMM_SMEM, s, mapA, mapB,
+                           L, tiles_m, tiles_n, kb0, kb1, boff, mode, cres, (int64_t)ldc, (int64_t)plane,
+                           (int64_t)c_row0, (int64_t)c_col0, status));
   }
   return HP_OK;
 }
@@ -976,18 +996,18 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
     const unsigned tay = (unsigned)(Mp / RT_R);
     dim3 g((unsigned)(Kp / (4 * RES_EPR)), tay + (unsigned)(Np / RT_R));
     if (!atb)
-      HP_CUDA_TRY(launch_k(pdl, residue_ab_kernel<true, RES_EPR>, g, dim3(256), 0, s, A2, (int64_t)m, (const int*)expA,
+      HP_CUDA_TRY(launch_k(pdl, residue_ab_kernel<true, RES_EPR, true>, g, dim3(256), 0, s, A2, (int64_t)m, (const int*)expA,
                            ares.as<int8_t>(), (int64_t)(Mp * Kp), tay, B2, (int64_t)n, (const int*)expB,
                            bres.as<int8_t>(), (int64_t)(Np * Kp), (int64_t)k, beta, L, (int64_t)Kp));
     else
-      HP_CUDA_TRY(launch_k(pdl, residue_ab_kernel<false, RES_EPR>, g, dim3(256), 0, s, A2, (int64_t)m, (const int*)expA,
+      HP_CUDA_TRY(launch_k(pdl, residue_ab_kernel<false, RES_EPR, true>, g, dim3(256), 0, s, A2, (int64_t)m, (const int*)expA,
                            ares.as<int8_t>(), (int64_t)(Mp * Kp), tay, B2, (int64_t)n, (const int*)expB,
                            bres.as<int8_t>(), (int64_t)(Np * Kp), (int64_t)k, beta, L, (int64_t)Kp));
   }
   profile_mark(s, "residues");
   // 3. one int8 GEMM per modulus
   HP_TRY(ozaki_residue_gemm_k(ares.as<int8_t>(), bres.as<int8_t>(), cres.as<uint8_t>(), L, Mp, Np, Kp, Kp, 0, Kp, 0, Np,
-                              Mp * Np, 0, 0, 0, s, Mp, Np, pdl));
+                              Mp * Np, 0, 0, 0, s, Mp, Np, pdl, true));
   profile_mark(s, "i8_gemm");
   // 4. CRT
   HP_TRY(launch_crt_dd(cres.as<uint8_t>(), Mp, Np, m, n, expA, expB, beta, D->crt + L, host_tables().crt[L].nc,
@@ -2035,7 +2055,7 @@ static int ozaki_dd_gemm_noalloc(const double* a, const double* b, double* c, si
   {
     const unsigned tay = (unsigned)(Mp / RT_R);
     dim3 g((unsigned)(Kp / RT_P), tay + (unsigned)(Np / RT_R));
-    residue_ab_kernel<true, 8><<<g, 256, 0, s>>>(A2, m, expA, ares, (int64_t)(Mp * Kp), tay, B2, n, expB, bres,
+    residue_ab_kernel<true, 8, false><<<g, 256, 0, s>>>(A2, m, expA, ares, (int64_t)(Mp * Kp), tay, B2, n, expB, bres,
                                               (int64_t)(Np * Kp), k, beta, L, (int64_t)Kp);
     HP_LAUNCH_CHECK();
   }

@@ -138,10 +138,11 @@ __device__ __forceinline__ uint64_t desc_k_sw128(uint32_t smem_addr) {
   return (uint64_t)((smem_addr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
          (2ull << 61);
 }
-// Instruction descriptor, kind::i8: D = s32 (bits 4-5 = 2), A = B = signed
-// 8-bit (bits 7-9 = 1, 10-12 = 1), both K-major, N>>3 at bit 17, M>>4 at 24.
-__host__ __device__ constexpr uint32_t idesc_i8(uint32_t M, uint32_t N) {
-  return (2u << 4) | (1u << 7) | (1u << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
+// Instruction descriptor, kind::i8: D = s32 (bits 4-5 = 2), A and B signed
+// 8-bit (bits 7-9 = 1, 10-12 = 1) or unsigned (0), both K-major, N>>3 at
+// bit 17, M>>4 at 24.
+__host__ __device__ constexpr uint32_t idesc_i8(uint32_t M, uint32_t N, bool u8 = false) {
+  return (2u << 4) | ((u8 ? 0u : 1u) << 7) | ((u8 ? 0u : 1u) << 10) | ((N >> 3) << 17) | ((M >> 4) << 24);
 }
 
 }  // namespace sm100
