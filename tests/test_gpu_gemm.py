@@ -164,3 +164,15 @@ def test_f256_ozaki_exact_small_integers(gpu):
     B[..., 0] = rng.integers(-1000, 1000, (k, n))
     c = gpu.f256_gemm(A, B, m, n, k, gpu.OZAKI)
     assert np.array_equal(c[..., 0], A[..., 0] @ B[..., 0]) and np.all(c[..., 1:] == 0)
+
+
+@pytest.mark.parametrize("atb", [False, True])
+def test_f128_ozaki_long_k_chunks(gpu, atb):
+    """k beyond one accumulation chunk of the unsigned residue GEMM (32768):
+    the second chunk adds into the first's residues modulo m."""
+    m, n, k = 5, 9, 40000
+    a, b = gemm_operands(m, n, k, seed=99, atb=atb)
+    c = gpu.f128_gemm(a, b, m, n, k, gpu.OZAKI, atb)
+    ref = O.gemm(a, b, m, n, k, atb=atb)
+    err = normwise_err(c, ref, abs_prod(a, b, atb))
+    assert err <= 4 * k * 2.0 ** -104, err
