@@ -78,15 +78,43 @@ __device__ __forceinline__ dd dd_sqrt(dd a) {  // dd.rs:61-78
   dd r = dd_add(ax, dd_mul(ax, dd_sub(dd_from(0.5), dd_mul(ax, hx))));
   return dd_mul(dd_add(r, dd_div(a, r)), dd_from(0.5));
 }
+// x / b for a small positive integer b with y = RN(1/b): the correctly
+// rounded quotient, i.e. the bits of DIV(x, b). q1 = q0 + (x - q0 b) y is a
+// faithful quotient, and Markstein's final step q1 + (x - q1 b) y with
+// y within half an ulp of 1/b then rounds to RN(x / b). Zeros, values below
+// 2^-900 (whose remainders would be subnormal) and non-finite values take
+// the IEEE division.
+__device__ __forceinline__ double div_small_int(double x, double b, double y) {
+  if (!(fabs(x) >= 0x1p-900) || !(fabs(x) <= 1.7976931348623157e308)) return DIV(x, b);
+  const double q0 = MUL(x, y);
+  const double q1 = __fma_rn(__fma_rn(-q0, b, x), y, q0);
+  return __fma_rn(__fma_rn(-q1, b, x), y, q1);
+}
+// dd_div(a, dd_from(b)) for a small positive integer b, bit for bit: both
+// double quotients through div_small_int, and q1 * (b, 0) without its two
+// zero cross products (for finite q1 they add exactly +0 to the error term,
+// which only turns a -0 into +0: e1 + 0.0 does the same).
+__device__ __forceinline__ dd dd_div_small_int(dd a, double b, double y) {
+  const double q1 = div_small_int(a.hi, b, y);
+  double p1, e1;
+  two_prod(q1, b, p1, e1);
+  const dd r = dd_sub(a, dd_renorm(p1, ADD(e1, 0.0)));
+  const double q2 = div_small_int(r.hi, b, y);
+  return dd_renorm(q1, q2);
+}
 // dd.rs:106-121 (argument reduction by ln 2, Taylor series, 2^k by bit trick).
+// The Taylor loop is unrolled, so each term divides by a constant i with its
+// reciprocal folded at compile time (dd_div_small_int: the same bits as the
+// reference's division).
 __device__ __forceinline__ dd dd_exp(dd a) {
   if (a.hi == 0.0 && a.lo == 0.0) return dd_from(1.0);
   const dd LN2 = {0.6931471805599453, 2.3190468138462996e-17};  // dd.rs:40
   double k = round(DIV(a.hi, LN2.hi));
   dd r = dd_sub(a, dd_mul(dd_from(k), LN2));
   dd term = dd_from(1.0), sum = dd_from(1.0);
+#pragma unroll
   for (int i = 1; i <= 25; i++) {
-    term = dd_div(dd_mul(term, r), dd_from((double)i));
+    term = dd_div_small_int(dd_mul(term, r), (double)i, 1.0 / (double)i);
     sum = dd_add(sum, term);
     if (dd_abs(term).hi < 1e-35) break;
   }

@@ -95,3 +95,21 @@ def test_qd_ops_bitexact(shim, op, name):
     for i in range(n):
         want = O.mf_op(name, 4, a[i], b[i]) if name != "sqrt" else O.mf_op("sqrt", 4, a[i])
         assert np.array_equal(got[i], want, equal_nan=True), (name, i, a[i], b[i], got[i], want)
+
+
+def test_dd_exp_overlap_range_bitexact(shim):
+    """The assembly's exp arguments -ab/(a+b) |R-R'|^2 lie in [-700, 0]: a
+    dense sweep there (and near 0, where the Taylor loop runs longest) must
+    reproduce the reference's bits, including its small-integer divisions."""
+    rng = np.random.default_rng(2024)
+    n = 100000
+    hi = np.concatenate([-700.0 * rng.random(n // 2), -rng.random(n // 4) * 2.0 ** -rng.integers(0, 40, n // 4),
+                         (rng.random(n - n // 2 - n // 4) - 0.5)])
+    a = np.stack([hi, hi * 2.0 ** -53 * (rng.random(n) - 0.5)], -1)
+    for i in range(n):  # renormalise (quick_two_sum)
+        s = a[i, 0] + a[i, 1]
+        a[i] = [s, a[i, 1] - (s - a[i, 0])]
+    got = run(shim, 5, a, a, 2)
+    want = np.array([O.dd_exp(a[i]) for i in range(n)])
+    bad = np.nonzero(np.any(got != want, axis=1))[0]
+    assert bad.size == 0, (bad[:5], a[bad[:5]], got[bad[:5]], want[bad[:5]])
