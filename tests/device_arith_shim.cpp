@@ -63,6 +63,36 @@ void sh_qd_add(const double* a, const double* b, double* o) { stq(o, qd_add(ldq(
 void sh_qd_mul(const double* a, const double* b, double* o) { stq(o, qd_mul(ldq(a), ldq(b))); }
 void sh_qd_div(const double* a, const double* b, double* o) { stq(o, qd_div(ldq(a), ldq(b))); }
 void sh_qd_sqrt(const double* a, double* o) { stq(o, qd_sqrt(ldq(a))); }
+// div_small_int (the Taylor divisions of dd_exp) against IEEE x / i for
+// i = 1..max_divisor, per_divisor random x each (random sign, mantissa and
+// exponent in [-1000, 1000], a quarter next to exact multiples of i and a
+// quarter on halfway points); returns the number of differing bit patterns.
+long sh_div_small_mismatches(long per_divisor, int max_divisor, unsigned long long seed) {
+  auto next = [&seed]() {  // SplitMix64
+    uint64_t z = (seed += 0x9e3779b97f4a7c15ull);
+    z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+    z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+    return z ^ (z >> 31);
+  };
+  long bad = 0;
+  for (int i = 1; i <= max_divisor; i++) {
+    const double b = (double)i, y = 1.0 / b;
+    for (long t = 0; t < per_divisor; t++) {
+      const uint64_t bits = next();
+      const double m = 1.0 + (double)(bits >> 12) * 0x1p-52;
+      double x = std::ldexp(m, (int)(next() % 2001) - 1000) * ((bits & 1) ? -1.0 : 1.0);
+      if (t % 4 == 1) {
+        x = std::ldexp(1.0 + (double)(next() >> 12) * 0x1p-52, (int)(next() % 200) - 100) * b;
+        x = std::nextafter(x, (t & 2) ? INFINITY : -INFINITY);
+      } else if (t % 4 == 2) {
+        x = (std::floor(std::ldexp(1.0 + (double)(next() >> 12) * 0x1p-52, (int)(next() % 60))) + 0.5) * b;
+      }
+      const double got = div_small_int(x, b, y), want = x / b;
+      if (std::memcmp(&got, &want, 8) != 0) bad++;
+    }
+  }
+  return bad;
+}
 // Many ops at once (count entries of 2 or 4 limbs each).
 void sh_batch(int op, const double* a, const double* b, double* o, long count) {
   for (long i = 0; i < count; i++) {

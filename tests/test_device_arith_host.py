@@ -113,3 +113,12 @@ def test_dd_exp_overlap_range_bitexact(shim):
     want = np.array([O.dd_exp(a[i]) for i in range(n)])
     bad = np.nonzero(np.any(got != want, axis=1))[0]
     assert bad.size == 0, (bad[:5], a[bad[:5]], got[bad[:5]], want[bad[:5]])
+
+
+def test_div_small_int_is_correctly_rounded(shim):
+    """dd_exp divides its Taylor terms by i = 1..25 with an FMA sequence; it
+    must give IEEE division's bits: 1e6 quotients per divisor 1..40,
+    including values next to exact multiples and halfway points."""
+    shim.sh_div_small_mismatches.restype = ctypes.c_long
+    shim.sh_div_small_mismatches.argtypes = [ctypes.c_long, ctypes.c_int, ctypes.c_ulonglong]
+    assert shim.sh_div_small_mismatches(1000000, 40, 2024) == 0
