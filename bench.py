@@ -143,6 +143,35 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------- helpers
+def init_dist(backend: str = "nccl"):
+    """(world, rank, local_rank, dist or None) from the launcher's environment;
+    one process per GPU, rendezvous on MASTER_ADDR (127.0.0.1 for this
+    launcher). A short timeout makes ranks that wait for a missing peer fail."""
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world == 1:
+        return world, rank, local, None
+    import datetime
+
+    import torch.distributed as dist
+
+    dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    return world, rank, local, dist
+
+
+def max_over_ranks(x: float, dist, device) -> float:
+    """The largest of the ranks' values (times are reported as the slowest
+    rank's); x itself when running on one process."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def peaks():
     p = os.path.join(REPO, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -246,7 +275,7 @@ def gemm_more_section(hp, torch, dev, stream, sptr, world, dist):
             fn()
         e0.record(stream)
         torch.cuda.synchronize()
-        return s0.elapsed_time(e0) / steps
+        return max_over_ranks(s0.elapsed_time(e0) / steps, dist, dev)
 
     out = {}
     a, b = gemm_operands(M, N, K, seed=1, atb=True)
@@ -336,10 +365,7 @@ def spd_section(hp, torch, dev, stream, sptr, args, rank, world, dist):
             evs.append((s, e))
         torch.cuda.synchronize()
         ms = sum(a.elapsed_time(z) for a, z in evs) / args.spd_steps
-        if dist is not None:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(ms, dist, dev)
         x = dx.cpu().numpy()
         err = None
         if xs is not None:
@@ -387,11 +413,7 @@ def batched_section(hp, torch, dev, stream, sptr, args, world, dist):
         solve()
     e0.record(stream)
     torch.cuda.synchronize()
-    ms = s0.elapsed_time(e0) / steps
-    if dist is not None:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(s0.elapsed_time(e0) / steps, dist, dev)
     status = st.cpu().numpy()
     ok = int((status == 0).sum())
     out = {"workload": "4096 overlap SPD systems, n = 4*round(16*24^U/4) in [16, 384] (mean %.1f), random "
@@ -427,7 +449,7 @@ def batched_section(hp, torch, dev, stream, sptr, args, world, dist):
                                                   vec.data_ptr(), sw.data_ptr(), jst.data_ptr(), sptr))
     e1.record(stream)
     torch.cuda.synchronize()
-    jms = s1.elapsed_time(e1)
+    jms = max_over_ranks(s1.elapsed_time(e1), dist, dev)
     sweeps = sw.cpu().numpy().astype(np.float64)
     nsel = ns[sel].astype(np.float64)
     rot = float((sweeps * nsel * (nsel - 1) / 2).sum())
@@ -482,7 +504,7 @@ def adjoint_section(hp, torch, dev, stream, sptr, args, world, dist):
             one()
         e0.record(stream)
         torch.cuda.synchronize()
-        ms = s0.elapsed_time(e0) / steps
+        ms = max_over_ranks(s0.elapsed_time(e0) / steps, dist, dev)
         out[name] = {"gradients_per_s": world * 1e3 / ms, "ms_per_gradient": ms, "converged": bool(info.converged)}
     out["chosen_over_plain"] = out["chosen"]["gradients_per_s"] / out["plain"]["gradients_per_s"]
     return out
@@ -564,17 +586,8 @@ def main():
     import numpy as np
     import torch
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    world, rank, local, dist = init_dist("nccl")
     torch.cuda.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
 
     import quadprec_b200 as hp
     from quadprec_b200.workloads import gemm_operands
@@ -609,12 +622,7 @@ def main():
             evs.append((s, e))
         torch.cuda.synchronize()
         barrier()
-        ms = sum(s.elapsed_time(e) for s, e in evs) / steps
-        if dist is not None:
-            t = torch.tensor([ms], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            ms = float(t.item())
-        return ms
+        return max_over_ranks(sum(s.elapsed_time(e) for s, e in evs) / steps, dist, dev)
 
     flops = 2.0 * M * N * K
     clk = ClockSampler(local)
@@ -675,11 +683,7 @@ def main():
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
         hp.check(lib.hp_f128_gemm(ha.data_ptr(), hb.data_ptr(), hc.data_ptr(), M, N, K, hp.OZAKI))
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    if dist is not None:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, dist, dev)
 
     more = gemm_more_section(hp, torch, dev, stream, sptr, world, dist)
     spd = None if args.no_spd else spd_section(hp, torch, dev, stream, sptr, args, rank, world, dist)
@@ -710,7 +714,7 @@ def main():
                 "h2d_bytes_per_step": int(2 * M * K * 16), "d2h_bytes_per_step": int(M * N * 16),
                 "path": "hp_f128_gemm (host pointers, pinned), copies inside the timed region"},
         "roofline": roofline, "phases_ms": phase_report, "phase_roofline": phase_roofline,
-        "gpu_launches": 6 * args.steps,
+        "gpu_launches": 4 * args.steps,  # exponents, residues, tcgen05 GEMM, CRT per step
         "clocks": clocks,
     }
     if cpu is not None:
