@@ -266,26 +266,32 @@ __device__ __forceinline__ int entry_exp(double2 v) {
   const int el = exp_field(v.y);
   return el == EXP_NONFINITE ? EXP_NONFINITE : max(exp_field(v.x), min(el + 1, EXP_NONFINITE));
 }
-__global__ void __launch_bounds__(256) maxexp_kernel(const double2* __restrict__ A, int64_t RA, int64_t CA,
-                                                     bool a_rows, int* __restrict__ outA,
-                                                     const double2* __restrict__ B, int64_t RB, int64_t CB,
-                                                     int* __restrict__ outB, int64_t slab, unsigned na) {
+// f256 entries: the same from limbs 0 and 1; any non-finite limb marks the entry
+__device__ __forceinline__ int entry_exp(double4 v) {
+  const int el = exp_field(v.y);
+  if (el == EXP_NONFINITE || exp_field(v.z) == EXP_NONFINITE || exp_field(v.w) == EXP_NONFINITE) return EXP_NONFINITE;
+  return max(exp_field(v.x), min(el + 1, EXP_NONFINITE));
+}
+template <class T>
+__global__ void __launch_bounds__(256) maxexp_kernel(const T* __restrict__ A, int64_t RA, int64_t CA, bool a_rows,
+                                                     int* __restrict__ outA, const T* __restrict__ B, int64_t RB,
+                                                     int64_t CB, int* __restrict__ outB, int64_t slab, unsigned na) {
   sm100::griddep_launch_dependents();
   const bool isA = blockIdx.x < na;
   const unsigned bid = isA ? blockIdx.x : blockIdx.x - na;
-  const double2* src = isA ? A : B;
+  const T* src = isA ? A : B;
   const int64_t R = isA ? RA : RB, C = isA ? CA : CB;
   int* out = isA ? outA : outB;
   const int lane = threadIdx.x % 32, wy = threadIdx.x / 32;
   if (isA && a_rows) {
     const int64_t row = (int64_t)bid * 8 + wy;
     if (row >= R) return;
-    const double2* rp = src + row * C;
+    const T* rp = src + row * C;
     int e = 0;
     for (int64_t p = lane; p < C; p += 128) {
-      double2 v[4];
+      T v[4];
 #pragma unroll
-      for (int u = 0; u < 4; u++) v[u] = p + 32 * u < C ? rp[p + 32 * u] : make_double2(0.0, 0.0);
+      for (int u = 0; u < 4; u++) v[u] = p + 32 * u < C ? rp[p + 32 * u] : T{};
 #pragma unroll
       for (int u = 0; u < 4; u++) e = max(e, entry_exp(v[u]));
     }
@@ -300,9 +306,9 @@ __global__ void __launch_bounds__(256) maxexp_kernel(const double2* __restrict__
   int e = 0;
   if (c < C) {
     for (int64_t r = r0 + wy; r < r1; r += 32) {
-      double2 v[4];
+      T v[4];
 #pragma unroll
-      for (int u = 0; u < 4; u++) v[u] = r + 8 * u < r1 ? src[(r + 8 * u) * C + c] : make_double2(0.0, 0.0);
+      for (int u = 0; u < 4; u++) v[u] = r + 8 * u < r1 ? src[(r + 8 * u) * C + c] : T{};
 #pragma unroll
       for (int u = 0; u < 4; u++) e = max(e, entry_exp(v[u]));
     }
@@ -317,8 +323,9 @@ __global__ void __launch_bounds__(256) maxexp_kernel(const double2* __restrict__
 // Exponents of the f128 GEMM's operands: expA per row of A (per column when
 // atb, A being k x m) and expB per column of B (k x n), both zeroed by the
 // caller.
-static int launch_maxexp(const double2* A, const double2* B, size_t m, size_t n, size_t k, bool atb, int* expA,
-                         int* expB, cudaStream_t s) {
+template <class T>
+static int launch_maxexp(const T* A, const T* B, size_t m, size_t n, size_t k, bool atb, int* expA, int* expB,
+                         cudaStream_t s) {
   const int64_t slab = 256;
   const int64_t kslabs = ((int64_t)k + slab - 1) / slab;
   const int64_t na = atb ? ((int64_t)m + 31) / 32 * kslabs : ((int64_t)m + 7) / 8;
@@ -327,7 +334,7 @@ static int launch_maxexp(const double2* A, const double2* B, size_t m, size_t n,
     set_error("ozaki: exponent pass grid too large");
     return HP_ERR_INVALID_ARG;
   }
-  maxexp_kernel<<<(unsigned)(na + nb), 256, 0, s>>>(A, atb ? (int64_t)k : (int64_t)m, atb ? (int64_t)m : (int64_t)k,
+  maxexp_kernel<T><<<(unsigned)(na + nb), 256, 0, s>>>(A, atb ? (int64_t)k : (int64_t)m, atb ? (int64_t)m : (int64_t)k,
                                                     !atb, expA, B, (int64_t)k, (int64_t)n, expB, slab, (unsigned)na);
   HP_LAUNCH_CHECK();
   return HP_OK;
@@ -1057,30 +1064,32 @@ __device__ __forceinline__ uint32_t balanced_byte21(const int32_t* D, const int*
 // Operand residues for the f256 GEMM. Element (r, p) is src[r*K + p]
 // (P_CONTIG) or src[p*R + r], 4 limbs. Writes hi digits at byte offset
 // hi_off and lo digits at lo_off of each 2*Kp-byte row, planes of Rp rows.
-template <bool P_CONTIG>
-__global__ void __launch_bounds__(256) residue_qd_kernel(const double4* __restrict__ src, int64_t R, int64_t K,
-                                                         const int* __restrict__ expf, int L, int64_t Rp, int64_t Kp,
-                                                         int64_t hi_off, int64_t lo_off, int8_t* __restrict__ out) {
-  __shared__ int w21[MAXL][5];
-  for (int q = threadIdx.x; q < L * 5; q += blockDim.x) {
-    const int l = q / 5, c = q % 5;
-    const int m = c_tab.mod[l];
-    int64_t r = 1;
-    for (int t = 0; t < 21 * c; t++) r = (r * 2) % m;
-    int b = (int)r;
-    if (b > m / 2) b -= m;
-    w21[l][c] = b;
-  }
-  __shared__ __align__(16) uint32_t T[2][2][RT_R][RT_P / 4 + 1];
-  __syncthreads();
+// residue of a 5-digit (base 2^21) number in [0, m) (w[0] = 2^0 mod m = 1)
+__device__ __forceinline__ uint32_t unsigned_byte21(const int32_t* D, const int* w, int l) {
+  int32_t x = D[0];
+#pragma unroll
+  for (int c = 1; c < 5; c++) x += D[c] * w[c];
+  return mod_reduce(x, l);
+}
+
+// One RT_R x (4 EPR) tile (block coordinates bx, by) of the f256 residue
+// rows [Xh | Xl]: EPR entries per thread (8 or 4), all L moduli, residues
+// balanced (signed bytes) or, with U8, in [0, m).
+template <bool P_CONTIG, int EPR, bool U8>
+__device__ __forceinline__ void residue_qd_tile(const double4* __restrict__ src, int64_t R, int64_t K,
+                                                const int* __restrict__ expf, int L, int64_t Rp, int64_t Kp,
+                                                int64_t hi_off, int64_t lo_off, int8_t* __restrict__ out,
+                                                unsigned bx, unsigned by, const int (*w21)[5]) {
+  constexpr int NW = EPR / 4;  // 32-bit words per half per thread
+  __shared__ __align__(16) uint32_t T[2][2][RT_R][EPR + 1];
   const int t = threadIdx.x;
   const int rl = P_CONTIG ? t / 4 : t % 64;
-  const int oct = P_CONTIG ? t % 4 : t / 64;
-  const int64_t r = (int64_t)blockIdx.y * RT_R + rl;
-  const int64_t p0 = (int64_t)blockIdx.x * RT_P + 8 * oct;
-  int32_t dig[8][10];
+  const int quad = P_CONTIG ? t % 4 : t / 64;
+  const int64_t r = (int64_t)by * RT_R + rl;
+  const int64_t p0 = (int64_t)bx * (4 * EPR) + EPR * quad;
+  int32_t dig[EPR][10];
 #pragma unroll
-  for (int e = 0; e < 8; e++)
+  for (int e = 0; e < EPR; e++)
 #pragma unroll
     for (int c = 0; c < 10; c++) dig[e][c] = 0;
   if (r < R) {
@@ -1088,7 +1097,7 @@ __global__ void __launch_bounds__(256) residue_qd_kernel(const double4* __restri
     if (ex != EXP_NONFINITE) {
       const int sh = BETA_QD + 1022 - ex;
 #pragma unroll
-      for (int e = 0; e < 8; e++) {
+      for (int e = 0; e < EPR; e++) {
         const int64_t p = p0 + e;
         if (p < K) {
           const double4 v = P_CONTIG ? src[r * K + p] : src[p * R + r];
@@ -1110,35 +1119,75 @@ __global__ void __launch_bounds__(256) residue_qd_kernel(const double4* __restri
       }
     }
   }
-  int8_t* const base = out + (size_t)(blockIdx.y * RT_R) * (2 * Kp) + blockIdx.x * RT_P;
+  int8_t* const base = out + (size_t)by * RT_R * (2 * Kp) + (size_t)bx * (4 * EPR);
   for (int l = 0; l < L; l++) {
     const int m = c_tab.mod[l];
-    uint32_t wh0 = 0, wh1 = 0, wl0 = 0, wl1 = 0;
+    uint32_t wh[NW], wl[NW];
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-      wl0 |= balanced_byte21(dig[e], w21[l], l, m) << (8 * e);
-      wl1 |= balanced_byte21(dig[e + 4], w21[l], l, m) << (8 * e);
-      wh0 |= balanced_byte21(dig[e] + 5, w21[l], l, m) << (8 * e);
-      wh1 |= balanced_byte21(dig[e + 4] + 5, w21[l], l, m) << (8 * e);
+    for (int q = 0; q < NW; q++) {
+      wh[q] = wl[q] = 0;
+#pragma unroll
+      for (int e = 0; e < 4; e++) {
+        const int32_t* dl = dig[4 * q + e];
+        const uint32_t bl = U8 ? unsigned_byte21(dl, w21[l], l) : balanced_byte21(dl, w21[l], l, m);
+        const uint32_t bh = U8 ? unsigned_byte21(dl + 5, w21[l], l) : balanced_byte21(dl + 5, w21[l], l, m);
+        wl[q] |= bl << (8 * e);
+        wh[q] |= bh << (8 * e);
+      }
     }
     int8_t* plane = base + (size_t)l * Rp * (2 * Kp);
     if (P_CONTIG) {
-      *reinterpret_cast<uint2*>(plane + (size_t)rl * (2 * Kp) + hi_off + 8 * oct) = make_uint2(wh0, wh1);
-      *reinterpret_cast<uint2*>(plane + (size_t)rl * (2 * Kp) + lo_off + 8 * oct) = make_uint2(wl0, wl1);
+      int8_t* row = plane + (size_t)rl * (2 * Kp) + EPR * quad;
+      if (NW == 2) {
+        *reinterpret_cast<uint2*>(row + hi_off) = make_uint2(wh[0], wh[NW - 1]);
+        *reinterpret_cast<uint2*>(row + lo_off) = make_uint2(wl[0], wl[NW - 1]);
+      } else {
+        *reinterpret_cast<uint32_t*>(row + hi_off) = wh[0];
+        *reinterpret_cast<uint32_t*>(row + lo_off) = wl[0];
+      }
     } else {
-      T[l & 1][0][rl][2 * oct] = wh0;
-      T[l & 1][0][rl][2 * oct + 1] = wh1;
-      T[l & 1][1][rl][2 * oct] = wl0;
-      T[l & 1][1][rl][2 * oct + 1] = wl1;
+#pragma unroll
+      for (int q = 0; q < NW; q++) {
+        T[l & 1][0][rl][NW * quad + q] = wh[q];
+        T[l & 1][1][rl][NW * quad + q] = wl[q];
+      }
       __syncthreads();
-      {
-        const int row = t / 4, part = (t % 4) / 2, half = t % 2;
+      if (t < RT_R * 2 * NW) {
+        const int row = t / (2 * NW), rem = t % (2 * NW), part = rem / NW, half = rem % NW;
         const uint32_t* sw = &T[l & 1][part][row][4 * half];
         *reinterpret_cast<uint4*>(plane + (size_t)row * (2 * Kp) + (part ? lo_off : hi_off) + 16 * half) =
             make_uint4(sw[0], sw[1], sw[2], sw[3]);
       }
     }
   }
+}
+
+// Both f256 operands' residues in one launch: block rows [0, tiles_ay) cover
+// A (row-contiguous when A_CONTIG; halves at hi 0, lo Kp), the rest B
+// (transposed; halves at hi Kp, lo 0).
+template <bool A_CONTIG, int EPR, bool U8>
+__global__ void __launch_bounds__(256, 3) residue_qd_ab_kernel(const double4* __restrict__ A, int64_t RA, int64_t RpA,
+                                                            const int* __restrict__ expA, int8_t* __restrict__ outA,
+                                                            unsigned tiles_ay, const double4* __restrict__ B,
+                                                            int64_t RB, int64_t RpB, const int* __restrict__ expB,
+                                                            int8_t* __restrict__ outB, int64_t K, int64_t Kp, int L) {
+  __shared__ int w21[MAXL][5];  // 2^(21 c) mod m, balanced
+  for (int q = threadIdx.x; q < L * 5; q += blockDim.x) {
+    const int l = q / 5, c = q % 5;
+    const int m = c_tab.mod[l];
+    int64_t rr = 1;
+    for (int t = 0; t < 21 * c; t++) rr = (rr * 2) % m;
+    int b = (int)rr;
+    if (b > m / 2) b -= m;
+    w21[l][c] = b;
+  }
+  sm100::griddep_launch_dependents();
+  sm100::griddep_wait();  // the exponents come from the preceding pass
+  __syncthreads();
+  if (blockIdx.y < tiles_ay)
+    residue_qd_tile<A_CONTIG, EPR, U8>(A, RA, K, expA, L, RpA, Kp, 0, Kp, outA, blockIdx.x, blockIdx.y, w21);
+  else
+    residue_qd_tile<false, EPR, U8>(B, RB, K, expB, L, RpB, Kp, Kp, 0, outB, blockIdx.x, blockIdx.y - tiles_ay, w21);
 }
 
 // f256 CRT: rebuild G1 and G2, C = (G1 2^105 + G2) 2^(105 - sa - sb).
@@ -1189,6 +1238,8 @@ __global__ void __launch_bounds__(256) crt_qd_kernel(const uint8_t* __restrict__
   const int L = tab->L;
   for (int i = threadIdx.x; i < L * NC; i += blockDim.x) w_s[i / NC][i % NC] = tab->w[i / NC][i % NC];
   if (threadIdx.x < NC) mch_s[threadIdx.x] = tab->mchunk[threadIdx.x];
+  sm100::griddep_launch_dependents();
+  sm100::griddep_wait();  // the product residues come from the preceding GEMM
   __syncthreads();
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= m * n) return;
@@ -1211,42 +1262,6 @@ __global__ void __launch_bounds__(256) crt_qd_kernel(const uint8_t* __restrict__
                         scale_pow2(c.l[3], shift));
 }
 
-// exponent scans over f256 rows / columns (limb 0 and 1 as in the f128 scan)
-__global__ void maxexp_rows_qd_kernel(const double4* __restrict__ src, int64_t R, int64_t C, int* __restrict__ out) {
-  int64_t row = (int64_t)blockIdx.x * (blockDim.x / 32) + threadIdx.x / 32;
-  int lane = threadIdx.x % 32;
-  if (row >= R) return;
-  int e = 0;
-  for (int64_t p = lane; p < C; p += 32) {
-    double4 v = src[row * C + p];
-    e = max(e, max(exp_field(v.x), min(exp_field(v.y) + 1, EXP_NONFINITE)));
-    if (exp_field(v.y) == EXP_NONFINITE || exp_field(v.z) == EXP_NONFINITE || exp_field(v.w) == EXP_NONFINITE)
-      e = EXP_NONFINITE;
-  }
-  for (int o = 16; o; o >>= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, o));
-  if (lane == 0) out[row] = e;
-}
-__global__ void maxexp_cols_qd_kernel(const double4* __restrict__ src, int64_t R, int64_t C, int64_t slab,
-                                      int* __restrict__ out) {
-  __shared__ int red[8][33];
-  int64_t c = (int64_t)blockIdx.x * 32 + threadIdx.x;
-  int64_t r0 = (int64_t)blockIdx.y * slab, r1 = min(R, r0 + slab);
-  int e = 0;
-  if (c < C) {
-    for (int64_t r = r0 + threadIdx.y; r < r1; r += 8) {
-      double4 v = src[r * C + c];
-      e = max(e, max(exp_field(v.x), min(exp_field(v.y) + 1, EXP_NONFINITE)));
-      if (exp_field(v.y) == EXP_NONFINITE || exp_field(v.z) == EXP_NONFINITE || exp_field(v.w) == EXP_NONFINITE)
-        e = EXP_NONFINITE;
-    }
-  }
-  red[threadIdx.y][threadIdx.x] = e;
-  __syncthreads();
-  if (threadIdx.y == 0 && c < C) {
-    for (int y = 1; y < 8; y++) e = max(e, red[y][threadIdx.x]);
-    atomicMax(out + c, e);
-  }
-}
 }  // namespace ozaki
 
 int ozaki_qd_gemm(const double* a, const double* b, double* c, size_t m, size_t n, size_t k, bool atb,
@@ -1266,52 +1281,45 @@ int ozaki_qd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
     return HP_ERR_UNSUPPORTED;
   }
   const size_t Mp = round_up(m, GB_M), Np = round_up(n, GB_N), Kp = round_up(k, GB_K);
-  DevBuf expA(Mp * sizeof(int), s), expB(Np * sizeof(int), s);
+  DevBuf exps((Mp + Np) * sizeof(int), s);
   DevBuf ares((size_t)L * Mp * 2 * Kp, s), bres((size_t)L * Np * 2 * Kp, s);
   DevBuf g1((size_t)L * Mp * Np, s), g2((size_t)L * Mp * Np, s);
-  if (!expA.p || !expB.p || !ares.p || !bres.p || !g1.p || !g2.p) {
+  if (!exps.p || !ares.p || !bres.p || !g1.p || !g2.p) {
     set_error("ozaki f256: workspace allocation failed");
     return HP_ERR_CUDA;
   }
-  HP_CUDA_TRY(cudaMemsetAsync(expA.p, 0, Mp * sizeof(int), s));
-  HP_CUDA_TRY(cudaMemsetAsync(expB.p, 0, Np * sizeof(int), s));
+  int* expAp = exps.as<int>();  // A's row (or column) exponents, then B's column exponents
+  int* expBp = expAp + Mp;
+  HP_CUDA_TRY(cudaMemsetAsync(exps.p, 0, (Mp + Np) * sizeof(int), s));
   const double4* A4 = reinterpret_cast<const double4*>(a);
   const double4* B4 = reinterpret_cast<const double4*>(b);
-  if (!atb) {
-    maxexp_rows_qd_kernel<<<(unsigned)((m + 7) / 8), 256, 0, s>>>(A4, m, k, expA.as<int>());
-  } else {
-    dim3 g((unsigned)((m + 31) / 32), (unsigned)((k + 255) / 256));
-    maxexp_cols_qd_kernel<<<g, dim3(32, 8), 0, s>>>(A4, k, m, 256, expA.as<int>());
-  }
-  HP_LAUNCH_CHECK();
-  {
-    dim3 g((unsigned)((n + 31) / 32), (unsigned)((k + 255) / 256));
-    maxexp_cols_qd_kernel<<<g, dim3(32, 8), 0, s>>>(B4, k, n, 256, expB.as<int>());
-    HP_LAUNCH_CHECK();
-  }
-  {
-    dim3 ga((unsigned)(Kp / RT_P), (unsigned)(Mp / RT_R));
+  HP_TRY(launch_maxexp(A4, B4, m, n, k, atb, expAp, expBp, s));
+  {  // residues of both operands as unsigned bytes, 4 entries per thread
+    const unsigned tay = (unsigned)(Mp / RT_R);
+    dim3 g((unsigned)(Kp / 16), tay + (unsigned)(Np / RT_R));
     if (!atb)
-      residue_qd_kernel<true><<<ga, 256, 0, s>>>(A4, m, k, expA.as<int>(), L, Mp, Kp, 0, Kp, ares.as<int8_t>());
+      HP_CUDA_TRY(launch_k(true, residue_qd_ab_kernel<true, 4, true>, g, dim3(256), 0, s, A4, (int64_t)m, (int64_t)Mp,
+                           (const int*)expAp, ares.as<int8_t>(), tay, B4, (int64_t)n, (int64_t)Np,
+                           (const int*)expBp, bres.as<int8_t>(), (int64_t)k, (int64_t)Kp, L));
     else
-      residue_qd_kernel<false><<<ga, 256, 0, s>>>(A4, m, k, expA.as<int>(), L, Mp, Kp, 0, Kp, ares.as<int8_t>());
-    HP_LAUNCH_CHECK();
-    dim3 gb((unsigned)(Kp / RT_P), (unsigned)(Np / RT_R));
-    residue_qd_kernel<false><<<gb, 256, 0, s>>>(B4, n, k, expB.as<int>(), L, Np, Kp, Kp, 0, bres.as<int8_t>());
-    HP_LAUNCH_CHECK();
+      HP_CUDA_TRY(launch_k(true, residue_qd_ab_kernel<false, 4, true>, g, dim3(256), 0, s, A4, (int64_t)m, (int64_t)Mp,
+                           (const int*)expAp, ares.as<int8_t>(), tay, B4, (int64_t)n, (int64_t)Np,
+                           (const int*)expBp, bres.as<int8_t>(), (int64_t)k, (int64_t)Kp, L));
   }
   // G1 = Xh Yh: A bytes [0, Kp), B bytes [Kp, 2Kp)
   HP_TRY(ozaki_residue_gemm_k(ares.as<int8_t>(), bres.as<int8_t>(), g1.as<uint8_t>(), L, Mp, Np, 2 * Kp, 2 * Kp, 0, Kp,
-                              Kp, Np, Mp * Np, 0, 0, 0, s, Mp, Np));
+                              Kp, Np, Mp * Np, 0, 0, 0, s, Mp, Np, true, true));
   // G2 = [Xh | Xl] [Yl ; Yh]: both over [0, 2Kp)
   HP_TRY(ozaki_residue_gemm_k(ares.as<int8_t>(), bres.as<int8_t>(), g2.as<uint8_t>(), L, Mp, Np, 2 * Kp, 2 * Kp, 0,
-                              2 * Kp, 0, Np, Mp * Np, 0, 0, 0, s, Mp, Np));
+                              2 * Kp, 0, Np, Mp * Np, 0, 0, 0, s, Mp, Np, false, true));
   const int nc = host_tables().crt[L].nc;
   const unsigned grid = (unsigned)((m * n + 255) / 256);
 #define HP_CRTQ(NC)                                                                                                  \
   case NC:                                                                                                           \
-    crt_qd_kernel<NC><<<grid, 256, 0, s>>>(g1.as<uint8_t>(), g2.as<uint8_t>(), (int64_t)(Mp * Np), (int64_t)Np, m, n, \
-                                           expA.as<int>(), expB.as<int>(), D->crt + L, reinterpret_cast<double4*>(c)); \
+    HP_CUDA_TRY(launch_k(true, crt_qd_kernel<NC>, dim3(grid), dim3(256), 0, s, (const uint8_t*)g1.as<uint8_t>(),     \
+                         (const uint8_t*)g2.as<uint8_t>(), (int64_t)(Mp * Np), (int64_t)Np, (int64_t)m, (int64_t)n,  \
+                         (const int*)expAp, (const int*)expBp, (const CrtTable*)(D->crt + L),               \
+                         reinterpret_cast<double4*>(c)));                                                            \
     break;
   switch (nc) {
     HP_CRTQ(5) HP_CRTQ(6) HP_CRTQ(7) HP_CRTQ(8)
@@ -1320,7 +1328,6 @@ int ozaki_qd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
       return HP_ERR_UNSUPPORTED;
   }
 #undef HP_CRTQ
-  HP_LAUNCH_CHECK();
   return HP_OK;
 }
 
