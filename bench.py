@@ -663,7 +663,9 @@ def main():
                 "30 moduli)", "achieved": i8_tops, "peak": i8_peak, "unit": "TOPS (int8)",
                 "frac": i8_tops / i8_peak, "traffic": I8_GEMM_TRAFFIC_BYTES,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch at 2048^3",
-                "peak_source": f"2 x {peak_kind} dense bf16 ({bf16_tf} TFLOP/s) in MEASURED_PEAKS.json",
+                "peak_source": (f"2 x measured dense bf16 ({bf16_tf} TFLOP/s, MEASURED_PEAKS.json)"
+                                if peak_kind == "measured" else
+                                f"2 x fallback dense bf16 ({bf16_tf} TFLOP/s; MEASURED_PEAKS.json absent)"),
                 "algorithmic": f"{L} moduli x 2mnk int8 ops = {L * 2.0 * M * N * K:.3e} per launch"}
     phase_report = {k: round(v, 4) for k, v in phases.items()}
     phase_roofline = {

@@ -82,6 +82,12 @@ struct CrtTable {
   double inv_m;           // 1 / M (rounded)
 };
 
+// CRT tables of the moduli counts the f128 GEMM uses (k <= 2^20 at beta =
+// 106), in constant memory so that the specialised CRT kernel's weights
+// are immediate operands of its multiply-adds.
+constexpr int CRT_CONST_L0 = 28, CRT_CONST_N = 5;
+__constant__ CrtTable c_crt[CRT_CONST_N];  // L = CRT_CONST_L0 + i
+
 // ---------------------------------------------------------------------------
 // Host tables
 // ---------------------------------------------------------------------------
@@ -219,6 +225,7 @@ static int device_tables(DevTables** out) {
   if (!D.ready) {
     const HostTables& T = host_tables();
     HP_CUDA_TRY(cudaMemcpyToSymbol(c_tab, &T.mt, sizeof(ModTable)));
+    HP_CUDA_TRY(cudaMemcpyToSymbol(c_crt, &T.crt[CRT_CONST_L0], sizeof(CrtTable) * CRT_CONST_N));
     HP_CUDA_TRY(cudaMalloc(&D.crt, sizeof(CrtTable) * (MAXL + 1)));
     HP_CUDA_TRY(cudaMemcpy(D.crt, T.crt.data(), sizeof(CrtTable) * (MAXL + 1), cudaMemcpyHostToDevice));
     HP_CUDA_TRY(cudaDeviceGetAttribute(&D.num_sms, cudaDevAttrMultiProcessorCount, d));
@@ -402,7 +409,10 @@ __device__ __forceinline__ uint32_t unsigned_byte(const int32_t* D, int l) {
   for (int c = 1; c < NDIG; c++) x += D[c] * c_tab.pw[l][c];
   return mod_reduce(x, l);
 }
-template <bool P_CONTIG, int EPR, bool U8>
+// LC > 0: the number of moduli is the compile-time LC (== L), the moduli
+// loop is unrolled (each modulus' constants are immediate operands) and the
+// transposed tile keeps all LC planes in shared memory until one barrier.
+template <bool P_CONTIG, int EPR, bool U8, int LC = 0>
 __device__ __forceinline__ void residue_tile(const double2* __restrict__ src, int64_t R, int64_t K,
                                              const int* __restrict__ expf, int beta, int L, int64_t ld,
                                              int64_t plane_stride, int8_t* __restrict__ out, unsigned bx,
@@ -439,6 +449,44 @@ __device__ __forceinline__ void residue_tile(const double2* __restrict__ src, in
     }
   }
   int8_t* const base = out + (size_t)by * RT_R * ld + (size_t)bx * (4 * EPR);
+  if constexpr (LC > 0) {
+    constexpr int TROWS = P_CONTIG ? 1 : RT_R;
+    __shared__ uint32_t TT[P_CONTIG ? 1 : LC][TROWS][EPR + 1];
+#pragma unroll
+    for (int l = 0; l < LC; l++) {
+      uint32_t w[NW];
+#pragma unroll
+      for (int q = 0; q < NW; q++) {
+        w[q] = 0;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const uint32_t byte =
+              U8 ? unsigned_byte(dig[4 * q + e], l) : balanced_byte(dig[4 * q + e], l, c_tab.mod[l]);
+          w[q] |= byte << (8 * e);
+        }
+      }
+      if constexpr (P_CONTIG) {
+        int8_t* dst = base + (size_t)l * plane_stride + (size_t)rl * ld + EPR * quad;
+        if (NW == 2)
+          *reinterpret_cast<uint2*>(dst) = make_uint2(w[0], w[NW - 1]);
+        else
+          *reinterpret_cast<uint32_t*>(dst) = w[0];
+      } else {
+#pragma unroll
+        for (int q = 0; q < NW; q++) TT[l][rl][NW * quad + q] = w[q];
+      }
+    }
+    if constexpr (!P_CONTIG) {
+      __syncthreads();
+      for (int u = t; u < LC * RT_R * NW; u += blockDim.x) {
+        const int l = u / (RT_R * NW), rem = u % (RT_R * NW), row = rem / NW, half = rem % NW;
+        const uint32_t* sw = &TT[l][row][4 * half];
+        *reinterpret_cast<uint4*>(base + (size_t)l * plane_stride + (size_t)row * ld + 16 * half) =
+            make_uint4(sw[0], sw[1], sw[2], sw[3]);
+      }
+    }
+    return;
+  }
   int it = 0;
   for (int l = 0; l < L; l++, it++) {
     const int m = c_tab.mod[l];
@@ -474,7 +522,7 @@ __device__ __forceinline__ void residue_tile(const double2* __restrict__ src, in
 
 // Residues of both operands of the f128 Ozaki GEMM in one launch: block
 // rows [0, tiles_ay) cover A (row-contiguous when A_CONTIG), the rest B.
-template <bool A_CONTIG, int EPR, bool U8>
+template <bool A_CONTIG, int EPR, bool U8, int LC = 0>
 __global__ void __launch_bounds__(256) residue_ab_kernel(const double2* __restrict__ A, int64_t RA,
                                                          const int* __restrict__ expA, int8_t* __restrict__ outA,
                                                          int64_t planeA, unsigned tiles_ay,
@@ -482,9 +530,9 @@ __global__ void __launch_bounds__(256) residue_ab_kernel(const double2* __restri
                                                          const int* __restrict__ expB, int8_t* __restrict__ outB,
                                                          int64_t planeB, int64_t K, int beta, int L, int64_t ld) {
   if (blockIdx.y < tiles_ay)
-    residue_tile<A_CONTIG, EPR, U8>(A, RA, K, expA, beta, L, ld, planeA, outA, blockIdx.x, blockIdx.y);
+    residue_tile<A_CONTIG, EPR, U8, LC>(A, RA, K, expA, beta, L, ld, planeA, outA, blockIdx.x, blockIdx.y);
   else
-    residue_tile<false, EPR, U8>(B, RB, K, expB, beta, L, ld, planeB, outB, blockIdx.x, blockIdx.y - tiles_ay);
+    residue_tile<false, EPR, U8, LC>(B, RB, K, expB, beta, L, ld, planeB, outB, blockIdx.x, blockIdx.y - tiles_ay);
 }
 
 // ---------------------------------------------------------------------------
@@ -722,9 +770,13 @@ __device__ __forceinline__ void carry_normalise(double* acc) {
     acc[c + 1] = __dadd_rn(acc[c + 1], carry);
   }
 }
+// acc[0..NC) hold the weighted residue sums, each an exact integer in
+// [0, 2^52) (L * 255 * 2^39 with L <= 32), acc[NC] = 0. The quotient
+// estimate needs only the top two chunks (the lower ones move X / M by less
+// than 2^-26); q < 2^13, so acc[c] - q mch[c] stays exact and every carry
+// below fits as well.
 template <int NC>
 __device__ __forceinline__ dd crt_finish(double* acc, const double* mch, double inv_m, bool* neg_out) {
-  carry_normalise<NC>(acc);
   // q = round(X / M): the true value is X - qM with |X - qM| <= M/4
   double xa = __fma_rn(acc[NC], 0x1p39, acc[NC - 1]);
   xa = __fma_rn(xa, 0x1p39, acc[NC - 2]);
@@ -753,20 +805,27 @@ __device__ __forceinline__ dd crt_finish(double* acc, const double* mch, double 
 // EPT consecutive entries of a row per thread (one 2- or 4-byte load per
 // modulus); fewer entries per thread hold fewer accumulators, so more warps
 // fit on an SM. The per-entry arithmetic does not depend on EPT.
-template <int NC, int EPT>
+// LC > 0: L == LC at compile time, the tables come from c_crt (weights as
+// immediate operands) and the moduli loop is unrolled.
+template <int NC, int EPT, int LC = 0>
 __global__ void __launch_bounds__(256) crt_dd_kernel(const uint8_t* __restrict__ cres, int64_t plane, int64_t Np,
                                                      int64_t m, int64_t n, const int* __restrict__ expA,
                                                      const int* __restrict__ expB, int beta,
                                                      const CrtTable* __restrict__ tab, double2* __restrict__ C) {
-  __shared__ double w_s[MAXL][NC];
-  __shared__ double mch_s[NC];
-  const int L = tab->L;
-  for (int i = threadIdx.x; i < L * NC; i += blockDim.x) w_s[i / NC][i % NC] = tab->w[i / NC][i % NC];
-  if (threadIdx.x < NC) mch_s[threadIdx.x] = tab->mchunk[threadIdx.x];
+  __shared__ double w_sm[LC > 0 ? 1 : MAXL][NC];
+  __shared__ double mch_sm[NC];
+  const int L = LC > 0 ? LC : tab->L;
+  if constexpr (LC == 0) {
+    for (int i = threadIdx.x; i < L * NC; i += blockDim.x) w_sm[i / NC][i % NC] = tab->w[i / NC][i % NC];
+    if (threadIdx.x < NC) mch_sm[threadIdx.x] = tab->mchunk[threadIdx.x];
+  }
+  const double(*w_s)[NCMAX] = LC > 0 ? c_crt[LC > 0 ? LC - CRT_CONST_L0 : 0].w : nullptr;
+  const double(*w_d)[NC] = w_sm;
+  const double* mch_s = LC > 0 ? c_crt[LC > 0 ? LC - CRT_CONST_L0 : 0].mchunk : mch_sm;
   sm100::griddep_launch_dependents();
   sm100::griddep_wait();  // the product residues come from the preceding GEMM
-  __syncthreads();
-  const double inv_m = tab->inv_m;
+  if constexpr (LC == 0) __syncthreads();
+  const double inv_m = LC > 0 ? c_crt[LC > 0 ? LC - CRT_CONST_L0 : 0].inv_m : tab->inv_m;
   const int64_t qpr = (n + EPT - 1) / EPT;  // EPT-entry groups per row
   const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (g >= m * qpr) return;
@@ -780,6 +839,7 @@ __global__ void __launch_bounds__(256) crt_dd_kernel(const uint8_t* __restrict__
   const uint8_t* rp = cres + (size_t)i * Np + j0;
   // Issue the residue loads of 8 moduli back to back, then consume them, so
   // each thread waits for memory once per 8 moduli rather than once each.
+#pragma unroll(LC > 0 ? 8 : 1)
   for (int l0 = 0; l0 < L; l0 += 8) {
     uint32_t v[8];
 #pragma unroll
@@ -795,7 +855,8 @@ __global__ void __launch_bounds__(256) crt_dd_kernel(const uint8_t* __restrict__
       for (int e = 0; e < EPT; e++) {
         const double r = byte_to_double((v[u] >> (8 * e)) & 0xFFu);
 #pragma unroll
-        for (int c = 0; c < NC; c++) acc[e][c] = __fma_rn(r, w_s[l0 + u][c], acc[e][c]);
+        for (int c = 0; c < NC; c++)
+          acc[e][c] = __fma_rn(r, LC > 0 ? w_s[l0 + u][c] : w_d[l0 + u][c], acc[e][c]);
       }
     }
   }
@@ -862,9 +923,18 @@ constexpr int RES_EPR = 4;  // entries per thread of the f128 GEMM's residue ker
 constexpr int CRT_EPT = 2;  // entries per thread of crt_dd_kernel (measured best of 1, 2, 4)
 static int launch_crt_dd(const uint8_t* cres, size_t Mp, size_t Np, size_t m, size_t n, const int* expA,
                          const int* expB, int beta, const CrtTable* tab, int nc, double2* C, cudaStream_t s,
-                         bool pdl = false) {
+                         bool pdl = false, int L = 0) {
   const int64_t groups = (int64_t)m * (int64_t)((n + CRT_EPT - 1) / CRT_EPT);
   const unsigned grid = (unsigned)((groups + 255) / 256);
+#define HP_CRT_LC(LCV, NCV)                                                                                   \
+  if (L == LCV && nc == NCV) {                                                                                \
+    HP_CUDA_TRY(launch_k(pdl, crt_dd_kernel<NCV, CRT_EPT, LCV>, dim3(grid), dim3(256), 0, s, cres,            \
+                         (int64_t)(Mp * Np), (int64_t)Np, (int64_t)m, (int64_t)n, expA, expB, beta, tab, C)); \
+    return HP_OK;                                                                                             \
+  }
+  HP_CRT_LC(28, 6) HP_CRT_LC(28, 7) HP_CRT_LC(29, 6) HP_CRT_LC(29, 7) HP_CRT_LC(30, 6) HP_CRT_LC(30, 7)
+  HP_CRT_LC(31, 6) HP_CRT_LC(31, 7) HP_CRT_LC(32, 6) HP_CRT_LC(32, 7)
+#undef HP_CRT_LC
 #define HP_CRT_CASE(NC)                                                                                       \
   case NC:                                                                                                    \
     HP_CUDA_TRY(launch_k(pdl, crt_dd_kernel<NC, CRT_EPT>, dim3(grid), dim3(256), 0, s, cres, (int64_t)(Mp * Np), \
@@ -959,6 +1029,49 @@ int ozaki_residue_gemm_k(const int8_t* ares, const int8_t* bres, uint8_t* cres, 
   return HP_OK;
 }
 
+namespace {
+// The f128 GEMM's residue launch, specialised on the moduli count for the
+// counts k <= 2^20 needs (28-32 at beta = 106; others take the runtime loop).
+template <bool A_CONTIG, int LC>
+cudaError_t launch_residues_lc(bool pdl, dim3 g, cudaStream_t s, const double2* A, int64_t RA, const int* expA,
+                               int8_t* outA, int64_t planeA, unsigned tay, const double2* B, int64_t RB,
+                               const int* expB, int8_t* outB, int64_t planeB, int64_t K, int beta, int L,
+                               int64_t ld) {
+  return launch_k(pdl, ozaki::residue_ab_kernel<A_CONTIG, ozaki::RES_EPR, true, LC>, g, dim3(256), 0, s, A, RA, expA,
+                  outA, planeA, tay, B, RB, expB, outB, planeB, K, beta, L, ld);
+}
+template <bool A_CONTIG>
+cudaError_t launch_residues_l(int L, bool pdl, dim3 g, cudaStream_t s, const double2* A, int64_t RA,
+                              const int* expA, int8_t* outA, int64_t planeA, unsigned tay, const double2* B,
+                              int64_t RB, const int* expB, int8_t* outB, int64_t planeB, int64_t K, int beta,
+                              int64_t ld) {
+#define HP_RES_CASE(N)                                                                                           \
+  case N:                                                                                                         \
+    return launch_residues_lc<A_CONTIG, N>(pdl, g, s, A, RA, expA, outA, planeA, tay, B, RB, expB, outB, planeB, \
+                                           K, beta, L, ld);
+  switch (L) {
+    HP_RES_CASE(28)
+    HP_RES_CASE(29)
+    HP_RES_CASE(30)
+    HP_RES_CASE(31)
+    HP_RES_CASE(32)
+    default:
+      return launch_residues_lc<A_CONTIG, 0>(pdl, g, s, A, RA, expA, outA, planeA, tay, B, RB, expB, outB, planeB,
+                                             K, beta, L, ld);
+  }
+#undef HP_RES_CASE
+}
+cudaError_t launch_residues_ab(bool atb, int L, bool pdl, dim3 g, cudaStream_t s, const double2* A, int64_t RA,
+                               const int* expA, int8_t* outA, int64_t planeA, unsigned tay, const double2* B,
+                               int64_t RB, const int* expB, int8_t* outB, int64_t planeB, int64_t K, int beta,
+                               int64_t ld) {
+  return atb ? launch_residues_l<false>(L, pdl, g, s, A, RA, expA, outA, planeA, tay, B, RB, expB, outB, planeB, K,
+                                        beta, ld)
+             : launch_residues_l<true>(L, pdl, g, s, A, RA, expA, outA, planeA, tay, B, RB, expB, outB, planeB, K,
+                                       beta, ld);
+}
+}  // namespace
+
 int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t n, size_t k, bool atb,
                   cudaStream_t s) {
   using namespace ozaki;
@@ -1002,14 +1115,9 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
   {
     const unsigned tay = (unsigned)(Mp / RT_R);
     dim3 g((unsigned)(Kp / (4 * RES_EPR)), tay + (unsigned)(Np / RT_R));
-    if (!atb)
-      HP_CUDA_TRY(launch_k(pdl, residue_ab_kernel<true, RES_EPR, true>, g, dim3(256), 0, s, A2, (int64_t)m, (const int*)expA,
-                           ares.as<int8_t>(), (int64_t)(Mp * Kp), tay, B2, (int64_t)n, (const int*)expB,
-                           bres.as<int8_t>(), (int64_t)(Np * Kp), (int64_t)k, beta, L, (int64_t)Kp));
-    else
-      HP_CUDA_TRY(launch_k(pdl, residue_ab_kernel<false, RES_EPR, true>, g, dim3(256), 0, s, A2, (int64_t)m, (const int*)expA,
-                           ares.as<int8_t>(), (int64_t)(Mp * Kp), tay, B2, (int64_t)n, (const int*)expB,
-                           bres.as<int8_t>(), (int64_t)(Np * Kp), (int64_t)k, beta, L, (int64_t)Kp));
+    HP_CUDA_TRY(launch_residues_ab(atb, L, pdl, g, s, A2, (int64_t)m, (const int*)expA, ares.as<int8_t>(),
+                                   (int64_t)(Mp * Kp), tay, B2, (int64_t)n, (const int*)expB, bres.as<int8_t>(),
+                                   (int64_t)(Np * Kp), (int64_t)k, beta, (int64_t)Kp));
   }
   profile_mark(s, "residues");
   // 3. one int8 GEMM per modulus
@@ -1018,7 +1126,7 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
   profile_mark(s, "i8_gemm");
   // 4. CRT
   HP_TRY(launch_crt_dd(cres.as<uint8_t>(), Mp, Np, m, n, expA, expB, beta, D->crt + L, host_tables().crt[L].nc,
-                       reinterpret_cast<double2*>(c), s, pdl));
+                       reinterpret_cast<double2*>(c), s, pdl, L));
   profile_mark(s, "crt");
   return HP_OK;
 }
