@@ -19,6 +19,9 @@ const char* last_error();
 // The library's own non-blocking stream for the host-pointer entry points
 // (one per device, created on first use).
 cudaStream_t library_stream();
+// Two more per-device streams for host<->device copies that overlap the
+// library stream's kernels (0: host to device, 1: device to host).
+cudaStream_t library_copy_stream(int which);
 
 // Stream-ordered device memory from the device's default pool. The pool is
 // configured once to keep freed blocks cached, so repeated calls of the same

@@ -1131,6 +1131,123 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
   return HP_OK;
 }
 
+// Host-pointer f128 GEMM C = A B (chosen mode) with the PCIe copies
+// overlapped: B goes to the device first and its exponents and residue
+// planes are formed once; A then streams in as row panels on a copy stream,
+// each panel's exponents, residues, residue GEMM and CRT run on the library
+// stream as soon as its rows have landed, and each finished panel of C goes
+// back on a second copy stream while the next panels are computed. The
+// arithmetic of every entry is that of ozaki_dd_gemm (same exponents,
+// residues and CRT), so the result is bit-identical to the one-shot path.
+namespace {
+struct StreamsDrain {  // every stream idle before the buffers above it are freed
+  cudaStream_t a, b, c;
+  ~StreamsDrain() {
+    cudaStreamSynchronize(a);
+    cudaStreamSynchronize(b);
+    cudaStreamSynchronize(c);
+  }
+};
+struct EventSet {
+  std::vector<cudaEvent_t> ev;
+  explicit EventSet(size_t count) : ev(count, nullptr) {
+    for (auto& e : ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  }
+  ~EventSet() {
+    for (auto e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+  bool ok() const {
+    for (auto e : ev)
+      if (!e) return false;
+    return true;
+  }
+};
+}  // namespace
+
+int ozaki_dd_gemm_host(const double* a, const double* b, double* c, size_t m, size_t n, size_t k) {
+  using namespace ozaki;
+  DevTables* D;
+  HP_TRY(device_tables(&D));
+  const int beta = BETA_DD;
+  const int L = ozaki_moduli_for(k, beta);
+  if (L < 0) {
+    set_error("ozaki: k = %zu needs more moduli than the table holds", k);
+    return HP_ERR_UNSUPPORTED;
+  }
+  const size_t Np = round_up(n, GB_N), Kp = round_up(k, GB_K);
+  const size_t panels_wanted = m >= 2048 ? 16 : m >= 1024 ? 8 : 4;
+  const size_t pr = round_up((m + panels_wanted - 1) / panels_wanted, GB_M);  // rows per panel
+  const size_t np = (m + pr - 1) / pr;
+  if (pr / GB_M * (Np / GB_N) * (size_t)L > (size_t)INT32_MAX || Kp > (size_t)INT32_MAX) {
+    set_error("ozaki: problem too large");
+    return HP_ERR_INVALID_ARG;
+  }
+  cudaStream_t s = library_stream(), sin = library_copy_stream(0), sout = library_copy_stream(1);
+  DevBuf dA(m * k * 16, s), dB(k * n * 16, s), dC(m * n * 16, s);
+  DevBuf exps((pr + Np) * sizeof(int), s);
+  DevBuf bres((size_t)L * Np * Kp, s), ares((size_t)L * pr * Kp, s), cres((size_t)L * pr * Np, s);
+  if (!dA.p || !dB.p || !dC.p || !exps.p || !bres.p || !ares.p || !cres.p) {
+    set_error("ozaki: workspace allocation failed");
+    return HP_ERR_CUDA;
+  }
+  EventSet ev(2 * np + 2);
+  if (!ev.ok()) {
+    set_error("ozaki: event creation failed");
+    return HP_ERR_CUDA;
+  }
+  StreamsDrain drain{s, sin, sout};
+  cudaEvent_t ready = ev.ev[0], eB = ev.ev[1];
+  cudaEvent_t* eA = ev.ev.data() + 2;
+  cudaEvent_t* eC = eA + np;
+  int* expA = exps.as<int>();
+  int* expB = expA + pr;
+  const bool pdl = !profiling_on();
+  // the buffers exist (stream-ordered) before the copy streams touch them
+  HP_CUDA_TRY(cudaEventRecord(ready, s));
+  HP_CUDA_TRY(cudaStreamWaitEvent(sin, ready, 0));
+  HP_CUDA_TRY(cudaStreamWaitEvent(sout, ready, 0));
+  HP_CUDA_TRY(cudaMemcpyAsync(dB.p, b, k * n * 16, cudaMemcpyHostToDevice, sin));
+  HP_CUDA_TRY(cudaEventRecord(eB, sin));
+  for (size_t i = 0; i < np; i++) {
+    const size_t r0 = i * pr, mi = std::min(pr, m - r0);
+    HP_CUDA_TRY(cudaMemcpyAsync(dA.as<char>() + r0 * k * 16, reinterpret_cast<const char*>(a) + r0 * k * 16,
+                                mi * k * 16, cudaMemcpyHostToDevice, sin));
+    HP_CUDA_TRY(cudaEventRecord(eA[i], sin));
+  }
+  // B once: column exponents and residue planes
+  HP_CUDA_TRY(cudaStreamWaitEvent(s, eB, 0));
+  HP_CUDA_TRY(cudaMemsetAsync(expB, 0, Np * sizeof(int), s));
+  const double2* B2 = dB.as<const double2>();
+  HP_TRY(launch_maxexp((const double2*)nullptr, B2, 0, n, k, false, nullptr, expB, s));
+  HP_CUDA_TRY(launch_residues_ab(false, L, pdl, dim3((unsigned)(Kp / (4 * RES_EPR)), (unsigned)(Np / RT_R)), s,
+                                 nullptr, 0, nullptr, nullptr, 0, 0, B2, (int64_t)n, expB, bres.as<int8_t>(),
+                                 (int64_t)(Np * Kp), (int64_t)k, beta, (int64_t)Kp));
+  const int nc = host_tables().crt[L].nc;
+  for (size_t i = 0; i < np; i++) {
+    const size_t r0 = i * pr, mi = std::min(pr, m - r0), Mpi = round_up(mi, GB_M);
+    const double2* A2 = dA.as<const double2>() + r0 * k;
+    double* Ci = dC.as<double>() + r0 * n * 2;
+    HP_CUDA_TRY(cudaStreamWaitEvent(s, eA[i], 0));
+    HP_TRY(launch_maxexp(A2, (const double2*)nullptr, mi, 0, k, false, expA, nullptr, s));
+    const unsigned tay = (unsigned)(Mpi / RT_R);
+    HP_CUDA_TRY(launch_residues_ab(false, L, pdl, dim3((unsigned)(Kp / (4 * RES_EPR)), tay), s, A2, (int64_t)mi,
+                                   expA, ares.as<int8_t>(), (int64_t)(Mpi * Kp), tay, nullptr, 0, nullptr, nullptr,
+                                   0, (int64_t)k, beta, (int64_t)Kp));
+    HP_TRY(ozaki_residue_gemm_k(ares.as<int8_t>(), bres.as<int8_t>(), cres.as<uint8_t>(), L, Mpi, Np, Kp, Kp, 0, Kp,
+                                0, Np, Mpi * Np, 0, 0, 0, s, Mpi, Np, pdl, true));
+    HP_TRY(launch_crt_dd(cres.as<uint8_t>(), Mpi, Np, mi, n, expA, expB, beta, D->crt + L, nc,
+                         reinterpret_cast<double2*>(Ci), s, pdl, L));
+    HP_CUDA_TRY(cudaEventRecord(eC[i], s));
+    HP_CUDA_TRY(cudaStreamWaitEvent(sout, eC[i], 0));
+    HP_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<char*>(c) + r0 * n * 16, Ci, mi * n * 16, cudaMemcpyDeviceToHost,
+                                sout));
+  }
+  HP_CUDA_TRY(cudaStreamSynchronize(sout));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  return consume_device_status(s);
+}
+
 // ===========================================================================
 // f256 (MultiFloat<4>) Ozaki-II GEMM.
 // Entries are scaled to integers X of <= 210 bits and split X = Xh 2^105 + Xl

@@ -21,6 +21,7 @@ namespace {
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 cudaStream_t g_stream[kMaxDevices] = {};
+cudaStream_t g_copy_stream[kMaxDevices][2] = {};
 bool g_pool_ready[kMaxDevices] = {};
 // One sticky status word per device: kernels OR bits into it, and the host
 // entry points read and clear it at their synchronisation points
@@ -49,6 +50,14 @@ cudaStream_t library_stream() {
   if (!g_stream[d]) cudaStreamCreateWithFlags(&g_stream[d], cudaStreamNonBlocking);
   ensure_pool(d);
   return g_stream[d];
+}
+
+cudaStream_t library_copy_stream(int which) {
+  std::lock_guard<std::mutex> lk(g_mu);
+  int d = cur_dev();
+  cudaStream_t& st = g_copy_stream[d][which & 1];
+  if (!st) cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+  return st;
 }
 
 void* dev_alloc(size_t bytes, cudaStream_t s) {

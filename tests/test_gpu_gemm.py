@@ -176,3 +176,24 @@ def test_f128_ozaki_long_k_chunks(gpu, atb):
     ref = O.gemm(a, b, m, n, k, atb=atb)
     err = normwise_err(c, ref, abs_prod(a, b, atb))
     assert err <= 4 * k * 2.0 ** -104, err
+
+
+@pytest.mark.parametrize("m,n,k", [(512, 130, 200), (700, 257, 129), (1100, 64, 300), (2050, 33, 65)])
+def test_f128_ozaki_host_pipeline_matches_device(gpu, m, n, k):
+    """Host-pointer chosen GEMMs with m >= 512 run B once and A in row panels
+    (copies overlapped with the panels' kernels); every entry must carry the
+    bits of the one-shot device-pointer path, ragged last panels included,
+    and the normwise tolerance against the oracle."""
+    import torch
+
+    a, b = gemm_operands(m, n, k, seed=7 + m)
+    c_host = gpu.f128_gemm(a, b, m, n, k, gpu.OZAKI)
+    da, db = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+    dc = torch.empty((m, n, 2), dtype=torch.float64, device="cuda")
+    s = torch.cuda.current_stream()
+    gpu.f128_gemm_dev(da, db, dc, m, n, k, gpu.OZAKI, stream=s.cuda_stream)
+    s.synchronize()
+    assert np.array_equal(c_host, dc.cpu().numpy())
+    if m == 700:
+        err = normwise_err(c_host, O.gemm(a, b, m, n, k), abs_prod(a, b, False))
+        assert err <= 4 * k * 2.0 ** -104, err
