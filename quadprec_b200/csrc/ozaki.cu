@@ -1717,24 +1717,26 @@ __global__ void __launch_bounds__(256) crt_block_kernel(const uint8_t* __restric
 //     pivoted and scaled, applied to column 2q + 3 inside the warp, and
 //     column 2q + 3 is pivoted and scaled; every lane forms each 1/sqrt from
 //     the same value, so nothing needs broadcasting but the two l values.
+//     The scaled columns replace their entries of the block in shared
+//     memory (no other warp touches columns 2q + 2, 2q + 3 in iteration q).
 //   the bulk warps (those on the three other schedulers, warp % 4 != 3):
 //     pair q applied to every column k >= 2q + 4 (rows i >= k; a table
 //     ordered by column makes these the first T slots).
-//   the other warps of warp 31's scheduler: pair q to Lout, L1 and rinv.
-// Each entry receives its column updates in column order, as in a plain
+//   the other warps of warp 31's scheduler stay idle, so that nothing
+//     competes with the pivot chain for its scheduler's FP64 pipe.
+// Lout, L1 and rinv are written by all warps after the last pair. Each
+// entry receives its column updates in column order, as in a plain
 // right-looking Cholesky; dd_fms_fast (f128-level accuracy, not the
 // reference's bits).
 constexpr int CI_THREADS = 1024;
 constexpr int CI_BULK = CI_THREADS / 4 * 3;  // warps with warp % 4 != 3
-constexpr int CI_OUT = CI_THREADS / 4 - 32;  // the other warps with warp % 4 == 3
 __global__ void __launch_bounds__(CI_THREADS) chol_block_kernel(const dd* __restrict__ P, int jb, int64_t kb,
                                                                 int64_t n, const int* __restrict__ e,
                                                                 dd* __restrict__ Lout, dd* __restrict__ L1g,
                                                                 dd* __restrict__ rinvg, RnsErr* err) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
-  dd* A = reinterpret_cast<dd*>(sm_raw);  // [64][65]
-  __shared__ dd Lc[2][2][64];             // scaled columns 2q, 2q + 1 of L~, double-buffered
-  __shared__ dd rinv[64], ldiag[64];      // 1 / l_jj and l_jj = sqrt(a_jj)
+  dd* A = reinterpret_cast<dd*>(sm_raw);  // [64][65]; factored columns hold L~ below the diagonal
+  __shared__ dd rinv[64], dpiv[64];       // 1 / l_jj and the pivot a_jj (l_jj = a_jj / l_jj)
   __shared__ uint16_t tab[2016];          // (i << 6) | k, column k = 63..1, rows i = k..63
   __shared__ int esh[64];
   __shared__ int fail;
@@ -1742,7 +1744,6 @@ __global__ void __launch_bounds__(CI_THREADS) chol_block_kernel(const dd* __rest
   const bool critical = warp == CI_THREADS / 32 - 1;
   const bool bulk = warp % 4 != 3;
   const int bt = (warp / 4 * 3 + warp % 4) * 32 + lane;  // bulk thread index
-  const int ot = (warp / 4) * 32 + lane;                 // index among the output warps (warp % 4 == 3)
   sm100::griddep_launch_dependents();
   sm100::griddep_wait();  // P comes from the preceding CRT
   if (err->flag) return;
@@ -1770,14 +1771,14 @@ __global__ void __launch_bounds__(CI_THREADS) chol_block_kernel(const dd* __rest
     r = dd_rsqrt_fast(d);
     if (lane == 0) {
       rinv[p] = r;
-      ldiag[p] = dd_mul(d, r);
+      dpiv[p] = d;  // l_jj = d r is formed after the loop, off the pivot chain
     }
     return true;
   };
   // Factor the pair (c0, c0 + 1) on warp 31 from its updated entries a?0
   // (column c0) and a?1 (column c0 + 1) at rows c0 + lane and c0 + 32 + lane;
-  // scaled columns to buffer b.
-  auto factor_pair = [&](int c0, dd a00, dd a10, dd a01, dd a11, int b) -> bool {
+  // the scaled columns go to A's columns c0, c0 + 1 below the diagonal.
+  auto factor_pair = [&](int c0, dd a00, dd a10, dd a01, dd a11) -> bool {
     const int c1 = c0 + 1, i0 = c0 + lane, i1 = c0 + 32 + lane;
     dd r0, r1;
     const dd d0 = {__shfl_sync(0xffffffffu, a00.hi, 0), __shfl_sync(0xffffffffu, a00.lo, 0)};
@@ -1789,64 +1790,58 @@ __global__ void __launch_bounds__(CI_THREADS) chol_block_kernel(const dd* __rest
     const dd d1 = {__shfl_sync(0xffffffffu, a01.hi, 1), __shfl_sync(0xffffffffu, a01.lo, 1)};
     if (!pivot(c1, d1, r1)) return false;
     const dd s01 = dd_mul(a01, r1), s11 = dd_mul(a11, r1);
-    if (i0 < 64 && i0 > c0) Lc[b][0][i0] = s00;
-    if (i1 < 64) Lc[b][0][i1] = s10;
-    if (i0 < 64 && i0 > c1) Lc[b][1][i0] = s01;
-    if (i1 < 64) Lc[b][1][i1] = s11;
+    if (i0 < 64 && i0 > c0) A[i0 * 65 + c0] = s00;
+    if (i1 < 64) A[i1 * 65 + c0] = s10;
+    if (i0 < 64 && i0 > c1) A[i0 * 65 + c1] = s01;
+    if (i1 < 64) A[i1 * 65 + c1] = s11;
     return true;
-  };
-  // pair q (columns 2q, 2q + 1, buffer q & 1) to Lout, L1 and rinv
-  auto outputs = [&](int q) {
-    for (int h = 0; h < 2; h++) {
-      const int j = 2 * q + h;
-      const dd rj = rinv[j];
-      for (int i = j + ot; i < 64; i += CI_OUT) {
-        const dd v = i == j ? ldiag[j] : Lc[q & 1][h][i];
-        if (i > j) L1g[i * 64 + j] = dd_mul(v, rj);
-        if (i < jb && j < jb) {
-          const int sh = -esh[i];
-          Lout[(kb + i) * n + kb + j] = dd_renorm(scale_pow2(v.hi, sh), scale_pow2(v.lo, sh));
-        }
-      }
-      if (ot == 0) rinvg[j] = rj;
-    }
   };
   if (critical) {  // pair 0
     const int i0 = lane, i1 = 32 + lane;
-    factor_pair(0, A[i0 * 65], A[i1 * 65], A[i0 * 65 + 1], A[i1 * 65 + 1], 0);
+    factor_pair(0, A[i0 * 65], A[i1 * 65], A[i0 * 65 + 1], A[i1 * 65 + 1]);
   }
   __syncthreads();
   for (int q = 0; q < 32; q++) {
     if (fail) return;
-    const int cur = q & 1, nxt = cur ^ 1;
+    const int ca = 2 * q, cb = ca + 1;  // pair q's columns (scaled L~ below the diagonal)
     if (critical) {
       if (q < 31) {
         // pair q + 1 (columns c0, c0 + 1): last updates from pair q. Indices
         // are clamped so the chains run unconditionally; stores are predicated.
         const int c0 = 2 * q + 2, c1 = c0 + 1;
         const int i0c = min(c0 + lane, 63), i1c = min(c0 + 32 + lane, 63);
-        const dd* la = Lc[cur][0];
-        const dd* lb = Lc[cur][1];
-        const dd a00 = dd_fms_fast(dd_fms_fast(A[i0c * 65 + c0], la[i0c], la[c0]), lb[i0c], lb[c0]);
-        const dd a10 = dd_fms_fast(dd_fms_fast(A[i1c * 65 + c0], la[i1c], la[c0]), lb[i1c], lb[c0]);
-        const dd a01 = dd_fms_fast(dd_fms_fast(A[i0c * 65 + c1], la[i0c], la[c1]), lb[i0c], lb[c1]);
-        const dd a11 = dd_fms_fast(dd_fms_fast(A[i1c * 65 + c1], la[i1c], la[c1]), lb[i1c], lb[c1]);
-        factor_pair(c0, a00, a10, a01, a11, nxt);
+        const dd la0 = A[c0 * 65 + ca], la1 = A[c1 * 65 + ca], lb0 = A[c0 * 65 + cb], lb1 = A[c1 * 65 + cb];
+        const dd lai = A[i0c * 65 + ca], laj = A[i1c * 65 + ca], lbi = A[i0c * 65 + cb], lbj = A[i1c * 65 + cb];
+        const dd a00 = dd_fms_fast(dd_fms_fast(A[i0c * 65 + c0], lai, la0), lbi, lb0);
+        const dd a10 = dd_fms_fast(dd_fms_fast(A[i1c * 65 + c0], laj, la0), lbj, lb0);
+        const dd a01 = dd_fms_fast(dd_fms_fast(A[i0c * 65 + c1], lai, la1), lbi, lb1);
+        const dd a11 = dd_fms_fast(dd_fms_fast(A[i1c * 65 + c1], laj, la1), lbj, lb1);
+        factor_pair(c0, a00, a10, a01, a11);
       }
     } else if (bulk) {
       const int m = 60 - 2 * q;  // columns >= 2q + 4: T = m (m + 1) / 2 slots
       const int Tn = m > 0 ? m * (m + 1) / 2 : 0;
-      const dd* la = Lc[cur][0];
-      const dd* lb = Lc[cur][1];
       for (int u = bt; u < Tn; u += CI_BULK) {
         const int ent = tab[u], i = ent >> 6, kk = ent & 63;
-        A[i * 65 + kk] = dd_fms_fast(dd_fms_fast(A[i * 65 + kk], la[i], la[kk]), lb[i], lb[kk]);
+        A[i * 65 + kk] =
+            dd_fms_fast(dd_fms_fast(A[i * 65 + kk], A[i * 65 + ca], A[kk * 65 + ca]), A[i * 65 + cb], A[kk * 65 + cb]);
       }
-    } else {
-      outputs(q);
     }
     __syncthreads();
   }
+  // outputs of every column: L~ (scaled back) to Lout, L1 = L~ / l_jj, rinv
+  for (int u = t; u < 64 * 64; u += CI_THREADS) {
+    const int i = u / 64, j = u % 64;
+    if (i < j) continue;
+    const dd rj = rinv[j];
+    const dd v = i == j ? dd_mul(dpiv[j], rj) : A[i * 65 + j];
+    if (i > j) L1g[i * 64 + j] = dd_mul(v, rj);
+    if (i < jb && j < jb) {
+      const int sh = -esh[i];
+      Lout[(kb + i) * n + kb + j] = dd_renorm(scale_pow2(v.hi, sh), scale_pow2(v.lo, sh));
+    }
+  }
+  if (t < 64) rinvg[t] = rinv[t];
 }
 
 // L21 = P21 L~11^-T for the rows below the diagonal block. With
