@@ -72,6 +72,7 @@ struct ModTable {
   uint32_t magic[MAXL];   // floor(2^32 / m)
   uint32_t offset[MAXL];  // m * ceil(2^31 / m): makes |x| <= 2^30 + 2^27 non-negative
   int pw[MAXL][NDIG2];    // 2^(22 c) mod m, balanced into [-m/2, m/2]
+  int pw21[MAXL][5];      // 2^(21 c) mod m, balanced (digits of the f256 operands)
 };
 __constant__ ModTable c_tab;
 
@@ -175,6 +176,13 @@ static const HostTables& host_tables() {
         int b = (int)r;
         if (b > m / 2) b -= m;
         T.mt.pw[l][c] = b;
+      }
+      for (int c = 0; c < 5; c++) {
+        uint64_t r = 1;
+        for (int t = 0; t < 21 * c; t++) r = (r * 2) % m;
+        int b = (int)r;
+        if (b > m / 2) b -= m;
+        T.mt.pw21[l][c] = b;
       }
       T.cum_log2[l + 1] = T.cum_log2[l] + std::log2((double)m);
     }
@@ -485,36 +493,36 @@ __device__ __forceinline__ void residue_tile(const double2* __restrict__ src, in
             make_uint4(sw[0], sw[1], sw[2], sw[3]);
       }
     }
-    return;
-  }
-  int it = 0;
-  for (int l = 0; l < L; l++, it++) {
-    const int m = c_tab.mod[l];
-    uint32_t w[NW];
+  } else {
+    int it = 0;
+    for (int l = 0; l < L; l++, it++) {
+      const int m = c_tab.mod[l];
+      uint32_t w[NW];
 #pragma unroll
-    for (int q = 0; q < NW; q++) {
-      w[q] = 0;
+      for (int q = 0; q < NW; q++) {
+        w[q] = 0;
 #pragma unroll
-      for (int e = 0; e < 4; e++) {
-        const uint32_t byte = U8 ? unsigned_byte(dig[4 * q + e], l) : balanced_byte(dig[4 * q + e], l, m);
-        w[q] |= byte << (8 * e);
+        for (int e = 0; e < 4; e++) {
+          const uint32_t byte = U8 ? unsigned_byte(dig[4 * q + e], l) : balanced_byte(dig[4 * q + e], l, m);
+          w[q] |= byte << (8 * e);
+        }
       }
-    }
-    int8_t* plane = base + (size_t)l * plane_stride;
-    if (P_CONTIG) {
-      if (NW == 2)
-        *reinterpret_cast<uint2*>(plane + (size_t)rl * ld + EPR * quad) = make_uint2(w[0], w[NW - 1]);
-      else
-        *reinterpret_cast<uint32_t*>(plane + (size_t)rl * ld + EPR * quad) = w[0];
-    } else {
+      int8_t* plane = base + (size_t)l * plane_stride;
+      if (P_CONTIG) {
+        if (NW == 2)
+          *reinterpret_cast<uint2*>(plane + (size_t)rl * ld + EPR * quad) = make_uint2(w[0], w[NW - 1]);
+        else
+          *reinterpret_cast<uint32_t*>(plane + (size_t)rl * ld + EPR * quad) = w[0];
+      } else {
 #pragma unroll
-      for (int q = 0; q < NW; q++) T[it & 1][rl][NW * quad + q] = w[q];
-      __syncthreads();
-      if (t < NW * RT_R) {
-        const int row = t / NW, half = t % NW;
-        const uint32_t* src_w = &T[it & 1][row][4 * half];
-        *reinterpret_cast<uint4*>(plane + (size_t)row * ld + 16 * half) =
-            make_uint4(src_w[0], src_w[1], src_w[2], src_w[3]);
+        for (int q = 0; q < NW; q++) T[it & 1][rl][NW * quad + q] = w[q];
+        __syncthreads();
+        if (t < NW * RT_R) {
+          const int row = t / NW, half = t % NW;
+          const uint32_t* src_w = &T[it & 1][row][4 * half];
+          *reinterpret_cast<uint4*>(plane + (size_t)row * ld + 16 * half) =
+              make_uint4(src_w[0], src_w[1], src_w[2], src_w[3]);
+        }
       }
     }
   }
@@ -1300,7 +1308,10 @@ __device__ __forceinline__ uint32_t unsigned_byte21(const int32_t* D, const int*
 // One RT_R x (4 EPR) tile (block coordinates bx, by) of the f256 residue
 // rows [Xh | Xl]: EPR entries per thread (8 or 4), all L moduli, residues
 // balanced (signed bytes) or, with U8, in [0, m).
-template <bool P_CONTIG, int EPR, bool U8>
+// LC > 0: L == LC at compile time; the moduli loop is unrolled with each
+// modulus' constants (c_tab.pw21) as immediate operands, and the
+// transposed tile stores its planes in groups of QG behind one barrier.
+template <bool P_CONTIG, int EPR, bool U8, int LC = 0>
 __device__ __forceinline__ void residue_qd_tile(const double4* __restrict__ src, int64_t R, int64_t K,
                                                 const int* __restrict__ expf, int L, int64_t Rp, int64_t Kp,
                                                 int64_t hi_off, int64_t lo_off, int8_t* __restrict__ out,
@@ -1345,43 +1356,95 @@ __device__ __forceinline__ void residue_qd_tile(const double4* __restrict__ src,
     }
   }
   int8_t* const base = out + (size_t)by * RT_R * (2 * Kp) + (size_t)bx * (4 * EPR);
-  for (int l = 0; l < L; l++) {
-    const int m = c_tab.mod[l];
-    uint32_t wh[NW], wl[NW];
+  if constexpr (LC > 0) {
+    constexpr int QG = 8;  // planes per barrier of the transposed store
+    __shared__ uint32_t TG[P_CONTIG ? 1 : QG][2][P_CONTIG ? 1 : RT_R][EPR + 1];
 #pragma unroll
-    for (int q = 0; q < NW; q++) {
-      wh[q] = wl[q] = 0;
-#pragma unroll
-      for (int e = 0; e < 4; e++) {
-        const int32_t* dl = dig[4 * q + e];
-        const uint32_t bl = U8 ? unsigned_byte21(dl, w21[l], l) : balanced_byte21(dl, w21[l], l, m);
-        const uint32_t bh = U8 ? unsigned_byte21(dl + 5, w21[l], l) : balanced_byte21(dl + 5, w21[l], l, m);
-        wl[q] |= bl << (8 * e);
-        wh[q] |= bh << (8 * e);
-      }
-    }
-    int8_t* plane = base + (size_t)l * Rp * (2 * Kp);
-    if (P_CONTIG) {
-      int8_t* row = plane + (size_t)rl * (2 * Kp) + EPR * quad;
-      if (NW == 2) {
-        *reinterpret_cast<uint2*>(row + hi_off) = make_uint2(wh[0], wh[NW - 1]);
-        *reinterpret_cast<uint2*>(row + lo_off) = make_uint2(wl[0], wl[NW - 1]);
-      } else {
-        *reinterpret_cast<uint32_t*>(row + hi_off) = wh[0];
-        *reinterpret_cast<uint32_t*>(row + lo_off) = wl[0];
-      }
-    } else {
+    for (int l = 0; l < LC; l++) {
+      uint32_t wh[NW], wl[NW];
 #pragma unroll
       for (int q = 0; q < NW; q++) {
-        T[l & 1][0][rl][NW * quad + q] = wh[q];
-        T[l & 1][1][rl][NW * quad + q] = wl[q];
+        wh[q] = wl[q] = 0;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int32_t* dl = dig[4 * q + e];
+          const uint32_t bl = U8 ? unsigned_byte21(dl, c_tab.pw21[l], l)
+                                 : balanced_byte21(dl, c_tab.pw21[l], l, c_tab.mod[l]);
+          const uint32_t bh = U8 ? unsigned_byte21(dl + 5, c_tab.pw21[l], l)
+                                 : balanced_byte21(dl + 5, c_tab.pw21[l], l, c_tab.mod[l]);
+          wl[q] |= bl << (8 * e);
+          wh[q] |= bh << (8 * e);
+        }
       }
-      __syncthreads();
-      if (t < RT_R * 2 * NW) {
-        const int row = t / (2 * NW), rem = t % (2 * NW), part = rem / NW, half = rem % NW;
-        const uint32_t* sw = &T[l & 1][part][row][4 * half];
-        *reinterpret_cast<uint4*>(plane + (size_t)row * (2 * Kp) + (part ? lo_off : hi_off) + 16 * half) =
-            make_uint4(sw[0], sw[1], sw[2], sw[3]);
+      int8_t* plane = base + (size_t)l * Rp * (2 * Kp);
+      if constexpr (P_CONTIG) {
+        int8_t* row = plane + (size_t)rl * (2 * Kp) + EPR * quad;
+        if (NW == 2) {
+          *reinterpret_cast<uint2*>(row + hi_off) = make_uint2(wh[0], wh[NW - 1]);
+          *reinterpret_cast<uint2*>(row + lo_off) = make_uint2(wl[0], wl[NW - 1]);
+        } else {
+          *reinterpret_cast<uint32_t*>(row + hi_off) = wh[0];
+          *reinterpret_cast<uint32_t*>(row + lo_off) = wl[0];
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < NW; q++) {
+          TG[l % QG][0][rl][NW * quad + q] = wh[q];
+          TG[l % QG][1][rl][NW * quad + q] = wl[q];
+        }
+        if (l % QG == QG - 1 || l == LC - 1) {  // a group of planes is complete
+          const int g0 = l - l % QG, gn = l % QG + 1;
+          __syncthreads();
+          for (int u = t; u < gn * RT_R * 2 * NW; u += blockDim.x) {
+            const int gl = u / (RT_R * 2 * NW), rem = u % (RT_R * 2 * NW);
+            const int row = rem / (2 * NW), r2 = rem % (2 * NW), part = r2 / NW, half = r2 % NW;
+            const uint32_t* sw = &TG[gl][part][row][4 * half];
+            *reinterpret_cast<uint4*>(base + (size_t)(g0 + gl) * Rp * (2 * Kp) + (size_t)row * (2 * Kp) +
+                                      (part ? lo_off : hi_off) + 16 * half) = make_uint4(sw[0], sw[1], sw[2], sw[3]);
+          }
+          __syncthreads();  // the group's buffers are rewritten by the next group
+        }
+      }
+    }
+  } else {
+    for (int l = 0; l < L; l++) {
+      const int m = c_tab.mod[l];
+      uint32_t wh[NW], wl[NW];
+#pragma unroll
+      for (int q = 0; q < NW; q++) {
+        wh[q] = wl[q] = 0;
+#pragma unroll
+        for (int e = 0; e < 4; e++) {
+          const int32_t* dl = dig[4 * q + e];
+          const uint32_t bl = U8 ? unsigned_byte21(dl, w21[l], l) : balanced_byte21(dl, w21[l], l, m);
+          const uint32_t bh = U8 ? unsigned_byte21(dl + 5, w21[l], l) : balanced_byte21(dl + 5, w21[l], l, m);
+          wl[q] |= bl << (8 * e);
+          wh[q] |= bh << (8 * e);
+        }
+      }
+      int8_t* plane = base + (size_t)l * Rp * (2 * Kp);
+      if (P_CONTIG) {
+        int8_t* row = plane + (size_t)rl * (2 * Kp) + EPR * quad;
+        if (NW == 2) {
+          *reinterpret_cast<uint2*>(row + hi_off) = make_uint2(wh[0], wh[NW - 1]);
+          *reinterpret_cast<uint2*>(row + lo_off) = make_uint2(wl[0], wl[NW - 1]);
+        } else {
+          *reinterpret_cast<uint32_t*>(row + hi_off) = wh[0];
+          *reinterpret_cast<uint32_t*>(row + lo_off) = wl[0];
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < NW; q++) {
+          T[l & 1][0][rl][NW * quad + q] = wh[q];
+          T[l & 1][1][rl][NW * quad + q] = wl[q];
+        }
+        __syncthreads();
+        if (t < RT_R * 2 * NW) {
+          const int row = t / (2 * NW), rem = t % (2 * NW), part = rem / NW, half = rem % NW;
+          const uint32_t* sw = &T[l & 1][part][row][4 * half];
+          *reinterpret_cast<uint4*>(plane + (size_t)row * (2 * Kp) + (part ? lo_off : hi_off) + 16 * half) =
+              make_uint4(sw[0], sw[1], sw[2], sw[3]);
+        }
       }
     }
   }
@@ -1390,29 +1453,20 @@ __device__ __forceinline__ void residue_qd_tile(const double4* __restrict__ src,
 // Both f256 operands' residues in one launch: block rows [0, tiles_ay) cover
 // A (row-contiguous when A_CONTIG; halves at hi 0, lo Kp), the rest B
 // (transposed; halves at hi Kp, lo 0).
-template <bool A_CONTIG, int EPR, bool U8>
+template <bool A_CONTIG, int EPR, bool U8, int LC = 0>
 __global__ void __launch_bounds__(256, 3) residue_qd_ab_kernel(const double4* __restrict__ A, int64_t RA, int64_t RpA,
                                                             const int* __restrict__ expA, int8_t* __restrict__ outA,
                                                             unsigned tiles_ay, const double4* __restrict__ B,
                                                             int64_t RB, int64_t RpB, const int* __restrict__ expB,
                                                             int8_t* __restrict__ outB, int64_t K, int64_t Kp, int L) {
-  __shared__ int w21[MAXL][5];  // 2^(21 c) mod m, balanced
-  for (int q = threadIdx.x; q < L * 5; q += blockDim.x) {
-    const int l = q / 5, c = q % 5;
-    const int m = c_tab.mod[l];
-    int64_t rr = 1;
-    for (int t = 0; t < 21 * c; t++) rr = (rr * 2) % m;
-    int b = (int)rr;
-    if (b > m / 2) b -= m;
-    w21[l][c] = b;
-  }
+  const int(*w21)[5] = c_tab.pw21;  // 2^(21 c) mod m, balanced
   sm100::griddep_launch_dependents();
   sm100::griddep_wait();  // the exponents come from the preceding pass
-  __syncthreads();
   if (blockIdx.y < tiles_ay)
-    residue_qd_tile<A_CONTIG, EPR, U8>(A, RA, K, expA, L, RpA, Kp, 0, Kp, outA, blockIdx.x, blockIdx.y, w21);
+    residue_qd_tile<A_CONTIG, EPR, U8, LC>(A, RA, K, expA, L, RpA, Kp, 0, Kp, outA, blockIdx.x, blockIdx.y, w21);
   else
-    residue_qd_tile<false, EPR, U8>(B, RB, K, expB, L, RpB, Kp, Kp, 0, outB, blockIdx.x, blockIdx.y - tiles_ay, w21);
+    residue_qd_tile<false, EPR, U8, LC>(B, RB, K, expB, L, RpB, Kp, Kp, 0, outB, blockIdx.x, blockIdx.y - tiles_ay,
+                                        w21);
 }
 
 // f256 CRT: rebuild G1 and G2, C = (G1 2^105 + G2) 2^(105 - sa - sb).
@@ -1430,12 +1484,13 @@ __device__ __forceinline__ qd chunks_to_qd(const double* acc, int nc) {
   qd_renormalize_from8(v, r.l);
   return r;
 }
-template <int NC>
-__device__ __forceinline__ qd crt_group_qd(const uint8_t* rp, int64_t plane, int L, const double (*w_s)[NC],
-                                           const double* mch, double inv_m) {
+template <int NC, int LC = 0, class W>
+__device__ __forceinline__ qd crt_group_qd(const uint8_t* rp, int64_t plane, int L, W w_s, const double* mch,
+                                           double inv_m) {
   double acc[NC + 1];
 #pragma unroll
   for (int q = 0; q <= NC; q++) acc[q] = 0.0;
+#pragma unroll(LC > 0 ? 8 : 1)
   for (int l0 = 0; l0 < L; l0 += 8) {
     uint32_t v[8];
 #pragma unroll
@@ -1453,19 +1508,23 @@ __device__ __forceinline__ qd crt_group_qd(const uint8_t* rp, int64_t plane, int
   qd r = chunks_to_qd(acc, NC);
   return neg ? qd_neg(r) : r;
 }
-template <int NC>
+// LC > 0: L == LC at compile time, tables from c_crt (weights as immediate
+// operands), moduli loop unrolled.
+template <int NC, int LC = 0>
 __global__ void __launch_bounds__(256) crt_qd_kernel(const uint8_t* __restrict__ g1, const uint8_t* __restrict__ g2,
                                                      int64_t plane, int64_t Np, int64_t m, int64_t n,
                                                      const int* __restrict__ expA, const int* __restrict__ expB,
                                                      const CrtTable* __restrict__ tab, double4* __restrict__ C) {
-  __shared__ double w_s[MAXL][NC];
-  __shared__ double mch_s[NC];
-  const int L = tab->L;
-  for (int i = threadIdx.x; i < L * NC; i += blockDim.x) w_s[i / NC][i % NC] = tab->w[i / NC][i % NC];
-  if (threadIdx.x < NC) mch_s[threadIdx.x] = tab->mchunk[threadIdx.x];
+  __shared__ double w_sm[LC > 0 ? 1 : MAXL][NC];
+  __shared__ double mch_sm[NC];
+  const int L = LC > 0 ? LC : tab->L;
+  if constexpr (LC == 0) {
+    for (int i = threadIdx.x; i < L * NC; i += blockDim.x) w_sm[i / NC][i % NC] = tab->w[i / NC][i % NC];
+    if (threadIdx.x < NC) mch_sm[threadIdx.x] = tab->mchunk[threadIdx.x];
+  }
   sm100::griddep_launch_dependents();
   sm100::griddep_wait();  // the product residues come from the preceding GEMM
-  __syncthreads();
+  if constexpr (LC == 0) __syncthreads();
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= m * n) return;
   const int64_t i = idx / n, j = idx % n;
@@ -1476,8 +1535,16 @@ __global__ void __launch_bounds__(256) crt_qd_kernel(const uint8_t* __restrict__
     return;
   }
   const size_t o = (size_t)i * Np + j;
-  const qd a = crt_group_qd<NC>(g1 + o, plane, L, w_s, mch_s, tab->inv_m);
-  const qd b = crt_group_qd<NC>(g2 + o, plane, L, w_s, mch_s, tab->inv_m);
+  qd a, b;
+  if constexpr (LC > 0) {
+    const CrtTable& ct = c_crt[LC - CRT_CONST_L0];
+    a = crt_group_qd<NC, LC>(g1 + o, plane, LC, ct.w, ct.mchunk, ct.inv_m);
+    b = crt_group_qd<NC, LC>(g2 + o, plane, LC, ct.w, ct.mchunk, ct.inv_m);
+  } else {
+    const double(*w_d)[NC] = w_sm;
+    a = crt_group_qd<NC>(g1 + o, plane, L, w_d, mch_sm, tab->inv_m);
+    b = crt_group_qd<NC>(g2 + o, plane, L, w_d, mch_sm, tab->inv_m);
+  }
   qd a_sh;
 #pragma unroll
   for (int q = 0; q < 4; q++) a_sh.l[q] = scale_pow2(a.l[q], 105);
@@ -1522,14 +1589,26 @@ int ozaki_qd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
   {  // residues of both operands as unsigned bytes, 4 entries per thread
     const unsigned tay = (unsigned)(Mp / RT_R);
     dim3 g((unsigned)(Kp / 16), tay + (unsigned)(Np / RT_R));
-    if (!atb)
-      HP_CUDA_TRY(launch_k(true, residue_qd_ab_kernel<true, 4, true>, g, dim3(256), 0, s, A4, (int64_t)m, (int64_t)Mp,
-                           (const int*)expAp, ares.as<int8_t>(), tay, B4, (int64_t)n, (int64_t)Np,
-                           (const int*)expBp, bres.as<int8_t>(), (int64_t)k, (int64_t)Kp, L));
-    else
-      HP_CUDA_TRY(launch_k(true, residue_qd_ab_kernel<false, 4, true>, g, dim3(256), 0, s, A4, (int64_t)m, (int64_t)Mp,
-                           (const int*)expAp, ares.as<int8_t>(), tay, B4, (int64_t)n, (int64_t)Np,
-                           (const int*)expBp, bres.as<int8_t>(), (int64_t)k, (int64_t)Kp, L));
+#define HP_RESQ(AC, LCV)                                                                                        \
+  HP_CUDA_TRY(launch_k(true, residue_qd_ab_kernel<AC, 4, true, LCV>, g, dim3(256), 0, s, A4, (int64_t)m,         \
+                       (int64_t)Mp, (const int*)expAp, ares.as<int8_t>(), tay, B4, (int64_t)n, (int64_t)Np,       \
+                       (const int*)expBp, bres.as<int8_t>(), (int64_t)k, (int64_t)Kp, L))
+#define HP_RESQ_L(AC)              \
+  switch (L) {                     \
+    case 28: HP_RESQ(AC, 28); break; \
+    case 29: HP_RESQ(AC, 29); break; \
+    case 30: HP_RESQ(AC, 30); break; \
+    case 31: HP_RESQ(AC, 31); break; \
+    case 32: HP_RESQ(AC, 32); break; \
+    default: HP_RESQ(AC, 0); break;  \
+  }
+    if (!atb) {
+      HP_RESQ_L(true)
+    } else {
+      HP_RESQ_L(false)
+    }
+#undef HP_RESQ_L
+#undef HP_RESQ
   }
   // G1 = Xh Yh: A bytes [0, Kp), B bytes [Kp, 2Kp)
   HP_TRY(ozaki_residue_gemm_k(ares.as<int8_t>(), bres.as<int8_t>(), g1.as<uint8_t>(), L, Mp, Np, 2 * Kp, 2 * Kp, 0, Kp,
@@ -1539,6 +1618,17 @@ int ozaki_qd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
                               2 * Kp, 0, Np, Mp * Np, 0, 0, 0, s, Mp, Np, false, true));
   const int nc = host_tables().crt[L].nc;
   const unsigned grid = (unsigned)((m * n + 255) / 256);
+#define HP_CRTQ_LC(NCV, LCV)                                                                                       \
+  if (nc == NCV && L == LCV) {                                                                                     \
+    HP_CUDA_TRY(launch_k(true, crt_qd_kernel<NCV, LCV>, dim3(grid), dim3(256), 0, s,                                \
+                         (const uint8_t*)g1.as<uint8_t>(), (const uint8_t*)g2.as<uint8_t>(), (int64_t)(Mp * Np),     \
+                         (int64_t)Np, (int64_t)m, (int64_t)n, (const int*)expAp, (const int*)expBp,                 \
+                         (const CrtTable*)(D->crt + L), reinterpret_cast<double4*>(c)));                            \
+    return HP_OK;                                                                                                  \
+  }
+  HP_CRTQ_LC(6, 28) HP_CRTQ_LC(6, 29) HP_CRTQ_LC(6, 30) HP_CRTQ_LC(6, 31) HP_CRTQ_LC(6, 32)
+  HP_CRTQ_LC(7, 28) HP_CRTQ_LC(7, 29) HP_CRTQ_LC(7, 30) HP_CRTQ_LC(7, 31) HP_CRTQ_LC(7, 32)
+#undef HP_CRTQ_LC
 #define HP_CRTQ(NC)                                                                                                  \
   case NC:                                                                                                           \
     HP_CUDA_TRY(launch_k(true, crt_qd_kernel<NC>, dim3(grid), dim3(256), 0, s, (const uint8_t*)g1.as<uint8_t>(),     \
