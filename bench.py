@@ -32,9 +32,9 @@ sys.path.insert(0, REPO)
 M = N = K = 2048
 # DRAM bytes (read + write) of one i8_gemm_mod_kernel<256> launch at this size,
 # from an ncu capture of `bench.py --profile-case gemm` (251.8 MB read: every
-# residue plane once; 98.3 MB written, the rest of the 125.8 MB of product
+# residue plane once; 99.1 MB written, the rest of the 125.8 MB of product
 # residues still in L2 when the kernel ends).
-I8_GEMM_TRAFFIC_BYTES = 350135296
+I8_GEMM_TRAFFIC_BYTES = 350834176
 METRIC = "f128 GEMM GFLOP/s; SPD solves/s at ≤1e-25 rel err: chosen vs plain, 1 B200"
 WORKLOAD = "f128 GEMM C=A*B, m=n=k=2048, full double-double entries (SplitMix64 seed 0)"
 
