@@ -240,13 +240,28 @@ __device__ __forceinline__ int rr_player(int slot, int round, int nn) {
   return 1 + (slot - 1 + round) % (nn - 1);
 }
 
-// Jacobi on a copy of A (row-major n x n f128) in the per-CTA slot.
+// Jacobi on A (row-major n x n f128, symmetric: its lower triangle is read)
+// with the working matrix in shared memory as a packed lower triangle
+// (n (n + 1) / 2 entries, 132 KB at n = 128) and V transposed in the per-CTA
+// slot of global memory (Vt[j][r] = V[r][j], so a column rotation of V is a
+// coalesced row update). A round has two barriers: the n/2 rotations
+// (linalg.rs:326-336), then every 2 x 2 block of A, rows of pair k1 by
+// columns of pair k2 (k1 <= k2), updated by one thread -- the column
+// rotation of pair k2 and then the row rotation of pair k1, the order of
+// A J followed by J^T (A J) -- with the diagonal blocks set by the
+// reference's formulas (linalg.rs:337-340), and V's columns rotated
+// (linalg.rs:342-357).
+__device__ __forceinline__ int packed_index(int i, int j) {  // lower triangle, row-major
+  return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i;
+}
 __global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __restrict__ n_off,
                                                             const int64_t* __restrict__ mat_off,
                                                             const dd* __restrict__ Ain, dd* __restrict__ evals,
                                                             dd* __restrict__ evecs, int* __restrict__ sweeps_out,
                                                             int* __restrict__ status, dd* __restrict__ work,
                                                             int64_t slot_elems, int max_sweeps) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  dd* Ap = reinterpret_cast<dd*>(sm_raw);  // packed lower triangle of A
   __shared__ dd cs[64][2];
   __shared__ dd old[64][3];  // a_pp, a_qq, a_pq before the round
   __shared__ dd tt[64];
@@ -256,20 +271,24 @@ __global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __res
   const int sys = blockIdx.x;
   const int n = (int)(n_off[sys + 1] - n_off[sys]);
   const dd* Asrc = Ain + mat_off[sys];
-  dd* A = work + (size_t)blockIdx.x * 2 * slot_elems;
-  dd* V = A + slot_elems;
+  dd* Vt = work + (size_t)blockIdx.x * slot_elems;
   for (int p = threadIdx.x; p < n * n; p += BT) {
-    A[p] = Asrc[p];
-    V[p] = dd_from(p / n == p % n ? 1.0 : 0.0);
+    const int i = p / n, j = p % n;
+    if (i >= j) Ap[packed_index(i, j)] = Asrc[p];
+    Vt[p] = dd_from(i == j ? 1.0 : 0.0);
   }
   __syncthreads();
   const int nn = n + (n & 1), half = nn / 2;
+  const int nblocks = half * (half + 1) / 2;
   int sweep = 0, converged = 0;
   for (sweep = 0; sweep < max_sweeps; sweep++) {
-    // off-diagonal norm (linalg.rs:307-315)
+    // off-diagonal norm (linalg.rs:307-315): the entries above the diagonal
     dd acc = dd{0.0, 0.0};
     for (int p = threadIdx.x; p < n * n; p += BT)
-      if (p % n > p / n) acc = dd_add(acc, dd_mul(A[p], A[p]));
+      if (p % n > p / n) {
+        const dd v = Ap[packed_index(p / n, p % n)];
+        acc = dd_add(acc, dd_mul(v, v));
+      }
     for (int w = 16; w; w >>= 1) {
       dd t;
       t.hi = __shfl_xor_sync(0xffffffffu, acc.hi, w);
@@ -300,9 +319,9 @@ __global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __res
         dd c = dd_from(1.0), sr = dd_from(0.0), t = dd_from(0.0);
         int rot = 0;
         if (q < n) {
-          const dd apq = A[(size_t)p * n + q];
+          const dd apq = Ap[packed_index(q, p)];
           if (!dd_lt(dd_abs(apq), dd_from(1e-60))) {  // linalg.rs:326-335
-            const dd app = A[(size_t)p * n + p], aqq = A[(size_t)q * n + q];
+            const dd app = Ap[packed_index(p, p)], aqq = Ap[packed_index(q, q)];
             const dd tau = dd_div(dd_sub(aqq, app), dd_mul(dd_from(2.0), apq));
             const dd tden = dd_add(dd_abs(tau), dd_sqrt(dd_add(dd_from(1.0), dd_mul(tau, tau))));
             t = tau.hi >= 0.0 ? dd_div(dd_from(1.0), tden) : dd_div(dd_neg(dd_from(1.0)), tden);
@@ -322,45 +341,71 @@ __global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __res
         tt[k] = t;
       }
       __syncthreads();
-      // columns p, q of A and V (linalg.rs:342-357)
+      // 2 x 2 blocks of A: rows of pair k1, columns of pair k2
+      for (int b = threadIdx.x; b < nblocks; b += BT) {
+        int k2 = (int)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
+        while (k2 * (k2 + 1) / 2 > b) k2--;
+        while ((k2 + 1) * (k2 + 2) / 2 <= b) k2++;
+        const int k1 = b - k2 * (k2 + 1) / 2;
+        const int r1 = prs[k1][2], r2 = prs[k2][2];
+        if (k1 == k2) {
+          if (r1) {  // linalg.rs:337-340
+            const int p = prs[k1][0], q = prs[k1][1];
+            Ap[packed_index(p, p)] = dd_sub(old[k1][0], dd_mul(tt[k1], old[k1][2]));
+            Ap[packed_index(q, q)] = dd_add(old[k1][1], dd_mul(tt[k1], old[k1][2]));
+            Ap[packed_index(q, p)] = dd{0.0, 0.0};
+          }
+          continue;
+        }
+        if (!r1 && !r2) continue;
+        const int rows[2] = {prs[k1][0], prs[k1][1]}, cols[2] = {prs[k2][0], prs[k2][1]};
+        dd x[2][2];
+#pragma unroll
+        for (int u = 0; u < 2; u++)
+#pragma unroll
+          for (int v = 0; v < 2; v++)
+            x[u][v] = rows[u] < n && cols[v] < n ? Ap[packed_index(rows[u], cols[v])] : dd{0.0, 0.0};
+        if (r2) {  // A J: columns p2, q2
+          const dd c = cs[k2][0], sr = cs[k2][1];
+#pragma unroll
+          for (int u = 0; u < 2; u++) {
+            const dd arp = x[u][0], arq = x[u][1];
+            x[u][0] = dd_sub(dd_mul(c, arp), dd_mul(sr, arq));
+            x[u][1] = dd_add(dd_mul(sr, arp), dd_mul(c, arq));
+          }
+        }
+        if (r1) {  // J^T (A J): rows p1, q1
+          const dd c = cs[k1][0], sr = cs[k1][1];
+#pragma unroll
+          for (int v = 0; v < 2; v++) {
+            const dd apr = x[0][v], aqr = x[1][v];
+            x[0][v] = dd_sub(dd_mul(c, apr), dd_mul(sr, aqr));
+            x[1][v] = dd_add(dd_mul(sr, apr), dd_mul(c, aqr));
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 2; u++)
+#pragma unroll
+          for (int v = 0; v < 2; v++)
+            if (rows[u] < n && cols[v] < n) Ap[packed_index(rows[u], cols[v])] = x[u][v];
+      }
+      // columns p, q of V (rows p, q of Vt)
       for (int e = threadIdx.x; e < half * n; e += BT) {
         const int k = e / n, row = e % n;
         if (!prs[k][2]) continue;
         const int p = prs[k][0], q = prs[k][1];
         const dd c = cs[k][0], sr = cs[k][1];
-        const dd arp = A[(size_t)row * n + p], arq = A[(size_t)row * n + q];
-        A[(size_t)row * n + p] = dd_sub(dd_mul(c, arp), dd_mul(sr, arq));
-        A[(size_t)row * n + q] = dd_add(dd_mul(sr, arp), dd_mul(c, arq));
-        const dd vrp = V[(size_t)row * n + p], vrq = V[(size_t)row * n + q];
-        V[(size_t)row * n + p] = dd_sub(dd_mul(c, vrp), dd_mul(sr, vrq));
-        V[(size_t)row * n + q] = dd_add(dd_mul(sr, vrp), dd_mul(c, vrq));
-      }
-      __syncthreads();
-      // rows p, q of A
-      for (int e = threadIdx.x; e < half * n; e += BT) {
-        const int k = e / n, col = e % n;
-        if (!prs[k][2]) continue;
-        const int p = prs[k][0], q = prs[k][1];
-        const dd c = cs[k][0], sr = cs[k][1];
-        const dd apr = A[(size_t)p * n + col], aqr = A[(size_t)q * n + col];
-        A[(size_t)p * n + col] = dd_sub(dd_mul(c, apr), dd_mul(sr, aqr));
-        A[(size_t)q * n + col] = dd_add(dd_mul(sr, apr), dd_mul(c, aqr));
-      }
-      __syncthreads();
-      if (threadIdx.x < half && prs[threadIdx.x][2]) {  // linalg.rs:337-340
-        const int k = threadIdx.x, p = prs[k][0], q = prs[k][1];
-        A[(size_t)p * n + p] = dd_sub(old[k][0], dd_mul(tt[k], old[k][2]));
-        A[(size_t)q * n + q] = dd_add(old[k][1], dd_mul(tt[k], old[k][2]));
-        A[(size_t)p * n + q] = dd{0.0, 0.0};
-        A[(size_t)q * n + p] = dd{0.0, 0.0};
+        const dd vrp = Vt[(size_t)p * n + row], vrq = Vt[(size_t)q * n + row];
+        Vt[(size_t)p * n + row] = dd_sub(dd_mul(c, vrp), dd_mul(sr, vrq));
+        Vt[(size_t)q * n + row] = dd_add(dd_mul(sr, vrp), dd_mul(c, vrq));
       }
       __syncthreads();
     }
   }
   dd* ev = evals + n_off[sys];
   dd* vo = evecs + mat_off[sys];
-  for (int i = threadIdx.x; i < n; i += BT) ev[i] = A[(size_t)i * n + i];
-  for (int p = threadIdx.x; p < n * n; p += BT) vo[p] = V[(size_t)(p % n) * n + p / n];  // rows = eigenvectors
+  for (int i = threadIdx.x; i < n; i += BT) ev[i] = Ap[packed_index(i, i)];
+  for (int p = threadIdx.x; p < n * n; p += BT) vo[p] = Vt[p];  // rows = eigenvectors
   if (threadIdx.x == 0) {
     sweeps_out[sys] = sweep;
     status[sys] = converged ? HP_OK : HP_ERR_NO_CONVERGE;
@@ -461,12 +506,14 @@ int batched_jacobi(int count, const int64_t* n_off, const int64_t* mat_off, cons
     set_error("batched jacobi: n <= 128 supported (got %d)", nmax);
     return HP_ERR_UNSUPPORTED;
   }
-  const int64_t slot = (int64_t)nmax * nmax;
-  DevBuf work((size_t)count * 2 * slot * 16, s);
+  const int64_t slot = (int64_t)nmax * nmax;  // V^T of each matrix
+  DevBuf work((size_t)count * slot * 16, s);
   if (!work.p) return HP_ERR_CUDA;
-  batched_jacobi_kernel<<<count, BT, 0, s>>>(n_off, mat_off, reinterpret_cast<const dd*>(A), reinterpret_cast<dd*>(evals),
-                                             reinterpret_cast<dd*>(evecs), sweeps, status, work.as<dd>(), slot,
-                                             max_sweeps);
+  const int smem = nmax * (nmax + 1) / 2 * 16;  // packed lower triangle of the largest matrix
+  HP_CUDA_TRY(cudaFuncSetAttribute(batched_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  batched_jacobi_kernel<<<count, BT, smem, s>>>(n_off, mat_off, reinterpret_cast<const dd*>(A),
+                                                reinterpret_cast<dd*>(evals), reinterpret_cast<dd*>(evecs), sweeps,
+                                                status, work.as<dd>(), slot, max_sweeps);
   HP_LAUNCH_CHECK();
   return HP_OK;
 }
