@@ -250,7 +250,8 @@ __device__ __forceinline__ int rr_player(int slot, int round, int nn) {
 // rotation of pair k2 and then the row rotation of pair k1, the order of
 // A J followed by J^T (A J) -- with the diagonal blocks set by the
 // reference's formulas (linalg.rs:337-340), and V's columns rotated
-// (linalg.rs:342-357).
+// (linalg.rs:342-357). The rotations of off-diagonal entries and of V use
+// the fused dd_rot_fast (f128 accuracy, not the reference's operation order).
 __device__ __forceinline__ int packed_index(int i, int j) {  // lower triangle, row-major
   return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i;
 }
@@ -368,20 +369,12 @@ __global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __res
         if (r2) {  // A J: columns p2, q2
           const dd c = cs[k2][0], sr = cs[k2][1];
 #pragma unroll
-          for (int u = 0; u < 2; u++) {
-            const dd arp = x[u][0], arq = x[u][1];
-            x[u][0] = dd_sub(dd_mul(c, arp), dd_mul(sr, arq));
-            x[u][1] = dd_add(dd_mul(sr, arp), dd_mul(c, arq));
-          }
+          for (int u = 0; u < 2; u++) dd_rot_fast(c, sr, x[u][0], x[u][1], x[u][0], x[u][1]);
         }
         if (r1) {  // J^T (A J): rows p1, q1
           const dd c = cs[k1][0], sr = cs[k1][1];
 #pragma unroll
-          for (int v = 0; v < 2; v++) {
-            const dd apr = x[0][v], aqr = x[1][v];
-            x[0][v] = dd_sub(dd_mul(c, apr), dd_mul(sr, aqr));
-            x[1][v] = dd_add(dd_mul(sr, apr), dd_mul(c, aqr));
-          }
+          for (int v = 0; v < 2; v++) dd_rot_fast(c, sr, x[0][v], x[1][v], x[0][v], x[1][v]);
         }
 #pragma unroll
         for (int u = 0; u < 2; u++)
@@ -395,9 +388,10 @@ __global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __res
         if (!prs[k][2]) continue;
         const int p = prs[k][0], q = prs[k][1];
         const dd c = cs[k][0], sr = cs[k][1];
-        const dd vrp = Vt[(size_t)p * n + row], vrq = Vt[(size_t)q * n + row];
-        Vt[(size_t)p * n + row] = dd_sub(dd_mul(c, vrp), dd_mul(sr, vrq));
-        Vt[(size_t)q * n + row] = dd_add(dd_mul(sr, vrp), dd_mul(c, vrq));
+        dd vp, vq;
+        dd_rot_fast(c, sr, Vt[(size_t)p * n + row], Vt[(size_t)q * n + row], vp, vq);
+        Vt[(size_t)p * n + row] = vp;
+        Vt[(size_t)q * n + row] = vq;
       }
       __syncthreads();
     }

@@ -148,6 +148,24 @@ __device__ __forceinline__ dd dd_fms_fast(dd a, dd b, dd c) {
   const double e = __dadd_rn(se, __dsub_rn(a.lo, __dadd_rn(pe, t)));
   return dd_renorm(s, e);
 }
+// Plane rotation of a pair, x = c a - s b and y = s a + c b, each output as
+// the exact products of the high parts (FMA error terms), the cross terms,
+// one two_sum of the high products and a final renormalisation: 17
+// operations per output instead of the 40 of a reference-order multiply,
+// multiply and add. Error below ~4 2^-104 (|c a| + |s b|), as for
+// dd_fms_fast.
+__device__ __forceinline__ dd dd_dot2_fast(dd c, dd a, dd s, dd b) {  // c a + s b
+  const double p1 = __dmul_rn(c.hi, a.hi), e1 = __fma_rn(c.hi, a.hi, -p1);
+  const double p2 = __dmul_rn(s.hi, b.hi), e2 = __fma_rn(s.hi, b.hi, -p2);
+  const double t = __fma_rn(c.hi, a.lo, __fma_rn(c.lo, a.hi, __fma_rn(s.hi, b.lo, __dmul_rn(s.lo, b.hi))));
+  double h, he;
+  two_sum(p1, p2, h, he);
+  return dd_renorm(h, __dadd_rn(he, __dadd_rn(__dadd_rn(e1, e2), t)));
+}
+__device__ __forceinline__ void dd_rot_fast(dd c, dd s, dd a, dd b, dd& x, dd& y) {
+  x = dd_dot2_fast(c, a, dd{-s.hi, -s.lo}, b);
+  y = dd_dot2_fast(s, a, c, b);
+}
 // 1/sqrt(d) to ~2^-103 from the f64 seed x = rsqrt(d.hi) (relative error
 // delta of a few 2^-53) by one Newton step x1 = x + x e / 2, e = 1 - d x^2.
 // e is ~delta, so it is needed only to ~2^-104 absolute: with x^2 = s + s'

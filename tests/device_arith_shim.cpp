@@ -93,6 +93,16 @@ long sh_div_small_mismatches(long per_divisor, int max_divisor, unsigned long lo
   }
   return bad;
 }
+// dd_dot2_fast (the fused rotation of the batched Jacobi): o = c a + s b
+// for count f128 entries of each operand.
+void sh_dd_dot2(const double* c, const double* a, const double* s, const double* b, double* o, long count) {
+  for (long i = 0; i < count; i++) {
+    const dd r = dd_dot2_fast(dd{c[2 * i], c[2 * i + 1]}, dd{a[2 * i], a[2 * i + 1]}, dd{s[2 * i], s[2 * i + 1]},
+                              dd{b[2 * i], b[2 * i + 1]});
+    o[2 * i] = r.hi;
+    o[2 * i + 1] = r.lo;
+  }
+}
 // Many ops at once (count entries of 2 or 4 limbs each).
 void sh_batch(int op, const double* a, const double* b, double* o, long count) {
   for (long i = 0; i < count; i++) {

@@ -122,3 +122,39 @@ def test_div_small_int_is_correctly_rounded(shim):
     shim.sh_div_small_mismatches.restype = ctypes.c_long
     shim.sh_div_small_mismatches.argtypes = [ctypes.c_long, ctypes.c_int, ctypes.c_ulonglong]
     assert shim.sh_div_small_mismatches(1000000, 40, 2024) == 0
+
+
+def test_dd_dot2_fast_error_bound(shim):
+    """dd_dot2_fast (the batched Jacobi's fused rotation, c a + s b) against
+    exact rational arithmetic: error below 4 2^-104 (|c a| + |s b|), on
+    rotation pairs (c^2 + s^2 = 1 to f128) and operands of mixed magnitude,
+    including near-total cancellation."""
+    from fractions import Fraction as F
+
+    shim.sh_dd_dot2.argtypes = [ctypes.c_void_p] * 5 + [ctypes.c_long]
+    rng = np.random.default_rng(77)
+    n = 4000
+    th = rng.uniform(-np.pi, np.pi, n)
+    c = np.stack([np.cos(th), np.zeros(n)], -1)
+    s = np.stack([np.sin(th), np.zeros(n)], -1)
+    c[:, 1] = c[:, 0] * 2.0 ** -53 * rng.uniform(-1, 1, n)
+    s[:, 1] = s[:, 0] * 2.0 ** -53 * rng.uniform(-1, 1, n)
+    a, b = rand_dd(rng, n, spread=20), rand_dd(rng, n, spread=20)
+    # cancellation: b ~ -c a / s
+    k = n // 4
+    for i in range(k):
+        ci = F(c[i, 0]) + F(c[i, 1])
+        si = F(s[i, 0]) + F(s[i, 1])
+        if si != 0:
+            t = -ci * (F(a[i, 0]) + F(a[i, 1])) / si
+            hi = float(t)
+            b[i] = [hi, float(t - F(hi))]
+    o = np.zeros((n, 2))
+    arrs = [np.ascontiguousarray(x) for x in (c, a, s, b)]
+    shim.sh_dd_dot2(*(x.ctypes.data for x in arrs), o.ctypes.data, n)
+    for i in range(n):
+        cv, av, sv, bv = (F(x[i, 0]) + F(x[i, 1]) for x in (c, a, s, b))
+        exact = cv * av + sv * bv
+        got = F(o[i, 0]) + F(o[i, 1])
+        bound = F(4) * F(2) ** -104 * (abs(cv * av) + abs(sv * bv))
+        assert abs(got - exact) <= bound, (i, float(abs(got - exact)), float(bound))
