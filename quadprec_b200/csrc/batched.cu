@@ -21,8 +21,10 @@
 // disjoint rotations at once, n-1 rounds per sweep. Rotation formulas, skip
 // rule (|a_pq| < 1e-60), stopping rule (off-norm < 1e-30 at the start of a
 // sweep) and the row-eigenvector output follow linalg.rs:299-362; the
-// rotation order differs (parallel instead of sequential), so results agree
-// with the reference to rounding, not bit-for-bit.
+// rotation order differs (parallel instead of sequential) and the rotations
+// are evaluated with the chosen-path f128 helpers (reciprocal, 1/sqrt,
+// fused plane rotation), so results agree with the reference to f128
+// rounding, not bit-for-bit.
 #include <algorithm>
 #include <vector>
 
@@ -322,11 +324,15 @@ __global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __res
         if (q < n) {
           const dd apq = Ap[packed_index(q, p)];
           if (!dd_lt(dd_abs(apq), dd_from(1e-60))) {  // linalg.rs:326-335
+            // the reference's formulas with the chosen-path reciprocal and
+            // 1/sqrt (f128 accuracy; the round's pivot chain is shorter)
             const dd app = Ap[packed_index(p, p)], aqq = Ap[packed_index(q, q)];
-            const dd tau = dd_div(dd_sub(aqq, app), dd_mul(dd_from(2.0), apq));
-            const dd tden = dd_add(dd_abs(tau), dd_sqrt(dd_add(dd_from(1.0), dd_mul(tau, tau))));
-            t = tau.hi >= 0.0 ? dd_div(dd_from(1.0), tden) : dd_div(dd_neg(dd_from(1.0)), tden);
-            c = dd_div(dd_from(1.0), dd_sqrt(dd_add(dd_from(1.0), dd_mul(t, t))));
+            const dd tau = dd_mul(dd_sub(aqq, app), dd_recip_fast(dd_mul(dd_from(2.0), apq)));
+            const dd y = dd_add(dd_from(1.0), dd_mul(tau, tau));
+            const dd tden = dd_add(dd_abs(tau), dd_mul(y, dd_rsqrt_fast(y)));  // |tau| + sqrt(1 + tau^2)
+            t = dd_recip_fast(tden);
+            if (tau.hi < 0.0) t = dd_neg(t);
+            c = dd_rsqrt_fast(dd_add(dd_from(1.0), dd_mul(t, t)));
             sr = dd_mul(t, c);
             old[k][0] = app;
             old[k][1] = aqq;

@@ -166,6 +166,16 @@ __device__ __forceinline__ void dd_rot_fast(dd c, dd s, dd a, dd b, dd& x, dd& y
   x = dd_dot2_fast(c, a, dd{-s.hi, -s.lo}, b);
   y = dd_dot2_fast(s, a, c, b);
 }
+// 1/d to ~2^-103 from the correctly rounded f64 seed x = 1/d.hi by one
+// Newton step x1 = x + x e, e = 1 - d x (relative error of x at most
+// 2^-53, so e, of that size, is needed only to ~2^-104 absolute: the fma
+// gives 1 - d.hi x to 2^-106, d.lo x is its small correction); the
+// result's error is delta^2 + O(2^-104).
+__device__ __forceinline__ dd dd_recip_fast(dd d) {
+  const double x = __drcp_rn(d.hi);
+  const double e = __fma_rn(-d.lo, x, __fma_rn(-d.hi, x, 1.0));
+  return dd_renorm(x, __dmul_rn(x, e));
+}
 // 1/sqrt(d) to ~2^-103 from the f64 seed x = rsqrt(d.hi) (relative error
 // delta of a few 2^-53) by one Newton step x1 = x + x e / 2, e = 1 - d x^2.
 // e is ~delta, so it is needed only to ~2^-104 absolute: with x^2 = s + s'

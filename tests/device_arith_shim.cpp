@@ -14,6 +14,7 @@ static inline double __dsub_rn(double a, double b) { return a - b; }
 static inline double __dmul_rn(double a, double b) { return a * b; }
 static inline double __ddiv_rn(double a, double b) { return a / b; }
 static inline double __fma_rn(double a, double b, double c) { return std::fma(a, b, c); }
+static inline double __drcp_rn(double a) { return 1.0 / a; }
 static inline double __dsqrt_rn(double a) { return std::sqrt(a); }
 // seed of the chosen-path 1/sqrt helper (not compared bit-for-bit here)
 static inline double rsqrt(double a) { return 1.0 / std::sqrt(a); }
@@ -113,6 +114,12 @@ void sh_batch(int op, const double* a, const double* b, double* o, long count) {
       case 3: sh_dd_sqrt(a + 2 * i, o + 2 * i); break;
       case 4: sh_dd_recip(a + 2 * i, o + 2 * i); break;
       case 5: sh_dd_exp(a + 2 * i, o + 2 * i); break;
+      case 6: {  // chosen-path reciprocal (error bound checked, not bits)
+        const dd r = dd_recip_fast(dd{a[2 * i], a[2 * i + 1]});
+        o[2 * i] = r.hi;
+        o[2 * i + 1] = r.lo;
+        break;
+      }
       case 10: sh_qd_add(a + 4 * i, b + 4 * i, o + 4 * i); break;
       case 11: sh_qd_mul(a + 4 * i, b + 4 * i, o + 4 * i); break;
       case 12: sh_qd_div(a + 4 * i, b + 4 * i, o + 4 * i); break;

@@ -158,3 +158,19 @@ def test_dd_dot2_fast_error_bound(shim):
         got = F(o[i, 0]) + F(o[i, 1])
         bound = F(4) * F(2) ** -104 * (abs(cv * av) + abs(sv * bv))
         assert abs(got - exact) <= bound, (i, float(abs(got - exact)), float(bound))
+
+
+def test_dd_recip_fast_error_bound(shim):
+    """dd_recip_fast (the batched Jacobi's rotation parameters): relative
+    error below 2^-102 against exact rationals, over magnitudes 2^+-300 and
+    both signs."""
+    from fractions import Fraction as F
+
+    rng = np.random.default_rng(78)
+    n = 4000
+    d = rand_dd(rng, n, spread=300)
+    o = run(shim, 6, d, None, 2)
+    for i in range(n):
+        dv = F(d[i, 0]) + F(d[i, 1])
+        got = F(o[i, 0]) + F(o[i, 1])
+        assert abs(got * dv - 1) <= F(2) ** -102, (i, d[i], o[i])
