@@ -249,12 +249,27 @@ int hp_f128_jacobi_eigen_batched_dev(int count, const int64_t* n_off, const doub
     acc += n * n;
     nmax = std::max<int>(nmax, (int)n);
   }
-  DevBuf doff((count + 1) * 8, s), dmat(count * 8, s);
-  if (!doff.p || !dmat.p) return HP_ERR_CUDA;
+  // largest first; the matrices above JACOBI_SMALL_N go in the first launch
+  std::vector<int> order(count);
+  for (int i = 0; i < count; i++) order[i] = i;
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+    return n_off[x + 1] - n_off[x] > n_off[y + 1] - n_off[y];
+  });
+  int count_big = 0, nmax_small = 0;
+  for (int i : order) {
+    const int n = (int)(n_off[i + 1] - n_off[i]);
+    if (n > JACOBI_SMALL_N)
+      count_big++;
+    else
+      nmax_small = std::max(nmax_small, n);
+  }
+  DevBuf doff((count + 1) * 8, s), dmat(count * 8, s), dord(count * sizeof(int), s);
+  if (!doff.p || !dmat.p || !dord.p) return HP_ERR_CUDA;
   HP_CUDA_TRY(cudaMemcpyAsync(doff.p, n_off, (count + 1) * 8, cudaMemcpyHostToDevice, s));
   HP_CUDA_TRY(cudaMemcpyAsync(dmat.p, mat.data(), count * 8, cudaMemcpyHostToDevice, s));
+  HP_CUDA_TRY(cudaMemcpyAsync(dord.p, order.data(), count * sizeof(int), cudaMemcpyHostToDevice, s));
   HP_TRY(batched_jacobi(count, doff.as<int64_t>(), dmat.as<int64_t>(), A, evals, evecs, sweeps, status, nmax,
-                        (int)std::min<size_t>(max_iter, 1 << 30), s));
+                        (int)std::min<size_t>(max_iter, 1 << 30), s, dord.as<int>(), count_big, nmax_small));
   HP_CUDA_TRY(cudaStreamSynchronize(s));
   return HP_OK;
 }

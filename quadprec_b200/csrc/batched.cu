@@ -257,12 +257,14 @@ __device__ __forceinline__ int rr_player(int slot, int round, int nn) {
 __device__ __forceinline__ int packed_index(int i, int j) {  // lower triangle, row-major
   return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i;
 }
+// CTA b takes matrix order[b] (b itself without an order) and the V slot b.
 __global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __restrict__ n_off,
                                                             const int64_t* __restrict__ mat_off,
                                                             const dd* __restrict__ Ain, dd* __restrict__ evals,
                                                             dd* __restrict__ evecs, int* __restrict__ sweeps_out,
                                                             int* __restrict__ status, dd* __restrict__ work,
-                                                            int64_t slot_elems, int max_sweeps) {
+                                                            int64_t slot_elems, int max_sweeps,
+                                                            const int* __restrict__ order) {
   extern __shared__ __align__(16) unsigned char sm_raw[];
   dd* Ap = reinterpret_cast<dd*>(sm_raw);  // packed lower triangle of A
   __shared__ dd cs[64][2];
@@ -271,7 +273,10 @@ __global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __res
   __shared__ int prs[64][3];  // p, q, rotated?
   __shared__ dd red[BT / 32];
   __shared__ int stop;
-  const int sys = blockIdx.x;
+  // a launch that follows this one on the stream works on other matrices:
+  // let it start on SMs this one leaves free
+  asm volatile("griddepcontrol.launch_dependents;");
+  const int sys = order ? order[blockIdx.x] : (int)blockIdx.x;
   const int n = (int)(n_off[sys + 1] - n_off[sys]);
   const dd* Asrc = Ain + mat_off[sys];
   dd* Vt = work + (size_t)blockIdx.x * slot_elems;
@@ -500,21 +505,39 @@ int batched_spd(int count, const int* order, const int64_t* off, const double* c
 }
 
 int batched_jacobi(int count, const int64_t* n_off, const int64_t* mat_off, const double* A, double* evals,
-                   double* evecs, int* sweeps, int* status, int nmax, int max_sweeps, cudaStream_t s) {
+                   double* evecs, int* sweeps, int* status, int nmax, int max_sweeps, cudaStream_t s,
+                   const int* order, int count_big, int nmax_small) {
   if (count == 0) return HP_OK;
   if (nmax > 128) {
     set_error("batched jacobi: n <= 128 supported (got %d)", nmax);
     return HP_ERR_UNSUPPORTED;
   }
+  if (!order) count_big = count;
   const int64_t slot = (int64_t)nmax * nmax;  // V^T of each matrix
   DevBuf work((size_t)count * slot * 16, s);
   if (!work.p) return HP_ERR_CUDA;
-  const int smem = nmax * (nmax + 1) / 2 * 16;  // packed lower triangle of the largest matrix
-  HP_CUDA_TRY(cudaFuncSetAttribute(batched_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  batched_jacobi_kernel<<<count, BT, smem, s>>>(n_off, mat_off, reinterpret_cast<const dd*>(A),
-                                                reinterpret_cast<dd*>(evals), reinterpret_cast<dd*>(evecs), sweeps,
-                                                status, work.as<dd>(), slot, max_sweeps);
-  HP_LAUNCH_CHECK();
+  // the packed lower triangle of each launch's largest matrix
+  auto smem_for = [](int m) { return m * (m + 1) / 2 * 16; };
+  HP_CUDA_TRY(cudaFuncSetAttribute(batched_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_for(nmax)));
+  auto launch = [&](int first, int cnt, int m, bool pdl) -> cudaError_t {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)cnt);
+    cfg.blockDim = dim3(BT);
+    cfg.dynamicSmemBytes = smem_for(m);
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? at : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    return cudaLaunchKernelEx(&cfg, batched_jacobi_kernel, n_off, mat_off, reinterpret_cast<const dd*>(A),
+                              reinterpret_cast<dd*>(evals), reinterpret_cast<dd*>(evecs), sweeps, status,
+                              work.as<dd>() + (size_t)first * slot, slot, max_sweeps, order ? order + first : order);
+  };
+  // the large matrices (one CTA per SM by shared memory), then the small
+  // ones, which start on the SMs the large ones' last wave leaves free
+  if (count_big > 0) HP_CUDA_TRY(launch(0, count_big, nmax, false));
+  if (count_big < count) HP_CUDA_TRY(launch(count_big, count - count_big, nmax_small, count_big > 0));
   return HP_OK;
 }
 

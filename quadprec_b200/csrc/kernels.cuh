@@ -114,8 +114,13 @@ int batched_spd(int count, const int* order, const int64_t* off, const double* c
 int batched_spd_launch(int count, const int* order, const int64_t* off, const double* centers, const double* alpha,
                        const double* b, double* x, int* status, int* iters, int nmax, double tol, int max_iter,
                        void* work, int* queue, const BatchedConfig& cfg, cudaStream_t s);
+// order (device, optional): matrices largest first; the first count_big
+// (n > JACOBI_SMALL_N) run in one launch, the rest (n <= nmax_small) in a
+// second one with less shared memory per CTA.
+constexpr int JACOBI_SMALL_N = 80;
 int batched_jacobi(int count, const int64_t* n_off, const int64_t* mat_off, const double* A, double* evals,
-                   double* evecs, int* sweeps, int* status, int nmax, int max_sweeps, cudaStream_t s);
+                   double* evecs, int* sweeps, int* status, int nmax, int max_sweeps, cudaStream_t s,
+                   const int* order = nullptr, int count_big = -1, int nmax_small = 0);
 int batched_assemble(int count, const int64_t* off, const double* centers, const double* alpha,
                      const int64_t* mat_off, double* S, cudaStream_t s);
 }  // namespace hp
