@@ -64,7 +64,7 @@ int tuned_config(int count, const int* order, const int64_t* off, const double* 
       return HP_OK;
     }
   }
-  std::vector<BatchedConfig> cands = autotune_enabled() ? batched_spd_candidates() : std::vector<BatchedConfig>{};
+  std::vector<BatchedConfig> cands = autotune_enabled() ? batched_spd_candidates(nmax) : std::vector<BatchedConfig>{};
   BatchedConfig best = kDefaultConfig;
   if (cands.size() > 1) {
     int gmax = 0;
@@ -162,6 +162,7 @@ int hp_spd_solve_batched_dev(int count, const int64_t* offsets, const double* ce
   const int grid = batched_spd_grid(cfg);
   HP_CUDA_TRY(cudaMalloc(&g_cache.work, batched_spd_work_bytes(grid, nmax)));
   HP_CUDA_TRY(cudaMalloc(&g_cache.queue, sizeof(int)));
+  HP_TRY(batched_spd_prepare(nmax));
   cudaStream_t cap;
   HP_CUDA_TRY(cudaStreamCreateWithFlags(&cap, cudaStreamNonBlocking));
   HP_CUDA_TRY(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal));

@@ -26,6 +26,7 @@
 // fused plane rotation), so results agree with the reference to f128
 // rounding, not bit-for-bit.
 #include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "hp_arith.cuh"
@@ -38,6 +39,7 @@ namespace hp {
 namespace {
 
 constexpr int BT = 512;  // threads per CTA
+constexpr int SPD_PANEL = 8;  // columns per panel of the batched Cholesky
 
 template <int NT>
 __device__ double block_max(double v, double* red) {
@@ -96,8 +98,11 @@ __global__ void __launch_bounds__(NT) batched_spd_kernel(int count, const int* _
                                                          dd* __restrict__ x_out, int* __restrict__ status,
                                                          int* __restrict__ iters, int* queue, dd* __restrict__ work,
                                                          int64_t slot_elems, double tol, int max_iter) {
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  dd* P = reinterpret_cast<dd*>(sm_raw);  // Cholesky panel: rows jb..n-1 x SPD_PANEL columns
   __shared__ int sys_sh;
   __shared__ dd bc;
+  __shared__ dd head[SPD_PANEL];  // scaled entries of the pivot's column at the panel's rows
   __shared__ double red[NT / 32];
   __shared__ int fail;
   dd* S = work + (size_t)blockIdx.x * 2 * slot_elems;
@@ -131,30 +136,57 @@ __global__ void __launch_bounds__(NT) batched_spd_kernel(int count, const int* _
       L[(size_t)i * n + j] = v;
     }
     __syncthreads();
-    // 2. right-looking Cholesky
-    for (int j = 0; j < n; j++) {
-      if (threadIdx.x == 0) {
-        const dd d = L[(size_t)j * n + j];
-        if (!(d.hi > 0.0)) {
-          fail = 1;
-        } else {
-          const dd rs = dd_rsqrt_fast(d);
-          L[(size_t)j * n + j] = dd_mul(d, rs);
-          rd[j] = rs;
-          bc = rs;
-        }
+    // 2. right-looking Cholesky in panels of SPD_PANEL columns: the panel
+    //    (its rows jb..n-1) is factored in shared memory, then the trailing
+    //    matrix takes the panel's columns in one pass per entry. Every entry
+    //    receives its column updates one at a time in column order with the
+    //    same operands as the column-by-column form, so the factor is the same.
+    for (int jb = 0; jb < n && !fail; jb += SPD_PANEL) {
+      const int kw = min(SPD_PANEL, n - jb), rows = n - jb;
+      for (int q = threadIdx.x; q < rows * kw; q += NT) {
+        const int r = q / kw, c = q % kw;
+        if (r >= c) P[r * SPD_PANEL + c] = L[(size_t)(jb + r) * n + jb + c];
       }
       __syncthreads();
+      for (int c = 0; c < kw; c++) {
+        if (threadIdx.x == 0) {
+          const dd d = P[c * SPD_PANEL + c];
+          if (!(d.hi > 0.0)) {
+            fail = 1;
+          } else {
+            const dd rs = dd_rsqrt_fast(d);
+            P[c * SPD_PANEL + c] = dd_mul(d, rs);
+            rd[jb + c] = rs;
+            bc = rs;
+            for (int c2 = c + 1; c2 < kw; c2++) head[c2] = dd_mul(P[c2 * SPD_PANEL + c], rs);  // l_{c2, c}
+          }
+        }
+        __syncthreads();
+        if (fail) break;
+        const dd rs = bc;
+        for (int r = c + 1 + threadIdx.x; r < rows; r += NT) {
+          const dd lrc = dd_mul(P[r * SPD_PANEL + c], rs);
+          P[r * SPD_PANEL + c] = lrc;
+          for (int c2 = c + 1; c2 < kw && c2 <= r; c2++)
+            P[r * SPD_PANEL + c2] = dd_fms_fast(P[r * SPD_PANEL + c2], lrc, head[c2]);
+        }
+        __syncthreads();
+      }
       if (fail) break;
-      const dd rs = bc;
-      for (int i = j + 1 + threadIdx.x; i < n; i += NT) L[(size_t)i * n + j] = dd_mul(L[(size_t)i * n + j], rs);
-      __syncthreads();
+      for (int q = threadIdx.x; q < rows * kw; q += NT) {  // the factored panel back to L
+        const int r = q / kw, c = q % kw;
+        if (r >= c) L[(size_t)(jb + r) * n + jb + c] = P[r * SPD_PANEL + c];
+      }
       {  // trailing update: one warp per row, lanes along k <= i
         const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
-        for (int i = j + 1 + warp; i < n; i += NT / 32) {
-          const dd lij = L[(size_t)i * n + j];
-          for (int k = j + 1 + lane; k <= i; k += 32)
-            L[(size_t)i * n + k] = dd_fms_fast(L[(size_t)i * n + k], lij, L[(size_t)k * n + j]);
+        for (int i = jb + kw + warp; i < n; i += NT / 32) {
+          const dd* pi = P + (i - jb) * SPD_PANEL;
+          for (int k = jb + kw + lane; k <= i; k += 32) {
+            const dd* pk = P + (k - jb) * SPD_PANEL;
+            dd a = L[(size_t)i * n + k];
+            for (int c = 0; c < kw; c++) a = dd_fms_fast(a, pi[c], pk[c]);
+            L[(size_t)i * n + k] = a;
+          }
         }
       }
       __syncthreads();
@@ -438,15 +470,43 @@ __global__ void batched_assemble_kernel(const int64_t* __restrict__ off, const d
 // (each entry's operation sequence is independent of the CTA size and
 // count: warp-per-row updates and residual cascades, in-CTA solves with the
 // same j order, order-free max reductions), so the choice is free.
-std::vector<BatchedConfig> batched_spd_candidates() {
+// Dynamic shared memory of the persistent kernel: the Cholesky panel of the
+// largest system (its rows x SPD_PANEL columns).
+size_t batched_spd_smem(int nmax) { return (size_t)std::max(nmax, 1) * SPD_PANEL * 16; }
+constexpr size_t SPD_SMEM_MAX = 200 * 1024;  // n <= 1600
+// Raises the kernels' dynamic shared-memory limit when a batch needs more
+// than any earlier one on this device (never inside a stream capture: the
+// graph path calls this before it captures).
+int batched_spd_prepare(int nmax) {
+  static std::mutex mu;
+  static size_t set_for[64] = {};
+  const size_t smem = batched_spd_smem(nmax);
+  if (smem > SPD_SMEM_MAX) {
+    set_error("batched: systems up to n = %zu supported (got %d)", SPD_SMEM_MAX / (SPD_PANEL * 16), nmax);
+    return HP_ERR_UNSUPPORTED;
+  }
+  int dev = 0;
+  HP_CUDA_TRY(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 64 && set_for[dev] >= smem) return HP_OK;
+  HP_CUDA_TRY(cudaFuncSetAttribute(batched_spd_kernel<256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  HP_CUDA_TRY(cudaFuncSetAttribute(batched_spd_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  HP_CUDA_TRY(cudaFuncSetAttribute(batched_spd_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  if (dev < 64) set_for[dev] = smem;
+  return HP_OK;
+}
+
+std::vector<BatchedConfig> batched_spd_candidates(int nmax) {
   std::vector<BatchedConfig> out;
+  if (batched_spd_prepare(nmax) != HP_OK) return out;
+  const size_t smem = batched_spd_smem(nmax);
   const int threads[3] = {256, 512, 1024};
   for (int t : threads) {
     int nb = 0;
     cudaError_t e = cudaErrorInvalidValue;
-    if (t == 256) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batched_spd_kernel<256>, 256, 0);
-    if (t == 512) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batched_spd_kernel<512>, 512, 0);
-    if (t == 1024) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batched_spd_kernel<1024>, 1024, 0);
+    if (t == 256) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batched_spd_kernel<256>, 256, smem);
+    if (t == 512) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batched_spd_kernel<512>, 512, smem);
+    if (t == 1024) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, batched_spd_kernel<1024>, 1024, smem);
     if (e != cudaSuccess) {
       cudaGetLastError();
       continue;
@@ -473,11 +533,13 @@ int batched_spd_launch(int count, const int* order, const int64_t* off, const do
                        void* work, int* queue, const BatchedConfig& cfg, cudaStream_t s) {
   const int64_t slot = (int64_t)nmax * nmax + 2 * (int64_t)nmax;
   const int grid = batched_spd_grid(cfg);
+  HP_TRY(batched_spd_prepare(nmax));
+  const size_t smem = batched_spd_smem(nmax);
   HP_CUDA_TRY(cudaMemsetAsync(queue, 0, sizeof(int), s));
 #define HP_BATCHED_LAUNCH(NT)                                                                                      \
-  batched_spd_kernel<NT><<<grid, NT, 0, s>>>(count, order, off, centers, alpha, reinterpret_cast<const dd*>(b),  \
-                                             reinterpret_cast<dd*>(x), status, iters, queue,                       \
-                                             reinterpret_cast<dd*>(work), slot, tol, max_iter)
+  batched_spd_kernel<NT><<<grid, NT, smem, s>>>(count, order, off, centers, alpha, reinterpret_cast<const dd*>(b), \
+                                                reinterpret_cast<dd*>(x), status, iters, queue,                    \
+                                                reinterpret_cast<dd*>(work), slot, tol, max_iter)
   switch (cfg.threads) {
     case 256: HP_BATCHED_LAUNCH(256); break;
     case 512: HP_BATCHED_LAUNCH(512); break;

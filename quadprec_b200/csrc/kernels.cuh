@@ -105,7 +105,8 @@ struct BatchedConfig {
   int threads;
   int ctas_per_sm;
 };
-std::vector<BatchedConfig> batched_spd_candidates();
+std::vector<BatchedConfig> batched_spd_candidates(int nmax);  // launch shapes that fit with n <= nmax
+int batched_spd_prepare(int nmax);  // shared-memory limit for systems up to nmax (call outside a capture)
 int batched_spd_grid(const BatchedConfig& cfg);
 size_t batched_spd_work_bytes(int grid, int nmax);
 int batched_spd(int count, const int* order, const int64_t* off, const double* centers, const double* alpha,
