@@ -57,23 +57,24 @@ __device__ double block_max(double v, double* red) {
   return m;
 }
 
-// In-CTA triangular solves with L (row-major n x n, lower) and rinv[j] =
-// 1 / l_jj from the factorisation, v in place.
+// In-CTA triangular solves with L (row-major n x n; the factor below the
+// diagonal, its mirror above it, so column j is read along row j) and
+// rinv[j] = 1 / l_jj, v in place; v and rinv in shared memory. Each step's
+// first entry of L is loaded before the barrier that publishes v_j.
 template <int NT>
 __device__ void cta_trsv(const dd* L, const dd* rinv, dd* v, int n, bool upper_t, dd* bc) {
   for (int s = 0; s < n; s++) {
     const int j = upper_t ? n - 1 - s : s;
+    const int i0 = upper_t ? threadIdx.x : j + 1 + threadIdx.x, i1 = upper_t ? j : n;
+    const dd l0 = i0 < i1 ? L[(size_t)j * n + i0] : dd{0.0, 0.0};
     if (threadIdx.x == 0) {
       v[j] = dd_mul(v[j], rinv[j]);
       *bc = v[j];
     }
     __syncthreads();
     const dd vj = *bc;
-    if (!upper_t) {
-      for (int i = j + 1 + threadIdx.x; i < n; i += NT) v[i] = dd_fms_fast(v[i], L[(size_t)i * n + j], vj);
-    } else {
-      for (int i = threadIdx.x; i < j; i += NT) v[i] = dd_fms_fast(v[i], L[(size_t)j * n + i], vj);
-    }
+    if (i0 < i1) v[i0] = dd_fms_fast(v[i0], l0, vj);
+    for (int i = i0 + NT; i < i1; i += NT) v[i] = dd_fms_fast(v[i], L[(size_t)j * n + i], vj);
     __syncthreads();
   }
 }
@@ -98,8 +99,10 @@ __global__ void __launch_bounds__(NT) batched_spd_kernel(int count, const int* _
                                                          dd* __restrict__ x_out, int* __restrict__ status,
                                                          int* __restrict__ iters, int* queue, dd* __restrict__ work,
                                                          int64_t slot_elems, double tol, int max_iter) {
+  // shared memory per system: the Cholesky panel (rows jb..n-1 x SPD_PANEL
+  // columns), then x, r and 1 / l_jj (n entries each)
   extern __shared__ __align__(16) unsigned char sm_raw[];
-  dd* P = reinterpret_cast<dd*>(sm_raw);  // Cholesky panel: rows jb..n-1 x SPD_PANEL columns
+  dd* P = reinterpret_cast<dd*>(sm_raw);
   __shared__ int sys_sh;
   __shared__ dd bc;
   __shared__ dd head[SPD_PANEL];  // scaled entries of the pivot's column at the panel's rows
@@ -107,7 +110,6 @@ __global__ void __launch_bounds__(NT) batched_spd_kernel(int count, const int* _
   __shared__ int fail;
   dd* S = work + (size_t)blockIdx.x * 2 * slot_elems;
   dd* L = S + slot_elems;
-  dd* r = x_out;  // placeholder, set per system
   while (true) {
     if (threadIdx.x == 0) {
       int q = atomicAdd(queue, 1);
@@ -121,9 +123,10 @@ __global__ void __launch_bounds__(NT) batched_spd_kernel(int count, const int* _
     const int n = (int)(off[sys + 1] - o);
     const double* cen = centers + 3 * o;
     const double* al = alpha + o;
-    dd* x = x_out + o;
-    r = L + (size_t)n * n;  // residual vector after L inside the slot
-    dd* rd = r + n;           // 1 / l_jj after it
+    dd* xg = x_out + o;
+    dd* x = P + (size_t)n * SPD_PANEL;
+    dd* r = x + n;
+    dd* rd = r + n;
     // 1. assemble S (lower triangle evaluated, mirrored), copy to L
     for (int p = threadIdx.x; p < n * (n + 1) / 2; p += NT) {
       int i = (int)((sqrtf(8.0f * (float)p + 1.0f) - 1.0f) * 0.5f);
@@ -173,9 +176,10 @@ __global__ void __launch_bounds__(NT) batched_spd_kernel(int count, const int* _
         __syncthreads();
       }
       if (fail) break;
-      for (int q = threadIdx.x; q < rows * kw; q += NT) {  // the factored panel back to L
+      for (int q = threadIdx.x; q < rows * kw; q += NT) {  // the factored panel back to L, and its mirror
         const int r = q / kw, c = q % kw;
         if (r >= c) L[(size_t)(jb + r) * n + jb + c] = P[r * SPD_PANEL + c];
+        if (r > c) L[(size_t)(jb + c) * n + jb + r] = P[r * SPD_PANEL + c];
       }
       {  // trailing update: one warp per row, lanes along k <= i
         const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
@@ -259,6 +263,7 @@ __global__ void __launch_bounds__(NT) batched_spd_kernel(int count, const int* _
         break;
       }
     }
+    for (int i = threadIdx.x; i < n; i += NT) xg[i] = x[i];
     if (threadIdx.x == 0) {
       status[sys] = conv ? HP_OK : HP_ERR_NO_CONVERGE;
       iters[sys] = conv ? it : max_iter;
@@ -471,9 +476,9 @@ __global__ void batched_assemble_kernel(const int64_t* __restrict__ off, const d
 // count: warp-per-row updates and residual cascades, in-CTA solves with the
 // same j order, order-free max reductions), so the choice is free.
 // Dynamic shared memory of the persistent kernel: the Cholesky panel of the
-// largest system (its rows x SPD_PANEL columns).
-size_t batched_spd_smem(int nmax) { return (size_t)std::max(nmax, 1) * SPD_PANEL * 16; }
-constexpr size_t SPD_SMEM_MAX = 200 * 1024;  // n <= 1600
+// largest system (its rows x SPD_PANEL columns) and its x, r and 1 / l_jj.
+size_t batched_spd_smem(int nmax) { return (size_t)std::max(nmax, 1) * (SPD_PANEL + 3) * 16; }
+constexpr size_t SPD_SMEM_MAX = 200 * 1024;  // n <= 1163
 // Raises the kernels' dynamic shared-memory limit when a batch needs more
 // than any earlier one on this device (never inside a stream capture: the
 // graph path calls this before it captures).
@@ -482,7 +487,7 @@ int batched_spd_prepare(int nmax) {
   static size_t set_for[64] = {};
   const size_t smem = batched_spd_smem(nmax);
   if (smem > SPD_SMEM_MAX) {
-    set_error("batched: systems up to n = %zu supported (got %d)", SPD_SMEM_MAX / (SPD_PANEL * 16), nmax);
+    set_error("batched: systems up to n = %zu supported (got %d)", SPD_SMEM_MAX / ((SPD_PANEL + 3) * 16), nmax);
     return HP_ERR_UNSUPPORTED;
   }
   int dev = 0;
