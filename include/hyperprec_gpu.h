@@ -256,6 +256,8 @@ int hp_overlap_norm_dd_dev(size_t n, const double* centers, const double* alpha,
  * f128 assembly, Cholesky, solve, refinement with ~2^-159 residuals until
  * max|dx| <= tol max|x| (at most max_iter steps).
  * status[s] = HP_OK, HP_ERR_NOT_SPD or HP_ERR_NO_CONVERGE; iters[s] = steps.
+ * Systems up to n = 1163 (a CTA keeps its system's Cholesky panel and
+ * vectors in shared memory); a larger one returns HP_ERR_UNSUPPORTED.
  * _dev: offsets is a HOST array (count+1), everything else device memory;
  * the launch is captured in a CUDA graph on first use and replayed for
  * identical arguments. The plain form takes host arrays (b as f128).
