@@ -84,7 +84,7 @@ def to_f64(x):
     return x[..., 0] + x[..., 1]
 
 
-@pytest.mark.parametrize("n", [2, 3, 4, 7, 16, 33, 64])
+@pytest.mark.parametrize("n", [2, 3, 4, 7, 16, 33, 64, 81, 128])
 def test_jacobi_matches_reference(gpu, n):
     rng = np.random.default_rng(n)
     m = rng.standard_normal((n, n))
@@ -144,3 +144,50 @@ def test_batched_jacobi_on_overlap_matrices(gpu, small_batch):
         wr = np.sort(np.linalg.eigvalsh(to_f64(ref)))
         assert np.allclose(w, wr, atol=1e-12)
         m0 += n * n
+
+
+def test_batched_jacobi_mixed_sizes(gpu):
+    """A batch spanning both launches of the batched Jacobi (n > 80 first,
+    largest first, then the rest with less shared memory per CTA): every
+    matrix converges to eigenpairs of its own matrix, eigenvalues matching
+    numpy's to f64 rounding, in the caller's order."""
+    import torch
+
+    ns = [5, 90, 40, 128, 81, 12, 2]
+    rng = np.random.default_rng(5)
+    mats = []
+    for n in ns:
+        m = rng.standard_normal((n, n))
+        mats.append((m + m.T) / 2.0)
+    off = np.zeros(len(ns) + 1, dtype=np.int64)
+    off[1:] = np.cumsum(ns)
+    A = np.concatenate([f128m(m).reshape(-1, 2) for m in mats])
+    dA = torch.from_numpy(np.ascontiguousarray(A)).cuda()
+    ev = torch.empty((int(off[-1]), 2), dtype=torch.float64, device="cuda")
+    vec = torch.empty_like(dA)
+    sw = torch.zeros(len(ns), dtype=torch.int32, device="cuda")
+    st = torch.zeros(len(ns), dtype=torch.int32, device="cuda")
+    gpu.check(gpu.lib().hp_f128_jacobi_eigen_batched_dev(len(ns), off.ctypes.data, dA.data_ptr(), 200,
+                                                         ev.data_ptr(), vec.data_ptr(), sw.data_ptr(),
+                                                         st.data_ptr(), 0))
+    torch.cuda.synchronize()
+    assert int(st.abs().sum()) == 0
+    evh, vh = to_f64(ev.cpu().numpy()), to_f64(vec.cpu().numpy())
+    m0 = 0
+    for s, (n, m) in enumerate(zip(ns, mats)):
+        lam = evh[off[s]:off[s + 1]]
+        V = vh[m0:m0 + n * n].reshape(n, n)  # rows are eigenvectors
+        m0 += n * n
+        assert np.allclose(np.sort(lam), np.linalg.eigvalsh(m), rtol=0, atol=1e-12 * max(1.0, np.abs(m).max()))
+        assert np.allclose(V @ V.T, np.eye(n), atol=1e-13)
+        assert np.allclose(m @ V.T, V.T * lam[None, :], atol=1e-12 * max(1.0, np.abs(m).max()))
+
+
+def test_batched_solve_size_limit(gpu):
+    """Systems beyond what a CTA's shared memory holds (n > 1163) are refused
+    with HP_ERR_UNSUPPORTED, not launched."""
+    B = batched_overlap_systems(count=1, seed=9, n_min=1168, n_max=1168)
+    assert int(B["offsets"][-1]) == 1168
+    with pytest.raises(gpu.HPError) as ei:
+        gpu.spd_solve_batched(B)
+    assert ei.value.code == gpu.HP_ERR_UNSUPPORTED
