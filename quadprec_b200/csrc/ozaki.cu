@@ -273,8 +273,8 @@ __device__ __forceinline__ uint32_t mod_reduce(int32_t x, int l) {
 // Exponent pass of the f128 Ozaki GEMM in one launch. A (RA x CA,
 // row-major) contributes one exponent per row (a_rows) or per column, B
 // (RB x CB) one per column; an entry's exponent is max(e(hi), e(lo) + 1),
-// or the non-finite marker. Row blocks: 8 warps, one row each, four loads
-// in flight per lane. Column blocks: 32 columns x 8 row lanes over a slab
+// or the non-finite marker. Row blocks: 8 warps, one row each, MAXEXP_U
+// loads in flight per lane. Column blocks: 32 columns x 8 row lanes over a slab
 // of `slab` rows, merged with atomicMax into outputs zeroed beforehand.
 // Blocks [0, na) serve A, the rest B.
 __device__ __forceinline__ int entry_exp(double2 v) {
@@ -287,6 +287,7 @@ __device__ __forceinline__ int entry_exp(double4 v) {
   if (el == EXP_NONFINITE || exp_field(v.z) == EXP_NONFINITE || exp_field(v.w) == EXP_NONFINITE) return EXP_NONFINITE;
   return max(exp_field(v.x), min(el + 1, EXP_NONFINITE));
 }
+constexpr int MAXEXP_U = 8;  // loads in flight per lane
 template <class T>
 __global__ void __launch_bounds__(256) maxexp_kernel(const T* __restrict__ A, int64_t RA, int64_t CA, bool a_rows,
                                                      int* __restrict__ outA, const T* __restrict__ B, int64_t RB,
@@ -303,12 +304,12 @@ __global__ void __launch_bounds__(256) maxexp_kernel(const T* __restrict__ A, in
     if (row >= R) return;
     const T* rp = src + row * C;
     int e = 0;
-    for (int64_t p = lane; p < C; p += 128) {
-      T v[4];
+    for (int64_t p = lane; p < C; p += 32 * MAXEXP_U) {
+      T v[MAXEXP_U];
 #pragma unroll
-      for (int u = 0; u < 4; u++) v[u] = p + 32 * u < C ? rp[p + 32 * u] : T{};
+      for (int u = 0; u < MAXEXP_U; u++) v[u] = p + 32 * u < C ? rp[p + 32 * u] : T{};
 #pragma unroll
-      for (int u = 0; u < 4; u++) e = max(e, entry_exp(v[u]));
+      for (int u = 0; u < MAXEXP_U; u++) e = max(e, entry_exp(v[u]));
     }
     for (int o = 16; o; o >>= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, o));
     if (lane == 0) out[row] = e;
@@ -320,12 +321,12 @@ __global__ void __launch_bounds__(256) maxexp_kernel(const T* __restrict__ A, in
   const int64_t r0 = (int64_t)(bid / ncb) * slab, r1 = min(R, r0 + slab);
   int e = 0;
   if (c < C) {
-    for (int64_t r = r0 + wy; r < r1; r += 32) {
-      T v[4];
+    for (int64_t r = r0 + wy; r < r1; r += 8 * MAXEXP_U) {
+      T v[MAXEXP_U];
 #pragma unroll
-      for (int u = 0; u < 4; u++) v[u] = r + 8 * u < r1 ? src[(r + 8 * u) * C + c] : T{};
+      for (int u = 0; u < MAXEXP_U; u++) v[u] = r + 8 * u < r1 ? src[(r + 8 * u) * C + c] : T{};
 #pragma unroll
-      for (int u = 0; u < 4; u++) e = max(e, entry_exp(v[u]));
+      for (int u = 0; u < MAXEXP_U; u++) e = max(e, entry_exp(v[u]));
     }
   }
   red[wy][lane] = e;
