@@ -1512,7 +1512,7 @@ __device__ __forceinline__ qd crt_group_qd(const uint8_t* rp, int64_t plane, int
 // LC > 0: L == LC at compile time, tables from c_crt (weights as immediate
 // operands), moduli loop unrolled.
 template <int NC, int LC = 0>
-__global__ void __launch_bounds__(256) crt_qd_kernel(const uint8_t* __restrict__ g1, const uint8_t* __restrict__ g2,
+__global__ void __launch_bounds__(256, 4) crt_qd_kernel(const uint8_t* __restrict__ g1, const uint8_t* __restrict__ g2,
                                                      int64_t plane, int64_t Np, int64_t m, int64_t n,
                                                      const int* __restrict__ expA, const int* __restrict__ expB,
                                                      const CrtTable* __restrict__ tab, double4* __restrict__ C) {
