@@ -1157,20 +1157,24 @@ struct StreamsDrain {  // every stream idle before the buffers above it are free
     cudaStreamSynchronize(c);
   }
 };
+// The calling thread's events on the current device, created once and
+// reused by every later call (event creation would otherwise sit in front
+// of the first copy of each call).
 struct EventSet {
   std::vector<cudaEvent_t> ev;
-  explicit EventSet(size_t count) : ev(count, nullptr) {
-    for (auto& e : ev) cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+  explicit EventSet(size_t count) {
+    static thread_local std::vector<cudaEvent_t> pool[64];
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::vector<cudaEvent_t>& p = pool[dev & 63];
+    while (p.size() < count) {
+      cudaEvent_t e = nullptr;
+      if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess) break;
+      p.push_back(e);
+    }
+    if (p.size() >= count) ev.assign(p.begin(), p.begin() + count);
   }
-  ~EventSet() {
-    for (auto e : ev)
-      if (e) cudaEventDestroy(e);
-  }
-  bool ok() const {
-    for (auto e : ev)
-      if (!e) return false;
-    return true;
-  }
+  bool ok() const { return !ev.empty(); }
 };
 }  // namespace
 
