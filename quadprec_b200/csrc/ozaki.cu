@@ -1475,24 +1475,11 @@ __global__ void __launch_bounds__(256, 3) residue_qd_ab_kernel(const double4* __
 }
 
 // f256 CRT: rebuild G1 and G2, C = (G1 2^105 + G2) 2^(105 - sa - sb).
-__device__ __forceinline__ qd chunks_to_qd(const double* acc, int nc) {
-  double v[8];
-#pragma unroll
-  for (int i = 0; i < 8; i++) v[i] = 0.0;
-  // most significant chunk first
-#pragma unroll
-  for (int i = 0; i < 8; i++) {
-    const int c = nc - 1 - i;
-    if (c >= 0) v[i] = scale_pow2(acc[c], CRT_BITS * c);
-  }
-  qd r;
-  qd_renormalize_from8(v, r.l);
-  return r;
-}
+// One group's weighted residue sums -> |G| as normalised 39-bit chunks
+// acc[0..NC] (acc[NC] = 0 when |G| < M/2); returns the sign.
 template <int NC, int LC = 0, class W>
-__device__ __forceinline__ qd crt_group_qd(const uint8_t* rp, int64_t plane, int L, W w_s, const double* mch,
-                                           double inv_m) {
-  double acc[NC + 1];
+__device__ __forceinline__ bool crt_group_chunks(const uint8_t* rp, int64_t plane, int L, W w_s, const double* mch,
+                                                 double inv_m, double* acc) {
 #pragma unroll
   for (int q = 0; q <= NC; q++) acc[q] = 0.0;
 #pragma unroll(LC > 0 ? 8 : 1)
@@ -1509,8 +1496,66 @@ __device__ __forceinline__ qd crt_group_qd(const uint8_t* rp, int64_t plane, int
     }
   }
   bool neg;
-  (void)crt_finish<NC>(acc, mch, inv_m, &neg);  // leaves |value| in normalised chunks
-  qd r = chunks_to_qd(acc, NC);
+  (void)crt_finish<NC>(acc, mch, inv_m, &neg);  // leaves |G| in normalised chunks
+  return neg;
+}
+// V = G1 2^105 + G2 as a quad-double. Both groups' signed chunks go on one
+// 39-bit grid (105 = 2 x 39 + 27: chunk c of G1 splits exactly at 12 bits
+// into cells c + 2 and c + 3), where every cell stays an exact integer below
+// 2^41; the cells are carry-normalised (the top one takes the sign; if it
+// is negative all are negated and normalised again), then added from the
+// top into four limbs by a two_sum cascade (each cell and every error term
+// exact except the last limb's additions, ~2^-212 of |V| each) and
+// renormalised once by two_sum passes. A V that fits one double comes out
+// exactly, with zero lower limbs. This is the chosen path's conversion (f256
+// accuracy), not the reference's MultiFloat renormalisation and addition.
+template <int NC>
+__device__ __forceinline__ qd crt_combine_qd(const double* a1, bool n1, const double* a2, bool n2) {
+  constexpr int NCELL = NC + 4;
+  double cell[NCELL];
+#pragma unroll
+  for (int k = 0; k < NCELL; k++) cell[k] = 0.0;
+  const double s1 = n1 ? -1.0 : 1.0, s2 = n2 ? -1.0 : 1.0;
+#pragma unroll
+  for (int c = 0; c <= NC; c++) cell[c] = s2 * a2[c];
+#pragma unroll
+  for (int c = 0; c <= NC; c++) {
+    const double hi = floor(__dmul_rn(a1[c], 0x1p-12));  // < 2^27
+    const double lo = __fma_rn(-hi, 0x1p12, a1[c]);      // < 2^12
+    cell[c + 2] = __fma_rn(s1 * lo, 0x1p27, cell[c + 2]);
+    cell[c + 3] = __dadd_rn(cell[c + 3], s1 * hi);
+  }
+  auto normalise = [&]() {
+#pragma unroll
+    for (int k = 0; k < NCELL - 1; k++) {
+      const double carry = floor(__dmul_rn(cell[k], 0x1p-39));
+      cell[k] = __fma_rn(-carry, 0x1p39, cell[k]);
+      cell[k + 1] = __dadd_rn(cell[k + 1], carry);
+    }
+  };
+  normalise();
+  const bool neg = cell[NCELL - 1] < 0.0;
+  if (neg) {
+#pragma unroll
+    for (int k = 0; k < NCELL; k++) cell[k] = -cell[k];
+    normalise();
+  }
+  double x0 = 0.0, x1 = 0.0, x2 = 0.0, x3 = 0.0;
+#pragma unroll
+  for (int k = NCELL - 1; k >= 0; k--) {
+    const double v = scale_pow2(cell[k], CRT_BITS * k);
+    double e;
+    two_sum(x0, v, x0, e);
+    two_sum(x1, e, x1, e);
+    two_sum(x2, e, x2, e);
+    x3 = __dadd_rn(x3, e);
+  }
+  two_sum(x2, x3, x2, x3);
+  two_sum(x1, x2, x1, x2);
+  two_sum(x0, x1, x0, x1);
+  two_sum(x1, x2, x1, x2);
+  two_sum(x2, x3, x2, x3);
+  qd r{{x0, x1, x2, x3}};
   return neg ? qd_neg(r) : r;
 }
 // LC > 0: L == LC at compile time, tables from c_crt (weights as immediate
@@ -1540,20 +1585,18 @@ __global__ void __launch_bounds__(256, 4) crt_qd_kernel(const uint8_t* __restric
     return;
   }
   const size_t o = (size_t)i * Np + j;
-  qd a, b;
+  double acc1[NC + 1], acc2[NC + 1];
+  bool n1, n2;
   if constexpr (LC > 0) {
     const CrtTable& ct = c_crt[LC - CRT_CONST_L0];
-    a = crt_group_qd<NC, LC>(g1 + o, plane, LC, ct.w, ct.mchunk, ct.inv_m);
-    b = crt_group_qd<NC, LC>(g2 + o, plane, LC, ct.w, ct.mchunk, ct.inv_m);
+    n1 = crt_group_chunks<NC, LC>(g1 + o, plane, LC, ct.w, ct.mchunk, ct.inv_m, acc1);
+    n2 = crt_group_chunks<NC, LC>(g2 + o, plane, LC, ct.w, ct.mchunk, ct.inv_m, acc2);
   } else {
     const double(*w_d)[NC] = w_sm;
-    a = crt_group_qd<NC>(g1 + o, plane, L, w_d, mch_sm, tab->inv_m);
-    b = crt_group_qd<NC>(g2 + o, plane, L, w_d, mch_sm, tab->inv_m);
+    n1 = crt_group_chunks<NC>(g1 + o, plane, L, w_d, mch_sm, tab->inv_m, acc1);
+    n2 = crt_group_chunks<NC>(g2 + o, plane, L, w_d, mch_sm, tab->inv_m, acc2);
   }
-  qd a_sh;
-#pragma unroll
-  for (int q = 0; q < 4; q++) a_sh.l[q] = scale_pow2(a.l[q], 105);
-  qd c = qd_add(a_sh, b);  // X Y / 2^105 = G1 2^105 + G2 (+ Xl Yl / 2^105, omitted)
+  const qd c = crt_combine_qd<NC>(acc1, n1, acc2, n2);  // X Y / 2^105 = G1 2^105 + G2 (+ Xl Yl / 2^105, omitted)
   const int shift = 105 - ((BETA_QD + 1022 - ea) + (BETA_QD + 1022 - eb));
   C[idx] = make_double4(scale_pow2(c.l[0], shift), scale_pow2(c.l[1], shift), scale_pow2(c.l[2], shift),
                         scale_pow2(c.l[3], shift));
