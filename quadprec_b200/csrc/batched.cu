@@ -38,7 +38,6 @@ namespace hp {
 
 namespace {
 
-constexpr int BT = 512;  // threads per CTA
 constexpr int SPD_PANEL = 8;  // columns per panel of the batched Cholesky
 
 template <int NT>
@@ -294,8 +293,10 @@ __device__ __forceinline__ int rr_player(int slot, int round, int nn) {
 __device__ __forceinline__ int packed_index(int i, int j) {  // lower triangle, row-major
   return i >= j ? i * (i + 1) / 2 + j : j * (j + 1) / 2 + i;
 }
-// CTA b takes matrix order[b] (b itself without an order) and the V slot b.
-__global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __restrict__ n_off,
+// CTA b takes matrix order[b] (b itself without an order) and the V slot b;
+// JT threads per CTA.
+template <int JT>
+__global__ void __launch_bounds__(JT) batched_jacobi_kernel(const int64_t* __restrict__ n_off,
                                                             const int64_t* __restrict__ mat_off,
                                                             const dd* __restrict__ Ain, dd* __restrict__ evals,
                                                             dd* __restrict__ evecs, int* __restrict__ sweeps_out,
@@ -308,7 +309,7 @@ __global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __res
   __shared__ dd old[64][3];  // a_pp, a_qq, a_pq before the round
   __shared__ dd tt[64];
   __shared__ int prs[64][3];  // p, q, rotated?
-  __shared__ dd red[BT / 32];
+  __shared__ dd red[JT / 32];
   __shared__ int stop;
   // a launch that follows this one on the stream works on other matrices:
   // let it start on SMs this one leaves free
@@ -317,7 +318,7 @@ __global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __res
   const int n = (int)(n_off[sys + 1] - n_off[sys]);
   const dd* Asrc = Ain + mat_off[sys];
   dd* Vt = work + (size_t)blockIdx.x * slot_elems;
-  for (int p = threadIdx.x; p < n * n; p += BT) {
+  for (int p = threadIdx.x; p < n * n; p += JT) {
     const int i = p / n, j = p % n;
     if (i >= j) Ap[packed_index(i, j)] = Asrc[p];
     Vt[p] = dd_from(i == j ? 1.0 : 0.0);
@@ -329,7 +330,7 @@ __global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __res
   for (sweep = 0; sweep < max_sweeps; sweep++) {
     // off-diagonal norm (linalg.rs:307-315): the entries above the diagonal
     dd acc = dd{0.0, 0.0};
-    for (int p = threadIdx.x; p < n * n; p += BT)
+    for (int p = threadIdx.x; p < n * n; p += JT)
       if (p % n > p / n) {
         const dd v = Ap[packed_index(p / n, p % n)];
         acc = dd_add(acc, dd_mul(v, v));
@@ -344,7 +345,7 @@ __global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __res
     __syncthreads();
     if (threadIdx.x == 0) {
       dd tot = dd{0.0, 0.0};
-      for (int w = 0; w < BT / 32; w++) tot = dd_add(tot, red[w]);
+      for (int w = 0; w < JT / 32; w++) tot = dd_add(tot, red[w]);
       stop = dd_lt(dd_sqrt(tot), dd_from(1e-30)) ? 1 : 0;
     }
     __syncthreads();
@@ -391,7 +392,7 @@ __global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __res
       }
       __syncthreads();
       // 2 x 2 blocks of A: rows of pair k1, columns of pair k2
-      for (int b = threadIdx.x; b < nblocks; b += BT) {
+      for (int b = threadIdx.x; b < nblocks; b += JT) {
         int k2 = (int)((sqrt(8.0 * (double)b + 1.0) - 1.0) * 0.5);
         while (k2 * (k2 + 1) / 2 > b) k2--;
         while ((k2 + 1) * (k2 + 2) / 2 <= b) k2++;
@@ -431,7 +432,7 @@ __global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __res
             if (rows[u] < n && cols[v] < n) Ap[packed_index(rows[u], cols[v])] = x[u][v];
       }
       // columns p, q of V (rows p, q of Vt)
-      for (int e = threadIdx.x; e < half * n; e += BT) {
+      for (int e = threadIdx.x; e < half * n; e += JT) {
         const int k = e / n, row = e % n;
         if (!prs[k][2]) continue;
         const int p = prs[k][0], q = prs[k][1];
@@ -446,8 +447,8 @@ __global__ void __launch_bounds__(BT) batched_jacobi_kernel(const int64_t* __res
   }
   dd* ev = evals + n_off[sys];
   dd* vo = evecs + mat_off[sys];
-  for (int i = threadIdx.x; i < n; i += BT) ev[i] = Ap[packed_index(i, i)];
-  for (int p = threadIdx.x; p < n * n; p += BT) vo[p] = Vt[p];  // rows = eigenvectors
+  for (int i = threadIdx.x; i < n; i += JT) ev[i] = Ap[packed_index(i, i)];
+  for (int p = threadIdx.x; p < n * n; p += JT) vo[p] = Vt[p];  // rows = eigenvectors
   if (threadIdx.x == 0) {
     sweeps_out[sys] = sweep;
     status[sys] = converged ? HP_OK : HP_ERR_NO_CONVERGE;
@@ -585,11 +586,17 @@ int batched_jacobi(int count, const int64_t* n_off, const int64_t* mat_off, cons
   if (!work.p) return HP_ERR_CUDA;
   // the packed lower triangle of each launch's largest matrix
   auto smem_for = [](int m) { return m * (m + 1) / 2 * 16; };
-  HP_CUDA_TRY(cudaFuncSetAttribute(batched_jacobi_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem_for(nmax)));
+  // the large matrices (one CTA per SM by shared memory) with 1024 threads,
+  // the small ones (two CTAs per SM) with 512
+  HP_CUDA_TRY(cudaFuncSetAttribute(batched_jacobi_kernel<1024>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   smem_for(nmax)));
+  HP_CUDA_TRY(cudaFuncSetAttribute(batched_jacobi_kernel<512>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   smem_for(nmax)));
   auto launch = [&](int first, int cnt, int m, bool pdl) -> cudaError_t {
+    const bool big = m > JACOBI_SMALL_N;
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3((unsigned)cnt);
-    cfg.blockDim = dim3(BT);
+    cfg.blockDim = dim3(big ? 1024 : 512);
     cfg.dynamicSmemBytes = smem_for(m);
     cfg.stream = s;
     cudaLaunchAttribute at[1];
@@ -597,9 +604,10 @@ int batched_jacobi(int count, const int64_t* n_off, const int64_t* mat_off, cons
     at[0].val.programmaticStreamSerializationAllowed = 1;
     cfg.attrs = pdl ? at : nullptr;
     cfg.numAttrs = pdl ? 1 : 0;
-    return cudaLaunchKernelEx(&cfg, batched_jacobi_kernel, n_off, mat_off, reinterpret_cast<const dd*>(A),
-                              reinterpret_cast<dd*>(evals), reinterpret_cast<dd*>(evecs), sweeps, status,
-                              work.as<dd>() + (size_t)first * slot, slot, max_sweeps, order ? order + first : order);
+    return cudaLaunchKernelEx(&cfg, big ? batched_jacobi_kernel<1024> : batched_jacobi_kernel<512>, n_off, mat_off,
+                              reinterpret_cast<const dd*>(A), reinterpret_cast<dd*>(evals), reinterpret_cast<dd*>(evecs),
+                              sweeps, status, work.as<dd>() + (size_t)first * slot, slot, max_sweeps,
+                              order ? order + first : order);
   };
   // the large matrices (one CTA per SM by shared memory), then the small
   // ones, which start on the SMs the large ones' last wave leaves free
