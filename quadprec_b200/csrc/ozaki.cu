@@ -799,13 +799,15 @@ __device__ __forceinline__ dd crt_finish(double* acc, const double* mch, double 
     for (int c = 0; c <= NC; c++) acc[c] = -acc[c];
     carry_normalise<NC>(acc);
   }
-  // sum the non-negative, non-overlapping chunks from the top into f128
+  // sum the non-negative, non-overlapping chunks from the top into f128:
+  // s.hi is 0 or above every chunk still to come, so quick_two_sum gives
+  // two_sum's exact pair with half the operations
   dd s = dd{0.0, 0.0};
 #pragma unroll
   for (int c = NC - 1; c >= 0; c--) {
     double v = scale_pow2(acc[c], CRT_BITS * c);
     double hs, he;
-    two_sum(s.hi, v, hs, he);
+    quick_two_sum(s.hi, v, hs, he);
     s = dd_renorm(hs, __dadd_rn(he, s.lo));
   }
   *neg_out = neg;
