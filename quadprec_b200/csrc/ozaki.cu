@@ -1810,18 +1810,26 @@ __global__ void __launch_bounds__(256) rns_init_kernel(const dd* __restrict__ S,
 }
 
 // P[r][c] = CRT(Res[.][r0 + r][c0 + c]) as an f128 integer, r < R, c < C.
-template <int NC>
+// LC > 0: L == LC at compile time, tables from c_crt (weights as immediate
+// operands), moduli loop unrolled.
+template <int NC, int LC = 0>
 __global__ void __launch_bounds__(256) crt_block_kernel(const uint8_t* __restrict__ res, int64_t ld, int64_t plane,
                                                         int64_t r0, int64_t c0, int64_t R, int64_t C,
                                                         const CrtTable* __restrict__ tab, dd* __restrict__ P) {
-  __shared__ double w_s[MAXL][NC];
-  __shared__ double mch_s[NC];
-  const int L = tab->L;
-  for (int i = threadIdx.x; i < L * NC; i += blockDim.x) w_s[i / NC][i % NC] = tab->w[i / NC][i % NC];
-  if (threadIdx.x < NC) mch_s[threadIdx.x] = tab->mchunk[threadIdx.x];
+  __shared__ double w_sm[LC > 0 ? 1 : MAXL][NC];
+  __shared__ double mch_sm[NC];
+  const int L = LC > 0 ? LC : tab->L;
+  if constexpr (LC == 0) {
+    for (int i = threadIdx.x; i < L * NC; i += blockDim.x) w_sm[i / NC][i % NC] = tab->w[i / NC][i % NC];
+    if (threadIdx.x < NC) mch_sm[threadIdx.x] = tab->mchunk[threadIdx.x];
+  }
+  const double(*w_s)[NCMAX] = LC > 0 ? c_crt[LC > 0 ? LC - CRT_CONST_L0 : 0].w : nullptr;
+  const double(*w_d)[NC] = w_sm;
+  const double* mch_s = LC > 0 ? c_crt[LC > 0 ? LC - CRT_CONST_L0 : 0].mchunk : mch_sm;
+  const double inv_m = LC > 0 ? c_crt[LC > 0 ? LC - CRT_CONST_L0 : 0].inv_m : tab->inv_m;
   sm100::griddep_launch_dependents();
   sm100::griddep_wait();  // the residues come from the preceding GEMM
-  __syncthreads();
+  if constexpr (LC == 0) __syncthreads();
   const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= R * C) return;
   const int64_t r = idx / C, c = idx % C;
@@ -1829,6 +1837,7 @@ __global__ void __launch_bounds__(256) crt_block_kernel(const uint8_t* __restric
   double acc[NC + 1];
 #pragma unroll
   for (int q = 0; q <= NC; q++) acc[q] = 0.0;
+#pragma unroll(LC > 0 ? 8 : 1)
   for (int l0 = 0; l0 < L; l0 += 8) {
     uint32_t v[8];
 #pragma unroll
@@ -1838,11 +1847,11 @@ __global__ void __launch_bounds__(256) crt_block_kernel(const uint8_t* __restric
       if (l0 + u >= L) break;
       const double x = byte_to_double(v[u]);
 #pragma unroll
-      for (int q = 0; q < NC; q++) acc[q] = __fma_rn(x, w_s[l0 + u][q], acc[q]);
+      for (int q = 0; q < NC; q++) acc[q] = __fma_rn(x, LC > 0 ? w_s[l0 + u][q] : w_d[l0 + u][q], acc[q]);
     }
   }
   bool neg;
-  dd s = crt_finish<NC>(acc, mch_s, tab->inv_m, &neg);
+  dd s = crt_finish<NC>(acc, mch_s, inv_m, &neg);
   P[idx] = neg ? dd_neg(s) : s;
 }
 
@@ -2192,6 +2201,15 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
                          (const uint8_t*)res.as<uint8_t>(), (int64_t)Np, (int64_t)(Np * Np), (int64_t)r0,        \
                          (int64_t)kb, (int64_t)rows, (int64_t)jb, (const CrtTable*)(D->crt + L), out));          \
     break;
+#define HP_CRTB_LC(NCV, LCV)                                                                                      \
+  if (nc == NCV && L == LCV) {                                                                                    \
+    HP_CUDA_TRY(launch_k(pdl, crt_block_kernel<NCV, LCV>, dim3((unsigned)((rows * jb + 255) / 256)), dim3(256), 0, \
+                         st, (const uint8_t*)res.as<uint8_t>(), (int64_t)Np, (int64_t)(Np * Np), (int64_t)r0,      \
+                         (int64_t)kb, (int64_t)rows, (int64_t)jb, (const CrtTable*)(D->crt + L), out));           \
+    return HP_OK;                                                                                                 \
+  }
+    HP_CRTB_LC(6, 28) HP_CRTB_LC(6, 29) HP_CRTB_LC(6, 30) HP_CRTB_LC(7, 28) HP_CRTB_LC(7, 29) HP_CRTB_LC(7, 30)
+#undef HP_CRTB_LC
     switch (nc) {
       HP_CRTB(5) HP_CRTB(6) HP_CRTB(7)
       default:
