@@ -2003,6 +2003,9 @@ __global__ void __launch_bounds__(CI_THREADS) chol_block_kernel(const dd* __rest
 // dd_fms_fast accumulation (f128 accuracy). Epilogue: each entry is rounded
 // to an integer, written scaled back to Lout (rows t0.., columns kb..) and,
 // as balanced bytes modulo every modulus, to the L~ residue planes.
+// LC > 0: L == LC at compile time (the residue epilogue's moduli loop is
+// unrolled with each modulus' constants as immediate operands).
+template <int LC = 0>
 __global__ void __launch_bounds__(256) panel_trsm_kernel(const dd* __restrict__ P21, const dd* __restrict__ L1g,
                                                          const dd* __restrict__ rinvg, int64_t r0, int64_t m, int jb,
                                                          int64_t t0,
@@ -2045,7 +2048,12 @@ __global__ void __launch_bounds__(256) panel_trsm_kernel(const dd* __restrict__ 
       int32_t D[NDIG];
       element_digits(make_double2(x.hi, x.lo), 0, D);
       int8_t* dst = lres + (t0 + r) * ld + kb + c;
-      for (int l = 0; l < L; l++) dst[(size_t)l * plane] = (int8_t)balanced_byte(D, l, c_tab.mod[l]);
+      if constexpr (LC > 0) {
+#pragma unroll
+        for (int l = 0; l < LC; l++) dst[(size_t)l * plane] = (int8_t)balanced_byte(D, l, c_tab.mod[l]);
+      } else {
+        for (int l = 0; l < L; l++) dst[(size_t)l * plane] = (int8_t)balanced_byte(D, l, c_tab.mod[l]);
+      }
     }
   }
 }
@@ -2189,7 +2197,9 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
   }
   const size_t blk_smem = 64 * 65 * 16, trsm_smem = CH_NB * (CH_NB + 1) * 16;
   HP_CUDA_TRY(cudaFuncSetAttribute(chol_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)blk_smem));
-  HP_CUDA_TRY(cudaFuncSetAttribute(panel_trsm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
+  HP_CUDA_TRY(cudaFuncSetAttribute(panel_trsm_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
+  HP_CUDA_TRY(cudaFuncSetAttribute(panel_trsm_kernel<28>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
+  HP_CUDA_TRY(cudaFuncSetAttribute(panel_trsm_kernel<29>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)trsm_smem));
   int8_t* lres8 = reinterpret_cast<int8_t*>(lres.as<uint8_t>());
   const size_t plane_l = RL * KL;
   const int gemm_ctas = std::max(1, D->num_sms - 8);  // leave SMs for the diagonal path
@@ -2222,7 +2232,8 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
   auto trsm = [&](int par, size_t kb, int jb, size_t r0, size_t m, cudaStream_t st, bool pdl) -> int {
     if (r0 >= m) return HP_OK;
     const unsigned blocks = (unsigned)std::min<size_t>((m - r0 + 7) / 8, (size_t)D->num_sms * 3);
-    HP_CUDA_TRY(launch_k(pdl, panel_trsm_kernel, dim3(blocks), dim3(256), trsm_smem, st,
+    auto kern = L == 28 ? panel_trsm_kernel<28> : L == 29 ? panel_trsm_kernel<29> : panel_trsm_kernel<0>;
+    HP_CUDA_TRY(launch_k(pdl, kern, dim3(blocks), dim3(256), trsm_smem, st,
                          (const dd*)(Pb.as<dd>() + (size_t)par * n * nb + (size_t)jb * jb),
                          (const dd*)(L1b.as<dd>() + (size_t)par * nb * nb), (const dd*)(RIb.as<dd>() + par * nb),
                          (int64_t)r0, (int64_t)m, jb, (int64_t)(kb + jb), (int64_t)kb, (int64_t)n,
