@@ -1755,21 +1755,27 @@ __device__ __forceinline__ void int_digits10(double v, int32_t* d) {
 // Res[l][i][j] = round((D S D)_ij) mod m_l (unbalanced bytes) for the tiles
 // that meet the lower triangle of n x n (the factorisation reads no other
 // entry below row n). Block tile 64 rows x 32 columns, 8 columns per thread.
+// EPT consecutive entries of a row per thread (tile 64 rows x 4 EPT
+// columns); LC > 0: L == LC at compile time (moduli loop unrolled, each
+// modulus' constants immediate operands). Every entry's digits and residues
+// are the same for any EPT and LC.
+template <int EPT, int LC>
 __global__ void __launch_bounds__(256) rns_init_kernel(const dd* __restrict__ S, int64_t n, const int* __restrict__ e,
-                                                       int L, int64_t Rp, uint8_t* __restrict__ res) {
-  const int64_t row0 = (int64_t)blockIdx.y * 64, col0 = (int64_t)blockIdx.x * 32;
+                                                       int L_, int64_t Rp, uint8_t* __restrict__ res) {
+  const int L = LC > 0 ? LC : L_;
+  const int64_t row0 = (int64_t)blockIdx.y * 64, col0 = (int64_t)blockIdx.x * (4 * EPT);
   if (row0 >= n || col0 >= n || col0 > row0 + 63) return;
   const int t = threadIdx.x;
   const int64_t i = (int64_t)blockIdx.y * 64 + t / 4;
-  const int64_t j0 = (int64_t)blockIdx.x * 32 + 8 * (t % 4);
-  int32_t dig[8][NDIG2];
+  const int64_t j0 = col0 + EPT * (t % 4);
+  int32_t dig[EPT][NDIG2];
 #pragma unroll
-  for (int q = 0; q < 8; q++)
+  for (int q = 0; q < EPT; q++)
 #pragma unroll
     for (int c = 0; c < NDIG2; c++) dig[q][c] = 0;
   if (i < n) {
 #pragma unroll
-    for (int q = 0; q < 8; q++) {
+    for (int q = 0; q < EPT; q++) {
       const int64_t j = j0 + q;
       if (j < n) {
         const dd v = S[i * n + j];
@@ -1788,11 +1794,12 @@ __global__ void __launch_bounds__(256) rns_init_kernel(const dd* __restrict__ S,
       }
     }
   }
+#pragma unroll(LC > 0 ? LC : 1)
   for (int l = 0; l < L; l++) {
     const uint32_t m = (uint32_t)c_tab.mod[l];
     uint32_t w0 = 0, w1 = 0;
 #pragma unroll
-    for (int q = 0; q < 8; q++) {
+    for (int q = 0; q < EPT; q++) {
       int32_t x1 = 0, x2 = 0;
 #pragma unroll
       for (int c = 0; c < 5; c++) x1 += dig[q][c] * c_tab.pw[l][c];
@@ -1805,7 +1812,11 @@ __global__ void __launch_bounds__(256) rns_init_kernel(const dd* __restrict__ S,
       else
         w1 |= r << (8 * (q - 4));
     }
-    *reinterpret_cast<uint2*>(res + (size_t)l * Rp * Rp + (size_t)i * Rp + j0) = make_uint2(w0, w1);
+    uint8_t* dst = res + (size_t)l * Rp * Rp + (size_t)i * Rp + j0;
+    if constexpr (EPT == 8)
+      *reinterpret_cast<uint2*>(dst) = make_uint2(w0, w1);
+    else
+      *reinterpret_cast<uint32_t*>(dst) = w0;
   }
 }
 
@@ -2191,8 +2202,11 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
   rns_scale_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(S, n, BETA_CH, ebuf.as<int>(), err.as<RnsErr>());
   HP_LAUNCH_CHECK();
   {
-    dim3 g((unsigned)(Np / 32), (unsigned)(Np / 64));
-    rns_init_kernel<<<g, 256, 0, s>>>(S, n, ebuf.as<int>(), L, Np, res.as<uint8_t>());
+    // 4 entries per thread; the moduli counts the factor uses (28-30) unrolled
+    dim3 g((unsigned)(Np / 16), (unsigned)(Np / 64));
+    auto kern = L == 28 ? rns_init_kernel<4, 28> : L == 29 ? rns_init_kernel<4, 29>
+                : L == 30 ? rns_init_kernel<4, 30> : rns_init_kernel<4, 0>;
+    kern<<<g, 256, 0, s>>>(S, n, ebuf.as<int>(), L, Np, res.as<uint8_t>());
     HP_LAUNCH_CHECK();
   }
   const size_t blk_smem = 64 * 65 * 16, trsm_smem = CH_NB * (CH_NB + 1) * 16;
