@@ -21,7 +21,8 @@
  *   - *_dev entry points take DEVICE pointers and a cudaStream_t (passed as
  *     void*; NULL = legacy default stream). They are stream-ordered and
  *     return after enqueueing; status codes that depend on data (e.g. a
- *     failed Cholesky pivot) are only available from the host-pointer form.
+ *     failed Cholesky pivot) are only available from the host-pointer form,
+ *     and a device-side wait that gave up is reported by hp_device_status.
  *   - Sizes of zero are valid and do nothing. NULL pointers with non-zero
  *     sizes return HP_ERR_INVALID_ARG. The Rust wrapper keeps the
  *     reference's assert_eq! length checks before calling (slices carry
@@ -58,6 +59,30 @@ const char* hp_version(void);
 /* 1 if a CUDA device of compute capability 10.0 is visible, else 0. */
 int hp_device_ok(void);
 
+/* Status of the stream-ordered *_dev calls (no counterpart in the
+ * reference: its calls are synchronous). The tensor-core kernels behind
+ * hp_f128_gemm_dev, hp_f128_gemm_atb_dev, hp_f256_gemm_dev and
+ * hp_f256_gemm_atb_dev (HP_MODE_OZAKI) bound every wait and, when one gives
+ * up, OR a bit into one sticky status word of the current device instead of
+ * trapping. This call synchronises `stream`, stores the word in *bits (may be
+ * NULL), clears it if `clear` is non-zero, and returns HP_ERR_TIMEOUT if the
+ * timeout bit is set (HP_ERR_NOT_SPD / HP_ERR_CUDA for the other bits), else
+ * HP_OK. Call it after a sequence of *_dev calls to learn whether any of them
+ * gave up; the host-pointer entry points read and clear the word themselves. */
+int hp_device_status(void* stream, uint32_t* bits, int clear);
+
+/* Diagnostic form of the blocked wavefront triangular solve that the refined
+ * SPD solvers run (no counterpart in the reference; the reference-order
+ * solves are hp_f128_forward_solve / hp_f128_backward_solve). Host pointers:
+ * l is n x n f128 lower triangular, b n f128, x receives L^-1 b (upper_t = 0)
+ * or L^-T b (upper_t != 0) to f128 accuracy. wait_ns bounds every wait of
+ * the launch (0 = the solver's 2 s). withheld_block >= 0 makes that 64-row
+ * block row solve without publishing its result, so that the waits of the
+ * rows after it run out: the call then returns HP_ERR_TIMEOUT with the
+ * device still usable (x unspecified). -1 = normal solve. */
+int hp_debug_trsv_wavefront(const double* l, const double* b, double* x, size_t n, int upper_t,
+                            uint64_t wait_ns, int withheld_block);
+
 /* Phase timing for benchmarks (no counterpart in the reference). While
  * enabled, the multi-kernel drivers record a CUDA event at each phase
  * boundary on their stream; hp_profile_read() waits for the last one and
@@ -93,7 +118,9 @@ int hp_f128_gemm_atb_dev(const double* a, const double* b, double* c, size_t m, 
  * return HP_ERR_INVALID_ARG naming the bytes needed). It calls no device
  * allocator. The first call on each device does a blocking set-up, so make
  * it before any stream capture; calls that overlap in time share the scratch
- * and race, so the caller must order them. */
+ * and race, so the caller must order them. Each call waits for its stream to
+ * finish the call and reads its own status word back: HP_ERR_TIMEOUT if a
+ * bounded device-side wait gave up (C is then unspecified). */
 int hp_f128_gemm_noalloc_dev(const double* a, const double* b, double* c, size_t m, size_t n,
                              size_t k, void* stream);
 

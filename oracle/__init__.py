@@ -89,6 +89,8 @@ def lib():
             "or_overlap_norm_dd": ([_sz, _d, _d, _d], None),
             "or_adjoint_f128": ([_sz, _d, _d, _d, ctypes.POINTER(ctypes.c_int32), _sz, _d, _d, _d], ctypes.c_int),
             "or_loss_f256": ([_sz, _d, _d, _d, _d], ctypes.c_int),
+            "or_fd_grad_f256": ([_sz, _d, _d, _d, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
+                                 _sz, ctypes.c_double, _d, _d], ctypes.c_int),
         }
         for name, (args, res) in sigs.items():
             f = getattr(L, name)
@@ -392,3 +394,20 @@ def loss_f256(centers4, alpha4, b):
     if rc != 0:
         raise RuntimeError("not positive definite")
     return out
+
+
+def fd_grad_f256(centers, alpha, b, center_of, cen_list, h=1e-20):
+    """f256 central differences of L = b^T S^-1 b wrt the coordinates of the
+    centres in cen_list and the log-exponents of their basis functions
+    (or_fd_grad_f256). Returns (gR (len(cen_list), 3, 4), funcs, ga (len(funcs), 4))."""
+    centers, alpha, b = _f(centers), _f(alpha), _f(b)
+    co = np.ascontiguousarray(center_of, dtype=np.int32)
+    cl = np.ascontiguousarray(cen_list, dtype=np.int32)
+    funcs = np.nonzero(np.isin(co, cl))[0]
+    gR = np.zeros((len(cl), 3, 4))
+    ga = np.zeros((len(funcs), 4))
+    i32 = ctypes.POINTER(ctypes.c_int32)
+    rc = lib().or_fd_grad_f256(len(alpha), _p(centers), _p(alpha), _p(b), co.ctypes.data_as(i32),
+                               cl.ctypes.data_as(i32), len(cl), h, _p(gR), _p(ga))
+    assert rc == 0, "f256 factorisation failed"
+    return gR, funcs, ga

@@ -987,6 +987,37 @@ int or_adjoint_f128(size_t n, const double* centers, const double* alpha, const 
   return 0;
 }
 
+}  // extern "C"
+
+namespace {
+// One normalised s-Gaussian overlap (the config formula) in MultiFloat<4>:
+// (4 a b / (a + b)^2)^{3/4} exp(-a b / (a + b) |Ri - Rj|^2); ci, cj: 3 coordinates.
+mf<4> overlap_pair_f256(const mf<4>& a, const mf<4>* ci, const mf<4>& bb, const mf<4>* cj) {
+  mf<4> sum = mf_add<4>(a, bb), prod = mf_mul<4>(a, bb);
+  mf<4> ratio = mf_div<4>(mf_mul<4>(mf_from<4>(4.0), prod), mf_mul<4>(sum, sum));
+  mf<4> sq = mf_sqrt<4>(ratio);
+  mf<4> pref = mf_mul<4>(sq, mf_sqrt<4>(sq));
+  mf<4> mu = mf_div<4>(prod, sum);
+  mf<4> r2 = mf_zero<4>();
+  for (int c = 0; c < 3; c++) {
+    mf<4> d = mf_sub<4>(ci[c], cj[c]);
+    r2 = mf_add<4>(r2, mf_mul<4>(d, d));
+  }
+  return mf_mul<4>(pref, mf_exp<4>(mf_neg<4>(mf_mul<4>(mu, r2))));
+}
+
+// L y = v for a row-major n x n lower factor in MultiFloat<4> (the forward
+// sweep of mf_cholesky_solve, multifloat/linalg.rs:145-160).
+void mf4_forward(const std::vector<mf<4>>& L, size_t n, std::vector<mf<4>>& v) {
+  for (size_t i = 0; i < n; i++) {
+    for (size_t j = 0; j < i; j++) v[i] = mf_sub<4>(v[i], mf_mul<4>(L[i * n + j], v[j]));
+    v[i] = mf_div<4>(v[i], L[i * n + i]);
+  }
+}
+}  // namespace
+
+extern "C" {
+
 // L = b^T S^-1 b in MultiFloat<4> with S from f256 centres / exponents
 // (for central finite differences): centers4 n x 3 x 4, alpha4 n x 4.
 int or_loss_f256(size_t n, const double* centers4, const double* alpha4, const double* b, double* loss4) {
@@ -995,18 +1026,9 @@ int or_loss_f256(size_t n, const double* centers4, const double* alpha4, const d
 #pragma omp parallel for schedule(dynamic, 4)
   for (size_t i = 0; i < n; i++)
     for (size_t j = 0; j <= i; j++) {
-      mf<4> a = ldq(alpha4 + 4 * i), bb = ldq(alpha4 + 4 * j);
-      mf<4> sum = mf_add<4>(a, bb), prod = mf_mul<4>(a, bb);
-      mf<4> ratio = mf_div<4>(mf_mul<4>(mf_from<4>(4.0), prod), mf_mul<4>(sum, sum));
-      mf<4> sq = mf_sqrt<4>(ratio);
-      mf<4> pref = mf_mul<4>(sq, mf_sqrt<4>(sq));
-      mf<4> mu = mf_div<4>(prod, sum);
-      mf<4> r2 = mf_zero<4>();
-      for (int c = 0; c < 3; c++) {
-        mf<4> d = mf_sub<4>(ldq(centers4 + 12 * i + 4 * c), ldq(centers4 + 12 * j + 4 * c));
-        r2 = mf_add<4>(r2, mf_mul<4>(d, d));
-      }
-      mf<4> v = mf_mul<4>(pref, mf_exp<4>(mf_neg<4>(mf_mul<4>(mu, r2))));
+      mf<4> ci[3], cj[3];
+      for (int c = 0; c < 3; c++) ci[c] = ldq(centers4 + 12 * i + 4 * c), cj[c] = ldq(centers4 + 12 * j + 4 * c);
+      mf<4> v = overlap_pair_f256(ldq(alpha4 + 4 * i), ci, ldq(alpha4 + 4 * j), cj);
       S[i * n + j] = v;
       S[j * n + i] = v;
     }
@@ -1018,6 +1040,145 @@ int or_loss_f256(size_t n, const double* centers4, const double* alpha4, const d
   mf<4> Ls = mf_zero<4>();
   for (size_t i = 0; i < n; i++) Ls = mf_add<4>(Ls, mf_mul<4>(mf_from<4>(b[i]), ldm<4>(x.data(), i)));
   stm<4>(loss4, 0, Ls);
+  return 0;
+}
+
+// Central finite differences in MultiFloat<4> (step h) of L = b^T S^-1 b with
+// respect to the three coordinates of each centre in cen_list and the
+// log-exponent of each basis function on those centres (test infrastructure
+// for the adjoint at sizes where one f256 solve per perturbation is too slow).
+// The basis functions P of those centres are ordered last; the rest, S11,
+// depends on none of the perturbed parameters and is factored once by the
+// restated mf_cholesky<4> (multifloat/linalg.rs:89-141). Each perturbed loss
+// is the block elimination of the symmetrically permuted system (the same
+// value b^T S^-1 b):
+//   L = z.z + y^T T^-1 y,  z = L11^-1 b1,  W = L11^-1 S12,
+//   T = S22 - W^T W,  y = b2 - W^T z,
+// where only the columns of W of the perturbed functions are recomputed.
+// A centre coordinate moves by +-h (an exact second limb); an exponent is
+// multiplied by (1 +- h) in f256 (d/d ln alpha to O(h^2)).
+// gR: n_cen x 3 f256 in cen_list order; ga: |P| f256 in increasing function
+// index. Returns -2 if a factorisation fails.
+int or_fd_grad_f256(size_t n, const double* centers, const double* alpha, const double* b,
+                    const int32_t* center_of, const int32_t* cen_list, size_t n_cen, double h, double* gR,
+                    double* ga) {
+  std::vector<size_t> P, R;
+  std::vector<int> pos_in_list(n, -1);
+  for (size_t u = 0; u < n; u++) {
+    int li = -1;
+    for (size_t c = 0; c < n_cen; c++)
+      if (center_of[u] == cen_list[c]) li = (int)c;
+    pos_in_list[u] = li;
+    (li >= 0 ? P : R).push_back(u);
+  }
+  const size_t m = R.size(), p = P.size();
+  std::vector<mf<4>> a4(n), c4(3 * n);
+  for (size_t u = 0; u < n; u++) {
+    a4[u] = mf_from<4>(alpha[u]);
+    for (int c = 0; c < 3; c++) c4[3 * u + c] = mf_from<4>(centers[3 * u + c]);
+  }
+  // S11 and its factor
+  std::vector<double> Sp(m * m * 4);
+#pragma omp parallel for schedule(dynamic, 4)
+  for (size_t i = 0; i < m; i++)
+    for (size_t j = 0; j <= i; j++) {
+      mf<4> v = overlap_pair_f256(a4[R[i]], &c4[3 * R[i]], a4[R[j]], &c4[3 * R[j]]);
+      stm<4>(Sp.data(), i * m + j, v);
+      stm<4>(Sp.data(), j * m + i, v);
+    }
+  if (mf_cholesky_t<4>(Sp.data(), m) != 0) return -2;
+  std::vector<mf<4>> L11(m * m);
+  for (size_t i = 0; i < m * m; i++) L11[i] = ldm<4>(Sp.data(), i);
+  std::vector<mf<4>> z(m);
+  for (size_t i = 0; i < m; i++) z[i] = mf_from<4>(b[R[i]]);
+  mf4_forward(L11, m, z);
+  mf<4> zz = mf_zero<4>();
+  for (size_t i = 0; i < m; i++) zz = mf_add<4>(zz, mf_mul<4>(z[i], z[i]));
+  // the unperturbed columns of W = L11^-1 S12
+  std::vector<std::vector<mf<4>>> W0(p, std::vector<mf<4>>(m));
+#pragma omp parallel for schedule(dynamic, 1)
+  for (size_t q = 0; q < p; q++) {
+    for (size_t i = 0; i < m; i++) W0[q][i] = overlap_pair_f256(a4[R[i]], &c4[3 * R[i]], a4[P[q]], &c4[3 * P[q]]);
+    mf4_forward(L11, m, W0[q]);
+  }
+  // perturbations: (kind 0: coordinate c of centre cen_list[ci]; kind 1: exponent of P[q]) x (+h, -h)
+  struct Pert {
+    int kind, idx, comp;
+  };
+  std::vector<Pert> perts;
+  for (size_t ci = 0; ci < n_cen; ci++)
+    for (int c = 0; c < 3; c++) perts.push_back({0, (int)ci, c});
+  for (size_t q = 0; q < p; q++) perts.push_back({1, (int)q, 0});
+  std::vector<mf<4>> loss(2 * perts.size());
+  int fail = 0;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (size_t t = 0; t < 2 * perts.size(); t++) {
+    const Pert& pt = perts[t / 2];
+    const double sg = (t % 2 == 0) ? 1.0 : -1.0;
+    std::vector<mf<4>> ap(p), cp(3 * p);
+    std::vector<char> moved(p, 0);
+    for (size_t q = 0; q < p; q++) {
+      ap[q] = a4[P[q]];
+      for (int c = 0; c < 3; c++) cp[3 * q + c] = c4[3 * P[q] + c];
+      if (pt.kind == 0 && pos_in_list[P[q]] == pt.idx) {
+        mf<4> d = mf_zero<4>();
+        d.l[0] = sg * h;
+        cp[3 * q + pt.comp] = mf_add<4>(cp[3 * q + pt.comp], d);
+        moved[q] = 1;
+      }
+      if (pt.kind == 1 && (int)q == pt.idx) {
+        mf<4> f = mf_from<4>(1.0);
+        f = mf_add<4>(f, mf_from<4>(sg * h));
+        ap[q] = mf_mul<4>(ap[q], f);
+        moved[q] = 1;
+      }
+    }
+    std::vector<std::vector<mf<4>>> Wc;  // recomputed columns, others from W0
+    std::vector<const std::vector<mf<4>>*> W(p);
+    Wc.reserve(p);
+    for (size_t q = 0; q < p; q++) {
+      if (!moved[q]) {
+        W[q] = &W0[q];
+        continue;
+      }
+      Wc.emplace_back(m);
+      std::vector<mf<4>>& col = Wc.back();
+      for (size_t i = 0; i < m; i++) col[i] = overlap_pair_f256(a4[R[i]], &c4[3 * R[i]], ap[q], &cp[3 * q]);
+      mf4_forward(L11, m, col);
+      W[q] = &col;
+    }
+    // T = S22 - W^T W (lower triangle), y = b2 - W^T z
+    std::vector<double> T(p * p * 4), y(p * 4, 0.0), xs(p * 4);
+    for (size_t q = 0; q < p; q++) {
+      mf<4> yq = mf_from<4>(b[P[q]]);
+      for (size_t i = 0; i < m; i++) yq = mf_sub<4>(yq, mf_mul<4>((*W[q])[i], z[i]));
+      stm<4>(y.data(), q, yq);
+      for (size_t r = 0; r <= q; r++) {
+        mf<4> v = overlap_pair_f256(ap[q], &cp[3 * q], ap[r], &cp[3 * r]);
+        for (size_t i = 0; i < m; i++) v = mf_sub<4>(v, mf_mul<4>((*W[q])[i], (*W[r])[i]));
+        stm<4>(T.data(), q * p + r, v);
+        stm<4>(T.data(), r * p + q, v);
+      }
+    }
+    if (mf_cholesky_t<4>(T.data(), p) != 0) {
+#pragma omp atomic write
+      fail = 1;
+      continue;
+    }
+    mf_cholesky_solve_t<4>(T.data(), y.data(), xs.data(), p);
+    mf<4> Ls = zz;
+    for (size_t q = 0; q < p; q++) Ls = mf_add<4>(Ls, mf_mul<4>(ldm<4>(y.data(), q), ldm<4>(xs.data(), q)));
+    loss[t] = Ls;
+  }
+  if (fail) return -2;
+  const mf<4> inv2h = mf_recip<4>(mf_from<4>(2.0 * h));
+  for (size_t k = 0; k < perts.size(); k++) {
+    mf<4> g = mf_mul<4>(mf_sub<4>(loss[2 * k], loss[2 * k + 1]), inv2h);
+    if (perts[k].kind == 0)
+      stm<4>(gR, 3 * perts[k].idx + perts[k].comp, g);
+    else
+      stm<4>(ga, perts[k].idx, g);
+  }
   return 0;
 }
 

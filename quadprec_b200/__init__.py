@@ -48,6 +48,8 @@ SIGNATURES = {
     "hp_last_error": ([], ctypes.c_char_p),
     "hp_version": ([], ctypes.c_char_p),
     "hp_device_ok": ([], ctypes.c_int),
+    "hp_device_status": ([_vp, ctypes.POINTER(ctypes.c_uint32), ctypes.c_int], ctypes.c_int),
+    "hp_debug_trsv_wavefront": ([_vp, _vp, _vp, _sz, ctypes.c_int, ctypes.c_uint64, ctypes.c_int], ctypes.c_int),
     "hp_profile_enable": ([ctypes.c_int], None),
     "hp_profile_read": ([_d, ctypes.c_int, ctypes.c_char_p, _sz], ctypes.c_int),
     "hp_f128_gemm": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int], ctypes.c_int),
@@ -287,6 +289,22 @@ def f128_forward_solve(l, b, n): return _solve("hp_f128_forward_solve", l, b, n)
 def f128_backward_solve(l, y, n): return _solve("hp_f128_backward_solve", l, y, n)
 def f128_solve_cholesky(l, b, n): return _solve("hp_f128_solve_cholesky", l, b, n)
 def f128_matvec(a, x, n): return _solve("hp_f128_matvec", a, x, n)
+
+
+def device_status(stream=0, clear=True) -> tuple[int, int]:
+    """(return code, status bits) of the *_dev calls enqueued on `stream`."""
+    bits = ctypes.c_uint32(0)
+    rc = lib().hp_device_status(stream, ctypes.byref(bits), int(clear))
+    return rc, int(bits.value)
+
+
+def debug_trsv_wavefront(l, b, n, upper_t=False, wait_ns=0, withheld_block=-1):
+    """(return code, x) of the wavefront solve L x = b (or L^T x = b)."""
+    l, b = _c(l), _c(b)
+    x = np.zeros((n, 2))
+    rc = lib().hp_debug_trsv_wavefront(_ptr(l), _ptr(b), _ptr(x), n, int(upper_t), int(wait_ns),
+                                       int(withheld_block))
+    return rc, x
 
 
 def f128_cond_estimate(l, n) -> float:

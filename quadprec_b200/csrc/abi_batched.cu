@@ -1,6 +1,7 @@
 // C ABI: batched overlap SPD solves (one persistent launch replayed from a
 // CUDA graph), batched / single Jacobi eigensolves, batched assembly.
 #include <algorithm>
+#include <cstring>
 #include <cstdlib>
 #include <map>
 #include <mutex>
@@ -102,51 +103,49 @@ int tuned_config(int count, const int* order, const int64_t* off, const double* 
   return HP_OK;
 }
 
-// One cached graph: the batched launch for one argument set.
+// One cached graph: the batched launch for one argument set. The graph bakes
+// in device copies of the offsets and of the largest-first order, so it is
+// replayed only when every argument matches: the pointers, count, max_iter,
+// the bit pattern of tol, the device ordinal and the whole offsets array.
 struct GraphCache {
   std::mutex mu;
   cudaGraphExec_t exec = nullptr;
   cudaGraph_t graph = nullptr;
   std::vector<const void*> key;
+  std::vector<int64_t> offsets;  // full copy of the host offsets the graph was built for
+  int dev = -1;
   void* order_dev = nullptr;
   void* off_dev = nullptr;
   void* work = nullptr;
   void* queue = nullptr;
+
+  // Drops the graph and every buffer it owns; each is released on its own,
+  // so a rebuild that failed part-way leaves nothing behind.
+  void release() {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    for (void** p : {&order_dev, &off_dev, &work, &queue})
+      if (*p) cudaFree(*p), *p = nullptr;
+    exec = nullptr;
+    graph = nullptr;
+    key.clear();
+    offsets.clear();
+    dev = -1;
+  }
+  bool matches(const std::vector<const void*>& k, const int64_t* off, int count, int d) const {
+    return exec && d == dev && k == key && offsets.size() == (size_t)count + 1 &&
+           std::memcmp(offsets.data(), off, ((size_t)count + 1) * sizeof(int64_t)) == 0;
+  }
 };
 GraphCache g_cache;
 
-}  // namespace
-}  // namespace hp
-
-extern "C" {
-
-int hp_spd_solve_batched_dev(int count, const int64_t* offsets, const double* centers, const double* alpha,
-                             const double* b, double* x, int32_t* status, int32_t* iters, double tol, int max_iter,
-                             void* stream) {
-  using namespace hp;
-  if (count <= 0) return count == 0 ? HP_OK : HP_ERR_INVALID_ARG;
-  if (!offsets || !centers || !alpha || !b || !x || !status || !iters) return HP_ERR_INVALID_ARG;
-  cudaStream_t s = (cudaStream_t)stream;
-  std::lock_guard<std::mutex> lk(g_cache.mu);
-  std::vector<const void*> key = {offsets, centers, alpha, b, x, status, iters, stream,
-                                  (const void*)(intptr_t)count, (const void*)(intptr_t)max_iter,
-                                  (const void*)(intptr_t)(tol * 1e30)};
-  // offsets is a host array: its contents are part of the key
-  for (int i = 0; i <= count; i += std::max(1, count / 64)) key.push_back((const void*)(intptr_t)offsets[i]);
-  key.push_back((const void*)(intptr_t)offsets[count]);
-  if (g_cache.exec && key == g_cache.key) {
-    HP_CUDA_TRY(cudaGraphLaunch(g_cache.exec, s));
-    return HP_OK;
-  }
-  if (g_cache.exec) {
-    cudaGraphExecDestroy(g_cache.exec);
-    cudaGraphDestroy(g_cache.graph);
-    cudaFree(g_cache.order_dev);
-    cudaFree(g_cache.off_dev);
-    cudaFree(g_cache.work);
-    cudaFree(g_cache.queue);
-    g_cache.exec = nullptr;
-  }
+// Builds g_cache's graph for one argument set: device copies of the
+// offsets and the queue order, the tuned launch shape, the workspace, and
+// the captured queue reset + persistent launch. On failure the caller
+// releases whatever was allocated.
+int batched_graph_build(int count, const int64_t* offsets, const double* centers, const double* alpha,
+                        const double* b, double* x, int32_t* status, int32_t* iters, double tol, int max_iter,
+                        cudaStream_t s) {
   std::vector<int> order;
   int nmax = 0;
   lpt_order(count, offsets, order, &nmax);
@@ -171,14 +170,52 @@ int hp_spd_solve_batched_dev(int count, const int64_t* offsets, const double* ce
   cudaGraph_t graph = nullptr;
   cudaError_t ce = cudaStreamEndCapture(cap, &graph);
   cudaStreamDestroy(cap);
-  if (rc != HP_OK) return rc;
+  if (rc != HP_OK) {
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+  }
   if (ce != cudaSuccess) {
     set_error("batched: graph capture failed: %s", cudaGetErrorString(ce));
     return HP_ERR_CUDA;
   }
-  HP_CUDA_TRY(cudaGraphInstantiate(&g_cache.exec, graph, 0));
   g_cache.graph = graph;
+  HP_CUDA_TRY(cudaGraphInstantiate(&g_cache.exec, graph, 0));
+  return HP_OK;
+}
+
+}  // namespace
+}  // namespace hp
+
+extern "C" {
+
+int hp_spd_solve_batched_dev(int count, const int64_t* offsets, const double* centers, const double* alpha,
+                             const double* b, double* x, int32_t* status, int32_t* iters, double tol, int max_iter,
+                             void* stream) {
+  using namespace hp;
+  if (count <= 0) return count == 0 ? HP_OK : HP_ERR_INVALID_ARG;
+  if (!offsets || !centers || !alpha || !b || !x || !status || !iters) return HP_ERR_INVALID_ARG;
+  cudaStream_t s = (cudaStream_t)stream;
+  int dev = 0;
+  HP_CUDA_TRY(cudaGetDevice(&dev));
+  uint64_t tol_bits = 0;
+  std::memcpy(&tol_bits, &tol, sizeof(tol_bits));
+  std::lock_guard<std::mutex> lk(g_cache.mu);
+  const std::vector<const void*> key = {offsets, centers, alpha, b, x, status, iters, stream,
+                                        (const void*)(intptr_t)count, (const void*)(intptr_t)max_iter,
+                                        (const void*)(uintptr_t)tol_bits};
+  if (g_cache.matches(key, offsets, count, dev)) {
+    HP_CUDA_TRY(cudaGraphLaunch(g_cache.exec, s));
+    return HP_OK;
+  }
+  g_cache.release();
+  int rc = batched_graph_build(count, offsets, centers, alpha, b, x, status, iters, tol, max_iter, s);
+  if (rc != HP_OK) {
+    g_cache.release();
+    return rc;
+  }
   g_cache.key = key;
+  g_cache.offsets.assign(offsets, offsets + count + 1);
+  g_cache.dev = dev;
   HP_CUDA_TRY(cudaGraphLaunch(g_cache.exec, s));
   return HP_OK;
 }

@@ -92,7 +92,12 @@ namespace hp {
 // trsv_blocked.cu: solves with precomputed inverses of the 64 x 64 diagonal blocks.
 int dd_block_inverses(const double* L, size_t n, double* Xall, cudaStream_t s);
 size_t dd_block_inverses_bytes(size_t n);
-int dd_trsv_blocked(const double* L, const double* Xall, double* v, size_t n, bool upper_t, cudaStream_t s);
+// Every wait of the solve gives up after wait_ns of global time (then the
+// launch records DEV_STATUS_TIMEOUT); withheld >= 0 is the diagnostic hook of
+// hp_debug_trsv_wavefront (that ticket's block is solved but not published).
+constexpr uint64_t TRSV_WAIT_NS = 2000000000ull;
+int dd_trsv_blocked(const double* L, const double* Xall, double* v, size_t n, bool upper_t, cudaStream_t s,
+                    uint64_t wait_ns = TRSV_WAIT_NS, int withheld = -1);
 // Device address of the status word of the solves on Xall (DEV_STATUS_TIMEOUT
 // once a wavefront wait gave up).
 const unsigned* dd_trsv_status_word(const double* Xall, size_t n);

@@ -2358,7 +2358,10 @@ int rns_cholesky(const double* S_, double* L_, size_t n, int64_t* pivot, cudaStr
 // threads, or two streams) race on it: the caller must order them. The
 // first call on each device does the set-up (symbol addresses, table
 // upload, kernel attribute) and blocks the host while it does, so that
-// first call should come before any stream capture.
+// first call should come before any stream capture. Each call returns once
+// its stream has run it: it reads the call's status word back, so that a
+// bounded wait in the tensor-core kernel that gave up is returned as
+// HP_ERR_TIMEOUT by this call rather than lost.
 // ===========================================================================
 namespace hp {
 namespace ozaki {
@@ -2483,8 +2486,19 @@ static int ozaki_dd_gemm_noalloc(const double* a, const double* b, double* c, si
       HP_LAUNCH_CHECK();
     }
   }
-  return launch_crt_dd(cres, Mp, Np, m, n, expA, expB, beta, N->crt + L, host_tables().crt[L].nc,
-                       reinterpret_cast<double2*>(c), s);
+  HP_TRY(launch_crt_dd(cres, Mp, Np, m, n, expA, expB, beta, N->crt + L, host_tables().crt[L].nc,
+                       reinterpret_cast<double2*>(c), s));
+  // The status word lives in the static array as well; it is read back here,
+  // before the next call clears it, so a wait that gave up is reported by
+  // the call it happened in.
+  uint32_t st = 0;
+  HP_CUDA_TRY(cudaMemcpyAsync(&st, N->status, sizeof(st), cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  if (st & DEV_STATUS_TIMEOUT) {
+    set_error("hp_f128_gemm_noalloc_dev: a bounded device-side wait gave up (status 0x%x)", st);
+    return HP_ERR_TIMEOUT;
+  }
+  return HP_OK;
 }
 
 }  // namespace hp

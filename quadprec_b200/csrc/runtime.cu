@@ -162,6 +162,37 @@ int hp_profile_read(double* ms, int max_phases, char* names, size_t names_len) {
   return n;
 }
 
+int hp_device_status(void* stream, uint32_t* bits, int clear) {
+  using namespace hp;
+  cudaStream_t s = (cudaStream_t)stream;
+  uint32_t* w = device_status(s);
+  if (!w) {
+    set_error("status word allocation failed");
+    return HP_ERR_CUDA;
+  }
+  uint32_t h = 0;
+  HP_CUDA_TRY(cudaMemcpyAsync(&h, w, sizeof(h), cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  if (bits) *bits = h;
+  if (clear && h) {
+    HP_CUDA_TRY(cudaMemsetAsync(w, 0, sizeof(uint32_t), s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  if (h & DEV_STATUS_TIMEOUT) {
+    set_error("a bounded device-side wait gave up (status 0x%x)", h);
+    return HP_ERR_TIMEOUT;
+  }
+  if (h & DEV_STATUS_NOT_SPD) {
+    set_error("a Cholesky pivot was not positive (status 0x%x)", h);
+    return HP_ERR_NOT_SPD;
+  }
+  if (h) {
+    set_error("device status 0x%x", h);
+    return HP_ERR_CUDA;
+  }
+  return HP_OK;
+}
+
 const char* hp_last_error(void) { return hp::last_error(); }
 const char* hp_version(void) { return "hyperprec-b200 0.1.0 (sm_100a)"; }
 

@@ -118,9 +118,8 @@ __global__ void __launch_bounds__(INV_COLS * 32) block_inverse_kernel(const dd* 
 }
 
 // Poll an exchange entry until both limbs hold a published value; false if
-// the wait gave up (time limit, or another CTA's abort).
-constexpr uint64_t TRSV_WAIT_NS = 2000000000ull;
-__device__ __forceinline__ bool poll_entry(const dd* p, dd& out, TrsvSync* sync) {
+// the wait gave up (wait_ns of global time, or another CTA's abort).
+__device__ __forceinline__ bool poll_entry(const dd* p, dd& out, TrsvSync* sync, uint64_t wait_ns) {
   const uint64_t t0 = sm100::globaltimer_ns();
   for (unsigned it = 1;; it++) {
     unsigned long long h, l;
@@ -129,7 +128,7 @@ __device__ __forceinline__ bool poll_entry(const dd* p, dd& out, TrsvSync* sync)
       out = dd{__longlong_as_double((long long)h), __longlong_as_double((long long)l)};
       return true;
     }
-    if ((it & 31) == 0 && (ld_relaxed_u32(&sync->abort) || sm100::globaltimer_ns() - t0 > TRSV_WAIT_NS)) {
+    if ((it & 31) == 0 && (ld_relaxed_u32(&sync->abort) || sm100::globaltimer_ns() - t0 > wait_ns)) {
       atomicOr(&sync->status, (unsigned)DEV_STATUS_TIMEOUT);
       atomicExch(&sync->abort, 1u);
       return false;
@@ -141,9 +140,14 @@ __device__ __forceinline__ bool poll_entry(const dd* p, dd& out, TrsvSync* sync)
 // the columns c = q (mod 4) of each 64 x 64 tile it multiplies; the four
 // partial sums of a row sit on neighbouring lanes and are combined by
 // shuffles (dd_add is commutative bit for bit, so all four agree).
+// withheld >= 0 names one block row that is solved but not published: the
+// diagnostic entry point uses this to make the waits of the CTAs after it
+// run out (with a short wait_ns) and checks that the launch ends with
+// DEV_STATUS_TIMEOUT; the solver passes -1.
 template <bool UPPER_T>
 __global__ void __launch_bounds__(256) trsv_wave_kernel(const dd* __restrict__ L, const dd* __restrict__ Xall,
-                                                        dd* v, int64_t n, int nblk, TrsvSync* sync, dd* xchg) {
+                                                        dd* v, int64_t n, int nblk, TrsvSync* sync, dd* xchg,
+                                                        uint64_t wait_ns, int withheld) {
   __shared__ unsigned my, par;
   __shared__ int bad[2];  // per dependency parity: a poll gave up
   __shared__ dd vj[2][TB], sv[TB];
@@ -185,7 +189,7 @@ __global__ void __launch_bounds__(256) trsv_wave_kernel(const dd* __restrict__ L
     }
     if (t < TB) {
       dd val = {0.0, 0.0};
-      if (t < jbj && !poll_entry(cur + j0 + t, val, sync)) bad[d & 1] = 1;
+      if (t < jbj && !poll_entry(cur + j0 + t, val, sync, wait_ns)) bad[d & 1] = 1;
       vj[d & 1][t] = val;
     }
     __syncthreads();
@@ -215,7 +219,7 @@ __global__ void __launch_bounds__(256) trsv_wave_kernel(const dd* __restrict__ L
     a = dd_add(acc0, acc1);
     a = dd_add(a, dd{__shfl_xor_sync(0xffffffffu, a.hi, 1), __shfl_xor_sync(0xffffffffu, a.lo, 1)});
     a = dd_add(a, dd{__shfl_xor_sync(0xffffffffu, a.hi, 2), __shfl_xor_sync(0xffffffffu, a.lo, 2)});
-    if (q == 0 && r < jb) {
+    if (q == 0 && r < jb && k != withheld) {
       st_relaxed_v2(cur + k0 + r, canonical_bits(a.hi), canonical_bits(a.lo));
       v[k0 + r] = a;
     }
@@ -249,7 +253,8 @@ int dd_block_inverses(const double* L, size_t n, double* Xall, cudaStream_t s) {
 
 size_t dd_block_inverses_bytes(size_t n) { return inverses_bytes(n) + sizeof(TrsvSync) + 2 * nblocks(n) * TB * 16; }
 
-int dd_trsv_blocked(const double* L, const double* Xall, double* v, size_t n, bool upper_t, cudaStream_t s) {
+int dd_trsv_blocked(const double* L, const double* Xall, double* v, size_t n, bool upper_t, cudaStream_t s,
+                    uint64_t wait_ns, int withheld) {
   if (n == 0) return HP_OK;
   char* tail = const_cast<char*>(reinterpret_cast<const char*>(Xall)) + inverses_bytes(n);
   TrsvSync* sync = reinterpret_cast<TrsvSync*>(tail);
@@ -259,9 +264,9 @@ int dd_trsv_blocked(const double* L, const double* Xall, double* v, size_t n, bo
   const dd* Xp = reinterpret_cast<const dd*>(Xall);
   dd* vp = reinterpret_cast<dd*>(v);
   if (upper_t)
-    trsv_wave_kernel<true><<<nblk, 256, 0, s>>>(Lp, Xp, vp, (int64_t)n, nblk, sync, xchg);
+    trsv_wave_kernel<true><<<nblk, 256, 0, s>>>(Lp, Xp, vp, (int64_t)n, nblk, sync, xchg, wait_ns, withheld);
   else
-    trsv_wave_kernel<false><<<nblk, 256, 0, s>>>(Lp, Xp, vp, (int64_t)n, nblk, sync, xchg);
+    trsv_wave_kernel<false><<<nblk, 256, 0, s>>>(Lp, Xp, vp, (int64_t)n, nblk, sync, xchg, wait_ns, withheld);
   HP_LAUNCH_CHECK();
   return HP_OK;
 }
@@ -272,3 +277,42 @@ const unsigned* dd_trsv_status_word(const double* Xall, size_t n) {
 }
 
 }  // namespace hp
+
+extern "C" int hp_debug_trsv_wavefront(const double* l, const double* b, double* x, size_t n, int upper_t,
+                                       uint64_t wait_ns, int withheld_block) {
+  using namespace hp;
+  if (n == 0) return HP_OK;
+  size_t t, bytes;
+  if (hp::mul_overflows(n, n, &t) || hp::mul_overflows(t, 16, &bytes)) {
+    set_error("matrix size overflows size_t");
+    return HP_ERR_INVALID_ARG;
+  }
+  if (!l || !b || !x) {
+    set_error("null pointer with non-zero size");
+    return HP_ERR_INVALID_ARG;
+  }
+  if (withheld_block >= (int)nblocks(n)) {
+    set_error("withheld_block %d is not a block of the %zu-row solve", withheld_block, n);
+    return HP_ERR_INVALID_ARG;
+  }
+  cudaStream_t s = library_stream();
+  DevBuf dl(bytes, s), dv(n * 16, s), dx(dd_block_inverses_bytes(n), s);
+  if (!dl.p || !dv.p || !dx.p) {
+    set_error("device allocation failed");
+    return HP_ERR_CUDA;
+  }
+  HP_CUDA_TRY(cudaMemcpyAsync(dl.p, l, bytes, cudaMemcpyHostToDevice, s));
+  HP_CUDA_TRY(cudaMemcpyAsync(dv.p, b, n * 16, cudaMemcpyHostToDevice, s));
+  HP_TRY(dd_block_inverses(dl.as<double>(), n, dx.as<double>(), s));
+  HP_TRY(dd_trsv_blocked(dl.as<double>(), dx.as<double>(), dv.as<double>(), n, upper_t != 0, s,
+                         wait_ns ? wait_ns : TRSV_WAIT_NS, withheld_block));
+  unsigned st = 0;
+  HP_CUDA_TRY(cudaMemcpyAsync(&st, dd_trsv_status_word(dx.as<double>(), n), sizeof(st), cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaMemcpyAsync(x, dv.p, n * 16, cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  if (st & DEV_STATUS_TIMEOUT) {
+    set_error("wavefront solve: a bounded wait gave up (status 0x%x)", st);
+    return HP_ERR_TIMEOUT;
+  }
+  return HP_OK;
+}

@@ -191,3 +191,56 @@ def test_batched_solve_size_limit(gpu):
     with pytest.raises(gpu.HPError) as ei:
         gpu.spd_solve_batched(B)
     assert ei.value.code == gpu.HP_ERR_UNSUPPORTED
+
+
+def _batch_of_sizes(sizes, seed0):
+    """Batch whose system s is a one-system cluster of exactly sizes[s] functions."""
+    parts = [batched_overlap_systems(count=1, seed=seed0 + s, n_min=n, n_max=n) for s, n in enumerate(sizes)]
+    off = np.zeros(len(sizes) + 1, dtype=np.int64)
+    off[1:] = np.cumsum(sizes)
+    return {"offsets": off, "centers": np.concatenate([p["centers"] for p in parts]),
+            "alpha": np.concatenate([p["alpha"] for p in parts]), "b": np.concatenate([p["b"] for p in parts])}
+
+
+def test_batched_graph_replays_only_for_identical_offsets(gpu):
+    """hp_spd_solve_batched_dev keeps one CUDA graph with device copies of the
+    first call's offsets and queue order. A second call on the same buffers
+    whose offsets differ only at entries a sparse sample of the array would
+    skip (here offsets[3] and offsets[67] of 130 systems, total unchanged) must
+    not replay the stale graph: its x must equal a fresh solve of the new
+    batch, bit for bit."""
+    import torch
+
+    rng = np.random.default_rng(11)
+    sizes1 = [int(4 * v) for v in rng.integers(4, 9, size=130)]
+    sizes2 = list(sizes1)
+    sizes2[2] += 8
+    sizes2[3] -= 8 if sizes2[3] > 16 else -8
+    sizes2[4] -= sizes2[2] + sizes2[3] - sizes1[2] - sizes1[3]  # offsets[4:] unchanged
+    sizes2[66] += 4
+    sizes2[67] -= 4
+    assert all(16 <= n <= 48 for n in sizes2) and sum(sizes2) == sum(sizes1)
+    B1, B2 = _batch_of_sizes(sizes1, 500), _batch_of_sizes(sizes2, 900)
+    diff = np.nonzero(B1["offsets"] != B2["offsets"])[0]
+    assert set(diff.tolist()) <= {3, 4, 67} and 3 in diff and 67 in diff, diff
+    N = int(B1["offsets"][-1])
+    dc = torch.empty((N, 3), dtype=torch.float64, device="cuda")
+    da = torch.empty(N, dtype=torch.float64, device="cuda")
+    db = torch.zeros((N, 2), dtype=torch.float64, device="cuda")
+    dx = torch.empty((N, 2), dtype=torch.float64, device="cuda")
+    dst = torch.empty(130, dtype=torch.int32, device="cuda")
+    dit = torch.empty(130, dtype=torch.int32, device="cuda")
+    offs = np.empty(131, dtype=np.int64)  # one host array, rewritten between the calls
+    for B in (B1, B2):
+        dc.copy_(torch.from_numpy(B["centers"]))
+        da.copy_(torch.from_numpy(B["alpha"]))
+        db[:, 0].copy_(torch.from_numpy(B["b"]))
+        offs[:] = B["offsets"]
+        gpu.check(gpu.lib().hp_spd_solve_batched_dev(130, offs.ctypes.data, dc.data_ptr(), da.data_ptr(),
+                                                     db.data_ptr(), dx.data_ptr(), dst.data_ptr(), dit.data_ptr(),
+                                                     1e-28, 10, 0))
+        torch.cuda.synchronize()
+        x_fresh, st_fresh, _ = gpu.spd_solve_batched(B)
+        assert np.all(st_fresh == 0)
+        assert np.array_equal(dst.cpu().numpy(), st_fresh)
+        assert np.array_equal(dx.cpu().numpy(), x_fresh)
