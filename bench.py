@@ -180,14 +180,18 @@ def peaks():
     return 6650.0, 1590.0, "fallback"
 
 
-def cpu_sample_gflops(target_s: float = 12.0) -> dict:
-    """Oracle (C++ restatement of linalg.rs:150 gemm) on a bounded row sample."""
+def cpu_sample_gflops(target_s: float = 12.0, threads: int | None = None) -> dict:
+    """Oracle (C++ restatement of linalg.rs:150 gemm) on a bounded row sample,
+    on all host threads or on `threads`."""
     import numpy as np
 
     import oracle
     from quadprec_b200.workloads import gemm_operands
 
     a, b = gemm_operands(M, N, K, seed=0)
+    prev = oracle.num_threads()
+    if threads is not None:
+        oracle.set_threads(threads)
     threads = oracle.num_threads()
     rows = max(1, threads)
     t0 = time.perf_counter()
@@ -201,6 +205,7 @@ def cpu_sample_gflops(target_s: float = 12.0) -> dict:
         oracle.gemm(a, b, M, N, K, rows=(r0, min(M, r0 + rows)))
         total_rows += min(M, r0 + rows) - r0
     dt = time.perf_counter() - t0
+    oracle.set_threads(prev)
     return {"value": 2.0 * total_rows * N * K / dt / 1e9, "unit": "GFLOP/s", "cores": threads, "kind": "port",
             "sample": f"{total_rows} of {M} rows of C (each a full 2048x2048 dd dot-product sweep), "
                       f"{dt:.1f} s; oracle/hp_oracle.cpp restates crates/quad/src/linalg.rs:150-165"}
@@ -260,10 +265,32 @@ def profile_case(args):
     return 0
 
 
-def gemm_more_section(hp, torch, dev, stream, sptr, world, dist):
-    """gemm_atb at 2048^3 (f128) and mf_gemm at 1024^3 (f256), chosen and plain."""
+def gemm_f512_fixture():
+    """f512 values of sampled entries of the benchmark GEMMs (seed-0 operands),
+    generated by tests/golden/make_gemm_f512_fixture.py; None if absent."""
     import numpy as np
 
+    p = os.path.join(REPO, "tests", "golden", "gemm_f512_sample.npz")
+    return np.load(p) if os.path.exists(p) else None
+
+
+def f512_errors(c, a, b, name, atb=False):
+    """Normwise error of C over the fixture's sampled entries (4096 random +
+    rows 0 and m-1) against the f512 oracle: || |A||B| ||-relative and ||C*||-relative."""
+    from quadprec_b200.workloads import sample_abs_products, sample_index, sampled_error
+
+    fx = gemm_f512_fixture()
+    if fx is None or name not in fx:
+        return None
+    m = c.shape[0]
+    idx = sample_index(m, c.shape[1])
+    e_ab, e_c = sampled_error(c, fx[name], sample_abs_products(a, b, idx, atb), idx)
+    return {"normwise_vs_absAB": e_ab, "normwise_vs_C": e_c, "entries": int(len(idx))}
+
+
+def gemm_more_section(hp, torch, dev, stream, sptr, world, dist):
+    """gemm_atb at 2048^3 (f128) and mf_gemm at 1024^3 (f256), chosen and plain,
+    each with its error against the f512 oracle on sampled entries."""
     from quadprec_b200.workloads import dd_to_qd, gemm_operands
 
     def timed(fn, steps):
@@ -278,36 +305,29 @@ def gemm_more_section(hp, torch, dev, stream, sptr, world, dist):
         return max_over_ranks(s0.elapsed_time(e0) / steps, dist, dev)
 
     out = {}
-    a, b = gemm_operands(M, N, K, seed=1, atb=True)
+    a, b = gemm_operands(M, N, K, seed=0, atb=True)
     A, B = torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)
     C = torch.empty((M, N, 2), dtype=torch.float64, device=dev)
+    sec = out.setdefault("f128_gemm_atb_2048", {"unit": "GFLOP/s (2mnk f128 ops)"})
     for name, mode, steps in (("chosen", hp.OZAKI, 5), ("plain", hp.PLAIN, 1)):
         ms = timed(lambda: hp.f128_gemm_dev(A, B, C, M, N, K, mode, atb=True, stream=sptr), steps)
-        out.setdefault("f128_gemm_atb_2048", {})[name] = {"gflops": world * 2.0 * M * N * K / (ms * 1e-3) / 1e9,
-                                                          "ms": ms}
+        torch.cuda.synchronize()
+        sec[name] = {"gflops": world * 2.0 * M * N * K / (ms * 1e-3) / 1e9, "ms": ms,
+                     "err_vs_f512": f512_errors(C.cpu().numpy(), a, b, "f128_gemm_atb_2048", atb=True)}
+    sec["chosen_over_plain"] = sec["plain"]["ms"] / sec["chosen"]["ms"]
     del A, B, C
     n4 = 1024
-    a, b = gemm_operands(n4, n4, n4, seed=2)
-    a4, b4 = dd_to_qd(a), dd_to_qd(b)
-    a4[..., 2] = a4[..., 1] * 2.0 ** -60  # full 4-limb entries
-    b4[..., 2] = b4[..., 1] * 2.0 ** -60
+    a, b = gemm_operands(n4, n4, n4, seed=0)
+    a4, b4 = dd_to_qd(a), dd_to_qd(b)  # limbs 2-3 zero (full double-double entries)
     A, B = torch.from_numpy(a4).to(dev), torch.from_numpy(b4).to(dev)
     C = torch.empty((n4, n4, 4), dtype=torch.float64, device=dev)
-    res = {}
+    sec = out.setdefault("f256_mf_gemm_1024", {"unit": "GFLOP/s (2mnk f256 ops)"})
     for name, mode, steps in (("chosen", hp.OZAKI, 5), ("plain", hp.PLAIN, 1)):
         ms = timed(lambda: hp.f256_gemm_dev(A, B, C, n4, n4, n4, mode, stream=sptr), steps)
-        res[name] = {"gflops": world * 2.0 * n4 ** 3 / (ms * 1e-3) / 1e9, "ms": ms}
         torch.cuda.synchronize()
-        res[name + "_c"] = C.cpu().numpy()
-    d = ((res["chosen_c"][..., 0] - res["plain_c"][..., 0]) + (res["chosen_c"][..., 1] - res["plain_c"][..., 1])
-         + (res["chosen_c"][..., 2] - res["plain_c"][..., 2]) + (res["chosen_c"][..., 3] - res["plain_c"][..., 3]))
-    absab = np.abs(a4[..., 0]) @ np.abs(b4[..., 0])
-    out["f256_mf_gemm_1024"] = {"chosen": res["chosen"], "plain": res["plain"],
-                                "chosen_over_plain": res["chosen"]["ms"] and res["plain"]["ms"] / res["chosen"]["ms"],
-                                "normwise_rel_err_vs_plain": float(np.linalg.norm(d) / np.linalg.norm(absab)),
-                                "unit": "GFLOP/s (2mnk f256 ops)"}
-    out["f128_gemm_atb_2048"]["chosen_over_plain"] = (out["f128_gemm_atb_2048"]["plain"]["ms"]
-                                                       / out["f128_gemm_atb_2048"]["chosen"]["ms"])
+        sec[name] = {"gflops": world * 2.0 * n4 ** 3 / (ms * 1e-3) / 1e9, "ms": ms,
+                     "err_vs_f512": f512_errors(C.cpu().numpy(), a4, b4, "f256_gemm_1024")}
+    sec["chosen_over_plain"] = sec["plain"]["ms"] / sec["chosen"]["ms"]
     return out
 
 
@@ -416,6 +436,21 @@ def batched_section(hp, torch, dev, stream, sptr, args, world, dist):
     ms = max_over_ranks(s0.elapsed_time(e0) / steps, dist, dev)
     status = st.cpu().numpy()
     ok = int((status == 0).sum())
+    acc = None
+    fixp = os.path.join(REPO, "tests", "golden", "batched_4096_sample.npz")
+    if os.path.exists(fixp):
+        fx = np.load(fixp)
+        xh = dx.cpu().numpy()
+        errs = []
+        for t, sidx in enumerate(fx["index"]):
+            xg, xr = xh[off[sidx]:off[sidx + 1]], fx["x_star"][fx["x_offsets"][t]:fx["x_offsets"][t + 1]]
+            d = (xg[:, 0] - xr[:, 0]) + (xg[:, 1] - xr[:, 1]) - xr[:, 2] - xr[:, 3]
+            errs.append(float(np.linalg.norm(d) / np.linalg.norm(xr[:, 0])))
+        acc = {"max_rel_err_vs_f512": max(errs), "systems_checked": len(errs),
+               "n_range": [int(fx["n"].min()), int(fx["n"].max())],
+               "kappa_range": [float(fx["kappa"].min()), float(fx["kappa"].max())],
+               "sample": "48 systems spread over the sizes + the 16 largest cond_estimate (tests/golden/"
+                         "batched_4096_sample.npz, mf_cholesky<8> solutions)"}
     out = {"workload": "4096 overlap SPD systems, n = 4*round(16*24^U/4) in [16, 384] (mean %.1f), random "
                        "3-D clusters (spacing 1.2-2.0 bohr), 4 exponents log-uniform in [0.01, 10], b ~ N(0,1); "
                        "each assembled in f128, factored and refined to max|dx| <= 1e-28 max|x|" % ns.mean(),
@@ -423,9 +458,24 @@ def batched_section(hp, torch, dev, stream, sptr, args, world, dist):
            "systems_per_s": world * ok * 1e3 / ms,
            "f128_gflops_factor": world * float((ns.astype(np.float64) ** 3).sum() / 3.0) / (ms * 1e-3) / 1e9,
            "refine_iterations_max": int(it.cpu().numpy().max()),
+           "accuracy": acc,
            "launch": "one persistent kernel (work queue, largest-first) replayed from a CUDA graph",
            "launch_shape": dict(zip(("threads_per_cta", "ctas_per_sm"), hp.batched_config()),
                                 picked_by="autotuner (every candidate timed on this batch at the first call)")}
+    # FP64-pipe roofline of the persistent kernel: the factorisations alone
+    # are sum n^3/6 f128 multiply-adds of 29 FP64 instructions each
+    # (reference-order Add + Mul); assembly, solves and refinement add more
+    fp64_peak = getattr(args, "fp64_tflops", None)
+    instr = float((ns.astype(np.float64) ** 3).sum() / 6.0) * 29.0
+    achieved = world * instr / (ms * 1e-3) / 1e12  # T FP64 instructions / s
+    out["roofline"] = {"bound": "fp64", "kernel": "batched_spd_kernel (persistent, graph-replayed)",
+                       "achieved": achieved, "unit": "T FP64 instr/s (factorisation only)",
+                       "peak": fp64_peak / 2.0 if fp64_peak else None,
+                       "frac": achieved / (fp64_peak / 2.0) if fp64_peak else None,
+                       "peak_source": "hp_measure_peaks DFMA loop, this run (TFLOP/s / 2)",
+                       "algorithmic": "sum_s n_s^3/6 f128 multiply-adds x 29 FP64 instructions"}
+    if getattr(args, "cpu_leg", False):
+        out["cpu_baseline"] = cpu_batched_sample(B)
     # batched Jacobi on the n <= 128 systems
     sel = np.nonzero(ns <= 128)[0]
     joff = np.zeros(len(sel) + 1, dtype=np.int64)
@@ -460,6 +510,63 @@ def batched_section(hp, torch, dev, stream, sptr, args, world, dist):
 
 
 ADJ_LATTICE = (5, 5, 10)  # 250 centres x 4 exponents = 1000 basis functions
+
+
+def cpu_batched_sample(B, target_s: float = 15.0) -> dict:
+    """The batch on the host cores (oracle.batched_refined: each system
+    assembled in f128, reference f128 cholesky + solve_cholesky, refinement
+    with f256 residuals; OpenMP over systems) on a bounded sample: every
+    stride-th system in size order, the rate scaled to the whole batch by
+    sum n^3 (the factorisations' share of the work)."""
+    import numpy as np
+
+    import oracle
+
+    off = B["offsets"]
+    ns = np.diff(off)
+    order = np.argsort(ns, kind="stable")
+    stride = 16
+    while True:
+        sel = order[::stride]
+        sub = {"offsets": np.concatenate([[0], np.cumsum(ns[sel])]).astype(np.int64),
+               "centers": np.concatenate([B["centers"][off[i]:off[i + 1]] for i in sel]),
+               "alpha": np.concatenate([B["alpha"][off[i]:off[i + 1]] for i in sel]),
+               "b": np.concatenate([B["b"][off[i]:off[i + 1]] for i in sel])}
+        t0 = time.perf_counter()
+        _, it = oracle.batched_refined(sub)
+        dt = time.perf_counter() - t0
+        if dt * 4 > target_s or stride <= 2:
+            break
+        stride //= 2
+    w_all = float((ns.astype(np.float64) ** 3).sum())
+    w_sub = float((ns[sel].astype(np.float64) ** 3).sum())
+    est = dt * w_all / w_sub
+    return {"value": len(ns) / est, "unit": "systems/s", "cores": oracle.num_threads(), "kind": "port",
+            "sample": f"{len(sel)} of {len(ns)} systems (every {stride}th in size order, n {int(ns[sel].min())}-"
+                      f"{int(ns[sel].max())}), {dt:.2f} s, scaled to the batch by sum n^3; all steps converged: "
+                      f"{bool((it > 0).all())}"}
+
+
+def adjoint_fd_error(gR, ga):
+    """Largest |g - g_fd| over the 56 parameters of tests/golden/adjoint_fd_1000.npz
+    (f256 central differences, h = 1e-20), relative to the largest component."""
+    import numpy as np
+
+    p = os.path.join(REPO, "tests", "golden", "adjoint_fd_1000.npz")
+    if not os.path.exists(p):
+        return None
+    fx = np.load(p)
+    gmax = max(np.abs(gR[..., 0]).max(), np.abs(ga[..., 0]).max())
+    errs = []
+    for ci, c in enumerate(fx["centres"]):
+        for comp in range(3):
+            fd, g = fx["gR"][ci, comp], gR[c, comp]
+            errs.append(abs(((g[0] - fd[0]) + (g[1] - fd[1])) - fd[2] - fd[3]))
+    for qi, u in enumerate(fx["funcs"]):
+        fd, g = fx["ga"][qi], ga[u]
+        errs.append(abs(((g[0] - fd[0]) + (g[1] - fd[1])) - fd[2] - fd[3]))
+    return {"max_abs_err_over_max_component": float(max(errs) / gmax), "parameters": len(errs),
+            "reference": "f256 central differences, h = 1e-20 (tests/golden/adjoint_fd_1000.npz)"}
 
 
 def adjoint_section(hp, torch, dev, stream, sptr, args, world, dist):
@@ -505,13 +612,124 @@ def adjoint_section(hp, torch, dev, stream, sptr, args, world, dist):
         e0.record(stream)
         torch.cuda.synchronize()
         ms = max_over_ranks(s0.elapsed_time(e0) / steps, dist, dev)
-        out[name] = {"gradients_per_s": world * 1e3 / ms, "ms_per_gradient": ms, "converged": bool(info.converged)}
+        out[name] = {"gradients_per_s": world * 1e3 / ms, "ms_per_gradient": ms, "converged": bool(info.converged),
+                     "accuracy_vs_f256_fd": adjoint_fd_error(gR.cpu().numpy(), ga.cpu().numpy())}
     out["chosen_over_plain"] = out["chosen"]["gradients_per_s"] / out["plain"]["gradients_per_s"]
+    if getattr(args, "cpu_leg", False):
+        import oracle
+
+        t0 = time.perf_counter()
+        _, cgR, cga = oracle.adjoint_f128_refined(cen, alpha, b, co, nc)
+        dt = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "gradients/s", "cores": oracle.num_threads(),
+                               "kind": "port", "accuracy_vs_f256_fd": adjoint_fd_error(cgR, cga),
+                               "sample": f"one full gradient, {dt:.2f} s: S in f128, lambda from the reference's "
+                                         "f128 cholesky + solve_cholesky refined with f256 residuals, then the "
+                                         "f128 contraction -lambda^T dS lambda (OpenMP rows)"}
+    return out
+
+
+CH_N = 512  # the plain f128 Cholesky solve of the reference's README matrix
+
+
+def cholesky512_section(hp, torch, dev, stream, sptr, args, world, dist):
+    """The reference's own plain path at n = 512: cholesky + solve_cholesky
+    (crates/quad/src/linalg.rs:42-126) of A_ij = 1/(i+j+1) + I, b = ones, no
+    refinement. One step = one factorisation + both triangular solves of a
+    fresh copy of A (device-resident; hp_f128_cholesky_dev synchronises its
+    stream to report a failed pivot, as the reference returns its Result)."""
+    import ctypes
+
+    import numpy as np
+
+    from quadprec_b200.workloads import shifted_hilbert
+
+    n = CH_N
+    a, b = shifted_hilbert(n)
+    lib = hp.lib()
+    dA = torch.from_numpy(a).to(dev)
+    db = torch.from_numpy(b).to(dev)
+    dL = torch.empty_like(dA)
+    dx = torch.empty_like(db)
+    pv, val = ctypes.c_int64(-1), ctypes.c_double(0.0)
+
+    def one():
+        dL.copy_(dA)
+        dx.copy_(db)
+        hp.check(lib.hp_f128_cholesky_dev(dL.data_ptr(), n, ctypes.byref(pv), ctypes.byref(val), sptr))
+        hp.check(lib.hp_f128_solve_cholesky_dev(dL.data_ptr(), dx.data_ptr(), n, sptr))
+
+    for _ in range(3):
+        one()
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    steps = 20
+    s0, e0 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for _ in range(steps):
+        one()
+    e0.record(stream)
+    torch.cuda.synchronize()
+    ms = max_over_ranks(s0.elapsed_time(e0) / steps, dist, dev)
+    x_dev = dx.cpu().numpy()
+    # end to end: the host-pointer entry points, as a caller of the Rust API would
+    L = np.empty_like(a)
+    x = np.empty_like(b)
+    ha = np.ascontiguousarray(a)
+
+    def one_host():
+        np.copyto(L, ha)
+        hp.check(lib.hp_f128_cholesky(L.ctypes.data, n, ctypes.byref(pv), ctypes.byref(val)))
+        hp.check(lib.hp_f128_solve_cholesky(L.ctypes.data, b.ctypes.data, x.ctypes.data, n))
+
+    one_host()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        one_host()
+    e2e_ms = max_over_ranks((time.perf_counter() - t0) * 1e3 / steps, dist, dev)
+    fma = n ** 3 / 6.0 + n * n  # f128 multiply-adds: factorisation + two triangular solves
+    fp64_peak = getattr(args, "fp64_tflops", None)
+    instr_rate = 29.0 * fma / (ms * 1e-3) / 1e12
+    out = {"workload": "plain f128 Cholesky solve (cholesky + solve_cholesky), n = 512, A_ij = 1/(i+j+1) + I "
+                       "(README matrix), b = ones, no refinement", "n": n, "unit": "solves/s",
+           "solves_per_s": world * 1e3 / ms, "ms_per_solve": ms,
+           "e2e": {"solves_per_s": world * 1e3 / e2e_ms, "ms_per_solve": e2e_ms,
+                   "path": "hp_f128_cholesky + hp_f128_solve_cholesky (host pointers, copies inside)",
+                   "h2d_bytes_per_step": int(n * n * 16 * 2 + n * 16), "d2h_bytes_per_step": int(n * n * 16 + n * 16)},
+           "roofline": {"bound": "fp64", "achieved": instr_rate, "unit": "T FP64 instr/s",
+                        "peak": fp64_peak / 2.0 if fp64_peak else None,
+                        "frac": instr_rate / (fp64_peak / 2.0) if fp64_peak else None,
+                        "algorithmic": "(n^3/6 + n^2) f128 multiply-adds x 29 FP64 instructions (reference Add + Mul)",
+                        "peak_source": "hp_measure_peaks DFMA loop, this run (TFLOP/s / 2)"},
+           "f128_gflops": world * 2.0 * fma / (ms * 1e-3) / 1e9}
+    if getattr(args, "cpu_leg", False):
+        import oracle
+
+        res = {}
+        for cores in (oracle.num_threads(), 1):
+            prev = oracle.num_threads()
+            oracle.set_threads(cores)
+            t0 = time.perf_counter()
+            Lc = oracle.cholesky(a, n)
+            xc = oracle.solve_cholesky(Lc, b, n)
+            res[cores] = time.perf_counter() - t0
+            oracle.set_threads(prev)
+        d = (x_dev[:, 0] - xc[:, 0]) + (x_dev[:, 1] - xc[:, 1])
+        out["cpu_baseline"] = {"value": 1.0 / res[max(res)], "unit": "solves/s", "cores": max(res), "kind": "port",
+                               "value_1_core": 1.0 / res[1],
+                               "gpu_vs_cpu_normwise_diff": float(np.linalg.norm(d) / np.linalg.norm(xc[:, 0])),
+                               "sample": f"one full solve on all cores ({res[max(res)]:.3f} s) and on 1 core "
+                                         f"({res[1]:.3f} s): the reference's cholesky + solve_cholesky restated"}
     return out
 
 
 def cpu_spd_sample() -> dict:
-    """The reference's solve_spd_f128 (solver/src/lib.rs:71) on the same S, host cores."""
+    """The same computation on the host cores: the reference's f128 cholesky +
+    solve_cholesky refined with f256 residuals to the same 1e-28 stopping rule
+    (oracle.spd_solve_refined; the reference's own solve_spd_f128 refines
+    with f128 residuals and stalls near 1e-17 on this matrix), plus the
+    assembly of S."""
     import numpy as np
 
     import oracle
@@ -519,21 +737,21 @@ def cpu_spd_sample() -> dict:
 
     cen, alpha, b = overlap_spd_problem(*SPD_LATTICE, seed=0)
     n = len(alpha)
-    S = oracle.overlap_norm_dd(cen, alpha)
-    b2 = np.stack([b, np.zeros_like(b)], -1)
     t0 = time.perf_counter()
-    sol = oracle.solve_spd_f128(S, b2, n)
+    S = oracle.overlap_norm_dd(cen, alpha)
+    x, steps = oracle.spd_solve_refined(S, b, n)
     dt = time.perf_counter() - t0
     fix = os.path.join(REPO, "tests", "golden", "overlap_5x10x10.npz")
     err = None
     if os.path.exists(fix):
         xs = np.load(fix)["x_star"]
-        x = sol["x"]
         d = (xs[:, 0] - x[:, 0]) + (xs[:, 1] - x[:, 1]) + xs[:, 2] + xs[:, 3]
         err = float(np.linalg.norm(d) / np.linalg.norm(xs[:, 0]))
     return {"value": 1.0 / dt, "unit": "solves/s", "cores": oracle.num_threads(), "kind": "port",
-            "sample": f"one solve_spd_f128 (f128 cholesky + solve_cholesky, crates/solver/src/lib.rs:127-144) "
-                      f"of the same n={n} S, {dt:.2f} s; reaches rel err {err} (f128 alone cannot reach 1e-25)"}
+            "rel_err_vs_f512": err,
+            "sample": f"one full solve of the same n={n} system, {dt:.2f} s: assembly of S in f128, the reference's "
+                      f"f128 cholesky + solve_cholesky (crates/quad/src/linalg.rs:42-126) and {steps} refinement "
+                      "steps with f256 residuals (mf_gemv semantics, multifloat/linalg.rs:17-37), OpenMP rows"}
 
 
 def profile_case_spd(args):
@@ -624,6 +842,11 @@ def main():
         barrier()
         return max_over_ranks(sum(s.elapsed_time(e) for s, e in evs) / steps, dist, dev)
 
+    # roofline denominators measured on this device (DFMA loop, tcgen05 kind::i8 loop)
+    pk = hp.measure_peaks(5)
+    args.fp64_tflops = pk["fp64_tflops"]
+    args.cpu_leg = rank == 0 and world == 1 and not args.no_cpu
+
     flops = 2.0 * M * N * K
     clk = ClockSampler(local)
     clk.start()
@@ -641,6 +864,10 @@ def main():
     diff = (c_oz[..., 0] - c_pl[..., 0]) + (c_oz[..., 1] - c_pl[..., 1])
     absab = np.abs(a_np[..., 0]) @ np.abs(b_np[..., 0])
     rel_err = float(np.linalg.norm(diff) / np.linalg.norm(absab))
+    # errors against the f512 oracle (fixture of the seed-0 operands)
+    err_f512 = ({"chosen": f512_errors(c_oz, a_np, b_np, "f128_gemm_2048"),
+                 "plain": f512_errors(c_pl, a_np, b_np, "f128_gemm_2048"),
+                 "bound": 4 * K * 2.0 ** -104} if rank == 0 else None)
 
     # phase timing of one chosen-path step (dominant kernel roofline)
     flush.fill_(1.0)
@@ -652,7 +879,7 @@ def main():
 
     L = 30
     hbm_gbs, bf16_tf, peak_kind = peaks()
-    i8_peak = 2.0 * bf16_tf  # dense int8 issue rate is twice dense bf16 on B200
+    i8_peak = pk["i8_tops"]
     mm = phases.get("i8_gemm", float("nan"))
     i8_tops = L * 2.0 * M * N * K / (mm * 1e-3) / 1e12
     res_ms = phases.get("residues", float("nan"))
@@ -663,9 +890,10 @@ def main():
                 "30 moduli)", "achieved": i8_tops, "peak": i8_peak, "unit": "TOPS (int8)",
                 "frac": i8_tops / i8_peak, "traffic": I8_GEMM_TRAFFIC_BYTES,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch at 2048^3",
-                "peak_source": (f"2 x measured dense bf16 ({bf16_tf} TFLOP/s, MEASURED_PEAKS.json)"
-                                if peak_kind == "measured" else
-                                f"2 x fallback dense bf16 ({bf16_tf} TFLOP/s; MEASURED_PEAKS.json absent)"),
+                "peak_source": ("measured in this run by hp_measure_peaks: tcgen05.mma kind::i8 (u8, M=128, "
+                                "N=256, K=32) back to back on every SM, CUDA events; for comparison 2 x the "
+                                f"{peak_kind} dense bf16 figure = {2.0 * bf16_tf:.1f} TOPS"),
+                "frac_of_2x_bf16": i8_tops / (2.0 * bf16_tf),
                 "algorithmic": f"{L} moduli x 2mnk int8 ops = {L * 2.0 * M * N * K:.3e} per launch"}
     phase_report = {k: round(v, 4) for k, v in phases.items()}
     phase_roofline = {
@@ -688,13 +916,15 @@ def main():
     e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps, dist, dev)
 
     more = gemm_more_section(hp, torch, dev, stream, sptr, world, dist)
+    chol512 = cholesky512_section(hp, torch, dev, stream, sptr, args, world, dist)
     spd = None if args.no_spd else spd_section(hp, torch, dev, stream, sptr, args, rank, world, dist)
     batched = None if args.no_batched else batched_section(hp, torch, dev, stream, sptr, args, world, dist)
     adjoint = None if args.no_adjoint else adjoint_section(hp, torch, dev, stream, sptr, args, world, dist)
 
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if args.cpu_leg:
         cpu = cpu_sample_gflops()
+        cpu["value_1_core"] = cpu_sample_gflops(target_s=4.0, threads=1)["value"]
         if spd is not None:
             spd["cpu_baseline"] = cpu_spd_sample()
 
@@ -712,6 +942,10 @@ def main():
                   "mode": "plain CUDA-core dd FMA, bit-identical to the reference"},
         "chosen_over_plain": value / plain_value,
         "normwise_rel_err_vs_plain": rel_err,
+        "err_vs_f512": err_f512,
+        "peaks_measured": {"fp64_tflops": pk["fp64_tflops"], "i8_tops": pk["i8_tops"],
+                           "how": "hp_measure_peaks: DFMA loop (8 chains per thread, 8 CTAs of 256 per SM) and "
+                                  "tcgen05.mma kind::i8 loop (one CTA per SM), best of 5, CUDA events"},
         "e2e": {"value": world * flops / e2e_s / 1e9, "unit": "GFLOP/s",
                 "h2d_bytes_per_step": int(2 * M * K * 16), "d2h_bytes_per_step": int(M * N * 16),
                 "path": "hp_f128_gemm (host pointers, pinned), copies inside the timed region"},
@@ -722,6 +956,7 @@ def main():
     if cpu is not None:
         line["cpu_baseline"] = cpu
     line["gemm_more"] = more
+    line["cholesky_512"] = chol512
     if spd is not None:
         line["spd"] = spd
     if batched is not None:

@@ -83,6 +83,14 @@ int hp_device_status(void* stream, uint32_t* bits, int clear);
 int hp_debug_trsv_wavefront(const double* l, const double* b, double* x, size_t n, int upper_t,
                             uint64_t wait_ns, int withheld_block);
 
+/* Roofline denominators measured on the current device (no counterpart in
+ * the reference): a DFMA loop at full occupancy (FP64 pipe, 2 flops per DFMA)
+ * and a tcgen05.mma kind::i8 loop (one CTA per SM, M = 128, N = 256, K = 32
+ * unsigned MMAs from shared memory into TMEM). Each runs reps + 1 times; the
+ * best of the last reps is returned as fp64_tflops / i8_tops (TFLOP/s, TOP/s)
+ * and its duration in ms. Any output pointer may be NULL. */
+int hp_measure_peaks(int reps, double* fp64_tflops, double* i8_tops, double* fp64_ms, double* i8_ms);
+
 /* Phase timing for benchmarks (no counterpart in the reference). While
  * enabled, the multi-kernel drivers record a CUDA event at each phase
  * boundary on their stream; hp_profile_read() waits for the last one and
@@ -167,9 +175,22 @@ int hp_f128_forward_solve(const double* l, const double* b, double* y, size_t n)
 int hp_f128_backward_solve(const double* l, const double* y, double* x, size_t n);
 /* replaces: pub fn solve_cholesky(l, b, n) -> Vec<f128>  linalg.rs:123-126 */
 int hp_f128_solve_cholesky(const double* l, const double* b, double* x, size_t n);
+/* Device-pointer form of hp_f128_solve_cholesky: x holds b on entry and
+ * L^-T L^-1 b on return (stream-ordered, the same kernels). */
+int hp_f128_solve_cholesky_dev(const double* l, double* x, size_t n, void* stream);
 /* replaces: pub fn matvec(a, x, n) -> Vec<f128>          linalg.rs:129-147
  * bit-identical. */
 int hp_f128_matvec(const double* a, const double* x, double* y, size_t n);
+/* replaces: pub fn dot(a: &[f128], b: &[f128]) -> f128   linalg.rs:7-26
+ * Below 1024 entries the serial sum (bit-identical); otherwise the serial
+ * sums of the 1024-entry chunks are folded left to right from zero (one
+ * order of the reference's rayon reduce, bit-identical to it). out: 1 f128. */
+int hp_f128_dot(const double* a, const double* b, size_t len, double* out);
+/* replaces: pub fn gemv(a: &[f128], rows, cols, x: &[f128], y: &mut [f128])
+ *           linalg.rs:29-38
+ * y (rows) = A (rows x cols) x; each row summed in column order
+ * (bit-identical). */
+int hp_f128_gemv(const double* a, size_t rows, size_t cols, const double* x, double* y);
 /* replaces: pub fn cond_estimate(l, n) -> f64            linalg.rs:185-194 */
 int hp_f128_cond_estimate(const double* l, size_t n, double* kappa);
 

@@ -89,6 +89,13 @@ def lib():
             "or_overlap_norm_dd": ([_sz, _d, _d, _d], None),
             "or_adjoint_f128": ([_sz, _d, _d, _d, ctypes.POINTER(ctypes.c_int32), _sz, _d, _d, _d], ctypes.c_int),
             "or_loss_f256": ([_sz, _d, _d, _d, _d], ctypes.c_int),
+            "or_adjoint_f128_lambda": ([_sz, _d, _d, _d, _d, ctypes.POINTER(ctypes.c_int32), _sz, _d, _d, _d],
+                                       ctypes.c_int),
+            "or_spd_solve_refined": ([_d, _d, _sz, ctypes.c_double, ctypes.c_int, _d], ctypes.c_int),
+            "or_batched_refined": ([ctypes.c_int, _i64, _d, _d, _d, ctypes.c_double, ctypes.c_int, _d,
+                                    ctypes.POINTER(ctypes.c_int32)], ctypes.c_int),
+            "or_gemm_entries_f512": ([ctypes.c_int, _d, _d, _d, _d, _sz, _sz, _sz, ctypes.c_int, _i64, _sz],
+                                     ctypes.c_int),
             "or_fd_grad_f256": ([_sz, _d, _d, _d, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32),
                                  _sz, ctypes.c_double, _d, _d], ctypes.c_int),
         }
@@ -271,6 +278,19 @@ def mf_gemm_entries(N, a, b, m, n, k, idx, atb=False):
     return out
 
 
+def gemm_entries_f512(a, b, m, n, k, idx, atb=False):
+    """f512 entries C[i, j] of op(A) B for f128 (..., 2) or f256 (..., 4) inputs:
+    (count x 4 leading limbs, count sums of |a||b|) -- the GEMMs' f512 checker."""
+    a, b = _f(a), _f(b)
+    limbs = a.shape[-1]
+    idx = np.ascontiguousarray(idx, dtype=np.int64)
+    out = np.zeros((len(idx), 4))
+    ab = np.zeros(len(idx))
+    assert lib().or_gemm_entries_f512(limbs, _p(a), _p(b), _p(out), _p(ab), m, n, k, int(atb),
+                                      idx.ctypes.data_as(_i64), len(idx)) == 0
+    return out, ab
+
+
 def mf_gemv(N, a, x, n, m):
     y = np.zeros((n, N))
     assert lib().or_mf_gemv(N, _p(_f(a)), _p(_f(x)), _p(y), n, m) == 0
@@ -307,6 +327,32 @@ def solve_spd(a_f64, b_f64, n):
     pv = ctypes.c_int64(0)
     rc = lib().or_solve_spd(_p(_f(a_f64)), _p(_f(b_f64)), n, _p(x), _p(xf), _p(info), ctypes.byref(pv))
     return _solution(rc, x, xf, info, pv)
+
+
+def spd_solve_refined(S, b, n, tol=1e-28, max_iter=10):
+    """f128 cholesky + solve_cholesky refined with f256 residuals (the host
+    counterpart of the GPU's plain refined solve). Returns (x (n, 2), steps)."""
+    S, b = _f(S), _f(b)
+    if b.ndim == 1:
+        b = np.stack([b, np.zeros_like(b)], -1)
+    x = np.zeros((n, 2))
+    it = lib().or_spd_solve_refined(_p(S), _p(b), n, tol, max_iter, _p(x))
+    if it < 0:
+        raise CholeskyError(-1, float("nan"))
+    return x, int(it)
+
+
+def batched_refined(batch, tol=1e-28, max_iter=10):
+    """Host counterpart of the GPU batched solver (or_batched_refined): every
+    system assembled in f128 and solved by spd_solve_refined, OpenMP over
+    systems. Returns (x (N, 2), iters (count,))."""
+    off = np.ascontiguousarray(batch["offsets"], dtype=np.int64)
+    count = len(off) - 1
+    x = np.zeros((int(off[-1]), 2))
+    it = np.zeros(count, dtype=np.int32)
+    lib().or_batched_refined(count, off.ctypes.data_as(_i64), _p(_f(batch["centers"])), _p(_f(batch["alpha"])),
+                             _p(_f(batch["b"])), tol, max_iter, _p(x), it.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)))
+    return x, it
 
 
 def solve_spd_f128(a, b, n):
@@ -377,13 +423,29 @@ def adjoint_f128(centers, alpha, b, center_of, n_centers):
     n = len(alpha)
     co = np.ascontiguousarray(center_of, dtype=np.int32)
     loss = np.zeros(2)
-    gR = np.zeros((max(n, n_centers), 3, 2))
+    gR = np.zeros((n_centers, 3, 2))
     ga = np.zeros((n, 2))
     rc = lib().or_adjoint_f128(n, _p(_f(centers)), _p(_f(alpha)), _p(_f(b)),
                                co.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), n_centers, _p(loss), _p(gR), _p(ga))
     if rc != 0:
         raise RuntimeError("not positive definite")
-    return loss, gR[:n_centers].copy(), ga
+    return loss, gR, ga
+
+
+def adjoint_f128_refined(centers, alpha, b, center_of, n_centers):
+    """The host counterpart of the GPU adjoint: lambda from the refined host
+    solve (spd_solve_refined: f128 factor, f256 residuals, to ~1e-25), then
+    the same f128 contraction. Returns (loss, gR (n_centers,3,2), ga (n,2))."""
+    n = len(alpha)
+    S = overlap_norm_dd(centers, alpha)
+    lam, _ = spd_solve_refined(S, np.asarray(b, dtype=np.float64), n)
+    co = np.ascontiguousarray(center_of, dtype=np.int32)
+    loss, gR, ga = np.zeros(2), np.zeros((n_centers, 3, 2)), np.zeros((n, 2))
+    rc = lib().or_adjoint_f128_lambda(n, _p(_f(centers)), _p(_f(alpha)), _p(_f(b)), _p(_f(lam)),
+                                      co.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), n_centers, _p(loss),
+                                      _p(gR), _p(ga))
+    assert rc == 0
+    return loss, gR, ga
 
 
 def loss_f256(centers4, alpha4, b):

@@ -608,6 +608,36 @@ int or_mf_gemm_entries(int N, const double* a, const double* b, double* out, siz
   MF_DISPATCH(N, C)
 #undef C
 }
+// f512 (MultiFloat<8>) entries of C = op(A) B for f128 (in_limbs = 2) or f256
+// (in_limbs = 4) inputs, each promoted exactly to MultiFloat<8> (the f512
+// checker of the GEMMs: every product of two 2- or 4-limb values and their
+// running sum is held to ~2^-420). out: count x 4 (the leading limbs of the
+// f512 value); absab: count doubles, sum_p |a_ip| |b_pj| over the leading limbs
+// (the normwise denominator).
+int or_gemm_entries_f512(int in_limbs, const double* a, const double* b, double* out, double* absab, size_t m,
+                         size_t n, size_t k, int atb, const int64_t* idx, size_t count) {
+  if (in_limbs != 2 && in_limbs != 4) return -1;
+  const size_t L = (size_t)in_limbs;
+  auto ld8 = [&](const double* p, size_t e) {
+    mf<8> r = mf_zero<8>();
+    for (size_t t = 0; t < L; t++) r.l[t] = p[L * e + t];
+    return r;
+  };
+#pragma omp parallel for schedule(dynamic, 4)
+  for (size_t t = 0; t < count; t++) {
+    const size_t i = (size_t)idx[2 * t], j = (size_t)idx[2 * t + 1];
+    mf<8> s = mf_zero<8>();
+    double ab = 0.0;
+    for (size_t p = 0; p < k; p++) {
+      const size_t ea = atb ? p * m + i : i * k + p, eb = p * n + j;
+      s = mf_add<8>(s, mf_mul<8>(ld8(a, ea), ld8(b, eb)));
+      ab += std::fabs(a[L * ea]) * std::fabs(b[L * eb]);
+    }
+    for (int q = 0; q < 4; q++) out[4 * t + q] = s.l[q];
+    absab[t] = ab;
+  }
+  return 0;
+}
 int or_mf_gemv(int N, const double* a, const double* x, double* y, size_t n, size_t m) {
 #define C(K) mf_gemv_t<K>(a, x, y, n, m)
   MF_DISPATCH(N, C)
@@ -656,6 +686,82 @@ static int solve_pure_f128_v(const std::vector<dd>& a128, const std::vector<dd>&
   info[3] = 0;
   return 0;
 }
+// Refined SPD solve to ~1e-25 on the host (the CPU counterpart of the GPU's
+// plain refined mode, used as its timed baseline): the reference's f128
+// cholesky (linalg.rs:42-96) and solve_cholesky (linalg.rs:123-126), and the
+// iterative_refinement loop of solver/src/lib.rs:75-125 with its residual
+// evaluated in MultiFloat<4> (mf_gemv semantics, multifloat/linalg.rs:17-37:
+// S and x promoted exactly, r = b - S x accumulated in f256 and rounded to
+// f128) instead of f128, until max|dx| <= tol max|x| or max_iter steps.
+// S: n x n f128, b: n f128; x: n f128. Returns the steps taken, or -2 if
+// the factorisation fails.
+int or_spd_solve_refined(const double* S, const double* b, size_t n, double tol, int max_iter, double* x_out) {
+  std::vector<dd> L = load_vec(S, n * n);
+  int64_t pv;
+  double val;
+  if (cholesky_vec(L, n, &pv, &val) != 0) return -2;
+  const std::vector<dd> bv = load_vec(b, n);
+  std::vector<dd> x = backward_solve_v(L, forward_solve_v(L, bv, n), n);
+  int it = 0;
+  for (; it < max_iter; it++) {
+    std::vector<dd> r(n);
+#pragma omp parallel for schedule(static) if (n >= PAR_THRESHOLD)
+    for (size_t i = 0; i < n; i++) {
+      mf<4> acc = mf_zero<4>();
+      for (size_t j = 0; j < n; j++) {
+        mf<4> sij = mf_zero<4>(), xj = mf_zero<4>();
+        sij.l[0] = S[2 * (i * n + j)];
+        sij.l[1] = S[2 * (i * n + j) + 1];
+        xj.l[0] = x[j].hi;
+        xj.l[1] = x[j].lo;
+        acc = mf_add<4>(acc, mf_mul<4>(sij, xj));
+      }
+      mf<4> bi = mf_zero<4>();
+      bi.l[0] = bv[i].hi;
+      bi.l[1] = bv[i].lo;
+      const mf<4> ri = mf_sub<4>(bi, acc);
+      r[i] = dd_renorm(ri.l[0], ri.l[1] + ri.l[2]);
+    }
+    const std::vector<dd> dx = backward_solve_v(L, forward_solve_v(L, r, n), n);
+    double mdx = 0.0, mx = 0.0;
+    for (size_t i = 0; i < n; i++) {
+      x[i] = dd_add(x[i], dx[i]);
+      mdx = std::max(mdx, std::fabs(dx[i].hi));
+      mx = std::max(mx, std::fabs(x[i].hi));
+    }
+    if (mdx <= tol * mx) {
+      it++;
+      break;
+    }
+  }
+  store_vec(x_out, x);
+  return it;
+}
+// A batch of overlap SPD systems solved on the host (the CPU counterpart of
+// the GPU's batched solver): OpenMP over systems, each assembled in f128
+// (the normalised s-Gaussian formula, dd.rs arithmetic) and solved by
+// or_spd_solve_refined on one thread. System s owns basis functions
+// offsets[s] .. offsets[s+1]-1 (centres 3 doubles, exponents, b f64); x is
+// f128 per basis function; iters[s] = steps taken or -2 (not SPD).
+int or_batched_refined(int count, const int64_t* offsets, const double* centers, const double* alpha,
+                       const double* b, double tol, int max_iter, double* x, int32_t* iters) {
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int s = 0; s < count; s++) {
+    const size_t o = (size_t)offsets[s], n = (size_t)(offsets[s + 1] - offsets[s]);
+    std::vector<double> S(n * n * 2), bb(n * 2, 0.0);
+    for (size_t i = 0; i < n; i++) {
+      bb[2 * i] = b[o + i];
+      for (size_t j = 0; j <= i; j++) {
+        const dd v = overlap_norm_dd(alpha[o + i], centers + 3 * (o + i), alpha[o + j], centers + 3 * (o + j));
+        st(S.data(), i * n + j, v);
+        st(S.data(), j * n + i, v);
+      }
+    }
+    iters[s] = or_spd_solve_refined(S.data(), bb.data(), n, tol, max_iter, x + 2 * o);
+  }
+  return 0;
+}
+
 int or_solve_spd_f128(const double* a, const double* b, size_t n, double* x_out, double* xf_out,
                       double* info, int64_t* pivot) {
   return solve_pure_f128_v(load_vec(a, n * n), load_vec(b, n), n, x_out, xf_out, info, pivot);
@@ -932,27 +1038,19 @@ extern "C" {
 // "Reference-primitive" gradient: lambda from the reference's f128
 // cholesky + solve_cholesky (linalg.rs:42-126) and the contraction in f128
 // operations, row by row in index order.
-int or_adjoint_f128(size_t n, const double* centers, const double* alpha, const double* b,
-                    const int32_t* center_of, size_t n_centers, double* loss, double* grad_R,
-                    double* grad_lnalpha) {
-  std::vector<dd> S(n * n);
-  for (size_t i = 0; i < n; i++)
-    for (size_t j = 0; j <= i; j++) {
-      dd v = overlap_norm_dd(alpha[i], centers + 3 * i, alpha[j], centers + 3 * j);
-      S[i * n + j] = v;
-      S[j * n + i] = v;
-    }
-  std::vector<dd> L = S;
-  int64_t pv;
-  double val;
-  if (cholesky_vec(L, n, &pv, &val) != 0) return -2;
-  std::vector<dd> bv(n);
-  for (size_t i = 0; i < n; i++) bv[i] = dd_from(b[i]);
-  std::vector<dd> lam = backward_solve_v(L, forward_solve_v(L, bv, n), n);
+}  // extern "C"
+
+namespace {
+// Loss and gradient of L = b^T S^-1 b given lambda = S^-1 b (f128): the
+// contraction g = -lambda^T (dS/dtheta) lambda with dS built from f128 ops.
+// grad_R: n_centers x 3 f128, grad_lnalpha: n f128.
+void adjoint_contract(size_t n, const double* centers, const double* alpha, const std::vector<dd>& S,
+                      const std::vector<dd>& bv, const std::vector<dd>& lam, const int32_t* center_of,
+                      size_t n_centers, double* loss, double* grad_R, double* grad_lnalpha) {
   dd Lsum{0, 0};
   for (size_t i = 0; i < n; i++) Lsum = dd_add(Lsum, dd_mul(bv[i], lam[i]));
   st(loss, 0, Lsum);
-  std::vector<dd> gR(3 * n_centers, dd{0, 0});
+  std::vector<dd> per(3 * n);
 #pragma omp parallel for schedule(dynamic, 8)
   for (size_t u = 0; u < n; u++) {
     dd accR[3] = {{0, 0}, {0, 0}, {0, 0}}, acca{0, 0};
@@ -974,16 +1072,57 @@ int or_adjoint_f128(size_t n, const double* centers, const double* alpha, const 
       acca = dd_add(acca, dd_mul(w, f));
     }
     const dd l4 = dd_mul(dd_from(4.0), lam[u]);
-    for (int c = 0; c < 3; c++) st(grad_R, 3 * u + c, dd_mul(l4, accR[c]));  // per basis function first
+    for (int c = 0; c < 3; c++) per[3 * u + c] = dd_mul(l4, accR[c]);  // per basis function first
     st(grad_lnalpha, u, dd_mul(dd_from(-2.0), dd_mul(lam[u], acca)));
   }
   // sum basis-function contributions per centre (index order)
-  std::vector<dd> per(3 * n);
-  for (size_t u = 0; u < 3 * n; u++) per[u] = ld(grad_R, u);
-  for (size_t c = 0; c < 3 * n_centers; c++) gR[c] = dd{0, 0};
+  std::vector<dd> gR(3 * n_centers, dd{0, 0});
   for (size_t u = 0; u < n; u++)
     for (int c = 0; c < 3; c++) gR[3 * center_of[u] + c] = dd_add(gR[3 * center_of[u] + c], per[3 * u + c]);
   for (size_t c = 0; c < 3 * n_centers; c++) st(grad_R, c, gR[c]);
+}
+
+std::vector<dd> overlap_matrix_dd(size_t n, const double* centers, const double* alpha) {
+  std::vector<dd> S(n * n);
+  for (size_t i = 0; i < n; i++)
+    for (size_t j = 0; j <= i; j++) {
+      dd v = overlap_norm_dd(alpha[i], centers + 3 * i, alpha[j], centers + 3 * j);
+      S[i * n + j] = v;
+      S[j * n + i] = v;
+    }
+  return S;
+}
+}  // namespace
+
+extern "C" {
+
+// The reference-primitive gradient: lambda from the restated f128 cholesky
+// and solve_cholesky (linalg.rs:42-126), then the contraction above.
+int or_adjoint_f128(size_t n, const double* centers, const double* alpha, const double* b,
+                    const int32_t* center_of, size_t n_centers, double* loss, double* grad_R,
+                    double* grad_lnalpha) {
+  const std::vector<dd> S = overlap_matrix_dd(n, centers, alpha);
+  std::vector<dd> L = S;
+  int64_t pv;
+  double val;
+  if (cholesky_vec(L, n, &pv, &val) != 0) return -2;
+  std::vector<dd> bv(n);
+  for (size_t i = 0; i < n; i++) bv[i] = dd_from(b[i]);
+  const std::vector<dd> lam = backward_solve_v(L, forward_solve_v(L, bv, n), n);
+  adjoint_contract(n, centers, alpha, S, bv, lam, center_of, n_centers, loss, grad_R, grad_lnalpha);
+  return 0;
+}
+
+// The same contraction with a given lambda (n f128), e.g. from the refined
+// host solve (or_spd_solve_refined): the host counterpart of the GPU adjoint.
+int or_adjoint_f128_lambda(size_t n, const double* centers, const double* alpha, const double* b,
+                           const double* lam_in, const int32_t* center_of, size_t n_centers, double* loss,
+                           double* grad_R, double* grad_lnalpha) {
+  const std::vector<dd> S = overlap_matrix_dd(n, centers, alpha);
+  std::vector<dd> bv(n);
+  for (size_t i = 0; i < n; i++) bv[i] = dd_from(b[i]);
+  adjoint_contract(n, centers, alpha, S, bv, load_vec(lam_in, n), center_of, n_centers, loss, grad_R,
+                   grad_lnalpha);
   return 0;
 }
 

@@ -49,6 +49,7 @@ SIGNATURES = {
     "hp_version": ([], ctypes.c_char_p),
     "hp_device_ok": ([], ctypes.c_int),
     "hp_device_status": ([_vp, ctypes.POINTER(ctypes.c_uint32), ctypes.c_int], ctypes.c_int),
+    "hp_measure_peaks": ([ctypes.c_int, _d, _d, _d, _d], ctypes.c_int),
     "hp_debug_trsv_wavefront": ([_vp, _vp, _vp, _sz, ctypes.c_int, ctypes.c_uint64, ctypes.c_int], ctypes.c_int),
     "hp_profile_enable": ([ctypes.c_int], None),
     "hp_profile_read": ([_d, ctypes.c_int, ctypes.c_char_p, _sz], ctypes.c_int),
@@ -68,6 +69,9 @@ SIGNATURES = {
     "hp_f128_backward_solve": ([_vp, _vp, _vp, _sz], ctypes.c_int),
     "hp_f128_solve_cholesky": ([_vp, _vp, _vp, _sz], ctypes.c_int),
     "hp_f128_matvec": ([_vp, _vp, _vp, _sz], ctypes.c_int),
+    "hp_f128_solve_cholesky_dev": ([_vp, _vp, _sz, _vp], ctypes.c_int),
+    "hp_f128_dot": ([_vp, _vp, _sz, _vp], ctypes.c_int),
+    "hp_f128_gemv": ([_vp, _sz, _sz, _vp, _vp], ctypes.c_int),
     "hp_f128_cond_estimate": ([_vp, _sz, _d], ctypes.c_int),
     "hp_f256_cholesky": ([_vp, _sz, _i64p], ctypes.c_int),
     "hp_f256_cholesky_dev": ([_vp, _sz, _i64p, _vp], ctypes.c_int),
@@ -291,6 +295,13 @@ def f128_solve_cholesky(l, b, n): return _solve("hp_f128_solve_cholesky", l, b, 
 def f128_matvec(a, x, n): return _solve("hp_f128_matvec", a, x, n)
 
 
+def measure_peaks(reps=5) -> dict:
+    """Measured FP64 (TFLOP/s) and int8 tensor (TOP/s) rates of this device."""
+    v = [ctypes.c_double(0.0) for _ in range(4)]
+    check(lib().hp_measure_peaks(reps, *[ctypes.byref(x) for x in v]))
+    return {"fp64_tflops": v[0].value, "i8_tops": v[1].value, "fp64_ms": v[2].value, "i8_ms": v[3].value}
+
+
 def device_status(stream=0, clear=True) -> tuple[int, int]:
     """(return code, status bits) of the *_dev calls enqueued on `stream`."""
     bits = ctypes.c_uint32(0)
@@ -305,6 +316,22 @@ def debug_trsv_wavefront(l, b, n, upper_t=False, wait_ns=0, withheld_block=-1):
     rc = lib().hp_debug_trsv_wavefront(_ptr(l), _ptr(b), _ptr(x), n, int(upper_t), int(wait_ns),
                                        int(withheld_block))
     return rc, x
+
+
+def f128_dot(a, b) -> np.ndarray:
+    """linalg.rs:7 dot: one f128 (2,)."""
+    a, b = _c(a), _c(b)
+    out = np.zeros(2)
+    check(lib().hp_f128_dot(_ptr(a), _ptr(b), len(a), _ptr(out)))
+    return out
+
+
+def f128_gemv(a, rows, cols, x) -> np.ndarray:
+    """linalg.rs:29 gemv: y (rows, 2) = A (rows x cols) x."""
+    a, x = _c(a), _c(x)
+    y = np.zeros((rows, 2))
+    check(lib().hp_f128_gemv(_ptr(a), rows, cols, _ptr(x), _ptr(y)))
+    return y
 
 
 def f128_cond_estimate(l, n) -> float:

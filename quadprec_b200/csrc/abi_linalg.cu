@@ -134,6 +134,67 @@ int hp_f128_solve_cholesky(const double* l, const double* b, double* x, size_t n
   return hp::trsv_host(l, b, x, n, 2);
 }
 
+int hp_f128_solve_cholesky_dev(const double* l, double* x, size_t n, void* stream) {
+  size_t bytes;
+  HP_TRY(hp::check_sq(n, 2, &bytes));
+  if (n == 0) return HP_OK;
+  if (!l || !x) {
+    hp::set_error("null pointer");
+    return HP_ERR_INVALID_ARG;
+  }
+  cudaStream_t s = (cudaStream_t)stream;
+  HP_TRY(hp::dd_trsv(l, x, n, false, s));
+  return hp::dd_trsv(l, x, n, true, s);
+}
+
+int hp_f128_dot(const double* a, const double* b, size_t len, double* out) {
+  size_t bytes;
+  if (hp::mul_overflows(len, 16, &bytes)) {
+    hp::set_error("length overflows size_t");
+    return HP_ERR_INVALID_ARG;
+  }
+  if (!out || (len && (!a || !b))) {
+    hp::set_error("null pointer");
+    return HP_ERR_INVALID_ARG;
+  }
+  if (len == 0) {
+    out[0] = out[1] = 0.0;
+    return HP_OK;
+  }
+  cudaStream_t s = hp::library_stream();
+  const size_t nch = (len + 1023) / 1024;
+  hp::DevBuf da(bytes, s), db(bytes, s), dp(nch * 16, s), dout(16, s);
+  if (!da.p || !db.p || !dp.p || !dout.p) return HP_ERR_CUDA;
+  HP_CUDA_TRY(cudaMemcpyAsync(da.p, a, bytes, cudaMemcpyHostToDevice, s));
+  HP_CUDA_TRY(cudaMemcpyAsync(db.p, b, bytes, cudaMemcpyHostToDevice, s));
+  HP_TRY(hp::dd_dot(da.as<double>(), db.as<double>(), len, dp.as<double>(), dout.as<double>(), s));
+  HP_CUDA_TRY(cudaMemcpyAsync(out, dout.p, 16, cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  return HP_OK;
+}
+
+int hp_f128_gemv(const double* a, size_t rows, size_t cols, const double* x, double* y) {
+  size_t t, bytes;
+  if (hp::mul_overflows(rows, cols, &t) || hp::mul_overflows(t, 16, &bytes) || hp::mul_overflows(cols, 16, &t)) {
+    hp::set_error("matrix size overflows size_t");
+    return HP_ERR_INVALID_ARG;
+  }
+  if (rows == 0) return HP_OK;
+  if (!y || (cols && (!a || !x))) {
+    hp::set_error("null pointer");
+    return HP_ERR_INVALID_ARG;
+  }
+  cudaStream_t s = hp::library_stream();
+  hp::DevBuf da(bytes, s), dx(cols * 16, s), dy(rows * 16, s);
+  if ((bytes && !da.p) || (cols && !dx.p) || !dy.p) return HP_ERR_CUDA;
+  if (bytes) HP_CUDA_TRY(cudaMemcpyAsync(da.p, a, bytes, cudaMemcpyHostToDevice, s));
+  if (cols) HP_CUDA_TRY(cudaMemcpyAsync(dx.p, x, cols * 16, cudaMemcpyHostToDevice, s));
+  HP_TRY(hp::dd_matvec(da.as<double>(), dx.as<double>(), dy.as<double>(), rows, cols, s));
+  HP_CUDA_TRY(cudaMemcpyAsync(y, dy.p, rows * 16, cudaMemcpyDeviceToHost, s));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  return HP_OK;
+}
+
 int hp_f128_matvec(const double* a, const double* x, double* y, size_t n) {
   size_t bytes;
   HP_TRY(hp::check_sq(n, 2, &bytes));

@@ -37,6 +37,8 @@ int f64_cholesky(double* a, size_t n, int64_t* pivot, cudaStream_t s);
 int dd_trsv(const double* L, double* y, size_t n, bool upper_t, cudaStream_t s);
 int f64_trsv(const double* L, double* y, size_t n, bool upper_t, cudaStream_t s);
 int dd_matvec(const double* A, const double* x, double* y, size_t rows, size_t cols, cudaStream_t s);
+// part: ceil(len / 1024) f128 of workspace; out: one f128 (device).
+int dd_dot(const double* a, const double* b, size_t len, double* part, double* out, cudaStream_t s);
 int dd_norm(const double* v, size_t n, double* out_dev, cudaStream_t s);
 int cond_estimate(const double* L, size_t n, bool is_dd, double* out_dev, cudaStream_t s);
 // op: 0 out=a-b, 1 out=a+b, 2 out=promote(f), 3 out(f64)=to_f64(a)

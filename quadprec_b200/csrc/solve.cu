@@ -179,6 +179,39 @@ int f64_trsv(const double* L, double* y, size_t n, bool upper_t, cudaStream_t s)
   if (n == 0) return HP_OK;
   return upper_t ? trsv_launch<VOpsF64, true>(L, y, n, s) : trsv_launch<VOpsF64, false>(L, y, n, s);
 }
+// dot (linalg.rs:7-26): below 1024 entries one serial sum (dot_serial);
+// otherwise each 1024-entry chunk is summed serially by one thread and the
+// chunk sums are folded left to right from zero by one thread (rayon's
+// reduce with the ZERO identity, in the order of a left fold).
+__global__ void dot_chunks_kernel(const dd* __restrict__ a, const dd* __restrict__ b, int64_t len,
+                                  dd* __restrict__ part) {
+  const int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (c * 1024 >= len) return;
+  const int64_t e = min(len, (c + 1) * 1024);
+  dd s = {0.0, 0.0};
+  for (int64_t i = c * 1024; i < e; i++) s = dd_add(s, dd_mul(a[i], b[i]));
+  part[c] = s;
+}
+__global__ void dot_fold_kernel(const dd* __restrict__ part, int64_t nch, int fold, dd* __restrict__ out) {
+  if (!fold) {
+    *out = part[0];
+    return;
+  }
+  dd t = {0.0, 0.0};
+  for (int64_t c = 0; c < nch; c++) t = dd_add(t, part[c]);
+  *out = t;
+}
+int dd_dot(const double* a, const double* b, size_t len, double* part, double* out, cudaStream_t s) {
+  const int64_t nch = ((int64_t)len + 1023) / 1024;
+  if (nch == 0) return HP_OK;
+  dot_chunks_kernel<<<(unsigned)((nch + 127) / 128), 128, 0, s>>>(
+      reinterpret_cast<const dd*>(a), reinterpret_cast<const dd*>(b), (int64_t)len, reinterpret_cast<dd*>(part));
+  HP_LAUNCH_CHECK();
+  dot_fold_kernel<<<1, 1, 0, s>>>(reinterpret_cast<const dd*>(part), nch, len >= 1024 ? 1 : 0,
+                                  reinterpret_cast<dd*>(out));
+  HP_LAUNCH_CHECK();
+  return HP_OK;
+}
 int dd_matvec(const double* A, const double* x, double* y, size_t rows, size_t cols, cudaStream_t s) {
   if (rows == 0) return HP_OK;
   matvec_dd_kernel<<<(unsigned)((rows + 127) / 128), 128, 0, s>>>(

@@ -56,6 +56,48 @@ def gemm_operands(m: int, n: int, k: int, seed: int = 0, atb: bool = False):
     return a, b
 
 
+def sample_index(m: int, n: int, count: int = 4096, seed: int = 7, rows=None) -> np.ndarray:
+    """(i, j) pairs: `count` entries from SplitMix64(seed), then every entry of
+    the rows in `rows` (default: the first and the last). Used to state a
+    GEMM's error against an f512 evaluation of sampled entries."""
+    u = uniform(2 * count, seed, 0).reshape(count, 2)
+    ij = np.stack([np.minimum((u[:, 0] * m).astype(np.int64), m - 1),
+                   np.minimum((u[:, 1] * n).astype(np.int64), n - 1)], -1)
+    rows = (0, m - 1) if rows is None else rows
+    full = [np.stack([np.full(n, r, dtype=np.int64), np.arange(n, dtype=np.int64)], -1) for r in rows]
+    return np.concatenate([ij, *full]).astype(np.int64)
+
+
+def sample_abs_products(a: np.ndarray, b: np.ndarray, idx: np.ndarray, atb: bool = False,
+                        chunk: int = 512) -> np.ndarray:
+    """sum_p |a_ip| |b_pj| (leading limbs) for each sampled (i, j): the entries
+    of |op(A)| |B| that normalise a sampled GEMM error."""
+    A = np.abs(a[..., 0])
+    A = A.T if atb else A
+    B = np.abs(b[..., 0])
+    out = np.empty(len(idx))
+    for c0 in range(0, len(idx), chunk):
+        i, j = idx[c0:c0 + chunk, 0], idx[c0:c0 + chunk, 1]
+        out[c0:c0 + chunk] = np.einsum("ek,ke->e", A[i], B[:, j])
+    return out
+
+
+def sampled_error(c: np.ndarray, c_star: np.ndarray, absab: np.ndarray, idx: np.ndarray) -> tuple[float, float]:
+    """Error of a computed GEMM over sampled entries against reference values
+    c_star (limbs, leading first): (||C - C*||_F / || |A| |B| ||_F,
+    ||C - C*||_F / ||C*||_F). The difference is taken limb by limb (each limb
+    difference is exact while the two values agree to that limb) and the
+    limb differences are summed from the leading one."""
+    got = c[idx[:, 0], idx[:, 1]]
+    nl = max(got.shape[-1], c_star.shape[-1])
+    d = np.zeros(len(idx))
+    for t in range(nl):
+        g = got[:, t] if t < got.shape[-1] else 0.0
+        r = c_star[:, t] if t < c_star.shape[-1] else 0.0
+        d = d + (g - r)
+    return float(np.linalg.norm(d) / np.linalg.norm(absab)), float(np.linalg.norm(d) / np.linalg.norm(c_star[:, 0]))
+
+
 def dd_to_qd(x: np.ndarray) -> np.ndarray:
     """Limb-extend f128 entries to f256 (MultiFloat<4>::from_f128, conv.rs:121-126)."""
     out = np.zeros(x.shape[:-1] + (4,))

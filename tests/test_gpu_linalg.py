@@ -158,3 +158,36 @@ def test_solve_spd_f128_hilbert12(gpu):  # solver/src/lib.rs:319-340
     err = np.sqrt(np.sum(((g["x"][:, 0] - 1.0) + g["x"][:, 1]) ** 2))
     assert err < 1e-15 and g["strategy"] == "Float128" and g["kappa"] == r["kappa"]
     assert abs(g["residual_norm"]) < 1e-30
+
+
+@pytest.mark.parametrize("length", [0, 1, 7, 1023, 1024, 1025, 5000])
+def test_dot_bitexact(gpu, length):
+    """linalg.rs:7-26: serial below 1024 entries, chunk sums folded above."""
+    a = dense_dd(1, max(length, 1), seed=300 + length)[0][:length]
+    b = dense_dd(1, max(length, 1), seed=400 + length)[0][:length]
+    got = gpu.f128_dot(a, b)
+    ref = O.dot(a, b) if length else np.zeros(2)
+    assert np.array_equal(got, ref)
+
+
+@pytest.mark.parametrize("rows,cols", [(1, 1), (3, 70), (70, 3), (129, 257), (1000, 17)])
+def test_gemv_bitexact(gpu, rows, cols):
+    """linalg.rs:29-38: every row summed in column order."""
+    a = dense_dd(rows, cols, seed=rows * 7 + cols)
+    x = dense_dd(1, cols, seed=cols + 11)[0]
+    assert np.array_equal(gpu.f128_gemv(a, rows, cols, x), O.gemv(a, rows, cols, x))
+
+
+def test_solve_cholesky_dev_matches_host_form(gpu):
+    import torch
+
+    n = 300
+    a = spd_dd(n, 21)
+    L = gpu.f128_cholesky(a, n)
+    b = dense_dd(1, n, seed=5)[0]
+    x_host = gpu.f128_solve_cholesky(L, b, n)
+    dL = torch.from_numpy(np.ascontiguousarray(L)).cuda()
+    dx = torch.from_numpy(np.ascontiguousarray(b)).cuda()
+    gpu.check(gpu.lib().hp_f128_solve_cholesky_dev(dL.data_ptr(), dx.data_ptr(), n, 0))
+    torch.cuda.synchronize()
+    assert np.array_equal(dx.cpu().numpy(), x_host)
