@@ -150,6 +150,30 @@ int hp_f256_gemm_atb_dev(const double* a, const double* b, double* c, size_t m, 
                          size_t k, int mode, void* stream);
 
 /* ------------------------------------------------------------------------
+ * f512 (MultiFloat<8>) GEMM, Cholesky and solve (plain CUDA-core kernels)
+ * replaces: pub fn mf_gemm<const N: usize>(a, b, c, m, n, k)      (N = 8)
+ *           pub fn mf_gemm_atb<const N: usize>(a, b, c, m, n, k)  (N = 8)
+ *           crates/quad/src/multifloat/linalg.rs:39-85
+ * AoS f512 (8 limbs per entry); each C entry summed s = s + a b in k order
+ * with the reference's MultiFloat<8> Add and Mul: bit-identical.
+ * _dev: device pointers (32-byte aligned), atb != 0 for A^T B.
+ * ---------------------------------------------------------------------- */
+int hp_f512_gemm(const double* a, const double* b, double* c, size_t m, size_t n, size_t k);
+int hp_f512_gemm_atb(const double* a, const double* b, double* c, size_t m, size_t n, size_t k);
+int hp_f512_gemm_dev(const double* a, const double* b, double* c, size_t m, size_t n, size_t k, int atb,
+                     void* stream);
+/* replaces: pub fn mf_cholesky<const N: usize>(a, n) -> Result<(), &str>  (N = 8)
+ *           crates/quad/src/multifloat/linalg.rs:88-139
+ * In place; the lower triangle becomes L, bit-identical; a first limb <= 0 on
+ * the diagonal returns HP_ERR_NOT_SPD with *pivot (may be NULL). */
+int hp_f512_cholesky(double* a, size_t n, int64_t* pivot);
+/* replaces: pub fn mf_cholesky_solve<const N: usize>(l, b, x, n)  (N = 8)
+ *           crates/quad/src/multifloat/linalg.rs:141-172
+ * L L^T x = b; forward sweep bit-identical, backward sweep with each row's
+ * subtractions in descending order (f512-level accuracy). */
+int hp_f512_cholesky_solve(const double* l, const double* b, double* x, size_t n);
+
+/* ------------------------------------------------------------------------
  * f128 Cholesky and triangular solves
  * ---------------------------------------------------------------------- */
 /* replaces: pub fn cholesky(a: &mut [f128], n: usize) -> Result<(), CholeskyError>
@@ -283,6 +307,19 @@ int hp_spd_solve_refined_dev(const double* S, const double* b, size_t n, int mod
 int hp_assemble_overlap_s(size_t n_shells, const double* centers, const int64_t* prim_off,
                           const double* alpha, const double* coeff, const double* params,
                           double* matrix, int64_t* tier_counts);
+/* replaces: pub fn assemble_overlap_mixed(basis: &BasisSet, params: &ScreenParams)
+ *           -> OverlapResult      crates/overlap/src/assemble.rs:35-85
+ * for shells of any kind: shell_l[s] = 0, 1, 2, 3 for ShellKind S, P, D, F
+ * (basis.rs:9-28). Shell s contributes (l+1)(l+2)/2 Cartesian AOs in the
+ * reference's order (integral.rs:223-233: lx descending, then ly
+ * descending); s-s pairs as in hp_assemble_overlap_s, other pairs by the
+ * contracted Obara-Saika recurrence (integral.rs:144-352) in f64 or f128 by
+ * the same screening tiers. matrix: n_ao x n_ao f64 (OverlapResult.matrix);
+ * *n_ao_out (may be NULL) = the AO count. Values agree with the reference to
+ * the last ulps of f64 (CUDA's exp is not the host libm's). */
+int hp_assemble_overlap(size_t n_shells, const int32_t* shell_l, const double* centers, const int64_t* prim_off,
+                        const double* alpha, const double* coeff, const double* params, double* matrix,
+                        int64_t* tier_counts, size_t* n_ao_out);
 /* f128 overlap matrix of normalised s Gaussians (one primitive per basis
  * function): S_ij = (4 a b/(a+b)^2)^{3/4} exp(-a b/(a+b) |R_i - R_j|^2),
  * evaluated with the reference's f128 operations (dd.rs:61-121) so it is
@@ -387,6 +424,26 @@ int hp_canonical_orthogonalize(const double* s, size_t n, double threshold, doub
  * HP_ERR_NO_CONVERGE if a Jacobi sweep limit is reached. */
 int hp_solve_gen_eigen(const double* f, const double* s, size_t n, double threshold,
                        double* eigenvalues, double* eigenvectors, size_t* n_basis);
+
+/* ------------------------------------------------------------------------
+ * Text exchange in the reference's serde formats (host only, no device)
+ * replaces: impl Serialize / Deserialize for f128   crates/quad/src/dd.rs:441-514
+ *           impl Serialize / Deserialize for MultiFloat<N>
+ *           crates/quad/src/multifloat/traits.rs:7-155
+ * Human-readable forms: f128 as format!("{:+.18e}+{:+.18e}", hi, lo), a
+ * MultiFloat<N> as its limbs in "{:+.14e}" joined by '+' (Rust's exponent
+ * style: "e-5", "e0"; NaN as "NaN"). The parsers split at the reference's
+ * separator (a '+' followed by a sign and not preceded by 'e'/'E') and read
+ * each part as Rust's f64::from_str does; anything Rust rejects returns
+ * HP_ERR_INVALID_ARG. The compact forms ({hi, lo}, {limbs: [..]}) are the
+ * in-memory limb layout. *_to_string write a NUL-terminated string of at
+ * most cap bytes (HP_ERR_INVALID_ARG if it does not fit: 54 bytes hold any
+ * f128, 24 N bytes any MultiFloat<N>).
+ * ---------------------------------------------------------------------- */
+int hp_f128_to_string(const double* v, char* out, size_t cap);
+int hp_f128_from_string(const char* s, double* out);
+int hp_mf_to_string(int n_limbs, const double* v, char* out, size_t cap);
+int hp_mf_from_string(int n_limbs, const char* s, double* out);
 
 #ifdef __cplusplus
 }

@@ -86,6 +86,8 @@ def lib():
             "or_overlap_primitive_f64": ([ctypes.c_double, _d, ctypes.c_double, _d], ctypes.c_double),
             "or_overlap_primitive_f128": ([ctypes.c_double, _d, ctypes.c_double, _d, _d], None),
             "or_assemble_overlap_s": ([_sz, _d, _i64, _d, _d, _d, _d, _i64], None),
+            "or_assemble_overlap": ([_sz, ctypes.POINTER(ctypes.c_int32), _d, _i64, _d, _d, _d, _d, _i64],
+                                    ctypes.c_int),
             "or_overlap_norm_dd": ([_sz, _d, _d, _d], None),
             "or_adjoint_f128": ([_sz, _d, _d, _d, ctypes.POINTER(ctypes.c_int32), _sz, _d, _d, _d], ctypes.c_int),
             "or_loss_f256": ([_sz, _d, _d, _d, _d], ctypes.c_int),
@@ -405,6 +407,25 @@ def assemble_overlap_s(centers, prim_alpha, prim_coeff, params=DEFAULT_SCREEN):
     lib().or_assemble_overlap_s(n, _p(_f(centers)), off.ctypes.data_as(_i64), _p(al), _p(co),
                                 _p(_f(params)), _p(mat), tc.ctypes.data_as(_i64))
     return mat, {"f64_pairs": int(tc[0]), "f128_pairs": int(tc[1]), "skipped_pairs": int(tc[2])}
+
+
+def assemble_overlap(shell_l, centers, prim_alpha, prim_coeff, params=DEFAULT_SCREEN):
+    """assemble.rs:35-85 for shells of kinds S/P/D/F (shell_l = 0..3) with the
+    Obara-Saika blocks of integral.rs:144-352: (matrix (n_ao, n_ao), tier_counts)."""
+    shell_l = np.ascontiguousarray(shell_l, dtype=np.int32)
+    n = len(shell_l)
+    off = np.zeros(n + 1, dtype=np.int64)
+    off[1:] = np.cumsum([len(a) for a in prim_alpha])
+    al = _f(np.concatenate(prim_alpha))
+    co = _f(np.concatenate(prim_coeff))
+    n_ao = int(sum((l + 1) * (l + 2) // 2 for l in shell_l))
+    mat = np.zeros((n_ao, n_ao))
+    tiers = np.zeros(3, dtype=np.int64)
+    rc = lib().or_assemble_overlap(n, shell_l.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)), _p(_f(centers)),
+                                   off.ctypes.data_as(_i64), _p(al), _p(co), _p(_f(params)), _p(mat),
+                                   tiers.ctypes.data_as(_i64))
+    assert rc == 0
+    return mat, tiers
 
 
 def overlap_norm_dd(centers, alpha) -> np.ndarray:

@@ -1012,6 +1012,201 @@ void or_assemble_overlap_s(size_t n_shells, const double* centers, const int64_t
       if (i != j) matrix[j * n + i] = vals[pidx];
     }
 }
+// ---- Obara-Saika overlaps of Cartesian shells (integral.rs:144-352) ----
+namespace {
+// integral.rs:156-186: S[i][j], i <= la, j <= lb, row stride lb + 1.
+void os1d_f64(int la, int lb, double pa, double pb, double gamma, double* s) {
+  const int nb = lb + 1;
+  const double oo2g = 0.5 / gamma;
+  for (int q = 0; q < (la + 1) * nb; q++) s[q] = 0.0;
+  s[0] = 1.0;
+  for (int i = 0; i < la; i++) s[(i + 1) * nb] = pa * s[i * nb] + oo2g * (double)i * (i > 0 ? s[(i - 1) * nb] : 0.0);
+  for (int j = 0; j < lb; j++)
+    for (int i = 0; i <= la; i++) {
+      const double term_im1 = oo2g * (double)i * (i > 0 ? s[(i - 1) * nb + j] : 0.0);
+      const double term_jm1 = oo2g * (double)j * (j > 0 ? s[i * nb + j - 1] : 0.0);
+      s[i * nb + j + 1] = pb * s[i * nb + j] + term_im1 + term_jm1;
+    }
+}
+// integral.rs:188-219
+void os1d_f128(int la, int lb, dd pa, dd pb, dd gamma, dd* s) {
+  const int nb = lb + 1;
+  const dd oo2g = dd_div(dd_from(0.5), gamma);
+  for (int q = 0; q < (la + 1) * nb; q++) s[q] = dd{0, 0};
+  s[0] = dd_from(1.0);
+  for (int i = 0; i < la; i++) {
+    const dd fi = dd_from((double)i);
+    const dd prev = i > 0 ? s[(i - 1) * nb] : dd{0, 0};
+    s[(i + 1) * nb] = dd_add(dd_mul(pa, s[i * nb]), dd_mul(dd_mul(oo2g, fi), prev));
+  }
+  for (int j = 0; j < lb; j++) {
+    const dd fj = dd_from((double)j);
+    for (int i = 0; i <= la; i++) {
+      const dd fi = dd_from((double)i);
+      const dd im1 = i > 0 ? s[(i - 1) * nb + j] : dd{0, 0};
+      const dd jm1 = j > 0 ? s[i * nb + j - 1] : dd{0, 0};
+      s[i * nb + j + 1] =
+          dd_add(dd_add(dd_mul(pb, s[i * nb + j]), dd_mul(dd_mul(oo2g, fi), im1)), dd_mul(dd_mul(oo2g, fj), jm1));
+    }
+  }
+}
+// integral.rs:223-233: (lx, ly, lz) with lx descending, then ly descending.
+int cart_components(int l, int (*c)[3]) {
+  int k = 0;
+  for (int lx = l; lx >= 0; lx--)
+    for (int ly = l - lx; ly >= 0; ly--) c[k][0] = lx, c[k][1] = ly, c[k][2] = l - lx - ly, k++;
+  return k;
+}
+struct ShellRef {
+  int l;
+  const double* center;
+  const double* alpha;
+  const double* coeff;
+  int np;
+};
+// integral.rs:235-284, block += over primitive pairs (ni x nj, row-major).
+void os_contracted_f64(const ShellRef& A, const ShellRef& B, double* block) {
+  int ca[10][3], cb[10][3];
+  const int ni = cart_components(A.l, ca), nj = cart_components(B.l, cb), nb = B.l + 1;
+  double sx[16], sy[16], sz[16];
+  for (int q = 0; q < ni * nj; q++) block[q] = 0.0;
+  for (int p = 0; p < A.np; p++)
+    for (int r = 0; r < B.np; r++) {
+      const double ai = A.alpha[p], aj = B.alpha[r];
+      const double gamma = ai + aj;
+      const double mu = ai * aj / gamma;
+      const double r2 = dist2_f64(A.center, B.center);
+      const double t = std::sqrt(M_PI / gamma);
+      const double prefactor = t * t * t * std::exp(-mu * r2);
+      double pa[3], pb[3];
+      for (int c = 0; c < 3; c++) {
+        const double pc = (ai * A.center[c] + aj * B.center[c]) / gamma;
+        pa[c] = pc - A.center[c];
+        pb[c] = pc - B.center[c];
+      }
+      os1d_f64(A.l, B.l, pa[0], pb[0], gamma, sx);
+      os1d_f64(A.l, B.l, pa[1], pb[1], gamma, sy);
+      os1d_f64(A.l, B.l, pa[2], pb[2], gamma, sz);
+      for (int x = 0; x < ni; x++)
+        for (int y = 0; y < nj; y++) {
+          const double val = sx[ca[x][0] * nb + cb[y][0]] * sy[ca[x][1] * nb + cb[y][1]] *
+                             sz[ca[x][2] * nb + cb[y][2]] * prefactor * A.coeff[p] * B.coeff[r];
+          block[x * nj + y] += val;
+        }
+    }
+}
+// integral.rs:286-352
+void os_contracted_f128(const ShellRef& A, const ShellRef& B, double* block) {
+  int ca[10][3], cb[10][3];
+  const int ni = cart_components(A.l, ca), nj = cart_components(B.l, cb), nb = B.l + 1;
+  dd sx[16], sy[16], sz[16], b128[100];
+  for (int q = 0; q < ni * nj; q++) b128[q] = dd{0, 0};
+  for (int p = 0; p < A.np; p++)
+    for (int r = 0; r < B.np; r++) {
+      const dd ai = dd_from(A.alpha[p]), aj = dd_from(B.alpha[r]);
+      const dd gamma = dd_add(ai, aj);
+      const dd mu = dd_div(dd_mul(ai, aj), gamma);
+      const dd dx = dd_from(A.center[0] - B.center[0]);
+      const dd dy = dd_from(A.center[1] - B.center[1]);
+      const dd dz = dd_from(A.center[2] - B.center[2]);
+      const dd r2 = dd_add(dd_add(dd_mul(dx, dx), dd_mul(dy, dy)), dd_mul(dz, dz));
+      const dd ratio = dd_div(dd_from(M_PI), gamma);
+      const dd prefactor = dd_mul(ratio, dd_sqrt(ratio));
+      const dd neg_mu_r2 = dd_mul(dd_sub(dd{0, 0}, mu), r2);
+      const dd exp_hi = dd_from(std::exp(neg_mu_r2.hi));
+      const dd exp_val = dd_mul(exp_hi, dd_add(dd_from(1.0), dd_from(neg_mu_r2.lo)));
+      const dd total_pre = dd_mul(prefactor, exp_val);
+      dd pa[3], pb[3];
+      for (int c = 0; c < 3; c++) {
+        const dd cic = dd_from(A.center[c]), cjc = dd_from(B.center[c]);
+        const dd pc = dd_div(dd_add(dd_mul(ai, cic), dd_mul(aj, cjc)), gamma);
+        pa[c] = dd_sub(pc, cic);
+        pb[c] = dd_sub(pc, cjc);
+      }
+      os1d_f128(A.l, B.l, pa[0], pb[0], gamma, sx);
+      os1d_f128(A.l, B.l, pa[1], pb[1], gamma, sy);
+      os1d_f128(A.l, B.l, pa[2], pb[2], gamma, sz);
+      const dd coeff = dd_mul(dd_mul(dd_from(A.coeff[p]), dd_from(B.coeff[r])), total_pre);
+      for (int x = 0; x < ni; x++)
+        for (int y = 0; y < nj; y++) {
+          const dd val = dd_mul(dd_mul(dd_mul(sx[ca[x][0] * nb + cb[y][0]], sy[ca[x][1] * nb + cb[y][1]]),
+                                       sz[ca[x][2] * nb + cb[y][2]]),
+                                coeff);
+          b128[x * nj + y] = dd_add(b128[x * nj + y], val);
+        }
+    }
+  for (int q = 0; q < ni * nj; q++) block[q] = dd_to_f64(b128[q]);
+}
+// integral.rs:66-138 overlap_shell_pair for tiers 0 (F64) and 1 (F128).
+void overlap_shell_pair(const ShellRef& A, const ShellRef& B, int tier, double* block) {
+  if (A.l == 0 && B.l == 0) {
+    if (tier == 0) {
+      double sum = 0.0;
+      for (int p = 0; p < A.np; p++)
+        for (int r = 0; r < B.np; r++)
+          sum += A.coeff[p] * B.coeff[r] * overlap_primitive_f64(A.alpha[p], A.center, B.alpha[r], B.center);
+      block[0] = sum;
+    } else {
+      dd sum{0, 0};
+      for (int p = 0; p < A.np; p++)
+        for (int r = 0; r < B.np; r++) {
+          const dd sp = overlap_primitive_f128(A.alpha[p], A.center, B.alpha[r], B.center);
+          sum = dd_add(sum, dd_mul(dd_mul(dd_from(A.coeff[p]), dd_from(B.coeff[r])), sp));
+        }
+      block[0] = dd_to_f64(sum);
+    }
+  } else if (tier == 0) {
+    os_contracted_f64(A, B, block);
+  } else {
+    os_contracted_f128(A, B, block);
+  }
+}
+}  // namespace
+
+// assemble_overlap_mixed (assemble.rs:35-85) for shells of any kind
+// S, P, D, F (shell_l[s] = 0..3; basis.rs:9-28, n_cart = (l+1)(l+2)/2 AOs in
+// cart_components order). matrix: n_ao x n_ao f64.
+int or_assemble_overlap(size_t n_shells, const int32_t* shell_l, const double* centers, const int64_t* prim_off,
+                        const double* alpha, const double* coeff, const double* params, double* matrix,
+                        int64_t* tier_counts) {
+  std::vector<size_t> off(n_shells + 1, 0);
+  for (size_t s = 0; s < n_shells; s++) {
+    if (shell_l[s] < 0 || shell_l[s] > 3) return -1;
+    off[s + 1] = off[s] + (size_t)((shell_l[s] + 1) * (shell_l[s] + 2) / 2);
+  }
+  const size_t n_ao = off[n_shells];
+  std::fill(matrix, matrix + n_ao * n_ao, 0.0);
+  const size_t npairs = n_shells * (n_shells + 1) / 2;
+  std::vector<int> tiers(npairs);
+  std::vector<double> blocks(npairs * 100);
+#pragma omp parallel for schedule(dynamic, 16)
+  for (size_t i = 0; i < n_shells; i++)
+    for (size_t j = 0; j <= i; j++) {
+      const size_t pidx = i * (i + 1) / 2 + j;
+      const ShellRef A{shell_l[i], centers + 3 * i, alpha + prim_off[i], coeff + prim_off[i],
+                       (int)(prim_off[i + 1] - prim_off[i])};
+      const ShellRef B{shell_l[j], centers + 3 * j, alpha + prim_off[j], coeff + prim_off[j],
+                       (int)(prim_off[j + 1] - prim_off[j])};
+      const int tier = screen_pair(A.center, A.alpha, A.np, B.center, B.alpha, B.np, params);
+      tiers[pidx] = tier;
+      if (tier != 2) overlap_shell_pair(A, B, tier, &blocks[pidx * 100]);
+    }
+  tier_counts[0] = tier_counts[1] = tier_counts[2] = 0;
+  for (size_t i = 0; i < n_shells; i++)
+    for (size_t j = 0; j <= i; j++) {
+      const size_t pidx = i * (i + 1) / 2 + j;
+      tier_counts[tiers[pidx]]++;
+      if (tiers[pidx] == 2) continue;
+      const size_t ni = off[i + 1] - off[i], nj = off[j + 1] - off[j];
+      for (size_t a = 0; a < ni; a++)
+        for (size_t b = 0; b < nj; b++) {
+          const double v = blocks[pidx * 100 + a * nj + b];
+          matrix[(off[i] + a) * n_ao + off[j] + b] = v;
+          if (i != j) matrix[(off[j] + b) * n_ao + off[i] + a] = v;
+        }
+    }
+  return 0;
+}
 // The dd problem matrix for the overlap SPD workloads (normalised s
 // Gaussians, one primitive per basis function). Full symmetric n x n.
 void or_overlap_norm_dd(size_t n, const double* centers, const double* alpha, double* s_out) {

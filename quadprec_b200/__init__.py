@@ -50,6 +50,10 @@ SIGNATURES = {
     "hp_device_ok": ([], ctypes.c_int),
     "hp_device_status": ([_vp, ctypes.POINTER(ctypes.c_uint32), ctypes.c_int], ctypes.c_int),
     "hp_measure_peaks": ([ctypes.c_int, _d, _d, _d, _d], ctypes.c_int),
+    "hp_f128_to_string": ([_vp, ctypes.c_char_p, _sz], ctypes.c_int),
+    "hp_f128_from_string": ([ctypes.c_char_p, _vp], ctypes.c_int),
+    "hp_mf_to_string": ([ctypes.c_int, _vp, ctypes.c_char_p, _sz], ctypes.c_int),
+    "hp_mf_from_string": ([ctypes.c_int, ctypes.c_char_p, _vp], ctypes.c_int),
     "hp_debug_trsv_wavefront": ([_vp, _vp, _vp, _sz, ctypes.c_int, ctypes.c_uint64, ctypes.c_int], ctypes.c_int),
     "hp_profile_enable": ([ctypes.c_int], None),
     "hp_profile_read": ([_d, ctypes.c_int, ctypes.c_char_p, _sz], ctypes.c_int),
@@ -62,6 +66,11 @@ SIGNATURES = {
     "hp_f256_gemm_atb": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int], ctypes.c_int),
     "hp_f256_gemm_dev": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int, _vp], ctypes.c_int),
     "hp_f256_gemm_atb_dev": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int, _vp], ctypes.c_int),
+    "hp_f512_gemm": ([_vp, _vp, _vp, _sz, _sz, _sz], ctypes.c_int),
+    "hp_f512_gemm_atb": ([_vp, _vp, _vp, _sz, _sz, _sz], ctypes.c_int),
+    "hp_f512_gemm_dev": ([_vp, _vp, _vp, _sz, _sz, _sz, ctypes.c_int, _vp], ctypes.c_int),
+    "hp_f512_cholesky": ([_vp, _sz, _i64p], ctypes.c_int),
+    "hp_f512_cholesky_solve": ([_vp, _vp, _vp, _sz], ctypes.c_int),
     "hp_f128_cholesky": ([_vp, _sz, _i64p, _d], ctypes.c_int),
     "hp_f128_cholesky_blocked": ([_vp, _sz, _sz, _i64p, _d], ctypes.c_int),
     "hp_f128_cholesky_dev": ([_vp, _sz, _i64p, _d, _vp], ctypes.c_int),
@@ -97,6 +106,7 @@ SIGNATURES = {
     "hp_overlap_adjoint": ([_sz, _vp, _vp, _vp, _vp, _sz, ctypes.c_int, _vp, _vp, _vp, _vp], ctypes.c_int),
     "hp_overlap_adjoint_dev": ([_sz, _vp, _vp, _vp, _vp, _sz, ctypes.c_int, _vp, _vp, _vp, _vp, _vp], ctypes.c_int),
     "hp_assemble_overlap_s": ([_sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp], ctypes.c_int),
+    "hp_assemble_overlap": ([_sz, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, ctypes.POINTER(_sz)], ctypes.c_int),
     "hp_overlap_norm_dd": ([_sz, _vp, _vp, _vp], ctypes.c_int),
     "hp_overlap_norm_dd_dev": ([_sz, _vp, _vp, _vp, _vp], ctypes.c_int),
 }
@@ -236,6 +246,34 @@ def f256_cholesky(a, n):
     return a
 
 
+def f512_gemm(a, b, m, n, k, atb=False) -> np.ndarray:
+    """multifloat/linalg.rs:39 mf_gemm::<8> / :64 mf_gemm_atb::<8> (bit-identical)."""
+    a, b = _c(a), _c(b)
+    c = np.empty((m, n, 8))
+    fn = lib().hp_f512_gemm_atb if atb else lib().hp_f512_gemm
+    check(fn(_ptr(a), _ptr(b), _ptr(c), m, n, k))
+    return c
+
+
+def f512_cholesky(a, n):
+    """multifloat/linalg.rs:89 mf_cholesky::<8>; returns a copy with L in the lower triangle."""
+    a = _c(a).copy()
+    pv = ctypes.c_int64(-1)
+    rc = lib().hp_f512_cholesky(_ptr(a), n, ctypes.byref(pv))
+    if rc == HP_ERR_NOT_SPD:
+        raise CholeskyError(pv.value, float("nan"))
+    check(rc)
+    return a
+
+
+def f512_cholesky_solve(l, b, n):
+    """multifloat/linalg.rs:145 mf_cholesky_solve::<8>: x (n, 8)."""
+    l, b = _c(l), _c(b)
+    x = np.empty((n, 8))
+    check(lib().hp_f512_cholesky_solve(_ptr(l), _ptr(b), _ptr(x), n))
+    return x
+
+
 def f256_cholesky_solve(l, b, n):
     """multifloat/linalg.rs:141 mf_cholesky_solve::<4>; l (n, n, 4), b (n, 4)."""
     l, b = _c(l), _c(b)
@@ -300,6 +338,37 @@ def measure_peaks(reps=5) -> dict:
     v = [ctypes.c_double(0.0) for _ in range(4)]
     check(lib().hp_measure_peaks(reps, *[ctypes.byref(x) for x in v]))
     return {"fp64_tflops": v[0].value, "i8_tops": v[1].value, "fp64_ms": v[2].value, "i8_ms": v[3].value}
+
+
+def f128_to_string(v) -> str:
+    """dd.rs:448-461 human-readable serde form of one f128 (hi, lo)."""
+    v = _c(v)
+    buf = ctypes.create_string_buffer(64)
+    check(lib().hp_f128_to_string(_ptr(v), buf, 64))
+    return buf.value.decode()
+
+
+def f128_from_string(s: str) -> np.ndarray:
+    """dd.rs:495-509 parse_dd_string."""
+    out = np.zeros(2)
+    check(lib().hp_f128_from_string(s.encode(), _ptr(out)))
+    return out
+
+
+def mf_to_string(v) -> str:
+    """multifloat/traits.rs:15-34 human-readable serde form of one MultiFloat<N>."""
+    v = _c(v)
+    cap = 24 * len(v) + 8
+    buf = ctypes.create_string_buffer(cap)
+    check(lib().hp_mf_to_string(len(v), _ptr(v), buf, cap))
+    return buf.value.decode()
+
+
+def mf_from_string(s: str, n_limbs: int) -> np.ndarray:
+    """multifloat/traits.rs:104-150 parse_limbs_string."""
+    out = np.zeros(n_limbs)
+    check(lib().hp_mf_from_string(n_limbs, s.encode(), _ptr(out)))
+    return out
 
 
 def device_status(stream=0, clear=True) -> tuple[int, int]:
@@ -381,6 +450,25 @@ def assemble_overlap_s(centers, prim_alpha, prim_coeff, params=DEFAULT_SCREEN):
     check(lib().hp_assemble_overlap_s(n, _ptr(_c(centers)), off.ctypes.data, _ptr(al), _ptr(co), _ptr(pr),
                                       _ptr(mat), tc.ctypes.data))
     return mat, {"f64_pairs": int(tc[0]), "f128_pairs": int(tc[1]), "skipped_pairs": int(tc[2])}
+
+
+def assemble_overlap(shell_l, centers, prim_alpha, prim_coeff, params=DEFAULT_SCREEN):
+    """assemble.rs:35 for shells of kinds S/P/D/F: (matrix (n_ao, n_ao), tier_counts)."""
+    shell_l = np.ascontiguousarray(shell_l, dtype=np.int32)
+    centers = _c(centers)
+    n = len(shell_l)
+    off = np.zeros(n + 1, dtype=np.int64)
+    off[1:] = np.cumsum([len(a) for a in prim_alpha])
+    al = _c(np.concatenate(prim_alpha))
+    co = _c(np.concatenate(prim_coeff))
+    n_ao = int(sum((l + 1) * (l + 2) // 2 for l in shell_l))
+    mat = np.zeros((n_ao, n_ao))
+    tiers = np.zeros(3, dtype=np.int64)
+    got = ctypes.c_size_t(0)
+    check(lib().hp_assemble_overlap(n, shell_l.ctypes.data, _ptr(centers), off.ctypes.data, _ptr(al), _ptr(co),
+                                    _ptr(_c(params)), _ptr(mat), tiers.ctypes.data, ctypes.byref(got)))
+    assert got.value == n_ao
+    return mat, tiers
 
 
 def overlap_norm_dd(centers, alpha) -> np.ndarray:

@@ -19,6 +19,7 @@
 // Three kernels per block column: diag (one CTA), panel (one thread per row),
 // syrk (64 x 64 lower-triangular tiles of the trailing matrix, CUDA cores).
 #include <algorithm>
+#include <type_traits>
 
 #include "hp_arith.cuh"
 #include "hp_runtime.cuh"
@@ -161,6 +162,121 @@ __global__ void __launch_bounds__(64) chol_panel_kernel(typename O::T* A, const 
   for (int j = 0; j < jb; j++) arow[j] = Lr[j * 64 + t];
 }
 
+// Right-looking forms of the two kernels above for the unblocked f128
+// factorisation (the reference's `cholesky`). Every sum s_ij still receives
+// the products L_ik L_jk one at a time in k order, starting from the value
+// the trailing updates of earlier blocks left in S, so the factor is the
+// same bit for bit; what changes is only when each product is added: as
+// soon as column k is final, all sums of the block take their k-th product
+// at once (independent operations), instead of each sum walking its k loop
+// after the column it waits for.
+//
+// Diagonal block: one CTA; per column j, one thread forms the pivot
+// (sqrt, recip), the rows below scale their entry of column j, and the
+// sums of the remaining lower triangle take their j-th product.
+constexpr int RL_THREADS = 256;
+template <class O>
+__global__ void __launch_bounds__(RL_THREADS) chol_diag_rl_kernel(typename O::T* A, const typename O::T* S, int64_t n,
+                                                                  int64_t kb, int jb, typename O::T* invd,
+                                                                  CholErr* err) {
+  using T = typename O::T;
+  extern __shared__ __align__(16) unsigned char sm_raw[];
+  T* Ls = reinterpret_cast<T*>(sm_raw);  // [64][65]: the block, then L
+  T* Ss = Ls + 64 * 65;                  // [64][65]: running sums
+  __shared__ T inv_s[CH_MAXNB];
+  __shared__ int fail;
+  const int t = threadIdx.x;
+  if (err->flag) return;
+  if (t == 0) fail = 0;
+  for (int e = t; e < jb * jb; e += RL_THREADS) {
+    const int r = e / jb, c = e % jb;
+    if (c <= r) {
+      Ls[r * 65 + c] = A[(kb + r) * n + kb + c];
+      Ss[r * 65 + c] = S[(kb + r) * n + kb + c];
+    }
+  }
+  __syncthreads();
+  for (int j = 0; j < jb; j++) {
+    if (t == 0) {
+      const T d = O::sub(Ls[j * 65 + j], Ss[j * 65 + j]);
+      if (!(O::hi(d) > 0.0) && !(O::hi(d) != O::hi(d))) {  // diag <= 0 (NaN passes, as in Rust)
+        fail = 1;
+        err->flag = 1;
+        err->pivot = kb + j;
+        err->value = O::to_f64(d);
+      } else {
+        const T l = O::sqrt_(d);
+        Ls[j * 65 + j] = l;
+        inv_s[j] = O::inv(l);
+      }
+    }
+    __syncthreads();
+    if (fail) return;
+    for (int r = j + 1 + t; r < jb; r += RL_THREADS)
+      Ls[r * 65 + j] = O::mul(O::sub(Ls[r * 65 + j], Ss[r * 65 + j]), inv_s[j]);
+    __syncthreads();
+    // sums (r, c), j < c <= r < jb, take the product L_rj L_cj
+    const int m = jb - j - 1;
+    for (int e = t; e < m * (m + 1) / 2; e += RL_THREADS) {
+      int r = (int)((sqrtf(8.0f * e + 1.0f) - 1.0f) * 0.5f);
+      while (r * (r + 1) / 2 > e) r--;
+      while ((r + 1) * (r + 2) / 2 <= e) r++;
+      const int c = e - r * (r + 1) / 2;
+      const int rr = j + 1 + r, cc = j + 1 + c;
+      Ss[rr * 65 + cc] = O::add(Ss[rr * 65 + cc],
+                                rr == cc ? O::mul(Ls[rr * 65 + j], Ls[rr * 65 + j]) : O::mul(Ls[rr * 65 + j], Ls[cc * 65 + j]));
+    }
+    __syncthreads();
+  }
+  for (int e = t; e < jb * jb; e += RL_THREADS) {
+    const int r = e / jb, c = e % jb;
+    if (c <= r) A[(kb + r) * n + kb + c] = Ls[r * 65 + c];
+  }
+  if (t < jb) invd[kb + t] = inv_s[t];
+}
+
+// Panel rows i >= kb + 32 below a full 32-column diagonal block: one warp
+// per row, lane q keeping the row's running sum s_iq. At step j lane j
+// forms L_ij = (A_ij - s_ij) recip(L_jj) and broadcasts it; every lane
+// q > j adds L_ij L_qj to its sum (the reference's product for k = j, in k
+// order). A step costs one scaling and one multiply-add of latency, and
+// the rows' warps fill the GPU.
+constexpr int PW_ROWS = 4;  // rows (warps) per CTA
+template <class O>
+__global__ void __launch_bounds__(PW_ROWS * 32) chol_panel_warp_kernel(typename O::T* A, const typename O::T* S,
+                                                                       int64_t n, int64_t kb,
+                                                                       const typename O::T* invd,
+                                                                       const CholErr* err) {
+  using T = typename O::T;
+  __shared__ T Ld[32][33];  // [q][j]: L_qj of the diagonal block
+  __shared__ T inv_s[32];
+  if (err->flag) return;
+  const int t = threadIdx.x, lane = t % 32;
+  for (int e = t; e < 32 * 32; e += PW_ROWS * 32) {
+    const int q = e / 32, j = e % 32;
+    Ld[q][j] = (j < q) ? A[(kb + q) * n + kb + j] : O::zero();
+  }
+  if (t < 32) inv_s[t] = invd[kb + t];
+  __syncthreads();
+  const int64_t i = kb + 32 + (int64_t)blockIdx.x * PW_ROWS + t / 32;
+  if (i >= n) return;
+  T* arow = A + i * n + kb;
+  const T a = arow[lane];
+  T sum = S[i * n + kb + lane], out = O::zero();
+#pragma unroll 4
+  for (int j = 0; j < 32; j++) {
+    T v = O::zero();
+    if (lane == j) {
+      v = O::mul(O::sub(a, sum), inv_s[j]);
+      out = v;
+    }
+    v.hi = __shfl_sync(0xffffffffu, v.hi, j);
+    v.lo = __shfl_sync(0xffffffffu, v.lo, j);
+    if (lane > j) sum = O::add(sum, O::mul(v, Ld[lane][j]));
+  }
+  arow[lane] = out;
+}
+
 // Trailing update on the lower triangle of rows/cols >= t0 = kb + jb:
 //   unblocked semantics: S_ij = S_ij + sum_{k in block} L_ik L_jk  (k order)
 //   BLOCKED:             A_ij = A_ij - (sum_{k in block} L_ik L_jk)
@@ -250,7 +366,7 @@ int cholesky_run(typename O::T* A, size_t n, size_t nb, CholErr* derr, cudaStrea
   constexpr int TL = 16 * TT;
   const size_t diag_smem = 64 * 65 * sizeof(T);
   const size_t panel_max = (size_t)(nb * nb + nb * 64) * sizeof(T);
-  static bool attr[64] = {};
+  static bool attr[64] = {}, attr_rl[64] = {};
   int dev = 0;
   HP_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 64 && !attr[dev]) {
@@ -264,18 +380,48 @@ int cholesky_run(typename O::T* A, size_t n, size_t nb, CholErr* derr, cudaStrea
     set_error("cholesky: block size %zu too large for this element type", nb);
     return HP_ERR_UNSUPPORTED;
   }
+  // the right-looking kernels serve the unblocked f128 factorisation at
+  // nb = RL_NB (its result does not depend on nb)
+  constexpr bool RL = !BLOCKED && std::is_same<T, dd>::value;
+  constexpr int RL_NB = 32;
+  if constexpr (RL) nb = RL_NB;
+  const size_t rl_smem = 2 * 64 * 65 * sizeof(T);
+  if constexpr (RL) {
+    if (dev < 64 && !attr_rl[dev]) {
+      HP_CUDA_TRY(cudaFuncSetAttribute(chol_diag_rl_kernel<O>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)rl_smem));
+      attr_rl[dev] = true;
+    }
+  }
   for (size_t kb = 0; kb < n; kb += nb) {
     const int jb = (int)std::min(nb, n - kb);
-    chol_diag_kernel<O, BLOCKED><<<1, CH_MAXNB, diag_smem, s>>>(A, S, n, kb, jb, invd.as<T>(), derr);
+    if constexpr (RL)
+      chol_diag_rl_kernel<O><<<1, RL_THREADS, rl_smem, s>>>(A, S, n, kb, jb, invd.as<T>(), derr);
+    else
+      chol_diag_kernel<O, BLOCKED><<<1, CH_MAXNB, diag_smem, s>>>(A, S, n, kb, jb, invd.as<T>(), derr);
     HP_LAUNCH_CHECK();
     const size_t rest = n - kb - jb;
     if (rest == 0) break;
-    const size_t panel_smem = (size_t)(jb * jb + jb * 64) * sizeof(T);
-    chol_panel_kernel<O, BLOCKED><<<(unsigned)((rest + 63) / 64), 64, panel_smem, s>>>(A, S, n, kb, jb,
-                                                                                      invd.as<T>(), derr);
+    if constexpr (RL) {
+      static_assert(RL_NB == 32, "one lane per column of the panel");
+      chol_panel_warp_kernel<O><<<(unsigned)((rest + PW_ROWS - 1) / PW_ROWS), PW_ROWS * 32, 0, s>>>(A, S, n, kb,
+                                                                                                  invd.as<T>(), derr);
+    } else {
+      const size_t panel_smem = (size_t)(jb * jb + jb * 64) * sizeof(T);
+      chol_panel_kernel<O, BLOCKED><<<(unsigned)((rest + 63) / 64), 64, panel_smem, s>>>(A, S, n, kb, jb,
+                                                                                        invd.as<T>(), derr);
+    }
     HP_LAUNCH_CHECK();
     const size_t tiles = (rest + TL - 1) / TL;
-    chol_syrk_kernel<O, BLOCKED, TT><<<(unsigned)(tiles * (tiles + 1) / 2), 256, 0, s>>>(A, S, n, kb, jb, derr);
+    // small trailing matrices: half-size tiles, so that more SMs take part
+    // (same per-entry operations and order, hence the same bits)
+    constexpr int TTS = TT > 2 ? TT / 2 : TT;
+    const size_t tiles_s = (rest + 16 * TTS - 1) / (16 * TTS);
+    if (TTS != TT && tiles * (tiles + 1) / 2 < 2 * 148)
+      chol_syrk_kernel<O, BLOCKED, TTS><<<(unsigned)(tiles_s * (tiles_s + 1) / 2), 256, 0, s>>>(A, S, n, kb, jb,
+                                                                                                 derr);
+    else
+      chol_syrk_kernel<O, BLOCKED, TT><<<(unsigned)(tiles * (tiles + 1) / 2), 256, 0, s>>>(A, S, n, kb, jb, derr);
     HP_LAUNCH_CHECK();
   }
   return HP_OK;

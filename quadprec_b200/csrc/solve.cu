@@ -39,19 +39,35 @@ namespace {
 
 constexpr int TS_THREADS = 1024;
 
-// One CTA; thread t owns rows t, t+1024, ... (RMAX of them).
+// One CTA; thread t owns rows t, t+1024, ... (RMAX of them). The entries of
+// L a step needs (its column below / row right of the diagonal, and the
+// next diagonal element) do not depend on y, so each step loads the next
+// step's while its own multiply-adds run: the per-step chain is the
+// owner's division, one barrier and one multiply-add.
 template <class O, int RMAX, bool UPPER_T>
 __global__ void __launch_bounds__(TS_THREADS) trsv_kernel(const typename O::T* __restrict__ L, typename O::T* y,
                                                           int64_t n) {
   using T = typename O::T;
   __shared__ T bc[2];
   const int t = threadIdx.x;
-  T yr[RMAX];
+  T yr[RMAX], lv[RMAX];
+  auto lval = [&](int64_t step, int r) {
+    const int64_t j = UPPER_T ? n - 1 - step : step;
+    const int64_t i = t + (int64_t)TS_THREADS * r;
+    const bool active = step < n && (UPPER_T ? (i < j) : (i > j && i < n));
+    return active ? (UPPER_T ? L[j * n + i] : L[i * n + j]) : O::zero();
+  };
+  auto ldiag = [&](int64_t step) {
+    const int64_t j = UPPER_T ? n - 1 - step : step;
+    return (step < n && (int)(j % TS_THREADS) == t) ? L[j * n + j] : O::zero();
+  };
 #pragma unroll
   for (int r = 0; r < RMAX; r++) {
     int64_t i = t + (int64_t)TS_THREADS * r;
     yr[r] = i < n ? y[i] : O::zero();
+    lv[r] = lval(0, r);
   }
+  T dg = ldiag(0);
   for (int64_t step = 0; step < n; step++) {
     const int64_t j = UPPER_T ? n - 1 - step : step;
     const int owner = (int)(j % TS_THREADS), rj = (int)(j / TS_THREADS);
@@ -59,17 +75,22 @@ __global__ void __launch_bounds__(TS_THREADS) trsv_kernel(const typename O::T* _
 #pragma unroll
       for (int r = 0; r < RMAX; r++)
         if (r == rj) {
-          yr[r] = O::div(yr[r], L[j * n + j]);
+          yr[r] = O::div(yr[r], dg);
           bc[step & 1] = yr[r];
         }
     }
     __syncthreads();
     const T yj = bc[step & 1];
+    T nx[RMAX];
+#pragma unroll
+    for (int r = 0; r < RMAX; r++) nx[r] = lval(step + 1, r);
+    dg = ldiag(step + 1);
 #pragma unroll
     for (int r = 0; r < RMAX; r++) {
       int64_t i = t + (int64_t)TS_THREADS * r;
       bool active = UPPER_T ? (i < j) : (i > j && i < n);
-      if (active) yr[r] = O::sub(yr[r], O::mul(UPPER_T ? L[j * n + i] : L[i * n + j], yj));
+      if (active) yr[r] = O::sub(yr[r], O::mul(lv[r], yj));
+      lv[r] = nx[r];
     }
   }
 #pragma unroll

@@ -29,6 +29,7 @@ using std::round;
 using std::signbit;
 
 #include "../quadprec_b200/csrc/hp_arith.cuh"
+#include "../quadprec_b200/csrc/hp_mf.cuh"
 
 using namespace hp;
 extern "C" {
@@ -102,6 +103,38 @@ void sh_dd_dot2(const double* c, const double* a, const double* s, const double*
                               dd{b[2 * i], b[2 * i + 1]});
     o[2 * i] = r.hi;
     o[2 * i + 1] = r.lo;
+  }
+}
+}  // extern "C"
+// The generic MultiFloat<N> templates (hp_mf.cuh) for N = 4 and 8.
+template <int N>
+static mfn<N> ldn(const double* p) {
+  mfn<N> r;
+  for (int i = 0; i < N; i++) r.l[i] = p[i];
+  return r;
+}
+template <int N>
+static void stn(double* p, const mfn<N>& v) {
+  for (int i = 0; i < N; i++) p[i] = v.l[i];
+}
+template <int N>
+static void mfn_op(int which, const double* a, const double* b, double* o) {
+  switch (which) {
+    case 0: stn<N>(o, mfn_add<N>(ldn<N>(a), ldn<N>(b))); break;
+    case 1: stn<N>(o, mfn_mul<N>(ldn<N>(a), ldn<N>(b))); break;
+    case 2: stn<N>(o, mfn_div<N>(ldn<N>(a), ldn<N>(b))); break;
+    case 3: stn<N>(o, mfn_sqrt<N>(ldn<N>(a))); break;
+  }
+}
+extern "C" {
+// ops 20-23: MultiFloat<8>, 30-33: MultiFloat<4> through the templates.
+void sh_mfn_batch(int op, const double* a, const double* b, double* o, long count) {
+  const int N = op >= 30 ? 4 : 8;
+  for (long i = 0; i < count; i++) {
+    if (N == 8)
+      mfn_op<8>(op - 20, a + 8 * i, b + 8 * i, o + 8 * i);
+    else
+      mfn_op<4>(op - 30, a + 4 * i, b + 4 * i, o + 4 * i);
   }
 }
 // Many ops at once (count entries of 2 or 4 limbs each).

@@ -25,8 +25,8 @@ def shim():
     os.makedirs(BUILD, exist_ok=True)
     so = os.path.join(BUILD, "libdevice_arith_shim.so")
     src = os.path.join(HERE, "device_arith_shim.cpp")
-    hdr = os.path.join(HERE, "..", "quadprec_b200", "csrc", "hp_arith.cuh")
-    if not os.path.exists(so) or os.path.getmtime(so) < max(os.path.getmtime(src), os.path.getmtime(hdr)):
+    hdrs = [os.path.join(HERE, "..", "quadprec_b200", "csrc", h) for h in ("hp_arith.cuh", "hp_mf.cuh")]
+    if not os.path.exists(so) or os.path.getmtime(so) < max(os.path.getmtime(p) for p in [src, *hdrs]):
         subprocess.run(["/usr/bin/g++", "-O2", "-march=x86-64-v3", "-ffp-contract=off", "-fPIC", "-shared",
                         "-std=c++17", "-o", so, src], check=True)
     L = ctypes.CDLL(so)
@@ -95,6 +95,43 @@ def test_qd_ops_bitexact(shim, op, name):
     for i in range(n):
         want = O.mf_op(name, 4, a[i], b[i]) if name != "sqrt" else O.mf_op("sqrt", 4, a[i])
         assert np.array_equal(got[i], want, equal_nan=True), (name, i, a[i], b[i], got[i], want)
+
+
+def rand_mf(rng, n, N, spread=8):
+    out = np.zeros((n, N))
+    for i in range(n):
+        x = rng.uniform(-1, 1) * 2.0 ** rng.integers(-spread, spread)
+        out[i] = [x * 2.0 ** (-53 * t) * rng.uniform(-1, 1) if t else x for t in range(N)]
+        O.lib().or_mf_renormalize(N, O._p(out[i]))
+    return out
+
+
+@pytest.mark.parametrize("N", [4, 8])
+@pytest.mark.parametrize("op,name", [(0, "add"), (1, "mul"), (2, "div"), (3, "sqrt")])
+def test_mfn_templates_bitexact(shim, N, op, name):
+    """hp_mf.cuh (the MultiFloat<N> templates behind the f512 kernels) against
+    the oracle's MultiFloat<N> for N = 8, and for N = 4 (where they must also
+    agree with the specialised qd_* of hp_arith.cuh)."""
+    shim.sh_mfn_batch.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long]
+    rng = np.random.default_rng(1000 * N + op)
+    n = 600 if N == 8 else 1200
+    a, b = rand_mf(rng, n, N), rand_mf(rng, n, N)
+    if name == "sqrt":
+        a = np.where(a[:, :1] < 0, -a, a)
+    a[:30] = -b[:30]
+    a[30:60] = b[30:60]
+    a[30:60, 2] = -a[30:60, 2]
+    a[60:70] = 0.0
+    a[70:80, 1:] = 0.0
+    a[80:90, N // 2:] = 0.0
+    a, b = np.ascontiguousarray(a), np.ascontiguousarray(b)
+    got = np.zeros_like(a)
+    shim.sh_mfn_batch((20 if N == 8 else 30) + op, a.ctypes.data, b.ctypes.data, got.ctypes.data, n)
+    if N == 4:
+        assert np.array_equal(got, run(shim, 10 + op, a, b, 4), equal_nan=True)
+    for i in range(n):
+        want = O.mf_op(name, N, a[i], b[i]) if name != "sqrt" else O.mf_op("sqrt", N, a[i])
+        assert np.array_equal(got[i], want, equal_nan=True), (N, name, i, a[i], b[i], got[i], want)
 
 
 def test_dd_exp_overlap_range_bitexact(shim):
