@@ -89,12 +89,23 @@ struct CrtTable {
 constexpr int CRT_CONST_L0 = 28, CRT_CONST_N = 5;
 __constant__ CrtTable c_crt[CRT_CONST_N];  // L = CRT_CONST_L0 + i
 
+// Tables of the tensor-core CRT (crt_tc_kernel), for the same moduli counts:
+// the bytes of every weight W_l (the B operand of a u8 MMA: row q holds byte
+// q of W_0 .. W_{L-1}), the 16-bit limbs of M and 2^192 / M.
+struct CrtTcTable {
+  uint8_t wb[32][32];
+  int32_t mlimb[16];
+  double k192;
+};
+__constant__ CrtTcTable c_crt_tc[CRT_CONST_N];  // L = CRT_CONST_L0 + i
+
 // ---------------------------------------------------------------------------
 // Host tables
 // ---------------------------------------------------------------------------
 struct HostTables {
   ModTable mt;
   std::vector<CrtTable> crt;  // index L (1..MAXL)
+  CrtTcTable crt_tc[CRT_CONST_N];
   double cum_log2[MAXL + 1];
 };
 
@@ -210,6 +221,23 @@ static const HostTables& host_tables() {
         Big W = P;
         big_mul_small(W, (uint32_t)inv);  // < M since inv < m_l
         for (int c = 0; c < ct.nc; c++) ct.w[l][c] = big_chunk(W, c);
+        if (L >= CRT_CONST_L0 && L < CRT_CONST_L0 + CRT_CONST_N) {
+          CrtTcTable& tc = T.crt_tc[L - CRT_CONST_L0];
+          for (int q = 0; q < 32; q++) {
+            const size_t w = (size_t)q / 4;
+            tc.wb[q][l] = w < W.d.size() ? (uint8_t)(W.d[w] >> (8 * (q % 4))) : 0;
+          }
+        }
+      }
+      if (L >= CRT_CONST_L0 && L < CRT_CONST_L0 + CRT_CONST_N) {
+        CrtTcTable& tc = T.crt_tc[L - CRT_CONST_L0];
+        for (int h = 0; h < 16; h++) {
+          const size_t w = (size_t)h / 2;
+          tc.mlimb[h] = w < M.d.size() ? (int32_t)((M.d[w] >> (16 * (h % 2))) & 0xFFFFu) : 0;
+        }
+        long double mv = 0;
+        for (size_t i = M.d.size(); i-- > 0;) mv = mv * 4294967296.0L + (long double)M.d[i];
+        tc.k192 = (double)(std::ldexp(1.0L, 192) / mv);
       }
     }
   });
@@ -234,6 +262,7 @@ static int device_tables(DevTables** out) {
     const HostTables& T = host_tables();
     HP_CUDA_TRY(cudaMemcpyToSymbol(c_tab, &T.mt, sizeof(ModTable)));
     HP_CUDA_TRY(cudaMemcpyToSymbol(c_crt, &T.crt[CRT_CONST_L0], sizeof(CrtTable) * CRT_CONST_N));
+    HP_CUDA_TRY(cudaMemcpyToSymbol(c_crt_tc, T.crt_tc, sizeof(CrtTcTable) * CRT_CONST_N));
     HP_CUDA_TRY(cudaMalloc(&D.crt, sizeof(CrtTable) * (MAXL + 1)));
     HP_CUDA_TRY(cudaMemcpy(D.crt, T.crt.data(), sizeof(CrtTable) * (MAXL + 1), cudaMemcpyHostToDevice));
     HP_CUDA_TRY(cudaDeviceGetAttribute(&D.num_sms, cudaDevAttrMultiProcessorCount, d));
@@ -761,6 +790,211 @@ __global__ void __launch_bounds__(256, 1)
 }
 
 // ---------------------------------------------------------------------------
+// The same residue GEMM on CTA pairs (a cluster of 2, tcgen05 cta_group::2):
+// a pair computes a 256 x 256 tile of one modulus; each CTA holds 128 rows
+// of the A tile and 128 rows of the B tile per K-block and its 128 x 256
+// half of the accumulator. Against the one-CTA kernel (128 x 256 per SM)
+// every SM stages half as many B bytes per MMA, so the shared memory that
+// TMA writes and the tensor core reads carries 8 KB instead of 12 KB per
+// 2 M int8 multiply-adds. Roles: warp 0 of each CTA issues its own TMA
+// loads, counted on the even CTA's barrier (which expects both CTAs'
+// bytes); warp 1 of the even CTA issues the pair MMAs and commits to both
+// CTAs' barriers; warps 4-11 of each CTA reduce their half of the
+// accumulator mod m (warps 4-7 columns 0-127, warps 8-11 columns 128-255:
+// TMEM lane group = warp index mod 4) and arrive on the even CTA's
+// accumulator-free barrier.
+// Waits are bounded as in the one-CTA kernel; every thread of both CTAs
+// meets at a cluster barrier before the TMEM is released.
+// ---------------------------------------------------------------------------
+constexpr int GP_M = 256, GP_N = 256, GP_HALF = 128, GP_STAGES = 6;
+constexpr int GP_THREADS = 384, GP_EPI_THREADS = 256;  // per CTA: warps 4-11 run the epilogue
+constexpr int GP_STAGE = 2 * GP_HALF * GB_K;  // A half + B half, bytes per CTA per stage
+constexpr int GP_SMEM = GP_STAGES * GP_STAGE + 1024 + 256;
+static_assert(GP_SMEM <= 227 * 1024, "pair GEMM stages fit the shared memory of one CTA");
+
+template <bool U8>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(GP_THREADS, 1)
+    i8_gemm_pair_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int L,
+                        int tiles_m, int tiles_n, int kb0, int kb1, int acc_mode, uint8_t* __restrict__ cres,
+                        int64_t ldc, int64_t plane, uint32_t* status) {
+  using namespace sm100;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
+  uint8_t* smem = smem_raw + pad;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smem + GP_STAGES * GP_STAGE);
+  uint64_t* full = bars;
+  uint64_t* empty = bars + GP_STAGES;
+  uint64_t* tfull = bars + 2 * GP_STAGES;
+  uint64_t* tempty = tfull + 2;
+  uint64_t* drain = tempty + 2;
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(drain + 1);
+  const int warp = threadIdx.x / 32, lane = threadIdx.x % 32;
+  const uint32_t rank = cluster_ctarank();
+  const bool leader = rank == 0;
+  if (threadIdx.x == 0) {
+    for (int st = 0; st < GP_STAGES; st++) {
+      mbar_init(&full[st], 1);
+      mbar_init(&empty[st], 1);
+    }
+    for (int a = 0; a < 2; a++) {
+      mbar_init(&tfull[a], 1);
+      mbar_init(&tempty[a], 2 * GP_EPI_THREADS);
+    }
+    mbar_init(drain, 1);
+    fence_mbarrier_init();
+  }
+  if (warp == 0 && lane == 0) {
+    prefetch_tmap(&mapA);
+    prefetch_tmap(&mapB);
+  }
+  if (warp == 2) {
+    tmem_alloc_pair(tmem_slot, 2 * GP_N);
+    tmem_relinquish_pair();
+  }
+  tc_fence_before();
+  cluster_sync_all();  // barriers initialised and TMEM allocated in both CTAs
+  tc_fence_after();
+  const uint32_t tmem_base = *tmem_slot;
+  griddep_launch_dependents();
+  griddep_wait();
+
+  const int pair = blockIdx.x / 2, npairs = gridDim.x / 2;
+  const int nkb = kb1 - kb0;
+  const int per_l = tiles_m * tiles_n;
+  const int num_tiles = L * per_l;
+  bool stalled = false;  // this thread gave up a wait
+
+  if (warp == 0) {
+    if (lane == 0) {
+      uint32_t stage = 0, phase = 0;
+      const uint32_t full0 = mapa_shared(smem_u32(full), 0);
+      for (int t = pair; t < num_tiles && !stalled; t += npairs) {
+        const int l = t / per_l, rem = t % per_l, tm = rem / tiles_n, tn = rem % tiles_n;
+        for (int kb = 0; kb < nkb; kb++) {
+          if (!mbar_wait(&empty[stage], phase ^ 1, status, DEV_STATUS_TIMEOUT)) {
+            stalled = true;
+            break;
+          }
+          if (leader) mbar_arrive_expect_tx(&full[stage], 2 * GP_STAGE);
+          uint8_t* sA = smem + stage * GP_STAGE;
+          const uint32_t bar = full0 + stage * (uint32_t)sizeof(uint64_t);
+          tma_load_3d_pair(sA, &mapA, bar, (kb0 + kb) * GB_K, tm * GP_M + (int)rank * GP_HALF, l);
+          tma_load_3d_pair(sA + GP_HALF * GB_K, &mapB, bar, (kb0 + kb) * GB_K, tn * GP_N + (int)rank * GP_HALF, l);
+          if (++stage == GP_STAGES) {
+            stage = 0;
+            phase ^= 1;
+          }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0 && leader) {
+      uint32_t stage = 0, phase = 0, it = 0;
+      bool issued = false;
+      const uint32_t idesc = idesc_i8(GP_M, GP_N, U8);
+      for (int t = pair; t < num_tiles && !stalled; t += npairs, it++) {
+        const uint32_t acc = it & 1, aph = (it >> 1) & 1;
+        if (!mbar_wait(&tempty[acc], aph ^ 1, status, DEV_STATUS_TIMEOUT)) {
+          stalled = true;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t d = tmem_base + acc * GP_N;
+        for (int kb = 0; kb < nkb; kb++) {
+          if (!mbar_wait(&full[stage], phase, status, DEV_STATUS_TIMEOUT)) {
+            stalled = true;
+            break;
+          }
+          tc_fence_after();
+          const uint32_t a0 = smem_u32(smem + stage * GP_STAGE), b0 = a0 + GP_HALF * GB_K;
+#pragma unroll
+          for (int kk = 0; kk < GB_K / 32; kk++)
+            mma_i8_pair(d, desc_k_sw128(a0 + kk * 32), desc_k_sw128(b0 + kk * 32), idesc, (kb | kk) ? 1u : 0u);
+          issued = true;
+          mma_commit_pair(&empty[stage], 0x3);
+          if (++stage == GP_STAGES) {
+            stage = 0;
+            phase ^= 1;
+          }
+        }
+        if (stalled) break;
+        mma_commit_pair(&tfull[acc], 0x3);
+      }
+      if (stalled && issued) {  // wait for issued MMAs before TMEM is released
+        mma_commit_pair(drain, 0x1);
+        mbar_wait(drain, 0, status, DEV_STATUS_TIMEOUT, 100000000ull);
+      }
+    }
+  } else if (warp >= 4) {
+    const int ew = warp % 4;                  // TMEM lane group
+    const int cbase = warp >= 8 ? GP_N / 2 : 0;  // this warp's 128 columns
+    constexpr int EC = GP_N / 2;
+    uint32_t it = 0;
+    const uint32_t tempty0 = mapa_shared(smem_u32(tempty), 0);
+    for (int t = pair; t < num_tiles; t += npairs, it++) {
+      const int l = t / per_l, rem = t % per_l, tm = rem / tiles_n, tn = rem % tiles_n;
+      const uint32_t acc = it & 1, aph = (it >> 1) & 1;
+      const uint32_t m = (uint32_t)c_tab.mod[l];
+      const int64_t row = (int64_t)tm * GP_M + (int64_t)rank * GP_HALF + ew * 32 + lane;
+      uint8_t* dst = cres + (size_t)l * plane + (size_t)row * ldc + (size_t)tn * GP_N + cbase;
+      uint4 prev[EC / 16];
+      if (acc_mode) {
+#pragma unroll
+        for (int q = 0; q < EC / 16; q++) prev[q] = *reinterpret_cast<const uint4*>(dst + 16 * q);
+      }
+      const bool ok = mbar_wait(&tfull[acc], aph, status, DEV_STATUS_TIMEOUT);
+      if (!__all_sync(0xffffffffu, ok)) break;
+      tc_fence_after();
+#pragma unroll
+      for (int ch = 0; ch < EC / 32; ch++) {
+        uint32_t v[32];
+        tmem_ld_32x32b_x32(tmem_base + ((uint32_t)(ew * 32) << 16) + acc * GP_N + cbase + ch * 32, v);
+        tmem_wait_ld();
+        uint4 prev0 = make_uint4(0, 0, 0, 0), prev1 = make_uint4(0, 0, 0, 0);
+        if (acc_mode) {
+#pragma unroll
+          for (int q = 0; q < EC / 32; q++)
+            if (q == ch) {
+              prev0 = prev[2 * q];
+              prev1 = prev[2 * q + 1];
+            }
+        }
+        const uint32_t pv[8] = {prev0.x, prev0.y, prev0.z, prev0.w, prev1.x, prev1.y, prev1.z, prev1.w};
+        uint32_t packed[8];
+#pragma unroll
+        for (int w = 0; w < 8; w++) {
+          uint32_t word = 0;
+#pragma unroll
+          for (int b = 0; b < 4; b++) {
+            uint32_t r = mod_reduce((int32_t)v[4 * w + b], l);
+            if (acc_mode) {  // C = (C + AB) mod m (a later K-chunk)
+              r += (pv[w] >> (8 * b)) & 0xFFu;
+              if (r >= m) r -= m;
+            }
+            word |= r << (8 * b);
+          }
+          packed[w] = word;
+        }
+        *reinterpret_cast<uint4*>(dst + ch * 32) = make_uint4(packed[0], packed[1], packed[2], packed[3]);
+        *reinterpret_cast<uint4*>(dst + ch * 32 + 16) = make_uint4(packed[4], packed[5], packed[6], packed[7]);
+      }
+      tc_fence_before();
+      mbar_arrive_cluster(tempty0 + acc * (uint32_t)sizeof(uint64_t));
+    }
+  }
+  if (stalled) {  // let loads this CTA issued land before its shared memory goes away
+    for (int q = 0; q < 1000; q++) __nanosleep(1000);
+  }
+  __syncthreads();
+  tc_fence_before();
+  cluster_sync_all();  // both CTAs done with the MMAs and their TMEM halves
+  if (warp == 2) {
+    tc_fence_after();
+    tmem_dealloc_pair(tmem_base, 2 * GP_N);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // CRT reconstruction: residues -> exact integer -> f128, scaled back.
 // Each thread reconstructs 4 consecutive entries of a row (one 4-byte load
 // per modulus). With NC chunks of 39 bits, every accumulator stays an exact
@@ -890,6 +1124,143 @@ __global__ void __launch_bounds__(256) crt_dd_kernel(const uint8_t* __restrict__
 }
 
 // ---------------------------------------------------------------------------
+// CRT on the tensor core (the f128 GEMM, L = 28..32 moduli). For an entry
+// with product residues r_l, the CRT value V = sum_l r_l W_l is split by the
+// bytes of the weights: V = sum_q 2^(8q) S_q with S_q = sum_l r_l w_lq, an
+// exact u8 x u8 dot product (< 30 * 255^2 < 2^21). A CTA takes 128
+// consecutive entries of a row, transposes their residues into a 128 x 32
+// byte tile (128-byte swizzled rows) and multiplies it by the 32 x 32 byte
+// matrix of the weights with one M = 128, N = 32, K = 32 tcgen05 MMA; each
+// thread then reads its entry's 32 sums from TMEM and finishes in integer
+// arithmetic: 16-bit limbs U_h = S_2h + 2^8 S_2h+1, the quotient q =
+// round(V / M) from the top limbs (|V - q M| <= M/4 leaves a wide margin
+// for the estimate), C = V - q M limb by limb with balanced carries, and the
+// exact limbs summed from the top into a double-double. Integer and tensor
+// work replace the FP64 pipe's 30 x 6 weighted multiply-adds per entry.
+// ---------------------------------------------------------------------------
+constexpr int CT_THREADS = 128, CT_SMEM = 1024 + 128 * 128 + 32 * 128;
+
+template <int LC>
+__global__ void __launch_bounds__(CT_THREADS, 4)
+    crt_tc_kernel(const uint8_t* __restrict__ cres, int64_t plane, int64_t Np, int64_t m, int64_t n,
+                  const int* __restrict__ expA, const int* __restrict__ expB, int beta, double2* __restrict__ C,
+                  uint32_t* status) {
+  using namespace sm100;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
+  uint8_t* sA = smem_raw + pad;   // 128 rows (entries) x 128 bytes, swizzled
+  uint8_t* sB = sA + 128 * 128;   // 32 rows (weight bytes q) x 128 bytes, swizzled
+  __shared__ uint64_t bar;
+  __shared__ uint32_t tmem_slot;
+  const CrtTcTable& T = c_crt_tc[LC - CRT_CONST_L0];
+  const int t = threadIdx.x, warp = t / 32, lane = t % 32;
+  // swizzled byte address of (row, logical byte k) in a 128-byte-row tile
+  auto swz = [](int row, int k) { return (row >> 3) * 1024 + (row & 7) * 128 + (((k >> 4) ^ (row & 7)) << 4) + (k & 15); };
+  for (int e = t; e < 32 * 32; e += CT_THREADS) sB[swz(e / 32, e % 32)] = T.wb[e / 32][e % 32];
+  if (t == 0) {
+    mbar_init(&bar, 1);
+    fence_mbarrier_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(&tmem_slot, 32);
+    tmem_relinquish();
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  griddep_launch_dependents();
+  griddep_wait();  // the product residues come from the preceding GEMM
+  const int64_t tpr = (n + 127) / 128, ntiles = m * tpr;
+  const uint32_t idesc = idesc_i8(128, 32, true);
+  uint32_t phase = 0;
+  bool ok = true;
+  for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    const int64_t i = tile / tpr, j0 = (tile % tpr) * 128;
+    // residues: warp w loads moduli 8w .. 8w+7, lane the 4 entries 4 lane .. 4 lane + 3
+    uint32_t wv[8];
+    const uint8_t* rp = cres + (size_t)i * Np + j0 + 4 * lane;
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int l = 8 * warp + u;
+      wv[u] = l < LC ? __ldg(reinterpret_cast<const uint32_t*>(rp + (size_t)l * plane)) : 0u;
+    }
+    // transpose to entry-major: entry e's bytes of moduli 8w .. 8w+7 -> row 4 lane + e, bytes 8w .. 8w+7
+#pragma unroll
+    for (int e = 0; e < 4; e++) {
+      const uint32_t sel = (uint32_t)e | ((uint32_t)(e + 4) << 4);
+      const uint32_t lo = __byte_perm(__byte_perm(wv[0], wv[1], sel), __byte_perm(wv[2], wv[3], sel), 0x5410);
+      const uint32_t hi = __byte_perm(__byte_perm(wv[4], wv[5], sel), __byte_perm(wv[6], wv[7], sel), 0x5410);
+      *reinterpret_cast<uint2*>(sA + swz(4 * lane + e, 8 * warp)) = make_uint2(lo, hi);
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    __syncthreads();  // tile written; the previous tile's TMEM reads are done
+    tc_fence_after();
+    if (t == 0) {
+      mma_i8(tmem, desc_k_sw128(smem_u32(sA)), desc_k_sw128(smem_u32(sB)), idesc, 0u);
+      mma_commit(&bar);
+    }
+    ok = mbar_wait(&bar, phase, status, DEV_STATUS_TIMEOUT);
+    phase ^= 1;
+    if (!__all_sync(0xffffffffu, ok)) {
+      ok = false;
+      break;
+    }
+    tc_fence_after();
+    uint32_t v[32];
+    tmem_ld_32x32b_x32(tmem + ((uint32_t)(warp * 32) << 16), v);
+    tmem_wait_ld();
+    const int64_t j = j0 + t;
+    if (j >= n) continue;
+    const int ea = expA[i], eb = expB[j];
+    if (ea == EXP_NONFINITE || eb == EXP_NONFINITE) {
+      C[i * n + j] = make_double2(__longlong_as_double(0x7ff8000000000000ll), 0.0);
+      continue;
+    }
+    int32_t U[16];
+#pragma unroll
+    for (int h = 0; h < 16; h++) U[h] = (int32_t)(v[2 * h] + (v[2 * h + 1] << 8));
+    // q = round(V / M) from the top limbs (the rest moves V / M by < 2^-29)
+    const double vt = __dadd_rn(__dadd_rn(__dmul_rn((double)U[15], 0x1p48), __dmul_rn((double)U[14], 0x1p32)),
+                                __dadd_rn(__dmul_rn((double)U[13], 0x1p16), (double)U[12]));
+    const int32_t q = (int32_t)rint(__dmul_rn(vt, T.k192));
+    // C = V - q M in balanced base-2^16 digits b_h in [-2^15, 2^15)
+    int32_t b[18];
+    int32_t carry = 0;
+#pragma unroll
+    for (int h = 0; h < 16; h++) {
+      const int32_t x = U[h] - q * T.mlimb[h] + carry;
+      carry = (x + 0x8000) >> 16;
+      b[h] = x - (carry << 16);
+    }
+    b[16] = carry;
+    b[17] = 0;
+    // exact 48-bit chunks, summed from the top into a double-double
+    dd sum = dd{0.0, 0.0};
+#pragma unroll
+    for (int k = 5; k >= 0; k--) {
+      const double ch = __dadd_rn(__dadd_rn((double)b[3 * k], __dmul_rn((double)b[3 * k + 1], 0x1p16)),
+                                  __dmul_rn((double)b[3 * k + 2], 0x1p32));
+      const double vk = scale_pow2(ch, 48 * k);
+      double hs, he;
+      two_sum(sum.hi, vk, hs, he);
+      sum = dd_renorm(hs, __dadd_rn(he, sum.lo));
+    }
+    const int shift = -((beta + 1022 - ea) + (beta + 1022 - eb));
+    const dd o = dd_renorm(scale_pow2(sum.hi, shift), scale_pow2(sum.lo, shift));
+    C[i * n + j] = make_double2(o.hi, o.lo);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 32);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Host driver
 // ---------------------------------------------------------------------------
 static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
@@ -959,6 +1330,24 @@ static int launch_crt_dd(const uint8_t* cres, size_t Mp, size_t Np, size_t m, si
   }
 #undef HP_CRT_CASE
   return HP_OK;
+}
+
+// The tensor-core CRT for L = 28..32 (the counts k <= 2^20 needs at beta =
+// 106); HP_ERR_UNSUPPORTED for other L. Np must be a multiple of 128.
+static int launch_crt_tc(const uint8_t* cres, size_t Mp, size_t Np, size_t m, size_t n, const int* expA,
+                         const int* expB, int beta, int L, double2* C, int num_sms, uint32_t* status, cudaStream_t s,
+                         bool pdl) {
+  const int grid = num_sms * 4;
+#define HP_CRT_TC(LCV)                                                                                         \
+  if (L == LCV) {                                                                                              \
+    HP_CUDA_TRY(launch_k(pdl, crt_tc_kernel<LCV>, dim3(grid), dim3(CT_THREADS), CT_SMEM, s, cres,              \
+                         (int64_t)(Mp * Np), (int64_t)Np, (int64_t)m, (int64_t)n, expA, expB, beta, C, status)); \
+    return HP_OK;                                                                                              \
+  }
+  HP_CRT_TC(28) HP_CRT_TC(29) HP_CRT_TC(30) HP_CRT_TC(31) HP_CRT_TC(32)
+#undef HP_CRT_TC
+  set_error("ozaki: no tensor-core CRT for %d moduli", L);
+  return HP_ERR_UNSUPPORTED;
 }
 
 static inline size_t round_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -1040,6 +1429,47 @@ int ozaki_residue_gemm_k(const int8_t* ares, const int8_t* bres, uint8_t* cres, 
   return HP_OK;
 }
 
+// Residue GEMM of the f128 GEMM on CTA pairs: cres[l] = (A_l B_l^T) mod m_l for
+// Mp x Np (Mp a multiple of 256, Np of 256), K of ka bytes per row.
+int ozaki_residue_gemm_pair(const int8_t* ares, const int8_t* bres, uint8_t* cres, int L, size_t Mp, size_t Np,
+                            size_t ka, cudaStream_t s, bool pdl, bool u8) {
+  using namespace ozaki;
+  DevTables* D;
+  HP_TRY(device_tables(&D));
+  static bool attr_set[64] = {};
+  int dev = 0;
+  HP_CUDA_TRY(cudaGetDevice(&dev));
+  if (dev < 64 && !attr_set[dev]) {
+    HP_CUDA_TRY(cudaFuncSetAttribute(i8_gemm_pair_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, GP_SMEM));
+    HP_CUDA_TRY(cudaFuncSetAttribute(i8_gemm_pair_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, GP_SMEM));
+    attr_set[dev] = true;
+  }
+  CUtensorMap mapA, mapB;
+  HP_TRY(make_map(&mapA, ares, ka, Mp, L, GP_HALF));
+  HP_TRY(make_map(&mapB, bres, ka, Np, L, GP_HALF));
+  uint32_t* status = device_status(s);
+  if (!status) {
+    set_error("status word allocation failed");
+    return HP_ERR_CUDA;
+  }
+  const int tiles_m = (int)(Mp / GP_M), tiles_n = (int)(Np / GP_N);
+  const int num_tiles = L * tiles_m * tiles_n;
+  const int grid = 2 * std::min(num_tiles, D->num_sms / 2);
+  const int nkb_total = (int)(ka / GB_K);
+  const int kb_chunk = (u8 ? MAX_K_CHUNK_U8 : MAX_K_CHUNK) / GB_K;
+  for (int c0 = 0; c0 < nkb_total; c0 += kb_chunk) {
+    const int kb1 = std::min(nkb_total, c0 + kb_chunk);
+    const int mode = c0 > 0 ? 1 : 0;
+    if (u8)
+      HP_CUDA_TRY(launch_k(pdl && c0 == 0, i8_gemm_pair_kernel<true>, dim3(grid), dim3(GP_THREADS), GP_SMEM, s, mapA, mapB, L,
+                           tiles_m, tiles_n, c0, kb1, mode, cres, (int64_t)Np, (int64_t)(Mp * Np), status));
+    else
+      HP_CUDA_TRY(launch_k(pdl && c0 == 0, i8_gemm_pair_kernel<false>, dim3(grid), dim3(GP_THREADS), GP_SMEM, s, mapA, mapB,
+                           L, tiles_m, tiles_n, c0, kb1, mode, cres, (int64_t)Np, (int64_t)(Mp * Np), status));
+  }
+  return HP_OK;
+}
+
 namespace {
 // The f128 GEMM's residue launch, specialised on the moduli count for the
 // counts k <= 2^20 needs (28-32 at beta = 106; others take the runtime loop).
@@ -1099,7 +1529,8 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
     set_error("ozaki: k = %zu needs more moduli than the table holds", k);
     return HP_ERR_UNSUPPORTED;
   }
-  const size_t Mp = round_up(m, GB_M), Np = round_up(n, GB_N), Kp = round_up(k, GB_K);
+  // rows padded to the CTA pair's 256-row tile (the padding holds zero residues)
+  const size_t Mp = round_up(m, GP_M), Np = round_up(n, GB_N), Kp = round_up(k, GB_K);
   if (Mp / GB_M * (Np / GB_N) * (size_t)L > (size_t)INT32_MAX || Kp > (size_t)INT32_MAX) {
     set_error("ozaki: problem too large");
     return HP_ERR_INVALID_ARG;
@@ -1131,13 +1562,22 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
                                    (int64_t)(Np * Kp), (int64_t)k, beta, (int64_t)Kp));
   }
   profile_mark(s, "residues");
-  // 3. one int8 GEMM per modulus
-  HP_TRY(ozaki_residue_gemm_k(ares.as<int8_t>(), bres.as<int8_t>(), cres.as<uint8_t>(), L, Mp, Np, Kp, Kp, 0, Kp, 0, Np,
-                              Mp * Np, 0, 0, 0, s, Mp, Np, pdl, true));
+  // 3. one int8 GEMM per modulus, on CTA pairs
+  HP_TRY(ozaki_residue_gemm_pair(ares.as<int8_t>(), bres.as<int8_t>(), cres.as<uint8_t>(), L, Mp, Np, Kp, s, pdl, true));
   profile_mark(s, "i8_gemm");
-  // 4. CRT
-  HP_TRY(launch_crt_dd(cres.as<uint8_t>(), Mp, Np, m, n, expA, expB, beta, D->crt + L, host_tables().crt[L].nc,
-                       reinterpret_cast<double2*>(c), s, pdl, L));
+  // 4. CRT (on the tensor core for the usual moduli counts)
+  if (L >= CRT_CONST_L0 && L < CRT_CONST_L0 + CRT_CONST_N) {
+    uint32_t* status = device_status(s);
+    if (!status) {
+      set_error("status word allocation failed");
+      return HP_ERR_CUDA;
+    }
+    HP_TRY(launch_crt_tc(cres.as<uint8_t>(), Mp, Np, m, n, expA, expB, beta, L, reinterpret_cast<double2*>(c),
+                         D->num_sms, status, s, pdl));
+  } else {
+    HP_TRY(launch_crt_dd(cres.as<uint8_t>(), Mp, Np, m, n, expA, expB, beta, D->crt + L, host_tables().crt[L].nc,
+                         reinterpret_cast<double2*>(c), s, pdl, L));
+  }
   profile_mark(s, "crt");
   return HP_OK;
 }
@@ -1192,7 +1632,7 @@ int ozaki_dd_gemm_host(const double* a, const double* b, double* c, size_t m, si
   }
   const size_t Np = round_up(n, GB_N), Kp = round_up(k, GB_K);
   const size_t panels_wanted = m >= 2048 ? 16 : m >= 1024 ? 8 : 4;
-  const size_t pr = round_up((m + panels_wanted - 1) / panels_wanted, GB_M);  // rows per panel
+  const size_t pr = round_up((m + panels_wanted - 1) / panels_wanted, GP_M);  // rows per panel (CTA-pair tiles)
   const size_t np = (m + pr - 1) / pr;
   if (pr / GB_M * (Np / GB_N) * (size_t)L > (size_t)INT32_MAX || Kp > (size_t)INT32_MAX) {
     set_error("ozaki: problem too large");
@@ -1240,7 +1680,7 @@ int ozaki_dd_gemm_host(const double* a, const double* b, double* c, size_t m, si
                                  (int64_t)(Np * Kp), (int64_t)k, beta, (int64_t)Kp));
   const int nc = host_tables().crt[L].nc;
   for (size_t i = 0; i < np; i++) {
-    const size_t r0 = i * pr, mi = std::min(pr, m - r0), Mpi = round_up(mi, GB_M);
+    const size_t r0 = i * pr, mi = std::min(pr, m - r0), Mpi = round_up(mi, GP_M);
     const double2* A2 = dA.as<const double2>() + r0 * k;
     double* Ci = dC.as<double>() + r0 * n * 2;
     HP_CUDA_TRY(cudaStreamWaitEvent(s, eA[i], 0));
@@ -1249,10 +1689,14 @@ int ozaki_dd_gemm_host(const double* a, const double* b, double* c, size_t m, si
     HP_CUDA_TRY(launch_residues_ab(false, L, pdl, dim3((unsigned)(Kp / (4 * RES_EPR)), tay), s, A2, (int64_t)mi,
                                    expA, ares.as<int8_t>(), (int64_t)(Mpi * Kp), tay, nullptr, 0, nullptr, nullptr,
                                    0, (int64_t)k, beta, (int64_t)Kp));
-    HP_TRY(ozaki_residue_gemm_k(ares.as<int8_t>(), bres.as<int8_t>(), cres.as<uint8_t>(), L, Mpi, Np, Kp, Kp, 0, Kp,
-                                0, Np, Mpi * Np, 0, 0, 0, s, Mpi, Np, pdl, true));
-    HP_TRY(launch_crt_dd(cres.as<uint8_t>(), Mpi, Np, mi, n, expA, expB, beta, D->crt + L, nc,
-                         reinterpret_cast<double2*>(Ci), s, pdl, L));
+    HP_TRY(ozaki_residue_gemm_pair(ares.as<int8_t>(), bres.as<int8_t>(), cres.as<uint8_t>(), L, Mpi, Np, Kp, s, pdl,
+                                   true));
+    if (L >= CRT_CONST_L0 && L < CRT_CONST_L0 + CRT_CONST_N)
+      HP_TRY(launch_crt_tc(cres.as<uint8_t>(), Mpi, Np, mi, n, expA, expB, beta, L, reinterpret_cast<double2*>(Ci),
+                           D->num_sms, device_status(s), s, pdl));
+    else
+      HP_TRY(launch_crt_dd(cres.as<uint8_t>(), Mpi, Np, mi, n, expA, expB, beta, D->crt + L, nc,
+                           reinterpret_cast<double2*>(Ci), s, pdl, L));
     HP_CUDA_TRY(cudaEventRecord(eC[i], s));
     HP_CUDA_TRY(cudaStreamWaitEvent(sout, eC[i], 0));
     HP_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<char*>(c) + r0 * n * 16, Ci, mi * n * 16, cudaMemcpyDeviceToHost,
@@ -2392,7 +2836,10 @@ static int noalloc_setup(NoAllocDev** out) {
   if (!N.ready) {
     const HostTables& T = host_tables();
     // the modulus table is uploaded by whichever Ozaki path runs first
-    if (!g_dev[d].ready) HP_CUDA_TRY(cudaMemcpyToSymbol(c_tab, &T.mt, sizeof(ModTable)));
+    if (!g_dev[d].ready) {
+      HP_CUDA_TRY(cudaMemcpyToSymbol(c_tab, &T.mt, sizeof(ModTable)));
+      HP_CUDA_TRY(cudaMemcpyToSymbol(c_crt_tc, T.crt_tc, sizeof(CrtTcTable) * CRT_CONST_N));
+    }
     HP_CUDA_TRY(cudaMemcpyToSymbol(g_noalloc_crt, T.crt.data(), sizeof(CrtTable) * (MAXL + 1)));
     HP_CUDA_TRY(cudaGetSymbolAddress((void**)&N.scratch, g_noalloc_scratch));
     HP_CUDA_TRY(cudaGetSymbolAddress((void**)&N.crt, g_noalloc_crt));
@@ -2486,8 +2933,12 @@ static int ozaki_dd_gemm_noalloc(const double* a, const double* b, double* c, si
       HP_LAUNCH_CHECK();
     }
   }
-  HP_TRY(launch_crt_dd(cres, Mp, Np, m, n, expA, expB, beta, N->crt + L, host_tables().crt[L].nc,
-                       reinterpret_cast<double2*>(c), s));
+  if (L >= CRT_CONST_L0 && L < CRT_CONST_L0 + CRT_CONST_N)
+    HP_TRY(launch_crt_tc(cres, Mp, Np, m, n, expA, expB, beta, L, reinterpret_cast<double2*>(c), N->num_sms,
+                         N->status, s, false));
+  else
+    HP_TRY(launch_crt_dd(cres, Mp, Np, m, n, expA, expB, beta, N->crt + L, host_tables().crt[L].nc,
+                         reinterpret_cast<double2*>(c), s));
   // The status word lives in the static array as well; it is read back here,
   // before the next call clears it, so a wait that gave up is reported by
   // the call it happened in.
