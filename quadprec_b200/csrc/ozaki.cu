@@ -574,6 +574,272 @@ __global__ void __launch_bounds__(256) residue_ab_kernel(const double2* __restri
 }
 
 // ---------------------------------------------------------------------------
+// Residues on the tensor core (the unsigned residue planes of the f128 GEMM,
+// L = 28..32 moduli). An entry's scaled integer X = rint(hi 2^s) +
+// rint(lo 2^s), |X| < 2^109, is offset to X' = X + 2^111 in (0, 2^112), and
+// its 16 bytes x_0 .. x_13, x_14 = 1, x_15 = 0 form one K-chunk of an MMA
+// operand. With the weights w_lb = 2^(8b) mod m_l (b < 14), w_l14 = -2^111
+// mod m_l and w_l15 = 0, the sum S_l = sum_b x_b w_lb is congruent to X mod
+// m_l, and S_l < 16 * 255^2 < 2^20, so one multiply-high by ceil(2^32 / m_l)
+// gives floor(S_l / m_l) exactly and S_l - m_l floor(S_l / m_l) is X's
+// residue in [0, m_l), the byte the integer kernel (residue_tile) writes.
+// A tile is 8 operand rows x 128 consecutive reduction indices p: TMA brings
+// its entries into a 3-stage ring, each thread turns 4 entries into bytes
+// (row p of a 128-byte-swizzled 128 x 128 byte tile, 16-byte slot j for
+// operand row j), and four M = 128, N = 128, K = 32 MMAs place the sums of
+// slot 4a + g, modulus l at TMEM lane 32 g + l of accumulator a: the weight
+// tile holds w_l in 16-byte chunk g of row 32 g + l. Warp w then reads lane
+// quarter g = w % 4 of accumulator a = w / 4: lane l owns modulus l and 128
+// consecutive p of one operand row, reduces them and stores 128 bytes.
+// ---------------------------------------------------------------------------
+constexpr int RC_THREADS = 256, RC_STAGES = 2, RC_ROWS = 8, RC_P = 128;
+constexpr int RC_IN_BYTES = RC_ROWS * RC_P * 16;
+constexpr int RC_OUT_PLANE = RC_ROWS * RC_P + 16;  // staged bytes of one modulus (padded: no bank conflicts)
+constexpr int RC_SMEM = 1024 + 2 * 128 * 128 + RC_STAGES * RC_IN_BYTES + 32 * RC_OUT_PLANE;
+
+struct ResidueOperand {  // one GEMM operand as the residue kernel sees it
+  int8_t* out;           // L planes of rows x ld bytes
+  int64_t plane, ld;     // plane stride, row stride (bytes)
+  const int* exps;       // per-row exponents
+  int64_t row_tiles, p_tiles;  // tiles of RC_ROWS rows x RC_P reduction indices
+};
+
+// The tiles of a persistent CTA (first, first + stride, ...) in a grid of
+// `cols` tiles per row, walked without a division per step.
+struct TileWalk {
+  int64_t r, c, dr, dc, cols;
+  __device__ __forceinline__ TileWalk(int64_t first, int64_t stride, int64_t cols_)
+      : r(first / cols_), c(first % cols_), dr(stride / cols_), dc(stride % cols_), cols(cols_) {}
+  __device__ __forceinline__ void next() {
+    c += dc;
+    r += dr;
+    if (c >= cols) {
+      c -= cols;
+      r++;
+    }
+  }
+};
+// A ring position: stage index and the parity of its current use.
+struct RingPos {
+  int st = 0;
+  uint32_t ph = 0;
+  template <int S>
+  __device__ __forceinline__ void next() {
+    if (++st == S) {
+      st = 0;
+      ph ^= 1u;
+    }
+  }
+};
+
+// |x| < 2^108, integer-valued: x as a two's-complement 128-bit integer
+__device__ __forceinline__ void int128_of(double x, uint64_t& lo, uint64_t& hi) {
+  const double a = fabs(x);
+  const double th = floor(__dmul_rn(a, 0x1p-64));        // exact
+  const double rh = __dsub_rn(a, __dmul_rn(th, 0x1p64));  // a mod 2^64, exact
+  lo = __double2ull_rz(rh);
+  hi = __double2ull_rz(th);
+  if (signbit(x)) {
+    lo = ~lo + 1ull;
+    hi = ~hi + (lo == 0ull ? 1ull : 0ull);
+  }
+}
+
+template <int LC, bool A_CONTIG>
+__global__ void __launch_bounds__(RC_THREADS, 2)
+    residue_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
+                      ResidueOperand opA, ResidueOperand opB, int beta, uint32_t* status) {
+  using namespace sm100;
+  extern __shared__ uint8_t smem_raw[];
+  const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
+  uint8_t* sW = smem_raw + pad;    // weights: 128 rows x 128 bytes, swizzled
+  uint8_t* sE = sW + 128 * 128;    // entry bytes: 128 rows (p) x 8 slots (operand rows), swizzled
+  uint8_t* sIn = sE + 128 * 128;   // RC_STAGES x 1024 entries as loaded
+  uint8_t* sOut = sIn + RC_STAGES * RC_IN_BYTES;  // the tile's residue bytes, per modulus 8 rows x 128
+  __shared__ uint64_t full[RC_STAGES], mdone;
+  __shared__ uint32_t tmem_slot;
+  const int t = threadIdx.x, warp = t / 32, lane = t % 32;
+  auto swz = [](int row, int chunk) { return (row >> 3) * 1024 + (row & 7) * 128 + ((chunk ^ (row & 7)) << 4); };
+  // weight tile: row 32 g + l, 16-byte chunk g = w_l (modulus l < LC); zero elsewhere
+  for (int e = t; e < 128 * 8; e += RC_THREADS) *reinterpret_cast<uint4*>(sW + 16 * e) = make_uint4(0, 0, 0, 0);
+  __syncthreads();
+  if (t < 128 && t % 32 < LC) {
+    const int g = t / 32, l = t % 32;
+    const uint32_t m = (uint32_t)c_tab.mod[l];
+    uint32_t w[4] = {0, 0, 0, 0}, p = 1, p104 = 1;
+    for (int b = 0; b < 14; b++) {
+      w[b / 4] |= p << (8 * (b % 4));
+      p104 = p;
+      p = (p * 256u) % m;
+    }
+    const uint32_t c111 = (p104 * 128u) % m;  // 2^111 mod m
+    w[3] |= ((m - c111) % m) << 16;           // byte 14
+    *reinterpret_cast<uint4*>(sW + swz(t, g)) = make_uint4(w[0], w[1], w[2], w[3]);
+  }
+  if (t == 0) {
+    prefetch_tmap(&mapA);
+    prefetch_tmap(&mapB);
+    for (int s = 0; s < RC_STAGES; s++) mbar_init(&full[s], 1);
+    mbar_init(&mdone, 1);
+    fence_mbarrier_init();
+  }
+  if (warp == 0) {
+    tmem_alloc(&tmem_slot, 256);
+    tmem_relinquish();
+  }
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_slot;
+  // this thread's modulus in the epilogue
+  const int el = lane;
+  const uint32_t em = el < LC ? (uint32_t)c_tab.mod[el] : 1u;
+  const uint32_t emag = el < LC ? 0xFFFFFFFFu / em + 1u : 0u;  // ceil(2^32 / m)
+  griddep_launch_dependents();
+  griddep_wait();  // the exponents come from the preceding pass
+  // tiles: row tiles of A then of B (both with opA.p_tiles reduction tiles), reduction tile fastest
+  const int64_t P = opA.p_tiles, rowsA = opA.row_tiles, ntiles = (rowsA + opB.row_tiles) * P;
+  const int64_t cnt = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  TileWalk prod(blockIdx.x, gridDim.x, P), cons(blockIdx.x, gridDim.x, P);
+  RingPos pring, cring;
+  auto issue = [&]() {  // thread 0: entries of the next tile into the next stage
+    const bool isA = prod.r < rowsA;
+    const int rt = (int)(isA ? prod.r : prod.r - rowsA), pt = (int)prod.c;
+    uint8_t* dst = sIn + pring.st * RC_IN_BYTES;
+    mbar_arrive_expect_tx(&full[pring.st], (uint32_t)RC_IN_BYTES);
+    if (isA && A_CONTIG)
+      tma_load_2d(dst, &mapA, &full[pring.st], 2 * RC_P * pt, RC_ROWS * rt);
+    else
+      tma_load_2d(dst, isA ? &mapA : &mapB, &full[pring.st], 2 * RC_ROWS * rt, RC_P * pt);
+    prod.next();
+    pring.next<RC_STAGES>();
+  };
+  int64_t issued = 0;
+  if (t == 0)
+    for (; issued < cnt && issued < RC_STAGES; issued++) issue();
+  const uint32_t idesc = idesc_i8(128, 128, true);
+  bool ok = true;
+  int64_t mma_issued = 0, mma_seen = 0;
+  for (int64_t u = 0; u < cnt; u++) {
+    const bool isA = cons.r < rowsA;
+    const ResidueOperand& o = isA ? opA : opB;
+    const int64_t rt = isA ? cons.r : cons.r - rowsA, pt = cons.c;
+    cons.next();
+    const bool contig = isA && A_CONTIG;
+    int exs[4];  // the exponents of this thread's 4 entries' rows, loaded before the wait
+#pragma unroll
+    for (int i = 0; i < 4; i++) {
+      const int k = t + RC_THREADS * i;
+      exs[i] = o.exps[rt * RC_ROWS + (contig ? k / RC_P : k % RC_ROWS)];
+    }
+    const int st = cring.st;
+    if (!mbar_wait(&full[st], cring.ph, status, DEV_STATUS_TIMEOUT)) ok = false;
+    cring.next<RC_STAGES>();
+    if (ok) {
+      const double2* in = reinterpret_cast<const double2*>(sIn + st * RC_IN_BYTES);
+#pragma unroll
+      for (int i = 0; i < 4; i++) {
+        const int k = t + RC_THREADS * i;
+        const int j = contig ? k / RC_P : k % RC_ROWS, n = contig ? k % RC_P : k / RC_ROWS;
+        const double2 v = in[k];
+        const int ex = exs[i];
+        uint64_t w0 = 0, w1 = 1ull << 47;  // X' = X + 2^111 (X = 0 for a non-finite row)
+        if (ex != EXP_NONFINITE) {
+          const int s = beta + 1022 - ex;
+          uint64_t hl, hh, ll, lh;
+          int128_of(rint(scale_pow2(v.x, s)), hl, hh);
+          int128_of(rint(scale_pow2(v.y, s)), ll, lh);
+          w0 = hl + ll;
+          w1 = hh + lh + (w0 < hl ? 1ull : 0ull) + (1ull << 47);
+        }
+        *reinterpret_cast<uint4*>(sE + swz(n, j)) =
+            make_uint4((uint32_t)w0, (uint32_t)(w0 >> 32), (uint32_t)w1, (uint32_t)((w1 >> 32) & 0xFFFFu) | 0x10000u);
+      }
+    }
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    tc_fence_before();
+    ok = __syncthreads_and(ok) != 0;  // entry tile written; the previous tile's TMEM read out
+    tc_fence_after();
+    if (!ok) break;
+    if (t == 0) {
+      const uint32_t wa = smem_u32(sW), ea = smem_u32(sE);
+#pragma unroll
+      for (int a = 0; a < 2; a++)
+#pragma unroll
+        for (int c = 0; c < 2; c++)
+          mma_i8(tmem + (uint32_t)a * 128u, desc_k_sw128(wa + 32 * c), desc_k_sw128(ea + 32 * (2 * a + c)), idesc,
+                 (uint32_t)c);
+      mma_commit(&mdone);
+      mma_issued++;
+      if (issued < cnt) {  // refill the stage just read
+        issue();
+        issued++;
+      }
+    }
+    bool got = mbar_wait(&mdone, (uint32_t)(u & 1), status, DEV_STATUS_TIMEOUT);
+    if (!__syncthreads_and(got)) {
+      ok = false;
+      break;
+    }
+    mma_seen = u + 1;
+    tc_fence_after();
+    // epilogue: lane quarter g of accumulator a = operand row 4 a + g of the
+    // tile; the bytes are staged so that the global stores run along rows
+    const int g = warp % 4, a = warp / 4;
+    uint8_t* so = sOut + el * RC_OUT_PLANE + (4 * a + g) * RC_P;
+#pragma unroll
+    for (int c2 = 0; c2 < 4; c2 += 2) {
+      uint32_t v[2][32];
+      const uint32_t col = tmem + (uint32_t)a * 128u + 32u * c2 + ((uint32_t)(32 * g) << 16);
+      tmem_ld_32x32b_x32(col, v[0]);
+      tmem_ld_32x32b_x32(col + 32u, v[1]);
+      tmem_wait_ld();
+      if (el < LC) {
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          uint32_t wds[8];
+#pragma unroll
+          for (int q = 0; q < 8; q++) {
+            uint32_t r[4];
+#pragma unroll
+            for (int e = 0; e < 4; e++) r[e] = v[h][4 * q + e] - __umulhi(v[h][4 * q + e], emag) * em;
+            wds[q] = __byte_perm(__byte_perm(r[0], r[1], 0x0040), __byte_perm(r[2], r[3], 0x0040), 0x5410);
+          }
+          uint8_t* d = so + 32 * (c2 + h);
+          *reinterpret_cast<uint4*>(d) = make_uint4(wds[0], wds[1], wds[2], wds[3]);
+          *reinterpret_cast<uint4*>(d + 16) = make_uint4(wds[4], wds[5], wds[6], wds[7]);
+        }
+      }
+    }
+    tc_fence_before();
+    __syncthreads();  // the tile's bytes staged (and its TMEM read out)
+    // full 128-byte rows of every plane, 8 threads per row
+    int8_t* ob = o.out + (size_t)(rt * RC_ROWS) * o.ld + (size_t)pt * RC_P;
+#pragma unroll 2
+    for (int e = t; e < LC * RC_ROWS * 8; e += RC_THREADS) {
+      const int l = e >> 6, j = (e >> 3) & 7, c = e & 7;
+      const uint4 val = *reinterpret_cast<const uint4*>(sOut + l * RC_OUT_PLANE + j * RC_P + 16 * c);
+      *reinterpret_cast<uint4*>(ob + (size_t)l * o.plane + (size_t)j * o.ld + 16 * c) = val;
+    }
+  }
+  if (!ok && t == 0) {
+    // a wait gave up: let the copies and the MMAs still in flight land (bounded) before the buffers go
+    for (int64_t u = mma_issued; u < issued; u++)
+      mbar_wait(&full[(int)(u % RC_STAGES)], (uint32_t)((u / RC_STAGES) & 1), status, DEV_STATUS_TIMEOUT,
+                100000000ull);
+    if (mma_issued > mma_seen)
+      mbar_wait(&mdone, (uint32_t)((mma_issued - 1) & 1), status, DEV_STATUS_TIMEOUT, 100000000ull);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    tmem_dealloc(tmem, 256);
+  }
+}
+
+// ---------------------------------------------------------------------------
 // tcgen05 int8 GEMM, one modulus per output tile:
 //   cres[l][i][j] = (sum_p Ares[l][i][p] * Bres[l][j][p]) mod m_l   (uint8)
 // Persistent, warp-specialised: warp 0 = TMA producer, warp 1 = MMA issuer,
@@ -1127,42 +1393,87 @@ __global__ void __launch_bounds__(256) crt_dd_kernel(const uint8_t* __restrict__
 // CRT on the tensor core (the f128 GEMM, L = 28..32 moduli). For an entry
 // with product residues r_l, the CRT value V = sum_l r_l W_l is split by the
 // bytes of the weights: V = sum_q 2^(8q) S_q with S_q = sum_l r_l w_lq, an
-// exact u8 x u8 dot product (< 30 * 255^2 < 2^21). A CTA takes 128
-// consecutive entries of a row, transposes their residues into a 128 x 32
-// byte tile (128-byte swizzled rows) and multiplies it by the 32 x 32 byte
-// matrix of the weights with one M = 128, N = 32, K = 32 tcgen05 MMA; each
-// thread then reads its entry's 32 sums from TMEM and finishes in integer
+// exact u8 x u8 dot product (< 30 * 255^2 < 2^21). A persistent CTA walks
+// tiles of 256 consecutive entries of a row: TMA brings each tile's residue
+// rows (one 256-byte row per modulus) into a 4-stage ring, the CTA
+// transposes them into two 128 x 32 byte K-major tiles (32-byte swizzle) and
+// multiplies each by the 32 x 32 byte matrix of the weights with one M = 128,
+// N = 32, K = 32 tcgen05 MMA. Each thread then finishes two entries (ILP
+// for the serial parts) from the 32 sums it reads from TMEM, in integer
 // arithmetic: 16-bit limbs U_h = S_2h + 2^8 S_2h+1, the quotient q =
-// round(V / M) from the top limbs (|V - q M| <= M/4 leaves a wide margin
-// for the estimate), C = V - q M limb by limb with balanced carries, and the
-// exact limbs summed from the top into a double-double. Integer and tensor
-// work replace the FP64 pipe's 30 x 6 weighted multiply-adds per entry.
+// round(V / M) from the top limbs (|V - q M| <= M/4 leaves a wide margin for
+// the estimate), the digits d_h = U_h - q M_h, their exact 48-bit chunks
+// with balanced carries, and the chunks summed from the top into a
+// double-double. The MMA of a tile runs while the previous tile is finished.
 // ---------------------------------------------------------------------------
-constexpr int CT_THREADS = 128, CT_SMEM = 1024 + 128 * 128 + 32 * 128;
+constexpr int CT_THREADS = 128, CT_STAGES = 4, CT_TILE = 256;
+constexpr int CT_SMEM = 1024 + 2 * 128 * 32 + 32 * 32 + CT_STAGES * 32 * CT_TILE;
+
+// byte offset of (row, logical byte k < 32) in a K-major tile of 32-byte rows, 32-byte swizzle
+__device__ __forceinline__ int swz32(int row, int k) {
+  return (row >> 3) * 256 + (row & 7) * 32 + ((((k >> 4) ^ (row >> 2)) & 1) << 4) + (k & 15);
+}
+
+// the f128 value of one entry from its 32 weight-byte sums
+__device__ __forceinline__ double2 crt_tc_entry(const uint32_t (&acc)[32], const CrtTcTable& T, int shift) {
+  int32_t U[16];
+#pragma unroll
+  for (int h = 0; h < 16; h++) U[h] = (int32_t)(acc[2 * h] + (acc[2 * h + 1] << 8));
+  // q = round(V / M) from the top limbs (the rest moves V / M by < 2^-29)
+  const double vt = __dadd_rn(__dadd_rn(__dmul_rn((double)U[15], 0x1p48), __dmul_rn((double)U[14], 0x1p32)),
+                              __dadd_rn(__dmul_rn((double)U[13], 0x1p16), (double)U[12]));
+  const int32_t q = (int32_t)rint(__dmul_rn(vt, T.k192));
+  // C = V - q M = sum_h d_h 2^(16 h), |d_h| < 2^31
+  int32_t d[18];
+#pragma unroll
+  for (int h = 0; h < 16; h++) d[h] = U[h] - q * T.mlimb[h];
+  d[16] = d[17] = 0;
+  // balanced 48-bit chunks b_k (|b_k| <= 2^47), C = sum_k b_k 2^(48 k)
+  double v[6];
+  int64_t carry = 0;
+#pragma unroll
+  for (int k = 0; k < 6; k++) {
+    const int64_t c = (int64_t)d[3 * k] + (int64_t)d[3 * k + 1] * 65536 + (int64_t)d[3 * k + 2] * 4294967296ll + carry;
+    carry = k < 5 ? (c + (1ll << 47)) >> 48 : 0;
+    v[k] = scale_pow2((double)(c - carry * 281474976710656ll), 48 * k);  // exact
+  }
+  // from the top: a nonzero partial sum is a multiple of 2^(48 (k+1)) and
+  // |b_k 2^(48 k)| < 2^(48 k + 48), so the quick two-sums are exact
+  dd s = dd{v[5], 0.0};
+#pragma unroll
+  for (int k = 4; k >= 0; k--) {
+    double hs, he;
+    quick_two_sum(s.hi, v[k], hs, he);
+    s = dd_renorm(hs, __dadd_rn(he, s.lo));
+  }
+  const dd o = dd_renorm(scale_pow2(s.hi, shift), scale_pow2(s.lo, shift));
+  return make_double2(o.hi, o.lo);
+}
 
 template <int LC>
 __global__ void __launch_bounds__(CT_THREADS, 4)
-    crt_tc_kernel(const uint8_t* __restrict__ cres, int64_t plane, int64_t Np, int64_t m, int64_t n,
-                  const int* __restrict__ expA, const int* __restrict__ expB, int beta, double2* __restrict__ C,
-                  uint32_t* status) {
+    crt_tc_kernel(const __grid_constant__ CUtensorMap map, int64_t m, int64_t n, const int* __restrict__ expA,
+                  const int* __restrict__ expB, int beta, double2* __restrict__ C, uint32_t* status) {
   using namespace sm100;
   extern __shared__ uint8_t smem_raw[];
   const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
-  uint8_t* sA = smem_raw + pad;   // 128 rows (entries) x 128 bytes, swizzled
-  uint8_t* sB = sA + 128 * 128;   // 32 rows (weight bytes q) x 128 bytes, swizzled
-  __shared__ uint64_t bar;
+  uint8_t* sA = smem_raw + pad;  // 2 x (128 rows (entries) x 32 bytes (moduli)), swizzled
+  uint8_t* sB = sA + 2 * 128 * 32;   // 32 rows (weight bytes q) x 32 bytes (moduli), swizzled
+  uint8_t* sR = sB + 32 * 32;        // CT_STAGES x (LC planes x 256 residues), as loaded
+  __shared__ uint64_t full[CT_STAGES], mdone[2];
   __shared__ uint32_t tmem_slot;
   const CrtTcTable& T = c_crt_tc[LC - CRT_CONST_L0];
   const int t = threadIdx.x, warp = t / 32, lane = t % 32;
-  // swizzled byte address of (row, logical byte k) in a 128-byte-row tile
-  auto swz = [](int row, int k) { return (row >> 3) * 1024 + (row & 7) * 128 + (((k >> 4) ^ (row & 7)) << 4) + (k & 15); };
-  for (int e = t; e < 32 * 32; e += CT_THREADS) sB[swz(e / 32, e % 32)] = T.wb[e / 32][e % 32];
+  for (int e = t; e < 32 * 32; e += CT_THREADS) sB[swz32(e / 32, e % 32)] = T.wb[e / 32][e % 32];
   if (t == 0) {
-    mbar_init(&bar, 1);
+    prefetch_tmap(&map);
+    for (int s = 0; s < CT_STAGES; s++) mbar_init(&full[s], 1);
+    mbar_init(&mdone[0], 1);
+    mbar_init(&mdone[1], 1);
     fence_mbarrier_init();
   }
   if (warp == 0) {
-    tmem_alloc(&tmem_slot, 32);
+    tmem_alloc(&tmem_slot, 128);
     tmem_relinquish();
   }
   asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -1172,91 +1483,125 @@ __global__ void __launch_bounds__(CT_THREADS, 4)
   const uint32_t tmem = tmem_slot;
   griddep_launch_dependents();
   griddep_wait();  // the product residues come from the preceding GEMM
-  const int64_t tpr = (n + 127) / 128, ntiles = m * tpr;
+  const int64_t tpr = (n + CT_TILE - 1) / CT_TILE, ntiles = m * tpr;
+  const int64_t cnt = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;  // this CTA's tiles
+  constexpr uint32_t TILE_BYTES = (uint32_t)CT_TILE * LC;
+  TileWalk prod(blockIdx.x, gridDim.x, tpr), cons(blockIdx.x, gridDim.x, tpr);
+  RingPos pring, cring;
+  auto issue = [&]() {  // thread 0: residues of the next tile into the next stage
+    mbar_arrive_expect_tx(&full[pring.st], TILE_BYTES);
+    tma_load_3d(sR + pring.st * 32 * CT_TILE, &map, &full[pring.st], (int)(prod.c * CT_TILE), (int)prod.r, 0);
+    prod.next();
+    pring.next<CT_STAGES>();
+  };
+  int64_t issued = 0;
+  if (t == 0)
+    for (; issued < cnt && issued < CT_STAGES; issued++) issue();
   const uint32_t idesc = idesc_i8(128, 32, true);
-  uint32_t phase = 0;
   bool ok = true;
-  for (int64_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-    const int64_t i = tile / tpr, j0 = (tile % tpr) * 128;
-    // residues: warp w loads moduli 8w .. 8w+7, lane the 4 entries 4 lane .. 4 lane + 3
-    uint32_t wv[8];
-    const uint8_t* rp = cres + (size_t)i * Np + j0 + 4 * lane;
-#pragma unroll
-    for (int u = 0; u < 8; u++) {
-      const int l = 8 * warp + u;
-      wv[u] = l < LC ? __ldg(reinterpret_cast<const uint32_t*>(rp + (size_t)l * plane)) : 0u;
+  int64_t mma_issued = 0, mma_seen = 0;  // thread 0's count of MMAs issued; every thread's count of MMAs awaited
+  int shift_prev[2] = {0, 0};            // the previous tile's scale shifts (or the non-finite marker)
+  int64_t i_prev = 0, j0_prev = 0;       // the previous tile's row and first column
+  // Iteration u waits for tile u - 1's MMAs, stages tile u, issues its MMAs
+  // and finishes tile u - 1 while they run.
+  for (int64_t u = 0; u <= cnt; u++) {
+    if (u >= 1) {
+      const int64_t v1 = u - 1;
+      if (!mbar_wait(&mdone[v1 & 1], (uint32_t)((v1 >> 1) & 1), status, DEV_STATUS_TIMEOUT)) ok = false;
+      else mma_seen = u;
     }
-    // transpose to entry-major: entry e's bytes of moduli 8w .. 8w+7 -> row 4 lane + e, bytes 8w .. 8w+7
+    int shift_cur[2] = {0, 0};
+    const int64_t i_cur = cons.r, j0_cur = cons.c * CT_TILE;
+    if (u < cnt) {
+      const int ea = expA[i_cur];
 #pragma unroll
-    for (int e = 0; e < 4; e++) {
-      const uint32_t sel = (uint32_t)e | ((uint32_t)(e + 4) << 4);
-      const uint32_t lo = __byte_perm(__byte_perm(wv[0], wv[1], sel), __byte_perm(wv[2], wv[3], sel), 0x5410);
-      const uint32_t hi = __byte_perm(__byte_perm(wv[4], wv[5], sel), __byte_perm(wv[6], wv[7], sel), 0x5410);
-      *reinterpret_cast<uint2*>(sA + swz(4 * lane + e, 8 * warp)) = make_uint2(lo, hi);
+      for (int h = 0; h < 2; h++) {
+        const int64_t j = j0_cur + 128 * h + t;
+        const int eb = j < n ? expB[j] : 0;
+        shift_cur[h] = (ea == EXP_NONFINITE || eb == EXP_NONFINITE)
+                           ? INT32_MIN
+                           : -((beta + 1022 - ea) + (beta + 1022 - eb));
+      }
+      const int st = cring.st;
+      if (ok && !mbar_wait(&full[st], cring.ph, status, DEV_STATUS_TIMEOUT)) ok = false;
+      cring.next<CT_STAGES>();
+      cons.next();
+      if (ok) {
+        // warp w takes moduli 8w .. 8w+7, lane the entries 4 lane .. 4 lane + 3 of each half
+#pragma unroll
+        for (int h = 0; h < 2; h++) {
+          const uint8_t* r = sR + st * 32 * CT_TILE + 128 * h + 4 * lane;
+          uint32_t wv[8];
+#pragma unroll
+          for (int v = 0; v < 8; v++) {
+            const int l = 8 * warp + v;
+            wv[v] = l < LC ? *reinterpret_cast<const uint32_t*>(r + l * CT_TILE) : 0u;
+          }
+          // entry e's bytes of moduli 8w .. 8w+7 -> row 4 lane + e, bytes 8w .. 8w+7
+          uint8_t* a = sA + h * 128 * 32;
+#pragma unroll
+          for (int e = 0; e < 4; e++) {
+            const uint32_t sel = (uint32_t)e | ((uint32_t)(e + 4) << 4);
+            const uint32_t lo = __byte_perm(__byte_perm(wv[0], wv[1], sel), __byte_perm(wv[2], wv[3], sel), 0x5410);
+            const uint32_t hi = __byte_perm(__byte_perm(wv[4], wv[5], sel), __byte_perm(wv[6], wv[7], sel), 0x5410);
+            *reinterpret_cast<uint2*>(a + swz32(4 * lane + e, 8 * warp)) = make_uint2(lo, hi);
+          }
+        }
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     tc_fence_before();
-    __syncthreads();  // tile written; the previous tile's TMEM reads are done
+    // tile u staged and its residues read; tile u - 2's TMEM columns read out
+    ok = __syncthreads_and(ok) != 0;
     tc_fence_after();
-    if (t == 0) {
-      mma_i8(tmem, desc_k_sw128(smem_u32(sA)), desc_k_sw128(smem_u32(sB)), idesc, 0u);
-      mma_commit(&bar);
+    if (!ok) break;
+    if (u < cnt && t == 0) {
+      const uint32_t d = tmem + (uint32_t)(u & 1) * 64u;
+      mma_i8(d, desc_k_sw32(smem_u32(sA)), desc_k_sw32(smem_u32(sB)), idesc, 0u);
+      mma_i8(d + 32u, desc_k_sw32(smem_u32(sA + 128 * 32)), desc_k_sw32(smem_u32(sB)), idesc, 0u);
+      mma_commit(&mdone[u & 1]);
+      mma_issued++;
+      if (issued < cnt) {  // refill the stage just read
+        issue();
+        issued++;
+      }
     }
-    ok = mbar_wait(&bar, phase, status, DEV_STATUS_TIMEOUT);
-    phase ^= 1;
-    if (!__all_sync(0xffffffffu, ok)) {
-      ok = false;
-      break;
+    if (u >= 1) {
+      // finish tile u - 1 (its MMAs were awaited above)
+      const int64_t v1 = u - 1;
+      const int64_t i = i_prev, j0 = j0_prev;
+      uint32_t acc0[32], acc1[32];
+      const uint32_t col = tmem + (uint32_t)(v1 & 1) * 64u + ((uint32_t)(warp * 32) << 16);
+      tmem_ld_32x32b_x32(col, acc0);
+      tmem_ld_32x32b_x32(col + 32u, acc1);
+      tmem_wait_ld();
+      const double2 nan2 = make_double2(__longlong_as_double(0x7ff8000000000000ll), 0.0);
+      const int64_t ja = j0 + t, jb = j0 + 128 + t;
+      const double2 ra = shift_prev[0] == INT32_MIN ? nan2 : crt_tc_entry(acc0, T, shift_prev[0]);
+      const double2 rb = shift_prev[1] == INT32_MIN ? nan2 : crt_tc_entry(acc1, T, shift_prev[1]);
+      if (ja < n) C[i * n + ja] = ra;
+      if (jb < n) C[i * n + jb] = rb;
     }
-    tc_fence_after();
-    uint32_t v[32];
-    tmem_ld_32x32b_x32(tmem + ((uint32_t)(warp * 32) << 16), v);
-    tmem_wait_ld();
-    const int64_t j = j0 + t;
-    if (j >= n) continue;
-    const int ea = expA[i], eb = expB[j];
-    if (ea == EXP_NONFINITE || eb == EXP_NONFINITE) {
-      C[i * n + j] = make_double2(__longlong_as_double(0x7ff8000000000000ll), 0.0);
-      continue;
+    shift_prev[0] = shift_cur[0];
+    shift_prev[1] = shift_cur[1];
+    i_prev = i_cur;
+    j0_prev = j0_cur;
+  }
+  if (!ok && t == 0) {
+    // a wait gave up: let the copies and the MMAs still in flight land (bounded) before the buffers go
+    for (int64_t u = mma_issued; u < issued; u++)
+      mbar_wait(&full[(int)(u % CT_STAGES)], (uint32_t)((u / CT_STAGES) & 1), status, DEV_STATUS_TIMEOUT,
+                100000000ull);
+    if (mma_issued > mma_seen) {
+      const int64_t v1 = mma_issued - 1;
+      mbar_wait(&mdone[v1 & 1], (uint32_t)((v1 >> 1) & 1), status, DEV_STATUS_TIMEOUT, 100000000ull);
     }
-    int32_t U[16];
-#pragma unroll
-    for (int h = 0; h < 16; h++) U[h] = (int32_t)(v[2 * h] + (v[2 * h + 1] << 8));
-    // q = round(V / M) from the top limbs (the rest moves V / M by < 2^-29)
-    const double vt = __dadd_rn(__dadd_rn(__dmul_rn((double)U[15], 0x1p48), __dmul_rn((double)U[14], 0x1p32)),
-                                __dadd_rn(__dmul_rn((double)U[13], 0x1p16), (double)U[12]));
-    const int32_t q = (int32_t)rint(__dmul_rn(vt, T.k192));
-    // C = V - q M in balanced base-2^16 digits b_h in [-2^15, 2^15)
-    int32_t b[18];
-    int32_t carry = 0;
-#pragma unroll
-    for (int h = 0; h < 16; h++) {
-      const int32_t x = U[h] - q * T.mlimb[h] + carry;
-      carry = (x + 0x8000) >> 16;
-      b[h] = x - (carry << 16);
-    }
-    b[16] = carry;
-    b[17] = 0;
-    // exact 48-bit chunks, summed from the top into a double-double
-    dd sum = dd{0.0, 0.0};
-#pragma unroll
-    for (int k = 5; k >= 0; k--) {
-      const double ch = __dadd_rn(__dadd_rn((double)b[3 * k], __dmul_rn((double)b[3 * k + 1], 0x1p16)),
-                                  __dmul_rn((double)b[3 * k + 2], 0x1p32));
-      const double vk = scale_pow2(ch, 48 * k);
-      double hs, he;
-      two_sum(sum.hi, vk, hs, he);
-      sum = dd_renorm(hs, __dadd_rn(he, sum.lo));
-    }
-    const int shift = -((beta + 1022 - ea) + (beta + 1022 - eb));
-    const dd o = dd_renorm(scale_pow2(sum.hi, shift), scale_pow2(sum.lo, shift));
-    C[i * n + j] = make_double2(o.hi, o.lo);
   }
   tc_fence_before();
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    tmem_dealloc(tmem, 32);
+    tmem_dealloc(tmem, 128);
   }
 }
 
@@ -1333,20 +1678,129 @@ static int launch_crt_dd(const uint8_t* cres, size_t Mp, size_t Np, size_t m, si
 }
 
 // The tensor-core CRT for L = 28..32 (the counts k <= 2^20 needs at beta =
-// 106); HP_ERR_UNSUPPORTED for other L. Np must be a multiple of 128.
+// 106); HP_ERR_UNSUPPORTED for other L. Np must be a multiple of 256.
 static int launch_crt_tc(const uint8_t* cres, size_t Mp, size_t Np, size_t m, size_t n, const int* expA,
                          const int* expB, int beta, int L, double2* C, int num_sms, uint32_t* status, cudaStream_t s,
                          bool pdl) {
+  if (L < CRT_CONST_L0 || L >= CRT_CONST_L0 + CRT_CONST_N || Np % CT_TILE != 0) {
+    set_error("ozaki: no tensor-core CRT for %d moduli", L);
+    return HP_ERR_UNSUPPORTED;
+  }
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63]) {
+    HP_CUDA_TRY(cudaFuncSetAttribute(crt_tc_kernel<28>, cudaFuncAttributeMaxDynamicSharedMemorySize, CT_SMEM));
+    HP_CUDA_TRY(cudaFuncSetAttribute(crt_tc_kernel<29>, cudaFuncAttributeMaxDynamicSharedMemorySize, CT_SMEM));
+    HP_CUDA_TRY(cudaFuncSetAttribute(crt_tc_kernel<30>, cudaFuncAttributeMaxDynamicSharedMemorySize, CT_SMEM));
+    HP_CUDA_TRY(cudaFuncSetAttribute(crt_tc_kernel<31>, cudaFuncAttributeMaxDynamicSharedMemorySize, CT_SMEM));
+    HP_CUDA_TRY(cudaFuncSetAttribute(crt_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, CT_SMEM));
+    attr_set[dev & 63] = true;
+  }
+  // product residue planes L x Mp x Np bytes; one box is 256 residues of one row in every plane
+  auto fn = encode_fn();
+  if (!fn) {
+    set_error("cuTensorMapEncodeTiled unavailable");
+    return HP_ERR_CUDA;
+  }
+  CUtensorMap map;
+  cuuint64_t dims[3] = {Np, Mp, (cuuint64_t)L};
+  cuuint64_t strides[2] = {Np, Np * Mp};
+  cuuint32_t box[3] = {(cuuint32_t)CT_TILE, 1, (cuuint32_t)L};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult rc = fn(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t*>(cres), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (rc != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (%d)", (int)rc);
+    return HP_ERR_CUDA;
+  }
   const int grid = num_sms * 4;
-#define HP_CRT_TC(LCV)                                                                                         \
-  if (L == LCV) {                                                                                              \
-    HP_CUDA_TRY(launch_k(pdl, crt_tc_kernel<LCV>, dim3(grid), dim3(CT_THREADS), CT_SMEM, s, cres,              \
-                         (int64_t)(Mp * Np), (int64_t)Np, (int64_t)m, (int64_t)n, expA, expB, beta, C, status)); \
-    return HP_OK;                                                                                              \
+#define HP_CRT_TC(LCV)                                                                                        \
+  if (L == LCV) {                                                                                             \
+    HP_CUDA_TRY(launch_k(pdl, crt_tc_kernel<LCV>, dim3(grid), dim3(CT_THREADS), CT_SMEM, s, map, (int64_t)m,  \
+                         (int64_t)n, expA, expB, beta, C, status));                                           \
+    return HP_OK;                                                                                             \
   }
   HP_CRT_TC(28) HP_CRT_TC(29) HP_CRT_TC(30) HP_CRT_TC(31) HP_CRT_TC(32)
 #undef HP_CRT_TC
-  set_error("ozaki: no tensor-core CRT for %d moduli", L);
+  return HP_ERR_UNSUPPORTED;
+}
+
+// Residue planes of the f128 GEMM's operands on the tensor core (unsigned
+// bytes, L = 28..32): A is m x k (k x m when atb), B is k x n, both f128
+// row-major; either may be null (its planes are not written). Writes the
+// same bytes as residue_tile<..., U8 = true> over Mp x Kp and Np x Kp.
+// HP_ERR_UNSUPPORTED (nothing launched) for other L or an operand not
+// 16-byte aligned.
+static int launch_residues_tc(bool atb, int L, const double2* A, size_t m, const int* expA, int8_t* outA, size_t Mp,
+                              const double2* B, size_t n, const int* expB, int8_t* outB, size_t Np, size_t k,
+                              size_t Kp, int beta, int num_sms, uint32_t* status, cudaStream_t s, bool pdl) {
+  if (L < CRT_CONST_L0 || L >= CRT_CONST_L0 + CRT_CONST_N || (!A && !B) ||
+      ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 15u) || Mp % RC_ROWS || Np % RC_ROWS ||
+      Kp % RC_P)
+    return HP_ERR_UNSUPPORTED;
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63]) {
+#define HP_RC_ATTR(LCV)                                                                                           \
+  HP_CUDA_TRY(cudaFuncSetAttribute(residue_tc_kernel<LCV, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,     \
+                                   RC_SMEM));                                                                     \
+  HP_CUDA_TRY(cudaFuncSetAttribute(residue_tc_kernel<LCV, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, RC_SMEM));
+    HP_RC_ATTR(28) HP_RC_ATTR(29) HP_RC_ATTR(30) HP_RC_ATTR(31) HP_RC_ATTR(32)
+#undef HP_RC_ATTR
+    attr_set[dev & 63] = true;
+  }
+  auto fn = encode_fn();
+  if (!fn) {
+    set_error("cuTensorMapEncodeTiled unavailable");
+    return HP_ERR_CUDA;
+  }
+  // f64 view of a row-major f128 matrix of `rows` rows and `cols` entries; a box is
+  // box_e entries x box_r rows (the entries of 8 operand rows, or 128 reduction indices)
+  auto map2d = [&](CUtensorMap* map, const double2* base, size_t rows, size_t cols, uint32_t box_e,
+                   uint32_t box_r) -> int {
+    cuuint64_t dims[2] = {2 * cols, rows};
+    cuuint64_t strides[1] = {2 * cols * sizeof(double)};
+    cuuint32_t box[2] = {2 * box_e, box_r};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult rc = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 2, const_cast<double2*>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (rc != CUDA_SUCCESS) {
+      set_error("cuTensorMapEncodeTiled failed (%d)", (int)rc);
+      return HP_ERR_CUDA;
+    }
+    return HP_OK;
+  };
+  CUtensorMap mapA, mapB;
+  ResidueOperand oa{outA, (int64_t)(Mp * Kp), (int64_t)Kp, expA, A ? (int64_t)(Mp / RC_ROWS) : 0,
+                    (int64_t)(Kp / RC_P)};
+  ResidueOperand ob{outB, (int64_t)(Np * Kp), (int64_t)Kp, expB, B ? (int64_t)(Np / RC_ROWS) : 0,
+                    (int64_t)(Kp / RC_P)};
+  if (B) HP_TRY(map2d(&mapB, B, k, n, RC_ROWS, RC_P));
+  if (A) {
+    if (atb)
+      HP_TRY(map2d(&mapA, A, k, m, RC_ROWS, RC_P));  // A is k x m: 8 operand rows x 128 reduction indices
+    else
+      HP_TRY(map2d(&mapA, A, m, k, RC_P, RC_ROWS));  // A is m x k: 128 reduction indices x 8 rows
+  }
+  if (!A) mapA = mapB;  // not read (no A tiles)
+  if (!B) mapB = mapA;
+  const int grid = num_sms * 2;
+#define HP_RC(LCV)                                                                                                \
+  if (L == LCV) {                                                                                                 \
+    if (atb)                                                                                                      \
+      HP_CUDA_TRY(launch_k(pdl, residue_tc_kernel<LCV, false>, dim3(grid), dim3(RC_THREADS), RC_SMEM, s, mapA,     \
+                           mapB, oa, ob, beta, status));                                                          \
+    else                                                                                                          \
+      HP_CUDA_TRY(launch_k(pdl, residue_tc_kernel<LCV, true>, dim3(grid), dim3(RC_THREADS), RC_SMEM, s, mapA, mapB, \
+                           oa, ob, beta, status));                                                                \
+    return HP_OK;                                                                                                 \
+  }
+  HP_RC(28) HP_RC(29) HP_RC(30) HP_RC(31) HP_RC(32)
+#undef HP_RC
   return HP_ERR_UNSUPPORTED;
 }
 
@@ -1553,13 +2007,22 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
   // 1. exponents
   HP_TRY(launch_maxexp(A2, B2, m, n, k, atb, expA, expB, s));
   profile_mark(s, "exponents");
-  // 2. residues (their loads of A and B overlap the exponent pass's tail)
-  {
+  // 2. residues (on the tensor core for the usual moduli counts)
+  uint32_t* status = device_status(s);
+  if (!status) {
+    set_error("status word allocation failed");
+    return HP_ERR_CUDA;
+  }
+  const int rc = launch_residues_tc(atb, L, A2, m, expA, ares.as<int8_t>(), Mp, B2, n, expB, bres.as<int8_t>(), Np,
+                                    k, Kp, beta, D->num_sms, status, s, pdl);
+  if (rc == HP_ERR_UNSUPPORTED) {
     const unsigned tay = (unsigned)(Mp / RT_R);
     dim3 g((unsigned)(Kp / (4 * RES_EPR)), tay + (unsigned)(Np / RT_R));
     HP_CUDA_TRY(launch_residues_ab(atb, L, pdl, g, s, A2, (int64_t)m, (const int*)expA, ares.as<int8_t>(),
                                    (int64_t)(Mp * Kp), tay, B2, (int64_t)n, (const int*)expB, bres.as<int8_t>(),
                                    (int64_t)(Np * Kp), (int64_t)k, beta, (int64_t)Kp));
+  } else if (rc != HP_OK) {
+    return rc;
   }
   profile_mark(s, "residues");
   // 3. one int8 GEMM per modulus, on CTA pairs
@@ -1567,11 +2030,6 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
   profile_mark(s, "i8_gemm");
   // 4. CRT (on the tensor core for the usual moduli counts)
   if (L >= CRT_CONST_L0 && L < CRT_CONST_L0 + CRT_CONST_N) {
-    uint32_t* status = device_status(s);
-    if (!status) {
-      set_error("status word allocation failed");
-      return HP_ERR_CUDA;
-    }
     HP_TRY(launch_crt_tc(cres.as<uint8_t>(), Mp, Np, m, n, expA, expB, beta, L, reinterpret_cast<double2*>(c),
                          D->num_sms, status, s, pdl));
   } else {
@@ -1675,9 +2133,19 @@ int ozaki_dd_gemm_host(const double* a, const double* b, double* c, size_t m, si
   HP_CUDA_TRY(cudaMemsetAsync(expB, 0, Np * sizeof(int), s));
   const double2* B2 = dB.as<const double2>();
   HP_TRY(launch_maxexp((const double2*)nullptr, B2, 0, n, k, false, nullptr, expB, s));
-  HP_CUDA_TRY(launch_residues_ab(false, L, pdl, dim3((unsigned)(Kp / (4 * RES_EPR)), (unsigned)(Np / RT_R)), s,
-                                 nullptr, 0, nullptr, nullptr, 0, 0, B2, (int64_t)n, expB, bres.as<int8_t>(),
-                                 (int64_t)(Np * Kp), (int64_t)k, beta, (int64_t)Kp));
+  uint32_t* status = device_status(s);
+  if (!status) {
+    set_error("status word allocation failed");
+    return HP_ERR_CUDA;
+  }
+  int rc = launch_residues_tc(false, L, nullptr, 0, nullptr, nullptr, 0, B2, n, expB, bres.as<int8_t>(), Np, k, Kp,
+                              beta, D->num_sms, status, s, pdl);
+  if (rc == HP_ERR_UNSUPPORTED)
+    HP_CUDA_TRY(launch_residues_ab(false, L, pdl, dim3((unsigned)(Kp / (4 * RES_EPR)), (unsigned)(Np / RT_R)), s,
+                                   nullptr, 0, nullptr, nullptr, 0, 0, B2, (int64_t)n, expB, bres.as<int8_t>(),
+                                   (int64_t)(Np * Kp), (int64_t)k, beta, (int64_t)Kp));
+  else if (rc != HP_OK)
+    return rc;
   const int nc = host_tables().crt[L].nc;
   for (size_t i = 0; i < np; i++) {
     const size_t r0 = i * pr, mi = std::min(pr, m - r0), Mpi = round_up(mi, GP_M);
@@ -1685,15 +2153,21 @@ int ozaki_dd_gemm_host(const double* a, const double* b, double* c, size_t m, si
     double* Ci = dC.as<double>() + r0 * n * 2;
     HP_CUDA_TRY(cudaStreamWaitEvent(s, eA[i], 0));
     HP_TRY(launch_maxexp(A2, (const double2*)nullptr, mi, 0, k, false, expA, nullptr, s));
-    const unsigned tay = (unsigned)(Mpi / RT_R);
-    HP_CUDA_TRY(launch_residues_ab(false, L, pdl, dim3((unsigned)(Kp / (4 * RES_EPR)), tay), s, A2, (int64_t)mi,
-                                   expA, ares.as<int8_t>(), (int64_t)(Mpi * Kp), tay, nullptr, 0, nullptr, nullptr,
-                                   0, (int64_t)k, beta, (int64_t)Kp));
+    rc = launch_residues_tc(false, L, A2, mi, expA, ares.as<int8_t>(), Mpi, nullptr, 0, nullptr, nullptr, 0, k, Kp,
+                            beta, D->num_sms, status, s, pdl);
+    if (rc == HP_ERR_UNSUPPORTED) {
+      const unsigned tay = (unsigned)(Mpi / RT_R);
+      HP_CUDA_TRY(launch_residues_ab(false, L, pdl, dim3((unsigned)(Kp / (4 * RES_EPR)), tay), s, A2, (int64_t)mi,
+                                     expA, ares.as<int8_t>(), (int64_t)(Mpi * Kp), tay, nullptr, 0, nullptr, nullptr,
+                                     0, (int64_t)k, beta, (int64_t)Kp));
+    } else if (rc != HP_OK) {
+      return rc;
+    }
     HP_TRY(ozaki_residue_gemm_pair(ares.as<int8_t>(), bres.as<int8_t>(), cres.as<uint8_t>(), L, Mpi, Np, Kp, s, pdl,
                                    true));
     if (L >= CRT_CONST_L0 && L < CRT_CONST_L0 + CRT_CONST_N)
       HP_TRY(launch_crt_tc(cres.as<uint8_t>(), Mpi, Np, mi, n, expA, expB, beta, L, reinterpret_cast<double2*>(Ci),
-                           D->num_sms, device_status(s), s, pdl));
+                           D->num_sms, status, s, pdl));
     else
       HP_TRY(launch_crt_dd(cres.as<uint8_t>(), Mpi, Np, mi, n, expA, expB, beta, D->crt + L, nc,
                            reinterpret_cast<double2*>(Ci), s, pdl, L));

@@ -76,6 +76,14 @@ __device__ __forceinline__ void tma_load_3d(void* dst, const CUtensorMap* map, u
       "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y), "r"(z)
       : "memory");
 }
+// TMA: 2-D tiled load into shared memory, completion counted on `bar`.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, uint64_t* bar, int x, int y) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];" ::"r"(
+          smem_u32(dst)),
+      "l"(map), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
+}
 __device__ __forceinline__ void prefetch_tmap(const CUtensorMap* map) {
   asm volatile("prefetch.tensormap [%0];" ::"l"(map) : "memory");
 }
@@ -204,6 +212,13 @@ __device__ __forceinline__ void mma_commit_pair(uint64_t* bar, uint16_t cta_mask
 __device__ __forceinline__ uint64_t desc_k_sw128(uint32_t smem_addr) {
   return (uint64_t)((smem_addr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
          (2ull << 61);
+}
+// The same for a K-major tile of 32-byte rows with 32-byte swizzle (one
+// K = 32 step of an 8-bit MMA): 8-row groups 256 bytes apart, layout 6. In
+// such a tile the 16-byte half c of row r sits at half c ^ ((r >> 2) & 1).
+__device__ __forceinline__ uint64_t desc_k_sw32(uint32_t smem_addr) {
+  return (uint64_t)((smem_addr >> 4) & 0x3FFFu) | (1ull << 16) | ((uint64_t)(256 >> 4) << 32) | (1ull << 46) |
+         (6ull << 61);
 }
 // Instruction descriptor, kind::i8: D = s32 (bits 4-5 = 2), A and B signed
 // 8-bit (bits 7-9 = 1, 10-12 = 1) or unsigned (0), both K-major, N>>3 at
