@@ -30,11 +30,11 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 M = N = K = 2048
-# DRAM bytes (read + write) of one i8_gemm_mod_kernel<256> launch at this size,
+# DRAM bytes (read + write) of one i8_gemm_pair_kernel launch at this size,
 # from an ncu capture of `bench.py --profile-case gemm` (251.8 MB read: every
-# residue plane once; 99.1 MB written, the rest of the 125.8 MB of product
+# residue plane once; 100.3 MB written, the rest of the 125.8 MB of product
 # residues still in L2 when the kernel ends).
-I8_GEMM_TRAFFIC_BYTES = 350834176
+I8_GEMM_TRAFFIC_BYTES = 352043776
 METRIC = "f128 GEMM GFLOP/s; SPD solves/s at ≤1e-25 rel err: chosen vs plain, 1 B200"
 WORKLOAD = "f128 GEMM C=A*B, m=n=k=2048, full double-double entries (SplitMix64 seed 0)"
 
@@ -886,8 +886,8 @@ def main():
     res_bytes = 2 * (M * K * 16) + L * (M * K + N * K)
     crt_ms = phases.get("crt", float("nan"))
     crt_bytes = L * M * N + M * N * 16
-    roofline = {"bound": "tensor", "kernel": "i8_gemm_mod_kernel (tcgen05.mma kind::i8, one launch for all "
-                "30 moduli)", "achieved": i8_tops, "peak": i8_peak, "unit": "TOPS (int8)",
+    roofline = {"bound": "tensor", "kernel": "i8_gemm_pair_kernel (tcgen05.mma.cta_group::2 kind::i8 on CTA "
+                "pairs, M = 256, one launch for all 30 moduli)", "achieved": i8_tops, "peak": i8_peak, "unit": "TOPS (int8)",
                 "frac": i8_tops / i8_peak, "traffic": I8_GEMM_TRAFFIC_BYTES,
                 "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one launch at 2048^3",
                 "peak_source": ("measured in this run by hp_measure_peaks: tcgen05.mma kind::i8 (u8, M=128, "
