@@ -174,7 +174,7 @@ __global__ void __launch_bounds__(64) chol_panel_kernel(typename O::T* A, const 
 // Diagonal block: one CTA; per column j, one thread forms the pivot
 // (sqrt, recip), the rows below scale their entry of column j, and the
 // sums of the remaining lower triangle take their j-th product.
-constexpr int RL_THREADS = 256;
+constexpr int RL_THREADS = 512;
 template <class O>
 __global__ void __launch_bounds__(RL_THREADS) chol_diag_rl_kernel(typename O::T* A, const typename O::T* S, int64_t n,
                                                                   int64_t kb, int jb, typename O::T* invd,

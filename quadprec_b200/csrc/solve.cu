@@ -37,40 +37,42 @@ struct VOpsDD {
 
 namespace {
 
-constexpr int TS_THREADS = 1024;
-
-// One CTA; thread t owns rows t, t+1024, ... (RMAX of them). The entries of
-// L a step needs (its column below / row right of the diagonal, and the
-// next diagonal element) do not depend on y, so each step loads the next
-// step's while its own multiply-adds run: the per-step chain is the
-// owner's division, one barrier and one multiply-add.
-template <class O, int RMAX, bool UPPER_T>
-__global__ void __launch_bounds__(TS_THREADS) trsv_kernel(const typename O::T* __restrict__ L, typename O::T* y,
-                                                          int64_t n) {
+// One CTA of TH threads; thread t owns rows t, t + TH, ... (RMAX of them).
+// The entries of L a step needs (its column below / row right of the
+// diagonal, and the next diagonal element) do not depend on y, so each step
+// loads the next step's while its own multiply-adds run: the per-step chain
+// is the owner's division, one barrier and one multiply-add. TH is one row
+// per thread up to n = 1024 (no idle warps in each step's barrier). Measured
+// at n = 512: 128 threads with four rows each is slower (the multiply-adds of
+// a step are the larger cost), and so is a barrier-free hand-off through a
+// shared-memory counter (the spinning threads slow the owner).
+template <class O, int TH, int RMAX, bool UPPER_T>
+__global__ void __launch_bounds__(TH) trsv_kernel(const typename O::T* __restrict__ L, typename O::T* y,
+                                                  int64_t n) {
   using T = typename O::T;
   __shared__ T bc[2];
   const int t = threadIdx.x;
   T yr[RMAX], lv[RMAX];
   auto lval = [&](int64_t step, int r) {
     const int64_t j = UPPER_T ? n - 1 - step : step;
-    const int64_t i = t + (int64_t)TS_THREADS * r;
+    const int64_t i = t + (int64_t)TH * r;
     const bool active = step < n && (UPPER_T ? (i < j) : (i > j && i < n));
     return active ? (UPPER_T ? L[j * n + i] : L[i * n + j]) : O::zero();
   };
   auto ldiag = [&](int64_t step) {
     const int64_t j = UPPER_T ? n - 1 - step : step;
-    return (step < n && (int)(j % TS_THREADS) == t) ? L[j * n + j] : O::zero();
+    return (step < n && (int)(j % TH) == t) ? L[j * n + j] : O::zero();
   };
 #pragma unroll
   for (int r = 0; r < RMAX; r++) {
-    int64_t i = t + (int64_t)TS_THREADS * r;
+    int64_t i = t + (int64_t)TH * r;
     yr[r] = i < n ? y[i] : O::zero();
     lv[r] = lval(0, r);
   }
   T dg = ldiag(0);
   for (int64_t step = 0; step < n; step++) {
     const int64_t j = UPPER_T ? n - 1 - step : step;
-    const int owner = (int)(j % TS_THREADS), rj = (int)(j / TS_THREADS);
+    const int owner = (int)(j % TH), rj = (int)(j / TH);
     if (t == owner) {
 #pragma unroll
       for (int r = 0; r < RMAX; r++)
@@ -87,7 +89,7 @@ __global__ void __launch_bounds__(TS_THREADS) trsv_kernel(const typename O::T* _
     dg = ldiag(step + 1);
 #pragma unroll
     for (int r = 0; r < RMAX; r++) {
-      int64_t i = t + (int64_t)TS_THREADS * r;
+      int64_t i = t + (int64_t)TH * r;
       bool active = UPPER_T ? (i < j) : (i > j && i < n);
       if (active) yr[r] = O::sub(yr[r], O::mul(lv[r], yj));
       lv[r] = nx[r];
@@ -95,7 +97,7 @@ __global__ void __launch_bounds__(TS_THREADS) trsv_kernel(const typename O::T* _
   }
 #pragma unroll
   for (int r = 0; r < RMAX; r++) {
-    int64_t i = t + (int64_t)TS_THREADS * r;
+    int64_t i = t + (int64_t)TH * r;
     if (i < n) y[i] = yr[r];
   }
 }
@@ -173,13 +175,14 @@ __global__ void vec_kernel(int op, const dd* a, const dd* b, dd* out, const doub
 
 template <class O, bool UPPER_T>
 int trsv_launch(const typename O::T* L, typename O::T* y, size_t n, cudaStream_t s) {
-  const size_t R = (n + TS_THREADS - 1) / TS_THREADS;
-#define HP_TRSV(RM) trsv_kernel<O, RM, UPPER_T><<<1, TS_THREADS, 0, s>>>(L, y, n)
-  if (R <= 1) HP_TRSV(1);
-  else if (R <= 2) HP_TRSV(2);
-  else if (R <= 4) HP_TRSV(4);
-  else if (R <= 8) HP_TRSV(8);
-  else if (R <= 16) HP_TRSV(16);
+#define HP_TRSV(TH, RM) trsv_kernel<O, TH, RM, UPPER_T><<<1, TH, 0, s>>>(L, y, n)
+  if (n <= 256) HP_TRSV(256, 1);
+  else if (n <= 512) HP_TRSV(512, 1);
+  else if (n <= 1024) HP_TRSV(1024, 1);
+  else if (n <= 1024 * 2) HP_TRSV(1024, 2);
+  else if (n <= 1024 * 4) HP_TRSV(1024, 4);
+  else if (n <= 1024 * 8) HP_TRSV(1024, 8);
+  else if (n <= 1024 * 16) HP_TRSV(1024, 16);
   else {
     set_error("triangular solve: n = %zu exceeds 16384", n);
     return HP_ERR_UNSUPPORTED;
