@@ -24,6 +24,7 @@
 #include "hp_arith.cuh"
 #include "hp_runtime.cuh"
 #include "kernels.cuh"
+#include "sm100_ptx.cuh"
 
 namespace hp {
 
@@ -171,10 +172,17 @@ __global__ void __launch_bounds__(64) chol_panel_kernel(typename O::T* A, const 
 // at once (independent operations), instead of each sum walking its k loop
 // after the column it waits for.
 //
-// Diagonal block: one CTA; per column j, one thread forms the pivot
-// (sqrt, recip), the rows below scale their entry of column j, and the
-// sums of the remaining lower triangle take their j-th product.
-constexpr int RL_THREADS = 512;
+// Diagonal block: one CTA, pivots on a critical warp. At step j warp 0's
+// lane 0 forms L_{j+1,j} = (A - s) recip(L_jj), adds its square to the sum of
+// the next diagonal entry (the k = j product, after the bulk's earlier ones),
+// and forms pivot j + 1 (sqrt, recip); the bulk warps meanwhile scale the
+// rest of column j and add its products to every other sum of the remaining
+// lower triangle. L_{j+1,j} reaches the bulk through a named barrier that the
+// critical warp passes without waiting, so the pivot chain runs while the
+// bulk's updates of step j run, with one block barrier per step. Each sum
+// still takes its products one at a time in k order, by the same formulas,
+// so the factor is the reference's bit for bit.
+constexpr int RL_THREADS = 512, RL_BULK = RL_THREADS - 32;
 template <class O>
 __global__ void __launch_bounds__(RL_THREADS) chol_diag_rl_kernel(typename O::T* A, const typename O::T* S, int64_t n,
                                                                   int64_t kb, int jb, typename O::T* invd,
@@ -185,7 +193,7 @@ __global__ void __launch_bounds__(RL_THREADS) chol_diag_rl_kernel(typename O::T*
   T* Ss = Ls + 64 * 65;                  // [64][65]: running sums
   __shared__ T inv_s[CH_MAXNB];
   __shared__ int fail;
-  const int t = threadIdx.x;
+  const int t = threadIdx.x, warp = t / 32, bt = t - 32;  // bt: bulk thread index (warps 1..)
   if (err->flag) return;
   if (t == 0) fail = 0;
   for (int e = t; e < jb * jb; e += RL_THREADS) {
@@ -196,35 +204,54 @@ __global__ void __launch_bounds__(RL_THREADS) chol_diag_rl_kernel(typename O::T*
     }
   }
   __syncthreads();
-  for (int j = 0; j < jb; j++) {
-    if (t == 0) {
-      const T d = O::sub(Ls[j * 65 + j], Ss[j * 65 + j]);
-      if (!(O::hi(d) > 0.0) && !(O::hi(d) != O::hi(d))) {  // diag <= 0 (NaN passes, as in Rust)
-        fail = 1;
-        err->flag = 1;
-        err->pivot = kb + j;
-        err->value = O::to_f64(d);
-      } else {
-        const T l = O::sqrt_(d);
-        Ls[j * 65 + j] = l;
-        inv_s[j] = O::inv(l);
-      }
+  // pivot p from its finished sum; false (and the error recorded) if not positive
+  auto pivot = [&](int p) -> bool {
+    const T d = O::sub(Ls[p * 65 + p], Ss[p * 65 + p]);
+    if (!(O::hi(d) > 0.0) && !(O::hi(d) != O::hi(d))) {  // diag <= 0 (NaN passes, as in Rust)
+      fail = 1;
+      err->flag = 1;
+      err->pivot = kb + p;
+      err->value = O::to_f64(d);
+      return false;
     }
-    __syncthreads();
+    const T l = O::sqrt_(d);
+    Ls[p * 65 + p] = l;
+    inv_s[p] = O::inv(l);
+    return true;
+  };
+  if (t == 0) pivot(0);
+  __syncthreads();
+  for (int j = 0; j < jb; j++) {
     if (fail) return;
-    for (int r = j + 1 + t; r < jb; r += RL_THREADS)
-      Ls[r * 65 + j] = O::mul(O::sub(Ls[r * 65 + j], Ss[r * 65 + j]), inv_s[j]);
-    __syncthreads();
-    // sums (r, c), j < c <= r < jb, take the product L_rj L_cj
-    const int m = jb - j - 1;
-    for (int e = t; e < m * (m + 1) / 2; e += RL_THREADS) {
-      int r = (int)((sqrtf(8.0f * e + 1.0f) - 1.0f) * 0.5f);
-      while (r * (r + 1) / 2 > e) r--;
-      while ((r + 1) * (r + 2) / 2 <= e) r++;
-      const int c = e - r * (r + 1) / 2;
-      const int rr = j + 1 + r, cc = j + 1 + c;
-      Ss[rr * 65 + cc] = O::add(Ss[rr * 65 + cc],
-                                rr == cc ? O::mul(Ls[rr * 65 + j], Ls[rr * 65 + j]) : O::mul(Ls[rr * 65 + j], Ls[cc * 65 + j]));
+    if (warp == 0) {
+      if (t == 0 && j + 1 < jb) {
+        const T l1 = O::mul(O::sub(Ls[(j + 1) * 65 + j], Ss[(j + 1) * 65 + j]), inv_s[j]);
+        Ls[(j + 1) * 65 + j] = l1;
+        __threadfence_block();
+      }
+      __syncwarp();
+      sm100::named_arrive(1, RL_THREADS);  // L_{j+1,j} is in place
+      if (t == 0 && j + 1 < jb) {
+        const T l1 = Ls[(j + 1) * 65 + j];
+        Ss[(j + 1) * 65 + j + 1] = O::add(Ss[(j + 1) * 65 + j + 1], O::mul(l1, l1));
+        pivot(j + 1);
+      }
+    } else {
+      for (int r = j + 2 + bt; r < jb; r += RL_BULK)
+        Ls[r * 65 + j] = O::mul(O::sub(Ls[r * 65 + j], Ss[r * 65 + j]), inv_s[j]);
+      sm100::named_sync(1, RL_THREADS);  // column j scaled (L_{j+1,j} by the critical warp)
+      // sums (r, c), j < c <= r < jb, take the product L_rj L_cj, except
+      // (j + 1, j + 1), which the critical warp has taken
+      const int m = jb - j - 1;
+      for (int e = bt + 1; e < m * (m + 1) / 2; e += RL_BULK) {
+        int r = (int)((sqrtf(8.0f * e + 1.0f) - 1.0f) * 0.5f);
+        while (r * (r + 1) / 2 > e) r--;
+        while ((r + 1) * (r + 2) / 2 <= e) r++;
+        const int c = e - r * (r + 1) / 2;
+        const int rr = j + 1 + r, cc = j + 1 + c;
+        Ss[rr * 65 + cc] = O::add(Ss[rr * 65 + cc],
+                                  rr == cc ? O::mul(Ls[rr * 65 + j], Ls[rr * 65 + j]) : O::mul(Ls[rr * 65 + j], Ls[cc * 65 + j]));
+      }
     }
     __syncthreads();
   }
