@@ -768,6 +768,36 @@ def profile_case_spd(args):
     return 0
 
 
+def profile_case_chol512(args):
+    """Plain f128 Cholesky solves at n = 512 (config 1), warmup + steps of them:
+    the command ncu captures."""
+    import ctypes
+
+    import torch
+
+    import quadprec_b200 as hp
+    from quadprec_b200.workloads import shifted_hilbert
+
+    dev = torch.device("cuda", 0)
+    sptr = torch.cuda.current_stream(dev).cuda_stream
+    n = CH_N
+    a, b = shifted_hilbert(n)
+    lib = hp.lib()
+    dA = torch.from_numpy(a).to(dev)
+    db = torch.from_numpy(b).to(dev)
+    dL = torch.empty_like(dA)
+    dx = torch.empty_like(db)
+    pv, val = ctypes.c_int64(-1), ctypes.c_double(0.0)
+    for _ in range(args.warmup + args.steps):
+        dL.copy_(dA)
+        dx.copy_(db)
+        hp.check(lib.hp_f128_cholesky_dev(dL.data_ptr(), n, ctypes.byref(pv), ctypes.byref(val), sptr))
+        hp.check(lib.hp_f128_solve_cholesky_dev(dL.data_ptr(), dx.data_ptr(), n, sptr))
+    torch.cuda.synchronize()
+    print("profile case done", file=sys.stderr)
+    return 0
+
+
 # ---------------------------------------------------------------- main arm
 def main():
     ap = argparse.ArgumentParser()
@@ -781,7 +811,7 @@ def main():
     ap.add_argument("--spd-steps", type=int, default=3)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched SPD / Jacobi section")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint section")
-    ap.add_argument("--profile-case", nargs="?", const="gemm", default=None, choices=["gemm", "spd", "batched"],
+    ap.add_argument("--profile-case", nargs="?", const="gemm", default=None, choices=["gemm", "spd", "batched", "chol512"],
                     help="only run warmup + steps of one chosen-path workload (for ncu captures)")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -790,6 +820,8 @@ def main():
         return profile_case(args)
     if args.profile_case == "spd":
         return profile_case_spd(args)
+    if args.profile_case == "chol512":
+        return profile_case_chol512(args)
     if args.profile_case == "batched":
         import torch
 

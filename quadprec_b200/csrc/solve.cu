@@ -39,8 +39,8 @@ namespace {
 
 // One CTA of TH threads; thread t owns rows t, t + TH, ... (RMAX of them).
 // The entries of L a step needs (its column below / row right of the
-// diagonal, and the next diagonal element) do not depend on y, so each step
-// loads the next step's while its own multiply-adds run: the per-step chain
+// diagonal, and the diagonal element) do not depend on y, so each step loads
+// those of the step after next while its own multiply-adds run: the per-step chain
 // is the owner's division, one barrier and one multiply-add. TH is one row
 // per thread up to n = 1024 (no idle warps in each step's barrier). Measured
 // at n = 512: 128 threads with four rows each is slower (the multiply-adds of
@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(TH) trsv_kernel(const typename O::T* __restric
   using T = typename O::T;
   __shared__ T bc[2];
   const int t = threadIdx.x;
-  T yr[RMAX], lv[RMAX];
+  T yr[RMAX], l0[RMAX], l1[RMAX];
   auto lval = [&](int64_t step, int r) {
     const int64_t j = UPPER_T ? n - 1 - step : step;
     const int64_t i = t + (int64_t)TH * r;
@@ -67,9 +67,10 @@ __global__ void __launch_bounds__(TH) trsv_kernel(const typename O::T* __restric
   for (int r = 0; r < RMAX; r++) {
     int64_t i = t + (int64_t)TH * r;
     yr[r] = i < n ? y[i] : O::zero();
-    lv[r] = lval(0, r);
+    l0[r] = lval(0, r);
+    l1[r] = lval(1, r);
   }
-  T dg = ldiag(0);
+  T d0 = ldiag(0), d1 = ldiag(1);  // the diagonal entries of this step and the next
   for (int64_t step = 0; step < n; step++) {
     const int64_t j = UPPER_T ? n - 1 - step : step;
     const int owner = (int)(j % TH), rj = (int)(j / TH);
@@ -77,23 +78,27 @@ __global__ void __launch_bounds__(TH) trsv_kernel(const typename O::T* __restric
 #pragma unroll
       for (int r = 0; r < RMAX; r++)
         if (r == rj) {
-          yr[r] = O::div(yr[r], dg);
+          yr[r] = O::div(yr[r], d0);
           bc[step & 1] = yr[r];
         }
     }
     __syncthreads();
     const T yj = bc[step & 1];
-    T nx[RMAX];
+    // entries of step + 2, loaded two steps ahead (an L2 round trip is longer than a step's work)
+    T l2[RMAX];
 #pragma unroll
-    for (int r = 0; r < RMAX; r++) nx[r] = lval(step + 1, r);
-    dg = ldiag(step + 1);
+    for (int r = 0; r < RMAX; r++) l2[r] = lval(step + 2, r);
+    const T d2 = ldiag(step + 2);
 #pragma unroll
     for (int r = 0; r < RMAX; r++) {
       int64_t i = t + (int64_t)TH * r;
       bool active = UPPER_T ? (i < j) : (i > j && i < n);
-      if (active) yr[r] = O::sub(yr[r], O::mul(lv[r], yj));
-      lv[r] = nx[r];
+      if (active) yr[r] = O::sub(yr[r], O::mul(l0[r], yj));
+      l0[r] = l1[r];
+      l1[r] = l2[r];
     }
+    d0 = d1;
+    d1 = d2;
   }
 #pragma unroll
   for (int r = 0; r < RMAX; r++) {
