@@ -592,6 +592,7 @@ def adjoint_section(hp, torch, dev, stream, sptr, args, world, dist):
     lib = hp.lib()
     out = {"workload": f"dL/dtheta for L = b^T S^-1 b, n = {n} s-Gaussians (250 jittered 5x5x10 lattice centres x 4 "
                        "exponents), theta = 750 centre coordinates + 1000 log-exponents", "unit": "gradients/s"}
+    grads = {}
     for name, mode in (("chosen", hp.OZAKI), ("plain", hp.PLAIN)):
         info = hp.RefineInfo()
 
@@ -612,8 +613,9 @@ def adjoint_section(hp, torch, dev, stream, sptr, args, world, dist):
         e0.record(stream)
         torch.cuda.synchronize()
         ms = max_over_ranks(s0.elapsed_time(e0) / steps, dist, dev)
+        grads[name] = (gR.cpu().numpy().copy(), ga.cpu().numpy().copy())
         out[name] = {"gradients_per_s": world * 1e3 / ms, "ms_per_gradient": ms, "converged": bool(info.converged),
-                     "accuracy_vs_f256_fd": adjoint_fd_error(gR.cpu().numpy(), ga.cpu().numpy())}
+                     "accuracy_vs_f256_fd": adjoint_fd_error(*grads[name])}
     out["chosen_over_plain"] = out["chosen"]["gradients_per_s"] / out["plain"]["gradients_per_s"]
     if getattr(args, "cpu_leg", False):
         import oracle
@@ -621,6 +623,17 @@ def adjoint_section(hp, torch, dev, stream, sptr, args, world, dist):
         t0 = time.perf_counter()
         _, cgR, cga = oracle.adjoint_f128_refined(cen, alpha, b, co, nc)
         dt = time.perf_counter() - t0
+        # every component of both GPU gradients against the oracle's full f128 gradient
+        ref = np.concatenate([np.asarray(cgR).reshape(-1, 2)[:, 0], np.asarray(cga).reshape(-1, 2)[:, 0]])
+        scale = float(np.max(np.abs(ref)))
+        for name, (gR_, ga_) in grads.items():
+            got = np.concatenate([gR_.reshape(-1, 2), ga_.reshape(-1, 2)])
+            want = np.concatenate([np.asarray(cgR).reshape(-1, 2), np.asarray(cga).reshape(-1, 2)])
+            err = np.abs((got[:, 0] - want[:, 0]) + (got[:, 1] - want[:, 1]))
+            out[name]["accuracy_vs_oracle_gradient"] = {
+                "max_abs_err_over_max_component": float(err.max() / scale), "components": int(len(err)),
+                "reference": "the oracle's full gradient (reference f128 cholesky + solve_cholesky, f256 residuals, "
+                             "f128 contraction)"}
         out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "gradients/s", "cores": oracle.num_threads(),
                                "kind": "port", "accuracy_vs_f256_fd": adjoint_fd_error(cgR, cga),
                                "sample": f"one full gradient, {dt:.2f} s: S in f128, lambda from the reference's "
