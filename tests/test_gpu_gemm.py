@@ -78,6 +78,43 @@ def test_f128_ozaki_wide_exponents_and_zeros(gpu):
     assert np.all(d <= 4 * k * 2.0 ** -104 * ab + 1e-300)
 
 
+@pytest.mark.parametrize("atb", [False, True])
+@pytest.mark.parametrize("m", [70, 600])
+def test_f128_ozaki_nonfinite_rows_and_columns(gpu, m, atb):
+    """An inf or NaN limb in a row of op(A) or a column of B makes that row or
+    column of C NaN (the chosen path's scaling has no finite exponent for it);
+    every other entry is the finite product, within the entrywise bound. m = 600
+    takes the host-pointer path's streamed A panels."""
+    n, k = 90, 150
+    a = dense_dd(k, m, seed=31) if atb else dense_dd(m, k, seed=31)
+    b = dense_dd(k, n, seed=32)
+    bad_rows, bad_cols = [3, 5, 7], [2, 6]
+    at = (lambda r, p: (p, r)) if atb else (lambda r, p: (r, p))
+    a[at(3, 10)][0] = np.nan        # NaN high limb
+    a[at(5, 0)][0] = np.inf         # inf high limb
+    a[at(7, 20)][1] = -np.inf       # non-finite low limb only
+    b[4, 2, 0] = np.inf
+    b[8, 6, 1] = np.nan
+    c = gpu.f128_gemm(a, b, m, n, k, gpu.OZAKI, atb)
+    assert np.all(np.isnan(c[bad_rows, :, 0])) and np.all(np.isnan(c[:, bad_cols, 0]))
+    # the other entries against the oracle on the inputs with the bad rows and columns cleared
+    a0, b0 = a.copy(), b.copy()
+    for r in bad_rows:
+        if atb:
+            a0[:, r] = 0.0
+        else:
+            a0[r] = 0.0
+    b0[:, bad_cols] = 0.0
+    ref = O.gemm(a0, b0, m, n, k, atb=atb)
+    good_r = np.setdiff1d(np.arange(m), bad_rows)
+    good_c = np.setdiff1d(np.arange(n), bad_cols)
+    cg, rg = c[np.ix_(good_r, good_c)], ref[np.ix_(good_r, good_c)]
+    assert np.all(np.isfinite(cg))
+    ab = abs_prod(a0, b0, atb)[np.ix_(good_r, good_c)]
+    d = np.abs((cg[..., 0] - rg[..., 0]) + (cg[..., 1] - rg[..., 1]))
+    assert np.all(d <= 4 * k * 2.0 ** -104 * ab + 1e-300)
+
+
 def test_f128_ozaki_cancellation(gpu):
     """C = A B with B = [x, -x]: the two halves must cancel to (near) zero."""
     m, k = 40, 200
