@@ -115,6 +115,19 @@ def test_f128_ozaki_nonfinite_rows_and_columns(gpu, m, atb):
     assert np.all(d <= 4 * k * 2.0 ** -104 * ab + 1e-300)
 
 
+@pytest.mark.parametrize("k", [128, 129, 600000])
+def test_f128_ozaki_moduli_count_boundaries(gpu, k):
+    """k = 128 / 129 straddle the step from 29 to 30 moduli; k = 600000 needs 32
+    (and 19 k-chunks of the unsigned residue GEMM): every moduli count the
+    tensor-core residue and CRT kernels are built for with k up to 2^20."""
+    m = n = 16
+    a, b = gemm_operands(m, n, k, seed=41 + k)
+    c = gpu.f128_gemm(a, b, m, n, k, gpu.OZAKI)
+    ref = O.gemm(a, b, m, n, k)
+    err = normwise_err(c, ref, abs_prod(a, b, False))
+    assert err <= 4 * k * 2.0 ** -104, err
+
+
 def test_f128_ozaki_cancellation(gpu):
     """C = A B with B = [x, -x]: the two halves must cancel to (near) zero."""
     m, k = 40, 200
