@@ -601,7 +601,8 @@ struct ResidueOperand {  // one GEMM operand as the residue kernel sees it
   int8_t* out;           // L planes of rows x ld bytes
   int64_t plane, ld;     // plane stride, row stride (bytes)
   const int* exps;       // per-row exponents
-  int64_t row_tiles, p_tiles;  // tiles of RC_ROWS rows x RC_P reduction indices
+  int64_t row_tiles, p_tiles;  // tiles of RC_ROWS (f256: 4) rows x RC_P reduction indices
+  int64_t half;          // f256: byte offset of a row's second half (the two 105-bit halves)
 };
 
 // The tiles of a persistent CTA (first, first + stride, ...) in a grid of
@@ -645,7 +646,22 @@ __device__ __forceinline__ void int128_of(double x, uint64_t& lo, uint64_t& hi) 
   }
 }
 
-template <int LC, bool A_CONTIG>
+// 128-bit two's-complement (lo, hi) += (a0, a1)
+__device__ __forceinline__ void add128(uint64_t& lo, uint64_t& hi, uint64_t a0, uint64_t a1) {
+  lo += a0;
+  hi += a1 + (lo < a0 ? 1ull : 0ull);
+}
+
+// QD: the f256 operands. An entry is 4 limbs; its scaled integer
+// X = sum_q rint(limb_q 2^s), |X| <= 2^210 + 2^157, is split exactly as
+// X = Xh 2^105 + Xl with Xl = X mods 2^105 in [-2^104, 2^104): each limb's
+// integer v is split by truncation, v = vh 2^105 + vl (both exact doubles),
+// the vh and the vl are summed in 128-bit integers, and the vl sum is brought
+// into range with its carry moved to Xh. Xh and Xl each take one 16-byte slot
+// of the entry-byte tile (tiles of 4 operand rows x 128 p: 8 slots), and go
+// to the two halves of the row (A: [Xh | Xl], B: [Yl | Yh], `half` bytes
+// apart), as the f256 GEMM's residue GEMMs read them.
+template <int LC, bool A_CONTIG, bool QD = false>
 __global__ void __launch_bounds__(RC_THREADS, 2)
     residue_tc_kernel(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB,
                       ResidueOperand opA, ResidueOperand opB, int beta, uint32_t* status) {
@@ -708,10 +724,17 @@ __global__ void __launch_bounds__(RC_THREADS, 2)
     const int rt = (int)(isA ? prod.r : prod.r - rowsA), pt = (int)prod.c;
     uint8_t* dst = sIn + pring.st * RC_IN_BYTES;
     mbar_arrive_expect_tx(&full[pring.st], (uint32_t)RC_IN_BYTES);
-    if (isA && A_CONTIG)
-      tma_load_2d(dst, &mapA, &full[pring.st], 2 * RC_P * pt, RC_ROWS * rt);
-    else
-      tma_load_2d(dst, isA ? &mapA : &mapB, &full[pring.st], 2 * RC_ROWS * rt, RC_P * pt);
+    if constexpr (QD) {  // 3-D view: 4 limbs x entries x rows
+      if (isA && A_CONTIG)
+        tma_load_3d(dst, &mapA, &full[pring.st], 0, RC_P * pt, 4 * rt);
+      else
+        tma_load_3d(dst, isA ? &mapA : &mapB, &full[pring.st], 0, 4 * rt, RC_P * pt);
+    } else {
+      if (isA && A_CONTIG)
+        tma_load_2d(dst, &mapA, &full[pring.st], 2 * RC_P * pt, RC_ROWS * rt);
+      else
+        tma_load_2d(dst, isA ? &mapA : &mapB, &full[pring.st], 2 * RC_ROWS * rt, RC_P * pt);
+    }
     prod.next();
     pring.next<RC_STAGES>();
   };
@@ -727,34 +750,79 @@ __global__ void __launch_bounds__(RC_THREADS, 2)
     const int64_t rt = isA ? cons.r : cons.r - rowsA, pt = cons.c;
     cons.next();
     const bool contig = isA && A_CONTIG;
-    int exs[4];  // the exponents of this thread's 4 entries' rows, loaded before the wait
+    constexpr int TR = QD ? 4 : RC_ROWS, NE = QD ? 2 : 4;  // operand rows per tile, entries per thread
+    int exs[NE];  // the exponents of this thread's entries' rows, loaded before the wait
 #pragma unroll
-    for (int i = 0; i < 4; i++) {
+    for (int i = 0; i < NE; i++) {
       const int k = t + RC_THREADS * i;
-      exs[i] = o.exps[rt * RC_ROWS + (contig ? k / RC_P : k % RC_ROWS)];
+      exs[i] = o.exps[rt * TR + (contig ? k / RC_P : k % TR)];
     }
     const int st = cring.st;
     if (!mbar_wait(&full[st], cring.ph, status, DEV_STATUS_TIMEOUT)) ok = false;
     cring.next<RC_STAGES>();
-    if (ok) {
-      const double2* in = reinterpret_cast<const double2*>(sIn + st * RC_IN_BYTES);
+    if constexpr (QD) {
+      if (ok) {
+        const double4* in = reinterpret_cast<const double4*>(sIn + st * RC_IN_BYTES);
 #pragma unroll
-      for (int i = 0; i < 4; i++) {
-        const int k = t + RC_THREADS * i;
-        const int j = contig ? k / RC_P : k % RC_ROWS, n = contig ? k % RC_P : k / RC_ROWS;
-        const double2 v = in[k];
-        const int ex = exs[i];
-        uint64_t w0 = 0, w1 = 1ull << 47;  // X' = X + 2^111 (X = 0 for a non-finite row)
-        if (ex != EXP_NONFINITE) {
-          const int s = beta + 1022 - ex;
-          uint64_t hl, hh, ll, lh;
-          int128_of(rint(scale_pow2(v.x, s)), hl, hh);
-          int128_of(rint(scale_pow2(v.y, s)), ll, lh);
-          w0 = hl + ll;
-          w1 = hh + lh + (w0 < hl ? 1ull : 0ull) + (1ull << 47);
+        for (int i = 0; i < NE; i++) {
+          const int k = t + RC_THREADS * i;
+          const int j = contig ? k / RC_P : k % TR, n = contig ? k % RC_P : k / TR;
+          const double4 v = in[k];
+          const int ex = exs[i];
+          uint64_t h0 = 0, h1 = 0, x0 = 0, x1 = 0;  // Xh, Xl (zero for a non-finite row)
+          if (ex != EXP_NONFINITE) {
+            const int s = beta + 1022 - ex;
+            const double lim[4] = {v.x, v.y, v.z, v.w};
+            uint64_t l0 = 0, l1 = 0;
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+              const double xq = rint(scale_pow2(lim[q], s));
+              const double vh = trunc(__dmul_rn(xq, 0x1p-105));        // exact
+              const double vl = __dsub_rn(xq, __dmul_rn(vh, 0x1p105));  // exact, |vl| < 2^105
+              uint64_t a0, a1;
+              int128_of(vh, a0, a1);
+              add128(h0, h1, a0, a1);
+              int128_of(vl, a0, a1);
+              add128(l0, l1, a0, a1);
+            }
+            x0 = l0;  // Xl: the low 105 bits, sign-extended from bit 104
+            x1 = l1 & ((1ull << 41) - 1);
+            if (x1 >> 40) x1 |= ~((1ull << 41) - 1);
+            const int64_t carry = (int64_t)(l1 - x1) >> 41;  // (sum - Xl) / 2^105 (low word cancels)
+            add128(h0, h1, (uint64_t)carry, carry < 0 ? ~0ull : 0ull);
+          }
+          // X' = X + 2^111 for each half; A: slot 2j = Xh, 2j + 1 = Xl; B: slot 2j = Yl, 2j + 1 = Yh
+          const uint64_t hw1 = h1 + (1ull << 47), xw1 = x1 + (1ull << 47);
+          const uint4 bh = make_uint4((uint32_t)h0, (uint32_t)(h0 >> 32), (uint32_t)hw1,
+                                      (uint32_t)((hw1 >> 32) & 0xFFFFu) | 0x10000u);
+          const uint4 bl = make_uint4((uint32_t)x0, (uint32_t)(x0 >> 32), (uint32_t)xw1,
+                                      (uint32_t)((xw1 >> 32) & 0xFFFFu) | 0x10000u);
+          *reinterpret_cast<uint4*>(sE + swz(n, 2 * j)) = isA ? bh : bl;
+          *reinterpret_cast<uint4*>(sE + swz(n, 2 * j + 1)) = isA ? bl : bh;
         }
-        *reinterpret_cast<uint4*>(sE + swz(n, j)) =
-            make_uint4((uint32_t)w0, (uint32_t)(w0 >> 32), (uint32_t)w1, (uint32_t)((w1 >> 32) & 0xFFFFu) | 0x10000u);
+      }
+    } else {
+      if (ok) {
+        const double2* in = reinterpret_cast<const double2*>(sIn + st * RC_IN_BYTES);
+#pragma unroll
+        for (int i = 0; i < 4; i++) {
+          const int k = t + RC_THREADS * i;
+          const int j = contig ? k / RC_P : k % RC_ROWS, n = contig ? k % RC_P : k / RC_ROWS;
+          const double2 v = in[k];
+          const int ex = exs[i];
+          uint64_t w0 = 0, w1 = 1ull << 47;  // X' = X + 2^111 (X = 0 for a non-finite row)
+          if (ex != EXP_NONFINITE) {
+            const int s = beta + 1022 - ex;
+            uint64_t hl, hh, ll, lh;
+            int128_of(rint(scale_pow2(v.x, s)), hl, hh);
+            int128_of(rint(scale_pow2(v.y, s)), ll, lh);
+            w0 = hl + ll;
+            w1 = hh + lh + (w0 < hl ? 1ull : 0ull) + (1ull << 47);
+          }
+          *reinterpret_cast<uint4*>(sE + swz(n, j)) =
+              make_uint4((uint32_t)w0, (uint32_t)(w0 >> 32), (uint32_t)w1, (uint32_t)((w1 >> 32) & 0xFFFFu) | 0x10000u);
+        }
+    
       }
     }
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -815,12 +883,13 @@ __global__ void __launch_bounds__(RC_THREADS, 2)
     tc_fence_before();
     __syncthreads();  // the tile's bytes staged (and its TMEM read out)
     // full 128-byte rows of every plane, 8 threads per row
-    int8_t* ob = o.out + (size_t)(rt * RC_ROWS) * o.ld + (size_t)pt * RC_P;
+    int8_t* ob = o.out + (size_t)(rt * TR) * o.ld + (size_t)pt * RC_P;
 #pragma unroll 2
     for (int e = t; e < LC * RC_ROWS * 8; e += RC_THREADS) {
-      const int l = e >> 6, j = (e >> 3) & 7, c = e & 7;
+      const int l = e >> 6, j = (e >> 3) & 7, c = e & 7;  // plane, slot, 16-byte piece
       const uint4 val = *reinterpret_cast<const uint4*>(sOut + l * RC_OUT_PLANE + j * RC_P + 16 * c);
-      *reinterpret_cast<uint4*>(ob + (size_t)l * o.plane + (size_t)j * o.ld + 16 * c) = val;
+      const size_t at = QD ? (size_t)(j >> 1) * o.ld + (size_t)(j & 1) * o.half : (size_t)j * o.ld;
+      *reinterpret_cast<uint4*>(ob + (size_t)l * o.plane + at + 16 * c) = val;
     }
   }
   if (!ok && t == 0) {
@@ -1776,9 +1845,9 @@ static int launch_residues_tc(bool atb, int L, const double2* A, size_t m, const
   };
   CUtensorMap mapA, mapB;
   ResidueOperand oa{outA, (int64_t)(Mp * Kp), (int64_t)Kp, expA, A ? (int64_t)(Mp / RC_ROWS) : 0,
-                    (int64_t)(Kp / RC_P)};
+                    (int64_t)(Kp / RC_P), 0};
   ResidueOperand ob{outB, (int64_t)(Np * Kp), (int64_t)Kp, expB, B ? (int64_t)(Np / RC_ROWS) : 0,
-                    (int64_t)(Kp / RC_P)};
+                    (int64_t)(Kp / RC_P), 0};
   if (B) HP_TRY(map2d(&mapB, B, k, n, RC_ROWS, RC_P));
   if (A) {
     if (atb)
@@ -2195,6 +2264,77 @@ int ozaki_dd_gemm_host(const double* a, const double* b, double* c, size_t m, si
 namespace ozaki {
 constexpr int BETA_QD = 210;
 
+// The f256 GEMM's residue rows on the tensor core (residue_tc_kernel<., ., QD>):
+// A (m x k, or k x m when atb) and B (k x n) of 4-limb entries; rows of 2 Kp
+// bytes, [Xh | Xl] for A and [Yl | Yh] for B, unsigned bytes. HP_ERR_UNSUPPORTED
+// (nothing launched) for moduli counts other than 28..32.
+static int launch_residues_tc_qd(bool atb, int L, const double4* A, size_t m, const int* expA, int8_t* outA,
+                                 size_t Mp, const double4* B, size_t n, const int* expB, int8_t* outB, size_t Np,
+                                 size_t k, size_t Kp, int num_sms, uint32_t* status, cudaStream_t s) {
+  if (L < CRT_CONST_L0 || L >= CRT_CONST_L0 + CRT_CONST_N || Mp % 4 || Np % 4 || Kp % RC_P ||
+      ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 31u))
+    return HP_ERR_UNSUPPORTED;
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63]) {
+#define HP_RQ_ATTR(LCV)                                                                                          \
+  HP_CUDA_TRY(cudaFuncSetAttribute(residue_tc_kernel<LCV, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                   RC_SMEM));                                                                    \
+  HP_CUDA_TRY(cudaFuncSetAttribute(residue_tc_kernel<LCV, false, true>,                                          \
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, RC_SMEM));
+    HP_RQ_ATTR(28) HP_RQ_ATTR(29) HP_RQ_ATTR(30) HP_RQ_ATTR(31) HP_RQ_ATTR(32)
+#undef HP_RQ_ATTR
+    attr_set[dev & 63] = true;
+  }
+  auto fn = encode_fn();
+  if (!fn) {
+    set_error("cuTensorMapEncodeTiled unavailable");
+    return HP_ERR_CUDA;
+  }
+  // f64 view (4 limbs x cols x rows) of a row-major f256 matrix; a box is
+  // 4 limbs x box_c entries x box_r rows
+  auto map3d = [&](CUtensorMap* map, const double4* base, size_t rows, size_t cols, uint32_t box_c,
+                   uint32_t box_r) -> int {
+    cuuint64_t dims[3] = {4, cols, rows};
+    cuuint64_t strides[2] = {32, cols * 32};
+    cuuint32_t box[3] = {4, box_c, box_r};
+    cuuint32_t estr[3] = {1, 1, 1};
+    CUresult rc = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double4*>(base), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                     CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (rc != CUDA_SUCCESS) {
+      set_error("cuTensorMapEncodeTiled failed (%d)", (int)rc);
+      return HP_ERR_CUDA;
+    }
+    return HP_OK;
+  };
+  CUtensorMap mapA, mapB;
+  HP_TRY(map3d(&mapB, B, k, n, 4, RC_P));  // B is k x n: 4 operand rows (columns) x 128 reduction indices
+  if (atb)
+    HP_TRY(map3d(&mapA, A, k, m, 4, RC_P));  // A is k x m
+  else
+    HP_TRY(map3d(&mapA, A, m, k, RC_P, 4));  // A is m x k: 128 reduction indices x 4 rows
+  ResidueOperand oa{outA, (int64_t)(Mp * 2 * Kp), (int64_t)(2 * Kp), expA, (int64_t)(Mp / 4), (int64_t)(Kp / RC_P),
+                    (int64_t)Kp};
+  ResidueOperand ob{outB, (int64_t)(Np * 2 * Kp), (int64_t)(2 * Kp), expB, (int64_t)(Np / 4), (int64_t)(Kp / RC_P),
+                    (int64_t)Kp};
+  const int grid = num_sms * 2;
+#define HP_RQ(LCV)                                                                                                \
+  if (L == LCV) {                                                                                                 \
+    if (atb)                                                                                                      \
+      HP_CUDA_TRY(launch_k(true, residue_tc_kernel<LCV, false, true>, dim3(grid), dim3(RC_THREADS), RC_SMEM, s,    \
+                           mapA, mapB, oa, ob, BETA_QD, status));                                                 \
+    else                                                                                                          \
+      HP_CUDA_TRY(launch_k(true, residue_tc_kernel<LCV, true, true>, dim3(grid), dim3(RC_THREADS), RC_SMEM, s,     \
+                           mapA, mapB, oa, ob, BETA_QD, status));                                                 \
+    return HP_OK;                                                                                                 \
+  }
+  HP_RQ(28) HP_RQ(29) HP_RQ(30) HP_RQ(31) HP_RQ(32)
+#undef HP_RQ
+  return HP_ERR_UNSUPPORTED;
+}
+
 // Balanced base-2^21 digits of rint(v) for |v| < 2^212 (exact).
 __device__ __forceinline__ void int_digits21x10(double v, int32_t* d) {
   double a = fabs(rint(v));
@@ -2554,7 +2694,15 @@ int ozaki_qd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
   const double4* A4 = reinterpret_cast<const double4*>(a);
   const double4* B4 = reinterpret_cast<const double4*>(b);
   HP_TRY(launch_maxexp(A4, B4, m, n, k, atb, expAp, expBp, s));
-  {  // residues of both operands as unsigned bytes, 4 entries per thread
+  uint32_t* status = device_status(s);
+  if (!status) {
+    set_error("status word allocation failed");
+    return HP_ERR_CUDA;
+  }
+  const int rq = launch_residues_tc_qd(atb, L, A4, m, expAp, ares.as<int8_t>(), Mp, B4, n, expBp, bres.as<int8_t>(),
+                                       Np, k, Kp, D->num_sms, status, s);
+  if (rq != HP_OK && rq != HP_ERR_UNSUPPORTED) return rq;
+  if (rq == HP_ERR_UNSUPPORTED) {  // residues of both operands as unsigned bytes, 4 entries per thread
     const unsigned tay = (unsigned)(Mp / RT_R);
     dim3 g((unsigned)(Kp / 16), tay + (unsigned)(Np / RT_R));
 #define HP_RESQ(AC, LCV)                                                                                        \
