@@ -141,3 +141,52 @@ def test_crt_reconstruction(L):
         # the double-double is C to f128 accuracy (relative to |C|)
         got = Fraction(hi) + Fraction(lo)
         assert abs(got - C) <= abs(Fraction(C)) * Fraction(1, 1 << 104) + Fraction(0), (L, C)
+
+
+def two_sum(a, b):
+    s = a + b
+    bb = s - a
+    return s, (a - (s - bb)) + (b - bb)
+
+
+@pytest.mark.parametrize("L", [28, 29, 30, 31, 32])
+def test_f256_crt_combination(L):
+    """The f256 GEMM's CRT: two reconstructions G1, G2 (each as the f128 CRT's
+    balanced 48-bit chunks), combined as G1 2^105 + G2 (105 = 2 chunks + 9 bits)
+    with one carry pass into 9 balanced chunks, then summed from the top into
+    four limbs: exact integer, and the limbs equal it to ~2^-208 relative."""
+    tables = crt_tables(L)
+    mods, M, W, wb, mlimb, k192 = tables
+    rng = random.Random(200 + L)
+    bound = M // 4
+    for _ in range(200):
+        G1 = rng.randrange(-bound, bound + 1)
+        G2 = rng.randrange(-bound, bound + 1)
+        b1 = crt_tc([G1 % m for m in mods], L, tables)[3]
+        b2 = crt_tc([G2 % m for m in mods], L, tables)[3]
+        c = [0] * 9
+        for k in range(6):
+            c[k] += b2[k]
+            c[k + 2] += b1[k] * 512
+        carry = 0
+        for k in range(9):
+            x = c[k] + carry
+            carry = (x + (1 << 47)) >> 48 if k < 8 else 0
+            c[k] = x - carry * (1 << 48)
+            assert k == 8 or -(1 << 47) <= c[k] < (1 << 47)
+        C = G1 * (1 << 105) + G2
+        assert sum(ck << (48 * k) for k, ck in enumerate(c)) == C
+        x = [0.0, 0.0, 0.0, 0.0]
+        for k in range(8, -1, -1):
+            v = math.ldexp(float(c[k]), 48 * k)
+            x[0], e = two_sum(x[0], v)
+            x[1], e = two_sum(x[1], e)
+            x[2], e = two_sum(x[2], e)
+            x[3] = x[3] + e
+        x[2], x[3] = two_sum(x[2], x[3])
+        x[1], x[2] = two_sum(x[1], x[2])
+        x[0], x[1] = two_sum(x[0], x[1])
+        x[1], x[2] = two_sum(x[1], x[2])
+        x[2], x[3] = two_sum(x[2], x[3])
+        got = sum(Fraction(v) for v in x)
+        assert abs(got - C) <= abs(Fraction(C)) * Fraction(1, 1 << 206) + 1, (L, C)
