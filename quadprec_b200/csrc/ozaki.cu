@@ -1483,8 +1483,8 @@ __device__ __forceinline__ int swz32(int row, int k) {
   return (row >> 3) * 256 + (row & 7) * 32 + ((((k >> 4) ^ (row >> 2)) & 1) << 4) + (k & 15);
 }
 
-// the f128 value of one entry from its 32 weight-byte sums
-__device__ __forceinline__ double2 crt_tc_entry(const uint32_t (&acc)[32], const CrtTcTable& T, int shift) {
+// the balanced 48-bit chunks b_k (|b_k| <= 2^47) of one entry's C = sum_k b_k 2^(48 k), from its 32 weight-byte sums
+__device__ __forceinline__ void crt_tc_chunks(const uint32_t (&acc)[32], const CrtTcTable& T, int64_t (&b)[6]) {
   int32_t U[16];
 #pragma unroll
   for (int h = 0; h < 16; h++) U[h] = (int32_t)(acc[2 * h] + (acc[2 * h + 1] << 8));
@@ -1497,15 +1497,22 @@ __device__ __forceinline__ double2 crt_tc_entry(const uint32_t (&acc)[32], const
 #pragma unroll
   for (int h = 0; h < 16; h++) d[h] = U[h] - q * T.mlimb[h];
   d[16] = d[17] = 0;
-  // balanced 48-bit chunks b_k (|b_k| <= 2^47), C = sum_k b_k 2^(48 k)
-  double v[6];
   int64_t carry = 0;
 #pragma unroll
   for (int k = 0; k < 6; k++) {
     const int64_t c = (int64_t)d[3 * k] + (int64_t)d[3 * k + 1] * 65536 + (int64_t)d[3 * k + 2] * 4294967296ll + carry;
     carry = k < 5 ? (c + (1ll << 47)) >> 48 : 0;
-    v[k] = scale_pow2((double)(c - carry * 281474976710656ll), 48 * k);  // exact
+    b[k] = c - carry * 281474976710656ll;
   }
+}
+
+// the f128 value of one entry from its 32 weight-byte sums
+__device__ __forceinline__ double2 crt_tc_entry(const uint32_t (&acc)[32], const CrtTcTable& T, int shift) {
+  int64_t b[6];
+  crt_tc_chunks(acc, T, b);
+  double v[6];
+#pragma unroll
+  for (int k = 0; k < 6; k++) v[k] = scale_pow2((double)b[k], 48 * k);  // exact
   // from the top: a nonzero partial sum is a multiple of 2^(48 (k+1)) and
   // |b_k 2^(48 k)| < 2^(48 k + 48), so the quick two-sums are exact
   dd s = dd{v[5], 0.0};
@@ -1519,16 +1526,65 @@ __device__ __forceinline__ double2 crt_tc_entry(const uint32_t (&acc)[32], const
   return make_double2(o.hi, o.lo);
 }
 
-template <int LC>
+// the f256 value of G1 2^105 + G2 from the two groups' weight-byte sums.
+// 105 = 2 x 48 + 9: G1's chunk k times 2^9 (|512 b| <= 2^56) joins G2's
+// chunk k + 2, and one balanced carry pass leaves nine chunks |c_k| <= 2^47
+// (the top one small) with C = sum_k c_k 2^(48 k) exactly. They are added
+// from the top into four limbs by a two-sum cascade (every step exact but
+// the last limb's additions, ~2^-212 of |C| each) and renormalised by
+// two-sum passes; the top nonzero chunk bounds |C| from below by half its
+// weight, so the error is relative to |C|.
+__device__ __forceinline__ double4 crt_tc_entry_qd(const uint32_t (&acc1)[32], const uint32_t (&acc2)[32],
+                                                   const CrtTcTable& T, int shift) {
+  int64_t b1[6], b2[6], c[9];
+  crt_tc_chunks(acc1, T, b1);
+  crt_tc_chunks(acc2, T, b2);
+#pragma unroll
+  for (int k = 0; k < 9; k++) c[k] = (k < 6 ? b2[k] : 0) + (k >= 2 && k < 8 ? b1[k - 2] * 512 : 0);
+  int64_t carry = 0;
+#pragma unroll
+  for (int k = 0; k < 9; k++) {
+    const int64_t x = c[k] + carry;
+    carry = k < 8 ? (x + (1ll << 47)) >> 48 : 0;
+    c[k] = x - carry * 281474976710656ll;
+  }
+  double x0 = 0.0, x1 = 0.0, x2 = 0.0, x3 = 0.0;
+#pragma unroll
+  for (int k = 8; k >= 0; k--) {
+    const double v = scale_pow2((double)c[k], 48 * k);  // exact
+    double e;
+    two_sum(x0, v, x0, e);
+    two_sum(x1, e, x1, e);
+    two_sum(x2, e, x2, e);
+    x3 = __dadd_rn(x3, e);
+  }
+  two_sum(x2, x3, x2, x3);
+  two_sum(x1, x2, x1, x2);
+  two_sum(x0, x1, x0, x1);
+  two_sum(x1, x2, x1, x2);
+  two_sum(x2, x3, x2, x3);
+  return make_double4(scale_pow2(x0, shift), scale_pow2(x1, shift), scale_pow2(x2, shift), scale_pow2(x3, shift));
+}
+
+// QD: the f256 GEMM's CRT. A tile is 128 entries of a row and the map spans
+// both groups' planes (G1's L planes, then G2's): the stage holds G1's box
+// and then G2's, each group is transposed into its own 128 x 32 tile and
+// multiplied by the weights, and each thread finishes one entry from both
+// groups' sums (crt_tc_entry_qd), writing four limbs.
+template <int LC, bool QD = false>
 __global__ void __launch_bounds__(CT_THREADS, 4)
     crt_tc_kernel(const __grid_constant__ CUtensorMap map, int64_t m, int64_t n, const int* __restrict__ expA,
-                  const int* __restrict__ expB, int beta, double2* __restrict__ C, uint32_t* status) {
+                  const int* __restrict__ expB, int beta, std::conditional_t<QD, double4, double2>* __restrict__ C,
+                  uint32_t* status) {
   using namespace sm100;
+  constexpr int TW = QD ? 128 : CT_TILE;        // entries of a row per tile
+  constexpr int PS = QD ? 128 : CT_TILE;        // bytes between two moduli's residues in a stage
+  constexpr int HALF = QD ? 32 * 128 : 128;     // stage offset of the second MMA tile's residues
   extern __shared__ uint8_t smem_raw[];
   const uint32_t pad = (1024u - (smem_u32(smem_raw) & 1023u)) & 1023u;
   uint8_t* sA = smem_raw + pad;  // 2 x (128 rows (entries) x 32 bytes (moduli)), swizzled
   uint8_t* sB = sA + 2 * 128 * 32;   // 32 rows (weight bytes q) x 32 bytes (moduli), swizzled
-  uint8_t* sR = sB + 32 * 32;        // CT_STAGES x (LC planes x 256 residues), as loaded
+  uint8_t* sR = sB + 32 * 32;        // CT_STAGES x (LC planes x 256 residues, or 2 x LC planes x 128), as loaded
   __shared__ uint64_t full[CT_STAGES], mdone[2];
   __shared__ uint32_t tmem_slot;
   const CrtTcTable& T = c_crt_tc[LC - CRT_CONST_L0];
@@ -1552,14 +1608,16 @@ __global__ void __launch_bounds__(CT_THREADS, 4)
   const uint32_t tmem = tmem_slot;
   griddep_launch_dependents();
   griddep_wait();  // the product residues come from the preceding GEMM
-  const int64_t tpr = (n + CT_TILE - 1) / CT_TILE, ntiles = m * tpr;
+  const int64_t tpr = (n + TW - 1) / TW, ntiles = m * tpr;
   const int64_t cnt = blockIdx.x < ntiles ? (ntiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;  // this CTA's tiles
-  constexpr uint32_t TILE_BYTES = (uint32_t)CT_TILE * LC;
+  constexpr uint32_t TILE_BYTES = (uint32_t)CT_TILE * LC;  // QD: 2 x 128 x LC
   TileWalk prod(blockIdx.x, gridDim.x, tpr), cons(blockIdx.x, gridDim.x, tpr);
   RingPos pring, cring;
   auto issue = [&]() {  // thread 0: residues of the next tile into the next stage
+    uint8_t* dst = sR + pring.st * 32 * CT_TILE;
     mbar_arrive_expect_tx(&full[pring.st], TILE_BYTES);
-    tma_load_3d(sR + pring.st * 32 * CT_TILE, &map, &full[pring.st], (int)(prod.c * CT_TILE), (int)prod.r, 0);
+    tma_load_3d(dst, &map, &full[pring.st], (int)(prod.c * TW), (int)prod.r, 0);
+    if constexpr (QD) tma_load_3d(dst + HALF, &map, &full[pring.st], (int)(prod.c * TW), (int)prod.r, LC);
     prod.next();
     pring.next<CT_STAGES>();
   };
@@ -1580,31 +1638,32 @@ __global__ void __launch_bounds__(CT_THREADS, 4)
       else mma_seen = u;
     }
     int shift_cur[2] = {0, 0};
-    const int64_t i_cur = cons.r, j0_cur = cons.c * CT_TILE;
+    const int64_t i_cur = cons.r, j0_cur = cons.c * TW;
     if (u < cnt) {
       const int ea = expA[i_cur];
 #pragma unroll
-      for (int h = 0; h < 2; h++) {
+      for (int h = 0; h < (QD ? 1 : 2); h++) {
         const int64_t j = j0_cur + 128 * h + t;
         const int eb = j < n ? expB[j] : 0;
+        // QD: the groups hold X Y / 2^105
         shift_cur[h] = (ea == EXP_NONFINITE || eb == EXP_NONFINITE)
                            ? INT32_MIN
-                           : -((beta + 1022 - ea) + (beta + 1022 - eb));
+                           : (QD ? 105 : 0) - ((beta + 1022 - ea) + (beta + 1022 - eb));
       }
       const int st = cring.st;
       if (ok && !mbar_wait(&full[st], cring.ph, status, DEV_STATUS_TIMEOUT)) ok = false;
       cring.next<CT_STAGES>();
       cons.next();
       if (ok) {
-        // warp w takes moduli 8w .. 8w+7, lane the entries 4 lane .. 4 lane + 3 of each half
+        // warp w takes moduli 8w .. 8w+7, lane the entries 4 lane .. 4 lane + 3 of each half (QD: each group)
 #pragma unroll
         for (int h = 0; h < 2; h++) {
-          const uint8_t* r = sR + st * 32 * CT_TILE + 128 * h + 4 * lane;
+          const uint8_t* r = sR + st * 32 * CT_TILE + HALF * h + 4 * lane;
           uint32_t wv[8];
 #pragma unroll
           for (int v = 0; v < 8; v++) {
             const int l = 8 * warp + v;
-            wv[v] = l < LC ? *reinterpret_cast<const uint32_t*>(r + l * CT_TILE) : 0u;
+            wv[v] = l < LC ? *reinterpret_cast<const uint32_t*>(r + l * PS) : 0u;
           }
           // entry e's bytes of moduli 8w .. 8w+7 -> row 4 lane + e, bytes 8w .. 8w+7
           uint8_t* a = sA + h * 128 * 32;
@@ -1644,12 +1703,19 @@ __global__ void __launch_bounds__(CT_THREADS, 4)
       tmem_ld_32x32b_x32(col, acc0);
       tmem_ld_32x32b_x32(col + 32u, acc1);
       tmem_wait_ld();
-      const double2 nan2 = make_double2(__longlong_as_double(0x7ff8000000000000ll), 0.0);
+      const double nan = __longlong_as_double(0x7ff8000000000000ll);
       const int64_t ja = j0 + t, jb = j0 + 128 + t;
-      const double2 ra = shift_prev[0] == INT32_MIN ? nan2 : crt_tc_entry(acc0, T, shift_prev[0]);
-      const double2 rb = shift_prev[1] == INT32_MIN ? nan2 : crt_tc_entry(acc1, T, shift_prev[1]);
-      if (ja < n) C[i * n + ja] = ra;
-      if (jb < n) C[i * n + jb] = rb;
+      if constexpr (QD) {
+        const double4 r = shift_prev[0] == INT32_MIN ? make_double4(nan, 0.0, 0.0, 0.0)
+                                                     : crt_tc_entry_qd(acc0, acc1, T, shift_prev[0]);
+        if (ja < n) C[i * n + ja] = r;
+      } else {
+        const double2 nan2 = make_double2(nan, 0.0);
+        const double2 ra = shift_prev[0] == INT32_MIN ? nan2 : crt_tc_entry(acc0, T, shift_prev[0]);
+        const double2 rb = shift_prev[1] == INT32_MIN ? nan2 : crt_tc_entry(acc1, T, shift_prev[1]);
+        if (ja < n) C[i * n + ja] = ra;
+        if (jb < n) C[i * n + jb] = rb;
+      }
     }
     shift_prev[0] = shift_cur[0];
     shift_prev[1] = shift_cur[1];
@@ -1793,6 +1859,57 @@ static int launch_crt_tc(const uint8_t* cres, size_t Mp, size_t Np, size_t m, si
   }
   HP_CRT_TC(28) HP_CRT_TC(29) HP_CRT_TC(30) HP_CRT_TC(31) HP_CRT_TC(32)
 #undef HP_CRT_TC
+  return HP_ERR_UNSUPPORTED;
+}
+
+// The f256 GEMM's CRT on the tensor core: g holds G1's L planes of Mp x Np
+// bytes followed by G2's. HP_ERR_UNSUPPORTED (nothing launched) for L
+// outside 28..32 or Np not a multiple of 128.
+static int launch_crt_tc_qd(const uint8_t* g, size_t Mp, size_t Np, size_t m, size_t n, const int* expA,
+                            const int* expB, int beta, int L, double4* C, int num_sms, uint32_t* status,
+                            cudaStream_t s) {
+  if (L < CRT_CONST_L0 || L >= CRT_CONST_L0 + CRT_CONST_N || Np % 128 != 0) {
+    set_error("ozaki f256: no tensor-core CRT for %d moduli", L);
+    return HP_ERR_UNSUPPORTED;
+  }
+  static bool attr_set[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (!attr_set[dev & 63]) {
+    HP_CUDA_TRY(cudaFuncSetAttribute(crt_tc_kernel<28, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, CT_SMEM));
+    HP_CUDA_TRY(cudaFuncSetAttribute(crt_tc_kernel<29, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, CT_SMEM));
+    HP_CUDA_TRY(cudaFuncSetAttribute(crt_tc_kernel<30, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, CT_SMEM));
+    HP_CUDA_TRY(cudaFuncSetAttribute(crt_tc_kernel<31, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, CT_SMEM));
+    HP_CUDA_TRY(cudaFuncSetAttribute(crt_tc_kernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, CT_SMEM));
+    attr_set[dev & 63] = true;
+  }
+  // 2L planes of Mp x Np bytes; one box is 128 residues of one row in L consecutive planes
+  auto fn = encode_fn();
+  if (!fn) {
+    set_error("cuTensorMapEncodeTiled unavailable");
+    return HP_ERR_CUDA;
+  }
+  CUtensorMap map;
+  cuuint64_t dims[3] = {Np, Mp, (cuuint64_t)(2 * L)};
+  cuuint64_t strides[2] = {Np, Np * Mp};
+  cuuint32_t box[3] = {128, 1, (cuuint32_t)L};
+  cuuint32_t estr[3] = {1, 1, 1};
+  CUresult rc = fn(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<uint8_t*>(g), dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (rc != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed (%d)", (int)rc);
+    return HP_ERR_CUDA;
+  }
+  const int grid = num_sms * 4;
+#define HP_CRT_TCQ(LCV)                                                                                       \
+  if (L == LCV) {                                                                                             \
+    HP_CUDA_TRY(launch_k(true, crt_tc_kernel<LCV, true>, dim3(grid), dim3(CT_THREADS), CT_SMEM, s, map,        \
+                         (int64_t)m, (int64_t)n, expA, expB, beta, C, status));                               \
+    return HP_OK;                                                                                             \
+  }
+  HP_CRT_TCQ(28) HP_CRT_TCQ(29) HP_CRT_TCQ(30) HP_CRT_TCQ(31) HP_CRT_TCQ(32)
+#undef HP_CRT_TCQ
   return HP_ERR_UNSUPPORTED;
 }
 
@@ -2683,8 +2800,8 @@ int ozaki_qd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
   const size_t Mp = round_up(m, GB_M), Np = round_up(n, GB_N), Kp = round_up(k, GB_K);
   DevBuf exps((Mp + Np) * sizeof(int), s);
   DevBuf ares((size_t)L * Mp * 2 * Kp, s), bres((size_t)L * Np * 2 * Kp, s);
-  DevBuf g1((size_t)L * Mp * Np, s), g2((size_t)L * Mp * Np, s);
-  if (!exps.p || !ares.p || !bres.p || !g1.p || !g2.p) {
+  DevBuf gg((size_t)2 * L * Mp * Np, s);  // G1's residue planes, then G2's
+  if (!exps.p || !ares.p || !bres.p || !gg.p) {
     set_error("ozaki f256: workspace allocation failed");
     return HP_ERR_CUDA;
   }
@@ -2726,18 +2843,23 @@ int ozaki_qd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
 #undef HP_RESQ_L
 #undef HP_RESQ
   }
+  uint8_t* g1 = gg.as<uint8_t>();
+  uint8_t* g2 = g1 + (size_t)L * Mp * Np;
   // G1 = Xh Yh: A bytes [0, Kp), B bytes [Kp, 2Kp)
-  HP_TRY(ozaki_residue_gemm_k(ares.as<int8_t>(), bres.as<int8_t>(), g1.as<uint8_t>(), L, Mp, Np, 2 * Kp, 2 * Kp, 0, Kp,
+  HP_TRY(ozaki_residue_gemm_k(ares.as<int8_t>(), bres.as<int8_t>(), g1, L, Mp, Np, 2 * Kp, 2 * Kp, 0, Kp,
                               Kp, Np, Mp * Np, 0, 0, 0, s, Mp, Np, true, true));
   // G2 = [Xh | Xl] [Yl ; Yh]: both over [0, 2Kp)
-  HP_TRY(ozaki_residue_gemm_k(ares.as<int8_t>(), bres.as<int8_t>(), g2.as<uint8_t>(), L, Mp, Np, 2 * Kp, 2 * Kp, 0,
+  HP_TRY(ozaki_residue_gemm_k(ares.as<int8_t>(), bres.as<int8_t>(), g2, L, Mp, Np, 2 * Kp, 2 * Kp, 0,
                               2 * Kp, 0, Np, Mp * Np, 0, 0, 0, s, Mp, Np, false, true));
-  const int nc = host_tables().crt[L].nc;
+  const int rc = launch_crt_tc_qd(g1, Mp, Np, m, n, expAp, expBp, BETA_QD, L, reinterpret_cast<double4*>(c),
+                                  D->num_sms, status, s);
+  if (rc != HP_ERR_UNSUPPORTED) return rc;
+  const int nc = host_tables().crt[L].nc;  // the FP64 CRT for other moduli counts
   const unsigned grid = (unsigned)((m * n + 255) / 256);
 #define HP_CRTQ_LC(NCV, LCV)                                                                                       \
   if (nc == NCV && L == LCV) {                                                                                     \
     HP_CUDA_TRY(launch_k(true, crt_qd_kernel<NCV, LCV>, dim3(grid), dim3(256), 0, s,                                \
-                         (const uint8_t*)g1.as<uint8_t>(), (const uint8_t*)g2.as<uint8_t>(), (int64_t)(Mp * Np),     \
+                         (const uint8_t*)g1, (const uint8_t*)g2, (int64_t)(Mp * Np),                               \
                          (int64_t)Np, (int64_t)m, (int64_t)n, (const int*)expAp, (const int*)expBp,                 \
                          (const CrtTable*)(D->crt + L), reinterpret_cast<double4*>(c)));                            \
     return HP_OK;                                                                                                  \
@@ -2747,8 +2869,8 @@ int ozaki_qd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
 #undef HP_CRTQ_LC
 #define HP_CRTQ(NC)                                                                                                  \
   case NC:                                                                                                           \
-    HP_CUDA_TRY(launch_k(true, crt_qd_kernel<NC>, dim3(grid), dim3(256), 0, s, (const uint8_t*)g1.as<uint8_t>(),     \
-                         (const uint8_t*)g2.as<uint8_t>(), (int64_t)(Mp * Np), (int64_t)Np, (int64_t)m, (int64_t)n,  \
+    HP_CUDA_TRY(launch_k(true, crt_qd_kernel<NC>, dim3(grid), dim3(256), 0, s, (const uint8_t*)g1,                   \
+                         (const uint8_t*)g2, (int64_t)(Mp * Np), (int64_t)Np, (int64_t)m, (int64_t)n,  \
                          (const int*)expAp, (const int*)expBp, (const CrtTable*)(D->crt + L),               \
                          reinterpret_cast<double4*>(c)));                                                            \
     break;

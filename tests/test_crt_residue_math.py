@@ -159,9 +159,11 @@ def test_f256_crt_combination(L):
     mods, M, W, wb, mlimb, k192 = tables
     rng = random.Random(200 + L)
     bound = M // 4
-    for _ in range(200):
-        G1 = rng.randrange(-bound, bound + 1)
-        G2 = rng.randrange(-bound, bound + 1)
+    pairs = [(0, 0), (0, 1), (0, -1), (1, -(1 << 105) + 3), (-1, (1 << 105) - 5), (bound, bound), (-bound, -bound),
+             (1 << 100, -(1 << 205)), (3, -(3 << 105))]
+    pairs += [(rng.randrange(-bound, bound + 1), rng.randrange(-bound, bound + 1)) for _ in range(200)]
+    pairs += [(rng.randrange(-(1 << 40), 1 << 40), rng.randrange(-(1 << 100), 1 << 100)) for _ in range(100)]
+    for G1, G2 in pairs:
         b1 = crt_tc([G1 % m for m in mods], L, tables)[3]
         b2 = crt_tc([G2 % m for m in mods], L, tables)[3]
         c = [0] * 9
@@ -189,4 +191,6 @@ def test_f256_crt_combination(L):
         x[1], x[2] = two_sum(x[1], x[2])
         x[2], x[3] = two_sum(x[2], x[3])
         got = sum(Fraction(v) for v in x)
-        assert abs(got - C) <= abs(Fraction(C)) * Fraction(1, 1 << 206) + 1, (L, C)
+        assert abs(got - C) <= abs(Fraction(C)) * Fraction(1, 1 << 206), (L, C)
+        if abs(C) < (1 << 150):
+            assert got == C, (L, C)

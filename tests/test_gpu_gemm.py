@@ -216,6 +216,73 @@ def test_f256_ozaki_exact_small_integers(gpu):
     assert np.array_equal(c[..., 0], A[..., 0] @ B[..., 0]) and np.all(c[..., 1:] == 0)
 
 
+def qd_abs_prod(a, b, atb):
+    A = np.abs(a[..., 0])
+    return (A.T if atb else A) @ np.abs(b[..., 0])
+
+
+def qd_entry_err(c, ref):
+    return np.abs(((c[..., 0] - ref[..., 0]) + (c[..., 1] - ref[..., 1])) + ((c[..., 2] - ref[..., 2]) + (c[..., 3] - ref[..., 3])))
+
+
+@pytest.mark.parametrize("atb", [False, True])
+def test_f256_ozaki_ragged_tiles(gpu, atb):
+    """Rows and columns over several 128-entry CRT tiles and 128-row residue
+    tiles, none a multiple of the tile sizes: every entry within the
+    entrywise bound 4 k 2^-208 |A| |B|."""
+    m, n, k = 140, 300, 150
+    a = qd_operand(k, m, 41) if atb else qd_operand(m, k, 41)
+    b = qd_operand(k, n, 43)
+    c = gpu.f256_gemm(a, b, m, n, k, gpu.OZAKI, atb)
+    ref = O.mf_gemm(4, a, b, m, n, k, atb=atb)
+    assert np.all(qd_entry_err(c, ref) <= 4 * k * 2.0 ** -208 * qd_abs_prod(a, b, atb) + 1e-300)
+
+
+@pytest.mark.parametrize("k", [1, 128, 129, 16384])
+def test_f256_ozaki_moduli_count_boundaries(gpu, k):
+    """The f256 GEMM needs 28 moduli at k = 1, 29 up to k = 128, 30 from 129
+    (to 8192) and 31 from 16384 (to 2^20): each count its tensor-core
+    residue and CRT kernels are built for."""
+    m, n = 8, 12
+    a = qd_operand(m, k, 51)
+    b = qd_operand(k, n, 53)
+    c = gpu.f256_gemm(a, b, m, n, k, gpu.OZAKI)
+    ref = O.mf_gemm(4, a, b, m, n, k)
+    assert np.all(qd_entry_err(c, ref) <= 4 * k * 2.0 ** -208 * qd_abs_prod(a, b, False) + 1e-300)
+
+
+@pytest.mark.parametrize("atb", [False, True])
+def test_f256_ozaki_nonfinite_rows_and_columns(gpu, atb):
+    """An inf or NaN limb in a row of op(A) or a column of B makes that row or
+    column of the f256 product NaN; the other entries are the finite product."""
+    m, n, k = 70, 140, 60
+    a = qd_operand(k, m, 61) if atb else qd_operand(m, k, 61)
+    b = qd_operand(k, n, 63)
+    bad_rows, bad_cols = [3, 5, 69], [2, 130]
+    at = (lambda r, p: (p, r)) if atb else (lambda r, p: (r, p))
+    a[at(3, 10)][0] = np.nan
+    a[at(5, 0)][2] = np.inf        # a lower limb only
+    a[at(69, 59)][0] = -np.inf
+    b[4, 2, 3] = np.nan
+    b[8, 130, 0] = np.inf
+    c = gpu.f256_gemm(a, b, m, n, k, gpu.OZAKI, atb)
+    assert np.all(np.isnan(c[bad_rows, :, 0])) and np.all(np.isnan(c[:, bad_cols, 0]))
+    a0, b0 = a.copy(), b.copy()
+    for r in bad_rows:
+        if atb:
+            a0[:, r] = 0.0
+        else:
+            a0[r] = 0.0
+    b0[:, bad_cols] = 0.0
+    ref = O.mf_gemm(4, a0, b0, m, n, k, atb=atb)
+    good_r = np.setdiff1d(np.arange(m), bad_rows)
+    good_c = np.setdiff1d(np.arange(n), bad_cols)
+    cg, rg = c[np.ix_(good_r, good_c)], ref[np.ix_(good_r, good_c)]
+    assert np.all(np.isfinite(cg))
+    ab = qd_abs_prod(a0, b0, atb)[np.ix_(good_r, good_c)]
+    assert np.all(qd_entry_err(cg, rg) <= 4 * k * 2.0 ** -208 * ab + 1e-300)
+
+
 @pytest.mark.parametrize("atb", [False, True])
 def test_f128_ozaki_long_k_chunks(gpu, atb):
     """k beyond one accumulation chunk of the unsigned residue GEMM (32768):
