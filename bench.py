@@ -811,6 +811,27 @@ def profile_case_chol512(args):
     return 0
 
 
+def profile_case_f256(args):
+    """Chosen-path f256 GEMMs at m = n = k = 1024 on the benchmark's operands
+    (double-double entries widened to four limbs): the command ncu captures."""
+    import torch
+
+    import quadprec_b200 as hp
+    from quadprec_b200.workloads import dd_to_qd, gemm_operands
+
+    n4 = 1024
+    a, b = gemm_operands(n4, n4, n4, seed=0)
+    A = torch.from_numpy(dd_to_qd(a)).cuda()
+    B = torch.from_numpy(dd_to_qd(b)).cuda()
+    C = torch.empty((n4, n4, 4), dtype=torch.float64, device="cuda")
+    sptr = torch.cuda.current_stream().cuda_stream
+    for _ in range(args.warmup + args.steps):
+        hp.f256_gemm_dev(A, B, C, n4, n4, n4, hp.OZAKI, stream=sptr)
+    torch.cuda.synchronize()
+    print("profile case done", file=sys.stderr)
+    return 0
+
+
 # ---------------------------------------------------------------- main arm
 def main():
     ap = argparse.ArgumentParser()
@@ -824,7 +845,7 @@ def main():
     ap.add_argument("--spd-steps", type=int, default=3)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched SPD / Jacobi section")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint section")
-    ap.add_argument("--profile-case", nargs="?", const="gemm", default=None, choices=["gemm", "spd", "batched", "chol512"],
+    ap.add_argument("--profile-case", nargs="?", const="gemm", default=None, choices=["gemm", "spd", "batched", "chol512", "f256"],
                     help="only run warmup + steps of one chosen-path workload (for ncu captures)")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -835,6 +856,8 @@ def main():
         return profile_case_spd(args)
     if args.profile_case == "chol512":
         return profile_case_chol512(args)
+    if args.profile_case == "f256":
+        return profile_case_f256(args)
     if args.profile_case == "batched":
         import torch
 

@@ -2069,10 +2069,13 @@ int ozaki_residue_gemm_k(const int8_t* ares, const int8_t* bres, uint8_t* cres, 
   return HP_OK;
 }
 
-// Residue GEMM of the f128 GEMM on CTA pairs: cres[l] = (A_l B_l^T) mod m_l for
-// Mp x Np (Mp a multiple of 256, Np of 256), K of ka bytes per row.
+// Residue GEMM on CTA pairs: cres[l] = (A_l B_l^T) mod m_l for Mp x Np (Mp a
+// multiple of 256, Np of 256) over ka bytes of K. Rows are pitch bytes long
+// (ka when 0); the product takes A's bytes [a_k0, a_k0 + ka) and B's
+// [b_k0, b_k0 + ka) of each row (offsets multiples of 128).
 int ozaki_residue_gemm_pair(const int8_t* ares, const int8_t* bres, uint8_t* cres, int L, size_t Mp, size_t Np,
-                            size_t ka, cudaStream_t s, bool pdl, bool u8) {
+                            size_t ka, cudaStream_t s, bool pdl, bool u8, size_t pitch = 0, size_t a_k0 = 0,
+                            size_t b_k0 = 0) {
   using namespace ozaki;
   DevTables* D;
   HP_TRY(device_tables(&D));
@@ -2085,8 +2088,8 @@ int ozaki_residue_gemm_pair(const int8_t* ares, const int8_t* bres, uint8_t* cre
     attr_set[dev] = true;
   }
   CUtensorMap mapA, mapB;
-  HP_TRY(make_map(&mapA, ares, ka, Mp, L, GP_HALF));
-  HP_TRY(make_map(&mapB, bres, ka, Np, L, GP_HALF));
+  HP_TRY(make_map(&mapA, ares + a_k0, ka, Mp, L, GP_HALF, pitch * Mp, pitch));
+  HP_TRY(make_map(&mapB, bres + b_k0, ka, Np, L, GP_HALF, pitch * Np, pitch));
   uint32_t* status = device_status(s);
   if (!status) {
     set_error("status word allocation failed");
@@ -2797,7 +2800,7 @@ int ozaki_qd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
     set_error("ozaki f256: k = %zu needs more moduli than the table holds", k);
     return HP_ERR_UNSUPPORTED;
   }
-  const size_t Mp = round_up(m, GB_M), Np = round_up(n, GB_N), Kp = round_up(k, GB_K);
+  const size_t Mp = round_up(m, GP_M), Np = round_up(n, GP_N), Kp = round_up(k, GB_K);
   DevBuf exps((Mp + Np) * sizeof(int), s);
   DevBuf ares((size_t)L * Mp * 2 * Kp, s), bres((size_t)L * Np * 2 * Kp, s);
   DevBuf gg((size_t)2 * L * Mp * Np, s);  // G1's residue planes, then G2's
@@ -2845,12 +2848,11 @@ int ozaki_qd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
   }
   uint8_t* g1 = gg.as<uint8_t>();
   uint8_t* g2 = g1 + (size_t)L * Mp * Np;
-  // G1 = Xh Yh: A bytes [0, Kp), B bytes [Kp, 2Kp)
-  HP_TRY(ozaki_residue_gemm_k(ares.as<int8_t>(), bres.as<int8_t>(), g1, L, Mp, Np, 2 * Kp, 2 * Kp, 0, Kp,
-                              Kp, Np, Mp * Np, 0, 0, 0, s, Mp, Np, true, true));
+  // on CTA pairs; G1 = Xh Yh: A bytes [0, Kp), B bytes [Kp, 2Kp) of rows 2Kp long
+  HP_TRY(ozaki_residue_gemm_pair(ares.as<int8_t>(), bres.as<int8_t>(), g1, L, Mp, Np, Kp, s, true, true, 2 * Kp, 0,
+                                 Kp));
   // G2 = [Xh | Xl] [Yl ; Yh]: both over [0, 2Kp)
-  HP_TRY(ozaki_residue_gemm_k(ares.as<int8_t>(), bres.as<int8_t>(), g2, L, Mp, Np, 2 * Kp, 2 * Kp, 0,
-                              2 * Kp, 0, Np, Mp * Np, 0, 0, 0, s, Mp, Np, false, true));
+  HP_TRY(ozaki_residue_gemm_pair(ares.as<int8_t>(), bres.as<int8_t>(), g2, L, Mp, Np, 2 * Kp, s, false, true));
   const int rc = launch_crt_tc_qd(g1, Mp, Np, m, n, expAp, expBp, BETA_QD, L, reinterpret_cast<double4*>(c),
                                   D->num_sms, status, s);
   if (rc != HP_ERR_UNSUPPORTED) return rc;
