@@ -302,10 +302,12 @@ __device__ __forceinline__ uint32_t mod_reduce(int32_t x, int l) {
 // Exponent pass of the f128 Ozaki GEMM in one launch. A (RA x CA,
 // row-major) contributes one exponent per row (a_rows) or per column, B
 // (RB x CB) one per column; an entry's exponent is max(e(hi), e(lo) + 1),
-// or the non-finite marker. Row blocks: 8 warps, one row each, MAXEXP_U
-// loads in flight per lane. Column blocks: 32 columns x 8 row lanes over a slab
-// of `slab` rows, merged with atomicMax into outputs zeroed beforehand.
-// Blocks [0, na) serve A, the rest B.
+// or the non-finite marker. Row blocks: 8 warps, each one chunk of `chunk`
+// entries of a row, MAXEXP_U loads in flight per lane. Column blocks: 256
+// consecutive columns, one per thread, over a slab of `slab` rows, so a
+// block's loads of one row cover 256 contiguous entries (DRAM pages are
+// opened for 4-8 KB, not 512 B). Partial maxima merge with atomicMax into
+// outputs zeroed beforehand. Blocks [0, na) serve A, the rest B.
 __device__ __forceinline__ int entry_exp(double2 v) {
   const int el = exp_field(v.y);
   return el == EXP_NONFINITE ? EXP_NONFINITE : max(exp_field(v.x), min(el + 1, EXP_NONFINITE));
@@ -316,11 +318,14 @@ __device__ __forceinline__ int entry_exp(double4 v) {
   if (el == EXP_NONFINITE || exp_field(v.z) == EXP_NONFINITE || exp_field(v.w) == EXP_NONFINITE) return EXP_NONFINITE;
   return max(exp_field(v.x), min(el + 1, EXP_NONFINITE));
 }
-constexpr int MAXEXP_U = 8;  // loads in flight per lane
+constexpr int MAXEXP_U = 8;       // loads in flight per lane
+constexpr int MAXEXP_ROUNDS = 4;  // rounds of MAXEXP_U loads per thread (a row chunk, a column slab)
+constexpr int MAXEXP_COLS = 256;  // columns of a column block
 template <class T>
 __global__ void __launch_bounds__(256) maxexp_kernel(const T* __restrict__ A, int64_t RA, int64_t CA, bool a_rows,
                                                      int* __restrict__ outA, const T* __restrict__ B, int64_t RB,
-                                                     int64_t CB, int* __restrict__ outB, int64_t slab, unsigned na) {
+                                                     int64_t CB, int* __restrict__ outB, int64_t slab, int64_t chunk,
+                                                     unsigned na) {
   sm100::griddep_launch_dependents();
   const bool isA = blockIdx.x < na;
   const unsigned bid = isA ? blockIdx.x : blockIdx.x - na;
@@ -329,41 +334,36 @@ __global__ void __launch_bounds__(256) maxexp_kernel(const T* __restrict__ A, in
   int* out = isA ? outA : outB;
   const int lane = threadIdx.x % 32, wy = threadIdx.x / 32;
   if (isA && a_rows) {
-    const int64_t row = (int64_t)bid * 8 + wy;
+    const int64_t nch = (C + chunk - 1) / chunk;
+    const int64_t item = (int64_t)bid * 8 + wy, row = item / nch;
     if (row >= R) return;
     const T* rp = src + row * C;
+    const int64_t p0 = (item % nch) * chunk, p1 = min(C, p0 + chunk);
     int e = 0;
-    for (int64_t p = lane; p < C; p += 32 * MAXEXP_U) {
+    for (int64_t p = p0 + lane; p < p1; p += 32 * MAXEXP_U) {
       T v[MAXEXP_U];
 #pragma unroll
-      for (int u = 0; u < MAXEXP_U; u++) v[u] = p + 32 * u < C ? rp[p + 32 * u] : T{};
+      for (int u = 0; u < MAXEXP_U; u++) v[u] = p + 32 * u < p1 ? rp[p + 32 * u] : T{};
 #pragma unroll
       for (int u = 0; u < MAXEXP_U; u++) e = max(e, entry_exp(v[u]));
     }
     for (int o = 16; o; o >>= 1) e = max(e, __shfl_xor_sync(0xffffffffu, e, o));
-    if (lane == 0) out[row] = e;
+    if (lane == 0) atomicMax(out + row, e);
     return;
   }
-  __shared__ int red[8][33];
-  const int64_t ncb = (C + 31) / 32;
-  const int64_t c = (int64_t)(bid % ncb) * 32 + lane;
+  const int64_t ncb = (C + MAXEXP_COLS - 1) / MAXEXP_COLS;
+  const int64_t c = (int64_t)(bid % ncb) * MAXEXP_COLS + threadIdx.x;
   const int64_t r0 = (int64_t)(bid / ncb) * slab, r1 = min(R, r0 + slab);
+  if (c >= C) return;
   int e = 0;
-  if (c < C) {
-    for (int64_t r = r0 + wy; r < r1; r += 8 * MAXEXP_U) {
-      T v[MAXEXP_U];
+  for (int64_t r = r0; r < r1; r += MAXEXP_U) {
+    T v[MAXEXP_U];
 #pragma unroll
-      for (int u = 0; u < MAXEXP_U; u++) v[u] = r + 8 * u < r1 ? src[(r + 8 * u) * C + c] : T{};
+    for (int u = 0; u < MAXEXP_U; u++) v[u] = r + u < r1 ? src[(r + u) * C + c] : T{};
 #pragma unroll
-      for (int u = 0; u < MAXEXP_U; u++) e = max(e, entry_exp(v[u]));
-    }
+    for (int u = 0; u < MAXEXP_U; u++) e = max(e, entry_exp(v[u]));
   }
-  red[wy][lane] = e;
-  __syncthreads();
-  if (wy == 0 && c < C) {
-    for (int y = 1; y < 8; y++) e = max(e, red[y][lane]);
-    atomicMax(out + c, e);
-  }
+  atomicMax(out + c, e);
 }
 // Exponents of the f128 GEMM's operands: expA per row of A (per column when
 // atb, A being k x m) and expB per column of B (k x n), both zeroed by the
@@ -371,16 +371,18 @@ __global__ void __launch_bounds__(256) maxexp_kernel(const T* __restrict__ A, in
 template <class T>
 static int launch_maxexp(const T* A, const T* B, size_t m, size_t n, size_t k, bool atb, int* expA, int* expB,
                          cudaStream_t s) {
-  const int64_t slab = 256;
-  const int64_t kslabs = ((int64_t)k + slab - 1) / slab;
-  const int64_t na = atb ? ((int64_t)m + 31) / 32 * kslabs : ((int64_t)m + 7) / 8;
-  const int64_t nb = ((int64_t)n + 31) / 32 * kslabs;
+  const int64_t slab = MAXEXP_ROUNDS * MAXEXP_U, chunk = MAXEXP_ROUNDS * MAXEXP_U * 32;
+  const int64_t kslabs = ((int64_t)k + slab - 1) / slab, kchunks = ((int64_t)k + chunk - 1) / chunk;
+  const int64_t na = atb ? ((int64_t)m + MAXEXP_COLS - 1) / MAXEXP_COLS * kslabs : ((int64_t)m * kchunks + 7) / 8;
+  const int64_t nb = ((int64_t)n + MAXEXP_COLS - 1) / MAXEXP_COLS * kslabs;
   if (na + nb > INT32_MAX) {
     set_error("ozaki: exponent pass grid too large");
     return HP_ERR_INVALID_ARG;
   }
+  if (na + nb == 0) return HP_OK;  // nothing to scan (k, or both m and n, zero)
   maxexp_kernel<T><<<(unsigned)(na + nb), 256, 0, s>>>(A, atb ? (int64_t)k : (int64_t)m, atb ? (int64_t)m : (int64_t)k,
-                                                    !atb, expA, B, (int64_t)k, (int64_t)n, expB, slab, (unsigned)na);
+                                                    !atb, expA, B, (int64_t)k, (int64_t)n, expB, slab, chunk,
+                                                    (unsigned)na);
   HP_LAUNCH_CHECK();
   return HP_OK;
 }
@@ -2341,6 +2343,7 @@ int ozaki_dd_gemm_host(const double* a, const double* b, double* c, size_t m, si
     const double2* A2 = dA.as<const double2>() + r0 * k;
     double* Ci = dC.as<double>() + r0 * n * 2;
     HP_CUDA_TRY(cudaStreamWaitEvent(s, eA[i], 0));
+    HP_CUDA_TRY(cudaMemsetAsync(expA, 0, mi * sizeof(int), s));  // the row maxima merge by atomicMax
     HP_TRY(launch_maxexp(A2, (const double2*)nullptr, mi, 0, k, false, expA, nullptr, s));
     rc = launch_residues_tc(false, L, A2, mi, expA, ares.as<int8_t>(), Mpi, nullptr, 0, nullptr, nullptr, 0, k, Kp,
                             beta, D->num_sms, status, s, pdl);
