@@ -492,6 +492,7 @@ def batched_section(hp, torch, dev, stream, sptr, args, world, dist):
     vec = torch.empty_like(S)
     sw = torch.zeros(len(sel), dtype=torch.int32, device=dev)
     jst = torch.zeros(len(sel), dtype=torch.int32, device=dev)
+    S_host = S.cpu().numpy() if getattr(args, "cpu_leg", False) else None  # the matrices, before the solver runs
     torch.cuda.synchronize()
     s1, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     s1.record(stream)
@@ -506,7 +507,58 @@ def batched_section(hp, torch, dev, stream, sptr, args, world, dist):
     out["jacobi"] = {"matrices": int(len(sel)), "converged": int((jst.cpu().numpy() == 0).sum()), "ms": jms,
                      "matrices_per_s": world * len(sel) * 1e3 / jms, "rotations_per_s": world * rot / (jms * 1e-3),
                      "mean_sweeps": float(sweeps.mean())}
+    if getattr(args, "cpu_leg", False):
+        out["jacobi"]["cpu_baseline"] = cpu_jacobi_sample(S_host, ns[sel], ev.cpu().numpy())
     return out
+
+
+def cpu_jacobi_sample(Sh, ns, evh, stride: int = 64) -> dict:
+    """The reference's jacobi_eigen (crates/quad/src/linalg.rs:299-362,
+    restated in the oracle) on a bounded sample of the batched Jacobi's
+    matrices: every stride-th in size order, on 1 core and on all cores (one
+    matrix per thread), each rate scaled to the whole set by sum n^3. Also the
+    largest eigenvalue difference between the GPU's and the oracle's on the
+    sample (both sorted; the rotation orders differ)."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import numpy as np
+
+    import oracle
+
+    ns = ns.astype(np.int64)
+    soff = np.concatenate([[0], np.cumsum(ns * ns)])
+    eoff = np.concatenate([[0], np.cumsum(ns)])
+    pick = np.argsort(ns, kind="stable")[::stride]
+
+    def one(t):
+        n = int(ns[t])
+        return oracle.jacobi_eigen(Sh[2 * soff[t]:2 * soff[t + 1]].reshape(n, n, 2), n, 200)
+
+    rates, res = {}, None
+    cores = oracle.num_threads()
+    for threads in (1, cores):
+        t0 = time.perf_counter()
+        if threads == 1:
+            res = [one(t) for t in pick]
+        else:
+            with ThreadPoolExecutor(max_workers=threads) as ex:
+                res = list(ex.map(one, pick))
+        rates[threads] = len(pick) / (time.perf_counter() - t0)
+    work = float((ns.astype(np.float64) ** 3).sum() / (ns[pick].astype(np.float64) ** 3).sum())
+    diff = 0.0
+    for t, (ev_c, _, _) in zip(pick, res):
+        g = evh[2 * eoff[t]:2 * eoff[t + 1]].reshape(-1, 2)
+        g = g[np.argsort(g[:, 0] + g[:, 1])]
+        c = ev_c[np.argsort(ev_c[:, 0] + ev_c[:, 1])]
+        d = np.abs((g[:, 0] - c[:, 0]) + (g[:, 1] - c[:, 1]))
+        diff = max(diff, float(d.max() / np.abs(c[:, 0]).max()))
+    whole = len(ns) / (len(pick) * work)  # sample rate -> matrices/s of the whole set
+    return {"value": rates[cores] * whole, "unit": "matrices/s", "cores": cores,
+            "kind": "port", "value_1_core": rates[1] * whole,
+            "max_eigenvalue_diff_over_max_vs_gpu": diff,
+            "sample": f"{len(pick)} of {len(ns)} matrices (every {stride}th in size order, n {int(ns[pick].min())}-"
+                      f"{int(ns[pick].max())}), the reference's cyclic jacobi_eigen, rate scaled to the set by "
+                      "sum n^3"}
 
 
 ADJ_LATTICE = (5, 5, 10)  # 250 centres x 4 exponents = 1000 basis functions
@@ -541,10 +593,24 @@ def cpu_batched_sample(B, target_s: float = 15.0) -> dict:
     w_all = float((ns.astype(np.float64) ** 3).sum())
     w_sub = float((ns[sel].astype(np.float64) ** 3).sum())
     est = dt * w_all / w_sub
+    # one core on a sparser sample (every 8th system of the one above)
+    sel1 = sel[::8]
+    sub1 = {"offsets": np.concatenate([[0], np.cumsum(ns[sel1])]).astype(np.int64),
+            "centers": np.concatenate([B["centers"][off[i]:off[i + 1]] for i in sel1]),
+            "alpha": np.concatenate([B["alpha"][off[i]:off[i + 1]] for i in sel1]),
+            "b": np.concatenate([B["b"][off[i]:off[i + 1]] for i in sel1])}
+    prev = oracle.num_threads()
+    oracle.set_threads(1)
+    t0 = time.perf_counter()
+    oracle.batched_refined(sub1)
+    dt1 = time.perf_counter() - t0
+    oracle.set_threads(prev)
+    est1 = dt1 * w_all / float((ns[sel1].astype(np.float64) ** 3).sum())
     return {"value": len(ns) / est, "unit": "systems/s", "cores": oracle.num_threads(), "kind": "port",
+            "value_1_core": len(ns) / est1,
             "sample": f"{len(sel)} of {len(ns)} systems (every {stride}th in size order, n {int(ns[sel].min())}-"
                       f"{int(ns[sel].max())}), {dt:.2f} s, scaled to the batch by sum n^3; all steps converged: "
-                      f"{bool((it > 0).all())}"}
+                      f"{bool((it > 0).all())}; 1 core: {len(sel1)} systems (every {8 * stride}th), {dt1:.2f} s"}
 
 
 def adjoint_fd_error(gR, ga):
@@ -623,6 +689,12 @@ def adjoint_section(hp, torch, dev, stream, sptr, args, world, dist):
         t0 = time.perf_counter()
         _, cgR, cga = oracle.adjoint_f128_refined(cen, alpha, b, co, nc)
         dt = time.perf_counter() - t0
+        prev = oracle.num_threads()
+        oracle.set_threads(1)
+        t0 = time.perf_counter()
+        oracle.adjoint_f128_refined(cen, alpha, b, co, nc)
+        dt1 = time.perf_counter() - t0
+        oracle.set_threads(prev)
         # every component of both GPU gradients against the oracle's full f128 gradient
         ref = np.concatenate([np.asarray(cgR).reshape(-1, 2)[:, 0], np.asarray(cga).reshape(-1, 2)[:, 0]])
         scale = float(np.max(np.abs(ref)))
@@ -635,8 +707,10 @@ def adjoint_section(hp, torch, dev, stream, sptr, args, world, dist):
                 "reference": "the oracle's full gradient (reference f128 cholesky + solve_cholesky, f256 residuals, "
                              "f128 contraction)"}
         out["cpu_baseline"] = {"value": 1.0 / dt, "unit": "gradients/s", "cores": oracle.num_threads(),
-                               "kind": "port", "accuracy_vs_f256_fd": adjoint_fd_error(cgR, cga),
-                               "sample": f"one full gradient, {dt:.2f} s: S in f128, lambda from the reference's "
+                               "kind": "port", "value_1_core": 1.0 / dt1,
+                               "accuracy_vs_f256_fd": adjoint_fd_error(cgR, cga),
+                               "sample": f"one full gradient, {dt:.2f} s ({dt1:.2f} s on 1 core): S in f128, lambda "
+                                         "from the reference's "
                                          "f128 cholesky + solve_cholesky refined with f256 residuals, then the "
                                          "f128 contraction -lambda^T dS lambda (OpenMP rows)"}
     return out
@@ -750,10 +824,16 @@ def cpu_spd_sample() -> dict:
 
     cen, alpha, b = overlap_spd_problem(*SPD_LATTICE, seed=0)
     n = len(alpha)
-    t0 = time.perf_counter()
-    S = oracle.overlap_norm_dd(cen, alpha)
-    x, steps = oracle.spd_solve_refined(S, b, n)
-    dt = time.perf_counter() - t0
+    times = {}
+    prev = oracle.num_threads()
+    for cores in (prev, 1):
+        oracle.set_threads(cores)
+        t0 = time.perf_counter()
+        S = oracle.overlap_norm_dd(cen, alpha)
+        x, steps = oracle.spd_solve_refined(S, b, n)
+        times[cores] = time.perf_counter() - t0
+    oracle.set_threads(prev)
+    dt = times[prev]
     fix = os.path.join(REPO, "tests", "golden", "overlap_5x10x10.npz")
     err = None
     if os.path.exists(fix):
@@ -761,10 +841,11 @@ def cpu_spd_sample() -> dict:
         d = (xs[:, 0] - x[:, 0]) + (xs[:, 1] - x[:, 1]) + xs[:, 2] + xs[:, 3]
         err = float(np.linalg.norm(d) / np.linalg.norm(xs[:, 0]))
     return {"value": 1.0 / dt, "unit": "solves/s", "cores": oracle.num_threads(), "kind": "port",
-            "rel_err_vs_f512": err,
-            "sample": f"one full solve of the same n={n} system, {dt:.2f} s: assembly of S in f128, the reference's "
-                      f"f128 cholesky + solve_cholesky (crates/quad/src/linalg.rs:42-126) and {steps} refinement "
-                      "steps with f256 residuals (mf_gemv semantics, multifloat/linalg.rs:17-37), OpenMP rows"}
+            "value_1_core": 1.0 / times[1], "rel_err_vs_f512": err,
+            "sample": f"one full solve of the same n={n} system, {dt:.2f} s ({times[1]:.2f} s on 1 core): assembly "
+                      "of S in f128, the reference's f128 cholesky + solve_cholesky (crates/quad/src/linalg.rs:42-126) "
+                      f"and {steps} refinement steps with f256 residuals (mf_gemv semantics, "
+                      "multifloat/linalg.rs:17-37), OpenMP rows"}
 
 
 def profile_case_spd(args):
