@@ -1,4 +1,4 @@
-"""The arithmetic of the f128 Ozaki GEMM's tensor-core residue and CRT kernels
+"""The arithmetic of the f128 and f256 Ozaki GEMMs' tensor-core residue and CRT kernels
 (ozaki.cu residue_tc_kernel, crt_tc_kernel), restated in Python and checked
 with exact integers on the CPU, for every moduli count those kernels serve
 (28..32):
@@ -13,7 +13,9 @@ with exact integers on the CPU, for every moduli count those kernels serve
   the quotient estimate q = rint(top limbs * 2^192/M) is the exact
   (V - C) / M, the digits d_h = U_h - q M_h carried into balanced 48-bit
   chunks |b_k| <= 2^47 rebuild C exactly, and their double-double sum from
-  the top (quick two-sums) is C to f128 accuracy.
+  the top (quick two-sums) is C to f128 accuracy;
+* f256 CRT: two groups' chunks combine exactly into G1 2^105 + G2 as nine
+  balanced chunks, whose four-limb sum is C to ~2^-206 (exactly below 2^150).
 """
 import math
 import random
