@@ -1577,7 +1577,7 @@ template <int LC, bool QD = false>
 __global__ void __launch_bounds__(CT_THREADS, 4)
     crt_tc_kernel(const __grid_constant__ CUtensorMap map, int64_t m, int64_t n, const int* __restrict__ expA,
                   const int* __restrict__ expB, int beta, std::conditional_t<QD, double4, double2>* __restrict__ C,
-                  uint32_t* status) {
+                  int64_t ldc, uint32_t* status) {
   using namespace sm100;
   constexpr int TW = QD ? 128 : CT_TILE;        // entries of a row per tile
   constexpr int PS = QD ? 128 : CT_TILE;        // bytes between two moduli's residues in a stage
@@ -1710,13 +1710,13 @@ __global__ void __launch_bounds__(CT_THREADS, 4)
       if constexpr (QD) {
         const double4 r = shift_prev[0] == INT32_MIN ? make_double4(nan, 0.0, 0.0, 0.0)
                                                      : crt_tc_entry_qd(acc0, acc1, T, shift_prev[0]);
-        if (ja < n) C[i * n + ja] = r;
+        if (ja < n) C[i * ldc + ja] = r;
       } else {
         const double2 nan2 = make_double2(nan, 0.0);
         const double2 ra = shift_prev[0] == INT32_MIN ? nan2 : crt_tc_entry(acc0, T, shift_prev[0]);
         const double2 rb = shift_prev[1] == INT32_MIN ? nan2 : crt_tc_entry(acc1, T, shift_prev[1]);
-        if (ja < n) C[i * n + ja] = ra;
-        if (jb < n) C[i * n + jb] = rb;
+        if (ja < n) C[i * ldc + ja] = ra;
+        if (jb < n) C[i * ldc + jb] = rb;
       }
     }
     shift_prev[0] = shift_cur[0];
@@ -1815,10 +1815,11 @@ static int launch_crt_dd(const uint8_t* cres, size_t Mp, size_t Np, size_t m, si
 }
 
 // The tensor-core CRT for L = 28..32 (the counts k <= 2^20 needs at beta =
-// 106); HP_ERR_UNSUPPORTED for other L. Np must be a multiple of 256.
+// 106); HP_ERR_UNSUPPORTED for other L. Np must be a multiple of 256. Row i
+// of the m x n result goes to C + i ldc (ldc = n when 0).
 static int launch_crt_tc(const uint8_t* cres, size_t Mp, size_t Np, size_t m, size_t n, const int* expA,
                          const int* expB, int beta, int L, double2* C, int num_sms, uint32_t* status, cudaStream_t s,
-                         bool pdl) {
+                         bool pdl, size_t ldc = 0) {
   if (L < CRT_CONST_L0 || L >= CRT_CONST_L0 + CRT_CONST_N || Np % CT_TILE != 0) {
     set_error("ozaki: no tensor-core CRT for %d moduli", L);
     return HP_ERR_UNSUPPORTED;
@@ -1856,7 +1857,7 @@ static int launch_crt_tc(const uint8_t* cres, size_t Mp, size_t Np, size_t m, si
 #define HP_CRT_TC(LCV)                                                                                        \
   if (L == LCV) {                                                                                             \
     HP_CUDA_TRY(launch_k(pdl, crt_tc_kernel<LCV>, dim3(grid), dim3(CT_THREADS), CT_SMEM, s, map, (int64_t)m,  \
-                         (int64_t)n, expA, expB, beta, C, status));                                           \
+                         (int64_t)n, expA, expB, beta, C, (int64_t)(ldc ? ldc : n), status));                 \
     return HP_OK;                                                                                             \
   }
   HP_CRT_TC(28) HP_CRT_TC(29) HP_CRT_TC(30) HP_CRT_TC(31) HP_CRT_TC(32)
@@ -1907,7 +1908,7 @@ static int launch_crt_tc_qd(const uint8_t* g, size_t Mp, size_t Np, size_t m, si
 #define HP_CRT_TCQ(LCV)                                                                                       \
   if (L == LCV) {                                                                                             \
     HP_CUDA_TRY(launch_k(true, crt_tc_kernel<LCV, true>, dim3(grid), dim3(CT_THREADS), CT_SMEM, s, map,        \
-                         (int64_t)m, (int64_t)n, expA, expB, beta, C, status));                               \
+                         (int64_t)m, (int64_t)n, expA, expB, beta, C, (int64_t)n, status));                   \
     return HP_OK;                                                                                             \
   }
   HP_CRT_TCQ(28) HP_CRT_TCQ(29) HP_CRT_TCQ(30) HP_CRT_TCQ(31) HP_CRT_TCQ(32)
@@ -2232,13 +2233,20 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
 }
 
 // Host-pointer f128 GEMM C = A B (chosen mode) with the PCIe copies
-// overlapped: B goes to the device first and its exponents and residue
-// planes are formed once; A then streams in as row panels on a copy stream,
-// each panel's exponents, residues, residue GEMM and CRT run on the library
-// stream as soon as its rows have landed, and each finished panel of C goes
-// back on a second copy stream while the next panels are computed. The
-// arithmetic of every entry is that of ozaki_dd_gemm (same exponents,
-// residues and CRT), so the result is bit-identical to the one-shot path.
+// overlapped. A streams in as row panels and B as column panels (two for
+// n >= 1024, else one) on a copy stream, in the order the blocks use them:
+// B's first panel, A's first panel, B's other panels, A's other panels.
+// Each panel's exponents and residue planes are formed once, as soon as its
+// entries have landed. Each block of C (row panel x column panel) then takes
+// a residue GEMM and the CRT on the library stream and goes back on a second
+// copy stream while the next blocks are computed. Splitting B lets results
+// start to flow back after half of B instead of all of it. The host link
+// carries both directions at once, but at ~79 GB/s together against ~55 one
+// way, so the time spent copying in before the first result can go back
+// sets most of the overhead (2048^3: 3.2 -> 2.98 ms per call; four column
+// panels measured 3.1). The arithmetic of every entry is that of
+// ozaki_dd_gemm (same exponents, residues and CRT), so the result is
+// bit-identical to the one-shot path.
 namespace {
 struct StreamsDrain {  // every stream idle before the buffers above it are freed
   cudaStream_t a, b, c;
@@ -2279,95 +2287,130 @@ int ozaki_dd_gemm_host(const double* a, const double* b, double* c, size_t m, si
     set_error("ozaki: k = %zu needs more moduli than the table holds", k);
     return HP_ERR_UNSUPPORTED;
   }
-  const size_t Np = round_up(n, GB_N), Kp = round_up(k, GB_K);
+  const bool tc_crt = L >= CRT_CONST_L0 && L < CRT_CONST_L0 + CRT_CONST_N;
+  const size_t Kp = round_up(k, GB_K);
   const size_t panels_wanted = m >= 2048 ? 16 : m >= 1024 ? 8 : 4;
-  const size_t pr = round_up((m + panels_wanted - 1) / panels_wanted, GP_M);  // rows per panel (CTA-pair tiles)
+  const size_t pr = round_up((m + panels_wanted - 1) / panels_wanted, GP_M);  // rows per A panel (CTA-pair tiles)
   const size_t np = (m + pr - 1) / pr;
-  if (pr / GB_M * (Np / GB_N) * (size_t)L > (size_t)INT32_MAX || Kp > (size_t)INT32_MAX) {
+  // B and C in column panels when n is wide: the first C blocks then need only
+  // B's first panel and A's first panel, so results start to flow back while
+  // most of the operands are still on their way in (the host link carries
+  // both directions at once, but not at twice one direction's rate). The
+  // FP64 CRT writes whole rows, so without the tensor-core CRT: one panel.
+  const size_t nq_wanted = (tc_crt && n >= 1024) ? 2 : 1;  // four measured slower (more, smaller blocks)
+  const size_t pc = round_up((n + nq_wanted - 1) / nq_wanted, GP_N);  // columns per B panel
+  const size_t nq = (n + pc - 1) / pc;
+  const size_t Mpa = np * pr;  // rows of A's residue planes, every panel padded to pr
+  if (pr / GB_M * (pc / GB_N) * (size_t)L > (size_t)INT32_MAX || Kp > (size_t)INT32_MAX) {
     set_error("ozaki: problem too large");
     return HP_ERR_INVALID_ARG;
   }
   cudaStream_t s = library_stream(), sin = library_copy_stream(0), sout = library_copy_stream(1);
   DevBuf dA(m * k * 16, s), dB(k * n * 16, s), dC(m * n * 16, s);
-  DevBuf exps((pr + Np) * sizeof(int), s);
-  DevBuf bres((size_t)L * Np * Kp, s), ares((size_t)L * pr * Kp, s), cres((size_t)L * pr * Np, s);
+  DevBuf exps((Mpa + nq * pc) * sizeof(int), s);
+  DevBuf bres((size_t)L * nq * pc * Kp, s), ares((size_t)L * Mpa * Kp, s), cres((size_t)L * pr * pc, s);
   if (!dA.p || !dB.p || !dC.p || !exps.p || !bres.p || !ares.p || !cres.p) {
     set_error("ozaki: workspace allocation failed");
     return HP_ERR_CUDA;
   }
-  EventSet ev(2 * np + 2);
+  EventSet ev(1 + nq + np + np * nq);
   if (!ev.ok()) {
     set_error("ozaki: event creation failed");
     return HP_ERR_CUDA;
   }
   StreamsDrain drain{s, sin, sout};
-  cudaEvent_t ready = ev.ev[0], eB = ev.ev[1];
-  cudaEvent_t* eA = ev.ev.data() + 2;
-  cudaEvent_t* eC = eA + np;
-  int* expA = exps.as<int>();
-  int* expB = expA + pr;
+  cudaEvent_t ready = ev.ev[0];
+  cudaEvent_t* eB = ev.ev.data() + 1;  // B panel j copied
+  cudaEvent_t* eA = eB + nq;           // A panel i copied
+  cudaEvent_t* eC = eA + np;           // C block (i, j) written
+  int* expA = exps.as<int>();          // every row's exponent (panel i at i pr)
+  int* expB = expA + Mpa;              // every column's (panel j at j pc)
   const bool pdl = !profiling_on();
   // the buffers exist (stream-ordered) before the copy streams touch them
   HP_CUDA_TRY(cudaEventRecord(ready, s));
+  profile_mark(s, "start");  // with profiling on: a timeline of the copies in, the blocks and the copies out
   HP_CUDA_TRY(cudaStreamWaitEvent(sin, ready, 0));
   HP_CUDA_TRY(cudaStreamWaitEvent(sout, ready, 0));
-  HP_CUDA_TRY(cudaMemcpyAsync(dB.p, b, k * n * 16, cudaMemcpyHostToDevice, sin));
-  HP_CUDA_TRY(cudaEventRecord(eB, sin));
-  for (size_t i = 0; i < np; i++) {
+  // copies in, in the order the blocks use them: B panel 0, A panel 0, B's
+  // other panels, A's other panels. B panel j (columns j pc ..) is stored as
+  // a compact k x nj matrix.
+  auto copy_b = [&](size_t j) -> int {
+    const size_t j0 = j * pc, nj = std::min(pc, n - j0);
+    HP_CUDA_TRY(cudaMemcpy2DAsync(dB.as<char>() + j0 * k * 16, nj * 16, reinterpret_cast<const char*>(b) + j0 * 16,
+                                  n * 16, nj * 16, k, cudaMemcpyHostToDevice, sin));
+    HP_CUDA_TRY(cudaEventRecord(eB[j], sin));
+    return HP_OK;
+  };
+  auto copy_a = [&](size_t i) -> int {
     const size_t r0 = i * pr, mi = std::min(pr, m - r0);
     HP_CUDA_TRY(cudaMemcpyAsync(dA.as<char>() + r0 * k * 16, reinterpret_cast<const char*>(a) + r0 * k * 16,
                                 mi * k * 16, cudaMemcpyHostToDevice, sin));
     HP_CUDA_TRY(cudaEventRecord(eA[i], sin));
-  }
-  // B once: column exponents and residue planes
-  HP_CUDA_TRY(cudaStreamWaitEvent(s, eB, 0));
-  HP_CUDA_TRY(cudaMemsetAsync(expB, 0, Np * sizeof(int), s));
-  const double2* B2 = dB.as<const double2>();
-  HP_TRY(launch_maxexp((const double2*)nullptr, B2, 0, n, k, false, nullptr, expB, s));
+    return HP_OK;
+  };
+  HP_TRY(copy_b(0));
+  profile_mark(sin, "b0_in");
+  HP_TRY(copy_a(0));
+  for (size_t j = 1; j < nq; j++) HP_TRY(copy_b(j));
+  for (size_t i = 1; i < np; i++) HP_TRY(copy_a(i));
+  profile_mark(sin, "all_in");
   uint32_t* status = device_status(s);
   if (!status) {
     set_error("status word allocation failed");
     return HP_ERR_CUDA;
   }
-  int rc = launch_residues_tc(false, L, nullptr, 0, nullptr, nullptr, 0, B2, n, expB, bres.as<int8_t>(), Np, k, Kp,
-                              beta, D->num_sms, status, s, pdl);
-  if (rc == HP_ERR_UNSUPPORTED)
-    HP_CUDA_TRY(launch_residues_ab(false, L, pdl, dim3((unsigned)(Kp / (4 * RES_EPR)), (unsigned)(Np / RT_R)), s,
-                                   nullptr, 0, nullptr, nullptr, 0, 0, B2, (int64_t)n, expB, bres.as<int8_t>(),
-                                   (int64_t)(Np * Kp), (int64_t)k, beta, (int64_t)Kp));
-  else if (rc != HP_OK)
-    return rc;
+  HP_CUDA_TRY(cudaMemsetAsync(exps.p, 0, (Mpa + nq * pc) * sizeof(int), s));  // maxima merge by atomicMax
   const int nc = host_tables().crt[L].nc;
   for (size_t i = 0; i < np; i++) {
     const size_t r0 = i * pr, mi = std::min(pr, m - r0), Mpi = round_up(mi, GP_M);
     const double2* A2 = dA.as<const double2>() + r0 * k;
-    double* Ci = dC.as<double>() + r0 * n * 2;
+    int8_t* aresi = ares.as<int8_t>() + (size_t)L * r0 * Kp;  // L planes of Mpi x Kp
     HP_CUDA_TRY(cudaStreamWaitEvent(s, eA[i], 0));
-    HP_CUDA_TRY(cudaMemsetAsync(expA, 0, mi * sizeof(int), s));  // the row maxima merge by atomicMax
-    HP_TRY(launch_maxexp(A2, (const double2*)nullptr, mi, 0, k, false, expA, nullptr, s));
-    rc = launch_residues_tc(false, L, A2, mi, expA, ares.as<int8_t>(), Mpi, nullptr, 0, nullptr, nullptr, 0, k, Kp,
-                            beta, D->num_sms, status, s, pdl);
+    HP_TRY(launch_maxexp(A2, (const double2*)nullptr, mi, 0, k, false, expA + r0, nullptr, s));
+    int rc = launch_residues_tc(false, L, A2, mi, expA + r0, aresi, Mpi, nullptr, 0, nullptr, nullptr, 0, k, Kp, beta,
+                                D->num_sms, status, s, pdl);
     if (rc == HP_ERR_UNSUPPORTED) {
       const unsigned tay = (unsigned)(Mpi / RT_R);
       HP_CUDA_TRY(launch_residues_ab(false, L, pdl, dim3((unsigned)(Kp / (4 * RES_EPR)), tay), s, A2, (int64_t)mi,
-                                     expA, ares.as<int8_t>(), (int64_t)(Mpi * Kp), tay, nullptr, 0, nullptr, nullptr,
-                                     0, (int64_t)k, beta, (int64_t)Kp));
+                                     expA + r0, aresi, (int64_t)(Mpi * Kp), tay, nullptr, 0, nullptr, nullptr, 0,
+                                     (int64_t)k, beta, (int64_t)Kp));
     } else if (rc != HP_OK) {
       return rc;
     }
-    HP_TRY(ozaki_residue_gemm_pair(ares.as<int8_t>(), bres.as<int8_t>(), cres.as<uint8_t>(), L, Mpi, Np, Kp, s, pdl,
-                                   true));
-    if (L >= CRT_CONST_L0 && L < CRT_CONST_L0 + CRT_CONST_N)
-      HP_TRY(launch_crt_tc(cres.as<uint8_t>(), Mpi, Np, mi, n, expA, expB, beta, L, reinterpret_cast<double2*>(Ci),
-                           D->num_sms, status, s, pdl));
-    else
-      HP_TRY(launch_crt_dd(cres.as<uint8_t>(), Mpi, Np, mi, n, expA, expB, beta, D->crt + L, nc,
-                           reinterpret_cast<double2*>(Ci), s, pdl, L));
-    HP_CUDA_TRY(cudaEventRecord(eC[i], s));
-    HP_CUDA_TRY(cudaStreamWaitEvent(sout, eC[i], 0));
-    HP_CUDA_TRY(cudaMemcpyAsync(reinterpret_cast<char*>(c) + r0 * n * 16, Ci, mi * n * 16, cudaMemcpyDeviceToHost,
-                                sout));
+    for (size_t j = 0; j < nq; j++) {
+      const size_t j0 = j * pc, nj = std::min(pc, n - j0);
+      int8_t* bresj = bres.as<int8_t>() + (size_t)L * j0 * Kp;  // L planes of pc x Kp
+      if (i == 0) {  // B panel j's column exponents and residue planes, once
+        const double2* Bj = dB.as<const double2>() + j0 * k;
+        HP_CUDA_TRY(cudaStreamWaitEvent(s, eB[j], 0));
+        HP_TRY(launch_maxexp((const double2*)nullptr, Bj, 0, nj, k, false, nullptr, expB + j0, s));
+        rc = launch_residues_tc(false, L, nullptr, 0, nullptr, nullptr, 0, Bj, nj, expB + j0, bresj, pc, k, Kp, beta,
+                                D->num_sms, status, s, pdl);
+        if (rc == HP_ERR_UNSUPPORTED)
+          HP_CUDA_TRY(launch_residues_ab(false, L, pdl, dim3((unsigned)(Kp / (4 * RES_EPR)), (unsigned)(pc / RT_R)), s,
+                                         nullptr, 0, nullptr, nullptr, 0, 0, Bj, (int64_t)nj, expB + j0, bresj,
+                                         (int64_t)(pc * Kp), (int64_t)k, beta, (int64_t)Kp));
+        else if (rc != HP_OK)
+          return rc;
+      }
+      HP_TRY(ozaki_residue_gemm_pair(aresi, bresj, cres.as<uint8_t>(), L, Mpi, pc, Kp, s, pdl, true));
+      double* Cij = dC.as<double>() + (r0 * n + j0) * 2;
+      if (tc_crt)
+        HP_TRY(launch_crt_tc(cres.as<uint8_t>(), Mpi, pc, mi, nj, expA + r0, expB + j0, beta, L,
+                             reinterpret_cast<double2*>(Cij), D->num_sms, status, s, pdl, n));
+      else  // one column panel (nj = n)
+        HP_TRY(launch_crt_dd(cres.as<uint8_t>(), Mpi, pc, mi, n, expA + r0, expB, beta, D->crt + L, nc,
+                             reinterpret_cast<double2*>(Cij), s, pdl, L));
+      cudaEvent_t e = eC[i * nq + j];
+      HP_CUDA_TRY(cudaEventRecord(e, s));
+      HP_CUDA_TRY(cudaStreamWaitEvent(sout, e, 0));
+      HP_CUDA_TRY(cudaMemcpy2DAsync(reinterpret_cast<char*>(c) + (r0 * n + j0) * 16, n * 16, Cij, n * 16, nj * 16, mi,
+                                    cudaMemcpyDeviceToHost, sout));
+      if (i == 0 && j == 0) profile_mark(sout, "c00_out");
+    }
   }
+  profile_mark(s, "blocks_done");
+  profile_mark(sout, "all_out");
   HP_CUDA_TRY(cudaStreamSynchronize(sout));
   HP_CUDA_TRY(cudaStreamSynchronize(s));
   return consume_device_status(s);

@@ -295,12 +295,14 @@ def test_f128_ozaki_long_k_chunks(gpu, atb):
     assert err <= 4 * k * 2.0 ** -104, err
 
 
-@pytest.mark.parametrize("m,n,k", [(512, 130, 200), (700, 257, 129), (1100, 64, 300), (2050, 33, 65)])
+@pytest.mark.parametrize("m,n,k", [(512, 130, 200), (700, 257, 129), (1100, 64, 300), (2050, 33, 65),
+                                   (600, 1100, 70), (1024, 2048, 130), (530, 1024, 129)])
 def test_f128_ozaki_host_pipeline_matches_device(gpu, m, n, k):
-    """Host-pointer chosen GEMMs with m >= 512 run B once and A in row panels
-    (copies overlapped with the panels' kernels); every entry must carry the
-    bits of the one-shot device-pointer path, ragged last panels included,
-    and the normwise tolerance against the oracle."""
+    """Host-pointer chosen GEMMs with m >= 512 run A in row panels and, for
+    n >= 1024, B and C in two column panels (copies overlapped with the
+    blocks' kernels); every entry must carry the bits of the one-shot
+    device-pointer path, ragged last panels included, and the normwise
+    tolerance against the oracle."""
     import torch
 
     a, b = gemm_operands(m, n, k, seed=7 + m)
@@ -311,6 +313,26 @@ def test_f128_ozaki_host_pipeline_matches_device(gpu, m, n, k):
     gpu.f128_gemm_dev(da, db, dc, m, n, k, gpu.OZAKI, stream=s.cuda_stream)
     s.synchronize()
     assert np.array_equal(c_host, dc.cpu().numpy())
-    if m == 700:
+    if m in (700, 600):
         err = normwise_err(c_host, O.gemm(a, b, m, n, k), abs_prod(a, b, False))
         assert err <= 4 * k * 2.0 ** -104, err
+
+
+def test_f128_ozaki_host_column_panels_nonfinite(gpu):
+    """The host pipeline's second column panel carries its own column
+    exponents: a NaN column there, an inf row, and every other entry equal bit
+    for bit to the one-shot device-pointer path."""
+    import torch
+
+    m, n, k = 600, 1100, 60
+    a, b = gemm_operands(m, n, k, seed=77)
+    a[11, 5, 0] = np.inf
+    b[7, 1050, 1] = np.nan
+    c_host = gpu.f128_gemm(a, b, m, n, k, gpu.OZAKI)
+    da, db = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+    dc = torch.empty((m, n, 2), dtype=torch.float64, device="cuda")
+    s = torch.cuda.current_stream()
+    gpu.f128_gemm_dev(da, db, dc, m, n, k, gpu.OZAKI, stream=s.cuda_stream)
+    s.synchronize()
+    assert np.all(np.isnan(c_host[11, :, 0])) and np.all(np.isnan(c_host[:, 1050, 0]))
+    assert np.array_equal(c_host, dc.cpu().numpy(), equal_nan=True)
