@@ -913,6 +913,41 @@ def profile_case_f256(args):
     return 0
 
 
+def profile_case_e2e(args):
+    """The host-pointer f128 GEMM at 2048^3 from pinned host buffers, with the
+    library's timeline marks on: per call, the device times (ms from the
+    call's start) at which B's first panel and all operands have landed, the
+    first C block is back, the last block is computed and all of C is back."""
+    import ctypes
+
+    import torch
+
+    import quadprec_b200 as hp
+    from quadprec_b200.workloads import gemm_operands
+
+    a_np, b_np = gemm_operands(M, N, K, seed=0)
+    ha, hb = torch.from_numpy(a_np).pin_memory(), torch.from_numpy(b_np).pin_memory()
+    hc = torch.empty((M, N, 2), dtype=torch.float64).pin_memory()
+    lib = hp.lib()
+    for _ in range(args.warmup):
+        hp.check(lib.hp_f128_gemm(ha.data_ptr(), hb.data_ptr(), hc.data_ptr(), M, N, K, hp.OZAKI))
+    for _ in range(args.steps):
+        lib.hp_profile_enable(1)
+        t0 = time.perf_counter()
+        hp.check(lib.hp_f128_gemm(ha.data_ptr(), hb.data_ptr(), hc.data_ptr(), M, N, K, hp.OZAKI))
+        wall = (time.perf_counter() - t0) * 1e3
+        ms = (ctypes.c_double * 32)()
+        names = ctypes.create_string_buffer(1024)
+        cnt = lib.hp_profile_read(ms, 32, names, 1024)
+        lib.hp_profile_enable(0)
+        t, marks = 0.0, []
+        for nm, d in zip(names.value.decode().split(","), ms[:cnt]):
+            t += d
+            marks.append(f"{nm}={t:.3f}")
+        print(f"call {wall:.3f} ms (host clock): " + " ".join(marks), flush=True)
+    return 0
+
+
 # ---------------------------------------------------------------- main arm
 def main():
     ap = argparse.ArgumentParser()
@@ -926,7 +961,7 @@ def main():
     ap.add_argument("--spd-steps", type=int, default=3)
     ap.add_argument("--no-batched", action="store_true", help="skip the batched SPD / Jacobi section")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint section")
-    ap.add_argument("--profile-case", nargs="?", const="gemm", default=None, choices=["gemm", "spd", "batched", "chol512", "f256"],
+    ap.add_argument("--profile-case", nargs="?", const="gemm", default=None, choices=["gemm", "spd", "batched", "chol512", "f256", "e2e"],
                     help="only run warmup + steps of one chosen-path workload (for ncu captures)")
     args = ap.parse_args()
     if args.impl == "reference":
@@ -939,6 +974,8 @@ def main():
         return profile_case_chol512(args)
     if args.profile_case == "f256":
         return profile_case_f256(args)
+    if args.profile_case == "e2e":
+        return profile_case_e2e(args)
     if args.profile_case == "batched":
         import torch
 
