@@ -46,9 +46,10 @@ int gemm_host(int limbs, const double* a, const double* b, double* c, size_t m, 
   size_t ba, bb, bc;
   HP_TRY(check_args(a, b, c, m, n, k, mode, limbs, &ba, &bb, &bc));
   if (bc == 0) return HP_OK;
-  // chosen f128 A B with enough rows to split: B first, then A in row panels
-  // whose kernels and copies back overlap the remaining copies
-  if (limbs == 2 && mode == HP_MODE_OZAKI && !atb && m >= 512 && k > 0) return ozaki_dd_gemm_host(a, b, c, m, n, k);
+  // chosen f128 op(A) B with enough rows to split: op(A) in row panels and B
+  // in column panels, the blocks' kernels and copies back overlapping the
+  // remaining copies
+  if (limbs == 2 && mode == HP_MODE_OZAKI && m >= 512 && k > 0) return ozaki_dd_gemm_host(a, b, c, m, n, k, atb);
   cudaStream_t s = library_stream();
   DevBuf da(ba, s), db(bb, s), dc(bc, s);
   if ((ba && !da.p) || (bb && !db.p) || !dc.p) {

@@ -2232,8 +2232,9 @@ int ozaki_dd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
   return HP_OK;
 }
 
-// Host-pointer f128 GEMM C = A B (chosen mode) with the PCIe copies
-// overlapped. A streams in as row panels and B as column panels (two for
+// Host-pointer f128 GEMM C = op(A) B (chosen mode) with the PCIe copies
+// overlapped. op(A) streams in as row panels (with atb, A's column panels,
+// each copied into a compact k x rows matrix) and B as column panels (two for
 // n >= 1024, else one) on a copy stream, in the order the blocks use them:
 // B's first panel, A's first panel, B's other panels, A's other panels.
 // Each panel's exponents and residue planes are formed once, as soon as its
@@ -2277,7 +2278,7 @@ struct EventSet {
 };
 }  // namespace
 
-int ozaki_dd_gemm_host(const double* a, const double* b, double* c, size_t m, size_t n, size_t k) {
+int ozaki_dd_gemm_host(const double* a, const double* b, double* c, size_t m, size_t n, size_t k, bool atb) {
   using namespace ozaki;
   DevTables* D;
   HP_TRY(device_tables(&D));
@@ -2341,10 +2342,14 @@ int ozaki_dd_gemm_host(const double* a, const double* b, double* c, size_t m, si
     HP_CUDA_TRY(cudaEventRecord(eB[j], sin));
     return HP_OK;
   };
-  auto copy_a = [&](size_t i) -> int {
+  auto copy_a = [&](size_t i) -> int {  // rows r0 .. of op(A); with atb, A's columns r0 .. as a compact k x mi panel
     const size_t r0 = i * pr, mi = std::min(pr, m - r0);
-    HP_CUDA_TRY(cudaMemcpyAsync(dA.as<char>() + r0 * k * 16, reinterpret_cast<const char*>(a) + r0 * k * 16,
-                                mi * k * 16, cudaMemcpyHostToDevice, sin));
+    if (atb)
+      HP_CUDA_TRY(cudaMemcpy2DAsync(dA.as<char>() + r0 * k * 16, mi * 16, reinterpret_cast<const char*>(a) + r0 * 16,
+                                    m * 16, mi * 16, k, cudaMemcpyHostToDevice, sin));
+    else
+      HP_CUDA_TRY(cudaMemcpyAsync(dA.as<char>() + r0 * k * 16, reinterpret_cast<const char*>(a) + r0 * k * 16,
+                                  mi * k * 16, cudaMemcpyHostToDevice, sin));
     HP_CUDA_TRY(cudaEventRecord(eA[i], sin));
     return HP_OK;
   };
@@ -2366,12 +2371,12 @@ int ozaki_dd_gemm_host(const double* a, const double* b, double* c, size_t m, si
     const double2* A2 = dA.as<const double2>() + r0 * k;
     int8_t* aresi = ares.as<int8_t>() + (size_t)L * r0 * Kp;  // L planes of Mpi x Kp
     HP_CUDA_TRY(cudaStreamWaitEvent(s, eA[i], 0));
-    HP_TRY(launch_maxexp(A2, (const double2*)nullptr, mi, 0, k, false, expA + r0, nullptr, s));
-    int rc = launch_residues_tc(false, L, A2, mi, expA + r0, aresi, Mpi, nullptr, 0, nullptr, nullptr, 0, k, Kp, beta,
+    HP_TRY(launch_maxexp(A2, (const double2*)nullptr, mi, 0, k, atb, expA + r0, nullptr, s));
+    int rc = launch_residues_tc(atb, L, A2, mi, expA + r0, aresi, Mpi, nullptr, 0, nullptr, nullptr, 0, k, Kp, beta,
                                 D->num_sms, status, s, pdl);
     if (rc == HP_ERR_UNSUPPORTED) {
       const unsigned tay = (unsigned)(Mpi / RT_R);
-      HP_CUDA_TRY(launch_residues_ab(false, L, pdl, dim3((unsigned)(Kp / (4 * RES_EPR)), tay), s, A2, (int64_t)mi,
+      HP_CUDA_TRY(launch_residues_ab(atb, L, pdl, dim3((unsigned)(Kp / (4 * RES_EPR)), tay), s, A2, (int64_t)mi,
                                      expA + r0, aresi, (int64_t)(Mpi * Kp), tay, nullptr, 0, nullptr, nullptr, 0,
                                      (int64_t)k, beta, (int64_t)Kp));
     } else if (rc != HP_OK) {

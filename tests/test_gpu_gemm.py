@@ -295,26 +295,28 @@ def test_f128_ozaki_long_k_chunks(gpu, atb):
     assert err <= 4 * k * 2.0 ** -104, err
 
 
+@pytest.mark.parametrize("atb", [False, True])
 @pytest.mark.parametrize("m,n,k", [(512, 130, 200), (700, 257, 129), (1100, 64, 300), (2050, 33, 65),
                                    (600, 1100, 70), (1024, 2048, 130), (530, 1024, 129)])
-def test_f128_ozaki_host_pipeline_matches_device(gpu, m, n, k):
-    """Host-pointer chosen GEMMs with m >= 512 run A in row panels and, for
+def test_f128_ozaki_host_pipeline_matches_device(gpu, m, n, k, atb):
+    """Host-pointer chosen GEMMs with m >= 512 run op(A) in row panels (with
+    atb, A's column panels copied into compact k x rows matrices) and, for
     n >= 1024, B and C in two column panels (copies overlapped with the
     blocks' kernels); every entry must carry the bits of the one-shot
     device-pointer path, ragged last panels included, and the normwise
     tolerance against the oracle."""
     import torch
 
-    a, b = gemm_operands(m, n, k, seed=7 + m)
-    c_host = gpu.f128_gemm(a, b, m, n, k, gpu.OZAKI)
+    a, b = gemm_operands(m, n, k, seed=7 + m, atb=atb)
+    c_host = gpu.f128_gemm(a, b, m, n, k, gpu.OZAKI, atb)
     da, db = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
     dc = torch.empty((m, n, 2), dtype=torch.float64, device="cuda")
     s = torch.cuda.current_stream()
-    gpu.f128_gemm_dev(da, db, dc, m, n, k, gpu.OZAKI, stream=s.cuda_stream)
+    gpu.f128_gemm_dev(da, db, dc, m, n, k, gpu.OZAKI, atb=atb, stream=s.cuda_stream)
     s.synchronize()
     assert np.array_equal(c_host, dc.cpu().numpy())
     if m in (700, 600):
-        err = normwise_err(c_host, O.gemm(a, b, m, n, k), abs_prod(a, b, False))
+        err = normwise_err(c_host, O.gemm(a, b, m, n, k, atb=atb), abs_prod(a, b, atb))
         assert err <= 4 * k * 2.0 ** -104, err
 
 
