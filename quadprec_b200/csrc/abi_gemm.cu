@@ -50,6 +50,7 @@ int gemm_host(int limbs, const double* a, const double* b, double* c, size_t m, 
   // in column panels, the blocks' kernels and copies back overlapping the
   // remaining copies
   if (limbs == 2 && mode == HP_MODE_OZAKI && m >= 512 && k > 0) return ozaki_dd_gemm_host(a, b, c, m, n, k, atb);
+  if (limbs == 4 && mode == HP_MODE_OZAKI && m >= 512 && k > 0) return ozaki_qd_gemm_host(a, b, c, m, n, k, atb);
   cudaStream_t s = library_stream();
   DevBuf da(ba, s), db(bb, s), dc(bc, s);
   if ((ba && !da.p) || (bb && !db.p) || !dc.p) {

@@ -26,6 +26,7 @@ int ozaki_qd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
 // Host pointers, C = A B: copies overlapped with the panels' kernels (bit-
 // identical to ozaki_dd_gemm); synchronous.
 int ozaki_dd_gemm_host(const double* a, const double* b, double* c, size_t m, size_t n, size_t k, bool atb);
+int ozaki_qd_gemm_host(const double* a, const double* b, double* c, size_t m, size_t n, size_t k, bool atb);
 }  // namespace hp
 
 namespace hp {

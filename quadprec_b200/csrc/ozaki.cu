@@ -1866,11 +1866,12 @@ static int launch_crt_tc(const uint8_t* cres, size_t Mp, size_t Np, size_t m, si
 }
 
 // The f256 GEMM's CRT on the tensor core: g holds G1's L planes of Mp x Np
-// bytes followed by G2's. HP_ERR_UNSUPPORTED (nothing launched) for L
-// outside 28..32 or Np not a multiple of 128.
+// bytes followed by G2's; row i of the m x n result goes to C + i ldc (ldc =
+// n when 0). HP_ERR_UNSUPPORTED (nothing launched) for L outside 28..32 or
+// Np not a multiple of 128.
 static int launch_crt_tc_qd(const uint8_t* g, size_t Mp, size_t Np, size_t m, size_t n, const int* expA,
                             const int* expB, int beta, int L, double4* C, int num_sms, uint32_t* status,
-                            cudaStream_t s) {
+                            cudaStream_t s, size_t ldc = 0) {
   if (L < CRT_CONST_L0 || L >= CRT_CONST_L0 + CRT_CONST_N || Np % 128 != 0) {
     set_error("ozaki f256: no tensor-core CRT for %d moduli", L);
     return HP_ERR_UNSUPPORTED;
@@ -1908,7 +1909,7 @@ static int launch_crt_tc_qd(const uint8_t* g, size_t Mp, size_t Np, size_t m, si
 #define HP_CRT_TCQ(LCV)                                                                                       \
   if (L == LCV) {                                                                                             \
     HP_CUDA_TRY(launch_k(true, crt_tc_kernel<LCV, true>, dim3(grid), dim3(CT_THREADS), CT_SMEM, s, map,        \
-                         (int64_t)m, (int64_t)n, expA, expB, beta, C, (int64_t)n, status));                   \
+                         (int64_t)m, (int64_t)n, expA, expB, beta, C, (int64_t)(ldc ? ldc : n), status));     \
     return HP_OK;                                                                                             \
   }
   HP_CRT_TCQ(28) HP_CRT_TCQ(29) HP_CRT_TCQ(30) HP_CRT_TCQ(31) HP_CRT_TCQ(32)
@@ -2436,13 +2437,14 @@ namespace ozaki {
 constexpr int BETA_QD = 210;
 
 // The f256 GEMM's residue rows on the tensor core (residue_tc_kernel<., ., QD>):
-// A (m x k, or k x m when atb) and B (k x n) of 4-limb entries; rows of 2 Kp
-// bytes, [Xh | Xl] for A and [Yl | Yh] for B, unsigned bytes. HP_ERR_UNSUPPORTED
-// (nothing launched) for moduli counts other than 28..32.
+// A (m x k, or k x m when atb) and B (k x n) of 4-limb entries, either may be
+// null (its planes are not written); rows of 2 Kp bytes, [Xh | Xl] for A and
+// [Yl | Yh] for B, unsigned bytes. HP_ERR_UNSUPPORTED (nothing launched) for
+// moduli counts other than 28..32 or operands not 32-byte aligned.
 static int launch_residues_tc_qd(bool atb, int L, const double4* A, size_t m, const int* expA, int8_t* outA,
                                  size_t Mp, const double4* B, size_t n, const int* expB, int8_t* outB, size_t Np,
                                  size_t k, size_t Kp, int num_sms, uint32_t* status, cudaStream_t s) {
-  if (L < CRT_CONST_L0 || L >= CRT_CONST_L0 + CRT_CONST_N || Mp % 4 || Np % 4 || Kp % RC_P ||
+  if (L < CRT_CONST_L0 || L >= CRT_CONST_L0 + CRT_CONST_N || (!A && !B) || Mp % 4 || Np % 4 || Kp % RC_P ||
       ((reinterpret_cast<uintptr_t>(A) | reinterpret_cast<uintptr_t>(B)) & 31u))
     return HP_ERR_UNSUPPORTED;
   static bool attr_set[64] = {};
@@ -2481,15 +2483,19 @@ static int launch_residues_tc_qd(bool atb, int L, const double4* A, size_t m, co
     return HP_OK;
   };
   CUtensorMap mapA, mapB;
-  HP_TRY(map3d(&mapB, B, k, n, 4, RC_P));  // B is k x n: 4 operand rows (columns) x 128 reduction indices
-  if (atb)
-    HP_TRY(map3d(&mapA, A, k, m, 4, RC_P));  // A is k x m
-  else
-    HP_TRY(map3d(&mapA, A, m, k, RC_P, 4));  // A is m x k: 128 reduction indices x 4 rows
-  ResidueOperand oa{outA, (int64_t)(Mp * 2 * Kp), (int64_t)(2 * Kp), expA, (int64_t)(Mp / 4), (int64_t)(Kp / RC_P),
-                    (int64_t)Kp};
-  ResidueOperand ob{outB, (int64_t)(Np * 2 * Kp), (int64_t)(2 * Kp), expB, (int64_t)(Np / 4), (int64_t)(Kp / RC_P),
-                    (int64_t)Kp};
+  if (B) HP_TRY(map3d(&mapB, B, k, n, 4, RC_P));  // B is k x n: 4 operand rows (columns) x 128 reduction indices
+  if (A) {
+    if (atb)
+      HP_TRY(map3d(&mapA, A, k, m, 4, RC_P));  // A is k x m
+    else
+      HP_TRY(map3d(&mapA, A, m, k, RC_P, 4));  // A is m x k: 128 reduction indices x 4 rows
+  }
+  if (!A) mapA = mapB;  // not read (no A tiles)
+  if (!B) mapB = mapA;
+  ResidueOperand oa{outA, (int64_t)(Mp * 2 * Kp), (int64_t)(2 * Kp), expA, A ? (int64_t)(Mp / 4) : 0,
+                    (int64_t)(Kp / RC_P), (int64_t)Kp};
+  ResidueOperand ob{outB, (int64_t)(Np * 2 * Kp), (int64_t)(2 * Kp), expB, B ? (int64_t)(Np / 4) : 0,
+                    (int64_t)(Kp / RC_P), (int64_t)Kp};
   const int grid = num_sms * 2;
 #define HP_RQ(LCV)                                                                                                \
   if (L == LCV) {                                                                                                 \
@@ -2935,6 +2941,138 @@ int ozaki_qd_gemm(const double* a, const double* b, double* c, size_t m, size_t 
   }
 #undef HP_CRTQ
   return HP_OK;
+}
+
+// Host-pointer f256 GEMM C = op(A) B (chosen mode) with the PCIe copies
+// overlapped, as ozaki_dd_gemm_host does for f128: op(A) in row panels (with
+// atb, A's column panels copied into compact k x rows matrices), B and C in
+// two column panels for n >= 1024, copies in the order B0, A0, B1, the rest
+// of A. Each panel's exponents and residue rows are formed once; each block of
+// C takes its two group GEMMs and the tensor-core CRT and goes back while later
+// blocks compute. Every entry's arithmetic is that of ozaki_qd_gemm, so the
+// result is bit-identical to the one-shot path. Moduli counts outside the
+// tensor-core kernels' 28..32 take the one-shot path with plain copies.
+int ozaki_qd_gemm_host(const double* a, const double* b, double* c, size_t m, size_t n, size_t k, bool atb) {
+  using namespace ozaki;
+  DevTables* D;
+  HP_TRY(device_tables(&D));
+  const int L = ozaki_moduli_for(2 * k, BETA_QD / 2);
+  if (L < 0) {
+    set_error("ozaki f256: k = %zu needs more moduli than the table holds", k);
+    return HP_ERR_UNSUPPORTED;
+  }
+  cudaStream_t s = library_stream(), sin = library_copy_stream(0), sout = library_copy_stream(1);
+  if (L < CRT_CONST_L0 || L >= CRT_CONST_L0 + CRT_CONST_N) {
+    DevBuf da(m * k * 32, s), db(k * n * 32, s), dc(m * n * 32, s);
+    if (!da.p || !db.p || !dc.p) {
+      set_error("ozaki f256: workspace allocation failed");
+      return HP_ERR_CUDA;
+    }
+    HP_CUDA_TRY(cudaMemcpyAsync(da.p, a, m * k * 32, cudaMemcpyHostToDevice, s));
+    HP_CUDA_TRY(cudaMemcpyAsync(db.p, b, k * n * 32, cudaMemcpyHostToDevice, s));
+    HP_TRY(ozaki_qd_gemm(da.as<double>(), db.as<double>(), dc.as<double>(), m, n, k, atb, s));
+    HP_CUDA_TRY(cudaMemcpyAsync(c, dc.p, m * n * 32, cudaMemcpyDeviceToHost, s));
+    HP_CUDA_TRY(cudaStreamSynchronize(s));
+    return consume_device_status(s);
+  }
+  const size_t Kp = round_up(k, GB_K);
+  const size_t panels_wanted = m >= 2048 ? 16 : m >= 1024 ? 8 : 4;
+  const size_t pr = round_up((m + panels_wanted - 1) / panels_wanted, GP_M);  // rows per A panel
+  const size_t np = (m + pr - 1) / pr;
+  const size_t pc = round_up((n + (n >= 1024 ? 1 : 0)) / (n >= 1024 ? 2 : 1), GP_N);  // columns per B panel
+  const size_t nq = (n + pc - 1) / pc;
+  const size_t Mpa = np * pr;
+  if (pr / GB_M * (pc / GB_N) * (size_t)L > (size_t)INT32_MAX || 2 * Kp > (size_t)INT32_MAX) {
+    set_error("ozaki f256: problem too large");
+    return HP_ERR_INVALID_ARG;
+  }
+  DevBuf dA(m * k * 32, s), dB(k * n * 32, s), dC(m * n * 32, s);
+  DevBuf exps((Mpa + nq * pc) * sizeof(int), s);
+  DevBuf ares((size_t)L * Mpa * 2 * Kp, s), bres((size_t)L * nq * pc * 2 * Kp, s), gg((size_t)2 * L * pr * pc, s);
+  if (!dA.p || !dB.p || !dC.p || !exps.p || !ares.p || !bres.p || !gg.p) {
+    set_error("ozaki f256: workspace allocation failed");
+    return HP_ERR_CUDA;
+  }
+  EventSet ev(1 + nq + np + np * nq);
+  if (!ev.ok()) {
+    set_error("ozaki f256: event creation failed");
+    return HP_ERR_CUDA;
+  }
+  StreamsDrain drain{s, sin, sout};
+  cudaEvent_t ready = ev.ev[0];
+  cudaEvent_t* eB = ev.ev.data() + 1;
+  cudaEvent_t* eA = eB + nq;
+  cudaEvent_t* eC = eA + np;
+  int* expA = exps.as<int>();
+  int* expB = expA + Mpa;
+  HP_CUDA_TRY(cudaEventRecord(ready, s));
+  HP_CUDA_TRY(cudaStreamWaitEvent(sin, ready, 0));
+  HP_CUDA_TRY(cudaStreamWaitEvent(sout, ready, 0));
+  auto copy_b = [&](size_t j) -> int {
+    const size_t j0 = j * pc, nj = std::min(pc, n - j0);
+    HP_CUDA_TRY(cudaMemcpy2DAsync(dB.as<char>() + j0 * k * 32, nj * 32, reinterpret_cast<const char*>(b) + j0 * 32,
+                                  n * 32, nj * 32, k, cudaMemcpyHostToDevice, sin));
+    HP_CUDA_TRY(cudaEventRecord(eB[j], sin));
+    return HP_OK;
+  };
+  auto copy_a = [&](size_t i) -> int {
+    const size_t r0 = i * pr, mi = std::min(pr, m - r0);
+    if (atb)
+      HP_CUDA_TRY(cudaMemcpy2DAsync(dA.as<char>() + r0 * k * 32, mi * 32, reinterpret_cast<const char*>(a) + r0 * 32,
+                                    m * 32, mi * 32, k, cudaMemcpyHostToDevice, sin));
+    else
+      HP_CUDA_TRY(cudaMemcpyAsync(dA.as<char>() + r0 * k * 32, reinterpret_cast<const char*>(a) + r0 * k * 32,
+                                  mi * k * 32, cudaMemcpyHostToDevice, sin));
+    HP_CUDA_TRY(cudaEventRecord(eA[i], sin));
+    return HP_OK;
+  };
+  HP_TRY(copy_b(0));
+  HP_TRY(copy_a(0));
+  for (size_t j = 1; j < nq; j++) HP_TRY(copy_b(j));
+  for (size_t i = 1; i < np; i++) HP_TRY(copy_a(i));
+  uint32_t* status = device_status(s);
+  if (!status) {
+    set_error("status word allocation failed");
+    return HP_ERR_CUDA;
+  }
+  HP_CUDA_TRY(cudaMemsetAsync(exps.p, 0, (Mpa + nq * pc) * sizeof(int), s));  // maxima merge by atomicMax
+  for (size_t i = 0; i < np; i++) {
+    const size_t r0 = i * pr, mi = std::min(pr, m - r0), Mpi = round_up(mi, GP_M);
+    const double4* A4 = dA.as<const double4>() + r0 * k;
+    int8_t* aresi = ares.as<int8_t>() + (size_t)L * r0 * 2 * Kp;  // L planes of Mpi x 2 Kp
+    HP_CUDA_TRY(cudaStreamWaitEvent(s, eA[i], 0));
+    HP_TRY(launch_maxexp(A4, (const double4*)nullptr, mi, 0, k, atb, expA + r0, nullptr, s));
+    int rc = launch_residues_tc_qd(atb, L, A4, mi, expA + r0, aresi, Mpi, nullptr, 0, nullptr, nullptr, 0, k, Kp,
+                                   D->num_sms, status, s);
+    if (rc != HP_OK) return rc == HP_ERR_UNSUPPORTED ? HP_ERR_CUDA : rc;  // device buffers are aligned
+    for (size_t j = 0; j < nq; j++) {
+      const size_t j0 = j * pc, nj = std::min(pc, n - j0);
+      int8_t* bresj = bres.as<int8_t>() + (size_t)L * j0 * 2 * Kp;  // L planes of pc x 2 Kp
+      if (i == 0) {
+        const double4* B4 = dB.as<const double4>() + j0 * k;
+        HP_CUDA_TRY(cudaStreamWaitEvent(s, eB[j], 0));
+        HP_TRY(launch_maxexp((const double4*)nullptr, B4, 0, nj, k, false, nullptr, expB + j0, s));
+        rc = launch_residues_tc_qd(false, L, nullptr, 0, nullptr, nullptr, 0, B4, nj, expB + j0, bresj, pc, k, Kp,
+                                   D->num_sms, status, s);
+        if (rc != HP_OK) return rc == HP_ERR_UNSUPPORTED ? HP_ERR_CUDA : rc;
+      }
+      uint8_t* g1 = gg.as<uint8_t>();
+      uint8_t* g2 = g1 + (size_t)L * Mpi * pc;
+      HP_TRY(ozaki_residue_gemm_pair(aresi, bresj, g1, L, Mpi, pc, Kp, s, true, true, 2 * Kp, 0, Kp));
+      HP_TRY(ozaki_residue_gemm_pair(aresi, bresj, g2, L, Mpi, pc, 2 * Kp, s, false, true));
+      double* Cij = dC.as<double>() + (r0 * n + j0) * 4;
+      HP_TRY(launch_crt_tc_qd(g1, Mpi, pc, mi, nj, expA + r0, expB + j0, BETA_QD, L, reinterpret_cast<double4*>(Cij),
+                              D->num_sms, status, s, n));
+      cudaEvent_t e = eC[i * nq + j];
+      HP_CUDA_TRY(cudaEventRecord(e, s));
+      HP_CUDA_TRY(cudaStreamWaitEvent(sout, e, 0));
+      HP_CUDA_TRY(cudaMemcpy2DAsync(reinterpret_cast<char*>(c) + (r0 * n + j0) * 32, n * 32, Cij, n * 32, nj * 32, mi,
+                                    cudaMemcpyDeviceToHost, sout));
+    }
+  }
+  HP_CUDA_TRY(cudaStreamSynchronize(sout));
+  HP_CUDA_TRY(cudaStreamSynchronize(s));
+  return consume_device_status(s);
 }
 
 

@@ -338,3 +338,26 @@ def test_f128_ozaki_host_column_panels_nonfinite(gpu):
     s.synchronize()
     assert np.all(np.isnan(c_host[11, :, 0])) and np.all(np.isnan(c_host[:, 1050, 0]))
     assert np.array_equal(c_host, dc.cpu().numpy(), equal_nan=True)
+
+
+@pytest.mark.parametrize("atb", [False, True])
+@pytest.mark.parametrize("m,n,k", [(512, 130, 60), (600, 1100, 70), (1024, 1024, 129), (530, 257, 200)])
+def test_f256_ozaki_host_pipeline_matches_device(gpu, m, n, k, atb):
+    """Host-pointer chosen f256 GEMMs with m >= 512 stream op(A) in row panels
+    and, for n >= 1024, B and C in two column panels; every entry must carry
+    the bits of the one-shot device-pointer path, and one shape is checked
+    against the oracle's mf_gemm at the entrywise bound 4 k 2^-208 |A||B|."""
+    import torch
+
+    a = qd_operand(k, m, 71 + m) if atb else qd_operand(m, k, 71 + m)
+    b = qd_operand(k, n, 73 + n)
+    c_host = gpu.f256_gemm(a, b, m, n, k, gpu.OZAKI, atb)
+    da, db = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+    dc = torch.empty((m, n, 4), dtype=torch.float64, device="cuda")
+    s = torch.cuda.current_stream()
+    gpu.f256_gemm_dev(da, db, dc, m, n, k, gpu.OZAKI, atb=atb, stream=s.cuda_stream)
+    s.synchronize()
+    assert np.array_equal(c_host, dc.cpu().numpy())
+    if (m, n) == (600, 1100):
+        ref = O.mf_gemm(4, a, b, m, n, k, atb=atb)
+        assert np.all(qd_entry_err(c_host, ref) <= 4 * k * 2.0 ** -208 * qd_abs_prod(a, b, atb) + 1e-300)
